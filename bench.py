@@ -1,0 +1,393 @@
+"""Benchmark: ns/day of NVE molecular dynamics on the 100k-atom LJ + PME water
+box (33,333 TIP3P-style waters, 90 Na+ / 90 Cl-, L = 99.90 A, PME grid 100^3,
+cutoff 10 A, skin 2 A, dt = 0.5 fs) through this package's fused engine.
+
+A step is one full MD step: conditional neighbor update (forced every 100
+steps as in the reference loop), LJ + direct Coulomb pair kernel, excluded
+correction, PME reciprocal, water bonds/angles and the leap-frog update, all
+in one CUDA graph with 64-bit fixed-point force accumulation.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank advances its own
+independent replica box (replicas only: one box does not shard across GPUs);
+value = total simulated ns of all replicas per day, timed as the max over
+ranks.  `--impl reference` times the reference's own CPU implementation of
+the same path (its neighbor_list / Lennard_Jones_force / PM_force code built
+from source into oracle/_ref) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ns/day at 100k-atom LJ+PME water; batched steps/s; force rel-err vs FP64"
+DT_FS = 0.5
+CUTOFF = 10.0
+SKIN = 2.0
+
+
+def ns_per_day(steps_per_s: float) -> float:
+    return steps_per_s * DT_FS * 1e-6 * 86400.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--waters", type=int, default=33333,
+                   help="box size (default: the 100k-atom configuration)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile-steps", type=int, default=30)
+    return p.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_box(n_waters: int, seed: int):
+    from sponge_b200 import systems
+    return systems.water_box(n_waters, seed=seed, ion_pairs=None)
+
+
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "pair_kernel_traffic.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return d
+    return None
+
+
+# --------------------------------------------------------------------------
+def cpu_reference_run(s, evals: int, warmup: int):
+    """Time the reference's own CPU path (oracle/_ref) on box `s`: per MD step
+    the conditional neighbor update, excluded correction, LJ + direct Coulomb
+    and PME reciprocal, plus 1/100 of a forced rebuild (the reference loop
+    forces one every 100 steps)."""
+    from oracle.oracle import REF_SO, ReferenceCPU
+    if not os.path.exists(REF_SO):
+        return None, "oracle/_ref/libsponge_ref.so not built"
+    ref = ReferenceCPU(exact=False)
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        ref.init(s, CUTOFF, SKIN)
+    cores = ref.max_threads()
+    t0 = time.perf_counter()
+    ref.nl_update_only(forced=True)
+    t_rebuild = time.perf_counter() - t0
+    for k in range(warmup):
+        ref.force_step(k)
+    t0 = time.perf_counter()
+    for k in range(evals):
+        ref.force_step(warmup + k)
+    t_step = (time.perf_counter() - t0) / evals + t_rebuild / 100.0
+    return dict(value=ns_per_day(1.0 / t_step), unit="ns/day", cores=cores,
+                kind="reference",
+                sample=(f"{evals} force evaluations (conditional neighbor update, "
+                        f"excluded correction, LJ + direct Coulomb, PME reciprocal) of "
+                        f"the {s.n}-atom box after {warmup} warm-up, plus one forced "
+                        f"rebuild amortised over 100 steps; {t_step * 1e3:.1f} ms/step "
+                        f"on {cores} threads"),
+                ms_per_step=t_step * 1e3), None
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    s = make_box(args.waters, seed=0)
+    evals = max(1, min(args.steps, 20))
+    warm = min(args.warmup, 1)
+    res, why = cpu_reference_run(s, evals, warm)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return 0
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": "ns/day", "n_gpus": args.gpus,
+        "steps": evals, "warmup": warm, "ms_per_step": res["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded water/NaCl box)",
+        "config": {"workload": f"{s.n}-atom water + NaCl NVE, cutoff 10 A, skin 2 A, "
+                               f"PME {100}^3, dt 0.5 fs", "atoms": s.n,
+                   "parallelism": "host threads (OpenMP)"},
+        "impl": "reference",
+        "cpu_baseline": {"value": res["value"], "unit": "ns/day", "cores": res["cores"],
+                         "kind": "reference", "sample": res["sample"]},
+        "e2e": {"value": res["value"], "unit": "ns/day", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from sponge_b200 import capi, systems
+    lib = capi.load()
+    s = make_box(args.waters, seed=rank)
+    n = s.n
+    opts = capi.options(cutoff=CUTOFF, skin=SKIN)
+    h = ctypes.c_void_p()
+    t = np.ascontiguousarray(s.lj_type, np.int32)
+    A = np.ascontiguousarray(s.lj_A, np.float32)
+    B = np.ascontiguousarray(s.lj_B, np.float32)
+    q = np.ascontiguousarray(s.charge, np.float32)
+    es = np.ascontiguousarray(s.excl_start, np.int32)
+    en = np.ascontiguousarray(s.excl_numbers, np.int32)
+    el = np.ascontiguousarray(s.excl_list, np.int32)
+    capi.check(lib.snb_engine_create(ctypes.byref(opts), n, capi.boundary(s.cell(), s.rcell()),
+                                     s.n_types, t.ctypes.data, A.ctypes.data, B.ctypes.data,
+                                     q.ctypes.data, es.ctypes.data, en.ctypes.data,
+                                     el.ctypes.data, len(el), ctypes.byref(h)), "engine_create")
+    nb, na = len(s.bonds), len(s.angles)
+    ba = np.ascontiguousarray(s.bonds[:, 0], np.int32)
+    bb = np.ascontiguousarray(s.bonds[:, 1], np.int32)
+    bk = np.full(nb, systems.BOND_K, np.float32)
+    br = np.full(nb, systems.BOND_R0, np.float32)
+    aa = np.ascontiguousarray(s.angles[:, 0], np.int32)
+    ab = np.ascontiguousarray(s.angles[:, 1], np.int32)
+    ac = np.ascontiguousarray(s.angles[:, 2], np.int32)
+    ak = np.full(na, systems.ANGLE_K, np.float32)
+    at = np.full(na, systems.ANGLE_T0, np.float32)
+    capi.check(lib.snb_engine_set_bonded(h, nb, ba.ctypes.data, bb.ctypes.data, bk.ctypes.data,
+                                         br.ctypes.data, na, aa.ctypes.data, ab.ctypes.data,
+                                         ac.ctypes.data, ak.ctypes.data, at.ctypes.data),
+               "set_bonded")
+    crd = torch.from_numpy(s.crd.reshape(-1).copy()).cuda()
+    vel = torch.from_numpy(s.vel.reshape(-1).copy()).cuda()
+    invm = torch.from_numpy((1.0 / s.mass).astype(np.float32)).cuda()
+    dt = DT_FS * 1e-3 * systems.TIME_CONVERSION
+    st = torch.cuda.Stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+    P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    K, W = args.steps, max(args.warmup, 3)
+
+    def steps(first, k):
+        capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm),
+                                                 ctypes.c_float(dt), first, k, sp),
+                   "md_steps_graph")
+
+    with torch.cuda.stream(st):
+        steps(0, W)
+    st.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    with torch.cuda.stream(st):
+        steps(W, K)
+    e1.record(st)
+    st.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * ns_per_day(K / (ms_max / 1e3))
+
+    # graph composition: our kernels per step
+    kn, libk = ctypes.c_int(0), ctypes.c_int(0)
+    capi.check(lib.snb_engine_graph_info(h, ctypes.byref(kn), ctypes.byref(libk), sp),
+               "graph_info")
+    ours_per_step = kn.value - libk.value
+    forced_steps = sum(1 for x in range(W, W + K) if x % 100 == 0)
+
+    # per-phase timing (stream launches, events between phases)
+    phases = np.zeros(7)
+    with torch.cuda.stream(st):
+        capi.check(lib.snb_engine_profile_steps(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                                W + K, args.profile_steps,
+                                                phases.ctypes.data, sp), "profile")
+    rebuilds, pairs = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    capi.check(lib.snb_engine_stats(h, ctypes.byref(rebuilds), ctypes.byref(pairs), sp), "stats")
+
+    # end-to-end through the public API with host buffers: every step copies
+    # crd + vel from pinned host memory, runs one step, reads crd + vel back
+    h_crd = torch.from_numpy(crd.cpu().numpy().copy()).pin_memory()
+    h_vel = torch.from_numpy(vel.cpu().numpy().copy()).pin_memory()
+    E = max(10, min(K, 200))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(st):
+        for k in range(E):
+            crd.copy_(h_crd, non_blocking=True)
+            vel.copy_(h_vel, non_blocking=True)
+            capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm),
+                                                     ctypes.c_float(dt), W + K + 1000 + k, 1,
+                                                     sp), "e2e step")
+            h_crd.copy_(crd, non_blocking=True)
+            h_vel.copy_(vel, non_blocking=True)
+            st.synchronize()
+    t_e2e = time.perf_counter() - t0
+    e2e_t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * ns_per_day(E / float(e2e_t.item()))
+    io_bytes = 2 * 3 * 4 * n
+
+    # roofline of the dominant kernel (the pair kernel), HBM view
+    pair_ms = float(phases[2])
+    listed = int(pairs.value)
+    alg_bytes = 4 * listed + 16 * n + 24 * n + 4 * (n + 1) + 4 * n
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (pair_ms * 1e-3) / 1e9
+    traffic = committed_traffic()
+    roofline = {"bound": "hbm", "kernel": "k_lj_direct", "achieved": achieved,
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": achieved / peak,
+                "traffic": (traffic["dram_bytes_per_launch"] if traffic else None),
+                "algorithmic_bytes": alg_bytes, "kernel_ms": pair_ms}
+    # FP32-pipe view: 47 flops per in-cutoff pair (force only) + 10 per other
+    # listed pair; in-cutoff count from the oracle-free density estimate
+    in_cut = listed * (CUTOFF / (CUTOFF + SKIN)) ** 3
+    flops = 47 * in_cut + 10 * (listed - in_cut)
+    roofline["fp32_tflops"] = flops / (pair_ms * 1e-3) / 1e12
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            res, why = cpu_reference_run(make_box(args.waters, seed=0), 10, 1)
+            cpu_base = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                        if res else {"unavailable": why})
+        except Exception as ex:  # noqa: BLE001
+            cpu_base = {"unavailable": f"{type(ex).__name__}: {ex}"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    lib.snb_engine_destroy(h)
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded water/NaCl box, random-orientation TIP3P-style waters)",
+        "config": {"workload": f"{n}-atom water + NaCl NVE MD, cutoff 10 A, skin 2 A, "
+                               f"PME 100^3 order 4, dt 0.5 fs, fixed-point accumulation",
+                   "atoms": n, "replicas": world,
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "working set > L2 (neighbor list alone ~140 MB)",
+                   "forced_rebuild_steps_in_timed_region": forced_steps},
+        "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": io_bytes,
+                "d2h_bytes_per_step": io_bytes, "steps": E},
+        "gpu_launches": ours_per_step * K,
+        "kernels_per_step": ours_per_step,
+        "library_kernels_per_step": libk.value,
+        "phase_ms": dict(zip(["neighbor", "pack", "pair", "excluded", "pme", "bonded",
+                              "integrate"], [round(float(x), 5) for x in phases])),
+        "nl_rebuilds": int(rebuilds.value), "pairs": listed,
+        "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clk,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,299 @@
+/* sponge_nb.h -- C ABI of the B200 (sm_100a) nonbonded hot path.
+ *
+ * Drop-in boundary for SPONGE's NEIGHBOR_LIST, LENNARD_JONES_INFORMATION,
+ * LJ_SOFT_CORE and Particle_Mesh modules.  Every module entry point below
+ * replaces one member function of those structs (file:line in the SPONGE
+ * source tree given beside it); arguments keep the reference's meaning and
+ * order.  Differences that follow from being a C ABI:
+ *   - `Boundary` is passed as snb_boundary (same fields: policy, cell, rcell);
+ *   - VECTOR* / LTMatrix3* are float* with 3 / 6 floats per atom;
+ *   - each call takes the CUDA stream to run on (NULL = legacy default
+ *     stream, what the reference uses) and returns a status code instead of
+ *     calling Throw_SPONGE_Error; snb_last_error() gives the message;
+ *   - the input keys the modules read from CONTROLLER are set on an
+ *     snb_options with snb_options_set() using the same key names.
+ * All pointer arguments of compute calls are device pointers unless named
+ * h_*.  Compute calls neither allocate nor synchronise, so they can be
+ * captured in a CUDA graph, except where a comment says otherwise.
+ *
+ * Accumulation: compute calls add (+=) into frc / atom_energy / atom_virial
+ * like the reference.  Internally each module accumulates in 64-bit fixed
+ * point (forces 2^40 per kcal/mol/A, energies and virials 2^32 per kcal/mol)
+ * so results do not depend on thread order, or, with
+ * accumulation = SNB_ACCUM_FLOAT, with float atomics (the plain path).
+ */
+#ifndef SPONGE_NB_H
+#define SPONGE_NB_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SNB_VERSION 1
+
+/* status codes */
+#define SNB_OK 0
+#define SNB_ERR_BAD_INPUT 1
+#define SNB_ERR_CUDA 2
+#define SNB_ERR_OVERFLOW 3
+#define SNB_ERR_TIMEOUT 4
+#define SNB_ERR_NOT_SUPPORTED 5
+
+#define SNB_ACCUM_FIXED64 0
+#define SNB_ACCUM_FLOAT 1
+
+/* NEIGHBOR_LIST::Update `update` argument (neighbor_list.h:112-116) */
+#define SNB_CONDITIONAL_UPDATE 0
+#define SNB_FORCED_UPDATE 1
+
+/* Boundary (utils/boundary.h:15-20): policy 0 open, 1 periodic; cell and
+ * rcell as LTMatrix3 {a11, a21, a22, a31, a32, a33}. */
+typedef struct snb_boundary {
+    int policy;
+    float cell[6];
+    float rcell[6];
+} snb_boundary;
+
+/* Input keys of the hot-path modules (docs/input-reference; defaults as the
+ * reference).  snb_options_set() accepts the reference key names:
+ *   cutoff, skin                                   (MD_core/nb.hpp:5-27)
+ *   neighbor_list_refresh_interval, neighbor_list_skin_permit,
+ *   neighbor_list_max_neighbor_numbers, neighbor_list_max_atom_in_grid_numbers,
+ *   neighbor_list_max_ghost_in_grid_numbers,
+ *   neighbor_list_check_overflow_interval,
+ *   neighbor_list_throw_error_when_overflow        (neighbor_list.cpp:276-305,
+ *                                                   885-940)
+ *   PM_fftx, PM_ffty, PM_fftz, PM_grid_spacing, PM_Direct_Tolerance,
+ *   PME_update_interval, PME_calculate_reciprocal_part,
+ *   PME_calculate_excluded_part                    (PM_force.cpp:315-503)
+ *   lambda_lj, soft_core_alpha, soft_core_powfer, soft_core_sigma,
+ *   soft_core_sigma_min                            (LJ_soft_core.cpp:496-558)
+ *   DOM_DEC_update_interval: the MD loop's forced neighbor rebuild period
+ *                                                  (Domain_decomposition.cpp:33-39,
+ *                                                   main.cpp:1805-1822)
+ * plus this library's own key `accumulation` = fixed64 | float. */
+typedef struct snb_options {
+    float cutoff;
+    float skin;
+    int nl_refresh_interval;
+    float nl_skin_permit;
+    int nl_max_neighbor_numbers;
+    int nl_max_atom_in_grid_numbers;
+    int nl_max_ghost_in_grid_numbers;
+    int nl_check_overflow_interval;
+    int nl_throw_error_when_overflow;
+    int pm_fftx, pm_ffty, pm_fftz;
+    float pm_grid_spacing;
+    float pm_direct_tolerance;
+    int pme_update_interval;
+    int pme_calculate_reciprocal_part;
+    int pme_calculate_excluded_part;
+    float lambda_lj;
+    float soft_core_alpha;
+    float soft_core_powfer;
+    float soft_core_sigma;
+    float soft_core_sigma_min;
+    int accumulation;
+    int dom_dec_update_interval;
+} snb_options;
+
+typedef struct snb_nl snb_nl;
+typedef struct snb_lj snb_lj;
+typedef struct snb_lj_soft snb_lj_soft;
+typedef struct snb_pme snb_pme;
+typedef struct snb_engine snb_engine;
+
+/* ---------------------------------------------------------------- misc */
+int snb_version(void);
+const char* snb_last_error(void);
+void snb_options_default(snb_options* opt);
+int snb_options_set(snb_options* opt, const char* key, const char* value);
+
+/* ------------------------------------------------------- NEIGHBOR_LIST */
+/* NEIGHBOR_LIST::Initial (neighbor_list.h:17-18, neighbor_list.cpp:871-972) */
+int snb_nl_create(const snb_options* opt, int atom_numbers, float cutoff,
+                  float skin, snb_boundary boundary, snb_nl** out);
+/* NEIGHBOR_LIST::Update (neighbor_list.h:19-22, neighbor_list.cpp:974-1025).
+ * crd: float[3*N].  ghost_numbers must be 0 (one domain). */
+int snb_nl_update(snb_nl* nl, const int* atom_local, int local_atom_numbers,
+                  int ghost_numbers, const float* crd, snb_boundary boundary,
+                  int step, int update, const int* excluded_list_start,
+                  const int* excluded_list, const int* excluded_numbers,
+                  void* stream);
+/* NEIGHBOR_LIST::Check_Overflow (neighbor_list.cpp:1027-1103): reads the
+ * overflow flag (host sync) and regrows the pair storage; *regrown = 1 when
+ * the last build overflowed and must be repeated (forced update). */
+int snb_nl_check_overflow(snb_nl* nl, int* regrown, void* stream);
+/* Number of listed pairs of the last build (host sync). */
+int snb_nl_pair_count(snb_nl* nl, long long* count, void* stream);
+/* The pair set as (global_i < global_j) pairs, unsorted (host sync). */
+int snb_nl_export_pairs(snb_nl* nl, int* d_pair_i, int* d_pair_j,
+                        long long capacity, long long* count, void* stream);
+/* NEIGHBOR_LIST::d_nl in the reference layout (neighbor_list.h:42-44,
+ * ATOM_GROUP {int atom_numbers; int ghost_numbers; int* atom_serial;},
+ * common.h:177-182): d_nl[N] rows point into d_serial_slab[N*max]; row i
+ * lists local j with atom_local[j] > atom_local[i].  Host sync. */
+int snb_nl_export_atom_groups(snb_nl* nl, void* d_nl, int* d_serial_slab,
+                              int max_neighbor_numbers, void* stream);
+/* NEIGHBOR_LIST::Clear (neighbor_list.cpp:1105-1119) */
+int snb_nl_destroy(snb_nl* nl);
+
+/* ------------------------------------------- LENNARD_JONES_INFORMATION */
+/* LENNARD_JONES_INFORMATION::Initial (Lennard_Jones_force.h:118-119,
+ * Lennard_Jones_force.cpp:147-250).  The type table replaces the Xponge
+ * LennardJones record: h_LJ_A/h_LJ_B are A'=12A, B'=6B per triangular pair
+ * index, as Xponge leaves them. */
+int snb_lj_create(const snb_options* opt, int atom_numbers,
+                  int atom_type_numbers, const int* h_atom_LJ_type,
+                  const float* h_LJ_A, const float* h_LJ_B, float cutoff,
+                  snb_lj** out);
+/* LENNARD_JONES_INFORMATION::Get_Local (Lennard_Jones_force.h:135-136) */
+int snb_lj_get_local(snb_lj* lj, const int* atom_local, int local_atom_numbers,
+                     int ghost_numbers, void* stream);
+/* LENNARD_JONES_INFORMATION::LJ_PME_Direct_Force_With_Atom_Energy_And_Virial
+ * (Lennard_Jones_force.h:139-145, Lennard_Jones_force.cpp:326-384).  `nl` is
+ * the neighbor list handle whose d_nl the reference would pass. */
+int snb_lj_pme_direct_force(snb_lj* lj, int atom_numbers,
+                            int local_atom_numbers, int solvent_numbers,
+                            int ghost_numbers, const float* crd,
+                            const float* charge, float* frc,
+                            snb_boundary boundary, snb_nl* nl, float pme_beta,
+                            int need_atom_energy, float* atom_energy,
+                            int need_virial, float* atom_virial,
+                            float* atom_direct_pme_energy, void* stream);
+/* LENNARD_JONES_INFORMATION::Long_Range_Correction (:168-170, .cpp:287-308) */
+int snb_lj_long_range_correction(snb_lj* lj, int need_pressure, float* d_virial,
+                                 int need_potential, float* d_potential,
+                                 float volume, void* stream);
+/* Step_Print's LJ_short sum (Lennard_Jones_force.cpp:386-400), host sync */
+int snb_lj_energy_sum(snb_lj* lj, float* h_LJ_energy_sum, void* stream);
+float snb_lj_long_range_factor(snb_lj* lj);
+int snb_lj_destroy(snb_lj* lj);
+
+/* -------------------------------------------------------- LJ_SOFT_CORE */
+/* LJ_SOFT_CORE::Initial (LJ_soft_core.h:238-239, LJ_soft_core.cpp:463-688):
+ * A/B end-state type tables and per-atom types, perturbation mask and the
+ * soft-core parameters (lambda_lj, soft_core_alpha, soft_core_powfer,
+ * soft_core_sigma, soft_core_sigma_min from opt). */
+int snb_lj_soft_create(const snb_options* opt, int atom_numbers,
+                       int atom_type_numbers_A, int atom_type_numbers_B,
+                       const int* h_LJ_type_A, const int* h_LJ_type_B,
+                       const float* h_LJ_AA, const float* h_LJ_AB,
+                       const float* h_LJ_BA, const float* h_LJ_BB,
+                       const int* h_subsys_mask, float cutoff,
+                       snb_lj_soft** out);
+/* LJ_SOFT_CORE::LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial
+ * (LJ_soft_core.h:247-254, LJ_soft_core.cpp:757-825).  charge_B_A is
+ * charge_B - charge_A per atom (NULL if charges are not perturbed). */
+int snb_lj_soft_pme_direct_force(snb_lj_soft* lj, int atom_numbers,
+                                 int local_atom_numbers, int ghost_numbers,
+                                 const float* crd, const float* charge,
+                                 const float* charge_B_A, float* frc,
+                                 snb_boundary boundary, snb_nl* nl,
+                                 float pme_beta, int need_atom_energy,
+                                 float* atom_energy, int need_virial,
+                                 float* atom_virial,
+                                 float* atom_direct_pme_energy, void* stream);
+/* LJ_SOFT_CORE::Get_Partial_H_Partial_Lambda_With_Columb_Direct
+ * (LJ_soft_core.h:256-260, .cpp:827-888): dH/dlambda of the pair terms,
+ * host sync. */
+int snb_lj_soft_dh_dlambda(snb_lj_soft* lj, const float* crd,
+                           const float* charge, const float* charge_B_A,
+                           snb_boundary boundary, snb_nl* nl, float pme_beta,
+                           int charge_perturbated, double* h_dH_dlambda,
+                           void* stream);
+/* LJ_SOFT_CORE::Long_Range_Correction (LJ_soft_core.h:262-264) */
+int snb_lj_soft_long_range_correction(snb_lj_soft* lj, int need_pressure,
+                                      float* d_virial, int need_potential,
+                                      float* d_potential, float volume,
+                                      void* stream);
+int snb_lj_soft_destroy(snb_lj_soft* lj);
+
+/* ------------------------------------------------------- Particle_Mesh */
+/* Particle_Mesh::Initial (PM_force.h:153-156, PM_force.cpp:295-654) */
+int snb_pme_create(const snb_options* opt, int atom_numbers,
+                   snb_boundary boundary, const float* box_length,
+                   float cutoff, snb_pme** out);
+float snb_pme_beta(snb_pme* pme);
+int snb_pme_grid(snb_pme* pme, int* fft3);
+/* Particle_Mesh::PME_Reciprocal_Force_With_Energy_And_Virial
+ * (PM_force.h:175-178, PM_force.cpp:1070-1168): forces += into force;
+ * self + reciprocal energy added to d_potential[0]; the reciprocal virial
+ * added to d_virial[0..5]. */
+int snb_pme_reciprocal_force(snb_pme* pme, const float* crd,
+                             snb_boundary boundary, const float* charge,
+                             float* force, int need_virial, int need_energy,
+                             float* d_virial, float* d_potential, int step,
+                             void* stream);
+/* Particle_Mesh::MPI_PME_Excluded_Force_With_Atom_Energy
+ * (PM_force.h:185-190, PM_force.cpp:1819-1842) */
+int snb_pme_excluded_force(snb_pme* pme, int atom_numbers,
+                           const int* atom_local, const int* atom_local_id,
+                           const float* crd, snb_boundary boundary,
+                           const float* charge, const int* excluded_list_start,
+                           const int* excluded_list,
+                           const int* excluded_atom_numbers, float* frc,
+                           int need_energy, float* atom_ene, int need_virial,
+                           float* atom_virial, void* stream);
+/* Step_Print detail: reciprocal and self energies and the reciprocal virial
+ * of the last energy/virial evaluation, FP64 (host sync). */
+int snb_pme_energies(snb_pme* pme, double* h_reciprocal, double* h_self,
+                     double* h_virial6, void* stream);
+int snb_pme_destroy(snb_pme* pme);
+
+/* ------------------------------------------------ fused force engine */
+/* The whole nonbonded force of Main_Calculate_Force (main.cpp:1389-1544:
+ * neighbor update, excluded correction, LJ + direct Coulomb, long-range LJ
+ * correction, PME reciprocal) for one box, in one stream, one fixed-point
+ * accumulator and one sorted frame: no host synchronisation, capturable in a
+ * CUDA graph.  Host arrays are copied at creation. */
+int snb_engine_create(const snb_options* opt, int atom_numbers,
+                      snb_boundary boundary, int atom_type_numbers,
+                      const int* h_atom_LJ_type, const float* h_LJ_A,
+                      const float* h_LJ_B, const float* h_charge,
+                      const int* h_excluded_list_start,
+                      const int* h_excluded_numbers, const int* h_excluded_list,
+                      int excluded_list_length, snb_engine** out);
+/* frc (float[3N]) += nonbonded force at crd (float[3N]).  When need_energy /
+ * need_virial, the FP64 totals are written to d_totals[0..7] =
+ * {LJ, LJ long-range, direct Coulomb, excluded correction, PME reciprocal,
+ *  PME self, (spare), potential sum} and d_totals[8..13] = virial tensor. */
+int snb_engine_force(snb_engine* e, const float* crd, float* frc, int step,
+                     int need_energy, int need_virial, double* d_totals,
+                     void* stream);
+/* Leap-frog NVE steps (MD_core/nve.hpp:3-16) of the same box with harmonic
+ * bonds E = k(r-r0)^2 and angles E = k(theta-theta0)^2 (bond.cpp:14-60,
+ * angle.cpp) on top of the nonbonded force: crd, vel updated in place. */
+int snb_engine_set_bonded(snb_engine* e, int bond_numbers, const int* h_bond_a,
+                          const int* h_bond_b, const float* h_bond_k,
+                          const float* h_bond_r0, int angle_numbers,
+                          const int* h_angle_a, const int* h_angle_b,
+                          const int* h_angle_c, const float* h_angle_k,
+                          const float* h_angle_theta0);
+int snb_engine_md_steps(snb_engine* e, float* crd, float* vel,
+                        const float* inverse_mass, float dt, int first_step,
+                        int steps, void* stream);
+/* Same as snb_engine_md_steps but replays a CUDA graph of one step (captured
+ * on first use). */
+int snb_engine_md_steps_graph(snb_engine* e, float* crd, float* vel,
+                              const float* inverse_mass, float dt,
+                              int first_step, int steps, void* stream);
+/* Tracing (the CUDA-event counterpart of the reference's TIME_RECORDER,
+ * utils/control/time_recorder.hpp:9-43): runs `steps` stream-launched steps
+ * with events between phases and writes the mean milliseconds per step of
+ * {neighbor update, pack, pair kernel, excluded correction, PME reciprocal,
+ *  bonded, integration} to h_phase_ms[0..6].  Host sync every step. */
+int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
+                             const float* inverse_mass, float dt, int first_step,
+                             int steps, double* h_phase_ms, void* stream);
+/* Kernel nodes of the captured one-step graph, total and cuFFT's share. */
+int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
+                          int* library_kernel_nodes, void* stream);
+/* Number of neighbor-list rebuilds so far and current pair count (host sync). */
+int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
+                     void* stream);
+int snb_engine_destroy(snb_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPONGE_NB_H */

@@ -1,0 +1,315 @@
+"""TEST INFRASTRUCTURE ONLY -- Python access to the two checkers.
+
+* ``Oracle``: the C restatement (``libsnb_oracle.so``): FP32 bit-exact neighbor
+  pair set and FP64 runs of the LJ/Coulomb direct sum, PME reciprocal part,
+  excluded-pair correction and long-range LJ correction.
+* ``ReferenceCPU``: the reference's own CPU modules compiled from its sources
+  (``oracle/_ref/libsponge_ref*.so``, built by ``make -C oracle ref``).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
+this module.  The product never does.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libsnb_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libsponge_ref.so")
+REF_EXACT_SO = os.path.join(HERE, "_ref", "libsponge_ref_exact.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def build_oracle(ref_root: str | None = None, with_reference: bool = True) -> None:
+    """Build the checkers (``make -C oracle [ref]``).  The reference part only
+    builds where its sources exist."""
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", HERE, "libsnb_oracle.so"])
+    ref_root = ref_root or "/root/reference/SPONGE"
+    if with_reference and os.path.isdir(ref_root):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"])
+
+
+class Oracle:
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build_oracle(with_reference=False)
+        L = ctypes.CDLL(path)
+        self.lib = L
+        L.snbo_get_beta.restype = ctypes.c_float
+        L.snbo_get_beta.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_int]
+        L.snbo_nl_pairs.restype = ctypes.c_int64
+        L.snbo_nl_pairs.argtypes = [
+            ctypes.c_int, _f32p, _f32p, _f32p, ctypes.c_float, ctypes.c_float,
+            _i32p, _i32p, _i32p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+        L.snbo_direct_f64.restype = None
+        L.snbo_direct_f64.argtypes = [
+            ctypes.c_int, _f32p, _f32p, _i32p, _f32p, _f32p, _f32p, _f32p,
+            ctypes.c_float, ctypes.c_float, _i64p, _i32p, _f64p, _f64p, _f64p,
+            _f64p, _f64p]
+        L.snbo_excluded_f64.restype = None
+        L.snbo_excluded_f64.argtypes = [
+            ctypes.c_int, _f32p, _f32p, _f32p, _f32p, ctypes.c_float, _i32p,
+            _i32p, _i32p, _f64p, _f64p, _f64p]
+        L.snbo_pme_f64.restype = None
+        L.snbo_pme_f64.argtypes = [
+            ctypes.c_int, _f32p, _f32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int,
+            ctypes.c_int, ctypes.c_float, _f64p, ctypes.POINTER(ctypes.c_double),
+            ctypes.POINTER(ctypes.c_double), _f64p, ctypes.c_void_p]
+        L.snbo_ewald_recip_f64.restype = ctypes.c_double
+        L.snbo_ewald_recip_f64.argtypes = [
+            ctypes.c_int, _f32p, _f32p, ctypes.c_float, ctypes.c_float,
+            ctypes.c_int, ctypes.c_void_p]
+        L.snbo_lrc_factor.restype = ctypes.c_float
+        L.snbo_lrc_factor.argtypes = [ctypes.c_int, _i32p, ctypes.c_int, _f32p,
+                                      ctypes.c_float]
+
+    # -- neighbor list (FP32, bit-exact contract) ---------------------------
+    def nl_pairs(self, crd, cell, rcell, cutoff, skin, excl_start=None,
+                 excl_numbers=None, excl_list=None):
+        """Half list as CSR (row_start int64[n+1], cols int32), rows sorted."""
+        crd = _c(crd, np.float32).reshape(-1)
+        n = crd.size // 3
+        if excl_start is None:
+            excl_start = np.zeros(n, np.int32)
+            excl_numbers = np.zeros(n, np.int32)
+            excl_list = np.zeros(1, np.int32)
+        es, en = _c(excl_start, np.int32), _c(excl_numbers, np.int32)
+        el = _c(excl_list if len(excl_list) else np.zeros(1), np.int32)
+        cell, rcell = _c(cell, np.float32), _c(rcell, np.float32)
+        total = self.lib.snbo_nl_pairs(n, crd, cell, rcell, cutoff, skin, es,
+                                       en, el, None, None, 0)
+        total = abs(int(total))
+        rs = np.zeros(n + 1, np.int64)
+        cols = np.zeros(max(total, 1), np.int32)
+        got = self.lib.snbo_nl_pairs(n, crd, cell, rcell, cutoff, skin, es, en,
+                                     el, rs.ctypes.data, cols.ctypes.data, total)
+        assert got == total, (got, total)
+        return rs, cols[:total]
+
+    def nl_pairs_system(self, s, cutoff, skin):
+        return self.nl_pairs(s.crd, s.cell(), s.rcell(), cutoff, skin,
+                             s.excl_start, s.excl_numbers, s.excl_list)
+
+    def get_beta(self, cutoff, tol=1e-5, precision=0):
+        return float(self.lib.snbo_get_beta(cutoff, tol, precision))
+
+    # -- FP64 method runs -----------------------------------------------------
+    def direct_f64(self, s, cutoff, beta, row_start, cols):
+        n = s.n
+        frc = np.zeros(3 * n)
+        ae, le, ce, vir = (np.zeros(n), np.zeros(n), np.zeros(n),
+                           np.zeros(6 * n))
+        self.lib.snbo_direct_f64(
+            n, _c(s.crd, np.float32).reshape(-1), _c(s.charge, np.float32),
+            _c(s.lj_type, np.int32), _c(s.lj_A, np.float32),
+            _c(s.lj_B, np.float32), s.cell(), s.rcell(), cutoff, beta,
+            _c(row_start, np.int64), _c(cols if len(cols) else np.zeros(1), np.int32),
+            frc, ae, le, ce, vir)
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, lj_energy=le,
+                    coulomb_energy=ce, virial=vir.reshape(n, 6))
+
+    def excluded_f64(self, s, beta):
+        n = s.n
+        frc, ae, vir = np.zeros(3 * n), np.zeros(n), np.zeros(6 * n)
+        el = s.excl_list if len(s.excl_list) else np.zeros(1, np.int32)
+        self.lib.snbo_excluded_f64(
+            n, _c(s.crd, np.float32).reshape(-1), _c(s.charge, np.float32),
+            s.cell(), s.rcell(), beta, _c(s.excl_start, np.int32),
+            _c(s.excl_numbers, np.int32), _c(el, np.int32), frc, ae, vir)
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6))
+
+    def pme_f64(self, s, grid, beta, want_phi=False):
+        n = s.n
+        frc = np.zeros(3 * n)
+        er, es = ctypes.c_double(0), ctypes.c_double(0)
+        vir = np.zeros(6)
+        phi = np.zeros(int(np.prod(grid))) if want_phi else None
+        self.lib.snbo_pme_f64(
+            n, _c(s.crd, np.float32).reshape(-1), _c(s.charge, np.float32),
+            s.cell(), s.rcell(), int(grid[0]), int(grid[1]), int(grid[2]), beta,
+            frc, ctypes.byref(er), ctypes.byref(es), vir,
+            phi.ctypes.data if want_phi else None)
+        out = dict(frc=frc.reshape(n, 3), e_recip=er.value, e_self=es.value,
+                   virial=vir)
+        if want_phi:
+            out["phi"] = phi.reshape(grid)
+        return out
+
+    def ewald_recip_f64(self, s, beta, kmax, with_force=True):
+        n = s.n
+        frc = np.zeros(3 * n) if with_force else None
+        e = self.lib.snbo_ewald_recip_f64(
+            n, _c(s.crd, np.float32).reshape(-1), _c(s.charge, np.float32),
+            float(s.box), beta, kmax, frc.ctypes.data if with_force else None)
+        return e, (frc.reshape(n, 3) if with_force else None)
+
+    def lrc_factor(self, s, cutoff):
+        return float(self.lib.snbo_lrc_factor(
+            s.n, _c(s.lj_type, np.int32), s.n_types, _c(s.lj_B, np.float32),
+            cutoff))
+
+
+class ReferenceCPU:
+    """The reference's own hot-path modules compiled for CPU (OpenMP)."""
+
+    def __init__(self, exact: bool = False):
+        path = REF_EXACT_SO if exact else REF_SO
+        if not os.path.exists(path):
+            raise FileNotFoundError(
+                f"{path} missing: build it with `make -C oracle ref` where the "
+                "reference sources are present")
+        L = ctypes.CDLL(path)
+        self.lib = L
+        L.ref_init.restype = ctypes.c_int
+        L.ref_init.argtypes = [
+            ctypes.c_int, _f32p, _f32p, _i32p, ctypes.c_int, _f32p, _f32p,
+            _i32p, _i32p, _i32p, ctypes.c_int, _f32p, ctypes.c_float,
+            ctypes.c_float, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
+        L.ref_grid.argtypes = [_i32p]
+        L.ref_nl_update.restype = ctypes.c_int
+        L.ref_nl_update.argtypes = [_f32p, ctypes.c_int, ctypes.c_int, _i32p,
+                                    ctypes.c_void_p, ctypes.c_longlong, _i32p]
+        L.ref_nl_update_only.restype = ctypes.c_int
+        L.ref_nl_update_only.argtypes = [_f32p, ctypes.c_int, ctypes.c_int]
+        L.ref_lj_direct.restype = ctypes.c_int
+        L.ref_lj_direct.argtypes = [_f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
+                                    ctypes.c_int, ctypes.c_int]
+        L.ref_pme_reciprocal.restype = ctypes.c_int
+        L.ref_pme_reciprocal.argtypes = [_f32p, _f32p, _f32p, _f32p, _f32p,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.ref_pme_excluded.restype = ctypes.c_int
+        L.ref_pme_excluded.argtypes = [_f32p, _f32p, _f32p, _f32p, ctypes.c_int,
+                                       ctypes.c_int]
+        L.ref_lj_long_range.restype = ctypes.c_int
+        L.ref_lj_long_range.argtypes = [_f32p, _f32p, ctypes.c_float]
+        L.ref_lj_long_range_factor.restype = ctypes.c_float
+        L.ref_set_threads.argtypes = [ctypes.c_int]
+        L.ref_max_threads.restype = ctypes.c_int
+        self.n = 0
+
+    def set_threads(self, t: int):
+        self.lib.ref_set_threads(int(t))
+
+    def max_threads(self) -> int:
+        return int(self.lib.ref_max_threads())
+
+    def init(self, s, cutoff, skin, commands: dict | None = None):
+        cmd = ";".join(f"{k}={v}" for k, v in (commands or {}).items())
+        beta = ctypes.c_float(0)
+        el = s.excl_list if len(s.excl_list) else np.zeros(1, np.int32)
+        self.crd = _c(s.crd, np.float32).reshape(-1)
+        rc = self.lib.ref_init(
+            s.n, self.crd, _c(s.charge, np.float32), _c(s.lj_type, np.int32),
+            s.n_types, _c(s.lj_A, np.float32), _c(s.lj_B, np.float32),
+            _c(s.excl_start, np.int32), _c(s.excl_numbers, np.int32),
+            _c(el, np.int32), int(len(s.excl_list)), s.cell(), cutoff, skin,
+            cmd.encode(), ctypes.byref(beta))
+        if rc != 0:
+            raise RuntimeError("reference init failed")
+        self.n = s.n
+        self.beta = beta.value
+        g = np.zeros(3, np.int32)
+        self.lib.ref_grid(g)
+        self.grid = tuple(int(x) for x in g)
+        return self.beta
+
+    def nl_update(self, crd=None, forced=True, step=0):
+        """Half list (reference order inside each row) as (counts, rows)."""
+        crd = self.crd if crd is None else _c(crd, np.float32).reshape(-1)
+        counts = np.zeros(self.n, np.int32)
+        ov = np.zeros(2, np.int32)
+        cap = self.n * 1200
+        serial = np.zeros(cap, np.int32)
+        rc = self.lib.ref_nl_update(crd, int(forced), step, counts,
+                                    serial.ctypes.data, cap, ov)
+        if rc != 0:
+            raise RuntimeError("reference NL update failed")
+        total = int(counts.sum())
+        return counts, serial[:total].copy(), ov
+
+    def nl_update_only(self, crd=None, forced=False, step=0):
+        crd = self.crd if crd is None else _c(crd, np.float32).reshape(-1)
+        if self.lib.ref_nl_update_only(crd, int(forced), step) != 0:
+            raise RuntimeError("reference NL update failed")
+
+    def force_step(self, step, crd=None):
+        """One force evaluation of the reference MD loop's nonbonded part
+        (main.cpp:1389-1544 order): conditional neighbor update, excluded
+        correction, LJ + direct Coulomb, PME reciprocal; forces only."""
+        crd = self.crd if crd is None else _c(crd, np.float32).reshape(-1)
+        n = self.n
+        if not hasattr(self, "_frc"):
+            self._frc = np.zeros(3 * n, np.float32)
+            self._e = np.zeros(n, np.float32)
+            self._v = np.zeros(6 * n, np.float32)
+            self._s = np.zeros(6, np.float32)
+            self._p = np.zeros(1, np.float32)
+            self._parts = np.zeros(2, np.float32)
+        self._frc[:] = 0
+        L = self.lib
+        ok = L.ref_nl_update_only(crd, 0, step) == 0
+        ok &= L.ref_pme_excluded(crd, self._frc, self._e, self._v, 0, 0) == 0
+        ok &= L.ref_lj_direct(crd, self._frc, self._e, self._v, self._e, self._e, 0, 0) == 0
+        ok &= L.ref_pme_reciprocal(crd, self._frc, self._s, self._p, self._parts, 0, 0,
+                                   step) == 0
+        if not ok:
+            raise RuntimeError("reference force step failed")
+        return self._frc
+
+    def lj_direct(self, crd=None, need_energy=True, need_virial=True):
+        crd = self.crd if crd is None else _c(crd, np.float32).reshape(-1)
+        n = self.n
+        frc = np.zeros(3 * n, np.float32)
+        ae, vir = np.zeros(n, np.float32), np.zeros(6 * n, np.float32)
+        le, ce = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        rc = self.lib.ref_lj_direct(crd, frc, ae, vir, le, ce, int(need_energy),
+                                    int(need_virial))
+        if rc != 0:
+            raise RuntimeError("reference LJ failed")
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6),
+                    lj_energy=le, coulomb_energy=ce)
+
+    def pme_reciprocal(self, crd=None, need_energy=True, need_virial=True, step=0):
+        crd = self.crd if crd is None else _c(crd, np.float32).reshape(-1)
+        n = self.n
+        frc = np.zeros(3 * n, np.float32)
+        vir = np.zeros(6, np.float32)
+        pot = np.zeros(1, np.float32)
+        parts = np.zeros(2, np.float32)
+        rc = self.lib.ref_pme_reciprocal(crd, frc, vir, pot, parts,
+                                         int(need_energy), int(need_virial), step)
+        if rc != 0:
+            raise RuntimeError("reference PME failed")
+        return dict(frc=frc.reshape(n, 3), virial=vir, potential=float(pot[0]),
+                    e_recip=float(parts[0]), e_self=float(parts[1]))
+
+    def pme_excluded(self, crd=None, need_energy=True, need_virial=True):
+        crd = self.crd if crd is None else _c(crd, np.float32).reshape(-1)
+        n = self.n
+        frc = np.zeros(3 * n, np.float32)
+        ae, vir = np.zeros(n, np.float32), np.zeros(6 * n, np.float32)
+        rc = self.lib.ref_pme_excluded(crd, frc, ae, vir, int(need_energy),
+                                       int(need_virial))
+        if rc != 0:
+            raise RuntimeError("reference excluded correction failed")
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6))
+
+    def lj_long_range(self, volume):
+        vir = np.zeros(6, np.float32)
+        pot = np.zeros(1, np.float32)
+        self.lib.ref_lj_long_range(vir, pot, volume)
+        return dict(virial=vir, potential=float(pot[0]),
+                    factor=float(self.lib.ref_lj_long_range_factor()))

@@ -1,0 +1,309 @@
+/* TEST INFRASTRUCTURE ONLY -- builds the reference's own CPU implementation
+ * of the nonbonded hot path (its unmodified neighbor_list.cpp,
+ * Lennard_Jones_force.cpp, LJ_soft_core.cpp, PM_force.cpp and common.cpp,
+ * compiled from the reference tree by oracle/Makefile) into oracle/_ref/.
+ *
+ * The reference's MD_core, Domain_decomposition, Xponge loaders and CONTROLLER
+ * implementation need HDF5 / toml++ and are not compiled.  This file supplies
+ * what the hot-path modules use of them: the CONTROLLER command map, printing
+ * and error entry points, the global Xponge::system, plus C entry points that
+ * let Python drive the modules on a synthetic system (host pointers: the CPU
+ * backend's "device" memory is host memory).  Nothing here re-implements the
+ * path itself; every force, list and energy comes from the reference code. */
+#include <omp.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "Lennard_Jones_force/LJ_soft_core.h"
+#include "Lennard_Jones_force/Lennard_Jones_force.h"
+#include "PM_force/PM_force.h"
+#include "control.h"
+#include "neighbor_list/neighbor_list.h"
+#include "xponge/xponge.h"
+
+/* ----------------------- CONTROLLER pieces ------------------------ */
+unsigned int CONTROLLER::device_optimized_block = 64;
+unsigned int CONTROLLER::device_warp = 32;
+unsigned int CONTROLLER::device_max_thread = 1024;
+int CONTROLLER::force_replica_count = 1;
+int CONTROLLER::MPI_rank = 0;
+int CONTROLLER::MPI_size = 1;
+int CONTROLLER::PP_MPI_size = 1;
+int CONTROLLER::PM_MPI_size = 1;
+int CONTROLLER::CC_MPI_size = 1;
+int CONTROLLER::PP_MPI_rank = 0;
+int CONTROLLER::PM_MPI_rank = 0;
+int CONTROLLER::CC_MPI_rank = 0;
+int CONTROLLER::CV_MPI_rank = 0;
+MPI_Comm CONTROLLER::pp_comm;
+MPI_Comm CONTROLLER::pm_comm;
+D_MPI_Comm CONTROLLER::D_MPI_COMM_WORLD;
+D_MPI_Comm CONTROLLER::d_pp_comm;
+D_MPI_Comm CONTROLLER::d_pm_comm;
+
+CONTROLLER controller;
+namespace Xponge
+{
+System system;
+}
+
+
+static std::string key_of(const char* prefix, const char* key)
+{
+    if (prefix == NULL || prefix[0] == 0) return key;
+    return std::string(prefix) + "_" + key;
+}
+bool CONTROLLER::Command_Exist(const char* key) { return commands.count(key); }
+bool CONTROLLER::Command_Exist(const char* prefix, const char* key)
+{
+    return commands.count(key_of(prefix, key));
+}
+const char* CONTROLLER::Command(const char* key)
+{
+    return commands[key].c_str();
+}
+const char* CONTROLLER::Command(const char* prefix, const char* key)
+{
+    return commands[key_of(prefix, key)].c_str();
+}
+bool CONTROLLER::Command_Choice(const char* key, const char* value,
+                                bool case_sensitive)
+{
+    return commands.count(key) && commands[key] == value;
+}
+bool CONTROLLER::Command_Choice(const char* prefix, const char* key,
+                                const char* value, bool case_sensitive)
+{
+    return Command_Choice(key_of(prefix, key).c_str(), value, case_sensitive);
+}
+TIME_RECORDER* CONTROLLER::Get_Time_Recorder(const char* name)
+{
+    return &time_recorders[name];
+}
+
+/* --------------------------- the system --------------------------- */
+namespace
+{
+struct RefContext
+{
+    int n = 0;
+    Boundary boundary;
+    VECTOR box;
+    float cutoff = 10.0f, skin = 2.0f;
+    std::vector<int> atom_local;
+    std::vector<int> excl_start, excl_numbers, excl_list;
+    std::vector<float> charge;
+    NEIGHBOR_LIST nl;
+    LENNARD_JONES_INFORMATION lj;
+    Particle_Mesh pm;
+    LJ_SOFT_CORE lj_soft;
+    bool soft_ready = false;
+    bool ready = false;
+};
+RefContext* g = NULL;
+std::string g_err;
+}  // namespace
+
+#define REF_TRY(body)                      \
+    try                                    \
+    {                                      \
+        body;                              \
+    }                                      \
+    catch (const std::exception& e)        \
+    {                                      \
+        g_err = e.what();                  \
+        fprintf(stderr, "%s\n", e.what()); \
+        return -1;                         \
+    }
+
+extern "C"
+{
+    const char* ref_last_error() { return g_err.c_str(); }
+    void ref_set_threads(int t)
+    {
+        if (t > 0) omp_set_num_threads(t);
+    }
+    int ref_max_threads() { return omp_get_max_threads(); }
+
+    /* commands: "key=value;key=value" in the reference's mdin key naming */
+    int ref_init(int n, const float* crd, const float* charge,
+                 const int* lj_type, int n_types, const float* lj_A,
+                 const float* lj_B, const int* excl_start,
+                 const int* excl_numbers, const int* excl_list, int n_excl,
+                 const float* cell6, float cutoff, float skin,
+                 const char* commands, float* beta_out)
+    {
+        REF_TRY({
+            delete g;
+            g = new RefContext();
+            g->n = n;
+            g->cutoff = cutoff;
+            g->skin = skin;
+            controller.commands.clear();
+            std::string c = commands ? commands : "";
+            size_t pos = 0;
+            while (pos < c.size())
+            {
+                size_t end = c.find(';', pos);
+                if (end == std::string::npos) end = c.size();
+                std::string kv = c.substr(pos, end - pos);
+                size_t eq = kv.find('=');
+                if (eq != std::string::npos)
+                    controller.commands[kv.substr(0, eq)] = kv.substr(eq + 1);
+                pos = end + 1;
+            }
+            g->boundary.policy = BoundaryPolicy::Periodic;
+            g->boundary.cell = LTMatrix3(cell6[0], cell6[1], cell6[2],
+                                         cell6[3], cell6[4], cell6[5]);
+            g->boundary.rcell = Invert_Lower_Triangular_Cell(g->boundary.cell);
+            g->box = VECTOR(cell6[0], cell6[2], cell6[5]);
+            g->atom_local.resize(n);
+            for (int i = 0; i < n; ++i) g->atom_local[i] = i;
+            g->excl_start.assign(excl_start, excl_start + n);
+            g->excl_numbers.assign(excl_numbers, excl_numbers + n);
+            g->excl_list.assign(excl_list, excl_list + (n_excl > 0 ? n_excl : 0));
+            g->excl_list.push_back(0);
+            g->charge.assign(charge, charge + n);
+
+            auto& ljff = Xponge::system.classical_force_field.lj;
+            ljff.atom_type.assign(lj_type, lj_type + n);
+            int npair = n_types * (n_types + 1) / 2;
+            ljff.pair_A.assign(lj_A, lj_A + npair);
+            ljff.pair_B.assign(lj_B, lj_B + npair);
+            ljff.atom_type_numbers = n_types;
+
+            g->lj.Initial(&controller, cutoff);
+            g->pm.Initial(&controller, n, g->boundary, g->box, cutoff, 0);
+            g->nl.Initial(&controller, n, cutoff, skin, g->boundary);
+            g->lj.Get_Local(g->atom_local.data(), n, 0);
+            if (beta_out) *beta_out = g->pm.beta;
+            g->ready = true;
+        });
+        return 0;
+    }
+
+    int ref_grid(int* fft3)
+    {
+        if (!g) return -1;
+        fft3[0] = g->pm.fftx;
+        fft3[1] = g->pm.ffty;
+        fft3[2] = g->pm.fftz;
+        return 0;
+    }
+
+    /* Runs NEIGHBOR_LIST::Update on crd (forced when forced != 0) and copies
+     * the half list out: counts[n] and, when serial != NULL, the rows packed
+     * back to back in list order (row i starts at sum of counts before it). */
+    int ref_nl_update(const float* crd, int forced, int step, int* counts,
+                      int* serial, long long cap, int* overflow)
+    {
+        if (!g) return -1;
+        REF_TRY({
+            g->nl.Update(g->atom_local.data(), g->n, 0, (VECTOR*)crd,
+                         g->boundary, step, forced ? 1 : 0,
+                         g->excl_start.data(), g->excl_list.data(),
+                         g->excl_numbers.data());
+            long long off = 0;
+            for (int i = 0; i < g->n; ++i)
+            {
+                ATOM_GROUP a = g->nl.d_nl[i];
+                counts[i] = a.atom_numbers;
+                if (serial && off + a.atom_numbers <= cap)
+                    memcpy(serial + off, a.atom_serial,
+                           sizeof(int) * a.atom_numbers);
+                off += a.atom_numbers;
+            }
+            if (overflow)
+            {
+                overflow[0] = g->nl.d_neighbor_list_overflow[0];
+                overflow[1] = g->nl.d_neighbor_grid_overflow[0];
+            }
+        });
+        return 0;
+    }
+
+    /* NEIGHBOR_LIST::Update alone (no copy-out): for timing the reference. */
+    int ref_nl_update_only(const float* crd, int forced, int step)
+    {
+        if (!g) return -1;
+        REF_TRY({
+            g->nl.Update(g->atom_local.data(), g->n, 0, (VECTOR*)crd,
+                         g->boundary, step, forced ? 1 : 0,
+                         g->excl_start.data(), g->excl_list.data(),
+                         g->excl_numbers.data());
+        });
+        return 0;
+    }
+
+    /* LJ_PME_Direct_Force_With_Atom_Energy_And_Virial with energy and virial.
+     * frc/atom_energy/atom_virial are accumulated into; lj_energy and
+     * coulomb_energy receive the module's per-atom arrays. */
+    int ref_lj_direct(const float* crd, float* frc, float* atom_energy,
+                      float* atom_virial, float* lj_energy,
+                      float* coulomb_energy, int need_energy, int need_virial)
+    {
+        if (!g) return -1;
+        REF_TRY({
+            std::vector<float> direct(g->n, 0.0f);
+            g->lj.LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(
+                g->n, g->n, 0, 0, (const VECTOR*)crd, g->charge.data(),
+                (VECTOR*)frc, g->boundary, g->nl.d_nl, g->pm.beta, need_energy,
+                atom_energy, need_virial, (LTMatrix3*)atom_virial,
+                direct.data());
+            if (lj_energy)
+                memcpy(lj_energy, g->lj.d_LJ_energy_atom, sizeof(float) * g->n);
+            if (coulomb_energy)
+                memcpy(coulomb_energy, direct.data(), sizeof(float) * g->n);
+        });
+        return 0;
+    }
+
+    /* PME_Reciprocal_Force_With_Energy_And_Virial: reciprocal forces into frc,
+     * self+reciprocal energy into potential[0], virial into virial6. */
+    int ref_pme_reciprocal(const float* crd, float* frc, float* virial6,
+                           float* potential, float* parts, int need_energy,
+                           int need_virial, int step)
+    {
+        if (!g) return -1;
+        REF_TRY({
+            g->pm.PME_Reciprocal_Force_With_Energy_And_Virial(
+                (const VECTOR*)crd, g->boundary, g->charge.data(),
+                (VECTOR*)frc, need_virial, need_energy, (LTMatrix3*)virial6,
+                potential, step);
+            if (parts)
+            {
+                parts[0] = g->pm.d_reciprocal_ene[0];
+                parts[1] = g->pm.d_self_ene[0];
+            }
+        });
+        return 0;
+    }
+
+    int ref_pme_excluded(const float* crd, float* frc, float* atom_energy,
+                         float* atom_virial, int need_energy, int need_virial)
+    {
+        if (!g) return -1;
+        REF_TRY({
+            g->pm.MPI_PME_Excluded_Force_With_Atom_Energy(
+                g->n, g->atom_local.data(), g->atom_local.data(),
+                (const VECTOR*)crd, g->boundary, g->charge.data(),
+                g->excl_start.data(), g->excl_list.data(),
+                g->excl_numbers.data(), (VECTOR*)frc, need_energy,
+                atom_energy, need_virial, (LTMatrix3*)atom_virial);
+        });
+        return 0;
+    }
+
+    int ref_lj_long_range(float* virial6, float* potential, float volume)
+    {
+        if (!g) return -1;
+        REF_TRY({
+            g->lj.Long_Range_Correction(1, (LTMatrix3*)virial6, 1, potential,
+                                        volume);
+        });
+        return 0;
+    }
+
+    float ref_lj_long_range_factor() { return g ? g->lj.long_range_factor : 0; }
+}

@@ -1,0 +1,681 @@
+/* TEST INFRASTRUCTURE ONLY -- the oracle.
+ *
+ * CPU restatement of SPONGE's nonbonded hot path, used only by tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg as the checker of the
+ * CUDA kernels.  The product (sponge_b200/) never links, loads or calls it.
+ *
+ * Two precisions on purpose:
+ *  - snbo_nl_pairs() evaluates the neighbor criterion exactly as the reference
+ *    does, in FP32 with no FMA contraction (build flag -ffp-contract=off), so
+ *    the pair set it returns is the bit-exact contract for the GPU list;
+ *  - everything else is an FP64 run of the same method (same formulas, same
+ *    weighting and per-atom assignment), the accuracy yardstick.
+ *
+ * Reference files restated (paths inside the SPONGE source tree):
+ *   utils/boundary.h:22-32           minimum image
+ *   utils/vector.hpp:249-346          LTMatrix3 products, virial from force/dis
+ *   neighbor_list/neighbor_list.cpp:504-548,637-733,736-807,847   half list
+ *   Lennard_Jones_force/Lennard_Jones_force.h:45-75, .cpp:45-137  pair terms
+ *   Lennard_Jones_force/Lennard_Jones_force.cpp:212-235,279-308  tail corr.
+ *   PM_force/PM_force.cpp:20-64,246-274,541-612,699-919,1024-1068,1142-1166,
+ *                         1745-1817                              PME
+ *   Lennard_Jones_force/LJ_soft_core.h:86-149, LJ_soft_core.cpp:196-461
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "fft_mixed.h"
+
+#define SNBO_API __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ */
+/* FP32 minimum image exactly as boundary.h:31 evaluates it:
+ *   dr - floorf(dr * rcell + 0.5f) * cell
+ * with VECTOR*LTMatrix3 = {x*a11 + y*a21 + z*a31, y*a22 + z*a32, z*a33}. */
+static void min_image_f32(const float* a, const float* b, const float* cell,
+                          const float* rcell, float* out)
+{
+    float dx = a[0] - b[0];
+    float dy = a[1] - b[1];
+    float dz = a[2] - b[2];
+    float sx = dx * rcell[0];
+    sx = sx + dy * rcell[1];
+    sx = sx + dz * rcell[3];
+    float sy = dy * rcell[2];
+    sy = sy + dz * rcell[4];
+    float sz = dz * rcell[5];
+    float fx = floorf(sx + 0.5f);
+    float fy = floorf(sy + 0.5f);
+    float fz = floorf(sz + 0.5f);
+    float cx = fx * cell[0];
+    cx = cx + fy * cell[1];
+    cx = cx + fz * cell[3];
+    float cy = fy * cell[2];
+    cy = cy + fz * cell[4];
+    float cz = fz * cell[5];
+    out[0] = dx - cx;
+    out[1] = dy - cy;
+    out[2] = dz - cz;
+}
+
+/* Same formula in double for the FP64 method runs. */
+static void min_image_f64(const float* a, const float* b, const float* cell,
+                          const float* rcell, double* out)
+{
+    double dx = (double)a[0] - b[0], dy = (double)a[1] - b[1],
+           dz = (double)a[2] - b[2];
+    double sx = dx * rcell[0] + dy * rcell[1] + dz * rcell[3];
+    double sy = dy * rcell[2] + dz * rcell[4];
+    double sz = dz * rcell[5];
+    double fx = floor(sx + 0.5), fy = floor(sy + 0.5), fz = floor(sz + 0.5);
+    out[0] = dx - (fx * cell[0] + fy * cell[1] + fz * cell[3]);
+    out[1] = dy - (fy * cell[2] + fz * cell[4]);
+    out[2] = dz - fz * cell[5];
+}
+
+/* LTMatrix3 += sign * Get_Virial_From_Force_Dis(f, d)   (vector.hpp:322-334) */
+static void virial_add(double* v, const double* f, const double* d, double s)
+{
+    v[0] += s * (f[0] * d[0]);
+    v[1] += s * (f[0] * d[1] + f[1] * d[0]);
+    v[2] += s * (f[1] * d[1]);
+    v[3] += s * (f[0] * d[2] + f[2] * d[0]);
+    v[4] += s * (f[1] * d[2] + f[2] * d[1]);
+    v[5] += s * (f[2] * d[2]);
+}
+
+/* ------------------------------------------------------------------ */
+/* Ewald beta by bisection, PM_force.cpp:246-274.  `precision` selects which
+ * erfc the comparison uses: 0 = float erfcf, 1 = double erfc.  All the
+ * iteration variables are float as in the reference. */
+SNBO_API float snbo_get_beta(float cutoff, float tolerance, int precision)
+{
+    float beta, low, high, tempf;
+    int ilow, ihigh;
+    high = 1.0f;
+    ihigh = 1;
+    for (;;)
+    {
+        tempf = precision ? (float)(erfc((double)(high * cutoff)) / cutoff)
+                          : erfcf(high * cutoff) / cutoff;
+        if (tempf <= tolerance) break;
+        high *= 2;
+        ihigh++;
+    }
+    ihigh += 50;
+    low = 0.0f;
+    beta = 0.0f;
+    for (ilow = 1; ilow < ihigh; ilow++)
+    {
+        beta = (low + high) / 2;
+        tempf = precision ? (float)(erfc((double)(beta * cutoff)) / cutoff)
+                          : erfcf(beta * cutoff) / cutoff;
+        if (tempf >= tolerance)
+            low = beta;
+        else
+            high = beta;
+    }
+    return beta;
+}
+
+/* ------------------------------------------------------------------ */
+/* Excluded test with the reference's semantics for a single domain
+ * (neighbor_list.cpp:744-773): pair (i, j), i < j, is removed when j appears
+ * in the exclusion list of i. */
+static int is_excluded(int i, int j, const int* excl_start,
+                       const int* excl_numbers, const int* excl_list)
+{
+    if (!excl_numbers) return 0;
+    int n = excl_numbers[i];
+    if (n <= 0) return 0;
+    const int* l = excl_list + excl_start[i];
+    for (int k = 0; k < n; ++k)
+        if (l[k] == j) return 1;
+    return 0;
+}
+
+typedef struct
+{
+    int* j;
+    int n, cap;
+} jlist;
+
+static void jl_push(jlist* l, int j)
+{
+    if (l->n == l->cap)
+    {
+        l->cap = l->cap ? 2 * l->cap : 64;
+        l->j = (int*)realloc(l->j, sizeof(int) * (size_t)l->cap);
+    }
+    l->j[l->n++] = j;
+}
+
+static int cmp_int(const void* a, const void* b)
+{
+    int x = *(const int*)a, y = *(const int*)b;
+    return (x > y) - (x < y);
+}
+
+/* Half neighbor list: all pairs i < j with dr.dr < rl2 (FP32, no contraction),
+ * dr = crd[i] - crd[j] minimum-imaged, exclusions removed.  rl2 is formed as
+ * the reference forms it, (0.5f*(cutoff+skin))^2 * 4.0f (neighbor_list.cpp:847,
+ * 1005).  Writes row offsets (n+1) and the j's of every row sorted ascending;
+ * returns the number of pairs, or -(needed) if cap is too small. */
+SNBO_API int64_t snbo_nl_pairs(int n, const float* crd, const float* cell,
+                               const float* rcell, float cutoff, float skin,
+                               const int* excl_start, const int* excl_numbers,
+                               const int* excl_list, int64_t* row_start,
+                               int* cols, int64_t cap)
+{
+    float grid_length = 0.5f * (cutoff + skin);
+    float rl2 = grid_length * grid_length * 4.0f;
+    jlist* rows = (jlist*)calloc((size_t)n, sizeof(jlist));
+    int orth = cell[1] == 0.0f && cell[3] == 0.0f && cell[4] == 0.0f;
+    float rl = sqrtf(rl2);
+    int nc[3] = {0, 0, 0};
+    if (orth)
+    {
+        nc[0] = (int)floor(cell[0] / (rl * 1.0001f));
+        nc[1] = (int)floor(cell[2] / (rl * 1.0001f));
+        nc[2] = (int)floor(cell[5] / (rl * 1.0001f));
+    }
+    if (orth && nc[0] >= 3 && nc[1] >= 3 && nc[2] >= 3)
+    {
+        int ncell = nc[0] * nc[1] * nc[2];
+        int* head = (int*)malloc(sizeof(int) * (size_t)ncell);
+        int* next = (int*)malloc(sizeof(int) * (size_t)n);
+        int* cid = (int*)malloc(sizeof(int) * (size_t)n);
+        for (int c = 0; c < ncell; ++c) head[c] = -1;
+        double L[3] = {cell[0], cell[2], cell[5]};
+        for (int i = n - 1; i >= 0; --i)
+        {
+            int c3[3];
+            for (int d = 0; d < 3; ++d)
+            {
+                double x = crd[3 * i + d];
+                x -= floor(x / L[d]) * L[d];
+                int k = (int)(x / L[d] * nc[d]);
+                if (k < 0) k = 0;
+                if (k >= nc[d]) k = nc[d] - 1;
+                c3[d] = k;
+            }
+            int c = (c3[0] * nc[1] + c3[1]) * nc[2] + c3[2];
+            cid[i] = c;
+            next[i] = head[c];
+            head[c] = i;
+        }
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int i = 0; i < n; ++i)
+        {
+            int c = cid[i];
+            int cx = c / (nc[1] * nc[2]), cy = (c / nc[2]) % nc[1],
+                cz = c % nc[2];
+            for (int ox = -1; ox <= 1; ++ox)
+                for (int oy = -1; oy <= 1; ++oy)
+                    for (int oz = -1; oz <= 1; ++oz)
+                    {
+                        int x = (cx + ox + nc[0]) % nc[0];
+                        int y = (cy + oy + nc[1]) % nc[1];
+                        int z = (cz + oz + nc[2]) % nc[2];
+                        for (int j = head[(x * nc[1] + y) * nc[2] + z]; j >= 0;
+                             j = next[j])
+                        {
+                            if (j <= i) continue;
+                            float dr[3];
+                            min_image_f32(crd + 3 * i, crd + 3 * j, cell, rcell,
+                                          dr);
+                            float d2 = dr[0] * dr[0];
+                            d2 = d2 + dr[1] * dr[1];
+                            d2 = d2 + dr[2] * dr[2];
+                            if (d2 < rl2 &&
+                                !is_excluded(i, j, excl_start, excl_numbers,
+                                             excl_list))
+                                jl_push(&rows[i], j);
+                        }
+                    }
+        }
+        free(head);
+        free(next);
+        free(cid);
+    }
+    else
+    {
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int i = 0; i < n; ++i)
+            for (int j = i + 1; j < n; ++j)
+            {
+                float dr[3];
+                min_image_f32(crd + 3 * i, crd + 3 * j, cell, rcell, dr);
+                float d2 = dr[0] * dr[0];
+                d2 = d2 + dr[1] * dr[1];
+                d2 = d2 + dr[2] * dr[2];
+                if (d2 < rl2 &&
+                    !is_excluded(i, j, excl_start, excl_numbers, excl_list))
+                    jl_push(&rows[i], j);
+            }
+    }
+    int64_t total = 0;
+    for (int i = 0; i < n; ++i) total += rows[i].n;
+    if (total > cap || !row_start || !cols)
+    {
+        for (int i = 0; i < n; ++i) free(rows[i].j);
+        free(rows);
+        return total > cap ? -total : total;
+    }
+    int64_t off = 0;
+    for (int i = 0; i < n; ++i)
+    {
+        row_start[i] = off;
+        if (rows[i].n) qsort(rows[i].j, (size_t)rows[i].n, sizeof(int), cmp_int);
+        memcpy(cols + off, rows[i].j, sizeof(int) * (size_t)rows[i].n);
+        off += rows[i].n;
+        free(rows[i].j);
+    }
+    row_start[n] = off;
+    free(rows);
+    return total;
+}
+
+/* ------------------------------------------------------------------ */
+/* Direct-space LJ + erfc-Coulomb over a half list, FP64 run of
+ * Lennard_Jones_And_Direct_Coulomb_Device (Lennard_Jones_force.cpp:45-137):
+ * for pair (i, j) of row i, dr = crd[j] - crd[i] (min image), r < cutoff:
+ *   F/r  = (B' - A' r^-6) r^-8 - q_i q_j r^-3 (2 beta r/sqrt(pi) e^{-b^2r^2}
+ *          + erfc(beta r))
+ *   f_i += (F/r) dr, f_j -= (F/r) dr, virial_i -= (F/r) dr (x) dr,
+ *   E_LJ,i += (A'/12 r^-6 - B'/6) r^-6,  E_C,i += q_i q_j erfc(beta r)/r.
+ * Outputs are accumulated (+=) like the reference. */
+SNBO_API void snbo_direct_f64(int n, const float* crd, const float* charge,
+                              const int* lj_type, const float* lj_A,
+                              const float* lj_B, const float* cell,
+                              const float* rcell, float cutoff, float beta,
+                              const int64_t* row_start, const int* cols,
+                              double* frc, double* atom_energy,
+                              double* lj_energy, double* coul_energy,
+                              double* virial)
+{
+    const double two_over_sqrt_pi = 1.1283791670955126;
+    double* fj = (double*)calloc((size_t)3 * n, sizeof(double));
+    double b = beta;
+#pragma omp parallel
+    {
+        double* fj_local = (double*)calloc((size_t)3 * n, sizeof(double));
+#pragma omp for schedule(dynamic, 64)
+        for (int i = 0; i < n; ++i)
+        {
+            double fi[3] = {0, 0, 0}, vir[6] = {0, 0, 0, 0, 0, 0};
+            double elj = 0, ec = 0;
+            int ti = lj_type[i];
+            double qi = charge[i];
+            for (int64_t k = row_start[i]; k < row_start[i + 1]; ++k)
+            {
+                int j = cols[k];
+                double dr[3];
+                min_image_f64(crd + 3 * j, crd + 3 * i, cell, rcell, dr);
+                double r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+                double r = sqrt(r2);
+                if (!(r < cutoff)) continue;
+                int tj = lj_type[j];
+                int hi = ti > tj ? ti : tj, lo = ti > tj ? tj : ti;
+                int pidx = hi * (hi + 1) / 2 + lo;
+                double A = lj_A[pidx], B = lj_B[pidx];
+                double ir2 = 1.0 / r2, ir6 = ir2 * ir2 * ir2;
+                double flj = (B - A * ir6) * ir6 * ir2;
+                double qq = qi * (double)charge[j];
+                double br = b * r;
+                double fc = qq / (r2 * r) *
+                            (br * two_over_sqrt_pi * exp(-br * br) + erfc(br));
+                double fabs_ = flj - fc;
+                double fl[3] = {fabs_ * dr[0], fabs_ * dr[1], fabs_ * dr[2]};
+                fi[0] += fl[0];
+                fi[1] += fl[1];
+                fi[2] += fl[2];
+                fj_local[3 * j + 0] -= fl[0];
+                fj_local[3 * j + 1] -= fl[1];
+                fj_local[3 * j + 2] -= fl[2];
+                virial_add(vir, fl, dr, -1.0);
+                elj += (A / 12.0 * ir6 - B / 6.0) * ir6;
+                ec += qq * erfc(br) / r;
+            }
+            frc[3 * i + 0] += fi[0];
+            frc[3 * i + 1] += fi[1];
+            frc[3 * i + 2] += fi[2];
+            if (atom_energy) atom_energy[i] += elj + ec;
+            if (lj_energy) lj_energy[i] += elj;
+            if (coul_energy) coul_energy[i] += ec;
+            if (virial)
+                for (int c = 0; c < 6; ++c) virial[6 * i + c] += vir[c];
+        }
+#pragma omp critical
+        for (int k = 0; k < 3 * n; ++k) fj[k] += fj_local[k];
+        free(fj_local);
+    }
+    for (int k = 0; k < 3 * n; ++k) frc[k] += fj[k];
+    free(fj);
+}
+
+/* ------------------------------------------------------------------ */
+/* Excluded-pair correction, FP64 run of
+ * MPI_PME_Excluded_Force_With_Atom_Energy_Correction (PM_force.cpp:1745-1817)
+ * with factor 1 (single process). */
+SNBO_API void snbo_excluded_f64(int n, const float* crd, const float* charge,
+                                const float* cell, const float* rcell,
+                                float beta, const int* excl_start,
+                                const int* excl_numbers, const int* excl_list,
+                                double* frc, double* atom_energy,
+                                double* virial)
+{
+    const double two_over_sqrt_pi = 1.1283791670955126;
+    for (int i = 0; i < n; ++i)
+    {
+        int cnt = excl_numbers[i];
+        if (cnt <= 0) continue;
+        double qi = charge[i];
+        double fi[3] = {0, 0, 0}, vir[6] = {0, 0, 0, 0, 0, 0}, e = 0;
+        for (int k = excl_start[i]; k < excl_start[i] + cnt; ++k)
+        {
+            int j = excl_list[k];
+            double dr[3];
+            min_image_f64(crd + 3 * j, crd + 3 * i, cell, rcell, dr);
+            double r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+            double r = sqrt(r2);
+            double br = (double)beta * r;
+            double f = br * two_over_sqrt_pi * exp(-br * br) + erfc(br);
+            f = (f - 1.0) / r2 / r;
+            f = -qi * (double)charge[j] * f;
+            double fl[3] = {f * dr[0], f * dr[1], f * dr[2]};
+            frc[3 * j + 0] -= fl[0];
+            frc[3 * j + 1] -= fl[1];
+            frc[3 * j + 2] -= fl[2];
+            fi[0] += fl[0];
+            fi[1] += fl[1];
+            fi[2] += fl[2];
+            e -= qi * (double)charge[j] * erf(br) / r;
+            virial_add(vir, fl, dr, -1.0);
+        }
+        frc[3 * i + 0] += fi[0];
+        frc[3 * i + 1] += fi[1];
+        frc[3 * i + 2] += fi[2];
+        if (atom_energy) atom_energy[i] += e;
+        if (virial)
+            for (int c = 0; c < 6; ++c) virial[6 * i + c] += vir[c];
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* PME reciprocal part in FP64 (PM_force.cpp:541-612 tables, 699-893 spread and
+ * gather, 896-919 + 1142-1166 energies, 1024-1068 virial). */
+
+/* |b(k)|^2 for order-4 B-splines: 1 / |sum_{j=0}^{2} M4(j+1) e^{2 pi i k j/K}|^2
+ * (getb, PM_force.cpp:40-64). */
+static double bspline_mod2(int k, int K)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    const double m4[3] = {1.0 / 6.0, 4.0 / 6.0, 1.0 / 6.0};
+    double re = 0, im = 0;
+    for (int j = 0; j < 3; ++j)
+    {
+        double a = two_pi * k * j / K;
+        re += m4[j] * cos(a);
+        im += m4[j] * sin(a);
+    }
+    return 1.0 / (re * re + im * im);
+}
+
+/* order-4 cardinal B-spline weights of the four points u, u-1, u-2, u-3 and
+ * their derivatives (power form of PME_Ma..PME_dMc, PM_force.cpp:20-26) */
+static void bspline4(double x, double* w, double* dw)
+{
+    double x2 = x * x, x3 = x2 * x;
+    w[0] = x3 / 6.0;
+    w[1] = -0.5 * x3 + 0.5 * x2 + 0.5 * x + 1.0 / 6.0;
+    w[2] = 0.5 * x3 - x2 + 4.0 / 6.0;
+    w[3] = -x3 / 6.0 + 0.5 * x2 - 0.5 * x + 1.0 / 6.0;
+    dw[0] = 0.5 * x2;
+    dw[1] = -1.5 * x2 + x + 0.5;
+    dw[2] = 1.5 * x2 - 2.0 * x;
+    dw[3] = -0.5 * x2 + x - 0.5;
+}
+
+/* Fractional coordinate handling of PME_Atom_Near (PM_force.cpp:707-733):
+ * frac = crd*rcell - floor(.), scaled by K, base u = (int) clamped, fraction. */
+static void pme_base(const float* r, const float* rcell, const int* K,
+                     int* u, double* fr)
+{
+    double f[3];
+    f[0] = (double)r[0] * rcell[0] + (double)r[1] * rcell[1] +
+           (double)r[2] * rcell[3];
+    f[1] = (double)r[1] * rcell[2] + (double)r[2] * rcell[4];
+    f[2] = (double)r[2] * rcell[5];
+    for (int d = 0; d < 3; ++d)
+    {
+        f[d] -= floor(f[d]);
+        if (!isfinite(f[d])) f[d] = 0.0;
+        f[d] *= K[d];
+        int t = (int)f[d];
+        t = t < 0 ? 0 : (t < K[d] ? t : K[d] - 1);
+        u[d] = t;
+        double x = f[d] - t;
+        fr[d] = x - floor(x);
+    }
+}
+
+/* Outputs: frc += reciprocal force (times update_interval = 1), *e_recip,
+ * *e_self (self + neutralising), virial6 (reference sign convention),
+ * optional phi (the convolved grid, Nall doubles). */
+SNBO_API void snbo_pme_f64(int n, const float* crd, const float* charge,
+                           const float* cell, const float* rcell, int K0,
+                           int K1, int K2, float beta, double* frc,
+                           double* e_recip, double* e_self, double* virial6,
+                           double* phi_out)
+{
+    const double pi = 3.141592653589793238462643383;
+    int K[3] = {K0, K1, K2};
+    size_t nall = (size_t)K0 * K1 * K2;
+    int nc = K2 / 2 + 1;
+    size_t nfft = (size_t)K0 * K1 * nc;
+    double* Q = (double*)calloc(nall, sizeof(double));
+    int* U = (int*)malloc(sizeof(int) * 3 * (size_t)n);
+    double* FR = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    for (int a = 0; a < n; ++a)
+    {
+        pme_base(crd + 3 * a, rcell, K, U + 3 * a, FR + 3 * a);
+        double wx[4], wy[4], wz[4], d[4];
+        bspline4(FR[3 * a + 0], wx, d);
+        bspline4(FR[3 * a + 1], wy, d);
+        bspline4(FR[3 * a + 2], wz, d);
+        double q = charge[a];
+        for (int ix = 0; ix < 4; ++ix)
+        {
+            int gx = (U[3 * a] - ix + K0) % K0;
+            for (int iy = 0; iy < 4; ++iy)
+            {
+                int gy = (U[3 * a + 1] - iy + K1) % K1;
+                for (int iz = 0; iz < 4; ++iz)
+                {
+                    int gz = (U[3 * a + 2] - iz + K2) % K2;
+                    Q[((size_t)gx * K1 + gy) * K2 + gz] +=
+                        q * wx[ix] * wy[iy] * wz[iz];
+                }
+            }
+        }
+    }
+    fftm_cplx* FQ = (fftm_cplx*)malloc(sizeof(fftm_cplx) * nfft);
+    fftm_r2c_3d(Q, FQ, K0, K1, K2);
+    /* tables and virial over the half spectrum */
+    double vol = (double)cell[0] * cell[2] * cell[5];
+    double b = beta;
+    double mpre = pi * pi / (b * b);
+    double vir[6] = {0, 0, 0, 0, 0, 0};
+    double* B0 = (double*)malloc(sizeof(double) * K0);
+    double* B1 = (double*)malloc(sizeof(double) * K1);
+    double* B2 = (double*)malloc(sizeof(double) * K2);
+    for (int k = 0; k < K0; ++k) B0[k] = bspline_mod2(k, K0);
+    for (int k = 0; k < K1; ++k) B1[k] = bspline_mod2(k, K1);
+    for (int k = 0; k < K2; ++k) B2[k] = bspline_mod2(k, K2);
+    for (int kx = 0; kx < K0; ++kx)
+    {
+        double kxr = kx > K0 / 2 ? kx - K0 : kx;
+        for (int ky = 0; ky < K1; ++ky)
+        {
+            double kyr = ky > K1 / 2 ? ky - K1 : ky;
+            for (int kz = 0; kz < nc; ++kz)
+            {
+                double kzr = kz;
+                /* m = MultiplyTranspose(k, rcell) (vector.hpp:286-291) */
+                double m[3] = {kxr * rcell[0], kxr * rcell[1] + kyr * rcell[2],
+                               kxr * rcell[3] + kyr * rcell[4] +
+                                   kzr * rcell[5]};
+                double msq = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+                size_t idx = ((size_t)kx * K1 + ky) * nc + kz;
+                double bc = 0.0, vb[6] = {0, 0, 0, 0, 0, 0};
+                if (kx + ky + kz != 0)
+                {
+                    bc = 1.0 / pi / msq * exp(-mpre * msq) / vol;
+                    double c = 2.0 / msq * (1.0 + mpre * msq);
+                    vb[0] = 1.0 - c * m[0] * m[0];
+                    vb[1] = 0.0 - c * m[1] * m[0];
+                    vb[2] = 1.0 - c * m[1] * m[1];
+                    vb[3] = 0.0 - c * m[2] * m[0];
+                    vb[4] = 0.0 - c * m[2] * m[1];
+                    vb[5] = 1.0 - c * m[2] * m[2];
+                }
+                bc *= B0[kx] * B1[ky] * B2[kz];
+                double f2 = FQ[idx].re * FQ[idx].re + FQ[idx].im * FQ[idx].im;
+                double factor = (kz == 0 || kz == nc - 1) ? 0.5 : 1.0;
+                for (int c = 0; c < 6; ++c)
+                    vir[c] -= factor * f2 * (0.5 * bc * vb[c]);
+                FQ[idx].re *= bc;
+                FQ[idx].im *= bc;
+            }
+        }
+    }
+    double* phi = (double*)malloc(sizeof(double) * nall);
+    fftm_c2r_3d(FQ, phi, K0, K1, K2);
+    double er = 0.0;
+    for (size_t g = 0; g < nall; ++g) er += Q[g] * phi[g];
+    *e_recip = 0.5 * er;
+    double q2 = 0, qs = 0;
+    for (int a = 0; a < n; ++a)
+    {
+        q2 += (double)charge[a] * charge[a];
+        qs += charge[a];
+    }
+    *e_self = -b / sqrt(pi) * q2 - 0.5 * pi / (b * b * vol) * qs * qs;
+    for (int c = 0; c < 6; ++c) virial6[c] += vir[c];
+    /* gather (PME_Final, PM_force.cpp:829-893) */
+#pragma omp parallel for
+    for (int a = 0; a < n; ++a)
+    {
+        double wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+        bspline4(FR[3 * a + 0], wx, dx);
+        bspline4(FR[3 * a + 1], wy, dy);
+        bspline4(FR[3 * a + 2], wz, dz);
+        double q = charge[a];
+        double acc[3] = {0, 0, 0};
+        for (int ix = 0; ix < 4; ++ix)
+        {
+            int gx = (U[3 * a] - ix + K0) % K0;
+            for (int iy = 0; iy < 4; ++iy)
+            {
+                int gy = (U[3 * a + 1] - iy + K1) % K1;
+                for (int iz = 0; iz < 4; ++iz)
+                {
+                    int gz = (U[3 * a + 2] - iz + K2) % K2;
+                    double p = -phi[((size_t)gx * K1 + gy) * K2 + gz] * q;
+                    double g0 = dx[ix] * wy[iy] * wz[iz] * K0;
+                    double g1 = dy[iy] * wx[ix] * wz[iz] * K1;
+                    double g2 = dz[iz] * wx[ix] * wy[iy] * K2;
+                    acc[0] += p * (g0 * rcell[0]);
+                    acc[1] += p * (g0 * rcell[1] + g1 * rcell[2]);
+                    acc[2] += p * (g0 * rcell[3] + g1 * rcell[4] + g2 * rcell[5]);
+                }
+            }
+        }
+        frc[3 * a + 0] += acc[0];
+        frc[3 * a + 1] += acc[1];
+        frc[3 * a + 2] += acc[2];
+    }
+    if (phi_out) memcpy(phi_out, phi, sizeof(double) * nall);
+    free(Q);
+    free(U);
+    free(FR);
+    free(FQ);
+    free(phi);
+    free(B0);
+    free(B1);
+    free(B2);
+}
+
+/* Plain Ewald reciprocal sum (no mesh) in FP64 for small systems: the exact
+ * quantity PME approximates, used to check the oracle's own PME. */
+SNBO_API double snbo_ewald_recip_f64(int n, const float* crd,
+                                     const float* charge, float box, float beta,
+                                     int kmax, double* frc)
+{
+    const double pi = 3.141592653589793238462643383;
+    double L = box, vol = L * L * L, e = 0.0;
+    for (int kx = -kmax; kx <= kmax; ++kx)
+        for (int ky = -kmax; ky <= kmax; ++ky)
+            for (int kz = -kmax; kz <= kmax; ++kz)
+            {
+                if (!kx && !ky && !kz) continue;
+                double m[3] = {kx / L, ky / L, kz / L};
+                double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+                double pre = exp(-pi * pi * m2 / ((double)beta * beta)) / m2;
+                double sr = 0, si = 0;
+                for (int a = 0; a < n; ++a)
+                {
+                    double ph = 2 * pi *
+                                (m[0] * crd[3 * a] + m[1] * crd[3 * a + 1] +
+                                 m[2] * crd[3 * a + 2]);
+                    sr += charge[a] * cos(ph);
+                    si += charge[a] * sin(ph);
+                }
+                e += pre * (sr * sr + si * si);
+                if (frc)
+                    for (int a = 0; a < n; ++a)
+                    {
+                        double ph = 2 * pi *
+                                    (m[0] * crd[3 * a] + m[1] * crd[3 * a + 1] +
+                                     m[2] * crd[3 * a + 2]);
+                        double s = sin(ph) * sr - cos(ph) * si;
+                        double f = 2.0 / vol * pre * charge[a] * s;
+                        frc[3 * a + 0] += f * m[0];
+                        frc[3 * a + 1] += f * m[1];
+                        frc[3 * a + 2] += f * m[2];
+                    }
+            }
+    return e / (2 * pi * vol);
+}
+
+/* ------------------------------------------------------------------ */
+/* Long-range LJ correction factor as the reference forms it
+ * (Lennard_Jones_force.cpp:212-235): type histogram, double C6 sum, then
+ * float scaling by -2/3 pi / rc^3 / 6.  E_lrc = factor/V, W_lrc = 2 factor/V
+ * on the diagonal (:279-306). */
+SNBO_API float snbo_lrc_factor(int n, const int* lj_type, int n_types,
+                               const float* lj_B, float cutoff)
+{
+    int64_t* cnt = (int64_t*)calloc((size_t)n_types, sizeof(int64_t));
+    for (int i = 0; i < n; ++i) cnt[lj_type[i]] += 1;
+    double c6 = 0.0;
+    for (int a = 0; a < n_types; ++a)
+    {
+        if (!cnt[a]) continue;
+        double inner = 0.0;
+        for (int b = 0; b < n_types; ++b)
+        {
+            if (!cnt[b]) continue;
+            int hi = a > b ? a : b, lo = a > b ? b : a;
+            inner += (double)cnt[b] * (double)lj_B[hi * (hi + 1) / 2 + lo];
+        }
+        c6 += (double)cnt[a] * inner;
+    }
+    free(cnt);
+    float f = (float)c6;
+    f *= -2.0f / 3.0f * 3.1415926535897932f / cutoff / cutoff / cutoff / 6.0f;
+    return f;
+}

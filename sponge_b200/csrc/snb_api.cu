@@ -1,0 +1,1224 @@
+// C ABI (include/sponge_nb.h): module handles that mirror SPONGE's
+// NEIGHBOR_LIST, LENNARD_JONES_INFORMATION, Particle_Mesh and the fused
+// engine.  Host-side logic only; kernels live in the other .cu files.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/sponge_nb.h"
+#include "snb_internal.h"
+
+namespace snb {
+std::string last_error();
+int launch_bonded(int nb, const int* ba, const int* bb, const float* bk,
+                  const float* br0, int na, const int* aa, const int* ab,
+                  const int* ac, const float* ak, const float* at0,
+                  const float3* crd, const Cell& cell, const Cell& rcell,
+                  const int* map, Accumulators& acc, long long* e_total,
+                  bool energy, cudaStream_t st);
+int launch_leap_frog(int n, const int* map, Accumulators& acc, float3* crd,
+                     float3* vel, const float* inv_mass, float dt, cudaStream_t st);
+int launch_totals(int n, Accumulators& acc, long long* isum, const long long* bonded,
+                  const double* pme_sums, double lrc_energy, double lrc_virial,
+                  double* totals, bool energy, bool virial, bool have_pme,
+                  cudaStream_t st);
+int launch_add_scalars(float* d_potential, float* d_virial, const double* sums,
+                       float lrc_e, float lrc_v, int mode, cudaStream_t st);
+int launch_sum_float(int n, const float* x, double* out, cudaStream_t st);
+int launch_gather_type(int n, const int* src, const int* atom_local, int* dst,
+                       cudaStream_t st);
+}  // namespace snb
+
+using namespace snb;
+
+static inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+static Cell cell_of(const snb_boundary& b) { return make_cell(b.cell); }
+static Cell rcell_of(const snb_boundary& b) { return make_cell(b.rcell); }
+
+// Tail-correction factor as LENNARD_JONES_INFORMATION::Initial forms it
+// (Lennard_Jones_force.cpp:212-237): type histogram, double C6 sum, float
+// scaling by -2/3 pi / rc^3 / 6.
+static float lrc_factor(const std::vector<int>& type, int n_types,
+                        const std::vector<float>& B, float cutoff) {
+  std::vector<long long> cnt(n_types, 0);
+  for (int t : type) cnt[t] += 1;
+  double c6 = 0.0;
+  for (int a = 0; a < n_types; ++a) {
+    if (!cnt[a]) continue;
+    double inner = 0.0;
+    for (int b = 0; b < n_types; ++b) {
+      if (!cnt[b]) continue;
+      inner += (double)cnt[b] * (double)B[lj_pair_index(a, b)];
+    }
+    c6 += (double)cnt[a] * inner;
+  }
+  float f = (float)c6;
+  f *= -2.0f / 3.0f * 3.1415926535897932f / cutoff / cutoff / cutoff / 6.0f;
+  return f;
+}
+
+// ============================================================== handles
+struct snb_nl {
+  NeighborList nl;
+  snb_options opt;
+};
+
+struct snb_lj {
+  LJParams p;
+  Accumulators acc;
+  int n = 0;
+  int accum = kAccumFixed;
+  float4* d_pos = nullptr;
+  int* d_type_sorted = nullptr;
+  float* d_lj_energy = nullptr;  // d_LJ_energy_atom
+  double* d_sum = nullptr;
+  float h_long_energy = 0.f;
+};
+
+struct snb_pme {
+  PME p;
+  Accumulators acc;
+  int accum = kAccumFixed;
+  float4* d_pos = nullptr;
+};
+
+struct snb_engine {
+  snb_options opt;
+  int n = 0;
+  int accum = kAccumFixed;
+  Cell cell{}, rcell{};
+  NeighborList nl;
+  LJParams lj;
+  PME pme;
+  Accumulators acc;
+  float4* d_pos = nullptr;
+  int* d_type_sorted = nullptr;
+  float* d_charge = nullptr;
+  int* d_excl_start = nullptr;
+  int* d_excl_numbers = nullptr;
+  int* d_excl_list = nullptr;
+  long long* d_isum = nullptr;    // [9]
+  long long* d_bonded_e = nullptr;  // [1]
+  double* d_totals_scratch = nullptr;
+  // bonded terms
+  int nb = 0, na = 0;
+  int *d_ba = nullptr, *d_bb = nullptr, *d_aa = nullptr, *d_ab = nullptr, *d_ac = nullptr;
+  float *d_bk = nullptr, *d_br0 = nullptr, *d_ak = nullptr, *d_at0 = nullptr;
+  // graph of one MD step
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  float* g_crd = nullptr;
+  float* g_vel = nullptr;
+  const float* g_invm = nullptr;
+  float g_dt = 0.f;
+  cudaStream_t g_stream = nullptr;
+  // recovery snapshot for neighbor-list overflow
+  float* d_snap_crd = nullptr;
+  float* d_snap_vel = nullptr;
+  long long steps_done = 0;
+  // per-phase CUDA events (profiling pass only)
+  bool prof_on = false;
+  cudaEvent_t prof_ev[8] = {};
+  double prof_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+};
+
+static void prof_mark(snb_engine* e, int k, cudaStream_t st) {
+  if (e->prof_on) cudaEventRecord(e->prof_ev[k], st);
+}
+
+// ============================================================ options
+extern "C" int snb_version(void) { return SNB_VERSION; }
+
+extern "C" const char* snb_last_error(void) {
+  static thread_local std::string s;
+  s = last_error();
+  return s.c_str();
+}
+
+extern "C" void snb_options_default(snb_options* o) {
+  memset(o, 0, sizeof(*o));
+  o->cutoff = 10.0f;
+  o->skin = 2.0f;
+  o->nl_refresh_interval = 0;
+  o->nl_skin_permit = 0.5f;
+  o->nl_max_neighbor_numbers = 1200;
+  o->nl_max_atom_in_grid_numbers = 150;
+  o->nl_max_ghost_in_grid_numbers = 150;
+  o->nl_check_overflow_interval = 150;
+  o->nl_throw_error_when_overflow = 0;
+  o->pm_fftx = o->pm_ffty = o->pm_fftz = -1;
+  o->pm_grid_spacing = 1.0f;
+  o->pm_direct_tolerance = 0.00001f;
+  o->pme_update_interval = 1;
+  o->pme_calculate_reciprocal_part = 1;
+  o->pme_calculate_excluded_part = 1;
+  o->lambda_lj = 0.0f;
+  o->soft_core_alpha = 0.5f;
+  o->soft_core_powfer = 1.0f;
+  o->soft_core_sigma = 3.0f;
+  o->soft_core_sigma_min = 0.0f;
+  o->accumulation = SNB_ACCUM_FIXED64;
+  o->dom_dec_update_interval = 100;
+}
+
+static bool parse_bool(const char* v) {
+  std::string s(v);
+  for (auto& c : s) c = (char)tolower(c);
+  return s == "1" || s == "true" || s == "yes" || s == "on";
+}
+
+extern "C" int snb_options_set(snb_options* o, const char* key, const char* value) {
+  if (!o || !key || !value) return fail(kBadInput, "options_set: null argument");
+  std::string k(key);
+  auto F = [&]() { return (float)atof(value); };
+  auto I = [&]() { return atoi(value); };
+  if (k == "cutoff") o->cutoff = F();
+  else if (k == "skin") o->skin = F();
+  else if (k == "neighbor_list_refresh_interval") o->nl_refresh_interval = I();
+  else if (k == "neighbor_list_skin_permit") o->nl_skin_permit = F();
+  else if (k == "neighbor_list_max_neighbor_numbers") o->nl_max_neighbor_numbers = I();
+  else if (k == "neighbor_list_max_atom_in_grid_numbers") o->nl_max_atom_in_grid_numbers = I();
+  else if (k == "neighbor_list_max_ghost_in_grid_numbers") o->nl_max_ghost_in_grid_numbers = I();
+  else if (k == "neighbor_list_check_overflow_interval") o->nl_check_overflow_interval = I();
+  else if (k == "neighbor_list_throw_error_when_overflow") o->nl_throw_error_when_overflow = parse_bool(value);
+  else if (k == "PM_fftx") o->pm_fftx = I();
+  else if (k == "PM_ffty") o->pm_ffty = I();
+  else if (k == "PM_fftz") o->pm_fftz = I();
+  else if (k == "PM_grid_spacing") o->pm_grid_spacing = F();
+  else if (k == "PM_Direct_Tolerance") o->pm_direct_tolerance = F();
+  else if (k == "PME_update_interval") o->pme_update_interval = I();
+  else if (k == "PME_calculate_reciprocal_part") o->pme_calculate_reciprocal_part = parse_bool(value);
+  else if (k == "PME_calculate_excluded_part") o->pme_calculate_excluded_part = parse_bool(value);
+  else if (k == "lambda_lj") o->lambda_lj = F();
+  else if (k == "soft_core_alpha") o->soft_core_alpha = F();
+  else if (k == "soft_core_powfer") o->soft_core_powfer = F();
+  else if (k == "soft_core_sigma") o->soft_core_sigma = F();
+  else if (k == "soft_core_sigma_min") o->soft_core_sigma_min = F();
+  else if (k == "DOM_DEC_update_interval") o->dom_dec_update_interval = I();
+  else if (k == "accumulation") {
+    std::string v(value);
+    if (v == "fixed64" || v == "fixed") o->accumulation = SNB_ACCUM_FIXED64;
+    else if (v == "float") o->accumulation = SNB_ACCUM_FLOAT;
+    else return fail(kBadInput, "accumulation must be fixed64 or float");
+  } else {
+    return fail(kBadInput, "unknown key " + k);
+  }
+  return kOk;
+}
+
+static snb_options opts_or_default(const snb_options* o) {
+  snb_options d;
+  if (o) return *o;
+  snb_options_default(&d);
+  return d;
+}
+
+// ========================================================= NEIGHBOR_LIST
+extern "C" int snb_nl_create(const snb_options* opt, int atom_numbers, float cutoff,
+                             float skin, snb_boundary boundary, snb_nl** out) {
+  if (!out) return fail(kBadInput, "nl_create: null out");
+  *out = nullptr;
+  if (boundary.policy != 1)
+    return fail(kNotSupported, "neighbor list: periodic boundary required");
+  snb_nl* h = new snb_nl();
+  h->opt = opts_or_default(opt);
+  int rc = nl_init(h->nl, atom_numbers, cutoff, skin, boundary.cell,
+                   h->opt.nl_refresh_interval, h->opt.nl_skin_permit,
+                   h->opt.nl_max_neighbor_numbers, 0);
+  if (rc) {
+    nl_free(h->nl);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return kOk;
+}
+
+extern "C" int snb_nl_update(snb_nl* h, const int* atom_local, int local_atom_numbers,
+                             int ghost_numbers, const float* crd, snb_boundary boundary,
+                             int step, int update, const int* excluded_list_start,
+                             const int* excluded_list, const int* excluded_numbers,
+                             void* stream) {
+  if (!h) return fail(kBadInput, "nl_update: null handle");
+  if (local_atom_numbers <= 0 && ghost_numbers <= 0) return kOk;
+  if (ghost_numbers != 0)
+    return fail(kNotSupported, "nl_update: ghost atoms (domain decomposition) are "
+                               "not supported");
+  if (local_atom_numbers != h->nl.n)
+    return fail(kBadInput, "nl_update: local_atom_numbers differs from Initial");
+  return nl_update(h->nl, crd, atom_local, boundary.cell, step,
+                   update == SNB_FORCED_UPDATE, excluded_list_start, excluded_list,
+                   excluded_numbers, S(stream));
+}
+
+extern "C" int snb_nl_check_overflow(snb_nl* h, int* regrown, void* stream) {
+  if (!h) return fail(kBadInput, "nl_check_overflow: null handle");
+  bool r = false;
+  int rc = nl_check_overflow(h->nl, &r, S(stream));
+  if (regrown) *regrown = r ? 1 : 0;
+  if (!rc && r && h->opt.nl_throw_error_when_overflow)
+    return fail(kOverflow, "NEIGHBOR_LIST::Check_Overflow: overflow occured in "
+                           "neighbor searching");
+  return rc;
+}
+
+extern "C" int snb_nl_pair_count(snb_nl* h, long long* count, void* stream) {
+  if (!h || !count) return fail(kBadInput, "nl_pair_count: null argument");
+  return nl_total_pairs(h->nl, count, S(stream));
+}
+
+extern "C" int snb_nl_export_pairs(snb_nl* h, int* d_pi, int* d_pj, long long cap,
+                                   long long* count, void* stream) {
+  if (!h || !count) return fail(kBadInput, "nl_export_pairs: null argument");
+  int rc = nl_export_pairs(h->nl, d_pi, d_pj, cap, count, S(stream));
+  if (rc) return rc;
+  SNB_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+  return kOk;
+}
+
+extern "C" int snb_nl_export_atom_groups(snb_nl* h, void* d_nl, int* d_slab, int maxn,
+                                         void* stream) {
+  if (!h || !d_nl || !d_slab || maxn <= 0)
+    return fail(kBadInput, "nl_export_atom_groups: bad argument");
+  return nl_export_atom_groups(h->nl, d_nl, d_slab, maxn, S(stream));
+}
+
+extern "C" int snb_nl_destroy(snb_nl* h) {
+  if (!h) return kOk;
+  nl_free(h->nl);
+  delete h;
+  return kOk;
+}
+
+// ============================================= LENNARD_JONES_INFORMATION
+extern "C" int snb_lj_create(const snb_options* opt, int atom_numbers,
+                             int atom_type_numbers, const int* h_type, const float* h_A,
+                             const float* h_B, float cutoff, snb_lj** out) {
+  if (!out) return fail(kBadInput, "lj_create: null out");
+  *out = nullptr;
+  if (atom_numbers <= 0 || atom_type_numbers <= 0 || !h_type || !h_A || !h_B)
+    return fail(kBadInput, "lj_create: bad argument");
+  snb_options o = opts_or_default(opt);
+  snb_lj* h = new snb_lj();
+  h->n = atom_numbers;
+  h->accum = o.accumulation;
+  LJParams& p = h->p;
+  p.n_types = atom_type_numbers;
+  p.n_pairs = atom_type_numbers * (atom_type_numbers + 1) / 2;
+  p.h_type.assign(h_type, h_type + atom_numbers);
+  for (int t : p.h_type)
+    if (t < 0 || t >= atom_type_numbers) {
+      delete h;
+      return fail(kBadInput, "lj_create: LJ type out of range");
+    }
+  p.h_A.assign(h_A, h_A + p.n_pairs);
+  p.h_B.assign(h_B, h_B + p.n_pairs);
+  p.cutoff = cutoff;
+  p.long_range_factor = lrc_factor(p.h_type, p.n_types, p.h_B, cutoff);
+  SNB_CUDA_TRY(cudaMalloc(&p.d_A, sizeof(float) * p.n_pairs));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_B, sizeof(float) * p.n_pairs));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_A, h_A, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_B, h_B, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_type, sizeof(int) * atom_numbers));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_type, h_type, sizeof(int) * atom_numbers,
+                          cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_type_local, sizeof(int) * atom_numbers));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_type_local, h_type, sizeof(int) * atom_numbers,
+                          cudaMemcpyHostToDevice));
+  int rc = acc_init(h->acc, atom_numbers);
+  if (rc) return rc;
+  SNB_CUDA_TRY(cudaMalloc(&h->d_pos, sizeof(float4) * atom_numbers));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_type_sorted, sizeof(int) * atom_numbers));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_lj_energy, sizeof(float) * atom_numbers));
+  SNB_CUDA_TRY(cudaMemset(h->d_lj_energy, 0, sizeof(float) * atom_numbers));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_sum, sizeof(double)));
+  *out = h;
+  return kOk;
+}
+
+extern "C" int snb_lj_get_local(snb_lj* h, const int* atom_local, int local_n,
+                                int ghost_n, void* stream) {
+  if (!h) return fail(kBadInput, "lj_get_local: null handle");
+  if (ghost_n != 0) return fail(kNotSupported, "lj_get_local: ghost atoms");
+  if (local_n != h->n) return fail(kBadInput, "lj_get_local: atom count");
+  return launch_gather_type(local_n, h->p.d_type, atom_local, h->p.d_type_local,
+                            S(stream));
+}
+
+extern "C" int snb_lj_pme_direct_force(snb_lj* h, int atom_numbers, int local_n,
+                                       int solvent_n, int ghost_n, const float* crd,
+                                       const float* charge, float* frc,
+                                       snb_boundary boundary, snb_nl* nl,
+                                       float pme_beta, int need_atom_energy,
+                                       float* atom_energy, int need_virial,
+                                       float* atom_virial,
+                                       float* atom_direct_pme_energy, void* stream) {
+  if (!h || !nl) return fail(kBadInput, "lj_pme_direct_force: null handle");
+  cudaStream_t st = S(stream);
+  if (need_atom_energy) {
+    if (atom_direct_pme_energy)
+      SNB_CUDA_TRY(cudaMemsetAsync(atom_direct_pme_energy, 0, sizeof(float) * h->n, st));
+    SNB_CUDA_TRY(cudaMemsetAsync(h->d_lj_energy, 0, sizeof(float) * h->n, st));
+  }
+  if (atom_numbers == 0 || local_n == 0) return kOk;
+  if (ghost_n != 0 || solvent_n != 0)
+    return fail(kNotSupported, "lj_pme_direct_force: ghost/solvent atoms");
+  if (local_n != h->n || nl->nl.n != h->n)
+    return fail(kBadInput, "lj_pme_direct_force: atom count mismatch");
+  int rc = launch_pack(h->n, reinterpret_cast<const float3*>(crd), charge,
+                       h->p.d_type_local, nl->nl.d_perm, h->d_pos, h->d_type_sorted, st);
+  if (rc) return rc;
+  PairArgs a;
+  a.n = h->n;
+  a.pos = h->d_pos;
+  a.type = h->d_type_sorted;
+  a.global = nl->nl.d_global;
+  a.row_start = nl->nl.d_row_start;
+  a.cols = nl->nl.d_cols;
+  a.nl_flags = nl->nl.d_flags;
+  a.A = h->p.d_A;
+  a.B = h->p.d_B;
+  a.n_types = h->p.n_types;
+  a.cell = cell_of(boundary);
+  a.rcell = rcell_of(boundary);
+  a.cutoff2 = h->p.cutoff * h->p.cutoff;
+  a.beta = pme_beta;
+  bool ortho = a.cell.a21 == 0.f && a.cell.a31 == 0.f && a.cell.a32 == 0.f;
+  bool en = need_atom_energy != 0, vi = need_virial != 0;
+  rc = launch_pair(a, h->acc, h->accum, en, vi, ortho, st);
+  if (rc) return rc;
+  return launch_unpack(h->n, nl->nl.d_inv_perm, h->acc, h->accum,
+                       reinterpret_cast<float3*>(frc), en ? atom_energy : nullptr,
+                       en ? h->d_lj_energy : nullptr,
+                       en ? atom_direct_pme_energy : nullptr,
+                       vi ? atom_virial : nullptr, en, vi, st);
+}
+
+extern "C" int snb_lj_long_range_correction(snb_lj* h, int need_pressure,
+                                            float* d_virial, int need_potential,
+                                            float* d_potential, float volume,
+                                            void* stream) {
+  if (!h) return fail(kBadInput, "lj_long_range_correction: null handle");
+  float e = h->p.long_range_factor / volume;
+  float v = 2 * h->p.long_range_factor / volume;
+  if (need_potential) h->h_long_energy = e;
+  return launch_add_scalars(need_potential ? d_potential : nullptr,
+                            need_pressure ? d_virial : nullptr, nullptr, e, v, 1,
+                            S(stream));
+}
+
+extern "C" int snb_lj_energy_sum(snb_lj* h, float* out, void* stream) {
+  if (!h || !out) return fail(kBadInput, "lj_energy_sum: null argument");
+  int rc = launch_sum_float(h->n, h->d_lj_energy, h->d_sum, S(stream));
+  if (rc) return rc;
+  double v = 0;
+  SNB_CUDA_TRY(cudaMemcpyAsync(&v, h->d_sum, sizeof(double), cudaMemcpyDeviceToHost,
+                               S(stream)));
+  SNB_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+  *out = (float)v;
+  return kOk;
+}
+
+extern "C" float snb_lj_long_range_factor(snb_lj* h) {
+  return h ? h->p.long_range_factor : 0.f;
+}
+
+extern "C" int snb_lj_destroy(snb_lj* h) {
+  if (!h) return kOk;
+  cudaFree(h->p.d_A);
+  cudaFree(h->p.d_B);
+  cudaFree(h->p.d_type);
+  cudaFree(h->p.d_type_local);
+  acc_free(h->acc);
+  cudaFree(h->d_pos);
+  cudaFree(h->d_type_sorted);
+  cudaFree(h->d_lj_energy);
+  cudaFree(h->d_sum);
+  delete h;
+  return kOk;
+}
+
+// ========================================================== LJ_SOFT_CORE
+struct snb_lj_soft {
+  int n = 0;
+  int accum = kAccumFixed;
+  int nA = 0, nB = 0;
+  float *d_AA = nullptr, *d_AB = nullptr, *d_BA = nullptr, *d_BB = nullptr;
+  int2* d_par = nullptr;         // caller frame {typeA | typeB << 16, mask}
+  int2* d_par_local = nullptr;   // after Get_Local
+  int2* d_par_sorted = nullptr;
+  float4* d_pos = nullptr;
+  float* d_dq_sorted = nullptr;
+  float* d_lj_energy = nullptr;  // d_LJ_energy_atom
+  float* d_inter = nullptr;      // d_LJ_energy_atom_intersys
+  float* d_intra = nullptr;      // d_LJ_energy_atom_intrasys
+  long long* d_dudl = nullptr;   // [2] fixed point: LJ, direct Coulomb
+  Accumulators acc;
+  float lambda = 0.f, alpha = 0.5f, p = 1.f, sigma6 = 729.f, sigma6_min = 0.f;
+  float cutoff = 10.f;
+  float lrc = 0.f, lrc_ti = 0.f;
+};
+
+__global__ void k_pack_soft(int n, const int* __restrict__ perm,
+                            const int2* __restrict__ par, const float* __restrict__ dq,
+                            int2* __restrict__ par_sorted, float* __restrict__ dq_sorted) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int i = perm[s];
+  par_sorted[s] = par[i];
+  if (dq_sorted) dq_sorted[s] = dq ? dq[i] : 0.f;
+}
+
+__global__ void k_gather_par(int n, const int2* __restrict__ src,
+                             const int* __restrict__ atom_local, int2* __restrict__ dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[atom_local ? atom_local[i] : i];
+}
+
+// inter/intra LJ energies (sorted accumulators) -> caller-frame arrays
+__global__ void k_unpack_aux(int n, const int* __restrict__ map, Accumulators a,
+                             float* inter, float* intra, int accum) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int s = map[i];
+  const int N = a.n;
+  if (accum == kAccumFixed) {
+    inter[i] += (float)((double)a.d_eaux[s] * kEnergyScaleInv);
+    intra[i] += (float)((double)a.d_eaux[N + s] * kEnergyScaleInv);
+    a.d_eaux[s] = 0;
+    a.d_eaux[N + s] = 0;
+  } else {
+    inter[i] += a.d_feaux[s];
+    intra[i] += a.d_feaux[N + s];
+    a.d_feaux[s] = 0.f;
+    a.d_feaux[N + s] = 0.f;
+  }
+}
+
+// Tail correction of LJ_SOFT_CORE::Initial (LJ_soft_core.cpp:640-672): the
+// O(N^2) Total_C6_Get / Total_C6_B_A_Get sums depend only on the type
+// histograms of each end state, so they are formed from those.
+static void soft_lrc(const std::vector<int>& tA, const std::vector<int>& tB, int nA,
+                     int nB, const float* AB, const float* BB, float lambda,
+                     float cutoff, float* lrc, float* lrc_ti) {
+  std::vector<double> cA(nA, 0.0), cB(nB, 0.0);
+  for (int t : tA) cA[t] += 1;
+  for (int t : tB) cB[t] += 1;
+  double sA = 0.0, sB = 0.0;
+  for (int a = 0; a < nA; ++a)
+    for (int b = 0; b < nA; ++b) sA += cA[a] * cA[b] * (double)AB[lj_pair_index(a, b)];
+  for (int a = 0; a < nB; ++a)
+    for (int b = 0; b < nB; ++b) sB += cB[a] * cB[b] * (double)BB[lj_pair_index(a, b)];
+  float f = (float)((double)(1.0f - lambda) * sA + (double)lambda * sB);
+  float fti = (float)(sB - sA);
+  const float k = -2.0f / 3.0f * 3.1415926535897932f / cutoff / cutoff / cutoff / 6.0f;
+  *lrc = f * k;
+  *lrc_ti = fti * k;
+}
+
+extern "C" int snb_lj_soft_create(const snb_options* opt, int n, int nA, int nB,
+                                  const int* h_tA, const int* h_tB, const float* h_AA,
+                                  const float* h_AB, const float* h_BA,
+                                  const float* h_BB, const int* h_mask, float cutoff,
+                                  snb_lj_soft** out) {
+  if (!out) return fail(kBadInput, "lj_soft_create: null out");
+  *out = nullptr;
+  if (n <= 0 || nA <= 0 || nB <= 0 || !h_tA || !h_tB || !h_AA || !h_AB || !h_BA || !h_BB)
+    return fail(kBadInput, "lj_soft_create: bad argument");
+  if (nA > 0xffff || nB > 0x7fff) return fail(kBadInput, "lj_soft_create: too many types");
+  snb_options o = opts_or_default(opt);
+  snb_lj_soft* h = new snb_lj_soft();
+  h->n = n;
+  h->accum = o.accumulation;
+  h->nA = nA;
+  h->nB = nB;
+  h->lambda = o.lambda_lj;
+  h->alpha = o.soft_core_alpha;
+  h->p = o.soft_core_powfer;
+  h->sigma6 = powf(o.soft_core_sigma, 6);
+  h->sigma6_min = powf(o.soft_core_sigma_min, 6);
+  h->cutoff = cutoff;
+  int pA = nA * (nA + 1) / 2, pB = nB * (nB + 1) / 2;
+  std::vector<int> tA(h_tA, h_tA + n), tB(h_tB, h_tB + n);
+  std::vector<int2> par(n);
+  for (int i = 0; i < n; ++i) {
+    if (tA[i] < 0 || tA[i] >= nA || tB[i] < 0 || tB[i] >= nB) {
+      delete h;
+      return fail(kBadInput, "lj_soft_create: LJ type out of range");
+    }
+    par[i] = make_int2(tA[i] | (tB[i] << 16), h_mask ? h_mask[i] : 0);
+  }
+  soft_lrc(tA, tB, nA, nB, h_AB, h_BB, h->lambda, cutoff, &h->lrc, &h->lrc_ti);
+  auto up = [](float** d, const float* src, int m) -> int {
+    SNB_CUDA_TRY(cudaMalloc(d, sizeof(float) * m));
+    SNB_CUDA_TRY(cudaMemcpy(*d, src, sizeof(float) * m, cudaMemcpyHostToDevice));
+    return kOk;
+  };
+  if (up(&h->d_AA, h_AA, pA) || up(&h->d_AB, h_AB, pA) || up(&h->d_BA, h_BA, pB) ||
+      up(&h->d_BB, h_BB, pB))
+    return fail(kCudaError, "lj_soft_create: upload failed");
+  SNB_CUDA_TRY(cudaMalloc(&h->d_par, sizeof(int2) * n));
+  SNB_CUDA_TRY(cudaMemcpy(h->d_par, par.data(), sizeof(int2) * n, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_par_local, sizeof(int2) * n));
+  SNB_CUDA_TRY(cudaMemcpy(h->d_par_local, par.data(), sizeof(int2) * n,
+                          cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_par_sorted, sizeof(int2) * n));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_pos, sizeof(float4) * n));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_dq_sorted, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_lj_energy, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_inter, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_intra, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMemset(h->d_lj_energy, 0, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMemset(h->d_inter, 0, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMemset(h->d_intra, 0, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMalloc(&h->d_dudl, sizeof(long long) * 2));
+  int rc = acc_init(h->acc, n);
+  if (rc) return rc;
+  *out = h;
+  return kOk;
+}
+
+static SoftArgs soft_args(snb_lj_soft* h, snb_nl* nl, const snb_boundary& b, float beta) {
+  SoftArgs a;
+  a.n = h->n;
+  a.pos = h->d_pos;
+  a.par = h->d_par_sorted;
+  a.dq = h->d_dq_sorted;
+  a.global = nl->nl.d_global;
+  a.row_start = nl->nl.d_row_start;
+  a.cols = nl->nl.d_cols;
+  a.nl_flags = nl->nl.d_flags;
+  a.AA = h->d_AA;
+  a.AB = h->d_AB;
+  a.BA = h->d_BA;
+  a.BB = h->d_BB;
+  a.n_types_A = h->nA;
+  a.n_types_B = h->nB;
+  a.cell = cell_of(b);
+  a.rcell = rcell_of(b);
+  a.cutoff2 = h->cutoff * h->cutoff;
+  a.beta = beta;
+  a.lambda = h->lambda;
+  a.alpha = h->alpha;
+  a.p = h->p;
+  a.sigma6 = h->sigma6;
+  a.sigma6_min = h->sigma6_min;
+  return a;
+}
+
+extern "C" int snb_lj_soft_pme_direct_force(snb_lj_soft* h, int atom_numbers, int local_n,
+                                            int ghost_n, const float* crd,
+                                            const float* charge, const float* charge_B_A,
+                                            float* frc, snb_boundary boundary,
+                                            snb_nl* nl, float pme_beta,
+                                            int need_atom_energy, float* atom_energy,
+                                            int need_virial, float* atom_virial,
+                                            float* atom_direct_pme_energy, void* stream) {
+  if (!h || !nl) return fail(kBadInput, "lj_soft_pme_direct_force: null handle");
+  cudaStream_t st = S(stream);
+  if (need_atom_energy) {
+    SNB_CUDA_TRY(cudaMemsetAsync(h->d_lj_energy, 0, sizeof(float) * h->n, st));
+    SNB_CUDA_TRY(cudaMemsetAsync(h->d_inter, 0, sizeof(float) * h->n, st));
+    SNB_CUDA_TRY(cudaMemsetAsync(h->d_intra, 0, sizeof(float) * h->n, st));
+    if (atom_direct_pme_energy)
+      SNB_CUDA_TRY(cudaMemsetAsync(atom_direct_pme_energy, 0, sizeof(float) * h->n, st));
+  }
+  if (atom_numbers == 0 || local_n == 0) return kOk;
+  if (ghost_n != 0) return fail(kNotSupported, "lj_soft: ghost atoms");
+  if (local_n != h->n || nl->nl.n != h->n) return fail(kBadInput, "lj_soft: atom count");
+  int rc = launch_pack(h->n, reinterpret_cast<const float3*>(crd), charge, nullptr,
+                       nl->nl.d_perm, h->d_pos, nullptr, st);
+  if (rc) return rc;
+  k_pack_soft<<<ceil_div(h->n, 256), 256, 0, st>>>(h->n, nl->nl.d_perm, h->d_par_local,
+                                                  charge_B_A, h->d_par_sorted,
+                                                  h->d_dq_sorted);
+  SoftArgs a = soft_args(h, nl, boundary, pme_beta);
+  bool en = need_atom_energy != 0, vi = need_virial != 0;
+  rc = launch_soft(a, h->acc, h->accum, en, vi, false, nullptr, st);
+  if (rc) return rc;
+  if (en)
+    k_unpack_aux<<<ceil_div(h->n, 256), 256, 0, st>>>(h->n, nl->nl.d_inv_perm, h->acc,
+                                                     h->d_inter, h->d_intra, h->accum);
+  return launch_unpack(h->n, nl->nl.d_inv_perm, h->acc, h->accum,
+                       reinterpret_cast<float3*>(frc), en ? atom_energy : nullptr,
+                       en ? h->d_lj_energy : nullptr, en ? atom_direct_pme_energy : nullptr,
+                       vi ? atom_virial : nullptr, en, vi, st);
+}
+
+extern "C" int snb_lj_soft_dh_dlambda(snb_lj_soft* h, const float* crd,
+                                      const float* charge, const float* charge_B_A,
+                                      snb_boundary boundary, snb_nl* nl, float pme_beta,
+                                      int charge_perturbated, double* out, void* stream) {
+  (void)charge_perturbated;
+  if (!h || !nl || !out) return fail(kBadInput, "lj_soft_dh_dlambda: bad argument");
+  cudaStream_t st = S(stream);
+  int rc = launch_pack(h->n, reinterpret_cast<const float3*>(crd), charge, nullptr,
+                       nl->nl.d_perm, h->d_pos, nullptr, st);
+  if (rc) return rc;
+  k_pack_soft<<<ceil_div(h->n, 256), 256, 0, st>>>(h->n, nl->nl.d_perm, h->d_par_local,
+                                                  charge_B_A, h->d_par_sorted,
+                                                  h->d_dq_sorted);
+  SNB_CUDA_TRY(cudaMemsetAsync(h->d_dudl, 0, sizeof(long long) * 2, st));
+  SoftArgs a = soft_args(h, nl, boundary, pme_beta);
+  rc = launch_soft(a, h->acc, h->accum, false, false, true, h->d_dudl, st);
+  if (rc) return rc;
+  long long v[2];
+  SNB_CUDA_TRY(cudaMemcpyAsync(v, h->d_dudl, sizeof(v), cudaMemcpyDeviceToHost, st));
+  SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  // the reference returns the LJ part plus the tail term (LJ_soft_core.cpp:883-885)
+  double vol = (double)boundary.cell[0] * boundary.cell[2] * boundary.cell[5];
+  *out = (double)v[0] * kEnergyScaleInv + (double)h->lrc_ti / vol;
+  return kOk;
+}
+
+extern "C" int snb_lj_soft_long_range_correction(snb_lj_soft* h, int need_pressure,
+                                                 float* d_virial, int need_potential,
+                                                 float* d_potential, float volume,
+                                                 void* stream) {
+  if (!h) return fail(kBadInput, "lj_soft_long_range_correction: null handle");
+  return launch_add_scalars(need_potential > 0 ? d_potential : nullptr,
+                            need_pressure > 0 ? d_virial : nullptr, nullptr,
+                            h->lrc / volume, 2 * h->lrc / volume, 1, S(stream));
+}
+
+extern "C" int snb_lj_soft_destroy(snb_lj_soft* h) {
+  if (!h) return kOk;
+  for (void* p : {(void*)h->d_AA, (void*)h->d_AB, (void*)h->d_BA, (void*)h->d_BB,
+                  (void*)h->d_par, (void*)h->d_par_local, (void*)h->d_par_sorted,
+                  (void*)h->d_pos, (void*)h->d_dq_sorted, (void*)h->d_lj_energy,
+                  (void*)h->d_inter, (void*)h->d_intra, (void*)h->d_dudl})
+    cudaFree(p);
+  acc_free(h->acc);
+  delete h;
+  return kOk;
+}
+
+// ========================================================= Particle_Mesh
+extern "C" int snb_pme_create(const snb_options* opt, int atom_numbers,
+                              snb_boundary boundary, const float* box_length,
+                              float cutoff, snb_pme** out) {
+  if (!out) return fail(kBadInput, "pme_create: null out");
+  *out = nullptr;
+  snb_options o = opts_or_default(opt);
+  snb_pme* h = new snb_pme();
+  h->accum = o.accumulation;
+  float box[3] = {boundary.cell[0], boundary.cell[2], boundary.cell[5]};
+  if (box_length) memcpy(box, box_length, sizeof(box));
+  int rc = pme_init(h->p, atom_numbers, boundary.cell, box, cutoff,
+                    o.pm_direct_tolerance, o.pm_fftx, o.pm_ffty, o.pm_fftz,
+                    o.pm_grid_spacing, o.pme_update_interval,
+                    o.pme_calculate_reciprocal_part != 0,
+                    o.pme_calculate_excluded_part != 0);
+  if (rc) {
+    pme_free(h->p);
+    delete h;
+    return rc;
+  }
+  rc = acc_init(h->acc, atom_numbers);
+  if (rc) return rc;
+  SNB_CUDA_TRY(cudaMalloc(&h->d_pos, sizeof(float4) * atom_numbers));
+  *out = h;
+  return kOk;
+}
+
+extern "C" float snb_pme_beta(snb_pme* h) { return h ? h->p.beta : 0.f; }
+
+extern "C" int snb_pme_grid(snb_pme* h, int* fft3) {
+  if (!h || !fft3) return fail(kBadInput, "pme_grid: null argument");
+  for (int d = 0; d < 3; ++d) fft3[d] = h->p.K[d];
+  return kOk;
+}
+
+extern "C" int snb_pme_reciprocal_force(snb_pme* h, const float* crd,
+                                        snb_boundary boundary, const float* charge,
+                                        float* force, int need_virial, int need_energy,
+                                        float* d_virial, float* d_potential, int step,
+                                        void* stream) {
+  if (!h) return fail(kBadInput, "pme_reciprocal_force: null handle");
+  if (!h->p.reciprocal) return kOk;
+  cudaStream_t st = S(stream);
+  if (step % h->p.update_interval == 0) {
+    int rc = launch_pack(h->p.n, reinterpret_cast<const float3*>(crd), charge, nullptr,
+                         nullptr, h->d_pos, nullptr, st);
+    if (rc) return rc;
+    rc = pme_reciprocal(h->p, h->d_pos, h->p.n, h->acc, h->accum, need_energy != 0,
+                        need_virial != 0, st);
+    if (rc) return rc;
+    rc = launch_unpack(h->p.n, nullptr, h->acc, h->accum,
+                       reinterpret_cast<float3*>(force), nullptr, nullptr, nullptr,
+                       nullptr, false, false, st);
+    if (rc) return rc;
+  }
+  if (need_energy || need_virial)
+    return launch_add_scalars(need_energy ? d_potential : nullptr,
+                              need_virial ? d_virial : nullptr, h->p.d_sums, 0.f, 0.f, 0,
+                              st);
+  return kOk;
+}
+
+extern "C" int snb_pme_excluded_force(snb_pme* h, int atom_numbers,
+                                      const int* atom_local, const int* atom_local_id,
+                                      const float* crd, snb_boundary boundary,
+                                      const float* charge, const int* es,
+                                      const int* el, const int* en, float* frc,
+                                      int need_energy, float* atom_ene, int need_virial,
+                                      float* atom_virial, void* stream) {
+  (void)atom_local;
+  (void)atom_local_id;
+  if (!h) return fail(kBadInput, "pme_excluded_force: null handle");
+  if (!h->p.excluded) return kOk;
+  if (atom_numbers != h->p.n) return fail(kBadInput, "pme_excluded_force: atom count");
+  cudaStream_t st = S(stream);
+  int rc = launch_excluded(atom_numbers, reinterpret_cast<const float3*>(crd), charge,
+                           cell_of(boundary), rcell_of(boundary), h->p.beta, es, el, en,
+                           nullptr, h->acc, h->accum, need_energy != 0,
+                           need_virial != 0, st);
+  if (rc) return rc;
+  return launch_unpack(atom_numbers, nullptr, h->acc, h->accum,
+                       reinterpret_cast<float3*>(frc), need_energy ? atom_ene : nullptr,
+                       nullptr, nullptr, need_virial ? atom_virial : nullptr,
+                       need_energy != 0, need_virial != 0, st);
+}
+
+extern "C" int snb_pme_energies(snb_pme* h, double* rec, double* self, double* vir,
+                                void* stream) {
+  if (!h) return fail(kBadInput, "pme_energies: null handle");
+  double s[8];
+  SNB_CUDA_TRY(cudaMemcpyAsync(s, h->p.d_sums, sizeof(s), cudaMemcpyDeviceToHost,
+                               S(stream)));
+  SNB_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+  if (rec) *rec = s[0];
+  if (self) *self = s[7];
+  if (vir)
+    for (int c = 0; c < 6; ++c) vir[c] = s[1 + c];
+  return kOk;
+}
+
+extern "C" int snb_pme_destroy(snb_pme* h) {
+  if (!h) return kOk;
+  pme_free(h->p);
+  acc_free(h->acc);
+  cudaFree(h->d_pos);
+  delete h;
+  return kOk;
+}
+
+// ============================================================= engine
+extern "C" int snb_engine_create(const snb_options* opt, int n, snb_boundary boundary,
+                                 int n_types, const int* h_type, const float* h_A,
+                                 const float* h_B, const float* h_charge,
+                                 const int* h_es, const int* h_en, const int* h_el,
+                                 int n_excl, snb_engine** out) {
+  if (!out) return fail(kBadInput, "engine_create: null out");
+  *out = nullptr;
+  if (n <= 0 || n_types <= 0 || !h_type || !h_A || !h_B || !h_charge)
+    return fail(kBadInput, "engine_create: bad argument");
+  if (boundary.policy != 1) return fail(kNotSupported, "engine: periodic box required");
+  snb_engine* e = new snb_engine();
+  e->opt = opts_or_default(opt);
+  e->n = n;
+  e->accum = e->opt.accumulation;
+  e->cell = cell_of(boundary);
+  e->rcell = rcell_of(boundary);
+  int rc = nl_init(e->nl, n, e->opt.cutoff, e->opt.skin, boundary.cell,
+                   e->opt.nl_refresh_interval, e->opt.nl_skin_permit,
+                   e->opt.nl_max_neighbor_numbers, 0);
+  if (rc) {
+    delete e;
+    return rc;
+  }
+  float box[3] = {boundary.cell[0], boundary.cell[2], boundary.cell[5]};
+  rc = pme_init(e->pme, n, boundary.cell, box, e->opt.cutoff, e->opt.pm_direct_tolerance,
+                e->opt.pm_fftx, e->opt.pm_ffty, e->opt.pm_fftz, e->opt.pm_grid_spacing,
+                e->opt.pme_update_interval, e->opt.pme_calculate_reciprocal_part != 0,
+                e->opt.pme_calculate_excluded_part != 0);
+  if (rc) return rc;
+  rc = acc_init(e->acc, n);
+  if (rc) return rc;
+  LJParams& p = e->lj;
+  p.n_types = n_types;
+  p.n_pairs = n_types * (n_types + 1) / 2;
+  p.h_type.assign(h_type, h_type + n);
+  p.h_A.assign(h_A, h_A + p.n_pairs);
+  p.h_B.assign(h_B, h_B + p.n_pairs);
+  p.cutoff = e->opt.cutoff;
+  p.long_range_factor = lrc_factor(p.h_type, n_types, p.h_B, p.cutoff);
+  SNB_CUDA_TRY(cudaMalloc(&p.d_A, sizeof(float) * p.n_pairs));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_B, sizeof(float) * p.n_pairs));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_A, h_A, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_B, h_B, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_type, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_type, h_type, sizeof(int) * n, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_charge, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMemcpy(e->d_charge, h_charge, sizeof(float) * n, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_pos, sizeof(float4) * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_type_sorted, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_start, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_numbers, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_list, sizeof(int) * std::max(n_excl, 1)));
+  if (h_es && h_en) {
+    for (int i = 0; i < n; ++i) {
+      if (h_en[i] < 0 || (h_en[i] > 0 && (h_es[i] < 0 || h_es[i] + h_en[i] > n_excl))) {
+        snb_engine_destroy(e);
+        return fail(kBadInput, "engine_create: exclusion list out of range");
+      }
+      for (int k = 0; k < h_en[i]; ++k)
+        if (h_el[h_es[i] + k] < 0 || h_el[h_es[i] + k] >= n) {
+          snb_engine_destroy(e);
+          return fail(kBadInput, "engine_create: excluded atom index out of range");
+        }
+    }
+    SNB_CUDA_TRY(cudaMemcpy(e->d_excl_start, h_es, sizeof(int) * n, cudaMemcpyHostToDevice));
+    SNB_CUDA_TRY(cudaMemcpy(e->d_excl_numbers, h_en, sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (n_excl > 0)
+      SNB_CUDA_TRY(cudaMemcpy(e->d_excl_list, h_el, sizeof(int) * n_excl,
+                              cudaMemcpyHostToDevice));
+  } else {
+    SNB_CUDA_TRY(cudaMemset(e->d_excl_start, 0, sizeof(int) * n));
+    SNB_CUDA_TRY(cudaMemset(e->d_excl_numbers, 0, sizeof(int) * n));
+  }
+  SNB_CUDA_TRY(cudaMalloc(&e->d_isum, sizeof(long long) * 9));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_bonded_e, sizeof(long long)));
+  SNB_CUDA_TRY(cudaMemset(e->d_bonded_e, 0, sizeof(long long)));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_totals_scratch, sizeof(double) * 16));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_snap_crd, sizeof(float) * 3 * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_snap_vel, sizeof(float) * 3 * n));
+  *out = e;
+  return kOk;
+}
+
+// nonbonded forces of one step into e->acc (sorted frame), no unpack
+static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
+                         bool virial, bool forced_nl, cudaStream_t st) {
+  prof_mark(e, 0, st);
+  int rc = nl_update(e->nl, crd, nullptr, nullptr, step, forced_nl ? 1 : 0,
+                     e->d_excl_start, e->d_excl_list, e->d_excl_numbers, st);
+  if (rc) return rc;
+  prof_mark(e, 1, st);
+  rc = launch_pack(e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
+                   e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st);
+  if (rc) return rc;
+  prof_mark(e, 2, st);
+  PairArgs a;
+  a.n = e->n;
+  a.pos = e->d_pos;
+  a.type = e->d_type_sorted;
+  a.global = e->nl.d_global;
+  a.row_start = e->nl.d_row_start;
+  a.cols = e->nl.d_cols;
+  a.nl_flags = e->nl.d_flags;
+  a.A = e->lj.d_A;
+  a.B = e->lj.d_B;
+  a.n_types = e->lj.n_types;
+  a.cell = e->cell;
+  a.rcell = e->rcell;
+  a.cutoff2 = e->opt.cutoff * e->opt.cutoff;
+  a.beta = e->pme.beta;
+  rc = launch_pair(a, e->acc, e->accum, energy, virial, true, st);
+  if (rc) return rc;
+  prof_mark(e, 3, st);
+  if (e->pme.excluded) {
+    rc = launch_excluded(e->n, reinterpret_cast<const float3*>(crd), e->d_charge, e->cell,
+                         e->rcell, e->pme.beta, e->d_excl_start, e->d_excl_list,
+                         e->d_excl_numbers, e->nl.d_inv_perm, e->acc, e->accum, energy,
+                         virial, st);
+    if (rc) return rc;
+  }
+  prof_mark(e, 4, st);
+  if (e->pme.reciprocal && step % e->pme.update_interval == 0) {
+    rc = pme_reciprocal(e->pme, e->d_pos, e->n, e->acc, e->accum, energy, virial, st);
+    if (rc) return rc;
+  }
+  prof_mark(e, 5, st);
+  return kOk;
+}
+
+extern "C" int snb_engine_force(snb_engine* e, const float* crd, float* frc, int step,
+                                int need_energy, int need_virial, double* d_totals,
+                                void* stream) {
+  if (!e) return fail(kBadInput, "engine_force: null handle");
+  cudaStream_t st = S(stream);
+  bool en = need_energy != 0, vi = need_virial != 0;
+  if ((en || vi) && !d_totals) return fail(kBadInput, "engine_force: d_totals required");
+  if (en || vi) SNB_CUDA_TRY(cudaMemsetAsync(e->d_bonded_e, 0, sizeof(long long), st));
+  int rc = engine_forces(e, crd, step, en, vi, e->steps_done == 0, st);
+  if (rc) return rc;
+  e->steps_done++;
+  if (en || vi) {
+    double vol = (double)e->cell.a11 * e->cell.a22 * e->cell.a33;
+    rc = launch_totals(e->n, e->acc, e->d_isum, nullptr, e->pme.d_sums,
+                       e->lj.long_range_factor / vol, 2.0 * e->lj.long_range_factor / vol,
+                       d_totals, en, vi, e->pme.reciprocal, st);
+    if (rc) return rc;
+  }
+  return launch_unpack(e->n, e->nl.d_inv_perm, e->acc, e->accum,
+                       reinterpret_cast<float3*>(frc), nullptr, nullptr, nullptr, nullptr,
+                       en, vi, st);
+}
+
+extern "C" int snb_engine_set_bonded(snb_engine* e, int nb, const int* ba, const int* bb,
+                                     const float* bk, const float* br0, int na,
+                                     const int* aa, const int* ab, const int* ac,
+                                     const float* ak, const float* at0) {
+  if (!e) return fail(kBadInput, "engine_set_bonded: null handle");
+  for (int t = 0; t < nb; ++t)
+    if (ba[t] < 0 || ba[t] >= e->n || bb[t] < 0 || bb[t] >= e->n)
+      return fail(kBadInput, "engine_set_bonded: bond atom index out of range");
+  for (int t = 0; t < na; ++t)
+    if (aa[t] < 0 || aa[t] >= e->n || ab[t] < 0 || ab[t] >= e->n || ac[t] < 0 ||
+        ac[t] >= e->n)
+      return fail(kBadInput, "engine_set_bonded: angle atom index out of range");
+  auto up_i = [](int** d, const int* h, int m) -> int {
+    cudaFree(*d);
+    *d = nullptr;
+    if (m <= 0) return kOk;
+    SNB_CUDA_TRY(cudaMalloc(d, sizeof(int) * m));
+    SNB_CUDA_TRY(cudaMemcpy(*d, h, sizeof(int) * m, cudaMemcpyHostToDevice));
+    return kOk;
+  };
+  auto up_f = [](float** d, const float* h, int m) -> int {
+    cudaFree(*d);
+    *d = nullptr;
+    if (m <= 0) return kOk;
+    SNB_CUDA_TRY(cudaMalloc(d, sizeof(float) * m));
+    SNB_CUDA_TRY(cudaMemcpy(*d, h, sizeof(float) * m, cudaMemcpyHostToDevice));
+    return kOk;
+  };
+  int rc = up_i(&e->d_ba, ba, nb) | up_i(&e->d_bb, bb, nb) | up_f(&e->d_bk, bk, nb) |
+           up_f(&e->d_br0, br0, nb) | up_i(&e->d_aa, aa, na) | up_i(&e->d_ab, ab, na) |
+           up_i(&e->d_ac, ac, na) | up_f(&e->d_ak, ak, na) | up_f(&e->d_at0, at0, na);
+  if (rc) return fail(kCudaError, "engine_set_bonded: upload failed");
+  e->nb = nb;
+  e->na = na;
+  if (e->graph_exec) {
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+    e->graph = nullptr;
+  }
+  return kOk;
+}
+
+static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* invm,
+                          float dt, int step, bool forced_nl, cudaStream_t st) {
+  if (e->accum != kAccumFixed)
+    return fail(kNotSupported, "md steps need the fixed-point accumulation");
+  int rc = engine_forces(e, crd, step, false, false, forced_nl, st);
+  if (rc) return rc;
+  rc = launch_bonded(e->nb, e->d_ba, e->d_bb, e->d_bk, e->d_br0, e->na, e->d_aa, e->d_ab,
+                     e->d_ac, e->d_ak, e->d_at0, reinterpret_cast<const float3*>(crd),
+                     e->cell, e->rcell, e->nl.d_inv_perm, e->acc, nullptr, false, st);
+  if (rc) return rc;
+  prof_mark(e, 6, st);
+  rc = launch_leap_frog(e->n, e->nl.d_inv_perm, e->acc, reinterpret_cast<float3*>(crd),
+                        reinterpret_cast<float3*>(vel), invm, dt, st);
+  prof_mark(e, 7, st);
+  return rc;
+}
+
+// Runs `steps` steps; every check_overflow_interval steps reads the list
+// overflow flag and, on overflow, regrows the list, restores the snapshot
+// and repeats the steps since it (the recovery loop Check_Overflow was meant
+// to provide, neighbor_list.cpp:1027-1103).
+static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, float dt,
+                      int first, int steps, cudaStream_t st, bool use_graph) {
+  const int chk = std::max(1, e->opt.nl_check_overflow_interval);
+  int s = 0;
+  int retries = 0;
+  while (s < steps) {
+    int chunk = std::min(chk, steps - s);
+    SNB_CUDA_TRY(cudaMemcpyAsync(e->d_snap_crd, crd, sizeof(float) * 3 * e->n,
+                                 cudaMemcpyDeviceToDevice, st));
+    SNB_CUDA_TRY(cudaMemcpyAsync(e->d_snap_vel, vel, sizeof(float) * 3 * e->n,
+                                 cudaMemcpyDeviceToDevice, st));
+    for (int k = 0; k < chunk; ++k) {
+      int step = first + s + k;
+      // forced rebuild on the first step and every DOM_DEC_update_interval
+      // steps, as the reference MD loop does (main.cpp:1805-1822)
+      const int ui = e->opt.dom_dec_update_interval;
+      bool forced = e->steps_done == 0 || (ui > 0 && step > 0 && step % ui == 0);
+      if (use_graph && !forced) {
+        if (!e->graph_exec || e->g_crd != crd || e->g_vel != vel || e->g_invm != invm ||
+            e->g_dt != dt || e->g_stream != st) {
+          if (e->graph_exec) {
+            cudaGraphExecDestroy(e->graph_exec);
+            cudaGraphDestroy(e->graph);
+            e->graph_exec = nullptr;
+          }
+          SNB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+          int rc = engine_md_step(e, crd, vel, invm, dt, step, false, st);
+          cudaGraph_t g = nullptr;
+          cudaError_t ce = cudaStreamEndCapture(st, &g);
+          if (rc) return rc;
+          if (ce != cudaSuccess)
+            return fail(kCudaError, std::string("graph capture: ") + cudaGetErrorString(ce));
+          e->graph = g;
+          SNB_CUDA_TRY(cudaGraphInstantiate(&e->graph_exec, g, 0));
+          e->g_crd = crd;
+          e->g_vel = vel;
+          e->g_invm = invm;
+          e->g_dt = dt;
+          e->g_stream = st;
+        }
+        SNB_CUDA_TRY(cudaGraphLaunch(e->graph_exec, st));
+      } else {
+        int rc = engine_md_step(e, crd, vel, invm, dt, step, forced, st);
+        if (rc) return rc;
+      }
+      e->steps_done++;
+    }
+    bool regrown = false;
+    int rc = nl_check_overflow(e->nl, &regrown, st);
+    if (rc) return rc;
+    if (regrown) {
+      if (e->opt.nl_throw_error_when_overflow)
+        return fail(kOverflow, "neighbor list overflow");
+      if (++retries > 8) return fail(kOverflow, "neighbor list overflow persists");
+      if (e->graph_exec) {  // the graph holds the old list pointer
+        cudaGraphExecDestroy(e->graph_exec);
+        cudaGraphDestroy(e->graph);
+        e->graph_exec = nullptr;
+      }
+      SNB_CUDA_TRY(cudaMemcpyAsync(crd, e->d_snap_crd, sizeof(float) * 3 * e->n,
+                                   cudaMemcpyDeviceToDevice, st));
+      SNB_CUDA_TRY(cudaMemcpyAsync(vel, e->d_snap_vel, sizeof(float) * 3 * e->n,
+                                   cudaMemcpyDeviceToDevice, st));
+      e->steps_done = 0;  // forces a rebuild on the next step
+      continue;
+    }
+    s += chunk;
+  }
+  return kOk;
+}
+
+extern "C" int snb_engine_md_steps(snb_engine* e, float* crd, float* vel,
+                                   const float* invm, float dt, int first, int steps,
+                                   void* stream) {
+  if (!e || !crd || !vel || !invm) return fail(kBadInput, "engine_md_steps: bad argument");
+  return engine_run(e, crd, vel, invm, dt, first, steps, S(stream), false);
+}
+
+extern "C" int snb_engine_md_steps_graph(snb_engine* e, float* crd, float* vel,
+                                         const float* invm, float dt, int first,
+                                         int steps, void* stream) {
+  if (!e || !crd || !vel || !invm) return fail(kBadInput, "engine_md_steps: bad argument");
+  if (S(stream) == nullptr)
+    return fail(kBadInput, "graph replay needs a non-default stream");
+  bool graphable = e->opt.nl_refresh_interval <= 0 && e->pme.update_interval == 1;
+  return engine_run(e, crd, vel, invm, dt, first, steps, S(stream), graphable);
+}
+
+// Stream-launched steps with CUDA events between phases; h_phase_ms gets the
+// mean per step of {neighbor update, pack, pair kernel, excluded correction,
+// PME reciprocal, bonded, integration}.  Synchronises after every step.
+extern "C" int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
+                                        const float* invm, float dt, int first,
+                                        int steps, double* h_phase_ms, void* stream) {
+  if (!e || !crd || !vel || !invm || !h_phase_ms || steps <= 0)
+    return fail(kBadInput, "engine_profile_steps: bad argument");
+  cudaStream_t st = S(stream);
+  for (int k = 0; k < 8; ++k)
+    if (!e->prof_ev[k]) SNB_CUDA_TRY(cudaEventCreate(&e->prof_ev[k]));
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  e->prof_on = true;
+  for (int s = 0; s < steps; ++s) {
+    bool forced = e->steps_done == 0;
+    int rc = engine_md_step(e, crd, vel, invm, dt, first + s, forced, st);
+    if (rc) {
+      e->prof_on = false;
+      return rc;
+    }
+    e->steps_done++;
+    SNB_CUDA_TRY(cudaEventSynchronize(e->prof_ev[7]));
+    for (int k = 0; k < 7; ++k) {
+      float ms = 0.f;
+      SNB_CUDA_TRY(cudaEventElapsedTime(&ms, e->prof_ev[k], e->prof_ev[k + 1]));
+      acc[k] += ms;
+    }
+  }
+  e->prof_on = false;
+  for (int k = 0; k < 7; ++k) h_phase_ms[k] = acc[k] / steps;
+  return kOk;
+}
+
+// Kernel nodes in the captured one-step graph: all, and those that belong to
+// cuFFT (counted from a graph holding only the two transforms).
+extern "C" int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
+                                     int* library_kernel_nodes, void* stream) {
+  if (!e || !kernel_nodes || !library_kernel_nodes)
+    return fail(kBadInput, "engine_graph_info: bad argument");
+  auto count = [](cudaGraph_t g, int* out) -> int {
+    size_t nn = 0;
+    SNB_CUDA_TRY(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    SNB_CUDA_TRY(cudaGraphGetNodes(g, nodes.data(), &nn));
+    int k = 0;
+    for (auto nd : nodes) {
+      cudaGraphNodeType t;
+      SNB_CUDA_TRY(cudaGraphNodeGetType(nd, &t));
+      k += t == cudaGraphNodeTypeKernel;
+    }
+    *out = k;
+    return kOk;
+  };
+  if (!e->graph) return fail(kBadInput, "engine_graph_info: no graph captured yet");
+  int rc = count(e->graph, kernel_nodes);
+  if (rc) return rc;
+  cudaStream_t st = S(stream);
+  cudaGraph_t g = nullptr;
+  cufftSetStream(e->pme.plan_r2c, st);
+  cufftSetStream(e->pme.plan_c2r, st);
+  SNB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cufftExecR2C(e->pme.plan_r2c, e->pme.d_Q, e->pme.d_FQ);
+  cufftExecC2R(e->pme.plan_c2r, e->pme.d_FQ, e->pme.d_phi);
+  SNB_CUDA_TRY(cudaStreamEndCapture(st, &g));
+  rc = count(g, library_kernel_nodes);
+  cudaGraphDestroy(g);
+  return rc;
+}
+
+extern "C" int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
+                                void* stream) {
+  if (!e) return fail(kBadInput, "engine_stats: null handle");
+  bool regrown;
+  int rc = nl_check_overflow(e->nl, &regrown, S(stream));
+  if (rc) return rc;
+  if (rebuilds) *rebuilds = e->nl.h_flags[3];
+  if (pairs) *pairs = e->nl.last_total;
+  return kOk;
+}
+
+extern "C" int snb_engine_destroy(snb_engine* e) {
+  if (!e) return kOk;
+  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  for (int k = 0; k < 8; ++k)
+    if (e->prof_ev[k]) cudaEventDestroy(e->prof_ev[k]);
+  nl_free(e->nl);
+  pme_free(e->pme);
+  acc_free(e->acc);
+  cudaFree(e->lj.d_A);
+  cudaFree(e->lj.d_B);
+  cudaFree(e->lj.d_type);
+  cudaFree(e->d_pos);
+  cudaFree(e->d_type_sorted);
+  cudaFree(e->d_charge);
+  cudaFree(e->d_excl_start);
+  cudaFree(e->d_excl_numbers);
+  cudaFree(e->d_excl_list);
+  cudaFree(e->d_isum);
+  cudaFree(e->d_bonded_e);
+  cudaFree(e->d_totals_scratch);
+  cudaFree(e->d_snap_crd);
+  cudaFree(e->d_snap_vel);
+  for (void* p : {(void*)e->d_ba, (void*)e->d_bb, (void*)e->d_bk, (void*)e->d_br0,
+                  (void*)e->d_aa, (void*)e->d_ab, (void*)e->d_ac, (void*)e->d_ak,
+                  (void*)e->d_at0})
+    cudaFree(p);
+  delete e;
+  return kOk;
+}

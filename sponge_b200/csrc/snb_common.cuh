@@ -1,0 +1,126 @@
+// Shared device helpers for the sm_100a nonbonded kernels.
+//
+// Conventions (SPONGE internal units, SPONGE/common.h):
+//   length Angstrom, energy kcal/mol, charge pre-scaled by 18.2223,
+//   LJ pair tables A' = 12*A, B' = 6*B indexed by Get_LJ_Type
+//   (Lennard_Jones_force.h:19-28), box and virial as LTMatrix3
+//   {a11, a21, a22, a31, a32, a33} (utils/vector.hpp:249).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace snb {
+
+// Fixed-point scales.  Forces: 2^40 units per kcal/mol/A (|F| < 8.4e6 per
+// atom).  Energies and virials: 2^32 units per kcal/mol (|E| < 2.1e9 for the
+// whole box), so per-atom values and box totals both fit in int64.
+constexpr double kForceScale = 1099511627776.0;        // 2^40
+constexpr double kForceScaleInv = 1.0 / 1099511627776.0;
+constexpr double kEnergyScale = 4294967296.0;          // 2^32
+constexpr double kEnergyScaleInv = 1.0 / 4294967296.0;
+constexpr float kForceScaleF = 1099511627776.0f;
+constexpr float kEnergyScaleF = 4294967296.0f;
+// PME charge grid accumulated in int32 inside shared memory: 2^22 units per
+// (charge unit), |Q(g)| must stay below 512 (18.2223-scaled charges).
+constexpr float kGridScale = 4194304.0f;               // 2^22
+constexpr float kGridScaleInv = 1.0f / 4194304.0f;
+
+struct Cell {
+  float a11, a21, a22, a31, a32, a33;
+};
+
+__host__ __device__ __forceinline__ Cell make_cell(const float* c) {
+  Cell r;
+  r.a11 = c[0]; r.a21 = c[1]; r.a22 = c[2];
+  r.a31 = c[3]; r.a32 = c[4]; r.a33 = c[5];
+  return r;
+}
+
+// Minimum image exactly as the reference writes it (utils/boundary.h:31),
+// dr = a - b; dr - floorf(dr*rcell + 0.5f)*cell, every product and sum
+// rounded separately (no FMA contraction).  Used where results must match
+// the reference bit for bit: the neighbor-pair criterion.
+__device__ __forceinline__ float3 min_image_exact(float3 a, float3 b,
+                                                  const Cell& cell,
+                                                  const Cell& rcell) {
+  float dx = __fsub_rn(a.x, b.x);
+  float dy = __fsub_rn(a.y, b.y);
+  float dz = __fsub_rn(a.z, b.z);
+  float sx = __fadd_rn(__fadd_rn(__fmul_rn(dx, rcell.a11), __fmul_rn(dy, rcell.a21)),
+                       __fmul_rn(dz, rcell.a31));
+  float sy = __fadd_rn(__fmul_rn(dy, rcell.a22), __fmul_rn(dz, rcell.a32));
+  float sz = __fmul_rn(dz, rcell.a33);
+  float fx = floorf(__fadd_rn(sx, 0.5f));
+  float fy = floorf(__fadd_rn(sy, 0.5f));
+  float fz = floorf(__fadd_rn(sz, 0.5f));
+  float cx = __fadd_rn(__fadd_rn(__fmul_rn(fx, cell.a11), __fmul_rn(fy, cell.a21)),
+                       __fmul_rn(fz, cell.a31));
+  float cy = __fadd_rn(__fmul_rn(fy, cell.a22), __fmul_rn(fz, cell.a32));
+  float cz = __fmul_rn(fz, cell.a33);
+  return make_float3(__fsub_rn(dx, cx), __fsub_rn(dy, cy), __fsub_rn(dz, cz));
+}
+
+// |dr|^2 in the reference's operator order ((x*x + y*y) + z*z), unfused.
+__device__ __forceinline__ float norm2_exact(float3 d) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(d.x, d.x), __fmul_rn(d.y, d.y)),
+                   __fmul_rn(d.z, d.z));
+}
+
+// Fast minimum image for force evaluation.  Same image choice as the
+// reference (floor(s + 0.5)), contraction allowed.  ORTHO skips the
+// off-diagonal terms of a rectangular box.
+template <bool ORTHO>
+__device__ __forceinline__ float3 min_image_fast(float3 a, float3 b,
+                                                 const Cell& cell,
+                                                 const Cell& rcell) {
+  float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+  if (ORTHO) {
+    dx -= floorf(dx * rcell.a11 + 0.5f) * cell.a11;
+    dy -= floorf(dy * rcell.a22 + 0.5f) * cell.a22;
+    dz -= floorf(dz * rcell.a33 + 0.5f) * cell.a33;
+  } else {
+    float sx = dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31;
+    float sy = dy * rcell.a22 + dz * rcell.a32;
+    float sz = dz * rcell.a33;
+    float fx = floorf(sx + 0.5f), fy = floorf(sy + 0.5f), fz = floorf(sz + 0.5f);
+    dx -= fx * cell.a11 + fy * cell.a21 + fz * cell.a31;
+    dy -= fy * cell.a22 + fz * cell.a32;
+    dz -= fz * cell.a33;
+  }
+  return make_float3(dx, dy, dz);
+}
+
+// Triangular LJ pair index, Get_LJ_Type (Lennard_Jones_force.h:19-28).
+__host__ __device__ __forceinline__ int lj_pair_index(int a, int b) {
+  int hi = a > b ? a : b, lo = a > b ? b : a;
+  return ((hi * (hi + 1)) >> 1) + lo;
+}
+
+__device__ __forceinline__ long long to_fixed_force(float f) {
+  return __float2ll_rn(f * kForceScaleF);
+}
+__device__ __forceinline__ long long to_fixed_energy(float e) {
+  return __float2ll_rn(e * kEnergyScaleF);
+}
+__device__ __forceinline__ void red_add(long long* p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(p),
+            static_cast<unsigned long long>(v));
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Ceiling division for launch shapes.
+__host__ __device__ __forceinline__ int ceil_div(long long a, int b) {
+  return static_cast<int>((a + b - 1) / b);
+}
+
+}  // namespace snb

@@ -1,0 +1,259 @@
+// Internal state of the nonbonded engine and the launchers each .cu exposes.
+// Not part of the public C-ABI (that is include/sponge_nb.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "snb_common.cuh"
+
+namespace snb {
+
+// ----------------------------------------------------------------------------
+// Status codes (mirrored in include/sponge_nb.h)
+enum Status {
+  kOk = 0,
+  kBadInput = 1,
+  kCudaError = 2,
+  kOverflow = 3,
+  kTimeout = 4,
+  kNotSupported = 5,
+};
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+#define SNB_CUDA_TRY(expr)                                                   \
+  do {                                                                       \
+    cudaError_t e_ = (expr);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      return ::snb::fail(::snb::kCudaError,                                  \
+                         std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Scratch for the device-wide exclusive scan (3-phase).
+struct ScanScratch {
+  int* block_sums = nullptr;
+  int capacity_blocks = 0;
+};
+constexpr int kScanBlock = 1024;
+int scan_exclusive(const int* in, int* out, int n, int* total_out,
+                   ScanScratch& s, cudaStream_t st);
+
+// ----------------------------------------------------------------------------
+// Neighbor list: cell grid of side >= (cutoff+skin)/2 (neighbor_list.cpp:943),
+// atoms counting-sorted by cell (stable: ties by caller index), half list in
+// the sorted frame stored as CSR rows.
+struct NeighborList {
+  int n = 0;
+  float cutoff = 10.f, skin = 2.f;
+  float grid_length = 6.f;
+  float rl2 = 144.f;           // (grid_length^2)*4, formed as the reference
+  int refresh_interval = 0;    // neighbor_list_refresh_interval
+  float skin_permit = 0.5f;    // neighbor_list_skin_permit
+  int max_neighbor_numbers = 1200;  // capacity of the exported ATOM_GROUP slab
+  int Nx = 0, Ny = 0, Nz = 0, ncell = 0;
+  Cell cell{}, rcell{};
+  bool ortho = true;
+  // per-cell runs of forward neighbor cells (cell index > own), merged into
+  // contiguous cell ranges [first, last]
+  int max_runs = 0;
+  int2* d_run_ranges = nullptr;  // [ncell][max_runs] {first_cell, last_cell}
+  int* d_run_count = nullptr;  // [ncell]
+  // binning
+  int* d_cell_count = nullptr;  // [ncell]
+  int* d_cell_start = nullptr;  // [ncell + 1]
+  int* d_atom_cell = nullptr;   // [n] cell of caller atom
+  int* d_atom_slot = nullptr;   // [n]
+  int* d_perm = nullptr;        // [n] sorted -> caller index
+  int* d_inv_perm = nullptr;    // [n] caller -> sorted index
+  int* d_global = nullptr;      // [n] sorted -> global id (atom_local)
+  float4* d_pos = nullptr;      // [n] sorted build-time coordinates (x,y,z,-)
+  float3* d_old_crd = nullptr;  // [n] caller-frame coordinates at last build
+  // list
+  int* d_row_count = nullptr;   // [n]
+  int* d_row_start = nullptr;   // [n + 1]
+  int* d_cols = nullptr;        // [cap] sorted-frame j of each pair
+  long long cap = 0;
+  int* d_unsorted = nullptr;    // [n] cell-binned caller indices before ordering
+  int* d_sorted_cell = nullptr;  // [n] cell of each sorted atom
+  int* d_flags = nullptr;       // [0] need_update  [1] list overflow  [2] pair total
+                                // [3] rebuild count  [4] export overflow
+  int* h_flags = nullptr;       // pinned mirror
+  ScanScratch scan;
+  long long last_total = 0;
+  int generation = 0;
+};
+
+int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell6,
+            int refresh_interval, float skin_permit, int max_neighbor_numbers,
+            long long initial_capacity);
+void nl_free(NeighborList& nl);
+// Update as NEIGHBOR_LIST::Update (neighbor_list.cpp:974-1025): forced, or
+// conditional on the displacement check / refresh interval.  Device-side
+// decision; no host sync.
+int nl_update(NeighborList& nl, const float* crd, const int* atom_local,
+              const float* cell6, int step, int forced, const int* excl_start,
+              const int* excl_list, const int* excl_numbers, cudaStream_t st);
+// Reads the overflow flag and regrows the pair storage if needed (host sync).
+int nl_check_overflow(NeighborList& nl, bool* regrown, cudaStream_t st);
+int nl_total_pairs(NeighborList& nl, long long* total, cudaStream_t st);
+// Reference-format export (ATOM_GROUP {int n, int ghost_n, int* serial}).
+int nl_export_atom_groups(NeighborList& nl, void* d_groups, int* d_slab,
+                          int max_neighbor_numbers, cudaStream_t st);
+int nl_export_pairs(NeighborList& nl, int* d_pi, int* d_pj, long long cap,
+                    long long* count, cudaStream_t st);
+
+// ----------------------------------------------------------------------------
+// Accumulation mode.
+enum Accum { kAccumFixed = 0, kAccumFloat = 1 };
+
+// Per-atom accumulators in the sorted frame.
+struct Accumulators {
+  int n = 0;
+  long long* d_f = nullptr;     // [3][n] fixed-point forces (2^40)
+  long long* d_e = nullptr;     // [n] fixed-point energy (2^32)  (pair owner)
+  long long* d_elj = nullptr;   // [n] LJ part
+  long long* d_ec = nullptr;    // [n] direct Coulomb part
+  long long* d_v = nullptr;     // [6][n] fixed-point virial (2^32)
+  float* d_ff = nullptr;        // [3][n] float forces (plain path)
+  float* d_fe = nullptr;        // [3][n] float energies e, elj, ec
+  float* d_fv = nullptr;        // [6][n] float virial
+  long long* d_eaux = nullptr;  // [2][n] soft-core LJ energy inter / intra subsystem
+  float* d_feaux = nullptr;     // [2][n] float version
+};
+int acc_init(Accumulators& a, int n);
+void acc_free(Accumulators& a);
+
+// ----------------------------------------------------------------------------
+// Lennard-Jones + direct Coulomb.
+struct LJParams {
+  int n_types = 0;
+  int n_pairs = 0;
+  float* d_A = nullptr;
+  float* d_B = nullptr;
+  int* d_type = nullptr;        // caller frame [n]
+  int* d_type_local = nullptr;  // after Get_Local
+  std::vector<int> h_type;
+  std::vector<float> h_A, h_B;
+  float cutoff = 10.f;
+  float long_range_factor = 0.f;
+};
+
+struct PairArgs {
+  int n;
+  const float4* pos;            // sorted (x,y,z,q)
+  const int* type;              // sorted LJ type
+  const int* global;            // sorted -> global id (owner rule)
+  const int* row_start;
+  const int* cols;
+  const int* nl_flags;          // neighbor-list flags: skip when the list overflowed
+  const float* A;
+  const float* B;
+  int n_types;
+  Cell cell, rcell;
+  float cutoff2;
+  float beta;
+};
+int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
+                bool virial, bool ortho, cudaStream_t st);
+
+// Soft-core LJ + direct Coulomb (LJ_SOFT_CORE).
+struct SoftArgs {
+  int n;
+  const float4* pos;            // sorted (x,y,z,q)
+  const int2* par;              // sorted {typeA | typeB << 16, mask}
+  const float* dq;              // sorted charge_B - charge_A (may be null)
+  const int* global;
+  const int* row_start;
+  const int* cols;
+  const int* nl_flags;
+  const float* AA;              // A' of state A, per pair of A types
+  const float* AB;              // B' of state A
+  const float* BA;              // A' of state B, per pair of B types
+  const float* BB;              // B' of state B
+  int n_types_A, n_types_B;
+  Cell cell, rcell;
+  float cutoff2;
+  float beta;
+  float lambda, alpha, p;
+  float sigma6, sigma6_min;
+};
+int launch_soft(const SoftArgs& a, Accumulators& acc, int accum, bool energy,
+                bool virial, bool dudl, long long* dudl_total, cudaStream_t st);
+
+// ----------------------------------------------------------------------------
+// Particle mesh Ewald (reciprocal part).
+struct PME {
+  int n = 0;
+  int K[3] = {0, 0, 0};
+  int nall = 0, nfft = 0;
+  float beta = 0.f;
+  float cutoff = 10.f;
+  float tolerance = 1e-5f;
+  int update_interval = 1;
+  bool reciprocal = true, excluded = true;
+  Cell cell{}, rcell{};
+  double volume = 0.0;
+  // tiles of the charge grid owned by spread CTAs
+  int T = 8;
+  int nt[3] = {0, 0, 0};
+  int ntiles = 0;
+  float* d_B[3] = {nullptr, nullptr, nullptr};  // |b(k)|^2 per axis
+  float* d_Q = nullptr;         // [nall]
+  cufftComplex* d_FQ = nullptr;  // [nfft]
+  float* d_phi = nullptr;       // [nall]
+  int* d_tile_count = nullptr;  // [ntiles]
+  int* d_tile_start = nullptr;  // [ntiles + 1]
+  int* d_atom_tile = nullptr;   // [n]
+  int* d_atom_slot = nullptr;   // [n]
+  float4* d_binned = nullptr;   // [n] (frx, fry, frz, q) in tile order
+  int* d_binned_u = nullptr;    // [n] packed base point in tile order
+  double* d_partial = nullptr;  // [nblocks][8] energy + virial partial sums
+  double* d_sums = nullptr;     // [8]: e_recip, virial[6], spare
+  int partial_blocks = 0;
+  int4* d_src[3] = {nullptr, nullptr, nullptr};  // per-axis source bins of a tile
+  float4* d_frq = nullptr;      // [n] (frx, fry, frz, q) in input order
+  int* d_upk = nullptr;         // [n] packed base point in input order
+  cufftHandle plan_r2c = 0, plan_c2r = 0;
+  ScanScratch scan;
+};
+int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
+             float cutoff, float tolerance, int fftx, int ffty, int fftz,
+             float grid_spacing, int update_interval, bool reciprocal,
+             bool excluded);
+void pme_free(PME& p);
+float get_beta(float cutoff, float tolerance);
+int fft_size(float length);
+
+// Reciprocal forces for atoms given as pos (x,y,z,q), accumulated into acc at
+// index i (the frame of pos).  Energy/virial sums land in p.d_sums (FP64).
+int pme_reciprocal(PME& p, const float4* pos, int n, Accumulators& acc,
+                   int accum, bool need_energy, bool need_virial,
+                   cudaStream_t st);
+
+// Excluded-pair correction (PM_force.cpp:1745-1817).  Caller-frame inputs;
+// forces land in acc at map[i] (map = inv_perm, or nullptr for identity).
+int launch_excluded(int n, const float3* crd, const float* charge,
+                    const Cell& cell, const Cell& rcell, float beta,
+                    const int* excl_start, const int* excl_list,
+                    const int* excl_numbers, const int* map, Accumulators& acc,
+                    int accum, bool energy, bool virial, cudaStream_t st);
+
+// ----------------------------------------------------------------------------
+// Frame conversion kernels.
+int launch_pack(int n, const float3* crd, const float* charge, const int* type,
+                const int* perm, float4* pos, int* type_sorted, cudaStream_t st);
+// frc[caller i] += acc[map[i]] (converted), optional energies/virials, then
+// zero the accumulators.
+int launch_unpack(int n, const int* map, Accumulators& acc, int accum,
+                  float3* frc, float* atom_energy, float* lj_energy,
+                  float* coul_energy, float* atom_virial, bool energy,
+                  bool virial, cudaStream_t st);
+int launch_zero_acc(Accumulators& acc, int accum, bool energy, bool virial,
+                    cudaStream_t st);
+
+}  // namespace snb

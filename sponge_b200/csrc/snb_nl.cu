@@ -1,0 +1,558 @@
+// Neighbor list build: the NEIGHBOR_LIST path (neighbor_list.cpp) re-designed
+// for sm_100a.
+//
+// The pair criterion is the reference's, bit for bit: pair (i, j) with global
+// ids gi < gj is listed when |Get_Displacement(crd_i, crd_j)|^2 < rl2, with
+// rl2 = (0.5*(cutoff+skin))^2*4 and the minimum image and square evaluated in
+// the reference's operation order without FMA contraction
+// (neighbor_list.cpp:509-517, 847; utils/boundary.h:31); excluded pairs are
+// dropped when gj is in the exclusion list of gi (:744-803).
+//
+// The layout is different.  Atoms are counting-sorted into cells of side
+// L/floor(L/((cutoff+skin)/2)) with a stable order inside each cell (caller
+// index), so the sorted order and the list are deterministic.  One warp scans,
+// for one sorted atom i, the atoms after i in its own cell and every
+// forward neighbor cell (cell index larger than its own, +-2 cells), walked as
+// merged runs of consecutive cells: each run is one contiguous slice of the
+// sorted coordinate array, read with coalesced 16-byte loads.  A count pass
+// and a fill pass (same scan) produce CSR rows: no per-atom capacity, no list
+// atomics, no ballot-order races.
+#include <algorithm>
+#include <set>
+#include <vector>
+
+#include "snb_internal.h"
+
+namespace snb {
+
+// flags layout
+enum { kFlagNeed = 0, kFlagListOverflow = 1, kFlagTotal = 2, kFlagGeneration = 3,
+       kFlagExportOverflow = 4, kNumFlags = 8 };
+
+// ---------------------------------------------------------------------------
+// Refresh decision (Check_Refresh, neighbor_list.cpp:307-321): any atom moved
+// more than skin*skin_permit since the last build.
+__global__ void k_check_refresh(int n, const float3* __restrict__ crd,
+                                const float3* __restrict__ old_crd, Cell cell,
+                                Cell rcell, float permit2, int* flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool moved = false;
+  if (i < n) {
+    float3 d = min_image_fast<false>(crd[i], old_crd[i], cell, rcell);
+    moved = d.x * d.x + d.y * d.y + d.z * d.z > permit2;
+  }
+  if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0)
+    atomicExch(&flags[kFlagNeed], 1);
+}
+
+__global__ void k_set_need(int* flags, int v) { flags[kFlagNeed] = v; }
+
+// ---------------------------------------------------------------------------
+// Binning.  Cell of the wrapped coordinate with uniform cells of side L/N.
+__device__ __forceinline__ int wrapped_cell(float3 r, const Cell& cell, int Nx,
+                                            int Ny, int Nz) {
+  // Wrap_Coordinate-style reduction into [0, L) for a rectangular box.
+  float x = r.x - floorf(r.x / cell.a11) * cell.a11;
+  float y = r.y - floorf(r.y / cell.a22) * cell.a22;
+  float z = r.z - floorf(r.z / cell.a33) * cell.a33;
+  int nx = (int)(x / cell.a11 * Nx);
+  int ny = (int)(y / cell.a22 * Ny);
+  int nz = (int)(z / cell.a33 * Nz);
+  nx = nx < 0 ? 0 : (nx < Nx ? nx : Nx - 1);
+  ny = ny < 0 ? 0 : (ny < Ny ? ny : Ny - 1);
+  nz = nz < 0 ? 0 : (nz < Nz ? nz : Nz - 1);
+  return (nx * Ny + ny) * Nz + nz;
+}
+
+__global__ void k_bin_count(int n, const float3* __restrict__ crd, Cell cell,
+                            int Nx, int Ny, int Nz, int* __restrict__ atom_cell,
+                            int* __restrict__ atom_slot, int* __restrict__ cell_count,
+                            const int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int c = wrapped_cell(crd[i], cell, Nx, Ny, Nz);
+  atom_cell[i] = c;
+  atom_slot[i] = atomicAdd(&cell_count[c], 1);
+}
+
+__global__ void k_bin_scatter(int n, const int* __restrict__ atom_cell,
+                              const int* __restrict__ atom_slot,
+                              const int* __restrict__ cell_start,
+                              int* __restrict__ unsorted, const int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsorted[cell_start[atom_cell[i]] + atom_slot[i]] = i;
+}
+
+// One warp per cell: stable order inside the cell by caller index (rank sort).
+__global__ void k_cell_order(int ncell, const int* __restrict__ cell_start,
+                             const int* __restrict__ unsorted,
+                             int* __restrict__ perm, const int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int lane = threadIdx.x & 31;
+  if (c >= ncell) return;
+  int a = cell_start[c], b = cell_start[c + 1];
+  for (int k = a + lane; k < b; k += 32) {
+    int v = unsorted[k];
+    int rank = 0;
+    for (int m = a; m < b; ++m) rank += unsorted[m] < v;
+    perm[a + rank] = v;
+  }
+}
+
+__global__ void k_fill_sorted(int n, const int* __restrict__ perm,
+                              const float3* __restrict__ crd,
+                              const int* __restrict__ atom_local,
+                              int* __restrict__ inv_perm, int* __restrict__ global,
+                              float4* __restrict__ pos, float3* __restrict__ old_crd,
+                              const int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int i = perm[s];
+  inv_perm[i] = s;
+  global[s] = atom_local ? atom_local[i] : i;
+  float3 r = crd[i];
+  pos[s] = make_float4(r.x, r.y, r.z, 0.f);
+  old_crd[i] = r;
+}
+
+// ---------------------------------------------------------------------------
+// Is gh in the exclusion list of gl?  (Delete_Excluded_Atoms_Serial_In_
+// Neighbor_List, neighbor_list.cpp:744-773, single domain.)
+__device__ __forceinline__ bool excluded_pair(int gl, int gh,
+                                              const int* __restrict__ excl_start,
+                                              const int* __restrict__ excl_list,
+                                              const int* __restrict__ excl_numbers) {
+  if (!excl_numbers) return false;
+  int cnt = excl_numbers[gl];
+  if (cnt <= 0) return false;
+  int st = excl_start[gl];
+  for (int k = 0; k < cnt; ++k)
+    if (excl_list[st + k] == gh) return true;
+  return false;
+}
+
+// Pair search for sorted atom i (one warp).  PASS 0 counts, PASS 1 writes.
+template <int PASS>
+__global__ void __launch_bounds__(256)
+k_pair_search(int n, const float4* __restrict__ pos, const int* __restrict__ global,
+              const int* __restrict__ sorted_cell, const int* __restrict__ cell_start,
+              const int2* __restrict__ runs, const int* __restrict__ run_count,
+              int max_runs, Cell cell, Cell rcell, float rl2,
+              const int* __restrict__ excl_start, const int* __restrict__ excl_list,
+              const int* __restrict__ excl_numbers, int* __restrict__ row_count,
+              const int* __restrict__ row_start, int* __restrict__ cols,
+              long long cap, int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  if (PASS == 1 && (long long)flags[kFlagTotal] > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) flags[kFlagListOverflow] = 1;
+    return;
+  }
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= n) return;
+  const float4 pi4 = pos[i];
+  const float3 ri = make_float3(pi4.x, pi4.y, pi4.z);
+  const int gi = global[i];
+  const int c = sorted_cell[i];
+  int count = 0;
+  int out = PASS == 1 ? row_start[i] : 0;
+  const int nr = run_count[c];
+  // range list: own cell after i, then forward runs
+  for (int r = -1; r < nr; ++r) {
+    int a, b;
+    if (r < 0) {
+      a = i + 1;
+      b = cell_start[c + 1];
+    } else {
+      int2 rr = runs[(size_t)c * max_runs + r];
+      a = cell_start[rr.x];
+      b = cell_start[rr.y + 1];
+    }
+    for (int base = a; base < b; base += 32) {
+      int j = base + lane;
+      bool hit = false;
+      if (j < b) {
+        float4 pj4 = pos[j];
+        float3 rj = make_float3(pj4.x, pj4.y, pj4.z);
+        int gj = global[j];
+        bool i_low = gi < gj;
+        float3 d = i_low ? min_image_exact(ri, rj, cell, rcell)
+                         : min_image_exact(rj, ri, cell, rcell);
+        if (norm2_exact(d) < rl2) {
+          hit = !excluded_pair(i_low ? gi : gj, i_low ? gj : gi, excl_start,
+                               excl_list, excl_numbers);
+        }
+      }
+      unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (PASS == 1 && hit) {
+        int rank = __popc(m & ((1u << lane) - 1u));
+        cols[out + rank] = j;
+      }
+      out += __popc(m);
+      count += __popc(m);
+    }
+  }
+  if (PASS == 0 && lane == 0) row_count[i] = count;
+}
+
+__global__ void k_sorted_cell(int n, const int* __restrict__ perm,
+                              const int* __restrict__ atom_cell, int* __restrict__ sc,
+                              const int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) sc[s] = atom_cell[perm[s]];
+}
+
+__global__ void k_finish_build(int* flags) {
+  if (flags[kFlagNeed] != 0) flags[kFlagGeneration] += 1;
+}
+
+// ---------------------------------------------------------------------------
+static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
+                       std::vector<int>& counts, int& max_runs) {
+  int ncell = Nx * Ny * Nz;
+  std::vector<std::vector<int2>> per(ncell);
+  max_runs = 0;
+  for (int cx = 0; cx < Nx; ++cx)
+    for (int cy = 0; cy < Ny; ++cy)
+      for (int cz = 0; cz < Nz; ++cz) {
+        int c = (cx * Ny + cy) * Nz + cz;
+        std::set<int> nb;
+        for (int dx = -2; dx <= 2; ++dx)
+          for (int dy = -2; dy <= 2; ++dy)
+            for (int dz = -2; dz <= 2; ++dz) {
+              int x = ((cx + dx) % Nx + Nx) % Nx;
+              int y = ((cy + dy) % Ny + Ny) % Ny;
+              int z = ((cz + dz) % Nz + Nz) % Nz;
+              int o = (x * Ny + y) * Nz + z;
+              if (o > c) nb.insert(o);
+            }
+        std::vector<int2> rr;
+        for (int o : nb) {
+          if (!rr.empty() && rr.back().y == o - 1)
+            rr.back().y = o;
+          else
+            rr.push_back(make_int2(o, o));
+        }
+        max_runs = std::max(max_runs, (int)rr.size());
+        per[c] = rr;
+      }
+  if (max_runs == 0) max_runs = 1;
+  runs.assign((size_t)ncell * max_runs, make_int2(0, -1));
+  counts.assign(ncell, 0);
+  for (int c = 0; c < ncell; ++c) {
+    counts[c] = (int)per[c].size();
+    for (size_t k = 0; k < per[c].size(); ++k) runs[(size_t)c * max_runs + k] = per[c][k];
+  }
+}
+
+int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell6,
+            int refresh_interval, float skin_permit, int max_neighbor_numbers,
+            long long initial_capacity) {
+  if (n <= 0) return fail(kBadInput, "neighbor list: atom_numbers must be > 0");
+  nl.n = n;
+  nl.cutoff = cutoff;
+  nl.skin = skin;
+  nl.grid_length = 0.5f * (cutoff + skin);
+  nl.rl2 = nl.grid_length * nl.grid_length * 4.0f;
+  nl.refresh_interval = refresh_interval;
+  nl.skin_permit = skin_permit;
+  nl.max_neighbor_numbers = max_neighbor_numbers;
+  nl.cell = make_cell(cell6);
+  if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f)
+    return fail(kNotSupported,
+                "neighbor list: only rectangular boxes are supported "
+                "(triclinic cells are not built on this path)");
+  Cell rc{};
+  rc.a11 = 1.0f / nl.cell.a11;
+  rc.a22 = 1.0f / nl.cell.a22;
+  rc.a33 = 1.0f / nl.cell.a33;
+  nl.rcell = rc;
+  nl.ortho = true;
+  nl.Nx = (int)floorf(nl.cell.a11 / nl.grid_length);
+  nl.Ny = (int)floorf(nl.cell.a22 / nl.grid_length);
+  nl.Nz = (int)floorf(nl.cell.a33 / nl.grid_length);
+  if (nl.Nx <= 2 || nl.Ny <= 2 || nl.Nz <= 2)
+    return fail(kBadInput, "NEIGHBOR_LIST::Initial: the box is too small.");
+  nl.ncell = nl.Nx * nl.Ny * nl.Nz;
+  std::vector<int2> runs;
+  std::vector<int> counts;
+  build_runs(nl.Nx, nl.Ny, nl.Nz, runs, counts, nl.max_runs);
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_run_ranges, sizeof(int2) * runs.size()));
+  SNB_CUDA_TRY(cudaMemcpy(nl.d_run_ranges, runs.data(), sizeof(int2) * runs.size(),
+                          cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_run_count, sizeof(int) * nl.ncell));
+  SNB_CUDA_TRY(cudaMemcpy(nl.d_run_count, counts.data(), sizeof(int) * nl.ncell,
+                          cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_cell_count, sizeof(int) * nl.ncell));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_cell_start, sizeof(int) * (nl.ncell + 1)));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_atom_cell, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_atom_slot, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_perm, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_inv_perm, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_global, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_pos, sizeof(float4) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_old_crd, sizeof(float3) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_row_count, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_row_start, sizeof(int) * (n + 1)));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_flags, sizeof(int) * kNumFlags));
+  SNB_CUDA_TRY(cudaMemset(nl.d_flags, 0, sizeof(int) * kNumFlags));
+  SNB_CUDA_TRY(cudaMallocHost(&nl.h_flags, sizeof(int) * kNumFlags));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_unsorted, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_sorted_cell, sizeof(int) * n));
+  {
+    // before the first build: identity frame and empty rows
+    std::vector<int> iota(n);
+    for (int i = 0; i < n; ++i) iota[i] = i;
+    SNB_CUDA_TRY(cudaMemcpy(nl.d_perm, iota.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    SNB_CUDA_TRY(cudaMemcpy(nl.d_inv_perm, iota.data(), sizeof(int) * n,
+                            cudaMemcpyHostToDevice));
+    SNB_CUDA_TRY(cudaMemcpy(nl.d_global, iota.data(), sizeof(int) * n,
+                            cudaMemcpyHostToDevice));
+    SNB_CUDA_TRY(cudaMemset(nl.d_row_count, 0, sizeof(int) * n));
+    SNB_CUDA_TRY(cudaMemset(nl.d_row_start, 0, sizeof(int) * (n + 1)));
+    SNB_CUDA_TRY(cudaMemset(nl.d_sorted_cell, 0, sizeof(int) * n));
+    SNB_CUDA_TRY(cudaMemset(nl.d_pos, 0, sizeof(float4) * n));
+  }
+  // Capacity estimate: half-sphere of radius rl at the box's mean density,
+  // with 30% headroom; regrown on overflow by nl_check_overflow.
+  if (initial_capacity <= 0) {
+    double vol = (double)nl.cell.a11 * nl.cell.a22 * nl.cell.a33;
+    double rho = n / vol;
+    double rl = sqrt((double)nl.rl2);
+    double per = 0.5 * rho * 4.18879020478639 * rl * rl * rl;
+    initial_capacity = (long long)(1.3 * per * n) + 1024;
+  }
+  nl.cap = initial_capacity;
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_cols, sizeof(int) * nl.cap));
+  return kOk;
+}
+
+void nl_free(NeighborList& nl) {
+  cudaFree(nl.d_unsorted);
+  cudaFree(nl.d_sorted_cell);
+  cudaFree(nl.d_run_ranges);
+  cudaFree(nl.d_run_count);
+  cudaFree(nl.d_cell_count);
+  cudaFree(nl.d_cell_start);
+  cudaFree(nl.d_atom_cell);
+  cudaFree(nl.d_atom_slot);
+  cudaFree(nl.d_perm);
+  cudaFree(nl.d_inv_perm);
+  cudaFree(nl.d_global);
+  cudaFree(nl.d_pos);
+  cudaFree(nl.d_old_crd);
+  cudaFree(nl.d_row_count);
+  cudaFree(nl.d_row_start);
+  cudaFree(nl.d_cols);
+  cudaFree(nl.d_flags);
+  if (nl.h_flags) cudaFreeHost(nl.h_flags);
+  cudaFree(nl.scan.block_sums);
+  nl = NeighborList();
+}
+
+int nl_update(NeighborList& nl, const float* crd_f, const int* atom_local,
+              const float* cell6, int step, int forced, const int* excl_start,
+              const int* excl_list, const int* excl_numbers, cudaStream_t st) {
+  const float3* crd = reinterpret_cast<const float3*>(crd_f);
+  if (cell6) {
+    Cell c = make_cell(cell6);
+    if (c.a11 != nl.cell.a11 || c.a22 != nl.cell.a22 || c.a33 != nl.cell.a33 ||
+        c.a21 != 0.f || c.a31 != 0.f || c.a32 != 0.f)
+      return fail(kNotSupported,
+                  "neighbor list: the box changed since Initial (NPT re-grid is "
+                  "not built on this path)");
+  }
+  const int n = nl.n;
+  if (nl.generation == 0) forced = 1;  // nothing built yet
+  nl.generation += 1;
+  // need_update decision (neighbor_list.cpp:983-999)
+  if (forced) {
+    k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 1);
+  } else if (nl.refresh_interval <= 0) {
+    k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 0);
+    float permit = nl.skin * nl.skin_permit;
+    k_check_refresh<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, nl.d_old_crd,
+                                                      nl.cell, nl.rcell,
+                                                      permit * permit, nl.d_flags);
+  } else {
+    k_set_need<<<1, 1, 0, st>>>(nl.d_flags, (step + 1) % nl.refresh_interval == 0);
+  }
+  SNB_CUDA_TRY(cudaMemsetAsync(nl.d_cell_count, 0, sizeof(int) * nl.ncell, st));
+  k_bin_count<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz,
+                                                nl.d_atom_cell, nl.d_atom_slot,
+                                                nl.d_cell_count, nl.d_flags);
+  int rc = scan_exclusive(nl.d_cell_count, nl.d_cell_start, nl.ncell, nullptr,
+                          nl.scan, st);
+  if (rc) return rc;
+  k_bin_scatter<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_atom_cell, nl.d_atom_slot,
+                                                  nl.d_cell_start, nl.d_unsorted,
+                                                  nl.d_flags);
+  k_cell_order<<<ceil_div(nl.ncell, 8), 256, 0, st>>>(nl.ncell, nl.d_cell_start,
+                                                      nl.d_unsorted, nl.d_perm,
+                                                      nl.d_flags);
+  k_fill_sorted<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_perm, crd, atom_local,
+                                                  nl.d_inv_perm, nl.d_global,
+                                                  nl.d_pos, nl.d_old_crd, nl.d_flags);
+  k_sorted_cell<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_perm, nl.d_atom_cell,
+                                                  nl.d_sorted_cell, nl.d_flags);
+  k_pair_search<0><<<ceil_div(n, 8), 256, 0, st>>>(
+      n, nl.d_pos, nl.d_global, nl.d_sorted_cell, nl.d_cell_start, nl.d_run_ranges,
+      nl.d_run_count, nl.max_runs, nl.cell, nl.rcell, nl.rl2, excl_start, excl_list,
+      excl_numbers, nl.d_row_count, nl.d_row_start, nl.d_cols, nl.cap, nl.d_flags);
+  rc = scan_exclusive(nl.d_row_count, nl.d_row_start, n, nl.d_flags + kFlagTotal,
+                      nl.scan, st);
+  if (rc) return rc;
+  k_pair_search<1><<<ceil_div(n, 8), 256, 0, st>>>(
+      n, nl.d_pos, nl.d_global, nl.d_sorted_cell, nl.d_cell_start, nl.d_run_ranges,
+      nl.d_run_count, nl.max_runs, nl.cell, nl.rcell, nl.rl2, excl_start, excl_list,
+      excl_numbers, nl.d_row_count, nl.d_row_start, nl.d_cols, nl.cap, nl.d_flags);
+  k_finish_build<<<1, 1, 0, st>>>(nl.d_flags);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+int nl_check_overflow(NeighborList& nl, bool* regrown, cudaStream_t st) {
+  *regrown = false;
+  SNB_CUDA_TRY(cudaMemcpyAsync(nl.h_flags, nl.d_flags, sizeof(int) * kNumFlags,
+                               cudaMemcpyDeviceToHost, st));
+  SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  nl.last_total = nl.h_flags[kFlagTotal];
+  if (nl.h_flags[kFlagListOverflow]) {
+    long long need = (long long)nl.h_flags[kFlagTotal];
+    long long cap = need + need / 5 + 1024;
+    SNB_CUDA_TRY(cudaFree(nl.d_cols));
+    SNB_CUDA_TRY(cudaMalloc(&nl.d_cols, sizeof(int) * cap));
+    nl.cap = cap;
+    int zero = 0;
+    SNB_CUDA_TRY(cudaMemcpyAsync(nl.d_flags + kFlagListOverflow, &zero, sizeof(int),
+                                 cudaMemcpyHostToDevice, st));
+    SNB_CUDA_TRY(cudaStreamSynchronize(st));
+    *regrown = true;
+  }
+  return kOk;
+}
+
+int nl_total_pairs(NeighborList& nl, long long* total, cudaStream_t st) {
+  bool regrown;
+  int rc = nl_check_overflow(nl, &regrown, st);
+  if (rc) return rc;
+  *total = nl.last_total;
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// Exports.
+struct AtomGroupABI {  // layout of the reference's ATOM_GROUP (common.h:177-182)
+  int atom_numbers;
+  int ghost_numbers;
+  int* atom_serial;
+};
+
+// pairs in global ids (lo, hi), in sorted-frame list order
+__global__ void k_export_pairs(int n, const int* __restrict__ row_start,
+                               const int* __restrict__ cols,
+                               const int* __restrict__ global, int* pi, int* pj,
+                               long long cap) {
+  int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  int gi = global[i];
+  for (int k = row_start[i] + lane; k < row_start[i + 1]; k += 32) {
+    if (k >= cap) break;
+    int gj = global[cols[k]];
+    pi[k] = gi < gj ? gi : gj;
+    pj[k] = gi < gj ? gj : gi;
+  }
+}
+
+__global__ void k_export_groups_reset(int n, AtomGroupABI* groups, int* slab,
+                                      int maxn, int* counts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  counts[i] = 0;
+  groups[i].ghost_numbers = 0;
+  groups[i].atom_serial = slab + (size_t)i * maxn;
+}
+
+// Reference row semantics: the row of local atom a holds local b with
+// global(b) > global(a).  Local index = caller index here.
+__global__ void k_export_groups_fill(int n, const int* __restrict__ row_start,
+                                     const int* __restrict__ cols,
+                                     const int* __restrict__ global,
+                                     const int* __restrict__ perm, int* slab, int maxn,
+                                     int* counts, int* flags) {
+  int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  if (flags[kFlagListOverflow]) return;
+  int gi = global[i];
+  int li = perm[i];
+  for (int k = row_start[i] + lane; k < row_start[i + 1]; k += 32) {
+    int j = cols[k];
+    int gj = global[j];
+    int lj = perm[j];
+    int owner = gi < gj ? li : lj;
+    int other = gi < gj ? lj : li;
+    int slot = atomicAdd(&counts[owner], 1);
+    if (slot < maxn)
+      slab[(size_t)owner * maxn + slot] = other;
+    else
+      flags[kFlagExportOverflow] = 1;
+  }
+}
+
+__global__ void k_export_groups_counts(int n, AtomGroupABI* groups, const int* counts,
+                                       int maxn) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  groups[i].atom_numbers = counts[i] < maxn ? counts[i] : maxn;
+}
+
+int nl_export_atom_groups(NeighborList& nl, void* d_groups, int* d_slab,
+                          int max_neighbor_numbers, cudaStream_t st) {
+  const int n = nl.n;
+  int* counts = nullptr;
+  SNB_CUDA_TRY(cudaMallocAsync(&counts, sizeof(int) * n, st));
+  AtomGroupABI* g = reinterpret_cast<AtomGroupABI*>(d_groups);
+  k_export_groups_reset<<<ceil_div(n, 256), 256, 0, st>>>(n, g, d_slab,
+                                                          max_neighbor_numbers, counts);
+  k_export_groups_fill<<<ceil_div(n, 8), 256, 0, st>>>(
+      n, nl.d_row_start, nl.d_cols, nl.d_global, nl.d_perm, d_slab,
+      max_neighbor_numbers, counts, nl.d_flags);
+  k_export_groups_counts<<<ceil_div(n, 256), 256, 0, st>>>(n, g, counts,
+                                                           max_neighbor_numbers);
+  SNB_CUDA_TRY(cudaFreeAsync(counts, st));
+  SNB_CUDA_TRY(cudaGetLastError());
+  int flag = 0;
+  SNB_CUDA_TRY(cudaMemcpyAsync(&flag, nl.d_flags + kFlagExportOverflow, sizeof(int),
+                               cudaMemcpyDeviceToHost, st));
+  SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (flag) {
+    int zero = 0;
+    cudaMemcpy(nl.d_flags + kFlagExportOverflow, &zero, sizeof(int),
+               cudaMemcpyHostToDevice);
+    return fail(kOverflow, "neighbor list export: max_neighbor_numbers exceeded");
+  }
+  return kOk;
+}
+
+int nl_export_pairs(NeighborList& nl, int* d_pi, int* d_pj, long long cap,
+                    long long* count, cudaStream_t st) {
+  long long total = 0;
+  int rc = nl_total_pairs(nl, &total, st);
+  if (rc) return rc;
+  *count = total;
+  if (total > cap) return fail(kOverflow, "export_pairs: capacity too small");
+  k_export_pairs<<<ceil_div(nl.n, 8), 256, 0, st>>>(nl.n, nl.d_row_start, nl.d_cols,
+                                                    nl.d_global, d_pi, d_pj, cap);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+}  // namespace snb

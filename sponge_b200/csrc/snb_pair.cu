@@ -1,0 +1,419 @@
+// Direct-space Lennard-Jones + erfc-screened Coulomb over the sorted half list:
+// the Lennard_Jones_And_Direct_Coulomb_Device path
+// (Lennard_Jones_force.cpp:45-137, pair terms Lennard_Jones_force.h:45-75)
+// re-designed for sm_100a.
+//
+// Per listed pair (i, j) with r = |r_j - r_i| (minimum image) below cutoff:
+//   F/r = (B' - A' r^-6) r^-8 - q_i q_j r^-3 (2 beta r/sqrt(pi) e^{-beta^2 r^2}
+//         + erfc(beta r))
+//   f_i += (F/r) dr, f_j -= (F/r) dr
+//   E_LJ = (A'/12 r^-6 - B'/6) r^-6, E_C = q_i q_j erfc(beta r)/r
+//   virial -= (F/r) dr (x) dr   (LTMatrix3 with summed off-diagonals)
+// Energy and virial of a pair go to the atom with the smaller global id, as
+// the reference's half list (global_j > global_i) assigns them.
+//
+// Layout: one warp per sorted atom i, lanes stride its CSR row (coalesced
+// 4-byte index loads, 16-byte float4 {x,y,z,q} gathers that hit L1/L2 since
+// the rows of neighbouring i are spatial neighbours).  The i force stays in
+// registers and is reduced with warp shuffles; j forces go straight to the
+// accumulators: 64-bit fixed point (deterministic, order-independent) or
+// float atomics (the plain path).
+#include <cfloat>
+
+#include "snb_internal.h"
+
+namespace snb {
+
+constexpr float kTwoOverSqrtPi = 1.1283791670955126f;
+
+template <int ACCUM>
+__device__ __forceinline__ void add_force(Accumulators& acc, int s, float fx,
+                                          float fy, float fz) {
+  const int N = acc.n;
+  if (ACCUM == kAccumFixed) {
+    red_add(acc.d_f + s, to_fixed_force(fx));
+    red_add(acc.d_f + N + s, to_fixed_force(fy));
+    red_add(acc.d_f + 2 * N + s, to_fixed_force(fz));
+  } else {
+    atomicAdd(acc.d_ff + s, fx);
+    atomicAdd(acc.d_ff + N + s, fy);
+    atomicAdd(acc.d_ff + 2 * N + s, fz);
+  }
+}
+
+template <int ACCUM>
+__device__ __forceinline__ void add_energy(Accumulators& acc, int s, float e,
+                                           float elj, float ec) {
+  const int N = acc.n;
+  if (ACCUM == kAccumFixed) {
+    red_add(acc.d_e + s, to_fixed_energy(e));
+    red_add(acc.d_elj + s, to_fixed_energy(elj));
+    red_add(acc.d_ec + s, to_fixed_energy(ec));
+  } else {
+    atomicAdd(acc.d_fe + s, e);
+    atomicAdd(acc.d_fe + N + s, elj);
+    atomicAdd(acc.d_fe + 2 * N + s, ec);
+  }
+}
+
+template <int ACCUM>
+__device__ __forceinline__ void add_virial(Accumulators& acc, int s, const float* v) {
+  const int N = acc.n;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    if (ACCUM == kAccumFixed)
+      red_add(acc.d_v + c * N + s, to_fixed_energy(v[c]));
+    else
+      atomicAdd(acc.d_fv + c * N + s, v[c]);
+  }
+}
+
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO>
+__global__ void __launch_bounds__(256)
+k_lj_direct(PairArgs a, Accumulators acc) {
+  extern __shared__ float sh_tab[];
+  float* sA = sh_tab;
+  float* sB = sh_tab + a.n_types * (a.n_types + 1) / 2;
+  const int npair = a.n_types * (a.n_types + 1) / 2;
+  for (int k = threadIdx.x; k < npair; k += blockDim.x) {
+    sA[k] = a.A[k];
+    sB[k] = a.B[k];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= a.n) return;
+  if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
+  const float4 pi = a.pos[i];
+  const float3 ri = make_float3(pi.x, pi.y, pi.z);
+  const int ti = a.type[i];
+  const int gi = ENERGY || VIRIAL ? a.global[i] : 0;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  float e_lj = 0.f, e_c = 0.f;
+  float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  const int k0 = a.row_start[i], k1 = a.row_start[i + 1];
+  for (int k = k0 + lane; k < k1; k += 32) {
+    const int j = a.cols[k];
+    const float4 pj = a.pos[j];
+    const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri,
+                                            a.cell, a.rcell);
+    const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+    if (r2 < a.cutoff2) {
+      const int p = lj_pair_index(ti, a.type[j]);
+      const float A = sA[p], B = sB[p];
+      const float rinv = rsqrtf(r2);
+      const float r = r2 * rinv;
+      const float ir2 = rinv * rinv;
+      const float ir6 = ir2 * ir2 * ir2;
+      const float flj = (B - A * ir6) * ir6 * ir2;
+      const float qq = pi.w * pj.w;
+      const float br = a.beta * r;
+      const float erfc_br = erfcf(br);
+      const float fc = qq * rinv * ir2 * (br * kTwoOverSqrtPi * expf(-br * br) + erfc_br);
+      const float fs = flj - fc;
+      const float gx = fs * dr.x, gy = fs * dr.y, gz = fs * dr.z;
+      fx += gx;
+      fy += gy;
+      fz += gz;
+      add_force<ACCUM>(acc, j, -gx, -gy, -gz);
+      if (ENERGY || VIRIAL) {
+        const bool own_i = gi < a.global[j];
+        if (ENERGY) {
+          const float elj = (0.083333333f * A * ir6 - 0.166666667f * B) * ir6;
+          const float ec = qq * erfc_br * rinv;
+          if (own_i) {
+            e_lj += elj;
+            e_c += ec;
+          } else {
+            add_energy<ACCUM>(acc, j, elj + ec, elj, ec);
+          }
+        }
+        if (VIRIAL) {
+          float v[6];
+          v[0] = -(gx * dr.x);
+          v[1] = -(gx * dr.y + gy * dr.x);
+          v[2] = -(gy * dr.y);
+          v[3] = -(gx * dr.z + gz * dr.x);
+          v[4] = -(gy * dr.z + gz * dr.y);
+          v[5] = -(gz * dr.z);
+          if (own_i) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) vir[c] += v[c];
+          } else {
+            add_virial<ACCUM>(acc, j, v);
+          }
+        }
+      }
+    }
+  }
+  fx = warp_sum(fx);
+  fy = warp_sum(fy);
+  fz = warp_sum(fz);
+  if (ENERGY) {
+    e_lj = warp_sum(e_lj);
+    e_c = warp_sum(e_c);
+  }
+  if (VIRIAL) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) vir[c] = warp_sum(vir[c]);
+  }
+  if (lane == 0) {
+    add_force<ACCUM>(acc, i, fx, fy, fz);
+    if (ENERGY) add_energy<ACCUM>(acc, i, e_lj + e_c, e_lj, e_c);
+    if (VIRIAL) add_virial<ACCUM>(acc, i, vir);
+  }
+}
+
+template <int ACCUM, bool ENERGY, bool VIRIAL>
+static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream_t st) {
+  const int warps = 8;
+  dim3 grid(ceil_div(a.n, warps)), block(32 * warps);
+  size_t smem = sizeof(float) * a.n_types * (a.n_types + 1);
+  if (ortho)
+    k_lj_direct<ACCUM, ENERGY, VIRIAL, true><<<grid, block, smem, st>>>(a, acc);
+  else
+    k_lj_direct<ACCUM, ENERGY, VIRIAL, false><<<grid, block, smem, st>>>(a, acc);
+}
+
+template <int ACCUM>
+static void launch2(const PairArgs& a, Accumulators& acc, bool energy, bool virial,
+                    bool ortho, cudaStream_t st) {
+  if (energy && virial)
+    launch3<ACCUM, true, true>(a, acc, ortho, st);
+  else if (energy)
+    launch3<ACCUM, true, false>(a, acc, ortho, st);
+  else if (virial)
+    launch3<ACCUM, false, true>(a, acc, ortho, st);
+  else
+    launch3<ACCUM, false, false>(a, acc, ortho, st);
+}
+
+int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
+                bool virial, bool ortho, cudaStream_t st) {
+  if (a.n <= 0) return kOk;
+  if (accum == kAccumFixed)
+    launch2<kAccumFixed>(a, acc, energy, virial, ortho, st);
+  else
+    launch2<kAccumFloat>(a, acc, energy, virial, ortho, st);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// Soft-core variant: Lennard_Jones_And_Direct_Coulomb_Soft_Core_CUDA
+// (LJ_soft_core.cpp:196-461; pair terms LJ_soft_core.h:33-149).
+// A pair whose end states both have LJ (A'_A * A'_B != 0), or neither has
+// (A'_A + A'_B == 0), mixes the hard-core forms linearly in lambda; any other
+// pair uses the soft-core radius r_sc = (r^6 + alpha lambda^p sigma^6)^(1/6)
+// for state A and (r^6 + alpha (1-lambda)^p sigma^6)^(1/6) for state B, with
+// sigma^6 = max(A'/(2B'), sigma_min^6), or the input sigma^6 when A' or B' is 0.
+__device__ __forceinline__ float lj_e(float A, float B, float ir6) {
+  return (0.083333333f * A * ir6 - 0.166666667f * B) * ir6;
+}
+__device__ __forceinline__ float sc_sigma(float A, float B, float s6, float s6min) {
+  return (A == 0.f || B == 0.f) ? s6 : fmaxf(0.5f * A / B, s6min);
+}
+// dU/dlambda chain term (Get_Soft_Core_dU_dlambda, LJ_soft_core.h:142-149)
+__device__ __forceinline__ float sc_dudl(float F, float sigma, float rsc, float alpha,
+                                         float p, float lambda) {
+  float rsc2 = rsc * rsc;
+  return 0.16666667f * p * alpha * (1.0f - lambda) * powf(lambda + FLT_MIN, p - 1.0f) *
+         F / (rsc2 * rsc2) * sigma;
+}
+__device__ __forceinline__ float coul_e(float qq, float beta, float r) {
+  return qq * erfcf(beta * r) / r;
+}
+__device__ __forceinline__ float coul_f(float qq, float beta, float r) {
+  float br = beta * r;
+  return qq / (r * r * r) * (br * kTwoOverSqrtPi * expf(-br * br) + erfcf(br));
+}
+
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool DUDL>
+__global__ void __launch_bounds__(256)
+k_lj_soft(SoftArgs a, Accumulators acc, long long* dudl_total) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= a.n) return;
+  if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
+  const float lam = a.lambda, lam_ = 1.0f - a.lambda;
+  const float alp_A = a.alpha * powf(lam, a.p);
+  const float alp_B = a.alpha * powf(lam_, a.p);
+  const float4 pi = a.pos[i];
+  const float3 ri = make_float3(pi.x, pi.y, pi.z);
+  const int2 pri = a.par[i];
+  const int tAi = pri.x & 0xffff, tBi = pri.x >> 16;
+  const float dqi = DUDL && a.dq ? a.dq[i] : 0.f;
+  const int gi = ENERGY || VIRIAL ? a.global[i] : 0;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  float e_lj = 0.f, e_c = 0.f, e_inter = 0.f, e_intra = 0.f;
+  float du_lj = 0.f, du_c = 0.f;
+  float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  const int k0 = a.row_start[i], k1 = a.row_start[i + 1];
+  for (int k = k0 + lane; k < k1; k += 32) {
+    const int j = a.cols[k];
+    const float4 pj = a.pos[j];
+    const float3 dr = min_image_fast<false>(make_float3(pj.x, pj.y, pj.z), ri, a.cell,
+                                            a.rcell);
+    const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+    if (!(r2 < a.cutoff2)) continue;
+    const int2 prj = a.par[j];
+    const int tAj = prj.x & 0xffff, tBj = prj.x >> 16;
+    const int pA = lj_pair_index(tAi, tAj), pB = lj_pair_index(tBi, tBj);
+    const float AA = a.AA[pA], AB = a.AB[pA], BA = a.BA[pB], BB = a.BB[pB];
+    const float r = sqrtf(r2);
+    const float qq = pi.w * pj.w;
+    float fs, elj, ec, dl = 0.f, dc = 0.f;
+    if (BA * AA != 0.f || BA + AA == 0.f) {
+      const float ir2 = 1.0f / r2, ir6 = ir2 * ir2 * ir2;
+      fs = lam_ * (AB - AA * ir6) * ir6 * ir2 + lam * (BB - BA * ir6) * ir6 * ir2 -
+           coul_f(qq, a.beta, r);
+      elj = lam_ * lj_e(AA, AB, ir6) + lam * lj_e(BA, BB, ir6);
+      ec = coul_e(qq, a.beta, r);
+      if (DUDL) {
+        dl = lj_e(BA, BB, ir6) - lj_e(AA, AB, ir6);
+        const float dqj = a.dq ? a.dq[j] : 0.f;
+        dc = erfcf(a.beta * r) * (dqj * pi.w + pj.w * dqi) / r;
+      }
+    } else {
+      const float sA = sc_sigma(AA, AB, a.sigma6, a.sigma6_min);
+      const float sB = sc_sigma(BA, BB, a.sigma6, a.sigma6_min);
+      const float r6 = r2 * r2 * r2;
+      const float rA = powf(r6 + alp_A * sA, 0.16666667f);
+      const float rB = powf(r6 + alp_B * sB, 0.16666667f);
+      const float r4 = r2 * r2;
+      const float iA2 = 1.0f / (rA * rA), iA6 = iA2 * iA2 * iA2;
+      const float iB2 = 1.0f / (rB * rB), iB6 = iB2 * iB2 * iB2;
+      const float flA = r4 * (AB - AA * iA6) * iA6 * iA6;
+      const float flB = r4 * (BB - BA * iB6) * iB6 * iB6;
+      const float bA = a.beta * rA, bB = a.beta * rB;
+      const float fcA = qq * r4 *
+                        (expf(-bA * bA) * kTwoOverSqrtPi * a.beta + erfcf(bA) / rA) * iA6;
+      const float fcB = qq * r4 *
+                        (expf(-bB * bB) * kTwoOverSqrtPi * a.beta + erfcf(bB) / rB) * iB6;
+      fs = lam_ * flA + lam * flB - (lam_ * fcA + lam * fcB);
+      ec = lam_ * coul_e(qq, a.beta, rA) + lam * coul_e(qq, a.beta, rB);
+      elj = lam_ * lj_e(AA, AB, iA6) + lam * lj_e(BA, BB, iB6);
+      if (DUDL) {
+        dl = lj_e(BA, BB, iB6) - lj_e(AA, AB, iA6);
+        dl += sc_dudl((AB - AA * iA6) * iA6 * iA2, sA, rA, a.alpha, a.p, lam) -
+              sc_dudl((BB - BA * iB6) * iB6 * iB2, sB, rB, a.alpha, a.p, lam_);
+        const float dqj = a.dq ? a.dq[j] : 0.f;
+        const float qd = dqj * pi.w + pj.w * dqi;
+        dc = coul_e(qq, a.beta, rB) - coul_e(qq, a.beta, rA);
+        dc += sc_dudl(coul_f(qq, a.beta, rB), sB, rB, a.alpha, a.p, lam_) -
+              sc_dudl(coul_f(qq, a.beta, rA), sA, rA, a.alpha, a.p, lam);
+        dc += lam * erfcf(a.beta * rB) * qd / rB + lam_ * erfcf(a.beta * rA) * qd / rA;
+      }
+    }
+    const float gx = fs * dr.x, gy = fs * dr.y, gz = fs * dr.z;
+    if (!DUDL) {
+      fx += gx;
+      fy += gy;
+      fz += gz;
+      add_force<ACCUM>(acc, j, -gx, -gy, -gz);
+    }
+    if (DUDL) {
+      du_lj += dl;
+      du_c += dc;
+    }
+    if (ENERGY || VIRIAL) {
+      const bool own_i = gi < a.global[j];
+      const bool intra = pri.y == prj.y;
+      if (ENERGY) {
+        if (own_i) {
+          e_lj += elj;
+          e_c += ec;
+          if (intra) e_intra += elj; else e_inter += elj;
+        } else {
+          add_energy<ACCUM>(acc, j, elj + ec, elj, ec);
+          const int N = acc.n;
+          if (ACCUM == kAccumFixed)
+            red_add(acc.d_eaux + (intra ? N : 0) + j, to_fixed_energy(elj));
+          else
+            atomicAdd(acc.d_feaux + (intra ? N : 0) + j, elj);
+        }
+      }
+      if (VIRIAL) {
+        float v[6];
+        v[0] = -(gx * dr.x);
+        v[1] = -(gx * dr.y + gy * dr.x);
+        v[2] = -(gy * dr.y);
+        v[3] = -(gx * dr.z + gz * dr.x);
+        v[4] = -(gy * dr.z + gz * dr.y);
+        v[5] = -(gz * dr.z);
+        if (own_i) {
+#pragma unroll
+          for (int c = 0; c < 6; ++c) vir[c] += v[c];
+        } else {
+          add_virial<ACCUM>(acc, j, v);
+        }
+      }
+    }
+  }
+  if (DUDL) {
+    du_lj = warp_sum(du_lj);
+    du_c = warp_sum(du_c);
+    if (lane == 0) {
+      red_add(dudl_total, to_fixed_energy(du_lj));
+      red_add(dudl_total + 1, to_fixed_energy(du_c));
+    }
+    return;
+  }
+  fx = warp_sum(fx);
+  fy = warp_sum(fy);
+  fz = warp_sum(fz);
+  if (ENERGY) {
+    e_lj = warp_sum(e_lj);
+    e_c = warp_sum(e_c);
+    e_inter = warp_sum(e_inter);
+    e_intra = warp_sum(e_intra);
+  }
+  if (VIRIAL) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) vir[c] = warp_sum(vir[c]);
+  }
+  if (lane == 0) {
+    add_force<ACCUM>(acc, i, fx, fy, fz);
+    if (ENERGY) {
+      add_energy<ACCUM>(acc, i, e_lj + e_c, e_lj, e_c);
+      const int N = acc.n;
+      if (ACCUM == kAccumFixed) {
+        red_add(acc.d_eaux + i, to_fixed_energy(e_inter));
+        red_add(acc.d_eaux + N + i, to_fixed_energy(e_intra));
+      } else {
+        atomicAdd(acc.d_feaux + i, e_inter);
+        atomicAdd(acc.d_feaux + N + i, e_intra);
+      }
+    }
+    if (VIRIAL) add_virial<ACCUM>(acc, i, vir);
+  }
+}
+
+template <int ACCUM>
+static void launch_soft2(const SoftArgs& a, Accumulators& acc, bool energy, bool virial,
+                         bool dudl, long long* dt, cudaStream_t st) {
+  dim3 grid(ceil_div(a.n, 8)), block(256);
+  if (dudl)
+    k_lj_soft<ACCUM, false, false, true><<<grid, block, 0, st>>>(a, acc, dt);
+  else if (energy && virial)
+    k_lj_soft<ACCUM, true, true, false><<<grid, block, 0, st>>>(a, acc, dt);
+  else if (energy)
+    k_lj_soft<ACCUM, true, false, false><<<grid, block, 0, st>>>(a, acc, dt);
+  else if (virial)
+    k_lj_soft<ACCUM, false, true, false><<<grid, block, 0, st>>>(a, acc, dt);
+  else
+    k_lj_soft<ACCUM, false, false, false><<<grid, block, 0, st>>>(a, acc, dt);
+}
+
+int launch_soft(const SoftArgs& a, Accumulators& acc, int accum, bool energy,
+                bool virial, bool dudl, long long* dudl_total, cudaStream_t st) {
+  if (a.n <= 0) return kOk;
+  if (accum == kAccumFixed)
+    launch_soft2<kAccumFixed>(a, acc, energy, virial, dudl, dudl_total, st);
+  else
+    launch_soft2<kAccumFloat>(a, acc, energy, virial, dudl, dudl_total, st);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+}  // namespace snb

@@ -1,0 +1,743 @@
+// Smooth PME reciprocal part (Particle_Mesh, PM_force.cpp) and the
+// excluded-pair correction, re-designed for sm_100a.
+//
+// Method (unchanged from the reference): order-4 cardinal B-spline spreading
+// of charges to a K0 x K1 x K2 grid from the fractional coordinates
+// (PME_Atom_Near :699-762, weights PME_Ma..PME_Md :20-23), R2C FFT, multiply
+// by BC(m) = |b(m)|^2 exp(-pi^2 m^2/beta^2)/(pi m^2 V) (tables :541-612),
+// C2R, then force F = -q sum_g phi(g) grad W(g) (PME_Final :829-893).
+// Energy E = 1/2 sum_m BC(m)|FQ(m)|^2 (equal to 1/2 sum_g Q phi, :896-919,
+// :1142-1147) and the virial over the half spectrum with the reference's
+// weights (PME_Sum_Virial :1024-1068), both reduced in FP64.
+//
+// What changes is how the grid is written.  Atoms are counting-sorted by the
+// 8x8x8 grid tile of their base point every step; one CTA owns one tile and
+// pulls the contributions of the atoms binned in the (at most 3 per axis)
+// tiles whose stencils reach it, accumulating in shared memory in int32 fixed
+// point (2^22 per charge unit).  The tile is then stored once: no global
+// atomics, and the grid is the same bit pattern for any atom order.
+#include <algorithm>
+#include <cmath>
+#include <set>
+#include <vector>
+
+#include "snb_internal.h"
+
+namespace snb {
+
+// ---------------------------------------------------------------------------
+// Host helpers.
+int fft_size(float length) {  // Get_Fft_Patameter (common.cpp:639-659)
+  int t = ((int)ceil(length + 3)) >> 2 << 2;
+  if (t >= 60 && t <= 68)
+    t = 64;
+  else if (t >= 120 && t <= 136)
+    t = 128;
+  else if (t >= 240 && t <= 272)
+    t = 256;
+  else if (t >= 480 && t <= 544)
+    t = 512;
+  else if (t >= 960 && t <= 1088)
+    t = 1024;
+  for (;;) {
+    int m = t;
+    for (int p : {2, 3, 5, 7})
+      while (m > 1 && m % p == 0) m /= p;
+    if (m == 1) return t;
+    t += 4;
+  }
+}
+
+// Ewald beta by bisection on erfc(beta*rc)/rc = tolerance with the
+// reference's float iteration (Get_Beta, PM_force.cpp:246-274).
+float get_beta(float cutoff, float tolerance) {
+  float beta = 0.f, low, high = 1.0f, tempf;
+  int ilow, ihigh = 1;
+  for (;;) {
+    tempf = erfcf(high * cutoff) / cutoff;
+    if (tempf <= tolerance) break;
+    high *= 2;
+    ihigh++;
+  }
+  ihigh += 50;
+  low = 0.0f;
+  for (ilow = 1; ilow < ihigh; ilow++) {
+    beta = (low + high) / 2;
+    tempf = erfcf(beta * cutoff) / cutoff;
+    if (tempf >= tolerance)
+      low = beta;
+    else
+      high = beta;
+  }
+  return beta;
+}
+
+// |b(k)|^2 of the order-4 Euler exponential spline (getb, PM_force.cpp:40-64),
+// evaluated in double: 1/|sum_{j=0..2} M4(j+1) e^{2 pi i k j/K}|^2.
+static double bspline_mod2(int k, int K) {
+  const double two_pi = 6.283185307179586476925286766559;
+  const double m4[3] = {1.0 / 6.0, 4.0 / 6.0, 1.0 / 6.0};
+  double re = 0, im = 0;
+  for (int j = 0; j < 3; ++j) {
+    double ang = two_pi * k * j / K;
+    re += m4[j] * cos(ang);
+    im += m4[j] * sin(ang);
+  }
+  return 1.0 / (re * re + im * im);
+}
+
+// ---------------------------------------------------------------------------
+// Per-step binning by grid tile.
+struct TileGeom {
+  int K0, K1, K2;
+  int T;
+  int nt0, nt1, nt2;
+  Cell rcell;
+};
+
+// Fractional coordinate, base point u and fraction as PME_Atom_Near
+// (PM_force.cpp:707-733).
+__device__ __forceinline__ void pme_base(float3 r, const Cell& rc, int K0, int K1,
+                                         int K2, int& ux, int& uy, int& uz,
+                                         float& fx, float& fy, float& fz) {
+  float sx = r.x * rc.a11 + r.y * rc.a21 + r.z * rc.a31;
+  float sy = r.y * rc.a22 + r.z * rc.a32;
+  float sz = r.z * rc.a33;
+  sx -= floorf(sx);
+  sy -= floorf(sy);
+  sz -= floorf(sz);
+  if (!isfinite(sx) || !isfinite(sy) || !isfinite(sz)) sx = sy = sz = 0.f;
+  sx *= K0;
+  sy *= K1;
+  sz *= K2;
+  ux = (int)sx;
+  uy = (int)sy;
+  uz = (int)sz;
+  ux = ux < 0 ? 0 : (ux < K0 ? ux : K0 - 1);
+  uy = uy < 0 ? 0 : (uy < K1 ? uy : K1 - 1);
+  uz = uz < 0 ? 0 : (uz < K2 ? uz : K2 - 1);
+  fx = sx - ux;
+  fx -= floorf(fx);
+  fy = sy - uy;
+  fy -= floorf(fy);
+  fz = sz - uz;
+  fz -= floorf(fz);
+}
+
+__device__ __forceinline__ int pack_u(int ux, int uy, int uz) {
+  return (ux << 20) | (uy << 10) | uz;
+}
+
+__global__ void k_pme_bin(int n, const float4* __restrict__ pos, TileGeom g,
+                          int* __restrict__ atom_tile, int* __restrict__ atom_slot,
+                          int* __restrict__ tile_count, float4* __restrict__ frq,
+                          int* __restrict__ upk) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = pos[i];
+  int ux, uy, uz;
+  float fx, fy, fz;
+  pme_base(make_float3(p.x, p.y, p.z), g.rcell, g.K0, g.K1, g.K2, ux, uy, uz, fx,
+           fy, fz);
+  int t = ((ux / g.T) * g.nt1 + (uy / g.T)) * g.nt2 + (uz / g.T);
+  atom_tile[i] = t;
+  atom_slot[i] = atomicAdd(&tile_count[t], 1);
+  frq[i] = make_float4(fx, fy, fz, p.w);
+  upk[i] = pack_u(ux, uy, uz);
+}
+
+__global__ void k_pme_scatter(int n, const int* __restrict__ atom_tile,
+                              const int* __restrict__ atom_slot,
+                              const int* __restrict__ tile_start,
+                              const float4* __restrict__ frq,
+                              const int* __restrict__ upk, float4* __restrict__ binned,
+                              int* __restrict__ binned_u) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int d = tile_start[atom_tile[i]] + atom_slot[i];
+  binned[d] = frq[i];
+  binned_u[d] = upk[i];
+}
+
+// B-spline weights of the points u, u-1, u-2, u-3 (power form of
+// PME_Ma..PME_Md) and their derivatives (PME_dMa..PME_dMc).
+__device__ __forceinline__ void bspline4(float x, float* w) {
+  float x2 = x * x, x3 = x2 * x;
+  w[0] = 0.16666667f * x3;
+  w[1] = -0.5f * x3 + 0.5f * x2 + 0.5f * x + 0.16666667f;
+  w[2] = 0.5f * x3 - x2 + 0.66666667f;
+  w[3] = -0.16666667f * x3 + 0.5f * x2 - 0.5f * x + 0.16666667f;
+}
+__device__ __forceinline__ void dbspline4(float x, float* d) {
+  float x2 = x * x;
+  d[0] = 0.5f * x2;
+  d[1] = -1.5f * x2 + x + 0.5f;
+  d[2] = 1.5f * x2 - 2.0f * x;
+  d[3] = 0.5f * x2 - x + 0.5f;
+}
+
+// Bitmask of stencil offsets o in {0..3} with (u - o) mod K in [lo, hi).
+__device__ __forceinline__ int stencil_mask(int u, int K, int lo, int hi) {
+  int m = 0;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    int p = u - o;
+    p += p < 0 ? K : 0;
+    m |= (p >= lo && p < hi) ? (1 << o) : 0;
+  }
+  return m;
+}
+
+constexpr int kTile = 8;
+constexpr int kTile3 = kTile * kTile * kTile;
+
+// One CTA per tile.  src_bins[d][t] = {count, b0, b1, b2} lists the bins along
+// axis d whose atoms reach tile t.
+__global__ void __launch_bounds__(256)
+k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
+             const float4* __restrict__ binned, const int* __restrict__ binned_u,
+             const int4* __restrict__ src0, const int4* __restrict__ src1,
+             const int4* __restrict__ src2, float* __restrict__ Q) {
+  __shared__ int sq[kTile3];
+  const int t = blockIdx.x;
+  const int t2 = t % g.nt2, t1 = (t / g.nt2) % g.nt1, t0 = t / (g.nt1 * g.nt2);
+  const int lo0 = t0 * g.T, hi0 = min(lo0 + g.T, g.K0);
+  const int lo1 = t1 * g.T, hi1 = min(lo1 + g.T, g.K1);
+  const int lo2 = t2 * g.T, hi2 = min(lo2 + g.T, g.K2);
+  for (int k = threadIdx.x; k < kTile3; k += blockDim.x) sq[k] = 0;
+  __syncthreads();
+  const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
+  const int b0[3] = {s0.y, s0.z, s0.w};
+  const int b1[3] = {s1.y, s1.z, s1.w};
+  const int b2[3] = {s2.y, s2.z, s2.w};
+  for (int a = 0; a < s0.x; ++a)
+    for (int b = 0; b < s1.x; ++b)
+      for (int c = 0; c < s2.x; ++c) {
+        int bin = (b0[a] * g.nt1 + b1[b]) * g.nt2 + b2[c];
+        int beg = tile_start[bin], end = tile_start[bin + 1];
+        for (int k = beg + threadIdx.x; k < end; k += blockDim.x) {
+          float4 f = binned[k];
+          int up = binned_u[k];
+          int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
+          int mx = stencil_mask(ux, g.K0, lo0, hi0);
+          int my = stencil_mask(uy, g.K1, lo1, hi1);
+          int mz = stencil_mask(uz, g.K2, lo2, hi2);
+          if (!mx || !my || !mz) continue;
+          float wx[4], wy[4], wz[4];
+          bspline4(f.x, wx);
+          bspline4(f.y, wy);
+          bspline4(f.z, wz);
+#pragma unroll
+          for (int ox = 0; ox < 4; ++ox) {
+            if (!(mx >> ox & 1)) continue;
+            int px = ux - ox;
+            px += px < 0 ? g.K0 : 0;
+            float qx = f.w * wx[ox];
+#pragma unroll
+            for (int oy = 0; oy < 4; ++oy) {
+              if (!(my >> oy & 1)) continue;
+              int py = uy - oy;
+              py += py < 0 ? g.K1 : 0;
+              float qxy = qx * wy[oy];
+#pragma unroll
+              for (int oz = 0; oz < 4; ++oz) {
+                if (!(mz >> oz & 1)) continue;
+                int pz = uz - oz;
+                pz += pz < 0 ? g.K2 : 0;
+                int loc = ((px - lo0) * kTile + (py - lo1)) * kTile + (pz - lo2);
+                atomicAdd(&sq[loc], __float2int_rn(qxy * wz[oz] * kGridScale));
+              }
+            }
+          }
+        }
+      }
+  __syncthreads();
+  const int w0 = hi0 - lo0, w1 = hi1 - lo1, w2 = hi2 - lo2;
+  for (int k = threadIdx.x; k < kTile3; k += blockDim.x) {
+    int x = k / (kTile * kTile), y = (k / kTile) % kTile, z = k % kTile;
+    if (x < w0 && y < w1 && z < w2)
+      Q[((size_t)(lo0 + x) * g.K1 + (lo1 + y)) * g.K2 + (lo2 + z)] =
+          (float)sq[k] * kGridScaleInv;
+  }
+}
+
+// Plain path: the reference's scheme, 64 global float atomics per atom.
+__global__ void k_pme_spread_atomic(int n, const float4* __restrict__ frq,
+                                    const int* __restrict__ upk, TileGeom g,
+                                    float* __restrict__ Q) {
+  int i = blockIdx.x * (blockDim.x >> 4) + (threadIdx.x >> 4);
+  int l = threadIdx.x & 15;
+  if (i >= n) return;
+  float4 f = frq[i];
+  int up = upk[i];
+  int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
+  float wx[4], wy[4], wz[4];
+  bspline4(f.x, wx);
+  bspline4(f.y, wy);
+  bspline4(f.z, wz);
+  int ox = l >> 2, oy = l & 3;
+  int px = ux - ox;
+  px += px < 0 ? g.K0 : 0;
+  int py = uy - oy;
+  py += py < 0 ? g.K1 : 0;
+  float qxy = f.w * wx[ox] * wy[oy];
+#pragma unroll
+  for (int oz = 0; oz < 4; ++oz) {
+    int pz = uz - oz;
+    pz += pz < 0 ? g.K2 : 0;
+    atomicAdd(&Q[((size_t)px * g.K1 + py) * g.K2 + pz], qxy * wz[oz]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Influence function, energy and virial over the half spectrum.
+struct SpecGeom {
+  int K0, K1, K2, nc;
+  Cell rcell;
+  float mpre;       // pi^2/beta^2
+  float inv_pi_v;   // 1/(pi V)
+};
+
+constexpr int kSpecBlock = 256;
+
+template <bool VIRIAL>
+__global__ void __launch_bounds__(kSpecBlock)
+k_pme_influence(int nfft, SpecGeom g, const float* __restrict__ B0,
+                const float* __restrict__ B1, const float* __restrict__ B2,
+                cufftComplex* __restrict__ FQ, double* __restrict__ partial,
+                bool energy) {
+  double e = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nfft;
+       idx += gridDim.x * blockDim.x) {
+    int kz = idx % g.nc;
+    int ky = (idx / g.nc) % g.K1;
+    int kx = idx / (g.nc * g.K1);
+    float kxr = kx > g.K0 / 2 ? kx - g.K0 : kx;
+    float kyr = ky > g.K1 / 2 ? ky - g.K1 : ky;
+    float kzr = kz;
+    float mx = kxr * g.rcell.a11;
+    float my = kxr * g.rcell.a21 + kyr * g.rcell.a22;
+    float mz = kxr * g.rcell.a31 + kyr * g.rcell.a32 + kzr * g.rcell.a33;
+    float msq = mx * mx + my * my + mz * mz;
+    float bc = 0.f;
+    if (idx != 0) bc = g.inv_pi_v / msq * expf(-g.mpre * msq) * B0[kx] * B1[ky] * B2[kz];
+    cufftComplex c = FQ[idx];
+    float f2 = c.x * c.x + c.y * c.y;
+    if (energy) {
+      float we = (kz == 0 || (2 * kz == g.K2)) ? 0.5f : 1.0f;
+      e += (double)(we * bc * f2);
+    }
+    if (VIRIAL && idx != 0) {
+      float factor = (kz == 0 || kz == g.nc - 1) ? 0.5f : 1.0f;
+      float s = factor * f2 * 0.5f * bc;
+      float cc = 2.0f / msq * (1.0f + g.mpre * msq);
+      v[0] -= (double)(s * (1.0f - cc * mx * mx));
+      v[1] -= (double)(s * (0.0f - cc * my * mx));
+      v[2] -= (double)(s * (1.0f - cc * my * my));
+      v[3] -= (double)(s * (0.0f - cc * mz * mx));
+      v[4] -= (double)(s * (0.0f - cc * mz * my));
+      v[5] -= (double)(s * (1.0f - cc * mz * mz));
+    }
+    c.x *= bc;
+    c.y *= bc;
+    FQ[idx] = c;
+  }
+  // block reduction in FP64, fixed order
+  __shared__ double sh[kSpecBlock / 32][7];
+  double vals[7] = {e, v[0], v[1], v[2], v[3], v[4], v[5]};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    double x = warp_sum(vals[c]);
+    if (lane == 0) sh[warp][c] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double s = 0.0;
+    for (int w = 0; w < kSpecBlock / 32; ++w) s += sh[w][threadIdx.x];
+    partial[(size_t)blockIdx.x * 8 + threadIdx.x] = s;
+  }
+}
+
+// Final FP64 sums of the block partials plus the self / neutralising energy:
+// E_self = -beta/sqrt(pi) sum q^2 - pi/(2 beta^2 V) (sum q)^2
+// (PM_force.cpp:1149-1162).
+__global__ void k_pme_finish(int nblocks, const double* __restrict__ partial,
+                             const float4* __restrict__ pos, int n, double beta,
+                             double volume, double* __restrict__ sums, bool energy) {
+  __shared__ double sh[32][3];
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (threadIdx.x < 7)
+    for (int b = 0; b < nblocks; ++b) acc[0] += partial[(size_t)b * 8 + threadIdx.x];
+  double q2 = 0.0, qs = 0.0;
+  if (energy)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      double q = pos[i].w;
+      q2 += q * q;
+      qs += q;
+    }
+  q2 = warp_sum(q2);
+  qs = warp_sum(qs);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[warp][0] = q2;
+    sh[warp][1] = qs;
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) sums[threadIdx.x] = acc[0];
+  if (threadIdx.x == 0 && energy) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += sh[w][0];
+      b += sh[w][1];
+    }
+    const double pi = 3.141592653589793238462643383;
+    sums[7] = -beta / sqrt(pi) * a - 0.5 * pi / (beta * beta * volume) * b * b;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gather: four lanes per atom, lane o handles the 16 points of x offset o.
+template <int ACCUM>
+__global__ void k_pme_gather(int n, const float4* __restrict__ frq,
+                             const int* __restrict__ upk, TileGeom g,
+                             const float* __restrict__ phi, float scale,
+                             Accumulators acc) {
+  int i = blockIdx.x * (blockDim.x >> 2) + (threadIdx.x >> 2);
+  int ox = threadIdx.x & 3;
+  bool active = i < n;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  if (active) {
+    float4 f = frq[i];
+    int up = upk[i];
+    int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
+    float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+    bspline4(f.x, wx);
+    bspline4(f.y, wy);
+    bspline4(f.z, wz);
+    dbspline4(f.x, dx);
+    dbspline4(f.y, dy);
+    dbspline4(f.z, dz);
+    int px = ux - ox;
+    px += px < 0 ? g.K0 : 0;
+    float gxs = 0.f, gys = 0.f, gzs = 0.f;
+#pragma unroll
+    for (int oy = 0; oy < 4; ++oy) {
+      int py = uy - oy;
+      py += py < 0 ? g.K1 : 0;
+      const float* row = phi + ((size_t)px * g.K1 + py) * g.K2;
+#pragma unroll
+      for (int oz = 0; oz < 4; ++oz) {
+        int pz = uz - oz;
+        pz += pz < 0 ? g.K2 : 0;
+        float p = row[pz];
+        gxs += p * dx[ox] * wy[oy] * wz[oz];
+        gys += p * wx[ox] * dy[oy] * wz[oz];
+        gzs += p * wx[ox] * wy[oy] * dz[oz];
+      }
+    }
+    // -q * grad, grad = (dW/du * K) transformed by rcell (MultiplyTranspose)
+    float q = -f.w * scale;
+    float t0 = gxs * g.K0, t1 = gys * g.K1, t2 = gzs * g.K2;
+    ax = q * (t0 * g.rcell.a11);
+    ay = q * (t0 * g.rcell.a21 + t1 * g.rcell.a22);
+    az = q * (t0 * g.rcell.a31 + t1 * g.rcell.a32 + t2 * g.rcell.a33);
+  }
+  ax += __shfl_xor_sync(0xffffffffu, ax, 1);
+  ay += __shfl_xor_sync(0xffffffffu, ay, 1);
+  az += __shfl_xor_sync(0xffffffffu, az, 1);
+  ax += __shfl_xor_sync(0xffffffffu, ax, 2);
+  ay += __shfl_xor_sync(0xffffffffu, ay, 2);
+  az += __shfl_xor_sync(0xffffffffu, az, 2);
+  if (active && ox == 0) {
+    const int N = acc.n;
+    if (ACCUM == kAccumFixed) {
+      red_add(acc.d_f + i, to_fixed_force(ax));
+      red_add(acc.d_f + N + i, to_fixed_force(ay));
+      red_add(acc.d_f + 2 * N + i, to_fixed_force(az));
+    } else {
+      atomicAdd(acc.d_ff + i, ax);
+      atomicAdd(acc.d_ff + N + i, ay);
+      atomicAdd(acc.d_ff + 2 * N + i, az);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
+             float cutoff, float tolerance, int fftx, int ffty, int fftz,
+             float grid_spacing, int update_interval, bool reciprocal,
+             bool excluded) {
+  if (n <= 0) return fail(kBadInput, "PME: atom_numbers must be > 0");
+  p.n = n;
+  p.cutoff = cutoff;
+  p.tolerance = tolerance;
+  p.update_interval = update_interval > 0 ? update_interval : 1;
+  p.reciprocal = reciprocal;
+  p.excluded = excluded;
+  p.cell = make_cell(cell6);
+  if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f)
+    return fail(kNotSupported, "PME: only rectangular boxes are supported");
+  Cell rc{};
+  rc.a11 = 1.0f / p.cell.a11;
+  rc.a22 = 1.0f / p.cell.a22;
+  rc.a33 = 1.0f / p.cell.a33;
+  p.rcell = rc;
+  p.volume = (double)p.cell.a11 * p.cell.a22 * p.cell.a33;
+  if (grid_spacing <= 0.f) grid_spacing = 1.0f;
+  p.K[0] = fftx > 0 ? fftx : fft_size(box_length3[0] / grid_spacing);
+  p.K[1] = ffty > 0 ? ffty : fft_size(box_length3[1] / grid_spacing);
+  p.K[2] = fftz > 0 ? fftz : fft_size(box_length3[2] / grid_spacing);
+  for (int d = 0; d < 3; ++d)
+    if (p.K[d] < 4 || p.K[d] > 1023)
+      return fail(kBadInput, "PME: grid dimension must be in [4, 1023]");
+  p.nall = p.K[0] * p.K[1] * p.K[2];
+  p.nfft = p.K[0] * p.K[1] * (p.K[2] / 2 + 1);
+  p.beta = get_beta(cutoff, tolerance);
+  p.T = kTile;
+  for (int d = 0; d < 3; ++d) p.nt[d] = ceil_div(p.K[d], p.T);
+  p.ntiles = p.nt[0] * p.nt[1] * p.nt[2];
+  for (int d = 0; d < 3; ++d) {
+    std::vector<float> b(p.K[d]);
+    for (int k = 0; k < p.K[d]; ++k) b[k] = (float)bspline_mod2(k, p.K[d]);
+    SNB_CUDA_TRY(cudaMalloc(&p.d_B[d], sizeof(float) * p.K[d]));
+    SNB_CUDA_TRY(cudaMemcpy(p.d_B[d], b.data(), sizeof(float) * p.K[d],
+                            cudaMemcpyHostToDevice));
+    // source bins per tile along this axis: bins holding a base point u with
+    // some stencil point (u - o) mod K, o in 0..3, inside the tile
+    std::vector<int4> src(p.nt[d]);
+    for (int t = 0; t < p.nt[d]; ++t) {
+      int lo = t * p.T, hi = std::min(lo + p.T, p.K[d]);
+      std::set<int> bins;
+      for (int u = 0; u < p.K[d]; ++u)
+        for (int o = 0; o < 4; ++o) {
+          int q = ((u - o) % p.K[d] + p.K[d]) % p.K[d];
+          if (q >= lo && q < hi) bins.insert(u / p.T);
+        }
+      if (bins.size() > 3) return fail(kBadInput, "PME: tile geometry");
+      int4 s = make_int4((int)bins.size(), 0, 0, 0);
+      int k = 0;
+      for (int b : bins) {
+        if (k == 0) s.y = b;
+        if (k == 1) s.z = b;
+        if (k == 2) s.w = b;
+        ++k;
+      }
+      src[t] = s;
+    }
+    SNB_CUDA_TRY(cudaMalloc(&p.d_src[d], sizeof(int4) * p.nt[d]));
+    SNB_CUDA_TRY(cudaMemcpy(p.d_src[d], src.data(), sizeof(int4) * p.nt[d],
+                            cudaMemcpyHostToDevice));
+  }
+  SNB_CUDA_TRY(cudaMalloc(&p.d_Q, sizeof(float) * p.nall));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_FQ, sizeof(cufftComplex) * p.nfft));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_phi, sizeof(float) * p.nall));
+  SNB_CUDA_TRY(cudaMemset(p.d_phi, 0, sizeof(float) * p.nall));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_tile_count, sizeof(int) * p.ntiles));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_tile_start, sizeof(int) * (p.ntiles + 1)));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_atom_tile, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_atom_slot, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_binned, sizeof(float4) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_binned_u, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_frq, sizeof(float4) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_upk, sizeof(int) * n));
+  p.partial_blocks = std::min(ceil_div(p.nfft, kSpecBlock), 148 * 8);
+  SNB_CUDA_TRY(cudaMalloc(&p.d_partial, sizeof(double) * 8 * p.partial_blocks));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_sums, sizeof(double) * 8));
+  SNB_CUDA_TRY(cudaMemset(p.d_sums, 0, sizeof(double) * 8));
+  if (cufftPlan3d(&p.plan_r2c, p.K[0], p.K[1], p.K[2], CUFFT_R2C) != CUFFT_SUCCESS ||
+      cufftPlan3d(&p.plan_c2r, p.K[0], p.K[1], p.K[2], CUFFT_C2R) != CUFFT_SUCCESS)
+    return fail(kCudaError, "PME: cuFFT plan creation failed");
+  return kOk;
+}
+
+void pme_free(PME& p) {
+  for (int d = 0; d < 3; ++d) cudaFree(p.d_src[d]);
+  cudaFree(p.d_frq);
+  cudaFree(p.d_upk);
+  for (int d = 0; d < 3; ++d) cudaFree(p.d_B[d]);
+  cudaFree(p.d_Q);
+  cudaFree(p.d_FQ);
+  cudaFree(p.d_phi);
+  cudaFree(p.d_tile_count);
+  cudaFree(p.d_tile_start);
+  cudaFree(p.d_atom_tile);
+  cudaFree(p.d_atom_slot);
+  cudaFree(p.d_binned);
+  cudaFree(p.d_binned_u);
+  cudaFree(p.d_partial);
+  cudaFree(p.d_sums);
+  cudaFree(p.scan.block_sums);
+  if (p.plan_r2c) cufftDestroy(p.plan_r2c);
+  if (p.plan_c2r) cufftDestroy(p.plan_c2r);
+  p = PME();
+}
+
+int pme_reciprocal(PME& p, const float4* pos, int n, Accumulators& acc, int accum,
+                   bool need_energy, bool need_virial, cudaStream_t st) {
+  if (n != p.n) return fail(kBadInput, "PME: atom count differs from Initial");
+  TileGeom g{p.K[0], p.K[1], p.K[2], p.T, p.nt[0], p.nt[1], p.nt[2], p.rcell};
+  if (cufftSetStream(p.plan_r2c, st) != CUFFT_SUCCESS ||
+      cufftSetStream(p.plan_c2r, st) != CUFFT_SUCCESS)
+    return fail(kCudaError, "PME: cufftSetStream failed");
+  SNB_CUDA_TRY(cudaMemsetAsync(p.d_tile_count, 0, sizeof(int) * p.ntiles, st));
+  k_pme_bin<<<ceil_div(n, 256), 256, 0, st>>>(n, pos, g, p.d_atom_tile, p.d_atom_slot,
+                                              p.d_tile_count, p.d_frq, p.d_upk);
+  if (accum == kAccumFixed) {
+    int rc = scan_exclusive(p.d_tile_count, p.d_tile_start, p.ntiles, nullptr, p.scan,
+                            st);
+    if (rc) return rc;
+    k_pme_scatter<<<ceil_div(n, 256), 256, 0, st>>>(
+        n, p.d_atom_tile, p.d_atom_slot, p.d_tile_start, p.d_frq, p.d_upk,
+        p.d_binned, p.d_binned_u);
+    k_pme_spread<<<p.ntiles, 256, 0, st>>>(g, p.d_tile_start, p.d_binned,
+                                           p.d_binned_u, p.d_src[0], p.d_src[1],
+                                           p.d_src[2], p.d_Q);
+  } else {
+    SNB_CUDA_TRY(cudaMemsetAsync(p.d_Q, 0, sizeof(float) * p.nall, st));
+    k_pme_spread_atomic<<<ceil_div(n, 16), 256, 0, st>>>(n, p.d_frq, p.d_upk, g,
+                                                         p.d_Q);
+  }
+  if (cufftExecR2C(p.plan_r2c, p.d_Q, p.d_FQ) != CUFFT_SUCCESS)
+    return fail(kCudaError, "PME: cufftExecR2C failed");
+  SpecGeom sg;
+  sg.K0 = p.K[0];
+  sg.K1 = p.K[1];
+  sg.K2 = p.K[2];
+  sg.nc = p.K[2] / 2 + 1;
+  sg.rcell = p.rcell;
+  sg.mpre = (float)(M_PI * M_PI / ((double)p.beta * p.beta));
+  sg.inv_pi_v = (float)(1.0 / (M_PI * p.volume));
+  if (need_virial)
+    k_pme_influence<true><<<p.partial_blocks, kSpecBlock, 0, st>>>(
+        p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy);
+  else
+    k_pme_influence<false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
+        p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy);
+  if (need_energy || need_virial)
+    k_pme_finish<<<1, 1024, 0, st>>>(p.partial_blocks, p.d_partial, pos, n,
+                                     (double)p.beta, p.volume, p.d_sums, need_energy);
+  if (cufftExecC2R(p.plan_c2r, p.d_FQ, p.d_phi) != CUFFT_SUCCESS)
+    return fail(kCudaError, "PME: cufftExecC2R failed");
+  const float scale = (float)p.update_interval;
+  if (accum == kAccumFixed)
+    k_pme_gather<kAccumFixed><<<ceil_div(n, 64), 256, 0, st>>>(n, p.d_frq, p.d_upk,
+                                                               g, p.d_phi, scale, acc);
+  else
+    k_pme_gather<kAccumFloat><<<ceil_div(n, 64), 256, 0, st>>>(n, p.d_frq, p.d_upk,
+                                                               g, p.d_phi, scale, acc);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// Excluded-pair correction: removes the reciprocal-space interaction of the
+// excluded pairs (MPI_PME_Excluded_Force_With_Atom_Energy_Correction,
+// PM_force.cpp:1745-1817, factor 1 for one process):
+//   F/r = -q_i q_j ((2 beta r/sqrt(pi) e^{-b^2r^2} + erfc(beta r)) - 1)/r^3,
+//   E_i -= q_i q_j erf(beta r)/r, virial_i -= (F/r) dr (x) dr.
+template <int ACCUM, bool ENERGY, bool VIRIAL>
+__global__ void k_excluded(int n, const float3* __restrict__ crd,
+                           const float* __restrict__ charge, Cell cell, Cell rcell,
+                           float beta, const int* __restrict__ excl_start,
+                           const int* __restrict__ excl_list,
+                           const int* __restrict__ excl_numbers,
+                           const int* __restrict__ map, Accumulators acc) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int cnt = excl_numbers[i];
+  if (cnt <= 0) return;
+  const int N = acc.n;
+  int st = excl_start[i];
+  float3 ri = crd[i];
+  float qi = charge[i];
+  float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f;
+  float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int k = st; k < st + cnt; ++k) {
+    int j = excl_list[k];
+    if ((unsigned)j >= (unsigned)n) continue;  // malformed list entry
+    float3 d = min_image_fast<false>(crd[j], ri, cell, rcell);
+    float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+    float r = sqrtf(r2);
+    float br = beta * r;
+    float fs = br * 1.1283791670955126f * expf(-br * br) + erfcf(br);
+    fs = -qi * charge[j] * ((fs - 1.0f) / r2 / r);
+    float gx = fs * d.x, gy = fs * d.y, gz = fs * d.z;
+    fx += gx;
+    fy += gy;
+    fz += gz;
+    int sj = map ? map[j] : j;
+    if (ACCUM == kAccumFixed) {
+      red_add(acc.d_f + sj, -to_fixed_force(gx));
+      red_add(acc.d_f + N + sj, -to_fixed_force(gy));
+      red_add(acc.d_f + 2 * N + sj, -to_fixed_force(gz));
+    } else {
+      atomicAdd(acc.d_ff + sj, -gx);
+      atomicAdd(acc.d_ff + N + sj, -gy);
+      atomicAdd(acc.d_ff + 2 * N + sj, -gz);
+    }
+    if (ENERGY) e -= qi * charge[j] * erff(br) / r;
+    if (VIRIAL) {
+      v[0] -= gx * d.x;
+      v[1] -= gx * d.y + gy * d.x;
+      v[2] -= gy * d.y;
+      v[3] -= gx * d.z + gz * d.x;
+      v[4] -= gy * d.z + gz * d.y;
+      v[5] -= gz * d.z;
+    }
+  }
+  int si = map ? map[i] : i;
+  if (ACCUM == kAccumFixed) {
+    red_add(acc.d_f + si, to_fixed_force(fx));
+    red_add(acc.d_f + N + si, to_fixed_force(fy));
+    red_add(acc.d_f + 2 * N + si, to_fixed_force(fz));
+    if (ENERGY) red_add(acc.d_e + si, to_fixed_energy(e));
+    if (VIRIAL)
+      for (int c = 0; c < 6; ++c) red_add(acc.d_v + c * N + si, to_fixed_energy(v[c]));
+  } else {
+    atomicAdd(acc.d_ff + si, fx);
+    atomicAdd(acc.d_ff + N + si, fy);
+    atomicAdd(acc.d_ff + 2 * N + si, fz);
+    if (ENERGY) atomicAdd(acc.d_fe + si, e);
+    if (VIRIAL)
+      for (int c = 0; c < 6; ++c) atomicAdd(acc.d_fv + c * N + si, v[c]);
+  }
+}
+
+template <int ACCUM>
+static void launch_excl2(int n, const float3* crd, const float* charge,
+                         const Cell& cell, const Cell& rcell, float beta,
+                         const int* es, const int* el, const int* en, const int* map,
+                         Accumulators& acc, bool energy, bool virial, cudaStream_t st) {
+  dim3 g(ceil_div(n, 256)), b(256);
+  if (energy && virial)
+    k_excluded<ACCUM, true, true><<<g, b, 0, st>>>(n, crd, charge, cell, rcell, beta,
+                                                  es, el, en, map, acc);
+  else if (energy)
+    k_excluded<ACCUM, true, false><<<g, b, 0, st>>>(n, crd, charge, cell, rcell, beta,
+                                                   es, el, en, map, acc);
+  else if (virial)
+    k_excluded<ACCUM, false, true><<<g, b, 0, st>>>(n, crd, charge, cell, rcell, beta,
+                                                   es, el, en, map, acc);
+  else
+    k_excluded<ACCUM, false, false><<<g, b, 0, st>>>(n, crd, charge, cell, rcell,
+                                                    beta, es, el, en, map, acc);
+}
+
+int launch_excluded(int n, const float3* crd, const float* charge, const Cell& cell,
+                    const Cell& rcell, float beta, const int* excl_start,
+                    const int* excl_list, const int* excl_numbers, const int* map,
+                    Accumulators& acc, int accum, bool energy, bool virial,
+                    cudaStream_t st) {
+  if (n <= 0 || !excl_numbers) return kOk;
+  if (accum == kAccumFixed)
+    launch_excl2<kAccumFixed>(n, crd, charge, cell, rcell, beta, excl_start, excl_list,
+                              excl_numbers, map, acc, energy, virial, st);
+  else
+    launch_excl2<kAccumFloat>(n, crd, charge, cell, rcell, beta, excl_start, excl_list,
+                              excl_numbers, map, acc, energy, virial, st);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+}  // namespace snb

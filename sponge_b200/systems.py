@@ -1,0 +1,220 @@
+"""Seeded synthetic water / NaCl boxes in SPONGE's internal units.
+
+The boxes stand in for the reference's benchmark inputs (no external dataset is
+used).  Units follow SPONGE (``SPONGE/common.h``): length in Angstrom, energy in
+kcal/mol, charges pre-multiplied by 18.2223 so that q_i*q_j/r is kcal/mol, time
+step in internal units (1 ps = 20.455 units).  LJ pair tables are stored the way
+``Xponge::Native_Load_LJ`` leaves them (``xponge/load/native/lj.hpp:47,57``):
+A' = 12 * 4*eps*sigma^12 and B' = 6 * 4*eps*sigma^6, indexed by the triangular
+pair index of ``Get_LJ_Type`` (``Lennard_Jones_force.h:19-28``).
+
+Geometry rule: stated molecule counts at 1.0 g/cm^3, box length from the
+density, PME grid from ``Get_Fft_Patameter(L / 1.0)`` (``common.cpp:639-659``).
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+CHARGE_SCALE = np.float32(18.2223)          # common.h CONSTANT_SPONGE_CHARGE_SCALE
+TIME_CONVERSION = 20.455                    # common.h CONSTANT_TIME_CONVERTION
+KB = 0.00198716                             # common.h CONSTANT_kB (kcal/mol/K)
+AVOGADRO = 6.02214076e23
+WATER_VOLUME_A3 = 18.01528 / AVOGADRO * 1e24  # volume of one molecule at 1 g/cm^3
+
+# LJ atom types: 0 O, 1 H (no LJ), 2 Na+, 3 Cl-
+LJ_SIGMA = np.array([3.1507, 0.0, 2.439, 4.478])
+LJ_EPS = np.array([0.1521, 0.0, 0.0874, 0.0355])
+MASS = np.array([15.9994, 1.008, 22.98977, 35.453])
+CHARGE_E = {"O": -0.834, "H": 0.417, "Na": 1.0, "Cl": -1.0}
+
+BOND_K, BOND_R0 = 553.0, 0.9572
+ANGLE_K, ANGLE_T0 = 100.0, math.radians(104.52)
+
+
+def lj_pair_index(a: int, b: int) -> int:
+    """Triangular pair index max*(max+1)/2 + min (Get_LJ_Type)."""
+    hi, lo = max(a, b), min(a, b)
+    return hi * (hi + 1) // 2 + lo
+
+
+def lj_tables(n_types: int = 4):
+    """Lorentz-Berthelot mixed A'/B' tables as float32 in SPONGE's stored form."""
+    npair = n_types * (n_types + 1) // 2
+    A = np.zeros(npair, np.float32)
+    B = np.zeros(npair, np.float32)
+    for a in range(n_types):
+        for b in range(a + 1):
+            eps = math.sqrt(LJ_EPS[a] * LJ_EPS[b])
+            if eps == 0.0:
+                continue
+            sig = 0.5 * (LJ_SIGMA[a] + LJ_SIGMA[b])
+            k = lj_pair_index(a, b)
+            A[k] = np.float32(4.0 * eps * sig ** 12) * np.float32(12.0)
+            B[k] = np.float32(4.0 * eps * sig ** 6) * np.float32(6.0)
+    return A, B
+
+
+def check_2357(n: int) -> bool:
+    for p in (2, 3, 5, 7):
+        while n > 1 and n % p == 0:
+            n //= p
+    return n == 1
+
+
+def fft_size(length: float) -> int:
+    """Grid size rule of Get_Fft_Patameter (common.cpp:639-659)."""
+    t = (int(math.ceil(length + 3)) >> 2) << 2
+    for lo, hi, v in ((60, 68, 64), (120, 136, 128), (240, 272, 256),
+                      (480, 544, 512), (960, 1088, 1024)):
+        if lo <= t <= hi:
+            t = v
+            break
+    while not check_2357(t):
+        t += 4
+    return t
+
+
+@dataclasses.dataclass
+class System:
+    """One periodic box, atoms in residue order (the caller's order)."""
+    crd: np.ndarray          # (N, 3) float32, Angstrom
+    vel: np.ndarray          # (N, 3) float32, Angstrom per internal time unit
+    charge: np.ndarray       # (N,) float32, scaled by 18.2223
+    lj_type: np.ndarray      # (N,) int32
+    lj_A: np.ndarray         # (npair,) float32
+    lj_B: np.ndarray         # (npair,) float32
+    mass: np.ndarray         # (N,) float32
+    excl_start: np.ndarray   # (N,) int32  one-directional (j > i) CSR, as Xponge
+    excl_numbers: np.ndarray  # (N,) int32
+    excl_list: np.ndarray    # (E,) int32
+    bonds: np.ndarray        # (nb, 2) int32
+    angles: np.ndarray       # (na, 3) int32  (H, O, H)
+    box: float               # cubic box length
+    n_types: int = 4
+
+    @property
+    def n(self) -> int:
+        return int(self.crd.shape[0])
+
+    def cell(self) -> np.ndarray:
+        """LTMatrix3 {a11, a21, a22, a31, a32, a33} of the box."""
+        L = np.float32(self.box)
+        return np.array([L, 0, L, 0, 0, L], np.float32)
+
+    def rcell(self) -> np.ndarray:
+        r = np.float32(1.0) / np.float32(self.box)
+        return np.array([r, 0, r, 0, 0, r], np.float32)
+
+
+def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    R = np.empty((n, 3, 3))
+    R[:, 0, 0] = 1 - 2 * (y * y + z * z)
+    R[:, 0, 1] = 2 * (x * y - z * w)
+    R[:, 0, 2] = 2 * (x * z + y * w)
+    R[:, 1, 0] = 2 * (x * y + z * w)
+    R[:, 1, 1] = 1 - 2 * (x * x + z * z)
+    R[:, 1, 2] = 2 * (y * z - x * w)
+    R[:, 2, 0] = 2 * (x * z - y * w)
+    R[:, 2, 1] = 2 * (y * z + x * w)
+    R[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return R
+
+
+def ion_pairs_for(box: float, molarity: float = 0.15) -> int:
+    return int(round(molarity * box ** 3 * 1e-27 * AVOGADRO))
+
+
+def water_box(n_waters: int, seed: int = 0, ion_pairs: int | None = 0,
+              temperature: float = 300.0, box: float | None = None) -> System:
+    """Flexible 3-site water on a jittered cubic lattice, optional NaCl.
+
+    ``ion_pairs=None`` means 0.15 M NaCl for the box volume.  Ions replace
+    randomly chosen waters (the ion sits at the oxygen site).
+    """
+    rng = np.random.default_rng(seed)
+    if box is None:
+        box = (n_waters * WATER_VOLUME_A3) ** (1.0 / 3.0)
+    if ion_pairs is None:
+        ion_pairs = ion_pairs_for(box)
+    n_side = int(math.ceil(n_waters ** (1.0 / 3.0) - 1e-9))
+    spacing = box / n_side
+    sites = np.sort(rng.permutation(n_side ** 3)[:n_waters])
+    ix, rem = np.divmod(sites, n_side * n_side)
+    iy, iz = np.divmod(rem, n_side)
+    o_pos = (np.stack([ix, iy, iz], 1) + 0.5) * spacing
+    o_pos += rng.uniform(-0.3, 0.3, size=o_pos.shape)
+    rot = _random_rotations(rng, n_waters)
+    half = ANGLE_T0 / 2
+    h_local = np.array([[math.sin(half), 0.0, math.cos(half)],
+                        [-math.sin(half), 0.0, math.cos(half)]]) * BOND_R0
+    h_pos = o_pos[:, None, :] + np.einsum("nij,kj->nki", rot, h_local)
+    kind = np.zeros(n_waters, np.int8)          # 0 water, 1 Na, 2 Cl
+    if ion_pairs:
+        pick = rng.choice(n_waters, size=2 * ion_pairs, replace=False)
+        kind[pick[:ion_pairs]] = 1
+        kind[pick[ion_pairs:]] = 2
+
+    crd, typ, chg, mass = [], [], [], []
+    excl = []
+    bonds, angles = [], []
+    for m in range(n_waters):
+        base = len(crd)
+        if kind[m] == 0:
+            crd.extend([o_pos[m], h_pos[m, 0], h_pos[m, 1]])
+            typ.extend([0, 1, 1])
+            chg.extend([CHARGE_E["O"], CHARGE_E["H"], CHARGE_E["H"]])
+            mass.extend([MASS[0], MASS[1], MASS[1]])
+            excl.extend([[base + 1, base + 2], [base + 2], []])
+            bonds.extend([[base, base + 1], [base, base + 2]])
+            angles.append([base + 1, base, base + 2])
+        else:
+            t = 2 if kind[m] == 1 else 3
+            crd.append(o_pos[m])
+            typ.append(t)
+            chg.append(CHARGE_E["Na"] if t == 2 else CHARGE_E["Cl"])
+            mass.append(MASS[t])
+            excl.append([])
+    n = len(crd)
+    crd = np.asarray(crd, np.float32)
+    charge = (np.asarray(chg, np.float32) * CHARGE_SCALE).astype(np.float32)
+    mass = np.asarray(mass, np.float32)
+    numbers = np.array([len(e) for e in excl], np.int32)
+    start = np.zeros(n, np.int32)
+    start[1:] = np.cumsum(numbers)[:-1]
+    flat = np.array([j for e in excl for j in e], np.int32)
+    # Maxwell-Boltzmann velocities in internal units (kcal/mol, g/mol -> A/unit)
+    sigma = np.sqrt(KB * temperature / mass.astype(np.float64))
+    vel = rng.normal(size=(n, 3)) * sigma[:, None]
+    vel -= (vel * mass[:, None]).sum(0) / mass.sum()
+    A, B = lj_tables(4)
+    return System(crd=crd, vel=vel.astype(np.float32), charge=charge,
+                  lj_type=np.asarray(typ, np.int32), lj_A=A, lj_B=B, mass=mass,
+                  excl_start=start, excl_numbers=numbers, excl_list=flat,
+                  bonds=np.asarray(bonds, np.int32).reshape(-1, 2),
+                  angles=np.asarray(angles, np.int32).reshape(-1, 3),
+                  box=float(box))
+
+
+def config_small(seed: int = 0) -> System:
+    """3,000 waters (9,000 atoms), L = 44.77 A, grid 48^3, cutoff 8, skin 2."""
+    return water_box(3000, seed=seed, ion_pairs=0)
+
+
+def config_100k(seed: int = 0) -> System:
+    """33,333 waters with 0.15 M NaCl replacing 180 waters: 99,639 atoms,
+    L = 99.90 A, grid 100^3, cutoff 10, skin 2."""
+    return water_box(33333, seed=seed, ion_pairs=None)
+
+
+def config_batch_member(seed: int) -> System:
+    """One box of the 256-box batch: water count U[200, 2000] from the seed."""
+    rng = np.random.default_rng(10_000 + seed)
+    nw = int(rng.integers(200, 2001))
+    return water_box(nw, seed=seed, ion_pairs=None)

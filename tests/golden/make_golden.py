@@ -1,0 +1,81 @@
+"""Generate the golden vectors in tests/golden/ from the reference itself.
+
+Runs the reference's own CPU build of the hot-path modules (oracle/_ref,
+compiled from its sources by `make -C oracle ref`) on small seeded boxes and
+stores inputs and outputs.  Needs the reference sources (this container);
+the committed .npz files are what the tests read everywhere else.
+
+    python tests/golden/make_golden.py
+"""
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.oracle import ReferenceCPU, build_oracle  # noqa: E402
+from sponge_b200 import systems  # noqa: E402
+
+
+def pair_digest(pairs: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(pairs, np.int32).tobytes()).hexdigest()
+
+
+def reference_pairs(counts, serial):
+    i = np.repeat(np.arange(len(counts)), counts)
+    p = np.stack([i, serial.astype(np.int64)], 1)
+    return p[np.lexsort((p[:, 1], p[:, 0]))]
+
+
+def make_case(name, s, cutoff, skin):
+    ref = ReferenceCPU(exact=False)
+    beta = ref.init(s, cutoff, skin)
+    counts, serial, ov = ref.nl_update()
+    assert not ov.any()
+    pairs = reference_pairs(counts, serial)
+    lj = ref.lj_direct()
+    pme = ref.pme_reciprocal()
+    ex = ref.pme_excluded()
+    V = float(np.float32(s.box) ** 3)
+    lrc = ref.lj_long_range(V)
+    # pair set again from the build without fast-math / FMA contraction
+    ref_exact = ReferenceCPU(exact=True)
+    ref_exact.init(s, cutoff, skin)
+    c2, s2, _ = ref_exact.nl_update()
+    pairs_exact = reference_pairs(c2, s2)
+    assert np.array_equal(pairs, pairs_exact)
+    out = dict(
+        crd=s.crd, charge=s.charge, lj_type=s.lj_type, lj_A=s.lj_A, lj_B=s.lj_B,
+        excl_start=s.excl_start, excl_numbers=s.excl_numbers, excl_list=s.excl_list,
+        box=np.float64(s.box), cutoff=np.float32(cutoff), skin=np.float32(skin),
+        beta=np.float32(beta), grid=np.array(ref.grid, np.int32),
+        nl_counts=counts, nl_pair_total=np.int64(len(pairs)),
+        nl_pair_sha256=np.array(pair_digest(pairs)),
+        lj_frc=lj["frc"], lj_atom_energy=lj["atom_energy"], lj_virial=lj["virial"],
+        lj_lj_energy=lj["lj_energy"], lj_coulomb_energy=lj["coulomb_energy"],
+        pme_frc=pme["frc"], pme_virial=pme["virial"], pme_potential=np.float32(pme["potential"]),
+        pme_e_recip=np.float32(pme["e_recip"]), pme_e_self=np.float32(pme["e_self"]),
+        excl_frc=ex["frc"], excl_atom_energy=ex["atom_energy"], excl_virial=ex["virial"],
+        lrc_factor=np.float32(lrc["factor"]), lrc_potential=np.float32(lrc["potential"]),
+        lrc_virial=lrc["virial"],
+    )
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes,", len(pairs), "pairs")
+
+
+def main():
+    build_oracle()
+    # 216 waters, L = 18.63 A, grid 20^3, cutoff 8
+    make_case("water216_rc8", systems.water_box(216, seed=1), 8.0, 2.0)
+    # 343 waters + 1 NaCl pair, cutoff 9, skin 1.5 (non-default keys)
+    make_case("water343_nacl_rc9", systems.water_box(343, seed=5, ion_pairs=1), 9.0, 1.5)
+
+
+if __name__ == "__main__":
+    main()

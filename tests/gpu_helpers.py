@@ -1,0 +1,205 @@
+"""Helpers for the -m gpu tests: device buffers from numpy and module handles
+over the C ABI (include/sponge_nb.h)."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from sponge_b200 import capi
+
+
+def dev(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a if dtype is None else a.astype(dtype)))
+    return t.cuda()
+
+
+def ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def bnd(s):
+    return capi.boundary(s.cell(), s.rcell())
+
+
+class Box:
+    """Device copies of a systems.System."""
+
+    def __init__(self, s):
+        self.s = s
+        self.n = s.n
+        self.crd = dev(s.crd.reshape(-1), np.float32)
+        self.charge = dev(s.charge, np.float32)
+        self.es = dev(s.excl_start, np.int32)
+        self.en = dev(s.excl_numbers, np.int32)
+        el = s.excl_list if len(s.excl_list) else np.zeros(1, np.int32)
+        self.el = dev(el, np.int32)
+        self.b = bnd(s)
+
+
+def make_nl(box: Box, cutoff, skin, **opts):
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    o = capi.options(cutoff=cutoff, skin=skin, **opts)
+    capi.check(lib.snb_nl_create(ctypes.byref(o), box.n, cutoff, skin, box.b,
+                                 ctypes.byref(h)), "nl_create")
+    return h
+
+
+def nl_update(h, box: Box, crd=None, forced=1, step=0):
+    lib = capi.load()
+    capi.check(lib.snb_nl_update(h, None, box.n, 0, ptr(box.crd if crd is None else crd),
+                                 box.b, step, forced, ptr(box.es), ptr(box.el),
+                                 ptr(box.en), stream()), "nl_update")
+
+
+def nl_pairs(h):
+    """Sorted (i < j) pair array (P, 2) of the current list."""
+    lib = capi.load()
+    cnt = ctypes.c_longlong(0)
+    capi.check(lib.snb_nl_pair_count(h, ctypes.byref(cnt), stream()), "pair_count")
+    n = cnt.value
+    pi = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    pj = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    capi.check(lib.snb_nl_export_pairs(h, ptr(pi), ptr(pj), n, ctypes.byref(cnt),
+                                       stream()), "export_pairs")
+    p = np.stack([pi[:n].cpu().numpy(), pj[:n].cpu().numpy()], 1).astype(np.int64)
+    order = np.lexsort((p[:, 1], p[:, 0]))
+    return p[order]
+
+
+def csr_to_pairs(rs, cols):
+    n = len(rs) - 1
+    i = np.repeat(np.arange(n), np.diff(rs))
+    return np.stack([i, cols.astype(np.int64)], 1)
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def lj_create(box: Box, cutoff, accumulation="fixed64"):
+    lib = capi.load()
+    s = box.s
+    h = ctypes.c_void_p()
+    o = capi.options(cutoff=cutoff, accumulation=accumulation)
+    t = np.ascontiguousarray(s.lj_type, np.int32)
+    A = np.ascontiguousarray(s.lj_A, np.float32)
+    B = np.ascontiguousarray(s.lj_B, np.float32)
+    capi.check(lib.snb_lj_create(ctypes.byref(o), s.n, s.n_types, t.ctypes.data,
+                                 A.ctypes.data, B.ctypes.data, cutoff, ctypes.byref(h)),
+               "lj_create")
+    return h
+
+
+def lj_force(h, nl, box: Box, beta, energy=True, virial=True):
+    lib = capi.load()
+    n = box.n
+    frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+    ae = torch.zeros(n, dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6 * n, dtype=torch.float32, device="cuda")
+    ce = torch.zeros(n, dtype=torch.float32, device="cuda")
+    capi.check(lib.snb_lj_pme_direct_force(
+        h, n, n, 0, 0, ptr(box.crd), ptr(box.charge), ptr(frc), box.b, nl,
+        ctypes.c_float(beta), int(energy), ptr(ae), int(virial), ptr(vir), ptr(ce),
+        stream()), "lj_pme_direct_force")
+    torch.cuda.synchronize()
+    return dict(frc=frc.cpu().numpy().reshape(n, 3), atom_energy=ae.cpu().numpy(),
+                virial=vir.cpu().numpy().reshape(n, 6), coulomb_energy=ce.cpu().numpy())
+
+
+def pme_create(box: Box, cutoff, accumulation="fixed64", **opts):
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    o = capi.options(cutoff=cutoff, accumulation=accumulation, **opts)
+    L = np.array([box.s.box] * 3, np.float32)
+    capi.check(lib.snb_pme_create(ctypes.byref(o), box.n, box.b, L.ctypes.data, cutoff,
+                                  ctypes.byref(h)), "pme_create")
+    beta = float(lib.snb_pme_beta(h))
+    g = np.zeros(3, np.int32)
+    capi.check(lib.snb_pme_grid(h, g.ctypes.data), "pme_grid")
+    return h, beta, tuple(int(x) for x in g)
+
+
+def pme_reciprocal(h, box: Box, energy=True, virial=True, step=0):
+    lib = capi.load()
+    n = box.n
+    frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6, dtype=torch.float32, device="cuda")
+    pot = torch.zeros(1, dtype=torch.float32, device="cuda")
+    capi.check(lib.snb_pme_reciprocal_force(h, ptr(box.crd), box.b, ptr(box.charge),
+                                            ptr(frc), int(virial), int(energy), ptr(vir),
+                                            ptr(pot), step, stream()), "pme_reciprocal")
+    rec, slf = ctypes.c_double(0), ctypes.c_double(0)
+    v6 = np.zeros(6)
+    capi.check(lib.snb_pme_energies(h, ctypes.byref(rec), ctypes.byref(slf),
+                                    v6.ctypes.data, stream()), "pme_energies")
+    torch.cuda.synchronize()
+    return dict(frc=frc.cpu().numpy().reshape(n, 3), virial=vir.cpu().numpy(),
+                potential=float(pot.cpu()[0]), e_recip=rec.value, e_self=slf.value,
+                virial64=v6)
+
+
+def pme_excluded(h, box: Box, energy=True, virial=True):
+    lib = capi.load()
+    n = box.n
+    frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+    ae = torch.zeros(n, dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6 * n, dtype=torch.float32, device="cuda")
+    capi.check(lib.snb_pme_excluded_force(h, n, None, None, ptr(box.crd), box.b,
+                                          ptr(box.charge), ptr(box.es), ptr(box.el),
+                                          ptr(box.en), ptr(frc), int(energy), ptr(ae),
+                                          int(virial), ptr(vir), stream()),
+               "pme_excluded")
+    torch.cuda.synchronize()
+    return dict(frc=frc.cpu().numpy().reshape(n, 3), atom_energy=ae.cpu().numpy(),
+                virial=vir.cpu().numpy().reshape(n, 6))
+
+
+def engine_create(s, cutoff, skin=2.0, accumulation="fixed64", **opts):
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    o = capi.options(cutoff=cutoff, skin=skin, accumulation=accumulation, **opts)
+    t = np.ascontiguousarray(s.lj_type, np.int32)
+    A = np.ascontiguousarray(s.lj_A, np.float32)
+    B = np.ascontiguousarray(s.lj_B, np.float32)
+    q = np.ascontiguousarray(s.charge, np.float32)
+    es = np.ascontiguousarray(s.excl_start, np.int32)
+    en = np.ascontiguousarray(s.excl_numbers, np.int32)
+    el = np.ascontiguousarray(s.excl_list if len(s.excl_list) else np.zeros(1), np.int32)
+    capi.check(lib.snb_engine_create(ctypes.byref(o), s.n, bnd(s), s.n_types,
+                                     t.ctypes.data, A.ctypes.data, B.ctypes.data,
+                                     q.ctypes.data, es.ctypes.data, en.ctypes.data,
+                                     el.ctypes.data, int(len(s.excl_list)),
+                                     ctypes.byref(h)), "engine_create")
+    return h
+
+
+def engine_set_water_bonded(h, s):
+    from sponge_b200 import systems
+    lib = capi.load()
+    b = np.ascontiguousarray(s.bonds, np.int32)
+    a = np.ascontiguousarray(s.angles, np.int32)
+    nb, na = len(b), len(a)
+    bk = np.full(max(nb, 1), systems.BOND_K, np.float32)
+    br = np.full(max(nb, 1), systems.BOND_R0, np.float32)
+    ak = np.full(max(na, 1), systems.ANGLE_K, np.float32)
+    at = np.full(max(na, 1), systems.ANGLE_T0, np.float32)
+    ba = np.ascontiguousarray(b[:, 0] if nb else np.zeros(1), np.int32)
+    bb = np.ascontiguousarray(b[:, 1] if nb else np.zeros(1), np.int32)
+    aa = np.ascontiguousarray(a[:, 0] if na else np.zeros(1), np.int32)
+    ab = np.ascontiguousarray(a[:, 1] if na else np.zeros(1), np.int32)
+    ac = np.ascontiguousarray(a[:, 2] if na else np.zeros(1), np.int32)
+    capi.check(lib.snb_engine_set_bonded(h, nb, ba.ctypes.data, bb.ctypes.data,
+                                         bk.ctypes.data, br.ctypes.data, na,
+                                         aa.ctypes.data, ab.ctypes.data, ac.ctypes.data,
+                                         ak.ctypes.data, at.ctypes.data),
+               "engine_set_bonded")
