@@ -173,7 +173,7 @@ __device__ __forceinline__ void dbspline4(float x, float* d) {
   d[0] = 0.5f * x2;
   d[1] = -1.5f * x2 + x + 0.5f;
   d[2] = 1.5f * x2 - 2.0f * x;
-  d[3] = 0.5f * x2 - x + 0.5f;
+  d[3] = -0.5f * x2 + x - 0.5f;
 }
 
 // Bitmask of stencil offsets o in {0..3} with (u - o) mod K in [lo, hi).
