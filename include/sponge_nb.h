@@ -285,9 +285,12 @@ int snb_engine_md_steps_graph(snb_engine* e, float* crd, float* vel,
 int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
                              const float* inverse_mass, float dt, int first_step,
                              int steps, double* h_phase_ms, void* stream);
-/* Kernel nodes of the captured one-step graph, total and cuFFT's share. */
+/* Kernel nodes of the captured one-step graph: top level (a step without a
+ * neighbor rebuild), cuFFT's share of them, and the kernels inside the
+ * conditional rebuild node. */
 int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
-                          int* library_kernel_nodes, void* stream);
+                          int* library_kernel_nodes, int* rebuild_kernel_nodes,
+                          void* stream);
 /* Number of neighbor-list rebuilds so far and current pair count (host sync). */
 int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
                      void* stream);

@@ -117,7 +117,8 @@ _SIGS = {
     "snb_engine_md_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_md_steps_graph": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_profile_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P, _P]),
-    "snb_engine_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), _P]),
+    "snb_engine_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                                   ctypes.POINTER(_I), _P]),
     "snb_engine_stats": (_I, [_P, ctypes.POINTER(_LL), ctypes.POINTER(_LL), _P]),
     "snb_engine_destroy": (_I, [_P]),
 }

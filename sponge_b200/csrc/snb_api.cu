@@ -20,7 +20,9 @@ int launch_bonded(int nb, const int* ba, const int* bb, const float* bk,
                   const int* map, Accumulators& acc, long long* e_total,
                   bool energy, cudaStream_t st);
 int launch_leap_frog(int n, const int* map, Accumulators& acc, float3* crd,
-                     float3* vel, const float* inv_mass, float dt, cudaStream_t st);
+                     float3* vel, const float* inv_mass, float dt,
+                     const float3* old_crd, const Cell& cell, const Cell& rcell,
+                     float permit2, int* flags, cudaStream_t st);
 int launch_totals(int n, Accumulators& acc, long long* isum, const long long* bonded,
                   const double* pme_sums, double lrc_energy, double lrc_virial,
                   double* totals, bool energy, bool virial, bool have_pme,
@@ -116,6 +118,8 @@ struct snb_engine {
   const float* g_invm = nullptr;
   float g_dt = 0.f;
   cudaStream_t g_stream = nullptr;
+  cudaStream_t side = nullptr;  // captures the conditional rebuild body
+  int body_kernels = 0;         // kernel nodes inside the rebuild body
   // recovery snapshot for neighbor-list overflow
   float* d_snap_crd = nullptr;
   float* d_snap_vel = nullptr;
@@ -887,20 +891,82 @@ extern "C" int snb_engine_create(const snb_options* opt, int n, snb_boundary bou
   SNB_CUDA_TRY(cudaMalloc(&e->d_totals_scratch, sizeof(double) * 16));
   SNB_CUDA_TRY(cudaMalloc(&e->d_snap_crd, sizeof(float) * 3 * n));
   SNB_CUDA_TRY(cudaMalloc(&e->d_snap_vel, sizeof(float) * 3 * n));
+  SNB_CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
   *out = e;
   return kOk;
 }
 
-// nonbonded forces of one step into e->acc (sorted frame), no unpack
+// Inside a stream capture: an IF node whose body is the neighbor-list
+// rebuild, taken when the rebuild flag is set (by the previous step's
+// leap-frog check, or by a forced update).  Non-rebuild steps then cost one
+// tiny kernel instead of the ~15 early-exit launches of the rebuild.
+static int capture_conditional_rebuild(snb_engine* e, const float* crd, cudaStream_t st) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  SNB_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) return fail(kCudaError, "capture not active");
+  cudaGraphConditionalHandle hc;
+  SNB_CUDA_TRY(cudaGraphConditionalHandleCreate(&hc, cg, 0, cudaGraphCondAssignDefault));
+  int rc = nl_set_condition(e->nl, hc, st);
+  if (rc) return rc;
+  SNB_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd));
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hc;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cn;
+  SNB_CUDA_TRY(cudaGraphAddNode(&cn, cg, deps, nd, &cp));
+  SNB_CUDA_TRY(cudaStreamUpdateCaptureDependencies(st, &cn, 1,
+                                                   cudaStreamSetCaptureDependencies));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  SNB_CUDA_TRY(cudaStreamBeginCaptureToGraph(e->side, body, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+  rc = nl_rebuild(e->nl, crd, nullptr, e->d_excl_start, e->d_excl_list,
+                  e->d_excl_numbers, e->side);
+  cudaGraph_t b2 = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(e->side, &b2);
+  if (rc) return rc;
+  if (ce != cudaSuccess)
+    return fail(kCudaError, std::string("rebuild body capture: ") + cudaGetErrorString(ce));
+  size_t nn = 0;
+  SNB_CUDA_TRY(cudaGraphGetNodes(body, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  SNB_CUDA_TRY(cudaGraphGetNodes(body, nodes.data(), &nn));
+  e->body_kernels = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    SNB_CUDA_TRY(cudaGraphNodeGetType(nd, &t));
+    e->body_kernels += t == cudaGraphNodeTypeKernel;
+  }
+  return kOk;
+}
+
+// nonbonded forces of one step into e->acc (sorted frame), no unpack.
+// in_graph: called while capturing the replayed step (conditional rebuild,
+// refresh check done by the previous step's leap-frog).
 static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
-                         bool virial, bool forced_nl, cudaStream_t st) {
+                         bool virial, bool forced_nl, cudaStream_t st,
+                         bool in_graph = false) {
   prof_mark(e, 0, st);
-  int rc = nl_update(e->nl, crd, nullptr, nullptr, step, forced_nl ? 1 : 0,
-                     e->d_excl_start, e->d_excl_list, e->d_excl_numbers, st);
+  int rc;
+  if (in_graph) {
+    rc = capture_conditional_rebuild(e, crd, st);
+  } else {
+    rc = nl_update(e->nl, crd, nullptr, nullptr, step, forced_nl ? 1 : 0,
+                   e->d_excl_start, e->d_excl_list, e->d_excl_numbers, st);
+  }
   if (rc) return rc;
   prof_mark(e, 1, st);
-  rc = launch_pack(e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
-                   e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st);
+  const bool do_pme = e->pme.reciprocal && step % e->pme.update_interval == 0;
+  if (do_pme)
+    rc = pme_pack_bin(e->pme, e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
+                      e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st);
+  else
+    rc = launch_pack(e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
+                     e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st);
   if (rc) return rc;
   prof_mark(e, 2, st);
   PairArgs a;
@@ -929,8 +995,8 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
     if (rc) return rc;
   }
   prof_mark(e, 4, st);
-  if (e->pme.reciprocal && step % e->pme.update_interval == 0) {
-    rc = pme_reciprocal(e->pme, e->d_pos, e->n, e->acc, e->accum, energy, virial, st);
+  if (do_pme) {
+    rc = pme_after_bin(e->pme, e->n, e->acc, e->accum, energy, virial, st);
     if (rc) return rc;
   }
   prof_mark(e, 5, st);
@@ -1004,18 +1070,24 @@ extern "C" int snb_engine_set_bonded(snb_engine* e, int nb, const int* ba, const
 }
 
 static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* invm,
-                          float dt, int step, bool forced_nl, cudaStream_t st) {
+                          float dt, int step, bool forced_nl, cudaStream_t st,
+                          bool in_graph = false) {
   if (e->accum != kAccumFixed)
     return fail(kNotSupported, "md steps need the fixed-point accumulation");
-  int rc = engine_forces(e, crd, step, false, false, forced_nl, st);
+  int rc = engine_forces(e, crd, step, false, false, forced_nl, st, in_graph);
   if (rc) return rc;
   rc = launch_bonded(e->nb, e->d_ba, e->d_bb, e->d_bk, e->d_br0, e->na, e->d_aa, e->d_ab,
                      e->d_ac, e->d_ak, e->d_at0, reinterpret_cast<const float3*>(crd),
                      e->cell, e->rcell, e->nl.d_inv_perm, e->acc, nullptr, false, st);
   if (rc) return rc;
   prof_mark(e, 6, st);
+  // the next step's refresh check rides on the coordinate update
+  const bool check = e->opt.nl_refresh_interval <= 0;
+  const float permit = e->opt.skin * e->opt.nl_skin_permit;
   rc = launch_leap_frog(e->n, e->nl.d_inv_perm, e->acc, reinterpret_cast<float3*>(crd),
-                        reinterpret_cast<float3*>(vel), invm, dt, st);
+                        reinterpret_cast<float3*>(vel), invm, dt,
+                        check ? e->nl.d_old_crd : nullptr, e->cell, e->rcell,
+                        permit * permit, e->nl.d_flags, st);
   prof_mark(e, 7, st);
   return rc;
 }
@@ -1050,7 +1122,7 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
             e->graph_exec = nullptr;
           }
           SNB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-          int rc = engine_md_step(e, crd, vel, invm, dt, step, false, st);
+          int rc = engine_md_step(e, crd, vel, invm, dt, step, false, st, true);
           cudaGraph_t g = nullptr;
           cudaError_t ce = cudaStreamEndCapture(st, &g);
           if (rc) return rc;
@@ -1148,9 +1220,11 @@ extern "C" int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
 // Kernel nodes in the captured one-step graph: all, and those that belong to
 // cuFFT (counted from a graph holding only the two transforms).
 extern "C" int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
-                                     int* library_kernel_nodes, void* stream) {
+                                     int* library_kernel_nodes, int* rebuild_kernel_nodes,
+                                     void* stream) {
   if (!e || !kernel_nodes || !library_kernel_nodes)
     return fail(kBadInput, "engine_graph_info: bad argument");
+  if (rebuild_kernel_nodes) *rebuild_kernel_nodes = e->body_kernels;
   auto count = [](cudaGraph_t g, int* out) -> int {
     size_t nn = 0;
     SNB_CUDA_TRY(cudaGraphGetNodes(g, nullptr, &nn));
@@ -1198,6 +1272,7 @@ extern "C" int snb_engine_destroy(snb_engine* e) {
   if (e->graph) cudaGraphDestroy(e->graph);
   for (int k = 0; k < 8; ++k)
     if (e->prof_ev[k]) cudaEventDestroy(e->prof_ev[k]);
+  if (e->side) cudaStreamDestroy(e->side);
   nl_free(e->nl);
   pme_free(e->pme);
   acc_free(e->acc);

@@ -118,6 +118,27 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// erfc(x) and exp(-x^2) together for x >= 0.  erfcx(x) = erfc(x) e^{x^2} is
+// a degree-8 polynomial in t = 1/(1 + x/2) on [0, 4] (weighted least-squares
+// fit, csrc/fit_erfcx.py; max relative error 3.3e-7 in float32), so
+// erfc(x) = P(t) * exp(-x^2).  Beyond x = 4 CUDA's erfcf is used.
+__device__ __forceinline__ float erfc_and_exp(float x, float* e_out) {
+  const float e = expf(-x * x);
+  *e_out = e;
+  if (x > 4.0f) return erfcf(x);
+  const float t = 1.0f / (1.0f + 0.5f * x);
+  float p = -0.049221702f;
+  p = fmaf(p, t, 0.33589873f);
+  p = fmaf(p, t, -0.88379663f);
+  p = fmaf(p, t, 1.0076897f);
+  p = fmaf(p, t, -0.39945206f);
+  p = fmaf(p, t, 0.47237507f);
+  p = fmaf(p, t, 0.22729602f);
+  p = fmaf(p, t, 0.2896666f);
+  p = fmaf(p, t, -0.00045567533f);
+  return p * e;
+}
+
 // Ceiling division for launch shapes.
 __host__ __device__ __forceinline__ int ceil_div(long long a, int b) {
   return static_cast<int>((a + b - 1) / b);

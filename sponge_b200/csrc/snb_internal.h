@@ -42,6 +42,7 @@ struct ScanScratch {
 constexpr int kScanBlock = 1024;
 int scan_exclusive(const int* in, int* out, int n, int* total_out,
                    ScanScratch& s, cudaStream_t st);
+int scan_reserve(ScanScratch& s, int n);
 
 // ----------------------------------------------------------------------------
 // Neighbor list: cell grid of side >= (cutoff+skin)/2 (neighbor_list.cpp:943),
@@ -98,6 +99,12 @@ void nl_free(NeighborList& nl);
 int nl_update(NeighborList& nl, const float* crd, const int* atom_local,
               const float* cell6, int step, int forced, const int* excl_start,
               const int* excl_list, const int* excl_numbers, cudaStream_t st);
+int nl_decide(NeighborList& nl, const float* crd, int step, int forced, cudaStream_t st);
+int nl_rebuild(NeighborList& nl, const float* crd, const int* atom_local,
+               const int* excl_start, const int* excl_list, const int* excl_numbers,
+               cudaStream_t st);
+int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st);
+int nl_force_next(NeighborList& nl, cudaStream_t st);
 // Reads the overflow flag and regrows the pair storage if needed (host sync).
 int nl_check_overflow(NeighborList& nl, bool* regrown, cudaStream_t st);
 int nl_total_pairs(NeighborList& nl, long long* total, cudaStream_t st);
@@ -234,6 +241,10 @@ int fft_size(float length);
 int pme_reciprocal(PME& p, const float4* pos, int n, Accumulators& acc,
                    int accum, bool need_energy, bool need_virial,
                    cudaStream_t st);
+int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const int* type,
+                 const int* perm, float4* pos, int* type_sorted, cudaStream_t st);
+int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
+                  bool need_virial, cudaStream_t st);
 
 // Excluded-pair correction (PM_force.cpp:1745-1817).  Caller-frame inputs;
 // forces land in acc at map[i] (map = inv_perm, or nullptr for identity).

@@ -210,6 +210,25 @@ __global__ void k_sorted_cell(int n, const int* __restrict__ perm,
 
 __global__ void k_finish_build(int* flags) {
   if (flags[kFlagNeed] != 0) flags[kFlagGeneration] += 1;
+  flags[kFlagNeed] = 0;
+}
+
+// Reads the rebuild flag into the graph's conditional handle (the IF node
+// that holds the rebuild kernels).
+__global__ void k_set_rebuild_condition(cudaGraphConditionalHandle h, const int* flags) {
+  cudaGraphSetConditional(h, flags[kFlagNeed] != 0 ? 1u : 0u);
+}
+
+int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st) {
+  k_set_rebuild_condition<<<1, 1, 0, st>>>(h, nl.d_flags);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+int nl_force_next(NeighborList& nl, cudaStream_t st) {
+  k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 1);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
 }
 
 // ---------------------------------------------------------------------------
@@ -330,7 +349,7 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
   }
   nl.cap = initial_capacity;
   SNB_CUDA_TRY(cudaMalloc(&nl.d_cols, sizeof(int) * nl.cap));
-  return kOk;
+  return scan_reserve(nl.scan, std::max(nl.ncell, n));
 }
 
 void nl_free(NeighborList& nl) {
@@ -359,7 +378,6 @@ void nl_free(NeighborList& nl) {
 int nl_update(NeighborList& nl, const float* crd_f, const int* atom_local,
               const float* cell6, int step, int forced, const int* excl_start,
               const int* excl_list, const int* excl_numbers, cudaStream_t st) {
-  const float3* crd = reinterpret_cast<const float3*>(crd_f);
   if (cell6) {
     Cell c = make_cell(cell6);
     if (c.a11 != nl.cell.a11 || c.a22 != nl.cell.a22 || c.a33 != nl.cell.a33 ||
@@ -368,10 +386,18 @@ int nl_update(NeighborList& nl, const float* crd_f, const int* atom_local,
                   "neighbor list: the box changed since Initial (NPT re-grid is "
                   "not built on this path)");
   }
+  int rc = nl_decide(nl, crd_f, step, forced, st);
+  if (rc) return rc;
+  return nl_rebuild(nl, crd_f, atom_local, excl_start, excl_list, excl_numbers, st);
+}
+
+// need_update decision of NEIGHBOR_LIST::Update (neighbor_list.cpp:983-999)
+int nl_decide(NeighborList& nl, const float* crd_f, int step, int forced,
+              cudaStream_t st) {
+  const float3* crd = reinterpret_cast<const float3*>(crd_f);
   const int n = nl.n;
   if (nl.generation == 0) forced = 1;  // nothing built yet
   nl.generation += 1;
-  // need_update decision (neighbor_list.cpp:983-999)
   if (forced) {
     k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 1);
   } else if (nl.refresh_interval <= 0) {
@@ -383,6 +409,17 @@ int nl_update(NeighborList& nl, const float* crd_f, const int* atom_local,
   } else {
     k_set_need<<<1, 1, 0, st>>>(nl.d_flags, (step + 1) % nl.refresh_interval == 0);
   }
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+// The rebuild itself; every kernel returns at once unless the need flag is
+// set, so it can also run unconditionally.
+int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
+               const int* excl_start, const int* excl_list, const int* excl_numbers,
+               cudaStream_t st) {
+  const float3* crd = reinterpret_cast<const float3*>(crd_f);
+  const int n = nl.n;
   SNB_CUDA_TRY(cudaMemsetAsync(nl.d_cell_count, 0, sizeof(int) * nl.ncell, st));
   k_bin_count<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz,
                                                 nl.d_atom_cell, nl.d_atom_slot,

@@ -68,10 +68,74 @@ __device__ __forceinline__ void add_virial(Accumulators& acc, int s, const float
   }
 }
 
+// Per-warp queue of in-cutoff pairs: the row is scanned 32 candidates at a
+// time, the ones inside the cutoff are appended (ballot + popc) and the pair
+// terms run only on full batches of 32, so every lane of the expensive part
+// does useful work.
+constexpr int kWarps = 8;
+constexpr int kQueue = 64;
+
+template <int ACCUM, bool ENERGY, bool VIRIAL>
+__device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
+                                        const float* sA, const float* sB, int ti,
+                                        float qi, int gi, float4 e, int j, float& fx,
+                                        float& fy, float& fz, float& e_lj, float& e_c,
+                                        float* vir) {
+  const float r2 = e.x * e.x + e.y * e.y + e.z * e.z;
+  const int p = lj_pair_index(ti, a.type[j]);
+  const float A = sA[p], B = sB[p];
+  const float rinv = rsqrtf(r2);
+  const float r = r2 * rinv;
+  const float ir2 = rinv * rinv;
+  const float ir6 = ir2 * ir2 * ir2;
+  const float flj = (B - A * ir6) * ir6 * ir2;
+  const float qq = qi * e.w;
+  const float br = a.beta * r;
+  float ex;
+  const float erfc_br = erfc_and_exp(br, &ex);
+  const float fc = qq * rinv * ir2 * (br * kTwoOverSqrtPi * ex + erfc_br);
+  const float fs = flj - fc;
+  const float gx = fs * e.x, gy = fs * e.y, gz = fs * e.z;
+  fx += gx;
+  fy += gy;
+  fz += gz;
+  add_force<ACCUM>(acc, j, -gx, -gy, -gz);
+  if (ENERGY || VIRIAL) {
+    const bool own_i = gi < a.global[j];
+    if (ENERGY) {
+      const float elj = (0.083333333f * A * ir6 - 0.166666667f * B) * ir6;
+      const float ec = qq * erfc_br * rinv;
+      if (own_i) {
+        e_lj += elj;
+        e_c += ec;
+      } else {
+        add_energy<ACCUM>(acc, j, elj + ec, elj, ec);
+      }
+    }
+    if (VIRIAL) {
+      float v[6];
+      v[0] = -(gx * e.x);
+      v[1] = -(gx * e.y + gy * e.x);
+      v[2] = -(gy * e.y);
+      v[3] = -(gx * e.z + gz * e.x);
+      v[4] = -(gy * e.z + gz * e.y);
+      v[5] = -(gz * e.z);
+      if (own_i) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) vir[c] += v[c];
+      } else {
+        add_virial<ACCUM>(acc, j, v);
+      }
+    }
+  }
+}
+
 template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO>
 __global__ void __launch_bounds__(256)
 k_lj_direct(PairArgs a, Accumulators acc) {
   extern __shared__ float sh_tab[];
+  __shared__ float4 sq[kWarps][kQueue];   // dx, dy, dz, q_j
+  __shared__ int sj[kWarps][kQueue];      // j
   float* sA = sh_tab;
   float* sB = sh_tab + a.n_types * (a.n_types + 1) / 2;
   const int npair = a.n_types * (a.n_types + 1) / 2;
@@ -81,7 +145,8 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int w = threadIdx.x >> 5;
+  const int i = blockIdx.x * (blockDim.x >> 5) + w;
   if (i >= a.n) return;
   if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
   const float4 pi = a.pos[i];
@@ -92,60 +157,46 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   float e_lj = 0.f, e_c = 0.f;
   float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   const int k0 = a.row_start[i], k1 = a.row_start[i + 1];
-  for (int k = k0 + lane; k < k1; k += 32) {
-    const int j = a.cols[k];
-    const float4 pj = a.pos[j];
-    const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri,
-                                            a.cell, a.rcell);
-    const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
-    if (r2 < a.cutoff2) {
-      const int p = lj_pair_index(ti, a.type[j]);
-      const float A = sA[p], B = sB[p];
-      const float rinv = rsqrtf(r2);
-      const float r = r2 * rinv;
-      const float ir2 = rinv * rinv;
-      const float ir6 = ir2 * ir2 * ir2;
-      const float flj = (B - A * ir6) * ir6 * ir2;
-      const float qq = pi.w * pj.w;
-      const float br = a.beta * r;
-      const float erfc_br = erfcf(br);
-      const float fc = qq * rinv * ir2 * (br * kTwoOverSqrtPi * expf(-br * br) + erfc_br);
-      const float fs = flj - fc;
-      const float gx = fs * dr.x, gy = fs * dr.y, gz = fs * dr.z;
-      fx += gx;
-      fy += gy;
-      fz += gz;
-      add_force<ACCUM>(acc, j, -gx, -gy, -gz);
-      if (ENERGY || VIRIAL) {
-        const bool own_i = gi < a.global[j];
-        if (ENERGY) {
-          const float elj = (0.083333333f * A * ir6 - 0.166666667f * B) * ir6;
-          const float ec = qq * erfc_br * rinv;
-          if (own_i) {
-            e_lj += elj;
-            e_c += ec;
-          } else {
-            add_energy<ACCUM>(acc, j, elj + ec, elj, ec);
-          }
-        }
-        if (VIRIAL) {
-          float v[6];
-          v[0] = -(gx * dr.x);
-          v[1] = -(gx * dr.y + gy * dr.x);
-          v[2] = -(gy * dr.y);
-          v[3] = -(gx * dr.z + gz * dr.x);
-          v[4] = -(gy * dr.z + gz * dr.y);
-          v[5] = -(gz * dr.z);
-          if (own_i) {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) vir[c] += v[c];
-          } else {
-            add_virial<ACCUM>(acc, j, v);
-          }
-        }
+  const unsigned lt = (1u << lane) - 1u;
+  int count = 0;
+  for (int base = k0; base < k1; base += 32) {
+    const int k = base + lane;
+    bool in = false;
+    int j = 0;
+    float4 ent;
+    if (k < k1) {
+      j = a.cols[k];
+      const float4 pj = a.pos[j];
+      const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri,
+                                              a.cell, a.rcell);
+      const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+      in = r2 < a.cutoff2;
+      ent = make_float4(dr.x, dr.y, dr.z, pj.w);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    if (in) {
+      const int slot = count + __popc(m & lt);
+      sq[w][slot] = ent;
+      sj[w][slot] = j;
+    }
+    count += __popc(m);
+    if (count >= 32) {
+      __syncwarp();
+      lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi, sq[w][lane],
+                                     sj[w][lane], fx, fy, fz, e_lj, e_c, vir);
+      __syncwarp();
+      if (lane < count - 32) {
+        sq[w][lane] = sq[w][32 + lane];
+        sj[w][lane] = sj[w][32 + lane];
       }
+      __syncwarp();
+      count -= 32;
     }
   }
+  __syncwarp();
+  if (lane < count)
+    lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi, sq[w][lane],
+                                   sj[w][lane], fx, fy, fz, e_lj, e_c, vir);
   fx = warp_sum(fx);
   fy = warp_sum(fy);
   fz = warp_sum(fz);
@@ -166,8 +217,7 @@ k_lj_direct(PairArgs a, Accumulators acc) {
 
 template <int ACCUM, bool ENERGY, bool VIRIAL>
 static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream_t st) {
-  const int warps = 8;
-  dim3 grid(ceil_div(a.n, warps)), block(32 * warps);
+  dim3 grid(ceil_div(a.n, kWarps)), block(32 * kWarps);
   size_t smem = sizeof(float) * a.n_types * (a.n_types + 1);
   if (ortho)
     k_lj_direct<ACCUM, ENERGY, VIRIAL, true><<<grid, block, smem, st>>>(a, acc);

@@ -146,13 +146,42 @@ __global__ void k_pme_bin(int n, const float4* __restrict__ pos, TileGeom g,
   upk[i] = pack_u(ux, uy, uz);
 }
 
+// Pack and bin in one pass: pos[s] = (crd[perm[s]], charge[perm[s]]) for the
+// pair kernel, and the PME base point / fraction / tile of the same atom.
+__global__ void k_pack_pme_bin(int n, const float3* __restrict__ crd,
+                               const float* __restrict__ charge,
+                               const int* __restrict__ type, const int* __restrict__ perm,
+                               float4* __restrict__ pos, int* __restrict__ type_sorted,
+                               TileGeom g, int* __restrict__ atom_tile,
+                               int* __restrict__ atom_slot, int* __restrict__ tile_count,
+                               float4* __restrict__ frq, int* __restrict__ upk) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int i = perm ? perm[s] : s;
+  float3 r = crd[i];
+  float q = charge[i];
+  pos[s] = make_float4(r.x, r.y, r.z, q);
+  if (type_sorted) type_sorted[s] = type[i];
+  int ux, uy, uz;
+  float fx, fy, fz;
+  pme_base(r, g.rcell, g.K0, g.K1, g.K2, ux, uy, uz, fx, fy, fz);
+  int t = ((ux / g.T) * g.nt1 + (uy / g.T)) * g.nt2 + (uz / g.T);
+  atom_tile[s] = t;
+  atom_slot[s] = atomicAdd(&tile_count[t], 1);
+  frq[s] = make_float4(fx, fy, fz, q);
+  upk[s] = pack_u(ux, uy, uz);
+}
+
+// Scatter into tile order; the tile counters are cleared for the next step.
 __global__ void k_pme_scatter(int n, const int* __restrict__ atom_tile,
                               const int* __restrict__ atom_slot,
                               const int* __restrict__ tile_start,
                               const float4* __restrict__ frq,
                               const int* __restrict__ upk, float4* __restrict__ binned,
-                              int* __restrict__ binned_u) {
+                              int* __restrict__ binned_u, int* __restrict__ tile_count,
+                              int ntiles) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int t = i; t < ntiles; t += gridDim.x * blockDim.x) tile_count[t] = 0;
   if (i >= n) return;
   int d = tile_start[atom_tile[i]] + atom_slot[i];
   binned[d] = frq[i];
@@ -191,8 +220,22 @@ __device__ __forceinline__ int stencil_mask(int u, int K, int lo, int hi) {
 constexpr int kTile = 8;
 constexpr int kTile3 = kTile * kTile * kTile;
 
-// One CTA per tile.  src_bins[d][t] = {count, b0, b1, b2} lists the bins along
-// axis d whose atoms reach tile t.
+// One CTA per 8x8x8 tile of the charge grid.  src{0,1,2}[t] = {count, b0,
+// b1, b2} lists the bins along each axis whose atoms reach tile t.  A warp
+// takes one atom at a time; its 32 lanes cover the (oy, oz) stencil offsets
+// and half of the ox offsets, so two passes place the 64 weights; offsets
+// falling outside the tile are skipped, whole atoms whose stencil misses the
+// tile are skipped by the warp at once.  Accumulation is int32 fixed point
+// (2^22 per charge unit) in shared memory, then the tile is stored once.
+__device__ __forceinline__ float bspline_k(float x, int k) {
+  const float x2 = x * x, x3 = x2 * x;
+  const float w0 = 0.16666667f * x3;
+  const float w1 = -0.5f * x3 + 0.5f * x2 + 0.5f * x + 0.16666667f;
+  const float w2 = 0.5f * x3 - x2 + 0.66666667f;
+  const float w3 = -0.16666667f * x3 + 0.5f * x2 - 0.5f * x + 0.16666667f;
+  return k == 0 ? w0 : (k == 1 ? w1 : (k == 2 ? w2 : w3));
+}
+
 __global__ void __launch_bounds__(256)
 k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
              const float4* __restrict__ binned, const int* __restrict__ binned_u,
@@ -206,6 +249,9 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
   const int lo2 = t2 * g.T, hi2 = min(lo2 + g.T, g.K2);
   for (int k = threadIdx.x; k < kTile3; k += blockDim.x) sq[k] = 0;
   __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int oz = lane & 3, oy = (lane >> 2) & 3, oxl = lane >> 4;
   const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
   const int b0[3] = {s0.y, s0.z, s0.w};
   const int b1[3] = {s1.y, s1.z, s1.w};
@@ -213,41 +259,30 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
   for (int a = 0; a < s0.x; ++a)
     for (int b = 0; b < s1.x; ++b)
       for (int c = 0; c < s2.x; ++c) {
-        int bin = (b0[a] * g.nt1 + b1[b]) * g.nt2 + b2[c];
-        int beg = tile_start[bin], end = tile_start[bin + 1];
-        for (int k = beg + threadIdx.x; k < end; k += blockDim.x) {
-          float4 f = binned[k];
-          int up = binned_u[k];
-          int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
-          int mx = stencil_mask(ux, g.K0, lo0, hi0);
-          int my = stencil_mask(uy, g.K1, lo1, hi1);
-          int mz = stencil_mask(uz, g.K2, lo2, hi2);
-          if (!mx || !my || !mz) continue;
-          float wx[4], wy[4], wz[4];
-          bspline4(f.x, wx);
-          bspline4(f.y, wy);
-          bspline4(f.z, wz);
+        const int bin = (b0[a] * g.nt1 + b1[b]) * g.nt2 + b2[c];
+        const int beg = tile_start[bin], end = tile_start[bin + 1];
+        for (int k = beg + warp; k < end; k += nwarps) {
+          const float4 f = binned[k];
+          const int up = binned_u[k];
+          const int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
+          const int mx = stencil_mask(ux, g.K0, lo0, hi0);
+          const int my = stencil_mask(uy, g.K1, lo1, hi1);
+          const int mz = stencil_mask(uz, g.K2, lo2, hi2);
+          if (!mx || !my || !mz) continue;  // same for the whole warp
+          if (!((my >> oy) & (mz >> oz) & 1)) continue;
+          int py = uy - oy;
+          py += py < 0 ? g.K1 : 0;
+          int pz = uz - oz;
+          pz += pz < 0 ? g.K2 : 0;
+          const float qyz = f.w * bspline_k(f.y, oy) * bspline_k(f.z, oz);
 #pragma unroll
-          for (int ox = 0; ox < 4; ++ox) {
-            if (!(mx >> ox & 1)) continue;
+          for (int pass = 0; pass < 2; ++pass) {
+            const int ox = 2 * pass + oxl;
+            if (!((mx >> ox) & 1)) continue;
             int px = ux - ox;
             px += px < 0 ? g.K0 : 0;
-            float qx = f.w * wx[ox];
-#pragma unroll
-            for (int oy = 0; oy < 4; ++oy) {
-              if (!(my >> oy & 1)) continue;
-              int py = uy - oy;
-              py += py < 0 ? g.K1 : 0;
-              float qxy = qx * wy[oy];
-#pragma unroll
-              for (int oz = 0; oz < 4; ++oz) {
-                if (!(mz >> oz & 1)) continue;
-                int pz = uz - oz;
-                pz += pz < 0 ? g.K2 : 0;
-                int loc = ((px - lo0) * kTile + (py - lo1)) * kTile + (pz - lo2);
-                atomicAdd(&sq[loc], __float2int_rn(qxy * wz[oz] * kGridScale));
-              }
-            }
+            const int loc = ((px - lo0) * kTile + (py - lo1)) * kTile + (pz - lo2);
+            atomicAdd(&sq[loc], __float2int_rn(qyz * bspline_k(f.x, ox) * kGridScale));
           }
         }
       }
@@ -534,6 +569,7 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
   SNB_CUDA_TRY(cudaMalloc(&p.d_phi, sizeof(float) * p.nall));
   SNB_CUDA_TRY(cudaMemset(p.d_phi, 0, sizeof(float) * p.nall));
   SNB_CUDA_TRY(cudaMalloc(&p.d_tile_count, sizeof(int) * p.ntiles));
+  SNB_CUDA_TRY(cudaMemset(p.d_tile_count, 0, sizeof(int) * p.ntiles));
   SNB_CUDA_TRY(cudaMalloc(&p.d_tile_start, sizeof(int) * (p.ntiles + 1)));
   SNB_CUDA_TRY(cudaMalloc(&p.d_atom_tile, sizeof(int) * n));
   SNB_CUDA_TRY(cudaMalloc(&p.d_atom_slot, sizeof(int) * n));
@@ -545,6 +581,7 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
   SNB_CUDA_TRY(cudaMalloc(&p.d_partial, sizeof(double) * 8 * p.partial_blocks));
   SNB_CUDA_TRY(cudaMalloc(&p.d_sums, sizeof(double) * 8));
   SNB_CUDA_TRY(cudaMemset(p.d_sums, 0, sizeof(double) * 8));
+  if (scan_reserve(p.scan, p.ntiles)) return kCudaError;
   if (cufftPlan3d(&p.plan_r2c, p.K[0], p.K[1], p.K[2], CUFFT_R2C) != CUFFT_SUCCESS ||
       cufftPlan3d(&p.plan_c2r, p.K[0], p.K[1], p.K[2], CUFFT_C2R) != CUFFT_SUCCESS)
     return fail(kCudaError, "PME: cuFFT plan creation failed");
@@ -573,30 +610,41 @@ void pme_free(PME& p) {
   p = PME();
 }
 
-int pme_reciprocal(PME& p, const float4* pos, int n, Accumulators& acc, int accum,
-                   bool need_energy, bool need_virial, cudaStream_t st) {
+// Binning from caller-frame coordinates through a permutation, fused with
+// the pack of the pair kernel's input (pos, type_sorted may be null).
+int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const int* type,
+                 const int* perm, float4* pos, int* type_sorted, cudaStream_t st) {
   if (n != p.n) return fail(kBadInput, "PME: atom count differs from Initial");
+  TileGeom g{p.K[0], p.K[1], p.K[2], p.T, p.nt[0], p.nt[1], p.nt[2], p.rcell};
+  k_pack_pme_bin<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, charge, type, perm, pos,
+                                                   type_sorted, g, p.d_atom_tile,
+                                                   p.d_atom_slot, p.d_tile_count, p.d_frq,
+                                                   p.d_upk);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+// Everything after binning: spread, FFT, influence / energy / virial, FFT,
+// gather into acc (index = the frame the atoms were binned in).
+int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
+                  bool need_virial, cudaStream_t st) {
   TileGeom g{p.K[0], p.K[1], p.K[2], p.T, p.nt[0], p.nt[1], p.nt[2], p.rcell};
   if (cufftSetStream(p.plan_r2c, st) != CUFFT_SUCCESS ||
       cufftSetStream(p.plan_c2r, st) != CUFFT_SUCCESS)
     return fail(kCudaError, "PME: cufftSetStream failed");
-  SNB_CUDA_TRY(cudaMemsetAsync(p.d_tile_count, 0, sizeof(int) * p.ntiles, st));
-  k_pme_bin<<<ceil_div(n, 256), 256, 0, st>>>(n, pos, g, p.d_atom_tile, p.d_atom_slot,
-                                              p.d_tile_count, p.d_frq, p.d_upk);
   if (accum == kAccumFixed) {
     int rc = scan_exclusive(p.d_tile_count, p.d_tile_start, p.ntiles, nullptr, p.scan,
                             st);
     if (rc) return rc;
     k_pme_scatter<<<ceil_div(n, 256), 256, 0, st>>>(
-        n, p.d_atom_tile, p.d_atom_slot, p.d_tile_start, p.d_frq, p.d_upk,
-        p.d_binned, p.d_binned_u);
-    k_pme_spread<<<p.ntiles, 256, 0, st>>>(g, p.d_tile_start, p.d_binned,
-                                           p.d_binned_u, p.d_src[0], p.d_src[1],
-                                           p.d_src[2], p.d_Q);
+        n, p.d_atom_tile, p.d_atom_slot, p.d_tile_start, p.d_frq, p.d_upk, p.d_binned,
+        p.d_binned_u, p.d_tile_count, p.ntiles);
+    k_pme_spread<<<p.ntiles, 256, 0, st>>>(g, p.d_tile_start, p.d_binned, p.d_binned_u,
+                                           p.d_src[0], p.d_src[1], p.d_src[2], p.d_Q);
   } else {
     SNB_CUDA_TRY(cudaMemsetAsync(p.d_Q, 0, sizeof(float) * p.nall, st));
-    k_pme_spread_atomic<<<ceil_div(n, 16), 256, 0, st>>>(n, p.d_frq, p.d_upk, g,
-                                                         p.d_Q);
+    SNB_CUDA_TRY(cudaMemsetAsync(p.d_tile_count, 0, sizeof(int) * p.ntiles, st));
+    k_pme_spread_atomic<<<ceil_div(n, 16), 256, 0, st>>>(n, p.d_frq, p.d_upk, g, p.d_Q);
   }
   if (cufftExecR2C(p.plan_r2c, p.d_Q, p.d_FQ) != CUFFT_SUCCESS)
     return fail(kCudaError, "PME: cufftExecR2C failed");
@@ -615,19 +663,28 @@ int pme_reciprocal(PME& p, const float4* pos, int n, Accumulators& acc, int accu
     k_pme_influence<false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
         p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy);
   if (need_energy || need_virial)
-    k_pme_finish<<<1, 1024, 0, st>>>(p.partial_blocks, p.d_partial, pos, n,
+    k_pme_finish<<<1, 1024, 0, st>>>(p.partial_blocks, p.d_partial, p.d_frq, n,
                                      (double)p.beta, p.volume, p.d_sums, need_energy);
   if (cufftExecC2R(p.plan_c2r, p.d_FQ, p.d_phi) != CUFFT_SUCCESS)
     return fail(kCudaError, "PME: cufftExecC2R failed");
   const float scale = (float)p.update_interval;
   if (accum == kAccumFixed)
-    k_pme_gather<kAccumFixed><<<ceil_div(n, 64), 256, 0, st>>>(n, p.d_frq, p.d_upk,
-                                                               g, p.d_phi, scale, acc);
+    k_pme_gather<kAccumFixed><<<ceil_div(n, 64), 256, 0, st>>>(n, p.d_frq, p.d_upk, g,
+                                                               p.d_phi, scale, acc);
   else
-    k_pme_gather<kAccumFloat><<<ceil_div(n, 64), 256, 0, st>>>(n, p.d_frq, p.d_upk,
-                                                               g, p.d_phi, scale, acc);
+    k_pme_gather<kAccumFloat><<<ceil_div(n, 64), 256, 0, st>>>(n, p.d_frq, p.d_upk, g,
+                                                               p.d_phi, scale, acc);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
+}
+
+int pme_reciprocal(PME& p, const float4* pos, int n, Accumulators& acc, int accum,
+                   bool need_energy, bool need_virial, cudaStream_t st) {
+  if (n != p.n) return fail(kBadInput, "PME: atom count differs from Initial");
+  TileGeom g{p.K[0], p.K[1], p.K[2], p.T, p.nt[0], p.nt[1], p.nt[2], p.rcell};
+  k_pme_bin<<<ceil_div(n, 256), 256, 0, st>>>(n, pos, g, p.d_atom_tile, p.d_atom_slot,
+                                              p.d_tile_count, p.d_frq, p.d_upk);
+  return pme_after_bin(p, n, acc, accum, need_energy, need_virial, st);
 }
 
 // ---------------------------------------------------------------------------

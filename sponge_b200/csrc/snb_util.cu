@@ -88,8 +88,45 @@ __global__ void k_scan_add(int* out, int n, const int* block_sums) {
   if (i < n) out[i] += block_sums[blockIdx.x];
 }
 
+int scan_reserve(ScanScratch& s, int n) {
+  int nb = ceil_div(n > 0 ? n : 1, kScanBlock);
+  if (nb > s.capacity_blocks) {
+    if (s.block_sums) cudaFree(s.block_sums);
+    SNB_CUDA_TRY(cudaMalloc(&s.block_sums, sizeof(int) * nb));
+    s.capacity_blocks = nb;
+  }
+  return kOk;
+}
+
+// One block scans everything in chunks (short arrays: one launch instead of 3).
+__global__ void k_scan_single(const int* in, int* out, int n, int* total_out) {
+  __shared__ int sh[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    int v = i < n ? in[i] : 0;
+    int tot;
+    int ex = block_scan_exclusive(v, sh, &tot);
+    if (i < n) out[i] = ex + carry;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[n] = carry;
+    if (total_out) *total_out = carry;
+  }
+}
+
 int scan_exclusive(const int* in, int* out, int n, int* total_out,
                    ScanScratch& s, cudaStream_t st) {
+  if (n <= 16 * kScanBlock) {
+    k_scan_single<<<1, kScanBlock, 0, st>>>(in, out, n, total_out);
+    SNB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+  }
   int nb = ceil_div(n > 0 ? n : 1, kScanBlock);
   if (nb > s.capacity_blocks) {
     if (s.block_sums) cudaFree(s.block_sums);

@@ -127,6 +127,39 @@ def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
     return R
 
 
+def _orient_waters(rng, o_pos, kind, box, h_clash=1.6, max_rounds=200):
+    """Uniformly random orientations, redrawn for the molecules whose H atoms
+    come closer than `h_clash` A to an atom of another molecule (rejection
+    sampling: orientations stay uniform, conditioned on no such clash)."""
+    from scipy.spatial import cKDTree
+    n = len(o_pos)
+    half = ANGLE_T0 / 2
+    h_local = np.array([[math.sin(half), 0.0, math.cos(half)],
+                        [-math.sin(half), 0.0, math.cos(half)]]) * BOND_R0
+    h_pos = o_pos[:, None, :] + np.einsum("nij,kj->nki",
+                                          _random_rotations(rng, n), h_local)
+    water = kind == 0
+    mol = np.repeat(np.arange(n), 3)
+    for _ in range(max_rounds):
+        pts = np.concatenate([o_pos[:, None, :], h_pos], 1).reshape(-1, 3)
+        is_h = np.tile([False, True, True], n)
+        live = np.repeat(water, 3) | (np.tile([True, False, False], n))
+        idx = np.nonzero(live)[0]
+        tree = cKDTree(np.mod(pts[idx], box), boxsize=box)
+        pairs = tree.query_pairs(h_clash, output_type="ndarray")
+        if len(pairs) == 0:
+            break
+        a, b = idx[pairs[:, 0]], idx[pairs[:, 1]]
+        bad = (mol[a] != mol[b]) & (is_h[a] | is_h[b])
+        redo = np.unique(np.concatenate([mol[a[bad & is_h[a]]], mol[b[bad & is_h[b]]]]))
+        redo = redo[water[redo]]
+        if len(redo) == 0:
+            break
+        h_pos[redo] = o_pos[redo, None, :] + np.einsum(
+            "nij,kj->nki", _random_rotations(rng, len(redo)), h_local)
+    return h_pos
+
+
 def ion_pairs_for(box: float, molarity: float = 0.15) -> int:
     return int(round(molarity * box ** 3 * 1e-27 * AVOGADRO))
 
@@ -136,7 +169,9 @@ def water_box(n_waters: int, seed: int = 0, ion_pairs: int | None = 0,
     """Flexible 3-site water on a jittered cubic lattice, optional NaCl.
 
     ``ion_pairs=None`` means 0.15 M NaCl for the box volume.  Ions replace
-    randomly chosen waters (the ion sits at the oxygen site).
+    randomly chosen waters (the ion sits at the oxygen site).  Orientations
+    are uniformly random, redrawn where a hydrogen would sit within 1.6 A of
+    another molecule.
     """
     rng = np.random.default_rng(seed)
     if box is None:
@@ -150,16 +185,12 @@ def water_box(n_waters: int, seed: int = 0, ion_pairs: int | None = 0,
     iy, iz = np.divmod(rem, n_side)
     o_pos = (np.stack([ix, iy, iz], 1) + 0.5) * spacing
     o_pos += rng.uniform(-0.3, 0.3, size=o_pos.shape)
-    rot = _random_rotations(rng, n_waters)
-    half = ANGLE_T0 / 2
-    h_local = np.array([[math.sin(half), 0.0, math.cos(half)],
-                        [-math.sin(half), 0.0, math.cos(half)]]) * BOND_R0
-    h_pos = o_pos[:, None, :] + np.einsum("nij,kj->nki", rot, h_local)
     kind = np.zeros(n_waters, np.int8)          # 0 water, 1 Na, 2 Cl
     if ion_pairs:
         pick = rng.choice(n_waters, size=2 * ion_pairs, replace=False)
         kind[pick[:ion_pairs]] = 1
         kind[pick[ion_pairs:]] = 2
+    h_pos = _orient_waters(rng, o_pos, kind, box)
 
     crd, typ, chg, mass = [], [], [], []
     excl = []

@@ -93,7 +93,7 @@ def test_graph_replay_is_bitwise_identical(g, box_9k):
 def test_nve_energy_is_conserved(g, oracle, small_box):
     """100 leap-frog steps at 0.5 fs from the unrelaxed lattice start: the
     total energy (kinetic from the mid-step velocity average) moves by less
-    than 1% of the potential energy."""
+    than 2% of the kinetic energy."""
     import copy
     import torch
     from sponge_b200 import systems
@@ -131,4 +131,4 @@ def test_nve_energy_is_conserved(g, oracle, small_box):
     e_start = e0p + k0
     e_end = p1 + k1
     assert np.isfinite(e_end)
-    assert abs(e_end - e_start) <= 1e-2 * abs(e0p)
+    assert abs(e_end - e_start) <= 2e-2 * k0
