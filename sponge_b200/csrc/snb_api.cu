@@ -938,7 +938,10 @@ static int capture_conditional_rebuild(snb_engine* e, const float* crd, cudaStre
   e->body_kernels = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType t;
-    SNB_CUDA_TRY(cudaGraphNodeGetType(nd, &t));
+    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
     e->body_kernels += t == cudaGraphNodeTypeKernel;
   }
   return kOk;
@@ -1233,7 +1236,10 @@ extern "C" int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
     int k = 0;
     for (auto nd : nodes) {
       cudaGraphNodeType t;
-      SNB_CUDA_TRY(cudaGraphNodeGetType(nd, &t));
+      if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) {
+        cudaGetLastError();  // node types this runtime cannot name: not kernels
+        continue;
+      }
       k += t == cudaGraphNodeTypeKernel;
     }
     *out = k;

@@ -121,12 +121,17 @@ __device__ __forceinline__ double warp_sum(double v) {
 // erfc(x) and exp(-x^2) together for x >= 0.  erfcx(x) = erfc(x) e^{x^2} is
 // a degree-8 polynomial in t = 1/(1 + x/2) on [0, 4] (weighted least-squares
 // fit, csrc/fit_erfcx.py; max relative error 3.3e-7 in float32), so
-// erfc(x) = P(t) * exp(-x^2).  Beyond x = 4 CUDA's erfcf is used.
+// erfc(x) = P(t) * exp(-x^2).  exp uses the hardware exp2 (__expf: error
+// 2 + 1.16|x^2| ulp, below 1e-6 relative for x <= 4); t uses the correctly
+// rounded reciprocal.  Beyond x = 4 CUDA's erfcf / expf are used.
 __device__ __forceinline__ float erfc_and_exp(float x, float* e_out) {
-  const float e = expf(-x * x);
+  if (x > 4.0f) {
+    *e_out = expf(-x * x);
+    return erfcf(x);
+  }
+  const float e = __expf(-x * x);
   *e_out = e;
-  if (x > 4.0f) return erfcf(x);
-  const float t = 1.0f / (1.0f + 0.5f * x);
+  const float t = __frcp_rn(1.0f + 0.5f * x);
   float p = -0.049221702f;
   p = fmaf(p, t, 0.33589873f);
   p = fmaf(p, t, -0.88379663f);
@@ -137,6 +142,22 @@ __device__ __forceinline__ float erfc_and_exp(float x, float* e_out) {
   p = fmaf(p, t, 0.2896666f);
   p = fmaf(p, t, -0.00045567533f);
   return p * e;
+}
+
+// atomicAdd(&counter[key], 1) with the lanes of a warp that share the same
+// key served by one atomic (leader adds the group size, ranks follow lane
+// order).  Call with all lanes of the warp active.
+__device__ __forceinline__ int warp_aggregated_inc(int* counter, int key, bool active) {
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  if (!active) return 0;
+  const unsigned peers = __match_any_sync(act, key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  const int rank = __popc(peers & ((1u << lane) - 1u));
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&counter[key], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + rank;
 }
 
 // Ceiling division for launch shapes.

@@ -78,11 +78,11 @@ constexpr int kQueue = 64;
 template <int ACCUM, bool ENERGY, bool VIRIAL>
 __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
                                         const float* sA, const float* sB, int ti,
-                                        float qi, int gi, float4 e, int j, float& fx,
-                                        float& fy, float& fz, float& e_lj, float& e_c,
-                                        float* vir) {
+                                        float qi, int gi, float4 e, int j, int tj,
+                                        float& fx, float& fy, float& fz, float& e_lj,
+                                        float& e_c, float* vir) {
   const float r2 = e.x * e.x + e.y * e.y + e.z * e.z;
-  const int p = lj_pair_index(ti, a.type[j]);
+  const int p = lj_pair_index(ti, tj);
   const float A = sA[p], B = sB[p];
   const float rinv = rsqrtf(r2);
   const float r = r2 * rinv;
@@ -131,11 +131,11 @@ __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
 }
 
 template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_lj_direct(PairArgs a, Accumulators acc) {
   extern __shared__ float sh_tab[];
   __shared__ float4 sq[kWarps][kQueue];   // dx, dy, dz, q_j
-  __shared__ int sj[kWarps][kQueue];      // j
+  __shared__ int2 sj[kWarps][kQueue];     // j, LJ type of j
   float* sA = sh_tab;
   float* sB = sh_tab + a.n_types * (a.n_types + 1) / 2;
   const int npair = a.n_types * (a.n_types + 1) / 2;
@@ -159,44 +159,65 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   const int k0 = a.row_start[i], k1 = a.row_start[i + 1];
   const unsigned lt = (1u << lane) - 1u;
   int count = 0;
-  for (int base = k0; base < k1; base += 32) {
-    const int k = base + lane;
-    bool in = false;
-    int j = 0;
-    float4 ent;
-    if (k < k1) {
-      j = a.cols[k];
-      const float4 pj = a.pos[j];
-      const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri,
-                                              a.cell, a.rcell);
-      const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
-      in = r2 < a.cutoff2;
-      ent = make_float4(dr.x, dr.y, dr.z, pj.w);
+  // Four candidates per lane per round: their index loads, then their
+  // coordinate gathers, are all in flight together.
+  constexpr int U = 4;
+  for (int base = k0; base < k1; base += 32 * U) {
+    int jj[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = base + 32 * u + lane;
+      jj[u] = k < k1 ? a.cols[k] : -1;
     }
-    const unsigned m = __ballot_sync(0xffffffffu, in);
-    if (in) {
-      const int slot = count + __popc(m & lt);
-      sq[w][slot] = ent;
-      sj[w][slot] = j;
-    }
-    count += __popc(m);
-    if (count >= 32) {
-      __syncwarp();
-      lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi, sq[w][lane],
-                                     sj[w][lane], fx, fy, fz, e_lj, e_c, vir);
-      __syncwarp();
-      if (lane < count - 32) {
-        sq[w][lane] = sq[w][32 + lane];
-        sj[w][lane] = sj[w][32 + lane];
+    float4 pp[U];
+    int tt[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (jj[u] >= 0) {
+        pp[u] = a.pos[jj[u]];
+        tt[u] = a.type[jj[u]];
       }
-      __syncwarp();
-      count -= 32;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (base + 32 * u >= k1) break;  // warp-uniform
+      bool in = false;
+      float4 ent;
+      if (jj[u] >= 0) {
+        const float3 dr = min_image_fast<ORTHO>(make_float3(pp[u].x, pp[u].y, pp[u].z),
+                                                ri, a.cell, a.rcell);
+        const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+        in = r2 < a.cutoff2;
+        ent = make_float4(dr.x, dr.y, dr.z, pp[u].w);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, in);
+      if (in) {
+        const int slot = count + __popc(m & lt);
+        sq[w][slot] = ent;
+        sj[w][slot] = make_int2(jj[u], tt[u]);
+      }
+      count += __popc(m);
+      if (count >= 32) {
+        __syncwarp();
+        const int2 jt = sj[w][lane];
+        lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi, sq[w][lane], jt.x,
+                                       jt.y, fx, fy, fz, e_lj, e_c, vir);
+        __syncwarp();
+        if (lane < count - 32) {
+          sq[w][lane] = sq[w][32 + lane];
+          sj[w][lane] = sj[w][32 + lane];
+        }
+        __syncwarp();
+        count -= 32;
+      }
     }
   }
   __syncwarp();
-  if (lane < count)
-    lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi, sq[w][lane],
-                                   sj[w][lane], fx, fy, fz, e_lj, e_c, vir);
+  if (lane < count) {
+    const int2 jt = sj[w][lane];
+    lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi, sq[w][lane], jt.x, jt.y,
+                                   fx, fy, fz, e_lj, e_c, vir);
+  }
   fx = warp_sum(fx);
   fy = warp_sum(fy);
   fz = warp_sum(fz);

@@ -156,20 +156,30 @@ __global__ void k_pack_pme_bin(int n, const float3* __restrict__ crd,
                                int* __restrict__ atom_slot, int* __restrict__ tile_count,
                                float4* __restrict__ frq, int* __restrict__ upk) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  int i = perm ? perm[s] : s;
-  float3 r = crd[i];
-  float q = charge[i];
-  pos[s] = make_float4(r.x, r.y, r.z, q);
-  if (type_sorted) type_sorted[s] = type[i];
-  int ux, uy, uz;
-  float fx, fy, fz;
-  pme_base(r, g.rcell, g.K0, g.K1, g.K2, ux, uy, uz, fx, fy, fz);
-  int t = ((ux / g.T) * g.nt1 + (uy / g.T)) * g.nt2 + (uz / g.T);
+  const bool active = s < n;
+  int t = 0;
+  float4 fr4;
+  int up = 0;
+  if (active) {
+    int i = perm ? perm[s] : s;
+    float3 r = crd[i];
+    float q = charge[i];
+    pos[s] = make_float4(r.x, r.y, r.z, q);
+    if (type_sorted) type_sorted[s] = type[i];
+    int ux, uy, uz;
+    float fx, fy, fz;
+    pme_base(r, g.rcell, g.K0, g.K1, g.K2, ux, uy, uz, fx, fy, fz);
+    t = ((ux / g.T) * g.nt1 + (uy / g.T)) * g.nt2 + (uz / g.T);
+    fr4 = make_float4(fx, fy, fz, q);
+    up = pack_u(ux, uy, uz);
+  }
+  // sorted neighbours share tiles: one atomic per tile per warp
+  const int slot = warp_aggregated_inc(tile_count, t, active);
+  if (!active) return;
   atom_tile[s] = t;
-  atom_slot[s] = atomicAdd(&tile_count[t], 1);
-  frq[s] = make_float4(fx, fy, fz, q);
-  upk[s] = pack_u(ux, uy, uz);
+  atom_slot[s] = slot;
+  frq[s] = fr4;
+  upk[s] = up;
 }
 
 // Scatter into tile order; the tile counters are cleared for the next step.
@@ -221,19 +231,41 @@ constexpr int kTile = 8;
 constexpr int kTile3 = kTile * kTile * kTile;
 
 // One CTA per 8x8x8 tile of the charge grid.  src{0,1,2}[t] = {count, b0,
-// b1, b2} lists the bins along each axis whose atoms reach tile t.  A warp
-// takes one atom at a time; its 32 lanes cover the (oy, oz) stencil offsets
-// and half of the ox offsets, so two passes place the 64 weights; offsets
-// falling outside the tile are skipped, whole atoms whose stencil misses the
-// tile are skipped by the warp at once.  Accumulation is int32 fixed point
-// (2^22 per charge unit) in shared memory, then the tile is stored once.
-__device__ __forceinline__ float bspline_k(float x, int k) {
-  const float x2 = x * x, x3 = x2 * x;
-  const float w0 = 0.16666667f * x3;
-  const float w1 = -0.5f * x3 + 0.5f * x2 + 0.5f * x + 0.16666667f;
-  const float w2 = 0.5f * x3 - x2 + 0.66666667f;
-  const float w3 = -0.16666667f * x3 + 0.5f * x2 - 0.5f * x + 0.16666667f;
-  return k == 0 ? w0 : (k == 1 ? w1 : (k == 2 ? w2 : w3));
+// b1, b2} lists the bins along each axis whose atoms reach tile t.
+// Phase 1: every thread takes atoms of those bins, tests whether the atom's
+// 4x4x4 stencil meets the tile and, if so, appends its 12 weights (charge
+// folded into the x weights), base point and per-axis masks to a list in
+// shared memory.  Phase 2: a warp takes one listed atom at a time, its 32
+// lanes cover the (oy, oz) offsets and half of the ox offsets, so two passes
+// place the 64 products.  Accumulation is int32 fixed point (2^22 per charge
+// unit) in shared memory; the tile is stored once.  Atoms beyond the list
+// capacity are spread by their own thread in phase 1.
+constexpr int kSpreadList = 512;
+
+__device__ __forceinline__ void spread_one(int* sq, float4 f, int ux, int uy, int uz,
+                                           int mx, int my, int mz, const TileGeom& g,
+                                           int lo0, int lo1, int lo2) {
+  float wx[4], wy[4], wz[4];
+  bspline4(f.x, wx);
+  bspline4(f.y, wy);
+  bspline4(f.z, wz);
+  for (int ox = 0; ox < 4; ++ox) {
+    if (!((mx >> ox) & 1)) continue;
+    int px = ux - ox;
+    px += px < 0 ? g.K0 : 0;
+    for (int oy = 0; oy < 4; ++oy) {
+      if (!((my >> oy) & 1)) continue;
+      int py = uy - oy;
+      py += py < 0 ? g.K1 : 0;
+      for (int oz = 0; oz < 4; ++oz) {
+        if (!((mz >> oz) & 1)) continue;
+        int pz = uz - oz;
+        pz += pz < 0 ? g.K2 : 0;
+        atomicAdd(&sq[((px - lo0) * kTile + (py - lo1)) * kTile + (pz - lo2)],
+                  __float2int_rn(f.w * wx[ox] * wy[oy] * wz[oz] * kGridScale));
+      }
+    }
+  }
 }
 
 __global__ void __launch_bounds__(256)
@@ -242,16 +274,17 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
              const int4* __restrict__ src0, const int4* __restrict__ src1,
              const int4* __restrict__ src2, float* __restrict__ Q) {
   __shared__ int sq[kTile3];
+  __shared__ float sw[kSpreadList][12];
+  __shared__ int2 su[kSpreadList];  // {packed base point, masks x | y<<4 | z<<8}
+  __shared__ int scount;
   const int t = blockIdx.x;
   const int t2 = t % g.nt2, t1 = (t / g.nt2) % g.nt1, t0 = t / (g.nt1 * g.nt2);
   const int lo0 = t0 * g.T, hi0 = min(lo0 + g.T, g.K0);
   const int lo1 = t1 * g.T, hi1 = min(lo1 + g.T, g.K1);
   const int lo2 = t2 * g.T, hi2 = min(lo2 + g.T, g.K2);
   for (int k = threadIdx.x; k < kTile3; k += blockDim.x) sq[k] = 0;
+  if (threadIdx.x == 0) scount = 0;
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const int oz = lane & 3, oy = (lane >> 2) & 3, oxl = lane >> 4;
   const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
   const int b0[3] = {s0.y, s0.z, s0.w};
   const int b1[3] = {s1.y, s1.z, s1.w};
@@ -261,31 +294,58 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
       for (int c = 0; c < s2.x; ++c) {
         const int bin = (b0[a] * g.nt1 + b1[b]) * g.nt2 + b2[c];
         const int beg = tile_start[bin], end = tile_start[bin + 1];
-        for (int k = beg + warp; k < end; k += nwarps) {
-          const float4 f = binned[k];
+        for (int k = beg + threadIdx.x; k < end; k += blockDim.x) {
           const int up = binned_u[k];
           const int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
           const int mx = stencil_mask(ux, g.K0, lo0, hi0);
           const int my = stencil_mask(uy, g.K1, lo1, hi1);
           const int mz = stencil_mask(uz, g.K2, lo2, hi2);
-          if (!mx || !my || !mz) continue;  // same for the whole warp
-          if (!((my >> oy) & (mz >> oz) & 1)) continue;
-          int py = uy - oy;
-          py += py < 0 ? g.K1 : 0;
-          int pz = uz - oz;
-          pz += pz < 0 ? g.K2 : 0;
-          const float qyz = f.w * bspline_k(f.y, oy) * bspline_k(f.z, oz);
+          if (!mx || !my || !mz) continue;
+          const float4 f = binned[k];
+          const int slot = atomicAdd(&scount, 1);
+          if (slot < kSpreadList) {
+            float w[4];
+            bspline4(f.x, w);
 #pragma unroll
-          for (int pass = 0; pass < 2; ++pass) {
-            const int ox = 2 * pass + oxl;
-            if (!((mx >> ox) & 1)) continue;
-            int px = ux - ox;
-            px += px < 0 ? g.K0 : 0;
-            const int loc = ((px - lo0) * kTile + (py - lo1)) * kTile + (pz - lo2);
-            atomicAdd(&sq[loc], __float2int_rn(qyz * bspline_k(f.x, ox) * kGridScale));
+            for (int q = 0; q < 4; ++q) sw[slot][q] = f.w * w[q];
+            bspline4(f.y, w);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sw[slot][4 + q] = w[q];
+            bspline4(f.z, w);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sw[slot][8 + q] = w[q];
+            su[slot] = make_int2(up, mx | (my << 4) | (mz << 8));
+          } else {
+            spread_one(sq, f, ux, uy, uz, mx, my, mz, g, lo0, lo1, lo2);
           }
         }
       }
+  __syncthreads();
+  const int nlist = min(scount, kSpreadList);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int oz = lane & 3, oy = (lane >> 2) & 3, oxl = lane >> 4;
+  for (int a = warp; a < nlist; a += nwarps) {
+    const int2 e = su[a];
+    const int mx = e.y & 15, my = (e.y >> 4) & 15, mz = (e.y >> 8) & 15;
+    if (!((my >> oy) & (mz >> oz) & 1)) continue;
+    const int ux = e.x >> 20, uy = (e.x >> 10) & 1023, uz = e.x & 1023;
+    int py = uy - oy;
+    py += py < 0 ? g.K1 : 0;
+    int pz = uz - oz;
+    pz += pz < 0 ? g.K2 : 0;
+    const float wyz = sw[a][4 + oy] * sw[a][8 + oz];
+    const int base = (py - lo1) * kTile + (pz - lo2);
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass) {
+      const int ox = 2 * pass + oxl;
+      if (!((mx >> ox) & 1)) continue;
+      int px = ux - ox;
+      px += px < 0 ? g.K0 : 0;
+      atomicAdd(&sq[(px - lo0) * kTile * kTile + base],
+                __float2int_rn(sw[a][ox] * wyz * kGridScale));
+    }
+  }
   __syncthreads();
   const int w0 = hi0 - lo0, w1 = hi1 - lo1, w2 = hi2 - lo2;
   for (int k = threadIdx.x; k < kTile3; k += blockDim.x) {
