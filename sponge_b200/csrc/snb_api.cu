@@ -382,6 +382,7 @@ extern "C" int snb_lj_pme_direct_force(snb_lj* h, int atom_numbers, int local_n,
   a.type = h->d_type_sorted;
   a.global = nl->nl.d_global;
   a.row_start = nl->nl.d_row_start;
+  a.row_count = nl->nl.d_row_count;
   a.cols = nl->nl.d_cols;
   a.nl_flags = nl->nl.d_flags;
   a.A = h->p.d_A;
@@ -594,6 +595,7 @@ static SoftArgs soft_args(snb_lj_soft* h, snb_nl* nl, const snb_boundary& b, flo
   a.dq = h->d_dq_sorted;
   a.global = nl->nl.d_global;
   a.row_start = nl->nl.d_row_start;
+  a.row_count = nl->nl.d_row_count;
   a.cols = nl->nl.d_cols;
   a.nl_flags = nl->nl.d_flags;
   a.AA = h->d_AA;
@@ -978,6 +980,7 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   a.type = e->d_type_sorted;
   a.global = e->nl.d_global;
   a.row_start = e->nl.d_row_start;
+  a.row_count = e->nl.d_row_count;
   a.cols = e->nl.d_cols;
   a.nl_flags = e->nl.d_flags;
   a.A = e->lj.d_A;

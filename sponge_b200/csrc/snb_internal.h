@@ -75,9 +75,10 @@ struct NeighborList {
   float4* d_pos = nullptr;      // [n] sorted build-time coordinates (x,y,z,-)
   float3* d_old_crd = nullptr;  // [n] caller-frame coordinates at last build
   // list
-  int* d_row_count = nullptr;   // [n]
-  int* d_row_start = nullptr;   // [n + 1]
-  int* d_cols = nullptr;        // [cap] sorted-frame j of each pair
+  int* d_row_count = nullptr;   // [n] entries in row i
+  int* d_row_start = nullptr;   // [n + 1] = i * row_cap
+  int* d_cols = nullptr;        // [n * row_cap] sorted-frame j of each pair
+  int row_cap = 0;
   long long cap = 0;
   int* d_unsorted = nullptr;    // [n] cell-binned caller indices before ordering
   int* d_sorted_cell = nullptr;  // [n] cell of each sorted atom
@@ -156,6 +157,7 @@ struct PairArgs {
   const int* type;              // sorted LJ type
   const int* global;            // sorted -> global id (owner rule)
   const int* row_start;
+  const int* row_count;
   const int* cols;
   const int* nl_flags;          // neighbor-list flags: skip when the list overflowed
   const float* A;
@@ -176,6 +178,7 @@ struct SoftArgs {
   const float* dq;              // sorted charge_B - charge_A (may be null)
   const int* global;
   const int* row_start;
+  const int* row_count;
   const int* cols;
   const int* nl_flags;
   const float* AA;              // A' of state A, per pair of A types

@@ -27,7 +27,7 @@ namespace snb {
 
 // flags layout
 enum { kFlagNeed = 0, kFlagListOverflow = 1, kFlagTotal = 2, kFlagGeneration = 3,
-       kFlagExportOverflow = 4, kNumFlags = 8 };
+       kFlagExportOverflow = 4, kFlagMaxRow = 5, kNumFlags = 8 };
 
 // ---------------------------------------------------------------------------
 // Refresh decision (Check_Refresh, neighbor_list.cpp:307-321): any atom moved
@@ -136,8 +136,10 @@ __device__ __forceinline__ bool excluded_pair(int gl, int gh,
   return false;
 }
 
-// Pair search for sorted atom i (one warp).  PASS 0 counts, PASS 1 writes.
-template <int PASS>
+// Pair search for sorted atom i (one warp), one pass: row i has room for
+// row_cap entries at cols[i * row_cap]; hits beyond it are counted (the
+// largest row is kept in flags[kFlagMaxRow]) and raise the overflow flag so
+// the host can regrow the rows and repeat the build.
 __global__ void __launch_bounds__(256)
 k_pair_search(int n, const float4* __restrict__ pos, const int* __restrict__ global,
               const int* __restrict__ sorted_cell, const int* __restrict__ cell_start,
@@ -145,13 +147,8 @@ k_pair_search(int n, const float4* __restrict__ pos, const int* __restrict__ glo
               int max_runs, Cell cell, Cell rcell, float rl2,
               const int* __restrict__ excl_start, const int* __restrict__ excl_list,
               const int* __restrict__ excl_numbers, int* __restrict__ row_count,
-              const int* __restrict__ row_start, int* __restrict__ cols,
-              long long cap, int* flags) {
+              int row_cap, int* __restrict__ cols, int* flags) {
   if (flags[kFlagNeed] == 0) return;
-  if (PASS == 1 && (long long)flags[kFlagTotal] > cap) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) flags[kFlagListOverflow] = 1;
-    return;
-  }
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (i >= n) return;
@@ -159,8 +156,8 @@ k_pair_search(int n, const float4* __restrict__ pos, const int* __restrict__ glo
   const float3 ri = make_float3(pi4.x, pi4.y, pi4.z);
   const int gi = global[i];
   const int c = sorted_cell[i];
+  int* out_row = cols + (size_t)i * row_cap;
   int count = 0;
-  int out = PASS == 1 ? row_start[i] : 0;
   const int nr = run_count[c];
   // range list: own cell after i, then forward runs
   for (int r = -1; r < nr; ++r) {
@@ -189,15 +186,32 @@ k_pair_search(int n, const float4* __restrict__ pos, const int* __restrict__ glo
         }
       }
       unsigned m = __ballot_sync(0xffffffffu, hit);
-      if (PASS == 1 && hit) {
-        int rank = __popc(m & ((1u << lane) - 1u));
-        cols[out + rank] = j;
+      if (hit) {
+        int slot = count + __popc(m & ((1u << lane) - 1u));
+        if (slot < row_cap) out_row[slot] = j;
       }
-      out += __popc(m);
       count += __popc(m);
     }
   }
-  if (PASS == 0 && lane == 0) row_count[i] = count;
+  if (lane == 0) {
+    row_count[i] = count < row_cap ? count : row_cap;
+    atomicAdd(&flags[kFlagTotal], count);
+    if (count > row_cap) {
+      flags[kFlagListOverflow] = 1;
+      atomicMax(&flags[kFlagMaxRow], count);
+    }
+  }
+}
+
+__global__ void k_rebuild_begin(int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  flags[kFlagTotal] = 0;
+  flags[kFlagMaxRow] = 0;
+}
+
+__global__ void k_row_starts(int n, int row_cap, int* row_start) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= n) row_start[i] = i * row_cap;
 }
 
 __global__ void k_sorted_cell(int n, const int* __restrict__ perm,
@@ -338,17 +352,23 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
     SNB_CUDA_TRY(cudaMemset(nl.d_sorted_cell, 0, sizeof(int) * n));
     SNB_CUDA_TRY(cudaMemset(nl.d_pos, 0, sizeof(float4) * n));
   }
-  // Capacity estimate: half-sphere of radius rl at the box's mean density,
-  // with 30% headroom; regrown on overflow by nl_check_overflow.
+  // Row capacity: 1.5x the mean half-sphere count at the box's density plus
+  // a margin; regrown on overflow by nl_check_overflow.
   if (initial_capacity <= 0) {
     double vol = (double)nl.cell.a11 * nl.cell.a22 * nl.cell.a33;
     double rho = n / vol;
     double rl = sqrt((double)nl.rl2);
     double per = 0.5 * rho * 4.18879020478639 * rl * rl * rl;
-    initial_capacity = (long long)(1.3 * per * n) + 1024;
+    initial_capacity = (long long)(1.5 * per) + 64;
   }
-  nl.cap = initial_capacity;
+  nl.row_cap = (int)std::min<long long>(initial_capacity, n);
+  if (nl.row_cap < 32) nl.row_cap = 32;
+  nl.cap = (long long)nl.row_cap * n;
+  if (nl.cap + nl.row_cap > 2147483647LL)
+    return fail(kBadInput, "neighbor list: rows exceed 32-bit offsets");
   SNB_CUDA_TRY(cudaMalloc(&nl.d_cols, sizeof(int) * nl.cap));
+  k_row_starts<<<ceil_div(n + 1, 256), 256>>>(n, nl.row_cap, nl.d_row_start);
+  SNB_CUDA_TRY(cudaGetLastError());
   return scan_reserve(nl.scan, std::max(nl.ncell, n));
 }
 
@@ -421,6 +441,7 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   const float3* crd = reinterpret_cast<const float3*>(crd_f);
   const int n = nl.n;
   SNB_CUDA_TRY(cudaMemsetAsync(nl.d_cell_count, 0, sizeof(int) * nl.ncell, st));
+  k_rebuild_begin<<<1, 1, 0, st>>>(nl.d_flags);
   k_bin_count<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz,
                                                 nl.d_atom_cell, nl.d_atom_slot,
                                                 nl.d_cell_count, nl.d_flags);
@@ -438,17 +459,10 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
                                                   nl.d_pos, nl.d_old_crd, nl.d_flags);
   k_sorted_cell<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_perm, nl.d_atom_cell,
                                                   nl.d_sorted_cell, nl.d_flags);
-  k_pair_search<0><<<ceil_div(n, 8), 256, 0, st>>>(
+  k_pair_search<<<ceil_div(n, 8), 256, 0, st>>>(
       n, nl.d_pos, nl.d_global, nl.d_sorted_cell, nl.d_cell_start, nl.d_run_ranges,
       nl.d_run_count, nl.max_runs, nl.cell, nl.rcell, nl.rl2, excl_start, excl_list,
-      excl_numbers, nl.d_row_count, nl.d_row_start, nl.d_cols, nl.cap, nl.d_flags);
-  rc = scan_exclusive(nl.d_row_count, nl.d_row_start, n, nl.d_flags + kFlagTotal,
-                      nl.scan, st);
-  if (rc) return rc;
-  k_pair_search<1><<<ceil_div(n, 8), 256, 0, st>>>(
-      n, nl.d_pos, nl.d_global, nl.d_sorted_cell, nl.d_cell_start, nl.d_run_ranges,
-      nl.d_run_count, nl.max_runs, nl.cell, nl.rcell, nl.rl2, excl_start, excl_list,
-      excl_numbers, nl.d_row_count, nl.d_row_start, nl.d_cols, nl.cap, nl.d_flags);
+      excl_numbers, nl.d_row_count, nl.row_cap, nl.d_cols, nl.d_flags);
   k_finish_build<<<1, 1, 0, st>>>(nl.d_flags);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
@@ -461,11 +475,15 @@ int nl_check_overflow(NeighborList& nl, bool* regrown, cudaStream_t st) {
   SNB_CUDA_TRY(cudaStreamSynchronize(st));
   nl.last_total = nl.h_flags[kFlagTotal];
   if (nl.h_flags[kFlagListOverflow]) {
-    long long need = (long long)nl.h_flags[kFlagTotal];
-    long long cap = need + need / 5 + 1024;
+    long long need = nl.h_flags[kFlagMaxRow];
+    int cap = (int)std::min<long long>(need + need / 5 + 32, nl.n);
     SNB_CUDA_TRY(cudaFree(nl.d_cols));
-    SNB_CUDA_TRY(cudaMalloc(&nl.d_cols, sizeof(int) * cap));
-    nl.cap = cap;
+    nl.row_cap = std::max(cap, nl.row_cap + 32);
+    nl.cap = (long long)nl.row_cap * nl.n;
+    if (nl.cap + nl.row_cap > 2147483647LL)
+      return fail(kOverflow, "neighbor list: rows exceed 32-bit offsets");
+    SNB_CUDA_TRY(cudaMalloc(&nl.d_cols, sizeof(int) * nl.cap));
+    k_row_starts<<<ceil_div(nl.n + 1, 256), 256, 0, st>>>(nl.n, nl.row_cap, nl.d_row_start);
     int zero = 0;
     SNB_CUDA_TRY(cudaMemcpyAsync(nl.d_flags + kFlagListOverflow, &zero, sizeof(int),
                                  cudaMemcpyHostToDevice, st));
@@ -493,18 +511,21 @@ struct AtomGroupABI {  // layout of the reference's ATOM_GROUP (common.h:177-182
 
 // pairs in global ids (lo, hi), in sorted-frame list order
 __global__ void k_export_pairs(int n, const int* __restrict__ row_start,
+                               const int* __restrict__ row_count,
                                const int* __restrict__ cols,
+                               const long long* __restrict__ out_start,
                                const int* __restrict__ global, int* pi, int* pj,
                                long long cap) {
   int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   int lane = threadIdx.x & 31;
   if (i >= n) return;
   int gi = global[i];
-  for (int k = row_start[i] + lane; k < row_start[i + 1]; k += 32) {
-    if (k >= cap) break;
-    int gj = global[cols[k]];
-    pi[k] = gi < gj ? gi : gj;
-    pj[k] = gi < gj ? gj : gi;
+  const long long o = out_start[i];
+  for (int q = lane; q < row_count[i]; q += 32) {
+    if (o + q >= cap) break;
+    int gj = global[cols[row_start[i] + q]];
+    pi[o + q] = gi < gj ? gi : gj;
+    pj[o + q] = gi < gj ? gj : gi;
   }
 }
 
@@ -520,6 +541,7 @@ __global__ void k_export_groups_reset(int n, AtomGroupABI* groups, int* slab,
 // Reference row semantics: the row of local atom a holds local b with
 // global(b) > global(a).  Local index = caller index here.
 __global__ void k_export_groups_fill(int n, const int* __restrict__ row_start,
+                                     const int* __restrict__ row_count,
                                      const int* __restrict__ cols,
                                      const int* __restrict__ global,
                                      const int* __restrict__ perm, int* slab, int maxn,
@@ -530,7 +552,7 @@ __global__ void k_export_groups_fill(int n, const int* __restrict__ row_start,
   if (flags[kFlagListOverflow]) return;
   int gi = global[i];
   int li = perm[i];
-  for (int k = row_start[i] + lane; k < row_start[i + 1]; k += 32) {
+  for (int k = row_start[i] + lane; k < row_start[i] + row_count[i]; k += 32) {
     int j = cols[k];
     int gj = global[j];
     int lj = perm[j];
@@ -560,7 +582,7 @@ int nl_export_atom_groups(NeighborList& nl, void* d_groups, int* d_slab,
   k_export_groups_reset<<<ceil_div(n, 256), 256, 0, st>>>(n, g, d_slab,
                                                           max_neighbor_numbers, counts);
   k_export_groups_fill<<<ceil_div(n, 8), 256, 0, st>>>(
-      n, nl.d_row_start, nl.d_cols, nl.d_global, nl.d_perm, d_slab,
+      n, nl.d_row_start, nl.d_row_count, nl.d_cols, nl.d_global, nl.d_perm, d_slab,
       max_neighbor_numbers, counts, nl.d_flags);
   k_export_groups_counts<<<ceil_div(n, 256), 256, 0, st>>>(n, g, counts,
                                                            max_neighbor_numbers);
@@ -586,8 +608,26 @@ int nl_export_pairs(NeighborList& nl, int* d_pi, int* d_pj, long long cap,
   if (rc) return rc;
   *count = total;
   if (total > cap) return fail(kOverflow, "export_pairs: capacity too small");
-  k_export_pairs<<<ceil_div(nl.n, 8), 256, 0, st>>>(nl.n, nl.d_row_start, nl.d_cols,
-                                                    nl.d_global, d_pi, d_pj, cap);
+  // output offsets of the rows (host prefix sum of the row counts)
+  std::vector<int> counts(nl.n);
+  SNB_CUDA_TRY(cudaMemcpy(counts.data(), nl.d_row_count, sizeof(int) * nl.n,
+                          cudaMemcpyDeviceToHost));
+  std::vector<long long> starts(nl.n);
+  long long acc = 0;
+  for (int i = 0; i < nl.n; ++i) {
+    starts[i] = acc;
+    acc += counts[i];
+  }
+  long long* d_starts = nullptr;
+  SNB_CUDA_TRY(cudaMalloc(&d_starts, sizeof(long long) * nl.n));
+  SNB_CUDA_TRY(cudaMemcpy(d_starts, starts.data(), sizeof(long long) * nl.n,
+                          cudaMemcpyHostToDevice));
+  k_export_pairs<<<ceil_div(nl.n, 8), 256, 0, st>>>(nl.n, nl.d_row_start, nl.d_row_count,
+                                                    nl.d_cols, d_starts, nl.d_global,
+                                                    d_pi, d_pj, cap);
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(d_starts);
+  if (e != cudaSuccess) return fail(kCudaError, cudaGetErrorString(e));
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }

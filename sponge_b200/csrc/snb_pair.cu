@@ -156,7 +156,7 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   float fx = 0.f, fy = 0.f, fz = 0.f;
   float e_lj = 0.f, e_c = 0.f;
   float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  const int k0 = a.row_start[i], k1 = a.row_start[i + 1];
+  const int k0 = a.row_start[i], k1 = k0 + a.row_count[i];
   const unsigned lt = (1u << lane) - 1u;
   int count = 0;
   // Four candidates per lane per round: their index loads, then their
@@ -319,7 +319,7 @@ k_lj_soft(SoftArgs a, Accumulators acc, long long* dudl_total) {
   float e_lj = 0.f, e_c = 0.f, e_inter = 0.f, e_intra = 0.f;
   float du_lj = 0.f, du_c = 0.f;
   float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  const int k0 = a.row_start[i], k1 = a.row_start[i + 1];
+  const int k0 = a.row_start[i], k1 = k0 + a.row_count[i];
   for (int k = k0 + lane; k < k1; k += 32) {
     const int j = a.cols[k];
     const float4 pj = a.pos[j];

@@ -285,16 +285,33 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
   for (int k = threadIdx.x; k < kTile3; k += blockDim.x) sq[k] = 0;
   if (threadIdx.x == 0) scount = 0;
   __syncthreads();
-  const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
-  const int b0[3] = {s0.y, s0.z, s0.w};
-  const int b1[3] = {s1.y, s1.z, s1.w};
-  const int b2[3] = {s2.y, s2.z, s2.w};
-  for (int a = 0; a < s0.x; ++a)
-    for (int b = 0; b < s1.x; ++b)
-      for (int c = 0; c < s2.x; ++c) {
-        const int bin = (b0[a] * g.nt1 + b1[b]) * g.nt2 + b2[c];
-        const int beg = tile_start[bin], end = tile_start[bin + 1];
-        for (int k = beg + threadIdx.x; k < end; k += blockDim.x) {
+  // the (up to 27) source bins as one flat range of atoms
+  __shared__ int sbeg[27], spre[28];
+  if (threadIdx.x == 0) {
+    const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
+    const int b0[3] = {s0.y, s0.z, s0.w};
+    const int b1[3] = {s1.y, s1.z, s1.w};
+    const int b2[3] = {s2.y, s2.z, s2.w};
+    int nb = 0, tot = 0;
+    for (int a = 0; a < s0.x; ++a)
+      for (int b = 0; b < s1.x; ++b)
+        for (int c = 0; c < s2.x; ++c) {
+          const int bin = (b0[a] * g.nt1 + b1[b]) * g.nt2 + b2[c];
+          sbeg[nb] = tile_start[bin];
+          spre[nb] = tot;
+          tot += tile_start[bin + 1] - tile_start[bin];
+          ++nb;
+        }
+    spre[nb] = tot;
+    for (int q = nb + 1; q < 28; ++q) spre[q] = tot;
+  }
+  __syncthreads();
+  const int total = spre[27];
+  for (int fi = threadIdx.x; fi < total; fi += blockDim.x) {
+    int bi = 0;
+    while (spre[bi + 1] <= fi) ++bi;
+    const int k = sbeg[bi] + (fi - spre[bi]);
+    {
           const int up = binned_u[k];
           const int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
           const int mx = stencil_mask(ux, g.K0, lo0, hi0);
