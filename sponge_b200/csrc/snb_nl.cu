@@ -150,8 +150,11 @@ k_pair_search(int n, const float4* __restrict__ pos, const int* __restrict__ glo
               int row_cap, int* __restrict__ cols, int* flags) {
   if (flags[kFlagNeed] == 0) return;
   const int lane = threadIdx.x & 31;
-  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (i >= n) return;
+  const int nw = blockDim.x >> 5;
+  // contiguous range of sorted atoms per block: shared neighbour cells in L1
+  const int per_block = (n + gridDim.x - 1) / gridDim.x;
+  const int i_end = min(n, (int)blockIdx.x * per_block + per_block);
+  for (int i = blockIdx.x * per_block + (threadIdx.x >> 5); i < i_end; i += nw) {
   const float4 pi4 = pos[i];
   const float3 ri = make_float3(pi4.x, pi4.y, pi4.z);
   const int gi = global[i];
@@ -200,6 +203,7 @@ k_pair_search(int n, const float4* __restrict__ pos, const int* __restrict__ glo
       flags[kFlagListOverflow] = 1;
       atomicMax(&flags[kFlagMaxRow], count);
     }
+  }
   }
 }
 
@@ -255,6 +259,14 @@ static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
     for (int cy = 0; cy < Ny; ++cy)
       for (int cz = 0; cz < Nz; ++cz) {
         int c = (cx * Ny + cy) * Nz + cz;
+        // Which cell of a neighbouring pair searches the pair.  With at least
+        // 5 cells per axis every neighbour has one offset (dx, dy, dz) in
+        // [-2, 2]^3 and the pair belongs to the cell that sees the other at
+        // a lexicographically positive offset: every cell owns 62 of its 124
+        // neighbours, so rows have about the same length everywhere.  With
+        // fewer cells an offset can alias (+2 and -2 meet), and the pair
+        // belongs to the cell with the smaller index.
+        const bool offset_rule = Nx >= 5 && Ny >= 5 && Nz >= 5;
         std::set<int> nb;
         for (int dx = -2; dx <= 2; ++dx)
           for (int dy = -2; dy <= 2; ++dy)
@@ -263,7 +275,10 @@ static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
               int y = ((cy + dy) % Ny + Ny) % Ny;
               int z = ((cz + dz) % Nz + Nz) % Nz;
               int o = (x * Ny + y) * Nz + z;
-              if (o > c) nb.insert(o);
+              bool own = offset_rule
+                             ? (dx > 0 || (dx == 0 && (dy > 0 || (dy == 0 && dz > 0))))
+                             : o > c;
+              if (own && o != c) nb.insert(o);
             }
         std::vector<int2> rr;
         for (int o : nb) {
@@ -359,7 +374,8 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
     double rho = n / vol;
     double rl = sqrt((double)nl.rl2);
     double per = 0.5 * rho * 4.18879020478639 * rl * rl * rl;
-    initial_capacity = (long long)(1.5 * per) + 64;
+    const bool balanced = nl.Nx >= 5 && nl.Ny >= 5 && nl.Nz >= 5;
+    initial_capacity = (long long)((balanced ? 1.5 : 2.5) * per) + 64;
   }
   nl.row_cap = (int)std::min<long long>(initial_capacity, n);
   if (nl.row_cap < 32) nl.row_cap = 32;
@@ -459,7 +475,9 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
                                                   nl.d_pos, nl.d_old_crd, nl.d_flags);
   k_sorted_cell<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_perm, nl.d_atom_cell,
                                                   nl.d_sorted_cell, nl.d_flags);
-  k_pair_search<<<ceil_div(n, 8), 256, 0, st>>>(
+  static int sms = 0;
+  if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  k_pair_search<<<std::min(ceil_div(n, 8), sms * 8), 256, 0, st>>>(
       n, nl.d_pos, nl.d_global, nl.d_sorted_cell, nl.d_cell_start, nl.d_run_ranges,
       nl.d_run_count, nl.max_runs, nl.cell, nl.rcell, nl.rl2, excl_start, excl_list,
       excl_numbers, nl.d_row_count, nl.row_cap, nl.d_cols, nl.d_flags);

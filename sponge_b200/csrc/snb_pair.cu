@@ -18,6 +18,7 @@
 // registers and is reduced with warp shuffles; j forces go straight to the
 // accumulators: 64-bit fixed point (deterministic, order-independent) or
 // float atomics (the plain path).
+#include <algorithm>
 #include <cfloat>
 
 #include "snb_internal.h"
@@ -146,9 +147,13 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
-  const int i = blockIdx.x * (blockDim.x >> 5) + w;
-  if (i >= a.n) return;
   if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
+  // Each block owns a contiguous range of sorted atoms, so the neighbours its
+  // warps gather overlap and stay in this SM's L1.
+  const int per_block = (a.n + gridDim.x - 1) / gridDim.x;
+  const int i_begin = blockIdx.x * per_block;
+  const int i_end = min(a.n, i_begin + per_block);
+  for (int i = i_begin + w; i < i_end; i += kWarps) {
   const float4 pi = a.pos[i];
   const float3 ri = make_float3(pi.x, pi.y, pi.z);
   const int ti = a.type[i];
@@ -234,16 +239,21 @@ k_lj_direct(PairArgs a, Accumulators acc) {
     if (ENERGY) add_energy<ACCUM>(acc, i, e_lj + e_c, e_lj, e_c);
     if (VIRIAL) add_virial<ACCUM>(acc, i, vir);
   }
+  }
 }
 
 template <int ACCUM, bool ENERGY, bool VIRIAL>
 static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream_t st) {
-  dim3 grid(ceil_div(a.n, kWarps)), block(32 * kWarps);
   size_t smem = sizeof(float) * a.n_types * (a.n_types + 1);
-  if (ortho)
-    k_lj_direct<ACCUM, ENERGY, VIRIAL, true><<<grid, block, smem, st>>>(a, acc);
-  else
-    k_lj_direct<ACCUM, ENERGY, VIRIAL, false><<<grid, block, smem, st>>>(a, acc);
+  auto kern = ortho ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true>
+                    : k_lj_direct<ACCUM, ENERGY, VIRIAL, false>;
+  // persistent grid: as many blocks as fit at once
+  static int sms = 0;
+  if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, smem);
+  int blocks = std::max(1, std::min(sms * std::max(per_sm, 1), ceil_div(a.n, kWarps)));
+  kern<<<blocks, 32 * kWarps, smem, st>>>(a, acc);
 }
 
 template <int ACCUM>
