@@ -240,6 +240,32 @@ int snb_pme_energies(snb_pme* pme, double* h_reciprocal, double* h_self,
                      double* h_virial6, void* stream);
 int snb_pme_destroy(snb_pme* pme);
 
+/* No counterpart in the reference.  The excluded-pair correction of
+ * snb_pme_excluded_force (fixed-point accumulation, same results) for
+ * callers that cannot allocate device memory while they run -- a loop
+ * sharing the GPU with a caching allocator that holds the rest of HBM, or
+ * one that must avoid the device-wide synchronisation of cudaMalloc/cudaFree
+ * -- and that keep no snb_pme handle (pme_beta comes from the caller).  It
+ * allocates nothing: its accumulator is a static device array of
+ * SNB_NOALLOC_MAX_ATOMS atoms (6 MiB per device), and larger atom_numbers
+ * are rejected with SNB_ERR_BAD_INPUT.  The array is shared by every call
+ * on a device, so calls that may overlap in time (unordered streams,
+ * concurrent threads) race and give wrong results: order them.  The array
+ * must start at zero; the first call on each device clears it and each
+ * completed call leaves it zero.  That first call looks up the array's
+ * address and enqueues the clear, so make it before any stream capture
+ * begins. */
+#define SNB_NOALLOC_MAX_ATOMS 65536
+int snb_pme_excluded_force_noalloc(int atom_numbers, const float* crd,
+                                   snb_boundary boundary, const float* charge,
+                                   float pme_beta,
+                                   const int* excluded_list_start,
+                                   const int* excluded_list,
+                                   const int* excluded_atom_numbers, float* frc,
+                                   int need_energy, float* atom_ene,
+                                   int need_virial, float* atom_virial,
+                                   void* stream);
+
 /* ------------------------------------------------ fused force engine */
 /* The whole nonbonded force of Main_Calculate_Force (main.cpp:1389-1544:
  * neighbor update, excluded correction, LJ + direct Coulomb, long-range LJ

@@ -58,6 +58,7 @@ EXPORTED = [
     "snb_lj_soft_long_range_correction", "snb_lj_soft_destroy",
     "snb_pme_create", "snb_pme_beta", "snb_pme_grid", "snb_pme_reciprocal_force",
     "snb_pme_excluded_force", "snb_pme_energies", "snb_pme_destroy",
+    "snb_pme_excluded_force_noalloc",
     "snb_engine_create", "snb_engine_force", "snb_engine_set_bonded",
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_profile_steps",
     "snb_engine_graph_info", "snb_engine_stats",
@@ -110,6 +111,8 @@ _SIGS = {
                                     _I, _P, _I, _P, _P]),
     "snb_pme_energies": (_I, [_P, _P, _P, _P, _P]),
     "snb_pme_destroy": (_I, [_P]),
+    "snb_pme_excluded_force_noalloc": (_I, [_I, _P, snb_boundary, _P, _F, _P, _P, _P, _P,
+                                            _I, _P, _I, _P, _P]),
     "snb_engine_create": (_I, [ctypes.POINTER(snb_options), _I, snb_boundary, _I, _P,
                                _P, _P, _P, _P, _P, _P, _I, ctypes.POINTER(_P)]),
     "snb_engine_force": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
