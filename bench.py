@@ -55,6 +55,12 @@ def parse():
     p.add_argument("--profile-steps", type=int, default=30)
     p.add_argument("--equilibrate", type=int, default=2000,
                    help="untimed NVE steps from the lattice start before warm-up")
+    p.add_argument("--no-graph", action="store_true",
+                   help="launch the step kernels on the stream instead of replaying "
+                        "the captured step graph (for kernel profilers)")
+    p.add_argument("--drift-steps", type=int, default=2000,
+                   help="NVE steps after the timed region over which the total-energy "
+                        "drift is fitted (0: skip)")
     return p.parse_args()
 
 
@@ -139,6 +145,74 @@ def committed_traffic():
         d = json.load(open(path))
         return d
     return None
+
+
+def bonded_energy(s, crd):
+    """Water bonds and angles at crd (host, FP64), the same harmonic forms
+    the engine integrates: k (r - r0)^2 and k (theta - theta0)^2."""
+    from sponge_b200 import systems
+    crd = crd.astype(np.float64)
+    b = s.bonds
+    d = crd[b[:, 0]] - crd[b[:, 1]]
+    d -= np.round(d / s.box) * s.box
+    r = np.linalg.norm(d, axis=1)
+    e = systems.BOND_K * ((r - systems.BOND_R0) ** 2).sum()
+    a = s.angles
+    u = crd[a[:, 0]] - crd[a[:, 1]]
+    w = crd[a[:, 2]] - crd[a[:, 1]]
+    u -= np.round(u / s.box) * s.box
+    w -= np.round(w / s.box) * s.box
+    c = (u * w).sum(1) / np.linalg.norm(u, axis=1) / np.linalg.norm(w, axis=1)
+    return e + systems.ANGLE_K * ((np.arccos(np.clip(c, -1, 1)) - systems.ANGLE_T0) ** 2).sum()
+
+
+def nve_drift(lib, h, s, crd, vel, invm, first, total, samples, dt, run_steps, st, sp):
+    """Total energy every total/(samples-1) steps: the engine's nonbonded
+    potential (FP64 sums), the bonded terms on the host, and the kinetic
+    energy from the average of the leap-frog half-step velocities around the
+    sample.  Returns the fitted drift in kcal/mol/ns/atom."""
+    import torch
+    from sponge_b200 import capi, systems
+    P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    n = s.n
+    tot = torch.zeros(16, dtype=torch.float64, device="cuda")
+    frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+    every = max(2, total // max(1, samples - 1))
+    step, ts, es, kes = first, [], [], []
+    m = s.mass.astype(np.float64)[:, None]
+    for _ in range(samples):
+        with torch.cuda.stream(st):
+            capi.check(lib.snb_engine_force(h, P(crd), P(frc), step, 1, 0, P(tot), sp),
+                       "engine_force")
+        st.synchronize()
+        c0 = crd.cpu().numpy().reshape(n, 3)
+        v0 = vel.cpu().numpy().reshape(n, 3).astype(np.float64)
+        pot = float(tot[7].item()) + bonded_energy(s, c0)
+        with torch.cuda.stream(st):
+            capi.check(run_steps(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                 step, 1, sp), "md_steps")
+        st.synchronize()
+        v1 = vel.cpu().numpy().reshape(n, 3).astype(np.float64)
+        ke = 0.5 * (m * (0.5 * (v0 + v1)) ** 2).sum()
+        ts.append(step)
+        es.append(pot + ke)
+        kes.append(ke)
+        step += 1
+        with torch.cuda.stream(st):
+            capi.check(run_steps(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                 step, every - 1, sp), "md_steps")
+        step += every - 1
+    st.synchronize()
+    ts = np.asarray(ts, np.float64)
+    es = np.asarray(es, np.float64)
+    slope = np.polyfit(ts, es, 1)[0]  # kcal/mol per step
+    per_ns = slope / (DT_FS * 1e-6)
+    return {"steps": int(ts[-1] - ts[0]), "samples": len(ts),
+            "kcal_per_mol_per_ns_per_atom": per_ns / n,
+            "e_total_first": es[0], "e_total_last": es[-1],
+            "e_total_std": float(es.std()),
+            "temperature_K": float(2.0 * np.mean(kes) / (3.0 * n * systems.KB))}
+
 
 
 # --------------------------------------------------------------------------
@@ -255,14 +329,25 @@ def run_ours(args):
     P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
     K, W = args.steps, max(args.warmup, 3)
 
+    run_steps = lib.snb_engine_md_steps if args.no_graph else lib.snb_engine_md_steps_graph
+
     def steps(first, k):
-        capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm),
-                                                 ctypes.c_float(dt), first, k, sp),
-                   "md_steps_graph")
+        capi.check(run_steps(h, P(crd), P(vel), P(invm), ctypes.c_float(dt), first, k, sp),
+                   "md_steps")
 
     EQ = max(0, args.equilibrate)
+    # Untimed equilibration from the lattice start, with the velocities
+    # rescaled to 300 K every 100 steps (the start releases potential energy
+    # that would otherwise heat the box far above 300 K), then plain NVE.
+    mass = torch.from_numpy(s.mass.astype(np.float64)).cuda()
+    for c0 in range(0, EQ, 100):
+        with torch.cuda.stream(st):
+            steps(c0, min(100, EQ - c0))
+            v = vel.view(n, 3).double()
+            ke = 0.5 * (mass[:, None] * v * v).sum()
+            t_now = 2.0 * ke / (3.0 * n * systems.KB)
+            vel.mul_(float(torch.sqrt(300.0 / t_now)))
     with torch.cuda.stream(st):
-        steps(0, EQ)
         steps(EQ, W)
     st.synchronize()
     r0 = ctypes.c_longlong(0)
@@ -295,8 +380,9 @@ def run_ours(args):
     timed_rebuilds = int(r1.value - r0.value)
     # graph composition: our kernels per step
     kn, libk, bodyk = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
-    capi.check(lib.snb_engine_graph_info(h, ctypes.byref(kn), ctypes.byref(libk),
-                                         ctypes.byref(bodyk), sp), "graph_info")
+    if not args.no_graph:  # with --no-graph no step graph exists to count
+        capi.check(lib.snb_engine_graph_info(h, ctypes.byref(kn), ctypes.byref(libk),
+                                             ctypes.byref(bodyk), sp), "graph_info")
     ours_per_step = kn.value - libk.value
     forced_steps = sum(1 for x in range(EQ + W, EQ + W + K) if x % 100 == 0)
 
@@ -320,9 +406,8 @@ def run_ours(args):
         for k in range(E):
             crd.copy_(h_crd, non_blocking=True)
             vel.copy_(h_vel, non_blocking=True)
-            capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm),
-                                                     ctypes.c_float(dt), EQ + W + K + 1000 + k, 1,
-                                                     sp), "e2e step")
+            capi.check(run_steps(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                 EQ + W + K + 1000 + k, 1, sp), "e2e step")
             h_crd.copy_(crd, non_blocking=True)
             h_vel.copy_(vel, non_blocking=True)
             st.synchronize()
@@ -332,6 +417,11 @@ def run_ours(args):
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = world * ns_per_day(E / float(e2e_t.item()))
     io_bytes = 2 * 3 * 4 * n
+
+    drift = None
+    if args.drift_steps > 0:
+        drift = nve_drift(lib, h, s, crd, vel, invm, EQ + W + K + 2000 + E,
+                          args.drift_steps, 21, dt, run_steps, st, sp)
 
     # roofline of the dominant kernel (the pair kernel), HBM view
     pair_ms = float(phases[2])
@@ -389,6 +479,7 @@ def run_ours(args):
         "phase_ms": dict(zip(["neighbor", "pack", "pair", "excluded", "pme", "bonded",
                               "integrate"], [round(float(x), 5) for x in phases])),
         "nl_rebuilds": int(rebuilds.value), "pairs": listed,
+        "nve_drift": drift,
         "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clk,
     }
     print(json.dumps(line))

@@ -60,24 +60,50 @@ __device__ __forceinline__ float3 min_image_exact(float3 a, float3 b,
   return make_float3(__fsub_rn(dx, cx), __fsub_rn(dy, cy), __fsub_rn(dz, cz));
 }
 
+// min_image_exact for a rectangular box, given dr = a - b.  The off-diagonal
+// entries of cell and rcell are zero, so the general form only adds signed
+// zeros to each sum; that can turn a -0 into +0 but never changes floorf of
+// (s + 0.5) or the square of any component, so |dr|^2 is bit-identical.
+__device__ __forceinline__ float3 min_image_exact_rect(float dx, float dy, float dz,
+                                                       const Cell& cell,
+                                                       const Cell& rcell) {
+  const float fx = floorf(__fadd_rn(__fmul_rn(dx, rcell.a11), 0.5f));
+  const float fy = floorf(__fadd_rn(__fmul_rn(dy, rcell.a22), 0.5f));
+  const float fz = floorf(__fadd_rn(__fmul_rn(dz, rcell.a33), 0.5f));
+  return make_float3(__fsub_rn(dx, __fmul_rn(fx, cell.a11)),
+                     __fsub_rn(dy, __fmul_rn(fy, cell.a22)),
+                     __fsub_rn(dz, __fmul_rn(fz, cell.a33)));
+}
+
 // |dr|^2 in the reference's operator order ((x*x + y*y) + z*z), unfused.
 __device__ __forceinline__ float norm2_exact(float3 d) {
   return __fadd_rn(__fadd_rn(__fmul_rn(d.x, d.x), __fmul_rn(d.y, d.y)),
                    __fmul_rn(d.z, d.z));
 }
 
-// Fast minimum image for force evaluation.  Same image choice as the
-// reference (floor(s + 0.5)), contraction allowed.  ORTHO skips the
-// off-diagonal terms of a rectangular box.
+// Minimum image of a rectangular box for force evaluation, on the FMA pipe:
+// k = round(d / L) by the 1.5*2^23 shift (exact for |d / L| < 2^22), then
+// d - k L.  It differs from floor(s + 0.5) only when d is an odd multiple of
+// half a box length: both images are then equally far, and with a cutoff
+// below half the box (the condition for the minimum image to be the only
+// image in range) the pair is beyond the cutoff.
+__device__ __forceinline__ float min_image_axis(float d, float L, float rL) {
+  const float k = __fsub_rn(__fmaf_rn(d, rL, 12582912.0f), 12582912.0f);
+  return __fmaf_rn(-k, L, d);
+}
+
+// Fast minimum image for force evaluation, contraction allowed.  ORTHO: a
+// rectangular box, rounded per axis by min_image_axis; otherwise the
+// reference's floor(s + 0.5) on the full cell.
 template <bool ORTHO>
 __device__ __forceinline__ float3 min_image_fast(float3 a, float3 b,
                                                  const Cell& cell,
                                                  const Cell& rcell) {
   float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
   if (ORTHO) {
-    dx -= floorf(dx * rcell.a11 + 0.5f) * cell.a11;
-    dy -= floorf(dy * rcell.a22 + 0.5f) * cell.a22;
-    dz -= floorf(dz * rcell.a33 + 0.5f) * cell.a33;
+    dx = min_image_axis(dx, cell.a11, rcell.a11);
+    dy = min_image_axis(dy, cell.a22, rcell.a22);
+    dz = min_image_axis(dz, cell.a33, rcell.a33);
   } else {
     float sx = dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31;
     float sy = dy * rcell.a22 + dz * rcell.a32;
@@ -88,6 +114,13 @@ __device__ __forceinline__ float3 min_image_fast(float3 a, float3 b,
     dz -= fz * cell.a33;
   }
   return make_float3(dx, dy, dz);
+}
+
+// Start pulling [p, p + bytes) into L2 (bytes a multiple of 16, p 16-byte
+// aligned); a hint with no completion to wait for.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes)
+               : "memory");
 }
 
 // Triangular LJ pair index, Get_LJ_Type (Lennard_Jones_force.h:19-28).
@@ -122,8 +155,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 // a degree-8 polynomial in t = 1/(1 + x/2) on [0, 4] (weighted least-squares
 // fit, csrc/fit_erfcx.py; max relative error 3.3e-7 in float32), so
 // erfc(x) = P(t) * exp(-x^2).  exp uses the hardware exp2 (__expf: error
-// 2 + 1.16|x^2| ulp, below 1e-6 relative for x <= 4); t uses the correctly
-// rounded reciprocal.  Beyond x = 4 CUDA's erfcf / expf are used.
+// 2 + 1.16|x^2| ulp, below 1e-6 relative for x <= 4); t uses the fast
+// hardware division (2 ulp; |t P'(t) / P(t)| <= 2.26 on the range, so P
+// moves by at most 5.4e-7 relative through it).  Beyond x = 4 CUDA's erfcf
+// and expf are used.
 __device__ __forceinline__ float erfc_and_exp(float x, float* e_out) {
   if (x > 4.0f) {
     *e_out = expf(-x * x);
@@ -131,7 +166,7 @@ __device__ __forceinline__ float erfc_and_exp(float x, float* e_out) {
   }
   const float e = __expf(-x * x);
   *e_out = e;
-  const float t = __frcp_rn(1.0f + 0.5f * x);
+  const float t = __fdividef(1.0f, 1.0f + 0.5f * x);
   float p = -0.049221702f;
   p = fmaf(p, t, 0.33589873f);
   p = fmaf(p, t, -0.88379663f);

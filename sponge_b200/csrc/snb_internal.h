@@ -63,7 +63,15 @@ struct NeighborList {
   // contiguous cell ranges [first, last]
   int max_runs = 0;
   int2* d_run_ranges = nullptr;  // [ncell][max_runs] {first_cell, last_cell}
+  char4* d_run_geom = nullptr;   // [ncell][max_runs] {dx, dy, dz first, dz last}
   int* d_run_count = nullptr;  // [ncell]
+  bool trim = false;           // runs are cut to the cells within reach of i
+  float reach2 = 0.f;
+  float wx = 0.f, wy = 0.f, iwz = 0.f;
+  // excluded partners per atom (rebuilt with the list when ids are the
+  // caller's indices): count [n] and up to 16 partners [n][16]
+  int* d_excl_count = nullptr;
+  int* d_excl_partner = nullptr;
   // binning
   int* d_cell_count = nullptr;  // [ncell]
   int* d_cell_start = nullptr;  // [ncell + 1]

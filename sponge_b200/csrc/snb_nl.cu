@@ -11,14 +11,15 @@
 // The layout is different.  Atoms are counting-sorted into cells of side
 // L/floor(L/((cutoff+skin)/2)) with a stable order inside each cell (caller
 // index), so the sorted order and the list are deterministic.  One warp scans,
-// for one sorted atom i, the atoms after i in its own cell and every
-// forward neighbor cell (cell index larger than its own, +-2 cells), walked as
-// merged runs of consecutive cells: each run is one contiguous slice of the
-// sorted coordinate array, read with coalesced 16-byte loads.  A count pass
-// and a fill pass (same scan) produce CSR rows: no per-atom capacity, no list
-// atomics, no ballot-order races.
+// for one sorted atom i, the atoms after i in its own cell and the neighbor
+// cells its cell owns (+-2 cells), walked as runs of consecutive cells along
+// z: each run is one contiguous slice of the sorted coordinate array, read
+// with coalesced 16-byte loads, and is trimmed to the cells whose box comes
+// within rl of atom i.  Hits go in one pass into rows of fixed capacity;
+// a row that would overflow raises a flag and the host regrows the rows.
 #include <algorithm>
-#include <set>
+#include <cmath>
+#include <map>
 #include <vector>
 
 #include "snb_internal.h"
@@ -67,23 +68,46 @@ __device__ __forceinline__ int wrapped_cell(float3 r, const Cell& cell, int Nx,
 __global__ void k_bin_count(int n, const float3* __restrict__ crd, Cell cell,
                             int Nx, int Ny, int Nz, int* __restrict__ atom_cell,
                             int* __restrict__ atom_slot, int* __restrict__ cell_count,
-                            const int* flags) {
+                            int* __restrict__ excl_count, const int* flags) {
   if (flags[kFlagNeed] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int c = wrapped_cell(crd[i], cell, Nx, Ny, Nz);
   atom_cell[i] = c;
   atom_slot[i] = atomicAdd(&cell_count[c], 1);
+  if (excl_count) excl_count[i] = 0;
 }
+
+// Excluded partners per atom, E(x) = {y : the pair (x, y) is removed}: the
+// reference removes a pair when the larger id is in the exclusion list of
+// the smaller one, so an entry y of list(x) counts only when y > x and then
+// excludes the pair for both ends.  Up to kExclCap partners are kept per
+// atom; the count is exact, and atoms with more use the list lookup.
+constexpr int kExclCap = 16;
 
 __global__ void k_bin_scatter(int n, const int* __restrict__ atom_cell,
                               const int* __restrict__ atom_slot,
                               const int* __restrict__ cell_start,
-                              int* __restrict__ unsorted, const int* flags) {
+                              int* __restrict__ unsorted, const int* __restrict__ excl_start,
+                              const int* __restrict__ excl_list,
+                              const int* __restrict__ excl_numbers,
+                              int* __restrict__ excl_count, int* __restrict__ excl_partner,
+                              const int* flags) {
   if (flags[kFlagNeed] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   unsorted[cell_start[atom_cell[i]] + atom_slot[i]] = i;
+  if (!excl_count) return;
+  const int cnt = excl_numbers[i];
+  const int s = cnt > 0 ? excl_start[i] : 0;
+  for (int k = 0; k < cnt; ++k) {
+    const int y = excl_list[s + k];
+    if (y <= i || y >= n) continue;
+    const int a = atomicAdd(&excl_count[i], 1);
+    if (a < kExclCap) excl_partner[i * kExclCap + a] = y;
+    const int b = atomicAdd(&excl_count[y], 1);
+    if (b < kExclCap) excl_partner[y * kExclCap + b] = i;
+  }
 }
 
 // One warp per cell: stable order inside the cell by caller index (rank sort).
@@ -114,9 +138,10 @@ __global__ void k_fill_sorted(int n, const int* __restrict__ perm,
   if (s >= n) return;
   int i = perm[s];
   inv_perm[i] = s;
-  global[s] = atom_local ? atom_local[i] : i;
+  const int g = atom_local ? atom_local[i] : i;
+  global[s] = g;
   float3 r = crd[i];
-  pos[s] = make_float4(r.x, r.y, r.z, 0.f);
+  pos[s] = make_float4(r.x, r.y, r.z, __int_as_float(g));  // w: global id bits
   old_crd[i] = r;
 }
 
@@ -136,72 +161,147 @@ __device__ __forceinline__ bool excluded_pair(int gl, int gh,
   return false;
 }
 
+// Arguments of the pair search.
+struct SearchArgs {
+  int n;
+  const float4* pos;        // sorted (x, y, z, global id bits)
+  const int* sorted_cell;
+  const int* cell_start;
+  const int2* runs;         // [ncell][max_runs] {first cell, last cell}
+  const char4* geom;        // [ncell][max_runs] {dx, dy, dz of first, dz of last}
+  const int* run_count;
+  int max_runs;
+  int Nx, Ny, Nz;
+  Cell cell, rcell;
+  float rl2;
+  bool trim;                // cell offsets are unique (>= 5 cells per axis)
+  float reach2;             // (rl + margin)^2 for trimming runs
+  float wx, wy, iwz;        // cell widths x, y and 1/width z
+  const int* excl_start;
+  const int* excl_list;
+  const int* excl_numbers;
+  const int* excl_count;    // E(x) sizes, or null: use the lists directly
+  const int* excl_partner;  // [n][kExclCap]
+  int* row_count;
+  int row_cap;
+  int* cols;
+  int* flags;
+};
+
+// Distance, in cell widths, from a point at fractional offset f inside its
+// cell to the cell at integer offset o along one axis.
+__device__ __forceinline__ float cell_gap(int o, float f) {
+  const float g = o > 0 ? (float)o - f : (o < 0 ? f - (float)(o + 1) : 0.f);
+  return fmaxf(g, 0.f);
+}
+
 // Pair search for sorted atom i (one warp), one pass: row i has room for
 // row_cap entries at cols[i * row_cap]; hits beyond it are counted (the
 // largest row is kept in flags[kFlagMaxRow]) and raise the overflow flag so
 // the host can regrow the rows and repeat the build.
+//
+// Each run is cut down to the cells whose box is within rl (plus a margin)
+// of atom i.  With at least 5 cells per axis a pair within rl sits at the
+// run's cell offset in its minimum image, so a cut cell holds no hit.
 __global__ void __launch_bounds__(256)
-k_pair_search(int n, const float4* __restrict__ pos, const int* __restrict__ global,
-              const int* __restrict__ sorted_cell, const int* __restrict__ cell_start,
-              const int2* __restrict__ runs, const int* __restrict__ run_count,
-              int max_runs, Cell cell, Cell rcell, float rl2,
-              const int* __restrict__ excl_start, const int* __restrict__ excl_list,
-              const int* __restrict__ excl_numbers, int* __restrict__ row_count,
-              int row_cap, int* __restrict__ cols, int* flags) {
-  if (flags[kFlagNeed] == 0) return;
+k_pair_search(SearchArgs a) {
+  if (a.flags[kFlagNeed] == 0) return;
   const int lane = threadIdx.x & 31;
   const int nw = blockDim.x >> 5;
   // contiguous range of sorted atoms per block: shared neighbour cells in L1
-  const int per_block = (n + gridDim.x - 1) / gridDim.x;
-  const int i_end = min(n, (int)blockIdx.x * per_block + per_block);
+  const int per_block = (a.n + gridDim.x - 1) / gridDim.x;
+  const int i_end = min(a.n, (int)blockIdx.x * per_block + per_block);
   for (int i = blockIdx.x * per_block + (threadIdx.x >> 5); i < i_end; i += nw) {
-  const float4 pi4 = pos[i];
-  const float3 ri = make_float3(pi4.x, pi4.y, pi4.z);
-  const int gi = global[i];
-  const int c = sorted_cell[i];
-  int* out_row = cols + (size_t)i * row_cap;
+  const float4 pi4 = a.pos[i];
+  const int gi = __float_as_int(pi4.w);
+  const int c = a.sorted_cell[i];
+  int* out_row = a.cols + (size_t)i * a.row_cap;
   int count = 0;
-  const int nr = run_count[c];
-  // range list: own cell after i, then forward runs
-  for (int r = -1; r < nr; ++r) {
-    int a, b;
-    if (r < 0) {
-      a = i + 1;
-      b = cell_start[c + 1];
+  const int nr = a.run_count[c];
+  // excluded partners of gi held one per lane (warp-uniform count)
+  int n_ex = 0, ex = -1;
+  bool ex_lists = a.excl_numbers != nullptr;
+  if (a.excl_count) {
+    n_ex = a.excl_count[gi];
+    if (n_ex <= kExclCap) {
+      ex_lists = false;
+      if (lane < n_ex) ex = a.excl_partner[gi * kExclCap + lane];
     } else {
-      int2 rr = runs[(size_t)c * max_runs + r];
-      a = cell_start[rr.x];
-      b = cell_start[rr.y + 1];
+      n_ex = 0;
     }
-    for (int base = a; base < b; base += 32) {
-      int j = base + lane;
-      bool hit = false;
-      if (j < b) {
-        float4 pj4 = pos[j];
-        float3 rj = make_float3(pj4.x, pj4.y, pj4.z);
-        int gj = global[j];
-        bool i_low = gi < gj;
-        float3 d = i_low ? min_image_exact(ri, rj, cell, rcell)
-                         : min_image_exact(rj, ri, cell, rcell);
-        if (norm2_exact(d) < rl2) {
-          hit = !excluded_pair(i_low ? gi : gj, i_low ? gj : gi, excl_start,
-                               excl_list, excl_numbers);
-        }
+  }
+  // position of i inside its cell, in cell widths (the binning's arithmetic)
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  if (a.trim) {
+    const int cz = c % a.Nz, cy = (c / a.Nz) % a.Ny, cx = c / (a.Nz * a.Ny);
+    const float x = pi4.x - floorf(pi4.x / a.cell.a11) * a.cell.a11;
+    const float y = pi4.y - floorf(pi4.y / a.cell.a22) * a.cell.a22;
+    const float z = pi4.z - floorf(pi4.z / a.cell.a33) * a.cell.a33;
+    fx = x / a.cell.a11 * a.Nx - (float)cx;
+    fy = y / a.cell.a22 * a.Ny - (float)cy;
+    fz = z / a.cell.a33 * a.Nz - (float)cz;
+  }
+  // range list: own cell after i, then the owned runs
+  for (int r = -1; r < nr; ++r) {
+    int lo, hi;
+    if (r < 0) {
+      lo = i + 1;
+      hi = a.cell_start[c + 1];
+    } else {
+      int2 rr = a.runs[(size_t)c * a.max_runs + r];
+      if (a.trim) {
+        const char4 g = a.geom[(size_t)c * a.max_runs + r];
+        const float gx = cell_gap(g.x, fx) * a.wx, gy = cell_gap(g.y, fy) * a.wy;
+        const float s2 = a.reach2 - gx * gx - gy * gy;
+        if (s2 < 0.f) continue;
+        const float s = sqrtf(s2) * a.iwz;
+        const int zmax = (int)floorf(fz + s), zmin = (int)ceilf(fz - 1.f - s);
+        const int z0 = max((int)g.z, zmin), z1 = min((int)g.w, zmax);
+        if (z0 > z1) continue;
+        rr.x += z0 - g.z;
+        rr.y -= g.w - z1;
       }
-      unsigned m = __ballot_sync(0xffffffffu, hit);
+      lo = a.cell_start[rr.x];
+      hi = a.cell_start[rr.y + 1];
+    }
+    for (int base = lo; base < hi; base += 32) {
+      const int j = base + lane;
+      bool hit = false;
+      int gj = -1;
+      if (j < hi) {
+        const float4 pj4 = a.pos[j];
+        gj = __float_as_int(pj4.w);
+        // dr = crd[lower id] - crd[higher id], as the reference forms it
+        float dx = __fsub_rn(pi4.x, pj4.x);
+        float dy = __fsub_rn(pi4.y, pj4.y);
+        float dz = __fsub_rn(pi4.z, pj4.z);
+        if (gj < gi) {
+          dx = -dx;
+          dy = -dy;
+          dz = -dz;
+        }
+        const float3 d = min_image_exact_rect(dx, dy, dz, a.cell, a.rcell);
+        hit = norm2_exact(d) < a.rl2;
+      }
+      for (int k = 0; k < n_ex; ++k)  // warp-uniform
+        if (__shfl_sync(0xffffffffu, ex, k) == gj) hit = false;
+      if (hit && ex_lists)
+        hit = !excluded_pair(min(gi, gj), max(gi, gj), a.excl_start, a.excl_list,
+                             a.excl_numbers);
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
       if (hit) {
-        int slot = count + __popc(m & ((1u << lane) - 1u));
-        if (slot < row_cap) out_row[slot] = j;
+        const int slot = count + __popc(m & ((1u << lane) - 1u));
+        if (slot < a.row_cap) out_row[slot] = j;
       }
       count += __popc(m);
     }
   }
   if (lane == 0) {
-    row_count[i] = count < row_cap ? count : row_cap;
-    atomicAdd(&flags[kFlagTotal], count);
-    if (count > row_cap) {
-      flags[kFlagListOverflow] = 1;
-      atomicMax(&flags[kFlagMaxRow], count);
+    a.row_count[i] = count < a.row_cap ? count : a.row_cap;
+    atomicAdd(&a.flags[kFlagTotal], count);
+    if (count > a.row_cap) {
+      a.flags[kFlagListOverflow] = 1;
+      atomicMax(&a.flags[kFlagMaxRow], count);
     }
   }
   }
@@ -251,9 +351,11 @@ int nl_force_next(NeighborList& nl, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
-                       std::vector<int>& counts, int& max_runs) {
+                       std::vector<char4>& geom, std::vector<int>& counts,
+                       int& max_runs) {
   int ncell = Nx * Ny * Nz;
   std::vector<std::vector<int2>> per(ncell);
+  std::vector<std::vector<char4>> per_geom(ncell);
   max_runs = 0;
   for (int cx = 0; cx < Nx; ++cx)
     for (int cy = 0; cy < Ny; ++cy)
@@ -267,7 +369,7 @@ static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
         // fewer cells an offset can alias (+2 and -2 meet), and the pair
         // belongs to the cell with the smaller index.
         const bool offset_rule = Nx >= 5 && Ny >= 5 && Nz >= 5;
-        std::set<int> nb;
+        std::map<int, char4> nb;  // owned cell -> its offset
         for (int dx = -2; dx <= 2; ++dx)
           for (int dy = -2; dy <= 2; ++dy)
             for (int dz = -2; dz <= 2; ++dz) {
@@ -278,24 +380,38 @@ static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
               bool own = offset_rule
                              ? (dx > 0 || (dx == 0 && (dy > 0 || (dy == 0 && dz > 0))))
                              : o > c;
-              if (own && o != c) nb.insert(o);
+              if (own && o != c && !nb.count(o))
+                nb[o] = make_char4((signed char)dx, (signed char)dy, (signed char)dz,
+                                   (signed char)dz);
             }
+        // runs: consecutive cells of one z column (dz then rises by one)
         std::vector<int2> rr;
-        for (int o : nb) {
-          if (!rr.empty() && rr.back().y == o - 1)
+        std::vector<char4> gg;
+        for (const auto& kv : nb) {
+          const int o = kv.first;
+          if (!rr.empty() && rr.back().y == o - 1 && (o - 1) / Nz == o / Nz &&
+              gg.back().w + 1 == kv.second.z) {
             rr.back().y = o;
-          else
+            gg.back().w = kv.second.z;
+          } else {
             rr.push_back(make_int2(o, o));
+            gg.push_back(kv.second);
+          }
         }
         max_runs = std::max(max_runs, (int)rr.size());
         per[c] = rr;
+        per_geom[c] = gg;
       }
   if (max_runs == 0) max_runs = 1;
   runs.assign((size_t)ncell * max_runs, make_int2(0, -1));
+  geom.assign((size_t)ncell * max_runs, make_char4(0, 0, 0, -1));
   counts.assign(ncell, 0);
   for (int c = 0; c < ncell; ++c) {
     counts[c] = (int)per[c].size();
-    for (size_t k = 0; k < per[c].size(); ++k) runs[(size_t)c * max_runs + k] = per[c][k];
+    for (size_t k = 0; k < per[c].size(); ++k) {
+      runs[(size_t)c * max_runs + k] = per[c][k];
+      geom[(size_t)c * max_runs + k] = per_geom[c][k];
+    }
   }
 }
 
@@ -329,11 +445,27 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
     return fail(kBadInput, "NEIGHBOR_LIST::Initial: the box is too small.");
   nl.ncell = nl.Nx * nl.Ny * nl.Nz;
   std::vector<int2> runs;
+  std::vector<char4> geom;
   std::vector<int> counts;
-  build_runs(nl.Nx, nl.Ny, nl.Nz, runs, counts, nl.max_runs);
+  build_runs(nl.Nx, nl.Ny, nl.Nz, runs, geom, counts, nl.max_runs);
   SNB_CUDA_TRY(cudaMalloc(&nl.d_run_ranges, sizeof(int2) * runs.size()));
   SNB_CUDA_TRY(cudaMemcpy(nl.d_run_ranges, runs.data(), sizeof(int2) * runs.size(),
                           cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_run_geom, sizeof(char4) * geom.size()));
+  SNB_CUDA_TRY(cudaMemcpy(nl.d_run_geom, geom.data(), sizeof(char4) * geom.size(),
+                          cudaMemcpyHostToDevice));
+  nl.trim = nl.Nx >= 5 && nl.Ny >= 5 && nl.Nz >= 5;
+  {
+    // margin of 0.01 A over rl: far above the float error of the cell
+    // geometry (positions are wrapped with one rounding each)
+    const double reach = sqrt((double)nl.rl2) + 0.01;
+    nl.reach2 = (float)(reach * reach);
+    nl.wx = nl.cell.a11 / nl.Nx;
+    nl.wy = nl.cell.a22 / nl.Ny;
+    nl.iwz = nl.Nz / nl.cell.a33;
+  }
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_excl_count, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_excl_partner, sizeof(int) * kExclCap * (size_t)n));
   SNB_CUDA_TRY(cudaMalloc(&nl.d_run_count, sizeof(int) * nl.ncell));
   SNB_CUDA_TRY(cudaMemcpy(nl.d_run_count, counts.data(), sizeof(int) * nl.ncell,
                           cudaMemcpyHostToDevice));
@@ -379,6 +511,7 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
   }
   nl.row_cap = (int)std::min<long long>(initial_capacity, n);
   if (nl.row_cap < 32) nl.row_cap = 32;
+  nl.row_cap = (nl.row_cap + 7) & ~7;  // rows start on 32-byte boundaries
   nl.cap = (long long)nl.row_cap * n;
   if (nl.cap + nl.row_cap > 2147483647LL)
     return fail(kBadInput, "neighbor list: rows exceed 32-bit offsets");
@@ -392,6 +525,9 @@ void nl_free(NeighborList& nl) {
   cudaFree(nl.d_unsorted);
   cudaFree(nl.d_sorted_cell);
   cudaFree(nl.d_run_ranges);
+  cudaFree(nl.d_run_geom);
+  cudaFree(nl.d_excl_count);
+  cudaFree(nl.d_excl_partner);
   cudaFree(nl.d_run_count);
   cudaFree(nl.d_cell_count);
   cudaFree(nl.d_cell_start);
@@ -456,17 +592,19 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
                cudaStream_t st) {
   const float3* crd = reinterpret_cast<const float3*>(crd_f);
   const int n = nl.n;
+  // Excluded-partner sets need global ids equal to the caller's indices.
+  int* excl_count = (excl_numbers && !atom_local) ? nl.d_excl_count : nullptr;
   SNB_CUDA_TRY(cudaMemsetAsync(nl.d_cell_count, 0, sizeof(int) * nl.ncell, st));
   k_rebuild_begin<<<1, 1, 0, st>>>(nl.d_flags);
   k_bin_count<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz,
                                                 nl.d_atom_cell, nl.d_atom_slot,
-                                                nl.d_cell_count, nl.d_flags);
+                                                nl.d_cell_count, excl_count, nl.d_flags);
   int rc = scan_exclusive(nl.d_cell_count, nl.d_cell_start, nl.ncell, nullptr,
                           nl.scan, st);
   if (rc) return rc;
-  k_bin_scatter<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_atom_cell, nl.d_atom_slot,
-                                                  nl.d_cell_start, nl.d_unsorted,
-                                                  nl.d_flags);
+  k_bin_scatter<<<ceil_div(n, 256), 256, 0, st>>>(
+      n, nl.d_atom_cell, nl.d_atom_slot, nl.d_cell_start, nl.d_unsorted, excl_start,
+      excl_list, excl_numbers, excl_count, nl.d_excl_partner, nl.d_flags);
   k_cell_order<<<ceil_div(nl.ncell, 8), 256, 0, st>>>(nl.ncell, nl.d_cell_start,
                                                       nl.d_unsorted, nl.d_perm,
                                                       nl.d_flags);
@@ -477,10 +615,36 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
                                                   nl.d_sorted_cell, nl.d_flags);
   static int sms = 0;
   if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-  k_pair_search<<<std::min(ceil_div(n, 8), sms * 8), 256, 0, st>>>(
-      n, nl.d_pos, nl.d_global, nl.d_sorted_cell, nl.d_cell_start, nl.d_run_ranges,
-      nl.d_run_count, nl.max_runs, nl.cell, nl.rcell, nl.rl2, excl_start, excl_list,
-      excl_numbers, nl.d_row_count, nl.row_cap, nl.d_cols, nl.d_flags);
+  SearchArgs sa;
+  sa.n = n;
+  sa.pos = nl.d_pos;
+  sa.sorted_cell = nl.d_sorted_cell;
+  sa.cell_start = nl.d_cell_start;
+  sa.runs = nl.d_run_ranges;
+  sa.geom = nl.d_run_geom;
+  sa.run_count = nl.d_run_count;
+  sa.max_runs = nl.max_runs;
+  sa.Nx = nl.Nx;
+  sa.Ny = nl.Ny;
+  sa.Nz = nl.Nz;
+  sa.cell = nl.cell;
+  sa.rcell = nl.rcell;
+  sa.rl2 = nl.rl2;
+  sa.trim = nl.trim;
+  sa.reach2 = nl.reach2;
+  sa.wx = nl.wx;
+  sa.wy = nl.wy;
+  sa.iwz = nl.iwz;
+  sa.excl_start = excl_start;
+  sa.excl_list = excl_list;
+  sa.excl_numbers = excl_numbers;
+  sa.excl_count = excl_count;
+  sa.excl_partner = nl.d_excl_partner;
+  sa.row_count = nl.d_row_count;
+  sa.row_cap = nl.row_cap;
+  sa.cols = nl.d_cols;
+  sa.flags = nl.d_flags;
+  k_pair_search<<<std::min(ceil_div(n, 8), sms * 8), 256, 0, st>>>(sa);
   k_finish_build<<<1, 1, 0, st>>>(nl.d_flags);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
@@ -496,7 +660,7 @@ int nl_check_overflow(NeighborList& nl, bool* regrown, cudaStream_t st) {
     long long need = nl.h_flags[kFlagMaxRow];
     int cap = (int)std::min<long long>(need + need / 5 + 32, nl.n);
     SNB_CUDA_TRY(cudaFree(nl.d_cols));
-    nl.row_cap = std::max(cap, nl.row_cap + 32);
+    nl.row_cap = (std::max(cap, nl.row_cap + 32) + 7) & ~7;
     nl.cap = (long long)nl.row_cap * nl.n;
     if (nl.cap + nl.row_cap > 2147483647LL)
       return fail(kOverflow, "neighbor list: rows exceed 32-bit offsets");

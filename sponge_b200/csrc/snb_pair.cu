@@ -69,12 +69,16 @@ __device__ __forceinline__ void add_virial(Accumulators& acc, int s, const float
   }
 }
 
-// Per-warp queue of in-cutoff pairs: the row is scanned 32 candidates at a
-// time, the ones inside the cutoff are appended (ballot + popc) and the pair
-// terms run only on full batches of 32, so every lane of the expensive part
-// does useful work.
+// Each warp owns one row at a time and takes it in two phases.  Phase 1
+// scans the listed candidates, four per lane in flight (index loads, then
+// float4 gathers), and appends the j inside the cutoff to a per-warp list in
+// shared memory (ballot + popc).  Phase 2 runs the pair terms over that list
+// 32 pairs at a time, so every lane of the expensive part does useful work
+// and the scan carries no force state.  A row with more hits than the list
+// holds is taken in several rounds.
 constexpr int kWarps = 8;
-constexpr int kQueue = 64;
+constexpr int kHitCap = 512;   // per-warp hit list (entries)
+constexpr int kScanU = 4;      // candidates per lane per scan round
 
 template <int ACCUM, bool ENERGY, bool VIRIAL>
 __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
@@ -135,8 +139,7 @@ template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO>
 __global__ void __launch_bounds__(256, 4)
 k_lj_direct(PairArgs a, Accumulators acc) {
   extern __shared__ float sh_tab[];
-  __shared__ float4 sq[kWarps][kQueue];   // dx, dy, dz, q_j
-  __shared__ int2 sj[kWarps][kQueue];     // j, LJ type of j
+  __shared__ int hits_all[kWarps][kHitCap];
   float* sA = sh_tab;
   float* sB = sh_tab + a.n_types * (a.n_types + 1) / 2;
   const int npair = a.n_types * (a.n_types + 1) / 2;
@@ -147,12 +150,14 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
+  int* hits = hits_all[w];
   if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
   // Each block owns a contiguous range of sorted atoms, so the neighbours its
   // warps gather overlap and stay in this SM's L1.
   const int per_block = (a.n + gridDim.x - 1) / gridDim.x;
   const int i_begin = blockIdx.x * per_block;
   const int i_end = min(a.n, i_begin + per_block);
+  const unsigned lt = (1u << lane) - 1u;
   for (int i = i_begin + w; i < i_end; i += kWarps) {
   const float4 pi = a.pos[i];
   const float3 ri = make_float3(pi.x, pi.y, pi.z);
@@ -162,66 +167,56 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   float e_lj = 0.f, e_c = 0.f;
   float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   const int k0 = a.row_start[i], k1 = k0 + a.row_count[i];
-  const unsigned lt = (1u << lane) - 1u;
-  int count = 0;
-  // Four candidates per lane per round: their index loads, then their
-  // coordinate gathers, are all in flight together.
-  constexpr int U = 4;
-  for (int base = k0; base < k1; base += 32 * U) {
-    int jj[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int k = base + 32 * u + lane;
-      jj[u] = k < k1 ? a.cols[k] : -1;
-    }
-    float4 pp[U];
-    int tt[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (jj[u] >= 0) {
-        pp[u] = a.pos[jj[u]];
-        tt[u] = a.type[jj[u]];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (base + 32 * u >= k1) break;  // warp-uniform
-      bool in = false;
-      float4 ent;
-      if (jj[u] >= 0) {
-        const float3 dr = min_image_fast<ORTHO>(make_float3(pp[u].x, pp[u].y, pp[u].z),
-                                                ri, a.cell, a.rcell);
-        const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
-        in = r2 < a.cutoff2;
-        ent = make_float4(dr.x, dr.y, dr.z, pp[u].w);
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, in);
-      if (in) {
-        const int slot = count + __popc(m & lt);
-        sq[w][slot] = ent;
-        sj[w][slot] = make_int2(jj[u], tt[u]);
-      }
-      count += __popc(m);
-      if (count >= 32) {
-        __syncwarp();
-        const int2 jt = sj[w][lane];
-        lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi, sq[w][lane], jt.x,
-                                       jt.y, fx, fy, fz, e_lj, e_c, vir);
-        __syncwarp();
-        if (lane < count - 32) {
-          sq[w][lane] = sq[w][32 + lane];
-          sj[w][lane] = sj[w][32 + lane];
-        }
-        __syncwarp();
-        count -= 32;
-      }
+  {
+    // the warp's next row: start pulling its indices from HBM into L2 now
+    // (row starts are multiples of 8 entries, so 16-byte aligned)
+    const int inext = i + kWarps;
+    if (lane == 0 && inext < i_end) {
+      const int cn = a.row_count[inext];
+      if (cn > 0)
+        prefetch_l2(a.cols + a.row_start[inext], (unsigned)(cn * 4 + 15) & ~15u);
     }
   }
-  __syncwarp();
-  if (lane < count) {
-    const int2 jt = sj[w][lane];
-    lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi, sq[w][lane], jt.x, jt.y,
-                                   fx, fy, fz, e_lj, e_c, vir);
+  for (int base = k0; base < k1;) {
+    // phase 1: candidates -> hit list
+    int count = 0;
+    for (; base < k1 && count <= kHitCap - 32 * kScanU; base += 32 * kScanU) {
+      int jj[kScanU];
+#pragma unroll
+      for (int u = 0; u < kScanU; ++u) {
+        const int k = base + 32 * u + lane;
+        jj[u] = k < k1 ? a.cols[k] : -1;
+      }
+      float4 pp[kScanU];
+#pragma unroll
+      for (int u = 0; u < kScanU; ++u)
+        if (jj[u] >= 0) pp[u] = a.pos[jj[u]];
+#pragma unroll
+      for (int u = 0; u < kScanU; ++u) {
+        bool in = false;
+        if (jj[u] >= 0) {
+          const float3 dr = min_image_fast<ORTHO>(make_float3(pp[u].x, pp[u].y, pp[u].z),
+                                                  ri, a.cell, a.rcell);
+          in = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z < a.cutoff2;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) hits[count + __popc(m & lt)] = jj[u];
+        count += __popc(m);
+      }
+    }
+    __syncwarp();
+    // phase 2: pair terms over the hit list
+    for (int h = lane; h < count; h += 32) {
+      const int j = hits[h];
+      const float4 pj = a.pos[j];
+      const int tj = a.type[j];
+      const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri, a.cell,
+                                              a.rcell);
+      lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi,
+                                     make_float4(dr.x, dr.y, dr.z, pj.w), j, tj, fx, fy,
+                                     fz, e_lj, e_c, vir);
+    }
+    __syncwarp();
   }
   fx = warp_sum(fx);
   fy = warp_sum(fy);
