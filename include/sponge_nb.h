@@ -206,6 +206,10 @@ int snb_lj_soft_long_range_correction(snb_lj_soft* lj, int need_pressure,
                                       float* d_virial, int need_potential,
                                       float* d_potential, float volume,
                                       void* stream);
+/* LJ_SOFT_CORE::Step_Print sums (LJ_soft_core.cpp:890-921): h_sums[0..3] =
+ * {LJ_soft_short, LJ_soft_inter, LJ_soft_intra, LJ_soft_long} from the last
+ * energy evaluation and the last tail correction (host sync). */
+int snb_lj_soft_energy_sums(snb_lj_soft* lj, float* h_sums, void* stream);
 int snb_lj_soft_destroy(snb_lj_soft* lj);
 
 /* ------------------------------------------------------- Particle_Mesh */

@@ -75,6 +75,17 @@ class Oracle:
         L.snbo_lrc_factor.restype = ctypes.c_float
         L.snbo_lrc_factor.argtypes = [ctypes.c_int, _i32p, ctypes.c_int, _f32p,
                                       ctypes.c_float]
+        L.snbo_soft_f64.restype = None
+        L.snbo_soft_f64.argtypes = [
+            ctypes.c_int, _f32p, _f32p, _f32p, _i32p, _i32p, _i32p, ctypes.c_int,
+            ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, ctypes.c_float,
+            ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+            ctypes.c_float, ctypes.c_float, _i64p, _i32p, _f64p, _f64p, _f64p,
+            _f64p, _f64p, _f64p, _f64p, _f64p]
+        L.snbo_soft_lrc.restype = None
+        L.snbo_soft_lrc.argtypes = [
+            ctypes.c_int, _i32p, _i32p, _f32p, _f32p, ctypes.c_float, ctypes.c_float,
+            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
 
     # -- neighbor list (FP32, bit-exact contract) ---------------------------
     def nl_pairs(self, crd, cell, rcell, cutoff, skin, excl_start=None,
@@ -156,6 +167,39 @@ class Oracle:
             float(s.box), beta, kmax, frc.ctypes.data if with_force else None)
         return e, (frc.reshape(n, 3) if with_force else None)
 
+    def soft_f64(self, s, sc, cutoff, beta, lam, alpha, p, sigma, sigma_min,
+                 row_start, cols):
+        """FP64 soft-core direct terms over the half-list rows (row_start,
+        cols); sigma and sigma_min are the input lengths (sigma^6 formed in
+        float as LJ_SOFT_CORE::Initial does)."""
+        n = s.n
+        frc = np.zeros(3 * n)
+        ae, le, inter, intra, ce = (np.zeros(n) for _ in range(5))
+        vir = np.zeros(6 * n)
+        dudl = np.zeros(2)
+        s6 = float(np.float32(sigma) ** np.float32(6))
+        s6min = float(np.float32(sigma_min) ** np.float32(6))
+        self.lib.snbo_soft_f64(
+            n, _c(s.crd, np.float32).reshape(-1), _c(s.charge, np.float32),
+            _c(sc.charge_B_A, np.float32), _c(sc.type_A, np.int32),
+            _c(sc.type_B, np.int32), _c(sc.mask, np.int32), sc.n_types_A,
+            sc.n_types_B, _c(sc.AA, np.float32), _c(sc.AB, np.float32),
+            _c(sc.BA, np.float32), _c(sc.BB, np.float32), s.cell(), s.rcell(),
+            cutoff, beta, lam, alpha, p, s6, s6min, _c(row_start, np.int64),
+            _c(cols if len(cols) else np.zeros(1), np.int32), frc, ae, le, inter,
+            intra, ce, vir, dudl)
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, lj_energy=le,
+                    inter=inter, intra=intra, coulomb_energy=ce,
+                    virial=vir.reshape(n, 6), dudl_lj=float(dudl[0]),
+                    dudl_direct=float(dudl[1]))
+
+    def soft_lrc(self, s, sc, lam, cutoff):
+        f, fti = ctypes.c_double(0), ctypes.c_double(0)
+        self.lib.snbo_soft_lrc(s.n, _c(sc.type_A, np.int32), _c(sc.type_B, np.int32),
+                               _c(sc.AB, np.float32), _c(sc.BB, np.float32), lam,
+                               cutoff, ctypes.byref(f), ctypes.byref(fti))
+        return f.value, fti.value
+
     def lrc_factor(self, s, cutoff):
         return float(self.lib.snbo_lrc_factor(
             s.n, _c(s.lj_type, np.int32), s.n_types, _c(s.lj_B, np.float32),
@@ -196,6 +240,17 @@ class ReferenceCPU:
         L.ref_lj_long_range.restype = ctypes.c_int
         L.ref_lj_long_range.argtypes = [_f32p, _f32p, ctypes.c_float]
         L.ref_lj_long_range_factor.restype = ctypes.c_float
+        L.ref_soft_init.restype = ctypes.c_int
+        L.ref_soft_init.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int, _f32p,
+                                    _f32p, _f32p, _f32p, _i32p, ctypes.c_char_p]
+        L.ref_soft_direct.restype = ctypes.c_int
+        L.ref_soft_direct.argtypes = [_f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
+                                      _f32p, _f32p, ctypes.c_int, ctypes.c_int]
+        L.ref_soft_dhdl.restype = ctypes.c_int
+        L.ref_soft_dhdl.argtypes = [_f32p, _f32p, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_float)]
+        L.ref_soft_long_range.restype = ctypes.c_int
+        L.ref_soft_long_range.argtypes = [_f32p, _f32p, ctypes.c_float, _f32p]
         L.ref_set_threads.argtypes = [ctypes.c_int]
         L.ref_max_threads.restype = ctypes.c_int
         self.n = 0
@@ -313,3 +368,45 @@ class ReferenceCPU:
         self.lib.ref_lj_long_range(vir, pot, volume)
         return dict(virial=vir, potential=float(pot[0]),
                     factor=float(self.lib.ref_lj_long_range_factor()))
+
+    # -- LJ_SOFT_CORE ---------------------------------------------------------
+    def soft_init(self, sc, commands: dict):
+        cmd = ";".join(f"{k}={v}" for k, v in commands.items())
+        rc = self.lib.ref_soft_init(
+            _c(sc.type_A, np.int32), _c(sc.type_B, np.int32), sc.n_types_A,
+            sc.n_types_B, _c(sc.AA, np.float32), _c(sc.AB, np.float32),
+            _c(sc.BA, np.float32), _c(sc.BB, np.float32), _c(sc.mask, np.int32),
+            cmd.encode())
+        if rc != 0:
+            raise RuntimeError("reference soft-core init failed")
+
+    def soft_direct(self, crd=None, need_energy=True, need_virial=True):
+        crd = self.crd if crd is None else _c(crd, np.float32).reshape(-1)
+        n = self.n
+        frc = np.zeros(3 * n, np.float32)
+        ae, vir = np.zeros(n, np.float32), np.zeros(6 * n, np.float32)
+        le, inter, intra, ce = (np.zeros(n, np.float32) for _ in range(4))
+        rc = self.lib.ref_soft_direct(crd, frc, ae, vir, le, inter, intra, ce,
+                                      int(need_energy), int(need_virial))
+        if rc != 0:
+            raise RuntimeError("reference soft-core force failed")
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6),
+                    lj_energy=le, inter=inter, intra=intra, coulomb_energy=ce)
+
+    def soft_dhdl(self, charge_B_A, crd=None, charge_perturbated=1):
+        crd = self.crd if crd is None else _c(crd, np.float32).reshape(-1)
+        out = ctypes.c_float(0)
+        rc = self.lib.ref_soft_dhdl(crd, _c(charge_B_A, np.float32),
+                                    int(charge_perturbated), ctypes.byref(out))
+        if rc != 0:
+            raise RuntimeError("reference soft-core dH/dlambda failed")
+        return float(out.value)
+
+    def soft_long_range(self, volume):
+        vir = np.zeros(6, np.float32)
+        pot = np.zeros(1, np.float32)
+        fac = np.zeros(2, np.float32)
+        if self.lib.ref_soft_long_range(vir, pot, volume, fac) != 0:
+            raise RuntimeError("reference soft-core tail failed")
+        return dict(virial=vir, potential=float(pot[0]), factor=float(fac[0]),
+                    factor_ti=float(fac[1]))

@@ -306,4 +306,102 @@ extern "C"
     }
 
     float ref_lj_long_range_factor() { return g ? g->lj.long_range_factor : 0; }
+
+    /* LJ_SOFT_CORE::Initial on the current system (after ref_init): end
+     * state types and tables, subsystem masks; lambda_lj and soft_core_*
+     * come from `commands` ("key=value;..."). */
+    int ref_soft_init(const int* type_A, const int* type_B, int nA, int nB,
+                      const float* AA, const float* AB, const float* BA,
+                      const float* BB, const int* mask, const char* commands)
+    {
+        if (!g) return -1;
+        REF_TRY({
+            std::string c = commands ? commands : "";
+            size_t pos = 0;
+            while (pos < c.size())
+            {
+                size_t end = c.find(';', pos);
+                if (end == std::string::npos) end = c.size();
+                std::string kv = c.substr(pos, end - pos);
+                size_t eq = kv.find('=');
+                if (eq != std::string::npos)
+                    controller.commands[kv.substr(0, eq)] = kv.substr(eq + 1);
+                pos = end + 1;
+            }
+            auto& sc = Xponge::system.classical_force_field.lj_soft_core;
+            const int n = g->n;
+            sc.atom_numbers = n;
+            sc.atom_type_numbers_A = nA;
+            sc.atom_type_numbers_B = nB;
+            const int pA = nA * (nA + 1) / 2;
+            const int pB = nB * (nB + 1) / 2;
+            sc.LJ_AA.assign(AA, AA + pA);
+            sc.LJ_AB.assign(AB, AB + pA);
+            sc.LJ_BA.assign(BA, BA + pB);
+            sc.LJ_BB.assign(BB, BB + pB);
+            sc.atom_LJ_type_A.assign(type_A, type_A + n);
+            sc.atom_LJ_type_B.assign(type_B, type_B + n);
+            sc.subsystem_division.assign(mask, mask + n);
+            g->lj_soft.Initial(&controller, g->cutoff);
+            g->lj_soft.Get_Local(g->atom_local.data(), n, 0);
+            g->soft_ready = true;
+        });
+        return 0;
+    }
+
+    /* LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial on the
+     * current half list; per-atom LJ, inter/intra LJ and direct Coulomb
+     * energies are copied out of the module. */
+    int ref_soft_direct(const float* crd, float* frc, float* atom_energy,
+                        float* atom_virial, float* lj_energy, float* inter,
+                        float* intra, float* coulomb_energy, int need_energy,
+                        int need_virial)
+    {
+        if (!g || !g->soft_ready) return -1;
+        REF_TRY({
+            std::vector<float> direct(g->n, 0.0f);
+            g->lj_soft.LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial(
+                g->n, g->n, 0, 0, (const VECTOR*)crd, g->charge.data(),
+                (VECTOR*)frc, g->boundary, g->nl.d_nl, g->pm.beta, need_energy,
+                atom_energy, need_virial, (LTMatrix3*)atom_virial,
+                direct.data());
+            const size_t b = sizeof(float) * g->n;
+            if (lj_energy) memcpy(lj_energy, g->lj_soft.d_LJ_energy_atom, b);
+            if (inter) memcpy(inter, g->lj_soft.d_LJ_energy_atom_intersys, b);
+            if (intra) memcpy(intra, g->lj_soft.d_LJ_energy_atom_intrasys, b);
+            if (coulomb_energy) memcpy(coulomb_energy, direct.data(), b);
+        });
+        return 0;
+    }
+
+    /* Get_Partial_H_Partial_Lambda_With_Columb_Direct: the module's return
+     * value (LJ dU/dlambda plus the tail term).  The module evaluates it at
+     * the coordinates of its last direct-force call. */
+    int ref_soft_dhdl(const float* crd, const float* charge_B_A,
+                      int charge_perturbated, float* out)
+    {
+        if (!g || !g->soft_ready) return -1;
+        REF_TRY({
+            *out = g->lj_soft.Get_Partial_H_Partial_Lambda_With_Columb_Direct(
+                0, (const VECTOR*)crd, g->boundary, g->charge.data(),
+                g->nl.d_nl, charge_B_A, g->pm.beta, charge_perturbated);
+        });
+        return 0;
+    }
+
+    int ref_soft_long_range(float* virial6, float* potential, float volume,
+                            float* factors)
+    {
+        if (!g || !g->soft_ready) return -1;
+        REF_TRY({
+            g->lj_soft.Long_Range_Correction(1, (LTMatrix3*)virial6, 1,
+                                             potential, volume);
+            if (factors)
+            {
+                factors[0] = g->lj_soft.long_range_factor;
+                factors[1] = g->lj_soft.long_range_factor_TI;
+            }
+        });
+        return 0;
+    }
 }

@@ -357,6 +357,185 @@ SNBO_API void snbo_direct_f64(int n, const float* crd, const float* charge,
 }
 
 /* ------------------------------------------------------------------ */
+/* Soft-core LJ + direct Coulomb, FP64 run of
+ * Lennard_Jones_And_Direct_Coulomb_Soft_Core_CUDA (LJ_soft_core.cpp:196-461)
+ * with the pair forms of VECTOR_LJ_SOFT_TYPE (LJ_soft_core.h:33-149), single
+ * process (ij_factor 1).  Pairs come from the half-list rows (i, j > i);
+ * energies, the inter/intra split by mask and the virial go to i.  dudl[0]
+ * and dudl[1] receive the LJ and direct-Coulomb dU/dlambda sums. */
+static double sc_lj_e(double A, double B, double r)
+{
+    double r6 = pow(r, -6.0);
+    return (A / 12.0 * r6 - B / 6.0) * r6;
+}
+static double sc_lj_f(double A, double B, double r)
+{
+    return (B - A * pow(r, -6.0)) * pow(r, -8.0);
+}
+static double sc_coul_e(double qq, double beta, double r)
+{
+    return qq * erfc(beta * r) / r;
+}
+static double sc_coul_f(double qq, double beta, double r)
+{
+    double br = beta * r;
+    return qq * pow(r, -3.0) *
+           (br * 1.1283791670955126 * exp(-br * br) + erfc(br));
+}
+static double sc_sigma6(double A, double B, double s6, double s6min)
+{
+    return (A == 0 || B == 0) ? s6 : fmax(0.5 * A / B, s6min);
+}
+static double sc_dudl(double F, double sigma6, double rs, double alpha,
+                      double p, double lambda)
+{
+    const double flt_min = 1.17549435082228751e-38;
+    return p * alpha * (1 - lambda) * pow(lambda + flt_min, p - 1.0) * F *
+           pow(rs, -4.0) * sigma6 / 6.0;
+}
+
+SNBO_API void snbo_soft_f64(int n, const float* crd, const float* charge,
+                            const float* charge_ba, const int* tA, const int* tB,
+                            const int* mask, int nA, int nB, const float* AA_t,
+                            const float* AB_t, const float* BA_t,
+                            const float* BB_t, const float* cell,
+                            const float* rcell, float cutoff, float beta,
+                            float lambda_f, float alpha_f, float p_f,
+                            float sigma6_f, float sigma6_min_f,
+                            const int64_t* row_start, const int* cols,
+                            double* frc, double* atom_energy, double* lj_energy,
+                            double* inter, double* intra, double* coul_energy,
+                            double* virial, double* dudl)
+{
+    const double lam = lambda_f, lam_ = 1.0 - lam, alpha = alpha_f, p = p_f;
+    const double b = beta, s6 = sigma6_f, s6min = sigma6_min_f;
+    const double alp_A = alpha * pow(lam, p), alp_B = alpha * pow(lam_, p);
+    double* fj = (double*)calloc((size_t)3 * n, sizeof(double));
+    double du_lj = 0, du_c = 0;
+    (void)nA;
+    (void)nB;
+#pragma omp parallel reduction(+ : du_lj, du_c)
+    {
+        double* fj_local = (double*)calloc((size_t)3 * n, sizeof(double));
+#pragma omp for schedule(dynamic, 64)
+        for (int i = 0; i < n; ++i)
+        {
+            double fi[3] = {0, 0, 0}, vir[6] = {0, 0, 0, 0, 0, 0};
+            double elj = 0, ec = 0, e_in = 0, e_out = 0;
+            const double qi = charge[i], dqi = charge_ba ? charge_ba[i] : 0.0;
+            for (int64_t k = row_start[i]; k < row_start[i + 1]; ++k)
+            {
+                int j = cols[k];
+                double dr[3];
+                min_image_f64(crd + 3 * j, crd + 3 * i, cell, rcell, dr);
+                double r = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+                if (!(r < cutoff)) continue;
+                int a1 = tA[i], a2 = tA[j], b1 = tB[i], b2 = tB[j];
+                int pa = (a1 > a2 ? a1 * (a1 + 1) / 2 + a2 : a2 * (a2 + 1) / 2 + a1);
+                int pb = (b1 > b2 ? b1 * (b1 + 1) / 2 + b2 : b2 * (b2 + 1) / 2 + b1);
+                double AA = AA_t[pa], AB = AB_t[pa], BA = BA_t[pb], BB = BB_t[pb];
+                double qq = qi * (double)charge[j];
+                double dqj = charge_ba ? charge_ba[j] : 0.0;
+                double qd = dqj * qi + (double)charge[j] * dqi;
+                double fs, e_lj_pair, e_c_pair;
+                if (BA * AA != 0 || BA + AA == 0)
+                {
+                    fs = lam_ * sc_lj_f(AA, AB, r) + lam * sc_lj_f(BA, BB, r) -
+                         sc_coul_f(qq, b, r);
+                    e_c_pair = sc_coul_e(qq, b, r);
+                    e_lj_pair = lam_ * sc_lj_e(AA, AB, r) + lam * sc_lj_e(BA, BB, r);
+                    du_lj += sc_lj_e(BA, BB, r) - sc_lj_e(AA, AB, r);
+                    du_c += erfc(b * r) * qd / r;
+                }
+                else
+                {
+                    double sA = sc_sigma6(AA, AB, s6, s6min);
+                    double sB = sc_sigma6(BA, BB, s6, s6min);
+                    double r6 = pow(r, 6.0);
+                    double rA = pow(r6 + alp_A * sA, 1.0 / 6.0);
+                    double rB = pow(r6 + alp_B * sB, 1.0 / 6.0);
+                    double r4 = pow(r, 4.0);
+                    double flA = r4 * (AB - AA * pow(rA, -6.0)) * pow(rA, -12.0);
+                    double flB = r4 * (BB - BA * pow(rB, -6.0)) * pow(rB, -12.0);
+                    double bA = b * rA, bB = b * rB;
+                    double fcA = qq * r4 *
+                                 (exp(-bA * bA) * 1.1283791670955126 * b +
+                                  erfc(bA) / rA) * pow(rA, -6.0);
+                    double fcB = qq * r4 *
+                                 (exp(-bB * bB) * 1.1283791670955126 * b +
+                                  erfc(bB) / rB) * pow(rB, -6.0);
+                    fs = lam_ * flA + lam * flB - (lam_ * fcA + lam * fcB);
+                    e_c_pair = lam_ * sc_coul_e(qq, b, rA) + lam * sc_coul_e(qq, b, rB);
+                    e_lj_pair = lam_ * sc_lj_e(AA, AB, rA) + lam * sc_lj_e(BA, BB, rB);
+                    du_lj += sc_lj_e(BA, BB, rB) - sc_lj_e(AA, AB, rA);
+                    du_lj += sc_dudl(sc_lj_f(AA, AB, rA), sA, rA, alpha, p, lam) -
+                             sc_dudl(sc_lj_f(BA, BB, rB), sB, rB, alpha, p, lam_);
+                    du_c += sc_coul_e(qq, b, rB) - sc_coul_e(qq, b, rA);
+                    du_c += sc_dudl(sc_coul_f(qq, b, rB), sB, rB, alpha, p, lam_) -
+                            sc_dudl(sc_coul_f(qq, b, rA), sA, rA, alpha, p, lam);
+                    du_c += lam * erfc(b * rB) * qd / rB + lam_ * erfc(b * rA) * qd / rA;
+                }
+                double fl[3] = {fs * dr[0], fs * dr[1], fs * dr[2]};
+                for (int c = 0; c < 3; ++c)
+                {
+                    fi[c] += fl[c];
+                    fj_local[3 * j + c] -= fl[c];
+                }
+                virial_add(vir, fl, dr, -1.0);
+                elj += e_lj_pair;
+                ec += e_c_pair;
+                if (mask[i] == mask[j])
+                    e_in += e_lj_pair;
+                else
+                    e_out += e_lj_pair;
+            }
+            for (int c = 0; c < 3; ++c) frc[3 * i + c] += fi[c];
+            if (atom_energy) atom_energy[i] += elj + ec;
+            if (lj_energy) lj_energy[i] += elj;
+            if (coul_energy) coul_energy[i] += ec;
+            if (intra) intra[i] += e_in;
+            if (inter) inter[i] += e_out;
+            if (virial)
+                for (int c = 0; c < 6; ++c) virial[6 * i + c] += vir[c];
+        }
+#pragma omp critical
+        for (int k = 0; k < 3 * n; ++k) fj[k] += fj_local[k];
+        free(fj_local);
+    }
+    for (int k = 0; k < 3 * n; ++k) frc[k] += fj[k];
+    free(fj);
+    if (dudl)
+    {
+        dudl[0] = du_lj;
+        dudl[1] = du_c;
+    }
+}
+
+/* Tail factors of LJ_SOFT_CORE::Initial (LJ_soft_core.cpp:640-672): the
+ * lambda-mixed sum over all atom pairs of B' (Total_C6_Get) and the state
+ * difference (Total_C6_B_A_Get), each times -2/3 pi / rc^3 / 6. */
+SNBO_API void snbo_soft_lrc(int n, const int* tA, const int* tB, const float* AB,
+                            const float* BB, float lambda, float cutoff,
+                            double* factor, double* factor_ti)
+{
+    double s = 0, sti = 0;
+    const double lam = lambda, lam_ = 1.0 - lam;
+#pragma omp parallel for reduction(+ : s, sti)
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+        {
+            int a1 = tA[i], a2 = tA[j], b1 = tB[i], b2 = tB[j];
+            int pa = (a1 > a2 ? a1 * (a1 + 1) / 2 + a2 : a2 * (a2 + 1) / 2 + a1);
+            int pb = (b1 > b2 ? b1 * (b1 + 1) / 2 + b2 : b2 * (b2 + 1) / 2 + b1);
+            s += lam_ * AB[pa] + lam * BB[pb];
+            sti += (double)BB[pb] - AB[pa];
+        }
+    const double k = -2.0 / 3.0 * 3.14159265358979323846 / cutoff / cutoff / cutoff / 6.0;
+    *factor = s * k;
+    *factor_ti = sti * k;
+}
+
+/* ------------------------------------------------------------------ */
 /* Excluded-pair correction, FP64 run of
  * MPI_PME_Excluded_Force_With_Atom_Energy_Correction (PM_force.cpp:1745-1817)
  * with factor 1 (single process). */

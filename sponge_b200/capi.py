@@ -55,7 +55,7 @@ EXPORTED = [
     "snb_lj_long_range_correction", "snb_lj_energy_sum", "snb_lj_long_range_factor",
     "snb_lj_destroy",
     "snb_lj_soft_create", "snb_lj_soft_pme_direct_force", "snb_lj_soft_dh_dlambda",
-    "snb_lj_soft_long_range_correction", "snb_lj_soft_destroy",
+    "snb_lj_soft_long_range_correction", "snb_lj_soft_energy_sums", "snb_lj_soft_destroy",
     "snb_pme_create", "snb_pme_beta", "snb_pme_grid", "snb_pme_reciprocal_force",
     "snb_pme_excluded_force", "snb_pme_energies", "snb_pme_destroy",
     "snb_pme_excluded_force_noalloc",
@@ -100,6 +100,7 @@ _SIGS = {
     "snb_lj_soft_dh_dlambda": (_I, [_P, _P, _P, _P, snb_boundary, _P, _F, _I,
                                     ctypes.POINTER(ctypes.c_double), _P]),
     "snb_lj_soft_long_range_correction": (_I, [_P, _I, _P, _I, _P, _F, _P]),
+    "snb_lj_soft_energy_sums": (_I, [_P, _P, _P]),
     "snb_lj_soft_destroy": (_I, [_P]),
     "snb_pme_create": (_I, [ctypes.POINTER(snb_options), _I, snb_boundary, _P, _F,
                             ctypes.POINTER(_P)]),

@@ -466,6 +466,8 @@ struct snb_lj_soft {
   float lambda = 0.f, alpha = 0.5f, p = 1.f, sigma6 = 729.f, sigma6_min = 0.f;
   float cutoff = 10.f;
   float lrc = 0.f, lrc_ti = 0.f;
+  float lrc_energy = 0.f;        // h_LJ_long_energy of the last tail call
+  double* d_sums = nullptr;      // [3] scratch for Step_Print sums
 };
 
 __global__ void k_pack_soft(int n, const int* __restrict__ perm,
@@ -686,9 +688,28 @@ extern "C" int snb_lj_soft_long_range_correction(snb_lj_soft* h, int need_pressu
                                                  float* d_potential, float volume,
                                                  void* stream) {
   if (!h) return fail(kBadInput, "lj_soft_long_range_correction: null handle");
+  if (need_potential > 0) h->lrc_energy = h->lrc / volume;
   return launch_add_scalars(need_potential > 0 ? d_potential : nullptr,
                             need_pressure > 0 ? d_virial : nullptr, nullptr,
                             h->lrc / volume, 2 * h->lrc / volume, 1, S(stream));
+}
+
+extern "C" int snb_lj_soft_energy_sums(snb_lj_soft* h, float* out, void* stream) {
+  if (!h || !out) return fail(kBadInput, "lj_soft_energy_sums: null argument");
+  cudaStream_t st = S(stream);
+  if (!h->d_sums) SNB_CUDA_TRY(cudaMalloc(&h->d_sums, sizeof(double) * 3));
+  int rc = launch_sum_float(h->n, h->d_lj_energy, h->d_sums, st);
+  if (!rc) rc = launch_sum_float(h->n, h->d_inter, h->d_sums + 1, st);
+  if (!rc) rc = launch_sum_float(h->n, h->d_intra, h->d_sums + 2, st);
+  if (rc) return rc;
+  double v[3];
+  SNB_CUDA_TRY(cudaMemcpyAsync(v, h->d_sums, sizeof(v), cudaMemcpyDeviceToHost, st));
+  SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  out[0] = (float)v[0];
+  out[1] = (float)v[1];
+  out[2] = (float)v[2];
+  out[3] = h->lrc_energy;
+  return kOk;
 }
 
 extern "C" int snb_lj_soft_destroy(snb_lj_soft* h) {
@@ -696,7 +717,8 @@ extern "C" int snb_lj_soft_destroy(snb_lj_soft* h) {
   for (void* p : {(void*)h->d_AA, (void*)h->d_AB, (void*)h->d_BA, (void*)h->d_BB,
                   (void*)h->d_par, (void*)h->d_par_local, (void*)h->d_par_sorted,
                   (void*)h->d_pos, (void*)h->d_dq_sorted, (void*)h->d_lj_energy,
-                  (void*)h->d_inter, (void*)h->d_intra, (void*)h->d_dudl})
+                  (void*)h->d_inter, (void*)h->d_intra, (void*)h->d_dudl,
+                  (void*)h->d_sums})
     cudaFree(p);
   acc_free(h->acc);
   delete h;

@@ -233,6 +233,132 @@ def water_box(n_waters: int, seed: int = 0, ion_pairs: int | None = 0,
                   box=float(box))
 
 
+def _subset(s: System, keep: np.ndarray) -> System:
+    """The atoms of `s` where `keep` (whole molecules only), re-indexed."""
+    idx = np.flatnonzero(keep)
+    new = -np.ones(s.n, np.int64)
+    new[idx] = np.arange(len(idx))
+    excl = []
+    for i in idx:
+        a, c = s.excl_start[i], s.excl_numbers[i]
+        excl.append([int(new[j]) for j in s.excl_list[a:a + c]])
+    numbers = np.array([len(e) for e in excl], np.int32)
+    start = np.zeros(len(idx), np.int32)
+    start[1:] = np.cumsum(numbers)[:-1]
+    flat = np.array([j for e in excl for j in e], np.int32)
+    bonds = s.bonds[keep[s.bonds[:, 0]]] if len(s.bonds) else s.bonds
+    angles = s.angles[keep[s.angles[:, 1]]] if len(s.angles) else s.angles
+    return dataclasses.replace(
+        s, crd=s.crd[idx], vel=s.vel[idx], charge=s.charge[idx],
+        lj_type=s.lj_type[idx], mass=s.mass[idx], excl_start=start,
+        excl_numbers=numbers, excl_list=flat,
+        bonds=new[bonds].astype(np.int32).reshape(-1, 2),
+        angles=new[angles].astype(np.int32).reshape(-1, 3))
+
+
+@dataclasses.dataclass
+class SoftCore:
+    """LJ_SOFT_CORE inputs of a box with an alchemical solute: end-state types
+    and A'/B' tables (same stored form as the plain tables), subsystem masks
+    and the charge difference B - A (scaled by 18.2223)."""
+    type_A: np.ndarray
+    type_B: np.ndarray
+    n_types_A: int
+    n_types_B: int
+    AA: np.ndarray
+    AB: np.ndarray
+    BA: np.ndarray
+    BB: np.ndarray
+    mask: np.ndarray
+    charge_B_A: np.ndarray
+
+
+def soft_core_box(n_waters: int, n_solute: int = 64, seed: int = 0,
+                  ion_pairs: int | None = None, clearance: float = 2.5):
+    """A water/NaCl box with a seeded compact cluster of `n_solute` LJ sites at
+    its centre (rejection-sampled at >= 2.5 A separations inside a sphere;
+    sigma ~ U[3, 4] A, epsilon ~ U[0.05, 0.2] kcal/mol, charges ~ N(0, 0.3) e
+    re-centred to sum 0).  Waters and ions within `clearance` of a site are
+    removed.  State A has the solute's LJ sites on (one type per site,
+    Lorentz-Berthelot mixing); state B turns them into a type without LJ and
+    their charges off.  Returns (System, SoftCore)."""
+    s = water_box(n_waters, seed=seed, ion_pairs=ion_pairs)
+    rng = np.random.default_rng(50_000 + seed)
+    radius = max(4.0, 1.4 * (n_solute ** (1.0 / 3.0)) * 2.5 / 1.6)
+    centre = np.full(3, s.box / 2)
+    sites = []
+    while len(sites) < n_solute:
+        p = rng.uniform(-radius, radius, 3)
+        if np.linalg.norm(p) > radius:
+            continue
+        if all(np.linalg.norm(p - q) >= 2.5 for q in sites):
+            sites.append(p)
+    sites = np.asarray(sites) + centre
+    # drop whole molecules near the cluster (water = O followed by its two H)
+    d = s.crd[:, None, :].astype(np.float64) - sites[None]
+    d -= np.round(d / s.box) * s.box
+    near = (np.linalg.norm(d, axis=2) < clearance).any(1)
+    mol = np.zeros(s.n, np.int64)
+    m = -1
+    for i in range(s.n):
+        if s.lj_type[i] != 1:
+            m += 1
+        mol[i] = m
+    drop_mol = np.zeros(m + 1, bool)
+    drop_mol[mol[near]] = True
+    w = _subset(s, ~drop_mol[mol])
+    sig = rng.uniform(3.0, 4.0, n_solute)
+    eps = rng.uniform(0.05, 0.2, n_solute)
+    q = rng.normal(0.0, 0.3, n_solute)
+    q -= q.mean()
+    # A-state types: 0..3 water/ions, 4 + k solute site k
+    nA = 4 + n_solute
+    sigA = np.concatenate([LJ_SIGMA, sig])
+    epsA = np.concatenate([LJ_EPS, eps])
+    npA = nA * (nA + 1) // 2
+    AA = np.zeros(npA, np.float32)
+    AB = np.zeros(npA, np.float32)
+    for a in range(nA):
+        for b in range(a + 1):
+            e = math.sqrt(epsA[a] * epsA[b])
+            if e == 0.0:
+                continue
+            sg = 0.5 * (sigA[a] + sigA[b])
+            k = lj_pair_index(a, b)
+            AA[k] = np.float32(4.0 * e * sg ** 12) * np.float32(12.0)
+            AB[k] = np.float32(4.0 * e * sg ** 6) * np.float32(6.0)
+    # B-state types: 0..3 as in A, 4 a site without LJ
+    nB = 5
+    BA = np.zeros(nB * (nB + 1) // 2, np.float32)
+    BB = np.zeros_like(BA)
+    A4, B4 = lj_tables(4)
+    BA[:len(A4)] = A4
+    BB[:len(B4)] = B4
+    n0 = w.n
+    n = n0 + n_solute
+    crd = np.concatenate([w.crd, sites.astype(np.float32)])
+    charge = np.concatenate([w.charge, (q * CHARGE_SCALE).astype(np.float32)])
+    typeA = np.concatenate([w.lj_type, 4 + np.arange(n_solute, dtype=np.int32)])
+    typeB = np.concatenate([w.lj_type, np.full(n_solute, 4, np.int32)])
+    mass = np.concatenate([w.mass, np.full(n_solute, 12.011, np.float32)])
+    sol_vel = rng.normal(size=(n_solute, 3)) * np.sqrt(KB * 300.0 / 12.011)
+    vel = np.concatenate([w.vel, sol_vel.astype(np.float32)])
+    sys_ = dataclasses.replace(
+        w, crd=crd.astype(np.float32), vel=vel.astype(np.float32), charge=charge,
+        lj_type=typeA.astype(np.int32), lj_A=AA, lj_B=AB, mass=mass.astype(np.float32),
+        excl_start=np.concatenate([w.excl_start, np.full(n_solute, len(w.excl_list),
+                                                         np.int32)]).astype(np.int32),
+        excl_numbers=np.concatenate([w.excl_numbers, np.zeros(n_solute, np.int32)]),
+        n_types=nA)
+    soft = SoftCore(type_A=typeA.astype(np.int32), type_B=typeB.astype(np.int32),
+                    n_types_A=nA, n_types_B=nB, AA=AA, AB=AB, BA=BA, BB=BB,
+                    mask=np.concatenate([np.zeros(n0, np.int32),
+                                         np.ones(n_solute, np.int32)]),
+                    charge_B_A=np.concatenate([np.zeros(n0, np.float32),
+                                               -charge[n0:]]).astype(np.float32))
+    return sys_, soft
+
+
 def config_small(seed: int = 0) -> System:
     """3,000 waters (9,000 atoms), L = 44.77 A, grid 48^3, cutoff 8, skin 2."""
     return water_box(3000, seed=seed, ion_pairs=0)

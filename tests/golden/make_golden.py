@@ -69,12 +69,57 @@ def make_case(name, s, cutoff, skin):
     print(path, os.path.getsize(path), "bytes,", len(pairs), "pairs")
 
 
+def make_soft_case(name, s, sc, cutoff, skin, params):
+    """LJ_SOFT_CORE on a box with an alchemical solute: forces, the energy
+    split, virial, dH/dlambda and the tail factors from the reference."""
+    ref = ReferenceCPU(exact=False)
+    beta = ref.init(s, cutoff, skin)
+    ref.soft_init(sc, params)
+    counts, serial, ov = ref.nl_update()
+    assert not ov.any()
+    pairs = reference_pairs(counts, serial)
+    r = ref.soft_direct()
+    dhdl = ref.soft_dhdl(sc.charge_B_A)
+    V = float(np.float32(s.box) ** 3)
+    lr = ref.soft_long_range(V)
+    out = dict(
+        crd=s.crd, charge=s.charge, lj_type=s.lj_type, lj_A=s.lj_A, lj_B=s.lj_B,
+        excl_start=s.excl_start, excl_numbers=s.excl_numbers, excl_list=s.excl_list,
+        box=np.float64(s.box), cutoff=np.float32(cutoff), skin=np.float32(skin),
+        beta=np.float32(beta), nl_pair_total=np.int64(len(pairs)),
+        nl_pair_sha256=np.array(pair_digest(pairs)),
+        type_A=sc.type_A, type_B=sc.type_B, n_types_A=np.int32(sc.n_types_A),
+        n_types_B=np.int32(sc.n_types_B), AA=sc.AA, AB=sc.AB, BA=sc.BA, BB=sc.BB,
+        mask=sc.mask, charge_B_A=sc.charge_B_A,
+        lam=np.float32(params["lambda_lj"]), alpha=np.float32(params["soft_core_alpha"]),
+        p=np.float32(params["soft_core_powfer"]),
+        sigma=np.float32(params["soft_core_sigma"]),
+        sigma_min=np.float32(params["soft_core_sigma_min"]),
+        frc=r["frc"], atom_energy=r["atom_energy"], virial=r["virial"],
+        lj_energy=r["lj_energy"], inter=r["inter"], intra=r["intra"],
+        coulomb_energy=r["coulomb_energy"], dhdl=np.float32(dhdl),
+        lrc_factor=np.float32(lr["factor"]), lrc_factor_ti=np.float32(lr["factor_ti"]),
+        lrc_potential=np.float32(lr["potential"]), lrc_virial=lr["virial"],
+    )
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes,", len(pairs), "pairs")
+
+
 def main():
     build_oracle()
     # 216 waters, L = 18.63 A, grid 20^3, cutoff 8
     make_case("water216_rc8", systems.water_box(216, seed=1), 8.0, 2.0)
     # 343 waters + 1 NaCl pair, cutoff 9, skin 1.5 (non-default keys)
     make_case("water343_nacl_rc9", systems.water_box(343, seed=5, ion_pairs=1), 9.0, 1.5)
+    # 300 waters + a 16-site alchemical solute; two soft-core parameter sets
+    s, sc = systems.soft_core_box(300, n_solute=16, seed=1)
+    make_soft_case("soft_water300_s16_lam050", s, sc, 8.0, 2.0,
+                   {"lambda_lj": 0.5, "soft_core_alpha": 0.5, "soft_core_powfer": 1.0,
+                    "soft_core_sigma": 3.0, "soft_core_sigma_min": 0.0})
+    make_soft_case("soft_water300_s16_lam025_p2", s, sc, 8.0, 2.0,
+                   {"lambda_lj": 0.25, "soft_core_alpha": 0.7, "soft_core_powfer": 2.0,
+                    "soft_core_sigma": 3.2, "soft_core_sigma_min": 3.6})
 
 
 if __name__ == "__main__":

@@ -203,3 +203,54 @@ def engine_set_water_bonded(h, s):
                                          aa.ctypes.data, ab.ctypes.data, ac.ctypes.data,
                                          ak.ctypes.data, at.ctypes.data),
                "engine_set_bonded")
+
+
+def soft_create(box: Box, sc, cutoff, params: dict, accumulation="fixed64"):
+    """snb_lj_soft handle for a SoftCore description; params are the
+    reference's keys (lambda_lj, soft_core_alpha, ...)."""
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    o = capi.options(cutoff=cutoff, accumulation=accumulation, **params)
+    arr = lambda a, dt: np.ascontiguousarray(a, dt)  # noqa: E731
+    tA, tB = arr(sc.type_A, np.int32), arr(sc.type_B, np.int32)
+    AA, AB = arr(sc.AA, np.float32), arr(sc.AB, np.float32)
+    BA, BB = arr(sc.BA, np.float32), arr(sc.BB, np.float32)
+    mask = arr(sc.mask, np.int32)
+    capi.check(lib.snb_lj_soft_create(ctypes.byref(o), box.n, sc.n_types_A, sc.n_types_B,
+                                      tA.ctypes.data, tB.ctypes.data, AA.ctypes.data,
+                                      AB.ctypes.data, BA.ctypes.data, BB.ctypes.data,
+                                      mask.ctypes.data, cutoff, ctypes.byref(h)),
+               "lj_soft_create")
+    return h
+
+
+def soft_force(h, nl, box: Box, sc, beta, energy=True, virial=True):
+    lib = capi.load()
+    n = box.n
+    frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+    ae = torch.zeros(n, dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6 * n, dtype=torch.float32, device="cuda")
+    ce = torch.zeros(n, dtype=torch.float32, device="cuda")
+    dq = dev(sc.charge_B_A, np.float32)
+    capi.check(lib.snb_lj_soft_pme_direct_force(
+        h, n, n, 0, ptr(box.crd), ptr(box.charge), ptr(dq), ptr(frc), box.b, nl,
+        ctypes.c_float(beta), int(energy), ptr(ae), int(virial), ptr(vir), ptr(ce),
+        stream()), "lj_soft_pme_direct_force")
+    sums = np.zeros(4, np.float32)
+    if energy:
+        capi.check(lib.snb_lj_soft_energy_sums(h, sums.ctypes.data, stream()),
+                   "lj_soft_energy_sums")
+    torch.cuda.synchronize()
+    return dict(frc=frc.cpu().numpy().reshape(n, 3), atom_energy=ae.cpu().numpy(),
+                virial=vir.cpu().numpy().reshape(n, 6), coulomb_energy=ce.cpu().numpy(),
+                sums=sums)
+
+
+def soft_dhdl(h, nl, box: Box, sc, beta):
+    lib = capi.load()
+    dq = dev(sc.charge_B_A, np.float32)
+    out = ctypes.c_double(0)
+    capi.check(lib.snb_lj_soft_dh_dlambda(h, ptr(box.crd), ptr(box.charge), ptr(dq), box.b,
+                                          nl, ctypes.c_float(beta), 1, ctypes.byref(out),
+                                          stream()), "lj_soft_dh_dlambda")
+    return out.value

@@ -14,7 +14,9 @@ import numpy as np
 import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-GOLDEN = sorted(f for f in os.listdir(os.path.join(HERE, "golden")) if f.endswith(".npz"))
+_FIXTURES = sorted(f for f in os.listdir(os.path.join(HERE, "golden")) if f.endswith(".npz"))
+GOLDEN = [f for f in _FIXTURES if not f.startswith("soft_")]
+SOFT = [f for f in _FIXTURES if f.startswith("soft_")]
 
 
 def load_case(name):
@@ -122,3 +124,44 @@ def test_reference_build_reproduces_golden_when_present(name=GOLDEN[0]):
     assert np.array_equal(counts, z["nl_counts"])
     lj = ref.lj_direct()
     assert rel_rms(lj["frc"], z["lj_frc"].astype(np.float64)) < 1e-6
+
+
+def load_soft_case(name):
+    from sponge_b200 import systems
+    s, z = load_case(name)
+    sc = systems.SoftCore(
+        type_A=z["type_A"], type_B=z["type_B"], n_types_A=int(z["n_types_A"]),
+        n_types_B=int(z["n_types_B"]), AA=z["AA"], AB=z["AB"], BA=z["BA"], BB=z["BB"],
+        mask=z["mask"], charge_B_A=z["charge_B_A"])
+    s.n_types = int(z["n_types_A"])
+    return s, sc, z
+
+
+@pytest.mark.parametrize("name", SOFT)
+def test_oracle_soft_core_matches_reference(oracle, name):
+    """FP64 soft-core restatement against LJ_SOFT_CORE's own output: forces,
+    the energy split (total, LJ, inter/intra subsystem, direct Coulomb),
+    virial, dH/dlambda and the tail factors, to FP32 accuracy."""
+    s, sc, z = load_soft_case(name)
+    cutoff, beta = float(z["cutoff"]), float(z["beta"])
+    rs, cols = oracle.nl_pairs_system(s, cutoff, float(z["skin"]))
+    i = np.repeat(np.arange(s.n), np.diff(rs))
+    pairs = np.stack([i, cols.astype(np.int64)], 1)
+    digest = hashlib.sha256(np.ascontiguousarray(pairs, np.int32).tobytes()).hexdigest()
+    assert digest == str(z["nl_pair_sha256"])
+    lam = float(z["lam"])
+    d = oracle.soft_f64(s, sc, cutoff, beta, lam, float(z["alpha"]), float(z["p"]),
+                        float(z["sigma"]), float(z["sigma_min"]), rs, cols)
+    assert rel_rms(z["frc"], d["frc"]) < 5e-6
+    for k in ("atom_energy", "lj_energy", "inter", "intra", "coulomb_energy"):
+        scale = np.abs(d[k]).sum()
+        assert abs(z[k].astype(np.float64).sum() - d[k].sum()) < 2e-6 * scale, k
+        assert np.abs(z[k] - d[k]).max() < 2e-3, k
+    vs = z["virial"].astype(np.float64).sum(0)
+    assert np.all(np.abs(vs - d["virial"].sum(0)) < 1e-5 * np.abs(vs).max() + 1e-3)
+    fac, fti = oracle.soft_lrc(s, sc, lam, cutoff)
+    assert fac == pytest.approx(float(z["lrc_factor"]), rel=1e-6)
+    assert fti == pytest.approx(float(z["lrc_factor_ti"]), rel=1e-6)
+    V = float(np.float32(s.box) ** 3)
+    # the reference sums dH/dlambda in float over the atoms
+    assert d["dudl_lj"] + fti / V == pytest.approx(float(z["dhdl"]), rel=2e-5, abs=1e-3)
