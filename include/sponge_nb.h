@@ -283,6 +283,25 @@ int snb_engine_create(const snb_options* opt, int atom_numbers,
                       const int* h_excluded_list_start,
                       const int* h_excluded_numbers, const int* h_excluded_list,
                       int excluded_list_length, snb_engine** out);
+/* No counterpart in the reference (it runs one system per process).  A batch
+ * of n_systems independent rectangular boxes advanced together: the atoms of
+ * system s are the next atoms_per_system[s] atoms of every per-atom array (all
+ * systems share one LJ type table), box_lengths[3s..3s+2] is its box, and
+ * exclusion indices are global atom indices that stay inside their system.
+ * Every engine call below then acts on all systems at once, each step being
+ * one launch per phase over all boxes (one neighbor list, one pair kernel,
+ * one PME spread / gather with a grid per box, one batched cuFFT plan per
+ * grid size).  Each box gets the single-box defaults: its own cell grid and
+ * PME grid (by PM_grid_spacing); PME every step, displacement-triggered list
+ * updates and fixed-point accumulation are required.  Energies and virials
+ * from snb_engine_force are sums over the systems. */
+int snb_batch_create(const snb_options* opt, int n_systems,
+                     const int* atoms_per_system, const float* box_lengths,
+                     int atom_type_numbers, const int* h_atom_LJ_type,
+                     const float* h_LJ_A, const float* h_LJ_B, const float* h_charge,
+                     const int* h_excluded_list_start, const int* h_excluded_numbers,
+                     const int* h_excluded_list, int excluded_list_length,
+                     snb_engine** out);
 /* frc (float[3N]) += nonbonded force at crd (float[3N]).  When need_energy /
  * need_virial, the FP64 totals are written to d_totals[0..7] =
  * {LJ, LJ long-range, direct Coulomb, excluded correction, PME reciprocal,

@@ -18,11 +18,11 @@ int launch_bonded(int nb, const int* ba, const int* bb, const float* bk,
                   const int* ac, const float* ak, const float* at0,
                   const float3* crd, const Cell& cell, const Cell& rcell,
                   const int* map, Accumulators& acc, long long* e_total,
-                  bool energy, cudaStream_t st);
+                  bool energy, cudaStream_t st, const BatchView& bv);
 int launch_leap_frog(int n, const int* map, Accumulators& acc, float3* crd,
                      float3* vel, const float* inv_mass, float dt,
                      const float3* old_crd, const Cell& cell, const Cell& rcell,
-                     float permit2, int* flags, cudaStream_t st);
+                     float permit2, int* flags, cudaStream_t st, const BatchView& bv);
 int launch_totals(int n, Accumulators& acc, long long* isum, const long long* bonded,
                   const double* pme_sums, double lrc_energy, double lrc_virial,
                   double* totals, bool energy, bool virial, bool have_pme,
@@ -118,6 +118,14 @@ struct snb_engine {
   const float* g_invm = nullptr;
   float g_dt = 0.f;
   cudaStream_t g_stream = nullptr;
+  // a batch of independent boxes (nsys > 0)
+  int nsys = 0;
+  std::vector<SysGeom> h_sys;
+  SysGeom* d_sys = nullptr;
+  int* d_sys_of = nullptr;
+  BatchView bv;
+  double lrc_energy = 0.0;   // tail energy summed over the boxes
+  double lrc_virial = 0.0;   // tail virial (diagonal) summed over the boxes
   cudaStream_t side = nullptr;  // captures the conditional rebuild body
   int body_kernels = 0;         // kernel nodes inside the rebuild body
   // recovery snapshot for neighbor-list overflow
@@ -836,6 +844,88 @@ extern "C" int snb_pme_destroy(snb_pme* h) {
 }
 
 // ============================================================= engine
+// Everything of engine creation after the neighbor list and PME: LJ tables,
+// charges, exclusions, accumulators and the step scratch.
+static int engine_finish_create(snb_engine* e, int n, int n_types, const int* h_type,
+                                const float* h_A, const float* h_B, const float* h_charge,
+                                const int* h_es, const int* h_en, const int* h_el,
+                                int n_excl) {
+  int rc = acc_init(e->acc, n);
+  if (rc) return rc;
+  LJParams& p = e->lj;
+  p.n_types = n_types;
+  p.n_pairs = n_types * (n_types + 1) / 2;
+  p.h_type.assign(h_type, h_type + n);
+  p.h_A.assign(h_A, h_A + p.n_pairs);
+  p.h_B.assign(h_B, h_B + p.n_pairs);
+  p.cutoff = e->opt.cutoff;
+  for (int i = 0; i < n; ++i)
+    if (h_type[i] < 0 || h_type[i] >= n_types)
+      return fail(kBadInput, "engine_create: LJ type out of range");
+  if (e->nsys > 0) {
+    // tail correction per box (its own type histogram and volume)
+    e->lrc_energy = e->lrc_virial = 0.0;
+    for (const auto& g : e->h_sys) {
+      std::vector<int> ts(h_type + g.atom_begin, h_type + g.atom_end);
+      const double f = lrc_factor(ts, n_types, p.h_B, p.cutoff);
+      e->lrc_energy += f / g.volume;
+      e->lrc_virial += 2.0 * f / g.volume;
+    }
+  } else {
+    p.long_range_factor = lrc_factor(p.h_type, n_types, p.h_B, p.cutoff);
+    const double vol = (double)e->cell.a11 * e->cell.a22 * e->cell.a33;
+    e->lrc_energy = p.long_range_factor / vol;
+    e->lrc_virial = 2.0 * p.long_range_factor / vol;
+  }
+  SNB_CUDA_TRY(cudaMalloc(&p.d_A, sizeof(float) * p.n_pairs));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_B, sizeof(float) * p.n_pairs));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_A, h_A, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_B, h_B, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_type, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_type, h_type, sizeof(int) * n, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_charge, sizeof(float) * n));
+  SNB_CUDA_TRY(cudaMemcpy(e->d_charge, h_charge, sizeof(float) * n, cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_pos, sizeof(float4) * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_type_sorted, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_start, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_numbers, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_list, sizeof(int) * std::max(n_excl, 1)));
+  if (h_es && h_en) {
+    for (int i = 0; i < n; ++i) {
+      if (h_en[i] < 0 || (h_en[i] > 0 && (h_es[i] < 0 || h_es[i] + h_en[i] > n_excl)))
+        return fail(kBadInput, "engine_create: exclusion list out of range");
+      for (int k = 0; k < h_en[i]; ++k) {
+        const int j = h_el[h_es[i] + k];
+        if (j < 0 || j >= n)
+          return fail(kBadInput, "engine_create: excluded atom index out of range");
+        if (e->nsys > 0) {  // an exclusion must stay inside its box
+          int si = 0, sj = 0;
+          while (i >= e->h_sys[si].atom_end) ++si;
+          while (j >= e->h_sys[sj].atom_end) ++sj;
+          if (si != sj)
+            return fail(kBadInput, "batch_create: exclusion between two systems");
+        }
+      }
+    }
+    SNB_CUDA_TRY(cudaMemcpy(e->d_excl_start, h_es, sizeof(int) * n, cudaMemcpyHostToDevice));
+    SNB_CUDA_TRY(cudaMemcpy(e->d_excl_numbers, h_en, sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (n_excl > 0)
+      SNB_CUDA_TRY(cudaMemcpy(e->d_excl_list, h_el, sizeof(int) * n_excl,
+                              cudaMemcpyHostToDevice));
+  } else {
+    SNB_CUDA_TRY(cudaMemset(e->d_excl_start, 0, sizeof(int) * n));
+    SNB_CUDA_TRY(cudaMemset(e->d_excl_numbers, 0, sizeof(int) * n));
+  }
+  SNB_CUDA_TRY(cudaMalloc(&e->d_isum, sizeof(long long) * 9));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_bonded_e, sizeof(long long)));
+  SNB_CUDA_TRY(cudaMemset(e->d_bonded_e, 0, sizeof(long long)));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_totals_scratch, sizeof(double) * 16));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_snap_crd, sizeof(float) * 3 * n));
+  SNB_CUDA_TRY(cudaMalloc(&e->d_snap_vel, sizeof(float) * 3 * n));
+  SNB_CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+  return kOk;
+}
+
 extern "C" int snb_engine_create(const snb_options* opt, int n, snb_boundary boundary,
                                  int n_types, const int* h_type, const float* h_A,
                                  const float* h_B, const float* h_charge,
@@ -855,67 +945,108 @@ extern "C" int snb_engine_create(const snb_options* opt, int n, snb_boundary bou
   int rc = nl_init(e->nl, n, e->opt.cutoff, e->opt.skin, boundary.cell,
                    e->opt.nl_refresh_interval, e->opt.nl_skin_permit,
                    e->opt.nl_max_neighbor_numbers, 0);
+  float box[3] = {boundary.cell[0], boundary.cell[2], boundary.cell[5]};
+  if (!rc)
+    rc = pme_init(e->pme, n, boundary.cell, box, e->opt.cutoff, e->opt.pm_direct_tolerance,
+                  e->opt.pm_fftx, e->opt.pm_ffty, e->opt.pm_fftz, e->opt.pm_grid_spacing,
+                  e->opt.pme_update_interval, e->opt.pme_calculate_reciprocal_part != 0,
+                  e->opt.pme_calculate_excluded_part != 0);
+  if (!rc)
+    rc = engine_finish_create(e, n, n_types, h_type, h_A, h_B, h_charge, h_es, h_en, h_el,
+                              n_excl);
   if (rc) {
-    delete e;
+    snb_engine_destroy(e);
     return rc;
   }
-  float box[3] = {boundary.cell[0], boundary.cell[2], boundary.cell[5]};
-  rc = pme_init(e->pme, n, boundary.cell, box, e->opt.cutoff, e->opt.pm_direct_tolerance,
-                e->opt.pm_fftx, e->opt.pm_ffty, e->opt.pm_fftz, e->opt.pm_grid_spacing,
-                e->opt.pme_update_interval, e->opt.pme_calculate_reciprocal_part != 0,
-                e->opt.pme_calculate_excluded_part != 0);
-  if (rc) return rc;
-  rc = acc_init(e->acc, n);
-  if (rc) return rc;
-  LJParams& p = e->lj;
-  p.n_types = n_types;
-  p.n_pairs = n_types * (n_types + 1) / 2;
-  p.h_type.assign(h_type, h_type + n);
-  p.h_A.assign(h_A, h_A + p.n_pairs);
-  p.h_B.assign(h_B, h_B + p.n_pairs);
-  p.cutoff = e->opt.cutoff;
-  p.long_range_factor = lrc_factor(p.h_type, n_types, p.h_B, p.cutoff);
-  SNB_CUDA_TRY(cudaMalloc(&p.d_A, sizeof(float) * p.n_pairs));
-  SNB_CUDA_TRY(cudaMalloc(&p.d_B, sizeof(float) * p.n_pairs));
-  SNB_CUDA_TRY(cudaMemcpy(p.d_A, h_A, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
-  SNB_CUDA_TRY(cudaMemcpy(p.d_B, h_B, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
-  SNB_CUDA_TRY(cudaMalloc(&p.d_type, sizeof(int) * n));
-  SNB_CUDA_TRY(cudaMemcpy(p.d_type, h_type, sizeof(int) * n, cudaMemcpyHostToDevice));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_charge, sizeof(float) * n));
-  SNB_CUDA_TRY(cudaMemcpy(e->d_charge, h_charge, sizeof(float) * n, cudaMemcpyHostToDevice));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_pos, sizeof(float4) * n));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_type_sorted, sizeof(int) * n));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_start, sizeof(int) * n));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_numbers, sizeof(int) * n));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_excl_list, sizeof(int) * std::max(n_excl, 1)));
-  if (h_es && h_en) {
-    for (int i = 0; i < n; ++i) {
-      if (h_en[i] < 0 || (h_en[i] > 0 && (h_es[i] < 0 || h_es[i] + h_en[i] > n_excl))) {
-        snb_engine_destroy(e);
-        return fail(kBadInput, "engine_create: exclusion list out of range");
-      }
-      for (int k = 0; k < h_en[i]; ++k)
-        if (h_el[h_es[i] + k] < 0 || h_el[h_es[i] + k] >= n) {
-          snb_engine_destroy(e);
-          return fail(kBadInput, "engine_create: excluded atom index out of range");
-        }
-    }
-    SNB_CUDA_TRY(cudaMemcpy(e->d_excl_start, h_es, sizeof(int) * n, cudaMemcpyHostToDevice));
-    SNB_CUDA_TRY(cudaMemcpy(e->d_excl_numbers, h_en, sizeof(int) * n, cudaMemcpyHostToDevice));
-    if (n_excl > 0)
-      SNB_CUDA_TRY(cudaMemcpy(e->d_excl_list, h_el, sizeof(int) * n_excl,
-                              cudaMemcpyHostToDevice));
-  } else {
-    SNB_CUDA_TRY(cudaMemset(e->d_excl_start, 0, sizeof(int) * n));
-    SNB_CUDA_TRY(cudaMemset(e->d_excl_numbers, 0, sizeof(int) * n));
+  *out = e;
+  return kOk;
+}
+
+extern "C" int snb_batch_create(const snb_options* opt, int n_systems,
+                                const int* atoms_per_system, const float* box_lengths,
+                                int n_types, const int* h_type, const float* h_A,
+                                const float* h_B, const float* h_charge,
+                                const int* h_es, const int* h_en, const int* h_el,
+                                int n_excl, snb_engine** out) {
+  if (!out) return fail(kBadInput, "batch_create: null out");
+  *out = nullptr;
+  if (n_systems <= 0 || !atoms_per_system || !box_lengths || n_types <= 0 || !h_type ||
+      !h_A || !h_B || !h_charge)
+    return fail(kBadInput, "batch_create: bad argument");
+  snb_engine* e = new snb_engine();
+  e->opt = opts_or_default(opt);
+  if (e->opt.pm_fftx > 0 || e->opt.pm_ffty > 0 || e->opt.pm_fftz > 0 ||
+      e->opt.pme_update_interval != 1 || e->opt.nl_refresh_interval > 0 ||
+      e->opt.accumulation != kAccumFixed) {
+    delete e;
+    return fail(kNotSupported,
+                "batch_create: per-box grids from PM_grid_spacing, PME every step, "
+                "displacement-triggered lists and fixed-point accumulation only");
   }
-  SNB_CUDA_TRY(cudaMalloc(&e->d_isum, sizeof(long long) * 9));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_bonded_e, sizeof(long long)));
-  SNB_CUDA_TRY(cudaMemset(e->d_bonded_e, 0, sizeof(long long)));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_totals_scratch, sizeof(double) * 16));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_snap_crd, sizeof(float) * 3 * n));
-  SNB_CUDA_TRY(cudaMalloc(&e->d_snap_vel, sizeof(float) * 3 * n));
-  SNB_CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+  long long total = 0;
+  e->nsys = n_systems;
+  e->h_sys.resize(n_systems);
+  for (int s = 0; s < n_systems; ++s) {
+    SysGeom& g = e->h_sys[s];
+    memset(&g, 0, sizeof(g));
+    const float* L = box_lengths + 3 * s;
+    if (atoms_per_system[s] <= 0 || !(L[0] > 0.f && L[1] > 0.f && L[2] > 0.f)) {
+      delete e;
+      return fail(kBadInput, "batch_create: empty system or bad box");
+    }
+    g.atom_begin = (int)total;
+    total += atoms_per_system[s];
+    g.atom_end = (int)total;
+    g.cell.a11 = L[0];
+    g.cell.a22 = L[1];
+    g.cell.a33 = L[2];
+    g.rcell.a11 = 1.0f / L[0];
+    g.rcell.a22 = 1.0f / L[1];
+    g.rcell.a33 = 1.0f / L[2];
+    g.volume = (double)L[0] * L[1] * L[2];
+  }
+  if (total > 2147483647LL / 16) {
+    delete e;
+    return fail(kBadInput, "batch_create: too many atoms");
+  }
+  const int n = (int)total;
+  e->n = n;
+  e->accum = kAccumFixed;
+  e->cell = e->h_sys[0].cell;
+  e->rcell = e->h_sys[0].rcell;
+  int rc = nl_init_batch(e->nl, n, e->opt.cutoff, e->opt.skin, e->h_sys,
+                         e->opt.nl_refresh_interval, e->opt.nl_skin_permit,
+                         e->opt.nl_max_neighbor_numbers);
+  if (!rc)
+    rc = pme_init_batch(e->pme, n, e->h_sys, e->opt.cutoff, e->opt.pm_direct_tolerance,
+                        e->opt.pm_grid_spacing, e->opt.pme_calculate_reciprocal_part != 0,
+                        e->opt.pme_calculate_excluded_part != 0);
+  if (!rc) {
+    std::vector<int> sys_of(n);
+    for (int s = 0; s < n_systems; ++s)
+      for (int i = e->h_sys[s].atom_begin; i < e->h_sys[s].atom_end; ++i) sys_of[i] = s;
+    if (cudaMalloc(&e->d_sys, sizeof(SysGeom) * n_systems) != cudaSuccess ||
+        cudaMemcpy(e->d_sys, e->h_sys.data(), sizeof(SysGeom) * n_systems,
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc(&e->d_sys_of, sizeof(int) * n) != cudaSuccess ||
+        cudaMemcpy(e->d_sys_of, sys_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+      rc = fail(kCudaError, "batch_create: system table upload failed");
+  }
+  if (!rc) {
+    e->bv.sys = e->d_sys;
+    e->bv.sys_of = e->d_sys_of;
+    e->bv.tile_sys = e->pme.d_tile_sys;
+    e->bv.nsys = n_systems;
+    e->nl.bv = e->bv;
+    e->pme.bv = e->bv;
+    rc = engine_finish_create(e, n, n_types, h_type, h_A, h_B, h_charge, h_es, h_en, h_el,
+                              n_excl);
+  }
+  if (rc) {
+    snb_engine_destroy(e);
+    return rc;
+  }
   *out = e;
   return kOk;
 }
@@ -1012,6 +1143,7 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   a.rcell = e->rcell;
   a.cutoff2 = e->opt.cutoff * e->opt.cutoff;
   a.beta = e->pme.beta;
+  a.bv = e->bv;
   rc = launch_pair(a, e->acc, e->accum, energy, virial, true, st);
   if (rc) return rc;
   prof_mark(e, 3, st);
@@ -1019,7 +1151,7 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
     rc = launch_excluded(e->n, reinterpret_cast<const float3*>(crd), e->d_charge, e->cell,
                          e->rcell, e->pme.beta, e->d_excl_start, e->d_excl_list,
                          e->d_excl_numbers, e->nl.d_inv_perm, e->acc, e->accum, energy,
-                         virial, st);
+                         virial, st, e->bv);
     if (rc) return rc;
   }
   prof_mark(e, 4, st);
@@ -1043,10 +1175,8 @@ extern "C" int snb_engine_force(snb_engine* e, const float* crd, float* frc, int
   if (rc) return rc;
   e->steps_done++;
   if (en || vi) {
-    double vol = (double)e->cell.a11 * e->cell.a22 * e->cell.a33;
-    rc = launch_totals(e->n, e->acc, e->d_isum, nullptr, e->pme.d_sums,
-                       e->lj.long_range_factor / vol, 2.0 * e->lj.long_range_factor / vol,
-                       d_totals, en, vi, e->pme.reciprocal, st);
+    rc = launch_totals(e->n, e->acc, e->d_isum, nullptr, e->pme.d_sums, e->lrc_energy,
+                       e->lrc_virial, d_totals, en, vi, e->pme.reciprocal, st);
     if (rc) return rc;
   }
   return launch_unpack(e->n, e->nl.d_inv_perm, e->acc, e->accum,
@@ -1106,7 +1236,8 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
   if (rc) return rc;
   rc = launch_bonded(e->nb, e->d_ba, e->d_bb, e->d_bk, e->d_br0, e->na, e->d_aa, e->d_ab,
                      e->d_ac, e->d_ak, e->d_at0, reinterpret_cast<const float3*>(crd),
-                     e->cell, e->rcell, e->nl.d_inv_perm, e->acc, nullptr, false, st);
+                     e->cell, e->rcell, e->nl.d_inv_perm, e->acc, nullptr, false, st,
+                     e->bv);
   if (rc) return rc;
   prof_mark(e, 6, st);
   // the next step's refresh check rides on the coordinate update
@@ -1115,7 +1246,7 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
   rc = launch_leap_frog(e->n, e->nl.d_inv_perm, e->acc, reinterpret_cast<float3*>(crd),
                         reinterpret_cast<float3*>(vel), invm, dt,
                         check ? e->nl.d_old_crd : nullptr, e->cell, e->rcell,
-                        permit * permit, e->nl.d_flags, st);
+                        permit * permit, e->nl.d_flags, st, e->bv);
   prof_mark(e, 7, st);
   return rc;
 }
@@ -1321,6 +1452,8 @@ extern "C" int snb_engine_destroy(snb_engine* e) {
   cudaFree(e->d_totals_scratch);
   cudaFree(e->d_snap_crd);
   cudaFree(e->d_snap_vel);
+  cudaFree(e->d_sys);
+  cudaFree(e->d_sys_of);
   for (void* p : {(void*)e->d_ba, (void*)e->d_bb, (void*)e->d_bk, (void*)e->d_br0,
                   (void*)e->d_aa, (void*)e->d_ab, (void*)e->d_ac, (void*)e->d_ak,
                   (void*)e->d_at0})

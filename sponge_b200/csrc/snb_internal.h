@@ -45,6 +45,38 @@ int scan_exclusive(const int* in, int* out, int n, int* total_out,
 int scan_reserve(ScanScratch& s, int n);
 
 // ----------------------------------------------------------------------------
+// Independent periodic boxes advanced together (a batch).  The atoms of
+// system s are [atom_begin, atom_end) in the caller's order; the counting
+// sort keeps each system's cells together and in system order, so the same
+// range holds in the sorted frame.  One SysGeom per system on the device;
+// kernels compiled with BATCH = true read their atom's (or tile's) entry,
+// the single-box kernels (BATCH = false) take the geometry as arguments.
+struct SysGeom {
+  Cell cell, rcell;             // rectangular box
+  int atom_begin, atom_end;
+  // neighbor grid: cells [cell_begin, cell_begin + Nx*Ny*Nz) of the batch
+  int Nx, Ny, Nz, cell_begin;
+  float wx, wy, iwz;            // cell widths (x, y) and 1/width (z)
+  int trim;                     // cell offsets unique (>= 5 cells per axis)
+  // PME: grid K0 x K1 x K2, 8^3 tiles [tile_begin, tile_begin + nt0*nt1*nt2)
+  int K0, K1, K2;
+  int nt0, nt1, nt2, tile_begin;
+  int grid_begin;               // first point of the real grid (Q, phi)
+  int spec_begin;               // first point of the half spectrum (FQ)
+  int src_begin0, src_begin1, src_begin2;  // per-axis source-bin tables
+  int b_begin0, b_begin1, b_begin2;        // per-axis |b|^2 tables
+  float mpre, inv_pi_v;         // pi^2 / beta^2, 1 / (pi V)
+  double volume;
+};
+
+struct BatchView {
+  const SysGeom* sys = nullptr;  // [nsys]
+  const int* sys_of = nullptr;   // [n] system of each atom
+  const int* tile_sys = nullptr;  // [ntiles] system of each PME tile
+  int nsys = 0;
+};
+
+// ----------------------------------------------------------------------------
 // Neighbor list: cell grid of side >= (cutoff+skin)/2 (neighbor_list.cpp:943),
 // atoms counting-sorted by cell (stable: ties by caller index), half list in
 // the sorted frame stored as CSR rows.
@@ -72,6 +104,7 @@ struct NeighborList {
   // caller's indices): count [n] and up to 16 partners [n][16]
   int* d_excl_count = nullptr;
   int* d_excl_partner = nullptr;
+  BatchView bv;                // nsys > 0: a batch of boxes (per-system grids)
   // binning
   int* d_cell_count = nullptr;  // [ncell]
   int* d_cell_start = nullptr;  // [ncell + 1]
@@ -101,6 +134,12 @@ struct NeighborList {
 int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell6,
             int refresh_interval, float skin_permit, int max_neighbor_numbers,
             long long initial_capacity);
+// A batch of rectangular boxes (sys[s].cell, rcell and atom ranges set);
+// fills the neighbor-grid fields of sys.  The caller sets nl.bv once the
+// SysGeom table is on the device.
+int nl_init_batch(NeighborList& nl, int n, float cutoff, float skin,
+                  std::vector<SysGeom>& sys, int refresh_interval, float skin_permit,
+                  int max_neighbor_numbers);
 void nl_free(NeighborList& nl);
 // Update as NEIGHBOR_LIST::Update (neighbor_list.cpp:974-1025): forced, or
 // conditional on the displacement check / refresh interval.  Device-side
@@ -174,6 +213,7 @@ struct PairArgs {
   Cell cell, rcell;
   float cutoff2;
   float beta;
+  BatchView bv;                 // nsys > 0: per-system boxes (rectangular)
 };
 int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool ortho, cudaStream_t st);
@@ -238,11 +278,30 @@ struct PME {
   int* d_upk = nullptr;         // [n] packed base point in input order
   cufftHandle plan_r2c = 0, plan_c2r = 0;
   ScanScratch scan;
+  // batch of boxes (bv.nsys > 0): grids of equal size are stored next to
+  // each other and transformed by one batched plan per size
+  BatchView bv;
+  struct FftGroup {
+    int K[3];
+    int count;
+    int grid_begin, spec_begin;
+    cufftHandle r2c = 0, c2r = 0;
+  };
+  std::vector<FftGroup> groups;
+  int4* d_spec_blocks = nullptr;   // [spec_blocks] {system, first, end}
+  int spec_blocks = 0;
+  int* d_sys_block_begin = nullptr;  // [nsys + 1]
+  double* d_sys_sums = nullptr;    // [nsys][8]
+  int* d_tile_sys = nullptr;       // [ntiles]
 };
 int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
              float cutoff, float tolerance, int fftx, int ffty, int fftz,
              float grid_spacing, int update_interval, bool reciprocal,
              bool excluded);
+// A batch of rectangular boxes (sys[s].cell, rcell, atom ranges set): one
+// grid per box by the reference's size rule; fills the PME fields of sys.
+int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
+                   float tolerance, float grid_spacing, bool reciprocal, bool excluded);
 void pme_free(PME& p);
 float get_beta(float cutoff, float tolerance);
 int fft_size(float length);
@@ -263,7 +322,8 @@ int launch_excluded(int n, const float3* crd, const float* charge,
                     const Cell& cell, const Cell& rcell, float beta,
                     const int* excl_start, const int* excl_list,
                     const int* excl_numbers, const int* map, Accumulators& acc,
-                    int accum, bool energy, bool virial, cudaStream_t st);
+                    int accum, bool energy, bool virial, cudaStream_t st,
+                    const BatchView& bv = BatchView());
 
 // ----------------------------------------------------------------------------
 // Frame conversion kernels.

@@ -20,58 +20,8 @@ __device__ __forceinline__ void acc_force(Accumulators& acc, int s, float fx, fl
   red_add(acc.d_f + 2 * N + s, to_fixed_force(fz));
 }
 
-__global__ void k_bonds(int nb, const int* __restrict__ a, const int* __restrict__ b,
-                        const float* __restrict__ k, const float* __restrict__ r0,
-                        const float3* __restrict__ crd, Cell cell, Cell rcell,
-                        const int* __restrict__ map, Accumulators acc,
-                        long long* __restrict__ e_total, bool energy) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nb) return;
-  int i = a[t], j = b[t];
-  float3 d = min_image_fast<false>(crd[i], crd[j], cell, rcell);
-  float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-  float dr = r - r0[t];
-  float s = -2.0f * dr * k[t] / r;
-  int si = map ? map[i] : i, sj = map ? map[j] : j;
-  acc_force(acc, si, s * d.x, s * d.y, s * d.z);
-  acc_force(acc, sj, -s * d.x, -s * d.y, -s * d.z);
-  if (energy) red_add(e_total, to_fixed_energy(k[t] * dr * dr));
-}
-
-__global__ void k_angles(int na, const int* __restrict__ ia, const int* __restrict__ ib,
-                         const int* __restrict__ ic, const float* __restrict__ k,
-                         const float* __restrict__ t0, const float3* __restrict__ crd,
-                         Cell cell, Cell rcell, const int* __restrict__ map,
-                         Accumulators acc, long long* __restrict__ e_total,
-                         bool energy) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= na) return;
-  int i = ia[t], j = ib[t], l = ic[t];
-  float3 dij = min_image_fast<false>(crd[i], crd[j], cell, rcell);
-  float3 dkj = min_image_fast<false>(crd[l], crd[j], cell, rcell);
-  float rij2 = 1.0f / (dij.x * dij.x + dij.y * dij.y + dij.z * dij.z);
-  float rkj2 = 1.0f / (dkj.x * dkj.x + dkj.y * dkj.y + dkj.z * dkj.z);
-  float rr = sqrtf(rij2 * rkj2);
-  float c = (dij.x * dkj.x + dij.y * dkj.y + dij.z * dkj.z) * rr;
-  c = fmaxf(-0.999999f, fminf(c, 0.999999f));
-  float th = acosf(c);
-  float dth = th - t0[t];
-  float kk = -2.0f * k[t] * dth / sinf(th);
-  float cross = kk * rr, self = kk * c;
-  float3 fi = make_float3(self * rij2 * dij.x - cross * dkj.x,
-                          self * rij2 * dij.y - cross * dkj.y,
-                          self * rij2 * dij.z - cross * dkj.z);
-  float3 fk = make_float3(self * rkj2 * dkj.x - cross * dij.x,
-                          self * rkj2 * dkj.y - cross * dij.y,
-                          self * rkj2 * dkj.z - cross * dij.z);
-  int si = map ? map[i] : i, sj = map ? map[j] : j, sk = map ? map[l] : l;
-  acc_force(acc, si, fi.x, fi.y, fi.z);
-  acc_force(acc, sk, fk.x, fk.y, fk.z);
-  acc_force(acc, sj, -fi.x - fk.x, -fi.y - fk.y, -fi.z - fk.z);
-  if (energy) red_add(e_total, to_fixed_energy(k[t] * dth * dth));
-}
-
 // Bonds and angles in one launch: the first ceil(nb/256) blocks take bonds.
+template <bool BATCH>
 __global__ void k_bonded(int nb, const int* __restrict__ ba, const int* __restrict__ bb,
                          const float* __restrict__ bk, const float* __restrict__ br0,
                          int na, const int* __restrict__ aa, const int* __restrict__ ab,
@@ -79,11 +29,16 @@ __global__ void k_bonded(int nb, const int* __restrict__ ba, const int* __restri
                          const float* __restrict__ at0, const float3* __restrict__ crd,
                          Cell cell, Cell rcell, const int* __restrict__ map,
                          Accumulators acc, long long* __restrict__ e_total, bool energy,
-                         int bond_blocks) {
+                         int bond_blocks, BatchView bv) {
   if ((int)blockIdx.x < bond_blocks) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nb) return;
     int i = ba[t], j = bb[t];
+    if (BATCH) {  // bonded terms never cross systems
+      const SysGeom& sg = bv.sys[bv.sys_of[i]];
+      cell = sg.cell;
+      rcell = sg.rcell;
+    }
     float3 d = min_image_fast<false>(crd[i], crd[j], cell, rcell);
     float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
     float dr = r - br0[t];
@@ -97,6 +52,11 @@ __global__ void k_bonded(int nb, const int* __restrict__ ba, const int* __restri
   int t = (blockIdx.x - bond_blocks) * blockDim.x + threadIdx.x;
   if (t >= na) return;
   int i = aa[t], j = ab[t], l = ac[t];
+  if (BATCH) {
+    const SysGeom& sg = bv.sys[bv.sys_of[j]];
+    cell = sg.cell;
+    rcell = sg.rcell;
+  }
   float3 dij = min_image_fast<false>(crd[i], crd[j], cell, rcell);
   float3 dkj = min_image_fast<false>(crd[l], crd[j], cell, rcell);
   float rij2 = 1.0f / (dij.x * dij.x + dij.y * dij.y + dij.z * dij.z);
@@ -126,13 +86,18 @@ int launch_bonded(int nb, const int* ba, const int* bb, const float* bk,
                   const int* ac, const float* ak, const float* at0,
                   const float3* crd, const Cell& cell, const Cell& rcell,
                   const int* map, Accumulators& acc, long long* e_total,
-                  bool energy, cudaStream_t st) {
+                  bool energy, cudaStream_t st, const BatchView& bv) {
   const int bblocks = nb > 0 ? ceil_div(nb, 256) : 0;
   const int ablocks = na > 0 ? ceil_div(na, 256) : 0;
   if (bblocks + ablocks == 0) return kOk;
-  k_bonded<<<bblocks + ablocks, 256, 0, st>>>(nb, ba, bb, bk, br0, na, aa, ab, ac, ak,
-                                             at0, crd, cell, rcell, map, acc, e_total,
-                                             energy, bblocks);
+  if (bv.nsys > 0)
+    k_bonded<true><<<bblocks + ablocks, 256, 0, st>>>(nb, ba, bb, bk, br0, na, aa, ab, ac,
+                                                     ak, at0, crd, cell, rcell, map, acc,
+                                                     e_total, energy, bblocks, bv);
+  else
+    k_bonded<false><<<bblocks + ablocks, 256, 0, st>>>(nb, ba, bb, bk, br0, na, aa, ab, ac,
+                                                      ak, at0, crd, cell, rcell, map, acc,
+                                                      e_total, energy, bblocks, bv);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -142,11 +107,12 @@ int launch_bonded(int nb, const int* ba, const int* bb, const float* bk,
 // When old_crd is given, also performs the refresh check of the next step
 // (Check_Refresh, neighbor_list.cpp:307-321) on the new coordinates and
 // raises flags[0] if any atom moved more than sqrt(permit2) since the build.
+template <bool BATCH>
 __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc,
                             float3* __restrict__ crd, float3* __restrict__ vel,
                             const float* __restrict__ inv_mass, float dt,
                             const float3* __restrict__ old_crd, Cell cell, Cell rcell,
-                            float permit2, int* flags) {
+                            float permit2, int* flags, BatchView bv) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int s = map[i];
@@ -169,6 +135,11 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
   r.z += dt * v.z;
   crd[i] = r;
   if (old_crd) {
+    if (BATCH) {
+      const SysGeom& sg = bv.sys[bv.sys_of[i]];
+      cell = sg.cell;
+      rcell = sg.rcell;
+    }
     float3 d = min_image_fast<false>(r, old_crd[i], cell, rcell);
     bool moved = d.x * d.x + d.y * d.y + d.z * d.z > permit2;
     if (__any_sync(__activemask(), moved) && moved) atomicExch(&flags[0], 1);
@@ -178,9 +149,15 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
 int launch_leap_frog(int n, const int* map, Accumulators& acc, float3* crd,
                      float3* vel, const float* inv_mass, float dt,
                      const float3* old_crd, const Cell& cell, const Cell& rcell,
-                     float permit2, int* flags, cudaStream_t st) {
-  k_leap_frog<<<ceil_div(n, 256), 256, 0, st>>>(n, map, acc, crd, vel, inv_mass, dt,
-                                                old_crd, cell, rcell, permit2, flags);
+                     float permit2, int* flags, cudaStream_t st, const BatchView& bv) {
+  if (bv.nsys > 0)
+    k_leap_frog<true><<<ceil_div(n, 256), 256, 0, st>>>(n, map, acc, crd, vel, inv_mass, dt,
+                                                      old_crd, cell, rcell, permit2, flags,
+                                                      bv);
+  else
+    k_leap_frog<false><<<ceil_div(n, 256), 256, 0, st>>>(n, map, acc, crd, vel, inv_mass,
+                                                       dt, old_crd, cell, rcell, permit2,
+                                                       flags, bv);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }

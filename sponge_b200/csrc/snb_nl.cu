@@ -33,12 +33,18 @@ enum { kFlagNeed = 0, kFlagListOverflow = 1, kFlagTotal = 2, kFlagGeneration = 3
 // ---------------------------------------------------------------------------
 // Refresh decision (Check_Refresh, neighbor_list.cpp:307-321): any atom moved
 // more than skin*skin_permit since the last build.
+template <bool BATCH>
 __global__ void k_check_refresh(int n, const float3* __restrict__ crd,
                                 const float3* __restrict__ old_crd, Cell cell,
-                                Cell rcell, float permit2, int* flags) {
+                                Cell rcell, float permit2, int* flags, BatchView bv) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool moved = false;
   if (i < n) {
+    if (BATCH) {
+      const SysGeom& g = bv.sys[bv.sys_of[i]];
+      cell = g.cell;
+      rcell = g.rcell;
+    }
     float3 d = min_image_fast<false>(crd[i], old_crd[i], cell, rcell);
     moved = d.x * d.x + d.y * d.y + d.z * d.z > permit2;
   }
@@ -65,14 +71,22 @@ __device__ __forceinline__ int wrapped_cell(float3 r, const Cell& cell, int Nx,
   return (nx * Ny + ny) * Nz + nz;
 }
 
+template <bool BATCH>
 __global__ void k_bin_count(int n, const float3* __restrict__ crd, Cell cell,
                             int Nx, int Ny, int Nz, int* __restrict__ atom_cell,
                             int* __restrict__ atom_slot, int* __restrict__ cell_count,
-                            int* __restrict__ excl_count, const int* flags) {
+                            int* __restrict__ excl_count, const int* flags,
+                            BatchView bv) {
   if (flags[kFlagNeed] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  int c = wrapped_cell(crd[i], cell, Nx, Ny, Nz);
+  int c;
+  if (BATCH) {
+    const SysGeom& g = bv.sys[bv.sys_of[i]];
+    c = g.cell_begin + wrapped_cell(crd[i], g.cell, g.Nx, g.Ny, g.Nz);
+  } else {
+    c = wrapped_cell(crd[i], cell, Nx, Ny, Nz);
+  }
   atom_cell[i] = c;
   atom_slot[i] = atomicAdd(&cell_count[c], 1);
   if (excl_count) excl_count[i] = 0;
@@ -186,6 +200,7 @@ struct SearchArgs {
   int row_cap;
   int* cols;
   int* flags;
+  BatchView bv;             // per-system grids when BATCH
 };
 
 // Distance, in cell widths, from a point at fractional offset f inside its
@@ -203,6 +218,7 @@ __device__ __forceinline__ float cell_gap(int o, float f) {
 // Each run is cut down to the cells whose box is within rl (plus a margin)
 // of atom i.  With at least 5 cells per axis a pair within rl sits at the
 // run's cell offset in its minimum image, so a cut cell holds no hit.
+template <bool BATCH>
 __global__ void __launch_bounds__(256)
 k_pair_search(SearchArgs a) {
   if (a.flags[kFlagNeed] == 0) return;
@@ -215,6 +231,24 @@ k_pair_search(SearchArgs a) {
   const float4 pi4 = a.pos[i];
   const int gi = __float_as_int(pi4.w);
   const int c = a.sorted_cell[i];
+  // grid of atom i's box
+  int Nx = a.Nx, Ny = a.Ny, Nz = a.Nz, c_local = c;
+  Cell cell = a.cell, rcell = a.rcell;
+  bool trim = a.trim;
+  float wx = a.wx, wy = a.wy, iwz = a.iwz;
+  if (BATCH) {
+    const SysGeom& g = a.bv.sys[a.bv.sys_of[i]];
+    Nx = g.Nx;
+    Ny = g.Ny;
+    Nz = g.Nz;
+    c_local = c - g.cell_begin;
+    cell = g.cell;
+    rcell = g.rcell;
+    trim = g.trim != 0;
+    wx = g.wx;
+    wy = g.wy;
+    iwz = g.iwz;
+  }
   int* out_row = a.cols + (size_t)i * a.row_cap;
   int count = 0;
   const int nr = a.run_count[c];
@@ -232,14 +266,14 @@ k_pair_search(SearchArgs a) {
   }
   // position of i inside its cell, in cell widths (the binning's arithmetic)
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  if (a.trim) {
-    const int cz = c % a.Nz, cy = (c / a.Nz) % a.Ny, cx = c / (a.Nz * a.Ny);
-    const float x = pi4.x - floorf(pi4.x / a.cell.a11) * a.cell.a11;
-    const float y = pi4.y - floorf(pi4.y / a.cell.a22) * a.cell.a22;
-    const float z = pi4.z - floorf(pi4.z / a.cell.a33) * a.cell.a33;
-    fx = x / a.cell.a11 * a.Nx - (float)cx;
-    fy = y / a.cell.a22 * a.Ny - (float)cy;
-    fz = z / a.cell.a33 * a.Nz - (float)cz;
+  if (trim) {
+    const int cz = c_local % Nz, cy = (c_local / Nz) % Ny, cx = c_local / (Nz * Ny);
+    const float x = pi4.x - floorf(pi4.x / cell.a11) * cell.a11;
+    const float y = pi4.y - floorf(pi4.y / cell.a22) * cell.a22;
+    const float z = pi4.z - floorf(pi4.z / cell.a33) * cell.a33;
+    fx = x / cell.a11 * Nx - (float)cx;
+    fy = y / cell.a22 * Ny - (float)cy;
+    fz = z / cell.a33 * Nz - (float)cz;
   }
   // range list: own cell after i, then the owned runs
   for (int r = -1; r < nr; ++r) {
@@ -249,12 +283,12 @@ k_pair_search(SearchArgs a) {
       hi = a.cell_start[c + 1];
     } else {
       int2 rr = a.runs[(size_t)c * a.max_runs + r];
-      if (a.trim) {
+      if (trim) {
         const char4 g = a.geom[(size_t)c * a.max_runs + r];
-        const float gx = cell_gap(g.x, fx) * a.wx, gy = cell_gap(g.y, fy) * a.wy;
+        const float gx = cell_gap(g.x, fx) * wx, gy = cell_gap(g.y, fy) * wy;
         const float s2 = a.reach2 - gx * gx - gy * gy;
         if (s2 < 0.f) continue;
-        const float s = sqrtf(s2) * a.iwz;
+        const float s = sqrtf(s2) * iwz;
         const int zmax = (int)floorf(fz + s), zmin = (int)ceilf(fz - 1.f - s);
         const int z0 = max((int)g.z, zmin), z1 = min((int)g.w, zmax);
         if (z0 > z1) continue;
@@ -280,7 +314,7 @@ k_pair_search(SearchArgs a) {
           dy = -dy;
           dz = -dz;
         }
-        const float3 d = min_image_exact_rect(dx, dy, dz, a.cell, a.rcell);
+        const float3 d = min_image_exact_rect(dx, dy, dz, cell, rcell);
         hit = norm2_exact(d) < a.rl2;
       }
       for (int k = 0; k < n_ex; ++k)  // warp-uniform
@@ -350,13 +384,11 @@ int nl_force_next(NeighborList& nl, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
-                       std::vector<char4>& geom, std::vector<int>& counts,
-                       int& max_runs) {
-  int ncell = Nx * Ny * Nz;
-  std::vector<std::vector<int2>> per(ncell);
-  std::vector<std::vector<char4>> per_geom(ncell);
-  max_runs = 0;
+// Owned neighbour runs of every cell of one Nx x Ny x Nz box whose cells are
+// numbered from `offset` in the list's cell space; appended to per/per_geom.
+static void box_runs(int Nx, int Ny, int Nz, int offset,
+                     std::vector<std::vector<int2>>& per,
+                     std::vector<std::vector<char4>>& per_geom) {
   for (int cx = 0; cx < Nx; ++cx)
     for (int cy = 0; cy < Ny; ++cy)
       for (int cz = 0; cz < Nz; ++cz) {
@@ -389,20 +421,28 @@ static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
         std::vector<char4> gg;
         for (const auto& kv : nb) {
           const int o = kv.first;
-          if (!rr.empty() && rr.back().y == o - 1 && (o - 1) / Nz == o / Nz &&
+          if (!rr.empty() && rr.back().y == offset + o - 1 && (o - 1) / Nz == o / Nz &&
               gg.back().w + 1 == kv.second.z) {
-            rr.back().y = o;
+            rr.back().y = offset + o;
             gg.back().w = kv.second.z;
           } else {
-            rr.push_back(make_int2(o, o));
+            rr.push_back(make_int2(offset + o, offset + o));
             gg.push_back(kv.second);
           }
         }
-        max_runs = std::max(max_runs, (int)rr.size());
-        per[c] = rr;
-        per_geom[c] = gg;
+        per[offset + c] = rr;
+        per_geom[offset + c] = gg;
       }
-  if (max_runs == 0) max_runs = 1;
+}
+
+// Per-cell run lists as fixed-width tables [ncell][max_runs].
+static void pack_runs(const std::vector<std::vector<int2>>& per,
+                      const std::vector<std::vector<char4>>& per_geom,
+                      std::vector<int2>& runs, std::vector<char4>& geom,
+                      std::vector<int>& counts, int& max_runs) {
+  const int ncell = (int)per.size();
+  max_runs = 1;
+  for (const auto& r : per) max_runs = std::max(max_runs, (int)r.size());
   runs.assign((size_t)ncell * max_runs, make_int2(0, -1));
   geom.assign((size_t)ncell * max_runs, make_char4(0, 0, 0, -1));
   counts.assign(ncell, 0);
@@ -415,10 +455,32 @@ static void build_runs(int Nx, int Ny, int Nz, std::vector<int2>& runs,
   }
 }
 
-int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell6,
-            int refresh_interval, float skin_permit, int max_neighbor_numbers,
-            long long initial_capacity) {
-  if (n <= 0) return fail(kBadInput, "neighbor list: atom_numbers must be > 0");
+// The reference's grid for one rectangular box (NEIGHBOR_LIST::Initial,
+// neighbor_list.cpp:943-960): N = floor(L / ((cutoff + skin) / 2)) per axis.
+static int box_grid(float grid_length, const Cell& cell, int* N) {
+  N[0] = (int)floorf(cell.a11 / grid_length);
+  N[1] = (int)floorf(cell.a22 / grid_length);
+  N[2] = (int)floorf(cell.a33 / grid_length);
+  if (N[0] <= 2 || N[1] <= 2 || N[2] <= 2)
+    return fail(kBadInput, "NEIGHBOR_LIST::Initial: the box is too small.");
+  return kOk;
+}
+
+static Cell rect_rcell(const Cell& c) {
+  Cell r{};
+  r.a11 = 1.0f / c.a11;
+  r.a22 = 1.0f / c.a22;
+  r.a33 = 1.0f / c.a33;
+  return r;
+}
+
+static int nl_alloc(NeighborList& nl, int n, long long initial_capacity,
+                    const std::vector<int2>& runs, const std::vector<char4>& geom,
+                    const std::vector<int>& counts, double max_per_atom,
+                    bool all_balanced);
+
+static void nl_common(NeighborList& nl, int n, float cutoff, float skin,
+                      int refresh_interval, float skin_permit, int max_neighbor_numbers) {
   nl.n = n;
   nl.cutoff = cutoff;
   nl.skin = skin;
@@ -427,43 +489,105 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
   nl.refresh_interval = refresh_interval;
   nl.skin_permit = skin_permit;
   nl.max_neighbor_numbers = max_neighbor_numbers;
+  // margin of 0.01 A over rl for trimming runs: far above the float error
+  // of the cell geometry (positions are wrapped with one rounding each)
+  const double reach = sqrt((double)nl.rl2) + 0.01;
+  nl.reach2 = (float)(reach * reach);
+}
+
+// Mean number of half-list entries per atom at density rho.
+static double half_sphere(double rho, float rl2) {
+  const double rl = sqrt((double)rl2);
+  return 0.5 * rho * 4.18879020478639 * rl * rl * rl;
+}
+
+int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell6,
+            int refresh_interval, float skin_permit, int max_neighbor_numbers,
+            long long initial_capacity) {
+  if (n <= 0) return fail(kBadInput, "neighbor list: atom_numbers must be > 0");
+  nl_common(nl, n, cutoff, skin, refresh_interval, skin_permit, max_neighbor_numbers);
   nl.cell = make_cell(cell6);
   if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f)
     return fail(kNotSupported,
                 "neighbor list: only rectangular boxes are supported "
                 "(triclinic cells are not built on this path)");
-  Cell rc{};
-  rc.a11 = 1.0f / nl.cell.a11;
-  rc.a22 = 1.0f / nl.cell.a22;
-  rc.a33 = 1.0f / nl.cell.a33;
-  nl.rcell = rc;
+  nl.rcell = rect_rcell(nl.cell);
   nl.ortho = true;
-  nl.Nx = (int)floorf(nl.cell.a11 / nl.grid_length);
-  nl.Ny = (int)floorf(nl.cell.a22 / nl.grid_length);
-  nl.Nz = (int)floorf(nl.cell.a33 / nl.grid_length);
-  if (nl.Nx <= 2 || nl.Ny <= 2 || nl.Nz <= 2)
-    return fail(kBadInput, "NEIGHBOR_LIST::Initial: the box is too small.");
+  int N[3];
+  int rc = box_grid(nl.grid_length, nl.cell, N);
+  if (rc) return rc;
+  nl.Nx = N[0];
+  nl.Ny = N[1];
+  nl.Nz = N[2];
   nl.ncell = nl.Nx * nl.Ny * nl.Nz;
+  nl.trim = nl.Nx >= 5 && nl.Ny >= 5 && nl.Nz >= 5;
+  nl.wx = nl.cell.a11 / nl.Nx;
+  nl.wy = nl.cell.a22 / nl.Ny;
+  nl.iwz = nl.Nz / nl.cell.a33;
+  std::vector<std::vector<int2>> per(nl.ncell);
+  std::vector<std::vector<char4>> per_geom(nl.ncell);
+  box_runs(nl.Nx, nl.Ny, nl.Nz, 0, per, per_geom);
   std::vector<int2> runs;
   std::vector<char4> geom;
   std::vector<int> counts;
-  build_runs(nl.Nx, nl.Ny, nl.Nz, runs, geom, counts, nl.max_runs);
+  pack_runs(per, per_geom, runs, geom, counts, nl.max_runs);
+  const double vol = (double)nl.cell.a11 * nl.cell.a22 * nl.cell.a33;
+  return nl_alloc(nl, n, initial_capacity, runs, geom, counts,
+                  half_sphere(n / vol, nl.rl2), nl.trim);
+}
+
+// A batch of independent rectangular boxes: each gets the reference's grid,
+// its cells numbered after the previous box's; fills the neighbor-grid
+// fields of sys.
+int nl_init_batch(NeighborList& nl, int n, float cutoff, float skin,
+                  std::vector<SysGeom>& sys, int refresh_interval, float skin_permit,
+                  int max_neighbor_numbers) {
+  if (n <= 0 || sys.empty()) return fail(kBadInput, "neighbor list: empty batch");
+  nl_common(nl, n, cutoff, skin, refresh_interval, skin_permit, max_neighbor_numbers);
+  int total = 0;
+  double max_per = 0.0;
+  bool all_balanced = true;
+  for (auto& g : sys) {
+    int N[3];
+    int rc = box_grid(nl.grid_length, g.cell, N);
+    if (rc) return rc;
+    g.Nx = N[0];
+    g.Ny = N[1];
+    g.Nz = N[2];
+    g.cell_begin = total;
+    total += N[0] * N[1] * N[2];
+    g.trim = N[0] >= 5 && N[1] >= 5 && N[2] >= 5;
+    all_balanced = all_balanced && g.trim;
+    g.wx = g.cell.a11 / N[0];
+    g.wy = g.cell.a22 / N[1];
+    g.iwz = N[2] / g.cell.a33;
+    const double vol = (double)g.cell.a11 * g.cell.a22 * g.cell.a33;
+    max_per = std::max(max_per, half_sphere((g.atom_end - g.atom_begin) / vol, nl.rl2));
+  }
+  nl.ncell = total;
+  nl.cell = sys[0].cell;
+  nl.rcell = sys[0].rcell;
+  nl.ortho = true;
+  std::vector<std::vector<int2>> per(total);
+  std::vector<std::vector<char4>> per_geom(total);
+  for (const auto& g : sys) box_runs(g.Nx, g.Ny, g.Nz, g.cell_begin, per, per_geom);
+  std::vector<int2> runs;
+  std::vector<char4> geom;
+  std::vector<int> counts;
+  pack_runs(per, per_geom, runs, geom, counts, nl.max_runs);
+  return nl_alloc(nl, n, 0, runs, geom, counts, max_per, all_balanced);
+}
+
+static int nl_alloc(NeighborList& nl, int n, long long initial_capacity,
+                    const std::vector<int2>& runs, const std::vector<char4>& geom,
+                    const std::vector<int>& counts, double max_per_atom,
+                    bool all_balanced) {
   SNB_CUDA_TRY(cudaMalloc(&nl.d_run_ranges, sizeof(int2) * runs.size()));
   SNB_CUDA_TRY(cudaMemcpy(nl.d_run_ranges, runs.data(), sizeof(int2) * runs.size(),
                           cudaMemcpyHostToDevice));
   SNB_CUDA_TRY(cudaMalloc(&nl.d_run_geom, sizeof(char4) * geom.size()));
   SNB_CUDA_TRY(cudaMemcpy(nl.d_run_geom, geom.data(), sizeof(char4) * geom.size(),
                           cudaMemcpyHostToDevice));
-  nl.trim = nl.Nx >= 5 && nl.Ny >= 5 && nl.Nz >= 5;
-  {
-    // margin of 0.01 A over rl: far above the float error of the cell
-    // geometry (positions are wrapped with one rounding each)
-    const double reach = sqrt((double)nl.rl2) + 0.01;
-    nl.reach2 = (float)(reach * reach);
-    nl.wx = nl.cell.a11 / nl.Nx;
-    nl.wy = nl.cell.a22 / nl.Ny;
-    nl.iwz = nl.Nz / nl.cell.a33;
-  }
   SNB_CUDA_TRY(cudaMalloc(&nl.d_excl_count, sizeof(int) * n));
   SNB_CUDA_TRY(cudaMalloc(&nl.d_excl_partner, sizeof(int) * kExclCap * (size_t)n));
   SNB_CUDA_TRY(cudaMalloc(&nl.d_run_count, sizeof(int) * nl.ncell));
@@ -499,16 +623,11 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
     SNB_CUDA_TRY(cudaMemset(nl.d_sorted_cell, 0, sizeof(int) * n));
     SNB_CUDA_TRY(cudaMemset(nl.d_pos, 0, sizeof(float4) * n));
   }
-  // Row capacity: 1.5x the mean half-sphere count at the box's density plus
-  // a margin; regrown on overflow by nl_check_overflow.
-  if (initial_capacity <= 0) {
-    double vol = (double)nl.cell.a11 * nl.cell.a22 * nl.cell.a33;
-    double rho = n / vol;
-    double rl = sqrt((double)nl.rl2);
-    double per = 0.5 * rho * 4.18879020478639 * rl * rl * rl;
-    const bool balanced = nl.Nx >= 5 && nl.Ny >= 5 && nl.Nz >= 5;
-    initial_capacity = (long long)((balanced ? 1.5 : 2.5) * per) + 64;
-  }
+  // Row capacity: 1.5x (2.5x where cell pairs are owned by index, which
+  // balances rows less well) the mean half-sphere count plus a margin;
+  // regrown on overflow by nl_check_overflow.
+  if (initial_capacity <= 0)
+    initial_capacity = (long long)((all_balanced ? 1.5 : 2.5) * max_per_atom) + 64;
   nl.row_cap = (int)std::min<long long>(initial_capacity, n);
   if (nl.row_cap < 32) nl.row_cap = 32;
   nl.row_cap = (nl.row_cap + 7) & ~7;  // rows start on 32-byte boundaries
@@ -575,9 +694,12 @@ int nl_decide(NeighborList& nl, const float* crd_f, int step, int forced,
   } else if (nl.refresh_interval <= 0) {
     k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 0);
     float permit = nl.skin * nl.skin_permit;
-    k_check_refresh<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, nl.d_old_crd,
-                                                      nl.cell, nl.rcell,
-                                                      permit * permit, nl.d_flags);
+    if (nl.bv.nsys > 0)
+      k_check_refresh<true><<<ceil_div(n, 256), 256, 0, st>>>(
+          n, crd, nl.d_old_crd, nl.cell, nl.rcell, permit * permit, nl.d_flags, nl.bv);
+    else
+      k_check_refresh<false><<<ceil_div(n, 256), 256, 0, st>>>(
+          n, crd, nl.d_old_crd, nl.cell, nl.rcell, permit * permit, nl.d_flags, nl.bv);
   } else {
     k_set_need<<<1, 1, 0, st>>>(nl.d_flags, (step + 1) % nl.refresh_interval == 0);
   }
@@ -596,9 +718,14 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   int* excl_count = (excl_numbers && !atom_local) ? nl.d_excl_count : nullptr;
   SNB_CUDA_TRY(cudaMemsetAsync(nl.d_cell_count, 0, sizeof(int) * nl.ncell, st));
   k_rebuild_begin<<<1, 1, 0, st>>>(nl.d_flags);
-  k_bin_count<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz,
-                                                nl.d_atom_cell, nl.d_atom_slot,
-                                                nl.d_cell_count, excl_count, nl.d_flags);
+  if (nl.bv.nsys > 0)
+    k_bin_count<true><<<ceil_div(n, 256), 256, 0, st>>>(
+        n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz, nl.d_atom_cell, nl.d_atom_slot,
+        nl.d_cell_count, excl_count, nl.d_flags, nl.bv);
+  else
+    k_bin_count<false><<<ceil_div(n, 256), 256, 0, st>>>(
+        n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz, nl.d_atom_cell, nl.d_atom_slot,
+        nl.d_cell_count, excl_count, nl.d_flags, nl.bv);
   int rc = scan_exclusive(nl.d_cell_count, nl.d_cell_start, nl.ncell, nullptr,
                           nl.scan, st);
   if (rc) return rc;
@@ -644,7 +771,12 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   sa.row_cap = nl.row_cap;
   sa.cols = nl.d_cols;
   sa.flags = nl.d_flags;
-  k_pair_search<<<std::min(ceil_div(n, 8), sms * 8), 256, 0, st>>>(sa);
+  sa.bv = nl.bv;
+  const int blocks = std::min(ceil_div(n, 8), sms * 8);
+  if (nl.bv.nsys > 0)
+    k_pair_search<true><<<blocks, 256, 0, st>>>(sa);
+  else
+    k_pair_search<false><<<blocks, 256, 0, st>>>(sa);
   k_finish_build<<<1, 1, 0, st>>>(nl.d_flags);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;

@@ -135,7 +135,7 @@ __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
   }
 }
 
-template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO>
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO, bool BATCH>
 __global__ void __launch_bounds__(256, 4)
 k_lj_direct(PairArgs a, Accumulators acc) {
   extern __shared__ float sh_tab[];
@@ -163,6 +163,10 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   const float3 ri = make_float3(pi.x, pi.y, pi.z);
   const int ti = a.type[i];
   const int gi = ENERGY || VIRIAL ? a.global[i] : 0;
+  // box of atom i (and of all its pairs)
+  const SysGeom* gs = BATCH ? a.bv.sys + a.bv.sys_of[i] : nullptr;
+  const Cell& cell = BATCH ? gs->cell : a.cell;
+  const Cell& rcell = BATCH ? gs->rcell : a.rcell;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   float e_lj = 0.f, e_c = 0.f;
   float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -196,7 +200,7 @@ k_lj_direct(PairArgs a, Accumulators acc) {
         bool in = false;
         if (jj[u] >= 0) {
           const float3 dr = min_image_fast<ORTHO>(make_float3(pp[u].x, pp[u].y, pp[u].z),
-                                                  ri, a.cell, a.rcell);
+                                                  ri, cell, rcell);
           in = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z < a.cutoff2;
         }
         const unsigned m = __ballot_sync(0xffffffffu, in);
@@ -210,8 +214,8 @@ k_lj_direct(PairArgs a, Accumulators acc) {
       const int j = hits[h];
       const float4 pj = a.pos[j];
       const int tj = a.type[j];
-      const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri, a.cell,
-                                              a.rcell);
+      const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri, cell,
+                                              rcell);
       lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi,
                                      make_float4(dr.x, dr.y, dr.z, pj.w), j, tj, fx, fy,
                                      fz, e_lj, e_c, vir);
@@ -240,8 +244,9 @@ k_lj_direct(PairArgs a, Accumulators acc) {
 template <int ACCUM, bool ENERGY, bool VIRIAL>
 static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream_t st) {
   size_t smem = sizeof(float) * a.n_types * (a.n_types + 1);
-  auto kern = ortho ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true>
-                    : k_lj_direct<ACCUM, ENERGY, VIRIAL, false>;
+  auto kern = a.bv.nsys > 0 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true>
+              : ortho        ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false>
+                             : k_lj_direct<ACCUM, ENERGY, VIRIAL, false, false>;
   // persistent grid: as many blocks as fit at once
   static int sms = 0;
   if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);

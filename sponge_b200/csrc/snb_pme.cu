@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <set>
+#include <tuple>
 #include <vector>
 
 #include "snb_internal.h"
@@ -94,6 +95,7 @@ struct TileGeom {
   int nt0, nt1, nt2;
   Cell rcell;
 };
+constexpr int kTileEdge = 8;  // grid tiles are kTileEdge^3 points
 
 // Fractional coordinate, base point u and fraction as PME_Atom_Near
 // (PM_force.cpp:707-733).
@@ -148,13 +150,29 @@ __global__ void k_pme_bin(int n, const float4* __restrict__ pos, TileGeom g,
 
 // Pack and bin in one pass: pos[s] = (crd[perm[s]], charge[perm[s]]) for the
 // pair kernel, and the PME base point / fraction / tile of the same atom.
+// The tile geometry of one system of a batch.
+__device__ __forceinline__ TileGeom sys_tiles(const SysGeom& s) {
+  TileGeom g;
+  g.K0 = s.K0;
+  g.K1 = s.K1;
+  g.K2 = s.K2;
+  g.T = kTileEdge;
+  g.nt0 = s.nt0;
+  g.nt1 = s.nt1;
+  g.nt2 = s.nt2;
+  g.rcell = s.rcell;
+  return g;
+}
+
+template <bool BATCH>
 __global__ void k_pack_pme_bin(int n, const float3* __restrict__ crd,
                                const float* __restrict__ charge,
                                const int* __restrict__ type, const int* __restrict__ perm,
                                float4* __restrict__ pos, int* __restrict__ type_sorted,
                                TileGeom g, int* __restrict__ atom_tile,
                                int* __restrict__ atom_slot, int* __restrict__ tile_count,
-                               float4* __restrict__ frq, int* __restrict__ upk) {
+                               float4* __restrict__ frq, int* __restrict__ upk,
+                               BatchView bv) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = s < n;
   int t = 0;
@@ -166,10 +184,16 @@ __global__ void k_pack_pme_bin(int n, const float3* __restrict__ crd,
     float q = charge[i];
     pos[s] = make_float4(r.x, r.y, r.z, q);
     if (type_sorted) type_sorted[s] = type[i];
+    int tile_begin = 0;
+    if (BATCH) {
+      const SysGeom& sg = bv.sys[bv.sys_of[s]];
+      g = sys_tiles(sg);
+      tile_begin = sg.tile_begin;
+    }
     int ux, uy, uz;
     float fx, fy, fz;
     pme_base(r, g.rcell, g.K0, g.K1, g.K2, ux, uy, uz, fx, fy, fz);
-    t = ((ux / g.T) * g.nt1 + (uy / g.T)) * g.nt2 + (uz / g.T);
+    t = tile_begin + ((ux / g.T) * g.nt1 + (uy / g.T)) * g.nt2 + (uz / g.T);
     fr4 = make_float4(fx, fy, fz, q);
     up = pack_u(ux, uy, uz);
   }
@@ -227,7 +251,7 @@ __device__ __forceinline__ int stencil_mask(int u, int K, int lo, int hi) {
   return m;
 }
 
-constexpr int kTile = 8;
+constexpr int kTile = kTileEdge;
 constexpr int kTile3 = kTile * kTile * kTile;
 
 // One CTA per 8x8x8 tile of the charge grid.  src{0,1,2}[t] = {count, b0,
@@ -268,16 +292,27 @@ __device__ __forceinline__ void spread_one(int* sq, float4 f, int ux, int uy, in
   }
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(256)
 k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
              const float4* __restrict__ binned, const int* __restrict__ binned_u,
              const int4* __restrict__ src0, const int4* __restrict__ src1,
-             const int4* __restrict__ src2, float* __restrict__ Q) {
+             const int4* __restrict__ src2, float* __restrict__ Q, BatchView bv) {
   __shared__ int sq[kTile3];
   __shared__ float sw[kSpreadList][12];
   __shared__ int2 su[kSpreadList];  // {packed base point, masks x | y<<4 | z<<8}
   __shared__ int scount;
-  const int t = blockIdx.x;
+  int t = blockIdx.x;
+  if (BATCH) {  // tile of one system: its geometry, tables and grid
+    const SysGeom& sg = bv.sys[bv.tile_sys[t]];
+    g = sys_tiles(sg);
+    t -= sg.tile_begin;
+    tile_start += sg.tile_begin;
+    src0 += sg.src_begin0;
+    src1 += sg.src_begin1;
+    src2 += sg.src_begin2;
+    Q += sg.grid_begin;
+  }
   const int t2 = t % g.nt2, t1 = (t / g.nt2) % g.nt1, t0 = t / (g.nt1 * g.nt2);
   const int lo0 = t0 * g.T, hi0 = min(lo0 + g.T, g.K0);
   const int lo1 = t1 * g.T, hi1 = min(lo1 + g.T, g.K1);
@@ -412,15 +447,33 @@ struct SpecGeom {
 
 constexpr int kSpecBlock = 256;
 
-template <bool VIRIAL>
+template <bool VIRIAL, bool BATCH>
 __global__ void __launch_bounds__(kSpecBlock)
 k_pme_influence(int nfft, SpecGeom g, const float* __restrict__ B0,
                 const float* __restrict__ B1, const float* __restrict__ B2,
                 cufftComplex* __restrict__ FQ, double* __restrict__ partial,
-                bool energy) {
+                bool energy, BatchView bv, const int4* __restrict__ blocks) {
   double e = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nfft;
-       idx += gridDim.x * blockDim.x) {
+  int first = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  if (BATCH) {  // block = {system, first, end} of one system's spectrum
+    const int4 bk = blocks[blockIdx.x];
+    const SysGeom& sg = bv.sys[bk.x];
+    g.K0 = sg.K0;
+    g.K1 = sg.K1;
+    g.K2 = sg.K2;
+    g.nc = sg.K2 / 2 + 1;
+    g.rcell = sg.rcell;
+    g.mpre = sg.mpre;
+    g.inv_pi_v = sg.inv_pi_v;
+    B0 += sg.b_begin0;
+    B1 += sg.b_begin1;
+    B2 += sg.b_begin2;
+    FQ += sg.spec_begin;
+    first = bk.y + threadIdx.x;
+    stride = blockDim.x;
+    nfft = bk.z;
+  }
+  for (int idx = first; idx < nfft; idx += stride) {
     int kz = idx % g.nc;
     int ky = (idx / g.nc) % g.K1;
     int kx = idx / (g.nc * g.K1);
@@ -508,18 +561,74 @@ __global__ void k_pme_finish(int nblocks, const double* __restrict__ partial,
   }
 }
 
+// Batch: one block per system sums its influence blocks (a contiguous range)
+// and its self / neutralising energy into sys_sums[s][8]; then one block adds
+// the systems in order into sums[8].  Fixed orders: deterministic.
+__global__ void k_pme_finish_batch(BatchView bv, const int* __restrict__ block_begin,
+                                   const double* __restrict__ partial,
+                                   const float4* __restrict__ frq, double beta,
+                                   double* __restrict__ sys_sums, bool energy) {
+  const int s = blockIdx.x;
+  const SysGeom& sg = bv.sys[s];
+  __shared__ double sh[32][2];
+  if (threadIdx.x < 7) {
+    double a = 0.0;
+    for (int b = block_begin[s]; b < block_begin[s + 1]; ++b)
+      a += partial[(size_t)b * 8 + threadIdx.x];
+    sys_sums[(size_t)s * 8 + threadIdx.x] = a;
+  }
+  if (!energy) return;
+  double q2 = 0.0, qs = 0.0;
+  for (int i = sg.atom_begin + threadIdx.x; i < sg.atom_end; i += blockDim.x) {
+    double q = frq[i].w;
+    q2 += q * q;
+    qs += q;
+  }
+  q2 = warp_sum(q2);
+  qs = warp_sum(qs);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[warp][0] = q2;
+    sh[warp][1] = qs;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += sh[w][0];
+      b += sh[w][1];
+    }
+    const double pi = 3.141592653589793238462643383;
+    sys_sums[(size_t)s * 8 + 7] =
+        -beta / sqrt(pi) * a - 0.5 * pi / (beta * beta * sg.volume) * b * b;
+  }
+}
+
+__global__ void k_pme_sum_systems(int nsys, const double* __restrict__ sys_sums,
+                                  double* __restrict__ sums) {
+  if (threadIdx.x >= 8) return;
+  double a = 0.0;
+  for (int s = 0; s < nsys; ++s) a += sys_sums[(size_t)s * 8 + threadIdx.x];
+  sums[threadIdx.x] = a;
+}
+
 // ---------------------------------------------------------------------------
 // Gather: four lanes per atom, lane o handles the 16 points of x offset o.
-template <int ACCUM>
+template <int ACCUM, bool BATCH>
 __global__ void k_pme_gather(int n, const float4* __restrict__ frq,
                              const int* __restrict__ upk, TileGeom g,
                              const float* __restrict__ phi, float scale,
-                             Accumulators acc) {
+                             Accumulators acc, BatchView bv) {
   int i = blockIdx.x * (blockDim.x >> 2) + (threadIdx.x >> 2);
   int ox = threadIdx.x & 3;
   bool active = i < n;
   float ax = 0.f, ay = 0.f, az = 0.f;
   if (active) {
+    if (BATCH) {
+      const SysGeom& sg = bv.sys[bv.sys_of[i]];
+      g = sys_tiles(sg);
+      phi += sg.grid_begin;
+    }
     float4 f = frq[i];
     int up = upk[i];
     int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
@@ -576,6 +685,34 @@ __global__ void k_pme_gather(int n, const float4* __restrict__ frq,
 }
 
 // ---------------------------------------------------------------------------
+// Source bins per tile along one axis of K points in tiles of T: the bins
+// holding a base point u with some stencil point (u - o) mod K, o in 0..3,
+// inside the tile.  Returns nonzero if a tile needs more than 3 bins.
+static int source_bins(int K, int T, std::vector<int4>& src) {
+  const int nt = ceil_div(K, T);
+  src.assign(nt, make_int4(0, 0, 0, 0));
+  for (int t = 0; t < nt; ++t) {
+    int lo = t * T, hi = std::min(lo + T, K);
+    std::set<int> bins;
+    for (int u = 0; u < K; ++u)
+      for (int o = 0; o < 4; ++o) {
+        int q = ((u - o) % K + K) % K;
+        if (q >= lo && q < hi) bins.insert(u / T);
+      }
+    if (bins.size() > 3) return 1;
+    int4 s = make_int4((int)bins.size(), 0, 0, 0);
+    int k = 0;
+    for (int b : bins) {
+      if (k == 0) s.y = b;
+      if (k == 1) s.z = b;
+      if (k == 2) s.w = b;
+      ++k;
+    }
+    src[t] = s;
+  }
+  return 0;
+}
+
 int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
              float cutoff, float tolerance, int fftx, int ffty, int fftz,
              float grid_spacing, int update_interval, bool reciprocal,
@@ -615,28 +752,8 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
     SNB_CUDA_TRY(cudaMalloc(&p.d_B[d], sizeof(float) * p.K[d]));
     SNB_CUDA_TRY(cudaMemcpy(p.d_B[d], b.data(), sizeof(float) * p.K[d],
                             cudaMemcpyHostToDevice));
-    // source bins per tile along this axis: bins holding a base point u with
-    // some stencil point (u - o) mod K, o in 0..3, inside the tile
-    std::vector<int4> src(p.nt[d]);
-    for (int t = 0; t < p.nt[d]; ++t) {
-      int lo = t * p.T, hi = std::min(lo + p.T, p.K[d]);
-      std::set<int> bins;
-      for (int u = 0; u < p.K[d]; ++u)
-        for (int o = 0; o < 4; ++o) {
-          int q = ((u - o) % p.K[d] + p.K[d]) % p.K[d];
-          if (q >= lo && q < hi) bins.insert(u / p.T);
-        }
-      if (bins.size() > 3) return fail(kBadInput, "PME: tile geometry");
-      int4 s = make_int4((int)bins.size(), 0, 0, 0);
-      int k = 0;
-      for (int b : bins) {
-        if (k == 0) s.y = b;
-        if (k == 1) s.z = b;
-        if (k == 2) s.w = b;
-        ++k;
-      }
-      src[t] = s;
-    }
+    std::vector<int4> src;
+    if (source_bins(p.K[d], p.T, src)) return fail(kBadInput, "PME: tile geometry");
     SNB_CUDA_TRY(cudaMalloc(&p.d_src[d], sizeof(int4) * p.nt[d]));
     SNB_CUDA_TRY(cudaMemcpy(p.d_src[d], src.data(), sizeof(int4) * p.nt[d],
                             cudaMemcpyHostToDevice));
@@ -665,7 +782,155 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
   return kOk;
 }
 
+int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
+                   float tolerance, float grid_spacing, bool reciprocal, bool excluded) {
+  if (n <= 0 || sys.empty()) return fail(kBadInput, "PME: empty batch");
+  const int nsys = (int)sys.size();
+  p.n = n;
+  p.cutoff = cutoff;
+  p.tolerance = tolerance;
+  p.update_interval = 1;
+  p.reciprocal = reciprocal;
+  p.excluded = excluded;
+  p.cell = sys[0].cell;
+  p.rcell = sys[0].rcell;
+  p.beta = get_beta(cutoff, tolerance);
+  p.T = kTile;
+  if (grid_spacing <= 0.f) grid_spacing = 1.0f;
+  const double mpre = M_PI * M_PI / ((double)p.beta * p.beta);
+  for (auto& g : sys) {
+    g.K0 = fft_size(g.cell.a11 / grid_spacing);
+    g.K1 = fft_size(g.cell.a22 / grid_spacing);
+    g.K2 = fft_size(g.cell.a33 / grid_spacing);
+    if (g.K0 > 1023 || g.K1 > 1023 || g.K2 > 1023)
+      return fail(kBadInput, "PME: grid dimension must be in [4, 1023]");
+    g.nt0 = ceil_div(g.K0, p.T);
+    g.nt1 = ceil_div(g.K1, p.T);
+    g.nt2 = ceil_div(g.K2, p.T);
+    g.volume = (double)g.cell.a11 * g.cell.a22 * g.cell.a33;
+    g.mpre = (float)mpre;
+    g.inv_pi_v = (float)(1.0 / (M_PI * g.volume));
+  }
+  // grids of the same size side by side (one batched FFT plan per size)
+  std::vector<int> order(nsys);
+  for (int s = 0; s < nsys; ++s) order[s] = s;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const SysGeom &x = sys[a], &y = sys[b];
+    return std::make_tuple(x.K0, x.K1, x.K2) < std::make_tuple(y.K0, y.K1, y.K2);
+  });
+  long long grid = 0, spec = 0;
+  for (int s : order) {
+    SysGeom& g = sys[s];
+    if (p.groups.empty() || p.groups.back().K[0] != g.K0 || p.groups.back().K[1] != g.K1 ||
+        p.groups.back().K[2] != g.K2) {
+      PME::FftGroup fg;
+      fg.K[0] = g.K0;
+      fg.K[1] = g.K1;
+      fg.K[2] = g.K2;
+      fg.count = 0;
+      fg.grid_begin = (int)grid;
+      fg.spec_begin = (int)spec;
+      p.groups.push_back(fg);
+    }
+    p.groups.back().count++;
+    g.grid_begin = (int)grid;
+    g.spec_begin = (int)spec;
+    grid += (long long)g.K0 * g.K1 * g.K2;
+    spec += (long long)g.K0 * g.K1 * (g.K2 / 2 + 1);
+  }
+  if (spec > 2147483647LL) return fail(kBadInput, "PME: batch grids exceed 32-bit offsets");
+  p.nall = (int)grid;
+  p.nfft = (int)spec;
+  // tiles, source bins and |b|^2 tables in system order
+  std::vector<int4> src_all[3];
+  std::vector<float> b_all[3];
+  std::vector<int> tile_sys;
+  std::vector<int4> blocks;
+  std::vector<int> block_begin(nsys + 1, 0);
+  int tiles = 0;
+  const int per_block = kSpecBlock * 8;  // spectrum points per influence block
+  for (int s = 0; s < nsys; ++s) {
+    SysGeom& g = sys[s];
+    g.tile_begin = tiles;
+    const int nt = g.nt0 * g.nt1 * g.nt2;
+    tiles += nt;
+    tile_sys.insert(tile_sys.end(), nt, s);
+    const int K[3] = {g.K0, g.K1, g.K2};
+    int* src_begin[3] = {&g.src_begin0, &g.src_begin1, &g.src_begin2};
+    int* b_begin[3] = {&g.b_begin0, &g.b_begin1, &g.b_begin2};
+    for (int d = 0; d < 3; ++d) {
+      std::vector<int4> src;
+      if (source_bins(K[d], p.T, src)) return fail(kBadInput, "PME: tile geometry");
+      *src_begin[d] = (int)src_all[d].size();
+      src_all[d].insert(src_all[d].end(), src.begin(), src.end());
+      *b_begin[d] = (int)b_all[d].size();
+      for (int k = 0; k < K[d]; ++k) b_all[d].push_back((float)bspline_mod2(k, K[d]));
+    }
+    const int nfft_s = g.K0 * g.K1 * (g.K2 / 2 + 1);
+    block_begin[s] = (int)blocks.size();
+    for (int b0 = 0; b0 < nfft_s; b0 += per_block)
+      blocks.push_back(make_int4(s, b0, std::min(b0 + per_block, nfft_s), 0));
+  }
+  block_begin[nsys] = (int)blocks.size();
+  p.ntiles = tiles;
+  p.spec_blocks = (int)blocks.size();
+  for (int d = 0; d < 3; ++d) {
+    SNB_CUDA_TRY(cudaMalloc(&p.d_B[d], sizeof(float) * b_all[d].size()));
+    SNB_CUDA_TRY(cudaMemcpy(p.d_B[d], b_all[d].data(), sizeof(float) * b_all[d].size(),
+                            cudaMemcpyHostToDevice));
+    SNB_CUDA_TRY(cudaMalloc(&p.d_src[d], sizeof(int4) * src_all[d].size()));
+    SNB_CUDA_TRY(cudaMemcpy(p.d_src[d], src_all[d].data(), sizeof(int4) * src_all[d].size(),
+                            cudaMemcpyHostToDevice));
+  }
+  SNB_CUDA_TRY(cudaMalloc(&p.d_tile_sys, sizeof(int) * tiles));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_tile_sys, tile_sys.data(), sizeof(int) * tiles,
+                          cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_spec_blocks, sizeof(int4) * blocks.size()));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_spec_blocks, blocks.data(), sizeof(int4) * blocks.size(),
+                          cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_sys_block_begin, sizeof(int) * (nsys + 1)));
+  SNB_CUDA_TRY(cudaMemcpy(p.d_sys_block_begin, block_begin.data(), sizeof(int) * (nsys + 1),
+                          cudaMemcpyHostToDevice));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_sys_sums, sizeof(double) * 8 * nsys));
+  SNB_CUDA_TRY(cudaMemset(p.d_sys_sums, 0, sizeof(double) * 8 * nsys));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_Q, sizeof(float) * p.nall));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_FQ, sizeof(cufftComplex) * p.nfft));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_phi, sizeof(float) * p.nall));
+  SNB_CUDA_TRY(cudaMemset(p.d_phi, 0, sizeof(float) * p.nall));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_tile_count, sizeof(int) * p.ntiles));
+  SNB_CUDA_TRY(cudaMemset(p.d_tile_count, 0, sizeof(int) * p.ntiles));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_tile_start, sizeof(int) * (p.ntiles + 1)));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_atom_tile, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_atom_slot, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_binned, sizeof(float4) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_binned_u, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_frq, sizeof(float4) * n));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_upk, sizeof(int) * n));
+  p.partial_blocks = p.spec_blocks;
+  SNB_CUDA_TRY(cudaMalloc(&p.d_partial, sizeof(double) * 8 * p.partial_blocks));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_sums, sizeof(double) * 8));
+  SNB_CUDA_TRY(cudaMemset(p.d_sums, 0, sizeof(double) * 8));
+  if (scan_reserve(p.scan, p.ntiles)) return kCudaError;
+  for (auto& fg : p.groups) {
+    int dims[3] = {fg.K[0], fg.K[1], fg.K[2]};
+    if (cufftPlanMany(&fg.r2c, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C,
+                      fg.count) != CUFFT_SUCCESS ||
+        cufftPlanMany(&fg.c2r, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R,
+                      fg.count) != CUFFT_SUCCESS)
+      return fail(kCudaError, "PME: cuFFT batched plan creation failed");
+  }
+  return kOk;
+}
+
 void pme_free(PME& p) {
+  for (auto& fg : p.groups) {
+    if (fg.r2c) cufftDestroy(fg.r2c);
+    if (fg.c2r) cufftDestroy(fg.c2r);
+  }
+  cudaFree(p.d_spec_blocks);
+  cudaFree(p.d_sys_block_begin);
+  cudaFree(p.d_sys_sums);
+  cudaFree(p.d_tile_sys);
   for (int d = 0; d < 3; ++d) cudaFree(p.d_src[d]);
   cudaFree(p.d_frq);
   cudaFree(p.d_upk);
@@ -693,10 +958,14 @@ int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const in
                  const int* perm, float4* pos, int* type_sorted, cudaStream_t st) {
   if (n != p.n) return fail(kBadInput, "PME: atom count differs from Initial");
   TileGeom g{p.K[0], p.K[1], p.K[2], p.T, p.nt[0], p.nt[1], p.nt[2], p.rcell};
-  k_pack_pme_bin<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, charge, type, perm, pos,
-                                                   type_sorted, g, p.d_atom_tile,
-                                                   p.d_atom_slot, p.d_tile_count, p.d_frq,
-                                                   p.d_upk);
+  if (p.bv.nsys > 0)
+    k_pack_pme_bin<true><<<ceil_div(n, 256), 256, 0, st>>>(
+        n, crd, charge, type, perm, pos, type_sorted, g, p.d_atom_tile, p.d_atom_slot,
+        p.d_tile_count, p.d_frq, p.d_upk, p.bv);
+  else
+    k_pack_pme_bin<false><<<ceil_div(n, 256), 256, 0, st>>>(
+        n, crd, charge, type, perm, pos, type_sorted, g, p.d_atom_tile, p.d_atom_slot,
+        p.d_tile_count, p.d_frq, p.d_upk, p.bv);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -706,9 +975,16 @@ int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const in
 int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
                   bool need_virial, cudaStream_t st) {
   TileGeom g{p.K[0], p.K[1], p.K[2], p.T, p.nt[0], p.nt[1], p.nt[2], p.rcell};
-  if (cufftSetStream(p.plan_r2c, st) != CUFFT_SUCCESS ||
-      cufftSetStream(p.plan_c2r, st) != CUFFT_SUCCESS)
+  const bool batch = p.bv.nsys > 0;
+  if (batch) {
+    for (auto& fg : p.groups)
+      if (cufftSetStream(fg.r2c, st) != CUFFT_SUCCESS ||
+          cufftSetStream(fg.c2r, st) != CUFFT_SUCCESS)
+        return fail(kCudaError, "PME: cufftSetStream failed");
+  } else if (cufftSetStream(p.plan_r2c, st) != CUFFT_SUCCESS ||
+             cufftSetStream(p.plan_c2r, st) != CUFFT_SUCCESS) {
     return fail(kCudaError, "PME: cufftSetStream failed");
+  }
   if (accum == kAccumFixed) {
     int rc = scan_exclusive(p.d_tile_count, p.d_tile_start, p.ntiles, nullptr, p.scan,
                             st);
@@ -716,15 +992,28 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
     k_pme_scatter<<<ceil_div(n, 256), 256, 0, st>>>(
         n, p.d_atom_tile, p.d_atom_slot, p.d_tile_start, p.d_frq, p.d_upk, p.d_binned,
         p.d_binned_u, p.d_tile_count, p.ntiles);
-    k_pme_spread<<<p.ntiles, 256, 0, st>>>(g, p.d_tile_start, p.d_binned, p.d_binned_u,
-                                           p.d_src[0], p.d_src[1], p.d_src[2], p.d_Q);
+    if (batch)
+      k_pme_spread<true><<<p.ntiles, 256, 0, st>>>(g, p.d_tile_start, p.d_binned,
+                                                   p.d_binned_u, p.d_src[0], p.d_src[1],
+                                                   p.d_src[2], p.d_Q, p.bv);
+    else
+      k_pme_spread<false><<<p.ntiles, 256, 0, st>>>(g, p.d_tile_start, p.d_binned,
+                                                    p.d_binned_u, p.d_src[0], p.d_src[1],
+                                                    p.d_src[2], p.d_Q, p.bv);
   } else {
+    if (batch) return fail(kNotSupported, "PME batch: fixed-point accumulation only");
     SNB_CUDA_TRY(cudaMemsetAsync(p.d_Q, 0, sizeof(float) * p.nall, st));
     SNB_CUDA_TRY(cudaMemsetAsync(p.d_tile_count, 0, sizeof(int) * p.ntiles, st));
     k_pme_spread_atomic<<<ceil_div(n, 16), 256, 0, st>>>(n, p.d_frq, p.d_upk, g, p.d_Q);
   }
-  if (cufftExecR2C(p.plan_r2c, p.d_Q, p.d_FQ) != CUFFT_SUCCESS)
+  if (batch) {
+    for (auto& fg : p.groups)
+      if (cufftExecR2C(fg.r2c, p.d_Q + fg.grid_begin, p.d_FQ + fg.spec_begin) !=
+          CUFFT_SUCCESS)
+        return fail(kCudaError, "PME: cufftExecR2C failed");
+  } else if (cufftExecR2C(p.plan_r2c, p.d_Q, p.d_FQ) != CUFFT_SUCCESS) {
     return fail(kCudaError, "PME: cufftExecR2C failed");
+  }
   SpecGeom sg;
   sg.K0 = p.K[0];
   sg.K1 = p.K[1];
@@ -733,12 +1022,38 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
   sg.rcell = p.rcell;
   sg.mpre = (float)(M_PI * M_PI / ((double)p.beta * p.beta));
   sg.inv_pi_v = (float)(1.0 / (M_PI * p.volume));
+  if (batch) {
+    if (need_virial)
+      k_pme_influence<true, true><<<p.spec_blocks, kSpecBlock, 0, st>>>(
+          p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy,
+          p.bv, p.d_spec_blocks);
+    else
+      k_pme_influence<false, true><<<p.spec_blocks, kSpecBlock, 0, st>>>(
+          p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy,
+          p.bv, p.d_spec_blocks);
+    if (need_energy || need_virial) {
+      k_pme_finish_batch<<<p.bv.nsys, 256, 0, st>>>(p.bv, p.d_sys_block_begin, p.d_partial,
+                                                    p.d_frq, (double)p.beta, p.d_sys_sums,
+                                                    need_energy);
+      k_pme_sum_systems<<<1, 32, 0, st>>>(p.bv.nsys, p.d_sys_sums, p.d_sums);
+    }
+    for (auto& fg : p.groups)
+      if (cufftExecC2R(fg.c2r, p.d_FQ + fg.spec_begin, p.d_phi + fg.grid_begin) !=
+          CUFFT_SUCCESS)
+        return fail(kCudaError, "PME: cufftExecC2R failed");
+    k_pme_gather<kAccumFixed, true><<<ceil_div(n, 64), 256, 0, st>>>(
+        n, p.d_frq, p.d_upk, g, p.d_phi, 1.0f, acc, p.bv);
+    SNB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+  }
   if (need_virial)
-    k_pme_influence<true><<<p.partial_blocks, kSpecBlock, 0, st>>>(
-        p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy);
+    k_pme_influence<true, false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
+        p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy, p.bv,
+        nullptr);
   else
-    k_pme_influence<false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
-        p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy);
+    k_pme_influence<false, false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
+        p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy, p.bv,
+        nullptr);
   if (need_energy || need_virial)
     k_pme_finish<<<1, 1024, 0, st>>>(p.partial_blocks, p.d_partial, p.d_frq, n,
                                      (double)p.beta, p.volume, p.d_sums, need_energy);
@@ -746,11 +1061,11 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
     return fail(kCudaError, "PME: cufftExecC2R failed");
   const float scale = (float)p.update_interval;
   if (accum == kAccumFixed)
-    k_pme_gather<kAccumFixed><<<ceil_div(n, 64), 256, 0, st>>>(n, p.d_frq, p.d_upk, g,
-                                                               p.d_phi, scale, acc);
+    k_pme_gather<kAccumFixed, false><<<ceil_div(n, 64), 256, 0, st>>>(
+        n, p.d_frq, p.d_upk, g, p.d_phi, scale, acc, p.bv);
   else
-    k_pme_gather<kAccumFloat><<<ceil_div(n, 64), 256, 0, st>>>(n, p.d_frq, p.d_upk, g,
-                                                               p.d_phi, scale, acc);
+    k_pme_gather<kAccumFloat, false><<<ceil_div(n, 64), 256, 0, st>>>(
+        n, p.d_frq, p.d_upk, g, p.d_phi, scale, acc, p.bv);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -770,17 +1085,22 @@ int pme_reciprocal(PME& p, const float4* pos, int n, Accumulators& acc, int accu
 // PM_force.cpp:1745-1817, factor 1 for one process):
 //   F/r = -q_i q_j ((2 beta r/sqrt(pi) e^{-b^2r^2} + erfc(beta r)) - 1)/r^3,
 //   E_i -= q_i q_j erf(beta r)/r, virial_i -= (F/r) dr (x) dr.
-template <int ACCUM, bool ENERGY, bool VIRIAL>
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool BATCH>
 __global__ void k_excluded(int n, const float3* __restrict__ crd,
                            const float* __restrict__ charge, Cell cell, Cell rcell,
                            float beta, const int* __restrict__ excl_start,
                            const int* __restrict__ excl_list,
                            const int* __restrict__ excl_numbers,
-                           const int* __restrict__ map, Accumulators acc) {
+                           const int* __restrict__ map, Accumulators acc, BatchView bv) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int cnt = excl_numbers[i];
   if (cnt <= 0) return;
+  if (BATCH) {  // excluded pairs never cross systems
+    const SysGeom& sg = bv.sys[bv.sys_of[i]];
+    cell = sg.cell;
+    rcell = sg.rcell;
+  }
   const int N = acc.n;
   int st = excl_start[i];
   float3 ri = crd[i];
@@ -838,38 +1158,47 @@ __global__ void k_excluded(int n, const float3* __restrict__ crd,
   }
 }
 
-template <int ACCUM>
+template <int ACCUM, bool BATCH>
 static void launch_excl2(int n, const float3* crd, const float* charge,
                          const Cell& cell, const Cell& rcell, float beta,
                          const int* es, const int* el, const int* en, const int* map,
-                         Accumulators& acc, bool energy, bool virial, cudaStream_t st) {
+                         Accumulators& acc, bool energy, bool virial, const BatchView& bv,
+                         cudaStream_t st) {
   dim3 g(ceil_div(n, 256)), b(256);
   if (energy && virial)
-    k_excluded<ACCUM, true, true><<<g, b, 0, st>>>(n, crd, charge, cell, rcell, beta,
-                                                  es, el, en, map, acc);
+    k_excluded<ACCUM, true, true, BATCH><<<g, b, 0, st>>>(n, crd, charge, cell, rcell, beta,
+                                                         es, el, en, map, acc, bv);
   else if (energy)
-    k_excluded<ACCUM, true, false><<<g, b, 0, st>>>(n, crd, charge, cell, rcell, beta,
-                                                   es, el, en, map, acc);
+    k_excluded<ACCUM, true, false, BATCH><<<g, b, 0, st>>>(n, crd, charge, cell, rcell,
+                                                          beta, es, el, en, map, acc, bv);
   else if (virial)
-    k_excluded<ACCUM, false, true><<<g, b, 0, st>>>(n, crd, charge, cell, rcell, beta,
-                                                   es, el, en, map, acc);
+    k_excluded<ACCUM, false, true, BATCH><<<g, b, 0, st>>>(n, crd, charge, cell, rcell,
+                                                          beta, es, el, en, map, acc, bv);
   else
-    k_excluded<ACCUM, false, false><<<g, b, 0, st>>>(n, crd, charge, cell, rcell,
-                                                    beta, es, el, en, map, acc);
+    k_excluded<ACCUM, false, false, BATCH><<<g, b, 0, st>>>(n, crd, charge, cell, rcell,
+                                                           beta, es, el, en, map, acc, bv);
 }
 
 int launch_excluded(int n, const float3* crd, const float* charge, const Cell& cell,
                     const Cell& rcell, float beta, const int* excl_start,
                     const int* excl_list, const int* excl_numbers, const int* map,
                     Accumulators& acc, int accum, bool energy, bool virial,
-                    cudaStream_t st) {
+                    cudaStream_t st, const BatchView& bv) {
   if (n <= 0 || !excl_numbers) return kOk;
-  if (accum == kAccumFixed)
-    launch_excl2<kAccumFixed>(n, crd, charge, cell, rcell, beta, excl_start, excl_list,
-                              excl_numbers, map, acc, energy, virial, st);
-  else
-    launch_excl2<kAccumFloat>(n, crd, charge, cell, rcell, beta, excl_start, excl_list,
-                              excl_numbers, map, acc, energy, virial, st);
+  if (bv.nsys > 0) {
+    if (accum != kAccumFixed) return fail(kNotSupported, "batch: fixed-point only");
+    launch_excl2<kAccumFixed, true>(n, crd, charge, cell, rcell, beta, excl_start,
+                                    excl_list, excl_numbers, map, acc, energy, virial, bv,
+                                    st);
+  } else if (accum == kAccumFixed) {
+    launch_excl2<kAccumFixed, false>(n, crd, charge, cell, rcell, beta, excl_start,
+                                     excl_list, excl_numbers, map, acc, energy, virial, bv,
+                                     st);
+  } else {
+    launch_excl2<kAccumFloat, false>(n, crd, charge, cell, rcell, beta, excl_start,
+                                     excl_list, excl_numbers, map, acc, energy, virial, bv,
+                                     st);
+  }
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }

@@ -254,3 +254,44 @@ def soft_dhdl(h, nl, box: Box, sc, beta):
                                           nl, ctypes.c_float(beta), 1, ctypes.byref(out),
                                           stream()), "lj_soft_dh_dlambda")
     return out.value
+
+
+def batch_concat(systems):
+    """Concatenated per-atom arrays of several boxes, exclusions made global."""
+    cat = lambda name, dt: np.ascontiguousarray(  # noqa: E731
+        np.concatenate([getattr(s, name) for s in systems]), dt)
+    es, el = [], []
+    atom_base = excl_base = 0
+    for s in systems:
+        es.append(s.excl_start + excl_base)
+        el.append(s.excl_list + atom_base)
+        atom_base += s.n
+        excl_base += len(s.excl_list)
+    return dict(
+        counts=np.array([s.n for s in systems], np.int32),
+        boxes=np.array([[s.box] * 3 for s in systems], np.float32).reshape(-1),
+        crd=cat("crd", np.float32).reshape(-1), vel=cat("vel", np.float32).reshape(-1),
+        charge=cat("charge", np.float32), lj_type=cat("lj_type", np.int32),
+        mass=cat("mass", np.float32),
+        excl_start=np.ascontiguousarray(np.concatenate(es), np.int32),
+        excl_numbers=cat("excl_numbers", np.int32),
+        excl_list=np.ascontiguousarray(np.concatenate(el) if sum(map(len, el)) else
+                                       np.zeros(1), np.int32),
+        n_excl=int(sum(len(x) for x in el)))
+
+
+def batch_create(systems, cutoff, skin=2.0, **opts):
+    lib = capi.load()
+    c = batch_concat(systems)
+    s0 = systems[0]
+    A = np.ascontiguousarray(s0.lj_A, np.float32)
+    B = np.ascontiguousarray(s0.lj_B, np.float32)
+    h = ctypes.c_void_p()
+    o = capi.options(cutoff=cutoff, skin=skin, **opts)
+    capi.check(lib.snb_batch_create(ctypes.byref(o), len(systems), c["counts"].ctypes.data,
+                                    c["boxes"].ctypes.data, s0.n_types,
+                                    c["lj_type"].ctypes.data, A.ctypes.data, B.ctypes.data,
+                                    c["charge"].ctypes.data, c["excl_start"].ctypes.data,
+                                    c["excl_numbers"].ctypes.data, c["excl_list"].ctypes.data,
+                                    c["n_excl"], ctypes.byref(h)), "batch_create")
+    return h, c

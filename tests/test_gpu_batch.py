@@ -1,0 +1,148 @@
+"""A batch of independent boxes in one engine (snb_batch_create): every box's
+forces against the FP64 oracle run of that box alone, and against the same
+box run through the single-box engine; energies summed over the boxes; NVE
+steps of the whole batch against single-box runs.
+
+Tolerances: forces relative RMS <= 1e-5 against FP64 per box; batch vs
+single-box engine <= 1e-6 relative RMS (same kernels and fixed-point sums;
+only the batched FFT plans differ); energies per component within 2e-6 of
+the component's magnitude, as for one box.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CUTOFF = 8.0
+
+
+@pytest.fixture(scope="module")
+def g():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need CUDA"
+    from tests import gpu_helpers
+    return gpu_helpers
+
+
+@pytest.fixture(scope="module")
+def boxes():
+    """Five boxes of 200-700 waters (grids 20^3-28^3; the two smallest have
+    3 cells per axis, the index ownership rule, the rest 5 and more)."""
+    from sponge_b200 import systems
+    return [systems.water_box(nw, seed=s, ion_pairs=None)
+            for s, nw in enumerate([200, 450, 700, 260, 520])]
+
+
+def _force(g, h, crd, n, energy=True):
+    import torch
+    lib = g.capi.load()
+    frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+    tot = torch.zeros(16, dtype=torch.float64, device="cuda")
+    g.capi.check(lib.snb_engine_force(h, g.ptr(crd), g.ptr(frc), 0, int(energy), 1,
+                                      g.ptr(tot), g.stream()), "engine_force")
+    torch.cuda.synchronize()
+    return frc.cpu().numpy().reshape(n, 3), tot.cpu().numpy()
+
+
+def test_batch_forces_match_fp64_and_single_box(g, oracle, boxes):
+    from sponge_b200 import systems
+    lib = g.capi.load()
+    h, c = g.batch_create(boxes, CUTOFF)
+    try:
+        crd = g.dev(c["crd"])
+        fb, tb = _force(g, h, crd, len(c["charge"]))
+    finally:
+        lib.snb_engine_destroy(h)
+    from tests.test_gpu_engine import oracle_total
+    base = 0
+    en_sum = {}
+    for s in boxes:
+        got = fb[base:base + s.n]
+        want, en, _ = oracle_total(oracle, s, CUTOFF)
+        assert g.rel_rms(got, want) <= 1e-5
+        for k, v in en.items():
+            en_sum[k] = en_sum.get(k, 0.0) + v
+        # the same box alone through the single-box engine
+        hs = g.engine_create(s, CUTOFF)
+        try:
+            fs, _ = _force(g, hs, g.dev(s.crd.reshape(-1), np.float32), s.n)
+        finally:
+            lib.snb_engine_destroy(hs)
+        assert g.rel_rms(got, fs) <= 1e-6
+        base += s.n
+    for k, idx in (("lj", 0), ("coul", 2), ("excl", 3), ("recip", 4), ("self", 5)):
+        assert abs(tb[idx] - en_sum[k]) <= 2e-6 * abs(en_sum[k]), k
+    assert tb[1] == pytest.approx(en_sum["lrc"], rel=1e-6)
+    assert abs(tb[7] - sum(en_sum.values())) <= 1e-6 * sum(abs(v) for v in en_sum.values())
+
+
+def test_batch_md_matches_single_boxes(g, boxes):
+    """100 graph-replayed NVE steps of the batch stay with single-box runs of
+    the same boxes (both fixed-point; coordinates agree to 1e-3 A)."""
+    import torch
+    from sponge_b200 import systems
+    lib = g.capi.load()
+    dt = 0.5e-3 * systems.TIME_CONVERSION
+    steps = 100
+    h, c = g.batch_create(boxes, CUTOFF)
+    st = torch.cuda.Stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+    try:
+        nb = np.concatenate([s.bonds + off for s, off in
+                             zip(boxes, np.cumsum([0] + [s.n for s in boxes])[:-1])])
+        na = np.concatenate([s.angles + off for s, off in
+                             zip(boxes, np.cumsum([0] + [s.n for s in boxes])[:-1])])
+        bonded = type("B", (), {})()
+        bonded.bonds, bonded.angles = nb.astype(np.int32), na.astype(np.int32)
+        g.engine_set_water_bonded(h, bonded)
+        crd, vel = g.dev(c["crd"]), g.dev(c["vel"])
+        invm = g.dev((1.0 / c["mass"]).astype(np.float32))
+        with torch.cuda.stream(st):
+            g.capi.check(lib.snb_engine_md_steps_graph(h, g.ptr(crd), g.ptr(vel), g.ptr(invm),
+                                                       ctypes.c_float(dt), 0, steps, sp),
+                         "batch md")
+        st.synchronize()
+        cb = crd.cpu().numpy().reshape(-1, 3)
+    finally:
+        lib.snb_engine_destroy(h)
+    base = 0
+    for s in boxes:
+        hs = g.engine_create(s, CUTOFF)
+        try:
+            g.engine_set_water_bonded(hs, s)
+            crd = g.dev(s.crd.reshape(-1), np.float32)
+            vel = g.dev(s.vel.reshape(-1), np.float32)
+            invm = g.dev((1.0 / s.mass).astype(np.float32))
+            with torch.cuda.stream(st):
+                g.capi.check(lib.snb_engine_md_steps_graph(hs, g.ptr(crd), g.ptr(vel),
+                                                           g.ptr(invm), ctypes.c_float(dt),
+                                                           0, steps, sp), "single md")
+            st.synchronize()
+            cs = crd.cpu().numpy().reshape(-1, 3)
+        finally:
+            lib.snb_engine_destroy(hs)
+        assert np.abs(cb[base:base + s.n] - cs).max() < 1e-3
+        base += s.n
+
+
+def test_batch_rejects_cross_system_exclusion(g, boxes):
+    lib = g.capi.load()
+    c = g.batch_concat(boxes[:2])
+    el = c["excl_list"].copy()
+    el[0] = boxes[0].n + 1  # points into the second box
+    import ctypes as ct
+    s0 = boxes[0]
+    A = np.ascontiguousarray(s0.lj_A, np.float32)
+    B = np.ascontiguousarray(s0.lj_B, np.float32)
+    h = ct.c_void_p()
+    o = g.capi.options(cutoff=CUTOFF)
+    rc = lib.snb_batch_create(ct.byref(o), 2, c["counts"].ctypes.data, c["boxes"].ctypes.data,
+                              s0.n_types, c["lj_type"].ctypes.data, A.ctypes.data,
+                              B.ctypes.data, c["charge"].ctypes.data,
+                              c["excl_start"].ctypes.data, c["excl_numbers"].ctypes.data,
+                              el.ctypes.data, c["n_excl"], ct.byref(h))
+    assert rc == 1
+    assert b"between two systems" in lib.snb_last_error()
