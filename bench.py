@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--no-graph", action="store_true",
                    help="launch the step kernels on the stream instead of replaying "
                         "the captured step graph (for kernel profilers)")
+    p.add_argument("--batch-systems", type=int, default=256,
+                   help="boxes in the batched measurement (0: skip)")
+    p.add_argument("--batch-steps", type=int, default=200)
     p.add_argument("--drift-steps", type=int, default=2000,
                    help="NVE steps after the timed region over which the total-energy "
                         "drift is fitted (0: skip)")
@@ -279,6 +282,153 @@ def run_reference_arm(args):
 
 
 # --------------------------------------------------------------------------
+def _batch_member(seed):
+    from sponge_b200 import systems
+    return systems.config_batch_member(seed)
+
+
+def make_batch(seeds):
+    """The batch boxes (water count U[200, 2000] from each seed), generated in
+    a pool of spawned worker processes."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    workers = max(1, min(16, os.cpu_count() or 1, len(seeds)))
+    with cf.ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_batch_member, seeds))
+
+
+def run_batch(args, lib, world, rank, dist):
+    """Batched steps/s: this rank's share of the boxes (seed % world == rank)
+    advanced by one engine, one launch per phase per step, against the same
+    boxes each advanced by its own single-box engine (one captured step graph
+    launched per box per step).  Both with water bonds/angles, NVE, 0.5 fs,
+    cutoff 8 A, skin 2 A, PME grid per box from 1 A spacing, fixed point."""
+    import torch
+    from sponge_b200 import capi, systems
+    seeds = [s for s in range(args.batch_systems) if s % world == rank]
+    boxes = make_batch(seeds)
+    P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    dt = DT_FS * 1e-3 * systems.TIME_CONVERSION
+    cut = 8.0
+    st = torch.cuda.Stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+
+    def bonded(h, bonds, angles):
+        nb, na = len(bonds), len(angles)
+        arr = lambda a: np.ascontiguousarray(a, np.int32)  # noqa: E731
+        ba, bb = arr(bonds[:, 0]), arr(bonds[:, 1])
+        aa, ab, ac = arr(angles[:, 0]), arr(angles[:, 1]), arr(angles[:, 2])
+        bk = np.full(nb, systems.BOND_K, np.float32)
+        br = np.full(nb, systems.BOND_R0, np.float32)
+        ak = np.full(na, systems.ANGLE_K, np.float32)
+        at = np.full(na, systems.ANGLE_T0, np.float32)
+        capi.check(lib.snb_engine_set_bonded(h, nb, ba.ctypes.data, bb.ctypes.data,
+                                             bk.ctypes.data, br.ctypes.data, na,
+                                             aa.ctypes.data, ab.ctypes.data, ac.ctypes.data,
+                                             ak.ctypes.data, at.ctypes.data), "set_bonded")
+
+    # ---- the batch in one engine
+    offs = np.cumsum([0] + [b.n for b in boxes])
+    cat = lambda name, dt_: np.ascontiguousarray(  # noqa: E731
+        np.concatenate([getattr(b, name) for b in boxes]), dt_)
+    es = np.concatenate([b.excl_start + sum(len(x.excl_list) for x in boxes[:k])
+                         for k, b in enumerate(boxes)]).astype(np.int32)
+    el = np.concatenate([b.excl_list + offs[k] for k, b in enumerate(boxes)]).astype(np.int32)
+    en = cat("excl_numbers", np.int32)
+    typ, q = cat("lj_type", np.int32), cat("charge", np.float32)
+    A = np.ascontiguousarray(boxes[0].lj_A, np.float32)
+    B = np.ascontiguousarray(boxes[0].lj_B, np.float32)
+    counts = np.array([b.n for b in boxes], np.int32)
+    lens = np.array([[b.box] * 3 for b in boxes], np.float32).reshape(-1)
+    opts = capi.options(cutoff=cut, skin=SKIN)
+    h = ctypes.c_void_p()
+    capi.check(lib.snb_batch_create(ctypes.byref(opts), len(boxes), counts.ctypes.data,
+                                    lens.ctypes.data, boxes[0].n_types, typ.ctypes.data,
+                                    A.ctypes.data, B.ctypes.data, q.ctypes.data,
+                                    es.ctypes.data, en.ctypes.data, el.ctypes.data, len(el),
+                                    ctypes.byref(h)), "batch_create")
+    bonded(h, np.concatenate([b.bonds + offs[k] for k, b in enumerate(boxes)]),
+           np.concatenate([b.angles + offs[k] for k, b in enumerate(boxes)]))
+    crd = torch.from_numpy(cat("crd", np.float32).reshape(-1).copy()).cuda()
+    vel = torch.from_numpy(cat("vel", np.float32).reshape(-1).copy()).cuda()
+    invm = torch.from_numpy((1.0 / cat("mass", np.float32)).astype(np.float32)).cuda()
+    KB, WB = max(1, args.batch_steps), 3
+    with torch.cuda.stream(st):
+        capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                                 0, 100 + WB, sp), "batch warm-up")
+    st.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    with torch.cuda.stream(st):
+        capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                                 100 + WB, KB, sp), "batch steps")
+    e1.record(st)
+    st.synchronize()
+    ms_b = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    kn, libk, bodyk = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    capi.check(lib.snb_engine_graph_info(h, ctypes.byref(kn), ctypes.byref(libk),
+                                         ctypes.byref(bodyk), sp), "graph_info")
+    lib.snb_engine_destroy(h)
+
+    # ---- one engine per box, one step graph launched per box per step
+    singles = []
+    for b in boxes:
+        hs = ctypes.c_void_p()
+        bes, ben = np.ascontiguousarray(b.excl_start, np.int32), np.ascontiguousarray(
+            b.excl_numbers, np.int32)
+        bel = np.ascontiguousarray(b.excl_list if len(b.excl_list) else np.zeros(1), np.int32)
+        bt, bq = np.ascontiguousarray(b.lj_type, np.int32), np.ascontiguousarray(b.charge,
+                                                                                 np.float32)
+        capi.check(lib.snb_engine_create(ctypes.byref(opts), b.n,
+                                         capi.boundary(b.cell(), b.rcell()), b.n_types,
+                                         bt.ctypes.data, A.ctypes.data, B.ctypes.data,
+                                         bq.ctypes.data, bes.ctypes.data, ben.ctypes.data,
+                                         bel.ctypes.data, len(b.excl_list), ctypes.byref(hs)),
+                   "engine_create")
+        bonded(hs, b.bonds, b.angles)
+        c = torch.from_numpy(b.crd.reshape(-1).copy()).cuda()
+        v = torch.from_numpy(b.vel.reshape(-1).copy()).cuda()
+        m = torch.from_numpy((1.0 / b.mass).astype(np.float32)).cuda()
+        singles.append((hs, c, v, m))
+    KS = max(1, min(KB, 20))
+    with torch.cuda.stream(st):
+        for hs, c, v, m in singles:
+            capi.check(lib.snb_engine_md_steps_graph(hs, P(c), P(v), P(m), ctypes.c_float(dt),
+                                                     0, 100 + WB, sp), "single warm-up")
+    st.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record(st)
+    with torch.cuda.stream(st):  # each box's KS steps back to back, box after box
+        for hs, c, v, m in singles:
+            capi.check(lib.snb_engine_md_steps_graph(hs, P(c), P(v), P(m), ctypes.c_float(dt),
+                                                     100 + WB, KS, sp), "single steps")
+    e1.record(st)
+    st.synchronize()
+    ms_s = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    for hs, _, _, _ in singles:
+        lib.snb_engine_destroy(hs)
+    if dist:
+        dist.all_reduce(ms_b, op=dist.ReduceOp.MAX)
+        dist.all_reduce(ms_s, op=dist.ReduceOp.MAX)
+    sps_b = KB / (float(ms_b.item()) / 1e3)
+    sps_s = KS / (float(ms_s.item()) / 1e3)
+    K = [systems.fft_size(b.box) for b in boxes]
+    return {"systems": args.batch_systems, "systems_per_rank": len(boxes),
+            "atoms_per_rank": int(offs[-1]), "steps": KB,
+            "steps_per_s": sps_b, "ms_per_step": float(ms_b.item()) / KB,
+            "one_system_per_launch_steps_per_s": sps_s,
+            "one_system_per_launch_steps": KS,
+            "speedup_vs_one_system_per_launch": sps_b / sps_s,
+            "kernels_per_step": kn.value - libk.value, "library_kernels_per_step": libk.value,
+            "pme_grids": f"{min(K)}^3..{max(K)}^3",
+            "workload": "256 water+NaCl boxes (seeds 0-255, 200-2000 waters each, 1 g/cm^3), "
+                        "cutoff 8 A, skin 2 A, PME order 4 at 1 A spacing, NVE 0.5 fs, "
+                        "fixed-point accumulation"}
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
@@ -451,10 +601,11 @@ def run_ours(args):
         except Exception as ex:  # noqa: BLE001
             cpu_base = {"unavailable": f"{type(ex).__name__}: {ex}"}
 
+    lib.snb_engine_destroy(h)
+    batch = run_batch(args, lib, world, rank, dist) if args.batch_systems > 0 else None
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    lib.snb_engine_destroy(h)
     if rank != 0:
         return 0
     line = {
@@ -480,6 +631,7 @@ def run_ours(args):
                               "integrate"], [round(float(x), 5) for x in phases])),
         "nl_rebuilds": int(rebuilds.value), "pairs": listed,
         "nve_drift": drift,
+        "batch": batch,
         "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clk,
     }
     print(json.dumps(line))

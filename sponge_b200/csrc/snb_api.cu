@@ -1406,11 +1406,24 @@ extern "C" int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
   if (rc) return rc;
   cudaStream_t st = S(stream);
   cudaGraph_t g = nullptr;
-  cufftSetStream(e->pme.plan_r2c, st);
-  cufftSetStream(e->pme.plan_c2r, st);
-  SNB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  cufftExecR2C(e->pme.plan_r2c, e->pme.d_Q, e->pme.d_FQ);
-  cufftExecC2R(e->pme.plan_c2r, e->pme.d_FQ, e->pme.d_phi);
+  PME& p = e->pme;
+  if (p.bv.nsys > 0) {  // a batch: one plan pair per grid size
+    for (auto& fg : p.groups) {
+      cufftSetStream(fg.r2c, st);
+      cufftSetStream(fg.c2r, st);
+    }
+    SNB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (auto& fg : p.groups) {
+      cufftExecR2C(fg.r2c, p.d_Q + fg.grid_begin, p.d_FQ + fg.spec_begin);
+      cufftExecC2R(fg.c2r, p.d_FQ + fg.spec_begin, p.d_phi + fg.grid_begin);
+    }
+  } else {
+    cufftSetStream(p.plan_r2c, st);
+    cufftSetStream(p.plan_c2r, st);
+    SNB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cufftExecR2C(p.plan_r2c, p.d_Q, p.d_FQ);
+    cufftExecC2R(p.plan_c2r, p.d_FQ, p.d_phi);
+  }
   SNB_CUDA_TRY(cudaStreamEndCapture(st, &g));
   rc = count(g, library_kernel_nodes);
   cudaGraphDestroy(g);
