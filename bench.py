@@ -298,14 +298,16 @@ def make_batch(seeds):
 
 
 def run_batch(args, lib, world, rank, dist):
-    """Batched steps/s: this rank's share of the boxes (seed % world == rank)
-    advanced by one engine, one launch per phase per step, against the same
+    """Batched steps/s: this rank's share of the boxes (cost-balanced by
+    sponge_b200.sharding) advanced by one engine, one launch per phase per
+    step, against the same
     boxes each advanced by its own single-box engine (one captured step graph
     launched per box per step).  Both with water bonds/angles, NVE, 0.5 fs,
     cutoff 8 A, skin 2 A, PME grid per box from 1 A spacing, fixed point."""
     import torch
-    from sponge_b200 import capi, systems
-    seeds = [s for s in range(args.batch_systems) if s % world == rank]
+    from sponge_b200 import capi, sharding, systems
+    sizes = [systems.batch_member_size(s) for s in range(args.batch_systems)]
+    seeds = sharding.shard([sharding.box_cost(n, k) for n, k in sizes], world)[rank]
     boxes = make_batch(seeds)
     P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
     dt = DT_FS * 1e-3 * systems.TIME_CONVERSION

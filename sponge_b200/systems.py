@@ -370,8 +370,20 @@ def config_100k(seed: int = 0) -> System:
     return water_box(33333, seed=seed, ion_pairs=None)
 
 
+def batch_member_waters(seed: int) -> int:
+    """Water count U[200, 2000] of the batch box with this seed."""
+    rng = np.random.default_rng(10_000 + seed)
+    return int(rng.integers(200, 2001))
+
+
+def batch_member_size(seed: int) -> tuple[int, int]:
+    """(atoms, PME grid edge) of the batch box with this seed, without
+    building it."""
+    nw = batch_member_waters(seed)
+    box = (nw * WATER_VOLUME_A3) ** (1.0 / 3.0)
+    return 3 * nw - 4 * ion_pairs_for(box), fft_size(box)  # an ion replaces a water
+
+
 def config_batch_member(seed: int) -> System:
     """One box of the 256-box batch: water count U[200, 2000] from the seed."""
-    rng = np.random.default_rng(10_000 + seed)
-    nw = int(rng.integers(200, 2001))
-    return water_box(nw, seed=seed, ion_pairs=None)
+    return water_box(batch_member_waters(seed), seed=seed, ion_pairs=None)
