@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--no-graph", action="store_true",
                    help="launch the step kernels on the stream instead of replaying "
                         "the captured step graph (for kernel profilers)")
+    p.add_argument("--no-tune", action="store_true",
+                   help="keep the default launch shapes (skip the autotuner)")
     p.add_argument("--batch-systems", type=int, default=256,
                    help="boxes in the batched measurement (0: skip)")
     p.add_argument("--batch-steps", type=int, default=200)
@@ -357,7 +359,15 @@ def run_batch(args, lib, world, rank, dist):
     KB, WB = max(1, args.batch_steps), 3
     with torch.cuda.stream(st):
         capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
-                                                 0, 100 + WB, sp), "batch warm-up")
+                                                 0, 100, sp), "batch warm-up")
+    tuned = np.zeros(4, np.int32)
+    if not args.no_tune:
+        with torch.cuda.stream(st):
+            capi.check(lib.snb_engine_autotune(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                               5, tuned.ctypes.data, sp), "batch autotune")
+    with torch.cuda.stream(st):
+        capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                                 100, WB, sp), "batch warm-up")
     st.synchronize()
     if dist:
         dist.barrier()
@@ -426,6 +436,9 @@ def run_batch(args, lib, world, rank, dist):
             "speedup_vs_one_system_per_launch": sps_b / sps_s,
             "kernels_per_step": kn.value - libk.value, "library_kernels_per_step": libk.value,
             "pme_grids": f"{min(K)}^3..{max(K)}^3",
+            "tuned": (None if args.no_tune else dict(zip(
+                ["pair_unroll", "pair_blocks_per_sm", "search_blocks_per_sm",
+                 "gather_threads"], [int(x) for x in tuned]))),
             "workload": "256 water+NaCl boxes (seeds 0-255, 200-2000 waters each, 1 g/cm^3), "
                         "cutoff 8 A, skin 2 A, PME order 4 at 1 A spacing, NVE 0.5 fs, "
                         "fixed-point accumulation"}
@@ -499,6 +512,11 @@ def run_ours(args):
             ke = 0.5 * (mass[:, None] * v * v).sum()
             t_now = 2.0 * ke / (3.0 * n * systems.KB)
             vel.mul_(float(torch.sqrt(300.0 / t_now)))
+    tuned = np.zeros(4, np.int32)
+    if not args.no_tune:
+        with torch.cuda.stream(st):
+            capi.check(lib.snb_engine_autotune(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                               10, tuned.ctypes.data, sp), "autotune")
     with torch.cuda.stream(st):
         steps(EQ, W)
     st.synchronize()
@@ -633,6 +651,9 @@ def run_ours(args):
                               "integrate"], [round(float(x), 5) for x in phases])),
         "nl_rebuilds": int(rebuilds.value), "pairs": listed,
         "nve_drift": drift,
+        "tuned": (None if args.no_tune else dict(zip(
+            ["pair_unroll", "pair_blocks_per_sm", "search_blocks_per_sm", "gather_threads"],
+            [int(x) for x in tuned]))),
         "batch": batch,
         "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clk,
     }

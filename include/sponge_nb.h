@@ -334,6 +334,17 @@ int snb_engine_md_steps_graph(snb_engine* e, float* crd, float* vel,
 int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
                              const float* inverse_mass, float dt, int first_step,
                              int steps, double* h_phase_ms, void* stream);
+/* Autotuner (no counterpart in the reference).  Times `steps` stream-launched
+ * steps from the same coordinates for each candidate launch shape and keeps
+ * the fastest: the pair kernel's candidates per lane per scan round
+ * (2, 4, 8) and persistent blocks per SM (occupancy maximum, 2, 3), the
+ * pair search's blocks per SM (4, 8, 16), the PME gather's threads per block
+ * (128, 256, 512).  crd / vel are restored; the next step rebuilds the list
+ * and recaptures the step graph.  h_choice[0..3] receives the choices in
+ * that order (0 blocks per SM = occupancy maximum).  Allocates scratch. */
+int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
+                        const float* inverse_mass, float dt, int steps,
+                        int* h_choice, void* stream);
 /* Kernel nodes of the captured one-step graph: top level (a step without a
  * neighbor rebuild), cuFFT's share of them, and the kernels inside the
  * conditional rebuild node. */

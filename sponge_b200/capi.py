@@ -61,7 +61,7 @@ EXPORTED = [
     "snb_pme_excluded_force_noalloc",
     "snb_engine_create", "snb_batch_create", "snb_engine_force", "snb_engine_set_bonded",
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_profile_steps",
-    "snb_engine_graph_info", "snb_engine_stats",
+    "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
     "snb_engine_destroy",
 ]
 
@@ -123,6 +123,7 @@ _SIGS = {
     "snb_engine_md_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_md_steps_graph": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_profile_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P, _P]),
+    "snb_engine_autotune": (_I, [_P, _P, _P, _P, _F, _I, _P, _P]),
     "snb_engine_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I),
                                    ctypes.POINTER(_I), _P]),
     "snb_engine_stats": (_I, [_P, ctypes.POINTER(_LL), ctypes.POINTER(_LL), _P]),

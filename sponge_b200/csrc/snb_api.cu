@@ -126,6 +126,9 @@ struct snb_engine {
   BatchView bv;
   double lrc_energy = 0.0;   // tail energy summed over the boxes
   double lrc_virial = 0.0;   // tail virial (diagonal) summed over the boxes
+  // launch shapes picked by snb_engine_autotune
+  int pair_unroll = 4;
+  int pair_blocks_per_sm = 0;
   cudaStream_t side = nullptr;  // captures the conditional rebuild body
   int body_kernels = 0;         // kernel nodes inside the rebuild body
   // recovery snapshot for neighbor-list overflow
@@ -1144,6 +1147,8 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   a.cutoff2 = e->opt.cutoff * e->opt.cutoff;
   a.beta = e->pme.beta;
   a.bv = e->bv;
+  a.unroll = e->pair_unroll;
+  a.blocks_per_sm = e->pair_blocks_per_sm;
   rc = launch_pair(a, e->acc, e->accum, energy, virial, true, st);
   if (rc) return rc;
   prof_mark(e, 3, st);
@@ -1373,6 +1378,110 @@ extern "C" int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
   }
   e->prof_on = false;
   for (int k = 0; k < 7; ++k) h_phase_ms[k] = acc[k] / steps;
+  return kOk;
+}
+
+// Times `steps` stream-launched steps from the same starting coordinates for
+// each candidate launch shape and keeps the fastest: the pair kernel's scan
+// unroll (2, 4, 8) and blocks per SM (occupancy maximum, 2, 3), the pair
+// search's blocks per SM (4, 8, 16; a rebuild is forced every step), and the
+// gather's threads per block (128, 256, 512).  crd / vel are restored.
+extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
+                                   const float* invm, float dt, int steps, int* h_choice,
+                                   void* stream) {
+  if (!e || !crd || !vel || !invm || steps <= 0)
+    return fail(kBadInput, "engine_autotune: bad argument");
+  if (e->accum != kAccumFixed) return fail(kNotSupported, "autotune: fixed point only");
+  cudaStream_t st = S(stream);
+  const size_t bytes = sizeof(float) * 3 * e->n;
+  float *c0 = nullptr, *v0 = nullptr;
+  SNB_CUDA_TRY(cudaMalloc(&c0, bytes));
+  SNB_CUDA_TRY(cudaMalloc(&v0, bytes));
+  SNB_CUDA_TRY(cudaMemcpyAsync(c0, crd, bytes, cudaMemcpyDeviceToDevice, st));
+  SNB_CUDA_TRY(cudaMemcpyAsync(v0, vel, bytes, cudaMemcpyDeviceToDevice, st));
+  for (int k = 0; k < 8; ++k)
+    if (!e->prof_ev[k]) SNB_CUDA_TRY(cudaEventCreate(&e->prof_ev[k]));
+  // mean ms of phase `ph` (between prof_ev[ph] and prof_ev[ph + 1]) over the
+  // steps, from the saved coordinates; force_nl: rebuild every step
+  auto measure = [&](int ph, bool force_nl, double* ms) -> int {
+    SNB_CUDA_TRY(cudaMemcpyAsync(crd, c0, bytes, cudaMemcpyDeviceToDevice, st));
+    SNB_CUDA_TRY(cudaMemcpyAsync(vel, v0, bytes, cudaMemcpyDeviceToDevice, st));
+    double acc = 0.0;
+    e->prof_on = true;
+    for (int s = -1; s < steps; ++s) {  // s = -1: untimed warm-up step
+      int rc = engine_md_step(e, crd, vel, invm, dt, 1 + s, force_nl || s < 0, st);
+      if (rc) {
+        e->prof_on = false;
+        return rc;
+      }
+      SNB_CUDA_TRY(cudaEventSynchronize(e->prof_ev[7]));
+      float m = 0.f;
+      SNB_CUDA_TRY(cudaEventElapsedTime(&m, e->prof_ev[ph], e->prof_ev[ph + 1]));
+      if (s >= 0) acc += m;
+    }
+    e->prof_on = false;
+    *ms = acc / steps;
+    return kOk;
+  };
+  int rc = kOk;
+  double best = 1e30, ms = 0.0;
+  int bu = e->pair_unroll, bb = e->pair_blocks_per_sm;
+  for (int u : {2, 4, 8})
+    for (int b : {0, 2, 3}) {
+      e->pair_unroll = u;
+      e->pair_blocks_per_sm = b;
+      if ((rc = measure(2, false, &ms))) break;
+      if (ms < best) {
+        best = ms;
+        bu = u;
+        bb = b;
+      }
+    }
+  e->pair_unroll = bu;
+  e->pair_blocks_per_sm = bb;
+  int bs = e->nl.search_blocks_per_sm;
+  best = 1e30;
+  for (int b : {4, 8, 16}) {
+    if (rc) break;
+    e->nl.search_blocks_per_sm = b;
+    if ((rc = measure(0, true, &ms))) break;
+    if (ms < best) {
+      best = ms;
+      bs = b;
+    }
+  }
+  e->nl.search_blocks_per_sm = bs;
+  int bg = e->pme.gather_threads;
+  best = 1e30;
+  for (int gt : {128, 256, 512}) {
+    if (rc) break;
+    e->pme.gather_threads = gt;
+    if ((rc = measure(4, false, &ms))) break;
+    if (ms < best) {
+      best = ms;
+      bg = gt;
+    }
+  }
+  e->pme.gather_threads = bg;
+  cudaMemcpyAsync(crd, c0, bytes, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(vel, v0, bytes, cudaMemcpyDeviceToDevice, st);
+  cudaStreamSynchronize(st);
+  cudaFree(c0);
+  cudaFree(v0);
+  if (rc) return rc;
+  e->steps_done = 0;  // the next step rebuilds the list for the restored frame
+  if (e->graph_exec) {  // recapture with the chosen shapes
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+    e->graph = nullptr;
+  }
+  if (h_choice) {
+    h_choice[0] = e->pair_unroll;
+    h_choice[1] = e->pair_blocks_per_sm;
+    h_choice[2] = e->nl.search_blocks_per_sm;
+    h_choice[3] = e->pme.gather_threads;
+  }
   return kOk;
 }
 

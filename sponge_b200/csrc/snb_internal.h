@@ -105,6 +105,7 @@ struct NeighborList {
   int* d_excl_count = nullptr;
   int* d_excl_partner = nullptr;
   BatchView bv;                // nsys > 0: a batch of boxes (per-system grids)
+  int search_blocks_per_sm = 8;  // persistent blocks of the pair search per SM
   // binning
   int* d_cell_count = nullptr;  // [ncell]
   int* d_cell_start = nullptr;  // [ncell + 1]
@@ -214,6 +215,8 @@ struct PairArgs {
   float cutoff2;
   float beta;
   BatchView bv;                 // nsys > 0: per-system boxes (rectangular)
+  int unroll = 4;               // scan candidates per lane per round (2, 4, 8)
+  int blocks_per_sm = 0;        // persistent blocks per SM, 0: occupancy maximum
 };
 int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool ortho, cudaStream_t st);
@@ -293,6 +296,7 @@ struct PME {
   int* d_sys_block_begin = nullptr;  // [nsys + 1]
   double* d_sys_sums = nullptr;    // [nsys][8]
   int* d_tile_sys = nullptr;       // [ntiles]
+  int gather_threads = 256;        // threads per block of the force gather
 };
 int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
              float cutoff, float tolerance, int fftx, int ffty, int fftz,

@@ -772,7 +772,7 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   sa.cols = nl.d_cols;
   sa.flags = nl.d_flags;
   sa.bv = nl.bv;
-  const int blocks = std::min(ceil_div(n, 8), sms * 8);
+  const int blocks = std::min(ceil_div(n, 8), sms * std::max(1, nl.search_blocks_per_sm));
   if (nl.bv.nsys > 0)
     k_pair_search<true><<<blocks, 256, 0, st>>>(sa);
   else

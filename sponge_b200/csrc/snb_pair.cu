@@ -78,7 +78,8 @@ __device__ __forceinline__ void add_virial(Accumulators& acc, int s, const float
 // holds is taken in several rounds.
 constexpr int kWarps = 8;
 constexpr int kHitCap = 512;   // per-warp hit list (entries)
-constexpr int kScanU = 4;      // candidates per lane per scan round
+// candidates per lane per scan round: a template parameter (2, 4 or 8) that
+// the engine's autotuner picks; 4 elsewhere
 
 template <int ACCUM, bool ENERGY, bool VIRIAL>
 __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
@@ -135,9 +136,10 @@ __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
   }
 }
 
-template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO, bool BATCH>
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO, bool BATCH, int kScanU>
 __global__ void __launch_bounds__(256, 4)
 k_lj_direct(PairArgs a, Accumulators acc) {
+  static_assert(kScanU >= 1 && 32 * kScanU < kHitCap, "scan round exceeds the hit list");
   extern __shared__ float sh_tab[];
   __shared__ int hits_all[kWarps][kHitCap];
   float* sA = sh_tab;
@@ -244,15 +246,30 @@ k_lj_direct(PairArgs a, Accumulators acc) {
 template <int ACCUM, bool ENERGY, bool VIRIAL>
 static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream_t st) {
   size_t smem = sizeof(float) * a.n_types * (a.n_types + 1);
-  auto kern = a.bv.nsys > 0 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true>
-              : ortho        ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false>
-                             : k_lj_direct<ACCUM, ENERGY, VIRIAL, false, false>;
-  // persistent grid: as many blocks as fit at once
+  using Kern = void (*)(PairArgs, Accumulators);
+  Kern kern;
+  // the unroll choice applies to the MD step's variant (fixed point, force
+  // only, rectangular); the others take 4
+  const bool tunable = ACCUM == kAccumFixed && !ENERGY && !VIRIAL && ortho;
+  const int u = tunable ? a.unroll : 4;
+  if (a.bv.nsys > 0)
+    kern = u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 2>
+         : u == 8 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 8>
+                  : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 4>;
+  else if (ortho)
+    kern = u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 2>
+         : u == 8 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 8>
+                  : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4>;
+  else
+    kern = k_lj_direct<ACCUM, ENERGY, VIRIAL, false, false, 4>;
+  // persistent grid: as many blocks as fit at once, or the tuned count
   static int sms = 0;
   if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, smem);
-  int blocks = std::max(1, std::min(sms * std::max(per_sm, 1), ceil_div(a.n, kWarps)));
+  per_sm = std::max(per_sm, 1);
+  if (a.blocks_per_sm > 0) per_sm = std::min(per_sm, a.blocks_per_sm);
+  int blocks = std::max(1, std::min(sms * per_sm, ceil_div(a.n, kWarps)));
   kern<<<blocks, 32 * kWarps, smem, st>>>(a, acc);
 }
 

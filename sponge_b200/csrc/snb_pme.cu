@@ -1041,7 +1041,8 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
       if (cufftExecC2R(fg.c2r, p.d_FQ + fg.spec_begin, p.d_phi + fg.grid_begin) !=
           CUFFT_SUCCESS)
         return fail(kCudaError, "PME: cufftExecC2R failed");
-    k_pme_gather<kAccumFixed, true><<<ceil_div(n, 64), 256, 0, st>>>(
+    const int gt = p.gather_threads;  // 4 lanes per atom
+    k_pme_gather<kAccumFixed, true><<<ceil_div(n, gt / 4), gt, 0, st>>>(
         n, p.d_frq, p.d_upk, g, p.d_phi, 1.0f, acc, p.bv);
     SNB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -1060,11 +1061,12 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
   if (cufftExecC2R(p.plan_c2r, p.d_FQ, p.d_phi) != CUFFT_SUCCESS)
     return fail(kCudaError, "PME: cufftExecC2R failed");
   const float scale = (float)p.update_interval;
+  const int gt = p.gather_threads;  // 4 lanes per atom
   if (accum == kAccumFixed)
-    k_pme_gather<kAccumFixed, false><<<ceil_div(n, 64), 256, 0, st>>>(
+    k_pme_gather<kAccumFixed, false><<<ceil_div(n, gt / 4), gt, 0, st>>>(
         n, p.d_frq, p.d_upk, g, p.d_phi, scale, acc, p.bv);
   else
-    k_pme_gather<kAccumFloat, false><<<ceil_div(n, 64), 256, 0, st>>>(
+    k_pme_gather<kAccumFloat, false><<<ceil_div(n, gt / 4), gt, 0, st>>>(
         n, p.d_frq, p.d_upk, g, p.d_phi, scale, acc, p.bv);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;

@@ -132,3 +132,51 @@ def test_nve_energy_is_conserved(g, oracle, small_box):
     e_end = p1 + k1
     assert np.isfinite(e_end)
     assert abs(e_end - e_start) <= 2e-2 * k0
+
+
+def test_autotune_keeps_results_bitwise(g, box_9k):
+    """Launch shapes change only the schedule: the fixed-point forces after
+    tuning equal those before, bit for bit, and crd / vel come back intact."""
+    import torch
+    from sponge_b200 import systems
+    s = box_9k
+    lib = g.capi.load()
+    e = g.engine_create(s, 8.0)
+    g.engine_set_water_bonded(e, s)
+    crd = g.dev(s.crd.reshape(-1), np.float32)
+    vel = g.dev(s.vel.reshape(-1), np.float32)
+    invm = g.dev((1.0 / s.mass).astype(np.float32))
+    st = torch.cuda.Stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+    dt = 0.5e-3 * systems.TIME_CONVERSION
+
+    def force():
+        f = torch.zeros(3 * s.n, dtype=torch.float32, device="cuda")
+        with torch.cuda.stream(st):
+            g.capi.check(lib.snb_engine_force(e, g.ptr(crd), g.ptr(f), 0, 0, 0, None, sp),
+                         "engine_force")
+        st.synchronize()
+        return f.cpu().numpy()
+
+    try:
+        f0 = force()
+        c0, v0 = crd.cpu().numpy(), vel.cpu().numpy()
+        choice = np.zeros(4, np.int32)
+        with torch.cuda.stream(st):
+            g.capi.check(lib.snb_engine_autotune(e, g.ptr(crd), g.ptr(vel), g.ptr(invm),
+                                                 ctypes.c_float(dt), 3, choice.ctypes.data,
+                                                 sp), "autotune")
+        st.synchronize()
+        assert np.array_equal(crd.cpu().numpy(), c0)
+        assert np.array_equal(vel.cpu().numpy(), v0)
+        assert choice[0] in (2, 4, 8) and choice[1] in (0, 2, 3)
+        assert choice[2] in (4, 8, 16) and choice[3] in (128, 256, 512)
+        f1 = force()
+        assert np.array_equal(f0, f1)
+        with torch.cuda.stream(st):  # graph steps with the tuned shapes
+            g.capi.check(lib.snb_engine_md_steps_graph(e, g.ptr(crd), g.ptr(vel), g.ptr(invm),
+                                                       ctypes.c_float(dt), 0, 20, sp), "md")
+        st.synchronize()
+        assert np.isfinite(crd.cpu().numpy()).all()
+    finally:
+        lib.snb_engine_destroy(e)
