@@ -221,6 +221,31 @@ def nve_drift(lib, h, s, crd, vel, invm, first, total, samples, dt, run_steps, s
 
 
 # --------------------------------------------------------------------------
+class stdout_to_stderr:
+    """Sends file descriptor 1 to stderr for the duration: the reference's
+    modules print their initialisation reports with C stdio, which Python's
+    own redirection does not catch, and stdout must carry only the result
+    line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        try:
+            import ctypes.util
+            libc = ctypes.CDLL(ctypes.util.find_library("c"))
+            libc.fflush(None)
+        except OSError:
+            pass
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def cpu_reference_run(s, evals: int, warmup: int, rebuild_rate: float = 0.01):
     """Time the reference's own CPU path (oracle/_ref) on box `s`: per MD step
     the conditional neighbor update, excluded correction, LJ + direct Coulomb
@@ -230,20 +255,18 @@ def cpu_reference_run(s, evals: int, warmup: int, rebuild_rate: float = 0.01):
     if not os.path.exists(REF_SO):
         return None, "oracle/_ref/libsponge_ref.so not built"
     ref = ReferenceCPU(exact=False)
-    import contextlib
-    import io
-    with contextlib.redirect_stdout(io.StringIO()):
+    with stdout_to_stderr():
         ref.init(s, CUTOFF, SKIN)
-    cores = ref.max_threads()
-    t0 = time.perf_counter()
-    ref.nl_update_only(forced=True)
-    t_rebuild = time.perf_counter() - t0
-    for k in range(warmup):
-        ref.force_step(k)
-    t0 = time.perf_counter()
-    for k in range(evals):
-        ref.force_step(warmup + k)
-    t_step = (time.perf_counter() - t0) / evals + t_rebuild * rebuild_rate
+        cores = ref.max_threads()
+        t0 = time.perf_counter()
+        ref.nl_update_only(forced=True)
+        t_rebuild = time.perf_counter() - t0
+        for k in range(warmup):
+            ref.force_step(k)
+        t0 = time.perf_counter()
+        for k in range(evals):
+            ref.force_step(warmup + k)
+        t_step = (time.perf_counter() - t0) / evals + t_rebuild * rebuild_rate
     return dict(value=ns_per_day(1.0 / t_step), unit="ns/day", cores=cores,
                 kind="reference",
                 sample=(f"{evals} force evaluations (conditional neighbor update, "
