@@ -254,55 +254,72 @@ __device__ __forceinline__ int stencil_mask(int u, int K, int lo, int hi) {
 constexpr int kTile = kTileEdge;
 constexpr int kTile3 = kTile * kTile * kTile;
 
-// One CTA per 8x8x8 tile of the charge grid.  src{0,1,2}[t] = {count, b0,
-// b1, b2} lists the bins along each axis whose atoms reach tile t.
-// Phase 1: every thread takes atoms of those bins, tests whether the atom's
-// 4x4x4 stencil meets the tile and, if so, appends its 12 weights (charge
-// folded into the x weights), base point and per-axis masks to a list in
-// shared memory.  Phase 2: a warp takes one listed atom at a time, its 32
-// lanes cover the (oy, oz) offsets and half of the ox offsets, so two passes
-// place the 64 products.  Accumulation is int32 fixed point (2^22 per charge
-// unit) in shared memory; the tile is stored once.  Atoms beyond the list
-// capacity are spread by their own thread in phase 1.
-constexpr int kSpreadList = 512;
+// One block of kSpreadWarps warps per 8x8x8 tile of the charge grid,
+// accumulating in a shared-memory tile.  src{0,1,2}[t] = {count, b0, b1, b2}
+// lists the bins along each axis whose atoms can reach tile t.  The warps
+// take interleaved rounds of 32 atoms from those bins (one flat range of up
+// to 27 bin slices); pass 1 tests whether the atom's 4x4x4 stencil meets the
+// tile and appends the ones that do to the warp's list (ballot + popc);
+// pass 2 gives one lane per listed atom, which adds its up-to-64 products
+// (charge folded into the x weights) to the tile in int32 fixed point (2^22
+// per charge unit).  Block barriers only after zeroing and before the single
+// store of the tile: no global atomics, and the grid is the same bit pattern
+// for any atom order.  A list that fills up is drained and refilled.
+constexpr int kSpreadWarps = 2;
+constexpr int kSpreadList = 256;  // per-warp list of contributing atoms
 
-__device__ __forceinline__ void spread_one(int* sq, float4 f, int ux, int uy, int uz,
-                                           int mx, int my, int mz, const TileGeom& g,
-                                           int lo0, int lo1, int lo2) {
+// Local index (p - lo) of the stencil point u - o on an axis of K points,
+// or -1 when it falls outside [lo, hi); four offsets packed in bytes.
+__device__ __forceinline__ void stencil_local(int u, int K, int lo, int hi, int* l) {
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    int p = u - o;
+    p += p < 0 ? K : 0;
+    l[o] = (p >= lo && p < hi) ? p - lo : -1;
+  }
+}
+
+__device__ __forceinline__ void spread_atom(int* sq, float4 f, int up, const TileGeom& g,
+                                            int lo0, int hi0, int lo1, int hi1, int lo2,
+                                            int hi2) {
+  const int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
+  int lx[4], ly[4], lz[4];
+  stencil_local(ux, g.K0, lo0, hi0, lx);
+  stencil_local(uy, g.K1, lo1, hi1, ly);
+  stencil_local(uz, g.K2, lo2, hi2, lz);
   float wx[4], wy[4], wz[4];
   bspline4(f.x, wx);
   bspline4(f.y, wy);
   bspline4(f.z, wz);
+  const float qs = f.w * kGridScale;
+#pragma unroll
   for (int ox = 0; ox < 4; ++ox) {
-    if (!((mx >> ox) & 1)) continue;
-    int px = ux - ox;
-    px += px < 0 ? g.K0 : 0;
+    if (lx[ox] < 0) continue;
+    const float wq = qs * wx[ox];
+#pragma unroll
     for (int oy = 0; oy < 4; ++oy) {
-      if (!((my >> oy) & 1)) continue;
-      int py = uy - oy;
-      py += py < 0 ? g.K1 : 0;
-      for (int oz = 0; oz < 4; ++oz) {
-        if (!((mz >> oz) & 1)) continue;
-        int pz = uz - oz;
-        pz += pz < 0 ? g.K2 : 0;
-        atomicAdd(&sq[((px - lo0) * kTile + (py - lo1)) * kTile + (pz - lo2)],
-                  __float2int_rn(f.w * wx[ox] * wy[oy] * wz[oz] * kGridScale));
-      }
+      if (ly[oy] < 0) continue;
+      const float wxy = wq * wy[oy];
+      int* row = sq + (lx[ox] * kTile + ly[oy]) * kTile;
+#pragma unroll
+      for (int oz = 0; oz < 4; ++oz)
+        if (lz[oz] >= 0) atomicAdd(row + lz[oz], __float2int_rn(wxy * wz[oz]));
     }
   }
 }
 
 template <bool BATCH>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(32 * kSpreadWarps)
 k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
              const float4* __restrict__ binned, const int* __restrict__ binned_u,
              const int4* __restrict__ src0, const int4* __restrict__ src1,
-             const int4* __restrict__ src2, float* __restrict__ Q, BatchView bv) {
+             const int4* __restrict__ src2, float* __restrict__ Q, int ntiles,
+             BatchView bv) {
   __shared__ int sq[kTile3];
-  __shared__ float sw[kSpreadList][12];
-  __shared__ int2 su[kSpreadList];  // {packed base point, masks x | y<<4 | z<<8}
-  __shared__ int scount;
+  __shared__ int list_all[kSpreadWarps][kSpreadList];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int t = blockIdx.x;
+  int* list = list_all[w];
   if (BATCH) {  // tile of one system: its geometry, tables and grid
     const SysGeom& sg = bv.sys[bv.tile_sys[t]];
     g = sys_tiles(sg);
@@ -318,84 +335,61 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
   const int lo1 = t1 * g.T, hi1 = min(lo1 + g.T, g.K1);
   const int lo2 = t2 * g.T, hi2 = min(lo2 + g.T, g.K2);
   for (int k = threadIdx.x; k < kTile3; k += blockDim.x) sq[k] = 0;
-  if (threadIdx.x == 0) scount = 0;
   __syncthreads();
-  // the (up to 27) source bins as one flat range of atoms
-  __shared__ int sbeg[27], spre[28];
-  if (threadIdx.x == 0) {
-    const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
-    const int b0[3] = {s0.y, s0.z, s0.w};
-    const int b1[3] = {s1.y, s1.z, s1.w};
-    const int b2[3] = {s2.y, s2.z, s2.w};
-    int nb = 0, tot = 0;
-    for (int a = 0; a < s0.x; ++a)
-      for (int b = 0; b < s1.x; ++b)
-        for (int c = 0; c < s2.x; ++c) {
-          const int bin = (b0[a] * g.nt1 + b1[b]) * g.nt2 + b2[c];
-          sbeg[nb] = tile_start[bin];
-          spre[nb] = tot;
-          tot += tile_start[bin + 1] - tile_start[bin];
-          ++nb;
-        }
-    spre[nb] = tot;
-    for (int q = nb + 1; q < 28; ++q) spre[q] = tot;
+  // the (up to 27) source bins: lane b holds bin b's first atom and count
+  const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
+  const int nb = s0.x * s1.x * s2.x;
+  int beg = 0, cnt = 0;
+  if (lane < nb) {
+    const int a = lane / (s1.x * s2.x), b = (lane / s2.x) % s1.x, c = lane % s2.x;
+    const int b0 = a == 0 ? s0.y : (a == 1 ? s0.z : s0.w);
+    const int b1 = b == 0 ? s1.y : (b == 1 ? s1.z : s1.w);
+    const int b2 = c == 0 ? s2.y : (c == 1 ? s2.z : s2.w);
+    const int bin = (b0 * g.nt1 + b1) * g.nt2 + b2;
+    beg = tile_start[bin];
+    cnt = tile_start[bin + 1] - beg;
   }
-  __syncthreads();
-  const int total = spre[27];
-  for (int fi = threadIdx.x; fi < total; fi += blockDim.x) {
-    int bi = 0;
-    while (spre[bi + 1] <= fi) ++bi;
-    const int k = sbeg[bi] + (fi - spre[bi]);
-    {
-          const int up = binned_u[k];
-          const int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
-          const int mx = stencil_mask(ux, g.K0, lo0, hi0);
-          const int my = stencil_mask(uy, g.K1, lo1, hi1);
-          const int mz = stencil_mask(uz, g.K2, lo2, hi2);
-          if (!mx || !my || !mz) continue;
-          const float4 f = binned[k];
-          const int slot = atomicAdd(&scount, 1);
-          if (slot < kSpreadList) {
-            float w[4];
-            bspline4(f.x, w);
+  int incl = cnt;  // inclusive prefix of the counts over the bins
 #pragma unroll
-            for (int q = 0; q < 4; ++q) sw[slot][q] = f.w * w[q];
-            bspline4(f.y, w);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) sw[slot][4 + q] = w[q];
-            bspline4(f.z, w);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) sw[slot][8 + q] = w[q];
-            su[slot] = make_int2(up, mx | (my << 4) | (mz << 8));
-          } else {
-            spread_one(sq, f, ux, uy, uz, mx, my, mz, g, lo0, lo1, lo2);
-          }
-        }
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  const int excl = incl - cnt;
+  __syncwarp();
+  const unsigned lt = (1u << lane) - 1u;
+  int n_list = 0, bin_cursor = 0;
+  for (int base = 32 * w; base < total; base += 32 * kSpreadWarps) {
+    // atom of flat index base + lane: the bin whose range holds it
+    const int fi = base + lane;
+    int k = -1;
+    for (int b = bin_cursor; b < nb; ++b) {  // warp-uniform walk over the bins
+      const int eb = __shfl_sync(0xffffffffu, excl, b);
+      const int cb = __shfl_sync(0xffffffffu, cnt, b);
+      const int bb = __shfl_sync(0xffffffffu, beg, b);
+      if (fi >= eb && fi < eb + cb) k = bb + (fi - eb);
+      if (eb + cb >= base + 32) break;
+      bin_cursor = b + 1;
+    }
+    bool in = false;
+    if (k >= 0) {
+      const int up = binned_u[k];
+      const int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
+      in = stencil_mask(ux, g.K0, lo0, hi0) && stencil_mask(uy, g.K1, lo1, hi1) &&
+           stencil_mask(uz, g.K2, lo2, hi2);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    if (in) list[n_list + __popc(m & lt)] = k;
+    n_list += __popc(m);
+    if (n_list > kSpreadList - 32 || base + 32 * kSpreadWarps >= total) {
+      __syncwarp();
+      for (int e = lane; e < n_list; e += 32) {
+        const int ka = list[e];
+        spread_atom(sq, binned[ka], binned_u[ka], g, lo0, hi0, lo1, hi1, lo2, hi2);
       }
-  __syncthreads();
-  const int nlist = min(scount, kSpreadList);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const int oz = lane & 3, oy = (lane >> 2) & 3, oxl = lane >> 4;
-  for (int a = warp; a < nlist; a += nwarps) {
-    const int2 e = su[a];
-    const int mx = e.y & 15, my = (e.y >> 4) & 15, mz = (e.y >> 8) & 15;
-    if (!((my >> oy) & (mz >> oz) & 1)) continue;
-    const int ux = e.x >> 20, uy = (e.x >> 10) & 1023, uz = e.x & 1023;
-    int py = uy - oy;
-    py += py < 0 ? g.K1 : 0;
-    int pz = uz - oz;
-    pz += pz < 0 ? g.K2 : 0;
-    const float wyz = sw[a][4 + oy] * sw[a][8 + oz];
-    const int base = (py - lo1) * kTile + (pz - lo2);
-#pragma unroll
-    for (int pass = 0; pass < 2; ++pass) {
-      const int ox = 2 * pass + oxl;
-      if (!((mx >> ox) & 1)) continue;
-      int px = ux - ox;
-      px += px < 0 ? g.K0 : 0;
-      atomicAdd(&sq[(px - lo0) * kTile * kTile + base],
-                __float2int_rn(sw[a][ox] * wyz * kGridScale));
+      __syncwarp();
+      n_list = 0;
     }
   }
   __syncthreads();
@@ -992,14 +986,15 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
     k_pme_scatter<<<ceil_div(n, 256), 256, 0, st>>>(
         n, p.d_atom_tile, p.d_atom_slot, p.d_tile_start, p.d_frq, p.d_upk, p.d_binned,
         p.d_binned_u, p.d_tile_count, p.ntiles);
+    const int sblocks = p.ntiles;  // one block per tile
     if (batch)
-      k_pme_spread<true><<<p.ntiles, 256, 0, st>>>(g, p.d_tile_start, p.d_binned,
-                                                   p.d_binned_u, p.d_src[0], p.d_src[1],
-                                                   p.d_src[2], p.d_Q, p.bv);
+      k_pme_spread<true><<<sblocks, 32 * kSpreadWarps, 0, st>>>(
+          g, p.d_tile_start, p.d_binned, p.d_binned_u, p.d_src[0], p.d_src[1], p.d_src[2],
+          p.d_Q, p.ntiles, p.bv);
     else
-      k_pme_spread<false><<<p.ntiles, 256, 0, st>>>(g, p.d_tile_start, p.d_binned,
-                                                    p.d_binned_u, p.d_src[0], p.d_src[1],
-                                                    p.d_src[2], p.d_Q, p.bv);
+      k_pme_spread<false><<<sblocks, 32 * kSpreadWarps, 0, st>>>(
+          g, p.d_tile_start, p.d_binned, p.d_binned_u, p.d_src[0], p.d_src[1], p.d_src[2],
+          p.d_Q, p.ntiles, p.bv);
   } else {
     if (batch) return fail(kNotSupported, "PME batch: fixed-point accumulation only");
     SNB_CUDA_TRY(cudaMemsetAsync(p.d_Q, 0, sizeof(float) * p.nall, st));
