@@ -130,6 +130,11 @@ struct snb_engine {
   int pair_unroll = 4;
   int pair_blocks_per_sm = 0;
   cudaStream_t side = nullptr;  // captures the conditional rebuild body
+  // second branch of a step: excluded correction, bonded terms and PME run
+  // on `branch` while the pair kernel runs on the step's stream; both add
+  // into the same fixed-point accumulator (integer adds commute)
+  cudaStream_t branch = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int body_kernels = 0;         // kernel nodes inside the rebuild body
   // recovery snapshot for neighbor-list overflow
   float* d_snap_crd = nullptr;
@@ -926,6 +931,9 @@ static int engine_finish_create(snb_engine* e, int n, int n_types, const int* h_
   SNB_CUDA_TRY(cudaMalloc(&e->d_snap_crd, sizeof(float) * 3 * n));
   SNB_CUDA_TRY(cudaMalloc(&e->d_snap_vel, sizeof(float) * 3 * n));
   SNB_CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+  SNB_CUDA_TRY(cudaStreamCreateWithFlags(&e->branch, cudaStreamNonBlocking));
+  SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+  SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
   return kOk;
 }
 
@@ -1108,9 +1116,19 @@ static int capture_conditional_rebuild(snb_engine* e, const float* crd, cudaStre
 // nonbonded forces of one step into e->acc (sorted frame), no unpack.
 // in_graph: called while capturing the replayed step (conditional rebuild,
 // refresh check done by the previous step's leap-frog).
+static int engine_bonded(snb_engine* e, const float* crd, cudaStream_t st) {
+  return launch_bonded(e->nb, e->d_ba, e->d_bb, e->d_bk, e->d_br0, e->na, e->d_aa, e->d_ab,
+                       e->d_ac, e->d_ak, e->d_at0, reinterpret_cast<const float3*>(crd),
+                       e->cell, e->rcell, e->nl.d_inv_perm, e->acc, nullptr, false, st,
+                       e->bv);
+}
+
+// with_bonded: also the water bonds and angles (MD steps).  Outside the
+// per-phase profiling pass the excluded correction, the bonded terms and the
+// PME chain run on a second stream, concurrently with the pair kernel.
 static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
                          bool virial, bool forced_nl, cudaStream_t st,
-                         bool in_graph = false) {
+                         bool in_graph = false, bool with_bonded = false) {
   prof_mark(e, 0, st);
   int rc;
   if (in_graph) {
@@ -1130,6 +1148,22 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
                      e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st);
   if (rc) return rc;
   prof_mark(e, 2, st);
+  const bool fork = !e->prof_on;
+  cudaStream_t sb = fork ? e->branch : st;
+  if (fork) {
+    SNB_CUDA_TRY(cudaEventRecord(e->ev_fork, st));
+    SNB_CUDA_TRY(cudaStreamWaitEvent(sb, e->ev_fork, 0));
+    if (with_bonded && (rc = engine_bonded(e, crd, sb))) return rc;
+    if (e->pme.excluded &&
+        (rc = launch_excluded(e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
+                              e->cell, e->rcell, e->pme.beta, e->d_excl_start,
+                              e->d_excl_list, e->d_excl_numbers, e->nl.d_inv_perm, e->acc,
+                              e->accum, energy, virial, sb, e->bv)))
+      return rc;
+    if (do_pme && (rc = pme_after_bin(e->pme, e->n, e->acc, e->accum, energy, virial, sb)))
+      return rc;
+    SNB_CUDA_TRY(cudaEventRecord(e->ev_join, sb));
+  }
   PairArgs a;
   a.n = e->n;
   a.pos = e->d_pos;
@@ -1151,6 +1185,10 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   a.blocks_per_sm = e->pair_blocks_per_sm;
   rc = launch_pair(a, e->acc, e->accum, energy, virial, true, st);
   if (rc) return rc;
+  if (fork) {
+    SNB_CUDA_TRY(cudaStreamWaitEvent(st, e->ev_join, 0));
+    return kOk;
+  }
   prof_mark(e, 3, st);
   if (e->pme.excluded) {
     rc = launch_excluded(e->n, reinterpret_cast<const float3*>(crd), e->d_charge, e->cell,
@@ -1165,6 +1203,8 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
     if (rc) return rc;
   }
   prof_mark(e, 5, st);
+  if (with_bonded && (rc = engine_bonded(e, crd, st))) return rc;
+  prof_mark(e, 6, st);
   return kOk;
 }
 
@@ -1237,14 +1277,8 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
                           bool in_graph = false) {
   if (e->accum != kAccumFixed)
     return fail(kNotSupported, "md steps need the fixed-point accumulation");
-  int rc = engine_forces(e, crd, step, false, false, forced_nl, st, in_graph);
+  int rc = engine_forces(e, crd, step, false, false, forced_nl, st, in_graph, true);
   if (rc) return rc;
-  rc = launch_bonded(e->nb, e->d_ba, e->d_bb, e->d_bk, e->d_br0, e->na, e->d_aa, e->d_ab,
-                     e->d_ac, e->d_ak, e->d_at0, reinterpret_cast<const float3*>(crd),
-                     e->cell, e->rcell, e->nl.d_inv_perm, e->acc, nullptr, false, st,
-                     e->bv);
-  if (rc) return rc;
-  prof_mark(e, 6, st);
   // the next step's refresh check rides on the coordinate update
   const bool check = e->opt.nl_refresh_interval <= 0;
   const float permit = e->opt.skin * e->opt.nl_skin_permit;
@@ -1557,6 +1591,9 @@ extern "C" int snb_engine_destroy(snb_engine* e) {
   for (int k = 0; k < 8; ++k)
     if (e->prof_ev[k]) cudaEventDestroy(e->prof_ev[k]);
   if (e->side) cudaStreamDestroy(e->side);
+  if (e->branch) cudaStreamDestroy(e->branch);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_join) cudaEventDestroy(e->ev_join);
   nl_free(e->nl);
   pme_free(e->pme);
   acc_free(e->acc);
