@@ -931,7 +931,12 @@ static int engine_finish_create(snb_engine* e, int n, int n_types, const int* h_
   SNB_CUDA_TRY(cudaMalloc(&e->d_snap_crd, sizeof(float) * 3 * n));
   SNB_CUDA_TRY(cudaMalloc(&e->d_snap_vel, sizeof(float) * 3 * n));
   SNB_CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
-  SNB_CUDA_TRY(cudaStreamCreateWithFlags(&e->branch, cudaStreamNonBlocking));
+  {
+    // the branch's short kernels take SMs ahead of the persistent pair kernel
+    int lo = 0, hi = 0;
+    SNB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    SNB_CUDA_TRY(cudaStreamCreateWithPriority(&e->branch, cudaStreamNonBlocking, hi));
+  }
   SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
   SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
   return kOk;
@@ -1417,7 +1422,8 @@ extern "C" int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
 
 // Times `steps` stream-launched steps from the same starting coordinates for
 // each candidate launch shape and keeps the fastest: the pair kernel's scan
-// unroll (2, 4, 8) and blocks per SM (occupancy maximum, 2, 3), the pair
+// unroll (2, 4, 8) and blocks per SM (occupancy maximum, 2, 3) by the whole
+// step (the PME branch shares the SMs with it), the pair
 // search's blocks per SM (4, 8, 16; a rebuild is forced every step), and the
 // gather's threads per block (128, 256, 512).  crd / vel are restored.
 extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
@@ -1435,22 +1441,32 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
   SNB_CUDA_TRY(cudaMemcpyAsync(v0, vel, bytes, cudaMemcpyDeviceToDevice, st));
   for (int k = 0; k < 8; ++k)
     if (!e->prof_ev[k]) SNB_CUDA_TRY(cudaEventCreate(&e->prof_ev[k]));
-  // mean ms of phase `ph` (between prof_ev[ph] and prof_ev[ph + 1]) over the
-  // steps, from the saved coordinates; force_nl: rebuild every step
+  // mean ms over the steps, from the saved coordinates, of phase `ph`
+  // (between prof_ev[ph] and prof_ev[ph + 1], phases run one after another),
+  // or with ph < 0 of the whole step as the MD loop runs it (branches
+  // concurrent); force_nl: rebuild every step
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  SNB_CUDA_TRY(cudaEventCreate(&t0));
+  SNB_CUDA_TRY(cudaEventCreate(&t1));
   auto measure = [&](int ph, bool force_nl, double* ms) -> int {
     SNB_CUDA_TRY(cudaMemcpyAsync(crd, c0, bytes, cudaMemcpyDeviceToDevice, st));
     SNB_CUDA_TRY(cudaMemcpyAsync(vel, v0, bytes, cudaMemcpyDeviceToDevice, st));
     double acc = 0.0;
-    e->prof_on = true;
+    e->prof_on = ph >= 0;
     for (int s = -1; s < steps; ++s) {  // s = -1: untimed warm-up step
+      SNB_CUDA_TRY(cudaEventRecord(t0, st));
       int rc = engine_md_step(e, crd, vel, invm, dt, 1 + s, force_nl || s < 0, st);
       if (rc) {
         e->prof_on = false;
         return rc;
       }
-      SNB_CUDA_TRY(cudaEventSynchronize(e->prof_ev[7]));
+      SNB_CUDA_TRY(cudaEventRecord(t1, st));
+      SNB_CUDA_TRY(cudaEventSynchronize(t1));
       float m = 0.f;
-      SNB_CUDA_TRY(cudaEventElapsedTime(&m, e->prof_ev[ph], e->prof_ev[ph + 1]));
+      if (ph >= 0)
+        SNB_CUDA_TRY(cudaEventElapsedTime(&m, e->prof_ev[ph], e->prof_ev[ph + 1]));
+      else
+        SNB_CUDA_TRY(cudaEventElapsedTime(&m, t0, t1));
       if (s >= 0) acc += m;
     }
     e->prof_on = false;
@@ -1464,7 +1480,7 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
     for (int b : {0, 2, 3}) {
       e->pair_unroll = u;
       e->pair_blocks_per_sm = b;
-      if ((rc = measure(2, false, &ms))) break;
+      if ((rc = measure(-1, false, &ms))) break;  // the step, PME branch alongside
       if (ms < best) {
         best = ms;
         bu = u;
@@ -1502,6 +1518,8 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
   cudaStreamSynchronize(st);
   cudaFree(c0);
   cudaFree(v0);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
   if (rc) return rc;
   e->steps_done = 0;  // the next step rebuilds the list for the restored frame
   if (e->graph_exec) {  // recapture with the chosen shapes
