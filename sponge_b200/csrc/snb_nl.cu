@@ -188,6 +188,7 @@ struct SearchArgs {
   int Nx, Ny, Nz;
   Cell cell, rcell;
   float rl2;
+  float rl2_lo, rl2_hi;     // rl2 (1 -+ 2e-5): outside, the fast |dr|^2 decides
   bool trim;                // cell offsets are unique (>= 5 cells per axis)
   float reach2;             // (rl + margin)^2 for trimming runs
   float wx, wy, iwz;        // cell widths x, y and 1/width z
@@ -264,6 +265,8 @@ k_pair_search(SearchArgs a) {
       n_ex = 0;
     }
   }
+  // the first two partners in every lane (a water atom has two)
+  const int ex0 = __shfl_sync(0xffffffffu, ex, 0), ex1 = __shfl_sync(0xffffffffu, ex, 1);
   // position of i inside its cell, in cell widths (the binning's arithmetic)
   float fx = 0.f, fy = 0.f, fz = 0.f;
   if (trim) {
@@ -302,10 +305,24 @@ k_pair_search(SearchArgs a) {
       const int j = base + lane;
       bool hit = false;
       int gj = -1;
+      bool unsure = false;
+      float4 pj4 = make_float4(0.f, 0.f, 0.f, 0.f);
       if (j < hi) {
-        const float4 pj4 = a.pos[j];
+        pj4 = a.pos[j];
         gj = __float_as_int(pj4.w);
-        // dr = crd[lower id] - crd[higher id], as the reference forms it
+        // fast |dr|^2 (contracted, FMA-pipe min image) first: it differs from
+        // the exact one by far less than the band, so outside the band it
+        // decides the criterion alone
+        const float ex_ = min_image_axis(pj4.x - pi4.x, cell.a11, rcell.a11);
+        const float ey_ = min_image_axis(pj4.y - pi4.y, cell.a22, rcell.a22);
+        const float ez_ = min_image_axis(pj4.z - pi4.z, cell.a33, rcell.a33);
+        const float r2f = ex_ * ex_ + ey_ * ey_ + ez_ * ez_;
+        hit = r2f < a.rl2_lo;
+        unsure = !hit && r2f <= a.rl2_hi;
+      }
+      if (__any_sync(0xffffffffu, unsure) && unsure) {
+        // the band: the exact criterion, dr = crd[lower id] - crd[higher id]
+        // as the reference forms it, no contraction
         float dx = __fsub_rn(pi4.x, pj4.x);
         float dy = __fsub_rn(pi4.y, pj4.y);
         float dz = __fsub_rn(pi4.z, pj4.z);
@@ -317,7 +334,8 @@ k_pair_search(SearchArgs a) {
         const float3 d = min_image_exact_rect(dx, dy, dz, cell, rcell);
         hit = norm2_exact(d) < a.rl2;
       }
-      for (int k = 0; k < n_ex; ++k)  // warp-uniform
+      if (n_ex > 0 && (gj == ex0 || gj == ex1)) hit = false;
+      for (int k = 2; k < n_ex; ++k)  // warp-uniform
         if (__shfl_sync(0xffffffffu, ex, k) == gj) hit = false;
       if (hit && ex_lists)
         hit = !excluded_pair(min(gi, gj), max(gi, gj), a.excl_start, a.excl_list,
@@ -757,6 +775,8 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   sa.cell = nl.cell;
   sa.rcell = nl.rcell;
   sa.rl2 = nl.rl2;
+  sa.rl2_lo = nl.rl2 * (1.0f - 2e-5f);
+  sa.rl2_hi = nl.rl2 * (1.0f + 2e-5f);
   sa.trim = nl.trim;
   sa.reach2 = nl.reach2;
   sa.wx = nl.wx;
