@@ -278,36 +278,68 @@ k_pair_search(SearchArgs a) {
     fy = y / cell.a22 * Ny - (float)cy;
     fz = z / cell.a33 * Nz - (float)cz;
   }
-  // range list: own cell after i, then the owned runs
-  for (int r = -1; r < nr; ++r) {
-    int lo, hi;
+  // Range list: the own cell after i, then the owned runs, 32 ranges at a
+  // time.  Lane r works out range r0 + r (its trimmed slice of the sorted
+  // array); a prefix sum over the lanes lays the slices end to end, and the
+  // candidates are taken 32 at a time across slice boundaries.
+  const unsigned lt = (1u << lane) - 1u;
+  for (int r0 = -1; r0 < nr; r0 += 32) {
+    const int r = r0 + lane;
+    int lo = 0, len = 0;
     if (r < 0) {
       lo = i + 1;
-      hi = a.cell_start[c + 1];
-    } else {
+      len = a.cell_start[c + 1] - lo;
+    } else if (r < nr) {
       int2 rr = a.runs[(size_t)c * a.max_runs + r];
+      bool keep = true;
       if (trim) {
         const char4 g = a.geom[(size_t)c * a.max_runs + r];
         const float gx = cell_gap(g.x, fx) * wx, gy = cell_gap(g.y, fy) * wy;
         const float s2 = a.reach2 - gx * gx - gy * gy;
-        if (s2 < 0.f) continue;
-        const float s = sqrtf(s2) * iwz;
-        const int zmax = (int)floorf(fz + s), zmin = (int)ceilf(fz - 1.f - s);
-        const int z0 = max((int)g.z, zmin), z1 = min((int)g.w, zmax);
-        if (z0 > z1) continue;
-        rr.x += z0 - g.z;
-        rr.y -= g.w - z1;
+        keep = s2 >= 0.f;
+        if (keep) {
+          const float s = sqrtf(s2) * iwz;
+          const int zmax = (int)floorf(fz + s), zmin = (int)ceilf(fz - 1.f - s);
+          const int z0 = max((int)g.z, zmin), z1 = min((int)g.w, zmax);
+          keep = z0 <= z1;
+          rr.x += z0 - g.z;
+          rr.y -= g.w - z1;
+        }
       }
-      lo = a.cell_start[rr.x];
-      hi = a.cell_start[rr.y + 1];
+      if (keep) {
+        lo = a.cell_start[rr.x];
+        len = a.cell_start[rr.y + 1] - lo;
+      }
     }
-    for (int base = lo; base < hi; base += 32) {
-      const int j = base + lane;
+    int incl = len;  // inclusive prefix of the slice lengths
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - len;
+    const int nq = min(32, nr - r0);  // ranges in this chunk
+    int cursor = 0;                   // first slice not yet used up
+    for (int base = 0; base < total; base += 32) {
+      // candidate of flat index base + lane: its slice among those that meet
+      // [base, base + 32)
+      const int fi = base + lane;
+      int j = -1;
+      for (int q = cursor; q < nq; ++q) {  // warp-uniform
+        const int eq = __shfl_sync(0xffffffffu, excl, q);
+        const int lq = __shfl_sync(0xffffffffu, len, q);
+        const int oq = __shfl_sync(0xffffffffu, lo, q);
+        if (eq >= base + 32) break;
+        if (fi >= eq && fi < eq + lq) j = oq + (fi - eq);
+        if (eq + lq > base + 32) break;  // goes on into the next batch
+        cursor = q + 1;
+      }
       bool hit = false;
       int gj = -1;
       bool unsure = false;
       float4 pj4 = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (j < hi) {
+      if (j >= 0) {
         pj4 = a.pos[j];
         gj = __float_as_int(pj4.w);
         // fast |dr|^2 (contracted, FMA-pipe min image) first: it differs from
@@ -342,7 +374,7 @@ k_pair_search(SearchArgs a) {
                              a.excl_numbers);
       const unsigned m = __ballot_sync(0xffffffffu, hit);
       if (hit) {
-        const int slot = count + __popc(m & ((1u << lane) - 1u));
+        const int slot = count + __popc(m & lt);
         if (slot < a.row_cap) out_row[slot] = j;
       }
       count += __popc(m);
