@@ -5,6 +5,9 @@
   excluded-pair correction and long-range LJ correction.
 * ``ReferenceCPU``: the reference's own CPU modules compiled from its sources
   (``oracle/_ref/libsponge_ref*.so``, built by ``make -C oracle ref``).
+* ``ReferenceGPU``: the reference's own GPU modules (FP32, float atomics)
+  compiled from its sources as CUDA (``oracle/_ref/libsponge_ref_gpu.so``,
+  ``make -C oracle refgpu``); one box per process.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
 this module.  The product never does.
@@ -21,6 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libsnb_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libsponge_ref.so")
 REF_EXACT_SO = os.path.join(HERE, "_ref", "libsponge_ref_exact.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libsponge_ref_gpu.so")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -32,7 +36,8 @@ def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
 
 
-def build_oracle(ref_root: str | None = None, with_reference: bool = True) -> None:
+def build_oracle(ref_root: str | None = None, with_reference: bool = True,
+                 with_gpu: bool = True) -> None:
     """Build the checkers (``make -C oracle [ref]``).  The reference part only
     builds where its sources exist."""
     import subprocess
@@ -40,6 +45,8 @@ def build_oracle(ref_root: str | None = None, with_reference: bool = True) -> No
     ref_root = ref_root or "/root/reference/SPONGE"
     if with_reference and os.path.isdir(ref_root):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"])
+        if with_gpu:
+            subprocess.check_call(["make", "-s", "-C", HERE, "refgpu", f"REF={ref_root}"])
 
 
 class Oracle:
@@ -410,3 +417,119 @@ class ReferenceCPU:
             raise RuntimeError("reference soft-core tail failed")
         return dict(virial=vir, potential=float(pot[0]), factor=float(fac[0]),
                     factor_ti=float(fac[1]))
+
+
+class ReferenceGPU:
+    """The reference's own GPU modules (neighbor list, LJ + direct Coulomb,
+    PME with the excluded correction, bonds, angles) driven in main.cpp's
+    order by ``ref_build/ref_harness_gpu.cu``.  FP32 with float atomics on
+    the legacy default stream.  The library holds one box per process."""
+
+    def __init__(self):
+        if not os.path.exists(REF_GPU_SO):
+            raise FileNotFoundError(
+                f"{REF_GPU_SO} missing: build it with `make -C oracle refgpu` where "
+                "the reference sources are present")
+        L = ctypes.CDLL(REF_GPU_SO)
+        self.lib = L
+        L.refg_last_error.restype = ctypes.c_char_p
+        L.refg_init.restype = ctypes.c_int
+        L.refg_init.argtypes = [
+            ctypes.c_int, _f32p, _f32p, _i32p, ctypes.c_int, _f32p, _f32p,
+            _i32p, _i32p, _i32p, ctypes.c_int, _f32p, ctypes.c_float,
+            ctypes.c_float, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
+        L.refg_grid.argtypes = [_i32p]
+        L.refg_set_bonded.restype = ctypes.c_int
+        L.refg_set_bonded.argtypes = [ctypes.c_int, _i32p, _i32p, _f32p, _f32p,
+                                      ctypes.c_int, _i32p, _i32p, _i32p, _f32p, _f32p]
+        L.refg_set_state.restype = ctypes.c_int
+        L.refg_set_state.argtypes = [_f32p, ctypes.c_void_p, ctypes.c_void_p]
+        L.refg_get_state.restype = ctypes.c_int
+        L.refg_get_state.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.refg_force.restype = ctypes.c_int
+        L.refg_force.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                 ctypes.c_void_p]
+        L.refg_md_steps.restype = ctypes.c_int
+        L.refg_md_steps.argtypes = [ctypes.c_int, ctypes.c_float,
+                                    ctypes.POINTER(ctypes.c_float)]
+        L.refg_pair_count.restype = ctypes.c_int
+        L.refg_pair_count.argtypes = [ctypes.POINTER(ctypes.c_longlong),
+                                      ctypes.POINTER(ctypes.c_int)]
+        self.n = 0
+
+    def _ok(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"reference GPU {what} failed: "
+                               f"{self.lib.refg_last_error().decode()}")
+
+    def init(self, s, cutoff, skin, commands: dict | None = None):
+        cmd = ";".join(f"{k}={v}" for k, v in (commands or {}).items())
+        beta = ctypes.c_float(0)
+        el = s.excl_list if len(s.excl_list) else np.zeros(1, np.int32)
+        self._ok(self.lib.refg_init(
+            s.n, _c(s.crd, np.float32).reshape(-1), _c(s.charge, np.float32),
+            _c(s.lj_type, np.int32), s.n_types, _c(s.lj_A, np.float32),
+            _c(s.lj_B, np.float32), _c(s.excl_start, np.int32),
+            _c(s.excl_numbers, np.int32), _c(el, np.int32), int(len(s.excl_list)),
+            s.cell(), cutoff, skin, cmd.encode(), ctypes.byref(beta)), "init")
+        self.n = s.n
+        self.beta = beta.value
+        g = np.zeros(3, np.int32)
+        self.lib.refg_grid(g)
+        self.grid = tuple(int(x) for x in g)
+        return self.beta
+
+    def set_bonded(self, bonds, bond_k, bond_r0, angles, angle_k, angle_t0):
+        b = np.ascontiguousarray(bonds, np.int32).reshape(-1, 2)
+        a = np.ascontiguousarray(angles, np.int32).reshape(-1, 3)
+        nb, na = len(b), len(a)
+        self._keep = [np.ascontiguousarray(x) for x in (
+            b[:, 0], b[:, 1], a[:, 0], a[:, 1], a[:, 2])]
+        self._ok(self.lib.refg_set_bonded(
+            nb, self._keep[0], self._keep[1], np.full(nb, bond_k, np.float32),
+            np.full(nb, bond_r0, np.float32), na, self._keep[2], self._keep[3],
+            self._keep[4], np.full(na, angle_k, np.float32),
+            np.full(na, angle_t0, np.float32)), "set_bonded")
+
+    def set_state(self, crd, vel=None, inv_mass=None):
+        crd = _c(crd, np.float32).reshape(-1)
+        v = None if vel is None else _c(vel, np.float32).reshape(-1)
+        m = None if inv_mass is None else _c(inv_mass, np.float32)
+        self._ok(self.lib.refg_set_state(
+            crd, None if v is None else v.ctypes.data,
+            None if m is None else m.ctypes.data), "set_state")
+
+    def get_state(self):
+        crd = np.zeros(3 * self.n, np.float32)
+        vel = np.zeros(3 * self.n, np.float32)
+        self._ok(self.lib.refg_get_state(crd.ctypes.data, vel.ctypes.data), "get_state")
+        return crd.reshape(-1, 3), vel.reshape(-1, 3)
+
+    def force(self, forced=True, need_energy=True, need_virial=True):
+        """Nonbonded forces, per-atom energies (LJ + direct + excluded),
+        the box-level potential (reciprocal + self + tail) and the summed
+        virial of one evaluation on the current coordinates."""
+        n = self.n
+        frc = np.zeros(3 * n, np.float32)
+        ae = np.zeros(n, np.float32)
+        pot = np.zeros(1, np.float32)
+        vir = np.zeros(6, np.float32)
+        self._ok(self.lib.refg_force(int(forced), int(need_energy), int(need_virial),
+                                     frc.ctypes.data, ae.ctypes.data, pot.ctypes.data,
+                                     vir.ctypes.data), "force")
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, potential=float(pot[0]),
+                    virial=vir)
+
+    def md_steps(self, steps, dt):
+        """NVE steps; returns their device time in ms."""
+        ms = ctypes.c_float(0)
+        self._ok(self.lib.refg_md_steps(int(steps), float(dt), ctypes.byref(ms)),
+                 "md_steps")
+        return float(ms.value)
+
+    def pair_count(self):
+        c = ctypes.c_longlong(0)
+        ov = ctypes.c_int(0)
+        self._ok(self.lib.refg_pair_count(ctypes.byref(c), ctypes.byref(ov)), "pair_count")
+        return int(c.value), int(ov.value)
