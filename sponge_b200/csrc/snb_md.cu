@@ -112,24 +112,30 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
                             float3* __restrict__ crd, float3* __restrict__ vel,
                             const float* __restrict__ inv_mass, float dt,
                             const float3* __restrict__ old_crd, Cell cell, Cell rcell,
-                            float permit2, int* flags, BatchView bv) {
+                            float permit2, int* __restrict__ flags, BatchView bv) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  int s = map[i];
-  const int N = acc.n;
-  float fx = (float)((double)acc.d_f[s] * kForceScaleInv);
-  float fy = (float)((double)acc.d_f[N + s] * kForceScaleInv);
-  float fz = (float)((double)acc.d_f[2 * N + s] * kForceScaleInv);
-  acc.d_f[s] = 0;
-  acc.d_f[N + s] = 0;
-  acc.d_f[2 * N + s] = 0;
-  float im = inv_mass[i];
+  // every load is issued before the first store: the force reads wait on the
+  // permutation, the rest do not
+  const int s = map[i];
+  const float im = inv_mass[i];
   float3 v = vel[i];
+  float3 r = crd[i];
+  float3 r_old = make_float3(0.f, 0.f, 0.f);
+  if (old_crd) r_old = old_crd[i];
+  const int N = acc.n;
+  long long* __restrict__ f = acc.d_f;
+  const long long fx_i = f[s], fy_i = f[N + s], fz_i = f[2 * N + s];
+  f[s] = 0;
+  f[N + s] = 0;
+  f[2 * N + s] = 0;
+  const float fx = (float)((double)fx_i * kForceScaleInv);
+  const float fy = (float)((double)fy_i * kForceScaleInv);
+  const float fz = (float)((double)fz_i * kForceScaleInv);
   v.x += dt * (im * fx);
   v.y += dt * (im * fy);
   v.z += dt * (im * fz);
   vel[i] = v;
-  float3 r = crd[i];
   r.x += dt * v.x;
   r.y += dt * v.y;
   r.z += dt * v.z;
@@ -140,7 +146,7 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
       cell = sg.cell;
       rcell = sg.rcell;
     }
-    float3 d = min_image_fast<false>(r, old_crd[i], cell, rcell);
+    float3 d = min_image_fast<false>(r, r_old, cell, rcell);
     bool moved = d.x * d.x + d.y * d.y + d.z * d.z > permit2;
     if (__any_sync(__activemask(), moved) && moved) atomicExch(&flags[0], 1);
   }

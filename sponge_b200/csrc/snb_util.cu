@@ -98,25 +98,29 @@ int scan_reserve(ScanScratch& s, int n) {
   return kOk;
 }
 
-// One block scans everything in chunks (short arrays: one launch instead of 3).
+// One block for short arrays (n <= 16 * blockDim.x): each thread takes a
+// contiguous chunk of up to 16 entries, so one block-wide scan covers all.
 __global__ void k_scan_single(const int* in, int* out, int n, int* total_out) {
   __shared__ int sh[32];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < n; base += blockDim.x) {
-    int i = base + threadIdx.x;
-    int v = i < n ? in[i] : 0;
-    int tot;
-    int ex = block_scan_exclusive(v, sh, &tot);
-    if (i < n) out[i] = ex + carry;
-    __syncthreads();
-    if (threadIdx.x == 0) carry += tot;
-    __syncthreads();
+  const int c = (n + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * c;
+  int v[16];
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    v[k] = (k < c && b + k < n) ? in[b + k] : 0;
+    sum += v[k];
+  }
+  int tot;
+  int ex = block_scan_exclusive(sum, sh, &tot);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    if (k < c && b + k < n) out[b + k] = ex;
+    ex += v[k];
   }
   if (threadIdx.x == 0) {
-    out[n] = carry;
-    if (total_out) *total_out = carry;
+    out[n] = tot;
+    if (total_out) *total_out = tot;
   }
 }
 
