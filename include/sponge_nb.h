@@ -318,6 +318,13 @@ int snb_engine_set_bonded(snb_engine* e, int bond_numbers, const int* h_bond_a,
                           const int* h_angle_a, const int* h_angle_b,
                           const int* h_angle_c, const float* h_angle_k,
                           const float* h_angle_theta0);
+/* Soft-core LJ in the engine (main.cpp:1460-1465 runs LJ_SOFT_CORE in place
+ * of the plain LJ module when it is initialised): the engine's pair step
+ * takes the end-state tables, types, perturbation mask and lambda / alpha /
+ * p / sigma of `soft` (created for the same atom count), and its tail
+ * correction.  `soft` must outlive the engine's use of it; NULL turns the
+ * plain LJ back on.  Single boxes, fixed-point accumulation. */
+int snb_engine_set_soft_core(snb_engine* e, snb_lj_soft* soft);
 int snb_engine_md_steps(snb_engine* e, float* crd, float* vel,
                         const float* inverse_mass, float dt, int first_step,
                         int steps, void* stream);

@@ -60,6 +60,7 @@ EXPORTED = [
     "snb_pme_excluded_force", "snb_pme_energies", "snb_pme_destroy",
     "snb_pme_excluded_force_noalloc",
     "snb_engine_create", "snb_batch_create", "snb_engine_force", "snb_engine_set_bonded",
+    "snb_engine_set_soft_core",
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_profile_steps",
     "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
     "snb_engine_destroy",
@@ -120,6 +121,7 @@ _SIGS = {
                               _P, _P, _P, _I, ctypes.POINTER(_P)]),
     "snb_engine_force": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
     "snb_engine_set_bonded": (_I, [_P, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
+    "snb_engine_set_soft_core": (_I, [_P, _P]),
     "snb_engine_md_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_md_steps_graph": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_profile_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P, _P]),

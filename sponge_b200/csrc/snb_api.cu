@@ -126,6 +126,8 @@ struct snb_engine {
   BatchView bv;
   double lrc_energy = 0.0;   // tail energy summed over the boxes
   double lrc_virial = 0.0;   // tail virial (diagonal) summed over the boxes
+  double lrc_energy_lj = 0.0, lrc_virial_lj = 0.0;  // the plain LJ module's
+  snb_lj_soft* soft = nullptr;  // soft-core pair terms in place of plain LJ
   // launch shapes picked by snb_engine_autotune
   int pair_unroll = 4;
   int pair_blocks_per_sm = 0;
@@ -885,6 +887,8 @@ static int engine_finish_create(snb_engine* e, int n, int n_types, const int* h_
     e->lrc_energy = p.long_range_factor / vol;
     e->lrc_virial = 2.0 * p.long_range_factor / vol;
   }
+  e->lrc_energy_lj = e->lrc_energy;
+  e->lrc_virial_lj = e->lrc_virial;
   SNB_CUDA_TRY(cudaMalloc(&p.d_A, sizeof(float) * p.n_pairs));
   SNB_CUDA_TRY(cudaMalloc(&p.d_B, sizeof(float) * p.n_pairs));
   SNB_CUDA_TRY(cudaMemcpy(p.d_A, h_A, sizeof(float) * p.n_pairs, cudaMemcpyHostToDevice));
@@ -1152,6 +1156,9 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
     rc = launch_pack(e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
                      e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st);
   if (rc) return rc;
+  if (e->soft)
+    k_pack_soft<<<ceil_div(e->n, 256), 256, 0, st>>>(e->n, e->nl.d_perm, e->soft->d_par_local,
+                                                    nullptr, e->soft->d_par_sorted, nullptr);
   prof_mark(e, 2, st);
   const bool fork = !e->prof_on;
   cudaStream_t sb = fork ? e->branch : st;
@@ -1188,7 +1195,36 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   a.bv = e->bv;
   a.unroll = e->pair_unroll;
   a.blocks_per_sm = e->pair_blocks_per_sm;
-  rc = launch_pair(a, e->acc, e->accum, energy, virial, true, st);
+  if (e->soft) {
+    SoftArgs sa;
+    sa.n = e->n;
+    sa.pos = e->d_pos;
+    sa.par = e->soft->d_par_sorted;
+    sa.dq = nullptr;
+    sa.global = e->nl.d_global;
+    sa.row_start = e->nl.d_row_start;
+    sa.row_count = e->nl.d_row_count;
+    sa.cols = e->nl.d_cols;
+    sa.nl_flags = e->nl.d_flags;
+    sa.AA = e->soft->d_AA;
+    sa.AB = e->soft->d_AB;
+    sa.BA = e->soft->d_BA;
+    sa.BB = e->soft->d_BB;
+    sa.n_types_A = e->soft->nA;
+    sa.n_types_B = e->soft->nB;
+    sa.cell = e->cell;
+    sa.rcell = e->rcell;
+    sa.cutoff2 = a.cutoff2;
+    sa.beta = a.beta;
+    sa.lambda = e->soft->lambda;
+    sa.alpha = e->soft->alpha;
+    sa.p = e->soft->p;
+    sa.sigma6 = e->soft->sigma6;
+    sa.sigma6_min = e->soft->sigma6_min;
+    rc = launch_soft_rows(sa, e->acc, energy, virial, st);
+  } else {
+    rc = launch_pair(a, e->acc, e->accum, energy, virial, true, st);
+  }
   if (rc) return rc;
   if (fork) {
     SNB_CUDA_TRY(cudaStreamWaitEvent(st, e->ev_join, 0));
@@ -1232,6 +1268,31 @@ extern "C" int snb_engine_force(snb_engine* e, const float* crd, float* frc, int
   return launch_unpack(e->n, e->nl.d_inv_perm, e->acc, e->accum,
                        reinterpret_cast<float3*>(frc), nullptr, nullptr, nullptr, nullptr,
                        en, vi, st);
+}
+
+extern "C" int snb_engine_set_soft_core(snb_engine* e, snb_lj_soft* soft) {
+  if (!e) return fail(kBadInput, "engine_set_soft_core: null handle");
+  if (soft) {
+    if (e->nsys > 0) return fail(kNotSupported, "engine_set_soft_core: batch engines");
+    if (e->accum != kAccumFixed || soft->accum != kAccumFixed)
+      return fail(kNotSupported, "engine_set_soft_core: fixed-point accumulation only");
+    if (soft->n != e->n) return fail(kBadInput, "engine_set_soft_core: atom count differs");
+  }
+  e->soft = soft;
+  if (soft) {
+    const double vol = (double)e->cell.a11 * e->cell.a22 * e->cell.a33;
+    e->lrc_energy = soft->lrc / vol;
+    e->lrc_virial = 2.0 * soft->lrc / vol;
+  } else {
+    e->lrc_energy = e->lrc_energy_lj;
+    e->lrc_virial = e->lrc_virial_lj;
+  }
+  if (e->graph_exec) {  // the captured step holds the previous pair kernel
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+  }
+  return kOk;
 }
 
 extern "C" int snb_engine_set_bonded(snb_engine* e, int nb, const int* ba, const int* bb,

@@ -245,6 +245,9 @@ struct SoftArgs {
 };
 int launch_soft(const SoftArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool dudl, long long* dudl_total, cudaStream_t st);
+// The engine's soft-core pair kernel (fixed point, rectangular box).
+int launch_soft_rows(const SoftArgs& a, Accumulators& acc, bool energy, bool virial,
+                     cudaStream_t st);
 
 // ----------------------------------------------------------------------------
 // Particle mesh Ewald (reciprocal part).

@@ -487,6 +487,216 @@ k_lj_soft(SoftArgs a, Accumulators acc, long long* dudl_total) {
   }
 }
 
+// Soft-core pair terms without dU/dlambda (the forms of k_lj_soft): force
+// over r, LJ and Coulomb energies.  alp_A = alpha lambda^p, alp_B = alpha
+// (1 - lambda)^p.
+__device__ __forceinline__ void soft_pair(const SoftArgs& a, float AA, float AB, float BA,
+                                          float BB, float r2, float qq, float alp_A,
+                                          float alp_B, float& fs, float& elj, float& ec) {
+  const float lam = a.lambda, lam_ = 1.0f - a.lambda;
+  const float r = sqrtf(r2);
+  if (BA * AA != 0.f || BA + AA == 0.f) {
+    const float ir2 = 1.0f / r2, ir6 = ir2 * ir2 * ir2;
+    fs = lam_ * (AB - AA * ir6) * ir6 * ir2 + lam * (BB - BA * ir6) * ir6 * ir2 -
+         coul_f(qq, a.beta, r);
+    elj = lam_ * lj_e(AA, AB, ir6) + lam * lj_e(BA, BB, ir6);
+    ec = coul_e(qq, a.beta, r);
+  } else {
+    const float sA = sc_sigma(AA, AB, a.sigma6, a.sigma6_min);
+    const float sB = sc_sigma(BA, BB, a.sigma6, a.sigma6_min);
+    const float r6 = r2 * r2 * r2;
+    const float rA = powf(r6 + alp_A * sA, 0.16666667f);
+    const float rB = powf(r6 + alp_B * sB, 0.16666667f);
+    const float r4 = r2 * r2;
+    const float iA2 = 1.0f / (rA * rA), iA6 = iA2 * iA2 * iA2;
+    const float iB2 = 1.0f / (rB * rB), iB6 = iB2 * iB2 * iB2;
+    const float flA = r4 * (AB - AA * iA6) * iA6 * iA6;
+    const float flB = r4 * (BB - BA * iB6) * iB6 * iB6;
+    const float bA = a.beta * rA, bB = a.beta * rB;
+    const float fcA =
+        qq * r4 * (expf(-bA * bA) * kTwoOverSqrtPi * a.beta + erfcf(bA) / rA) * iA6;
+    const float fcB =
+        qq * r4 * (expf(-bB * bB) * kTwoOverSqrtPi * a.beta + erfcf(bB) / rB) * iB6;
+    fs = lam_ * flA + lam * flB - (lam_ * fcA + lam * fcB);
+    ec = lam_ * coul_e(qq, a.beta, rA) + lam * coul_e(qq, a.beta, rB);
+    elj = lam_ * lj_e(AA, AB, iA6) + lam * lj_e(BA, BB, iB6);
+  }
+}
+
+// Soft-core LJ + direct Coulomb for the fused engine, in the two-phase row
+// scheme of k_lj_direct (scan to a shared hit list, then dense batches of
+// pair terms).  A pair whose end states carry the same LJ parameters
+// (A'_A == A'_B and B'_A == B'_B, as between unperturbed atoms) takes the
+// plain pair terms of lj_pair, to which the lambda mix of the two equal
+// forms reduces; the other pairs take soft_pair.  Energies and virial split
+// by global id as in k_lj_direct; no inter/intra split and no dU/dlambda
+// (the module's k_lj_soft provides those).
+template <int ACCUM, bool ENERGY, bool VIRIAL>
+__global__ void __launch_bounds__(256, 4)
+k_lj_soft_rows(SoftArgs a, Accumulators acc) {
+  constexpr int kScanU = 4;
+  extern __shared__ float sh_soft[];
+  __shared__ int hits_all[kWarps][kHitCap];
+  const int pA_n = a.n_types_A * (a.n_types_A + 1) / 2;
+  const int pB_n = a.n_types_B * (a.n_types_B + 1) / 2;
+  float* sAA = sh_soft;
+  float* sAB = sAA + pA_n;
+  float* sBA = sAB + pA_n;
+  float* sBB = sBA + pB_n;
+  for (int k = threadIdx.x; k < pA_n; k += blockDim.x) {
+    sAA[k] = a.AA[k];
+    sAB[k] = a.AB[k];
+  }
+  for (int k = threadIdx.x; k < pB_n; k += blockDim.x) {
+    sBA[k] = a.BA[k];
+    sBB[k] = a.BB[k];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  int* hits = hits_all[w];
+  if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
+  const float alp_A = a.alpha * powf(a.lambda, a.p);
+  const float alp_B = a.alpha * powf(1.0f - a.lambda, a.p);
+  const int per_block = (a.n + gridDim.x - 1) / gridDim.x;
+  const int i_begin = blockIdx.x * per_block;
+  const int i_end = min(a.n, i_begin + per_block);
+  const unsigned lt = (1u << lane) - 1u;
+  // the plain-path constants of lj_pair
+  PairArgs pa;
+  pa.beta = a.beta;
+  pa.global = a.global;
+  for (int i = i_begin + w; i < i_end; i += kWarps) {
+    const float4 pi = a.pos[i];
+    const float3 ri = make_float3(pi.x, pi.y, pi.z);
+    const int2 pri = a.par[i];
+    const int tAi = pri.x & 0xffff, tBi = pri.x >> 16;
+    const int gi = ENERGY || VIRIAL ? a.global[i] : 0;
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    float e_lj = 0.f, e_c = 0.f;
+    float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const int k0 = a.row_start[i], k1 = k0 + a.row_count[i];
+    for (int base = k0; base < k1;) {
+      int count = 0;
+      for (; base < k1 && count <= kHitCap - 32 * kScanU; base += 32 * kScanU) {
+        int jj[kScanU];
+#pragma unroll
+        for (int u = 0; u < kScanU; ++u) {
+          const int k = base + 32 * u + lane;
+          jj[u] = k < k1 ? a.cols[k] : -1;
+        }
+        float4 pp[kScanU];
+#pragma unroll
+        for (int u = 0; u < kScanU; ++u)
+          if (jj[u] >= 0) pp[u] = a.pos[jj[u]];
+#pragma unroll
+        for (int u = 0; u < kScanU; ++u) {
+          bool in = false;
+          if (jj[u] >= 0) {
+            const float3 dr = min_image_fast<true>(make_float3(pp[u].x, pp[u].y, pp[u].z),
+                                                   ri, a.cell, a.rcell);
+            in = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z < a.cutoff2;
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, in);
+          if (in) hits[count + __popc(m & lt)] = jj[u];
+          count += __popc(m);
+        }
+      }
+      __syncwarp();
+      for (int h = lane; h < count; h += 32) {
+        const int j = hits[h];
+        const float4 pj = a.pos[j];
+        const int2 prj = a.par[j];
+        const float3 dr = min_image_fast<true>(make_float3(pj.x, pj.y, pj.z), ri, a.cell,
+                                               a.rcell);
+        const int pA = lj_pair_index(tAi, prj.x & 0xffff);
+        const int pB = lj_pair_index(tBi, prj.x >> 16);
+        const float AA = sAA[pA], AB = sAB[pA], BA = sBA[pB], BB = sBB[pB];
+        if (AA == BA && AB == BB) {
+          // one table entry carries the pair's (equal) end-state parameters
+          lj_pair<ACCUM, ENERGY, VIRIAL>(pa, acc, sAA, sAB, tAi, pi.w, gi,
+                                         make_float4(dr.x, dr.y, dr.z, pj.w), j,
+                                         prj.x & 0xffff, fx, fy, fz, e_lj, e_c, vir);
+          continue;
+        }
+        const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+        float fs, elj, ec;
+        soft_pair(a, AA, AB, BA, BB, r2, pi.w * pj.w, alp_A, alp_B, fs, elj, ec);
+        const float gx = fs * dr.x, gy = fs * dr.y, gz = fs * dr.z;
+        fx += gx;
+        fy += gy;
+        fz += gz;
+        add_force<ACCUM>(acc, j, -gx, -gy, -gz);
+        if (ENERGY || VIRIAL) {
+          const bool own_i = gi < a.global[j];
+          if (ENERGY) {
+            if (own_i) {
+              e_lj += elj;
+              e_c += ec;
+            } else {
+              add_energy<ACCUM>(acc, j, elj + ec, elj, ec);
+            }
+          }
+          if (VIRIAL) {
+            float v[6];
+            v[0] = -(gx * dr.x);
+            v[1] = -(gx * dr.y + gy * dr.x);
+            v[2] = -(gy * dr.y);
+            v[3] = -(gx * dr.z + gz * dr.x);
+            v[4] = -(gy * dr.z + gz * dr.y);
+            v[5] = -(gz * dr.z);
+            if (own_i) {
+#pragma unroll
+              for (int c = 0; c < 6; ++c) vir[c] += v[c];
+            } else {
+              add_virial<ACCUM>(acc, j, v);
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+    fx = warp_sum(fx);
+    fy = warp_sum(fy);
+    fz = warp_sum(fz);
+    if (ENERGY) {
+      e_lj = warp_sum(e_lj);
+      e_c = warp_sum(e_c);
+    }
+    if (VIRIAL) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) vir[c] = warp_sum(vir[c]);
+    }
+    if (lane == 0) {
+      add_force<ACCUM>(acc, i, fx, fy, fz);
+      if (ENERGY) add_energy<ACCUM>(acc, i, e_lj + e_c, e_lj, e_c);
+      if (VIRIAL) add_virial<ACCUM>(acc, i, vir);
+    }
+  }
+}
+
+int launch_soft_rows(const SoftArgs& a, Accumulators& acc, bool energy, bool virial,
+                     cudaStream_t st) {
+  if (a.n <= 0) return kOk;
+  const size_t smem = sizeof(float) * (a.n_types_A * (a.n_types_A + 1) +
+                                       a.n_types_B * (a.n_types_B + 1));
+  using Kern = void (*)(SoftArgs, Accumulators);
+  Kern kern = energy && virial ? k_lj_soft_rows<kAccumFixed, true, true>
+              : energy         ? k_lj_soft_rows<kAccumFixed, true, false>
+              : virial         ? k_lj_soft_rows<kAccumFixed, false, true>
+                               : k_lj_soft_rows<kAccumFixed, false, false>;
+  if (smem > 48 * 1024) return fail(kNotSupported, "soft-core rows: type tables too large");
+  static int sms = 0;
+  if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, smem);
+  per_sm = std::max(per_sm, 1);
+  const int blocks = std::max(1, std::min(sms * per_sm, ceil_div(a.n, kWarps)));
+  kern<<<blocks, 32 * kWarps, smem, st>>>(a, acc);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
 template <int ACCUM>
 static void launch_soft2(const SoftArgs& a, Accumulators& acc, bool energy, bool virial,
                          bool dudl, long long* dt, cudaStream_t st) {
