@@ -140,13 +140,24 @@ def _orient_waters(rng, o_pos, kind, box, h_clash=1.6, max_rounds=200):
                                           _random_rotations(rng, n), h_local)
     water = kind == 0
     mol = np.repeat(np.arange(n), 3)
+    is_h = np.tile([False, True, True], n)
+    live = np.repeat(water, 3) | (np.tile([True, False, False], n))
+    idx = np.nonzero(live)[0]
+    redo = None
     for _ in range(max_rounds):
         pts = np.concatenate([o_pos[:, None, :], h_pos], 1).reshape(-1, 3)
-        is_h = np.tile([False, True, True], n)
-        live = np.repeat(water, 3) | (np.tile([True, False, False], n))
-        idx = np.nonzero(live)[0]
         tree = cKDTree(np.mod(pts[idx], box), boxsize=box)
-        pairs = tree.query_pairs(h_clash, output_type="ndarray")
+        if redo is None:
+            pairs = tree.query_pairs(h_clash, output_type="ndarray")
+        else:
+            # only molecules redrawn last round can clash now: every clashing
+            # pair has a redrawn member (the water owning the H), and pairs
+            # between unchanged molecules were clash-free before
+            moved = np.nonzero(np.isin(mol[idx], redo))[0]
+            near = tree.query_ball_point(tree.data[moved], h_clash)
+            pairs = np.array(sorted({(min(p, q), max(p, q))
+                                     for p, row in zip(moved, near) for q in row if q != p}),
+                             dtype=np.int64).reshape(-1, 2)
         if len(pairs) == 0:
             break
         a, b = idx[pairs[:, 0]], idx[pairs[:, 1]]
@@ -295,15 +306,16 @@ def soft_core_box(n_waters: int, n_solute: int = 64, seed: int = 0,
             sites.append(p)
     sites = np.asarray(sites) + centre
     # drop whole molecules near the cluster (water = O followed by its two H)
-    d = s.crd[:, None, :].astype(np.float64) - sites[None]
+    # only atoms within radius + clearance of the centre can be near a site
+    dc = s.crd.astype(np.float64) - centre
+    dc -= np.round(dc / s.box) * s.box
+    cand = np.nonzero(np.linalg.norm(dc, axis=1) < radius + clearance)[0]
+    d = s.crd[cand][:, None, :].astype(np.float64) - sites[None]
     d -= np.round(d / s.box) * s.box
-    near = (np.linalg.norm(d, axis=2) < clearance).any(1)
-    mol = np.zeros(s.n, np.int64)
-    m = -1
-    for i in range(s.n):
-        if s.lj_type[i] != 1:
-            m += 1
-        mol[i] = m
+    near = np.zeros(s.n, bool)
+    near[cand] = (np.linalg.norm(d, axis=2) < clearance).any(1)
+    mol = np.cumsum(s.lj_type != 1) - 1  # a new molecule at every non-H atom
+    m = int(mol[-1])
     drop_mol = np.zeros(m + 1, bool)
     drop_mol[mol[near]] = True
     w = _subset(s, ~drop_mol[mol])
