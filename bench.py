@@ -63,9 +63,14 @@ def parse():
     p.add_argument("--batch-systems", type=int, default=256,
                    help="boxes in the batched measurement (0: skip)")
     p.add_argument("--batch-steps", type=int, default=200)
-    p.add_argument("--drift-steps", type=int, default=2000,
+    p.add_argument("--drift-steps", type=int, default=10000,
                    help="NVE steps after the timed region over which the total-energy "
                         "drift is fitted (0: skip)")
+    p.add_argument("--no-small-box", action="store_true",
+                   help="skip the 9,000-atom box")
+    p.add_argument("--soft-core-waters", type=int, default=333333,
+                   help="waters of the soft-core box (about 1M atoms; 0: skip)")
+    p.add_argument("--soft-core-equilibrate", type=int, default=1000)
     return p.parse_args()
 
 
@@ -467,6 +472,173 @@ def run_batch(args, lib, world, rank, dist):
                         "fixed-point accumulation"}
 
 
+def make_engine(lib, s, cutoff):
+    """Single-box engine over System `s` with its water bonds and angles."""
+    from sponge_b200 import capi, systems
+    opts = capi.options(cutoff=cutoff, skin=SKIN)
+    h = ctypes.c_void_p()
+    arr = np.ascontiguousarray
+    t, A, B = arr(s.lj_type, np.int32), arr(s.lj_A, np.float32), arr(s.lj_B, np.float32)
+    q = arr(s.charge, np.float32)
+    es, en = arr(s.excl_start, np.int32), arr(s.excl_numbers, np.int32)
+    el = arr(s.excl_list if len(s.excl_list) else np.zeros(1), np.int32)
+    capi.check(lib.snb_engine_create(ctypes.byref(opts), s.n, capi.boundary(s.cell(), s.rcell()),
+                                     s.n_types, t.ctypes.data, A.ctypes.data, B.ctypes.data,
+                                     q.ctypes.data, es.ctypes.data, en.ctypes.data,
+                                     el.ctypes.data, len(s.excl_list), ctypes.byref(h)),
+               "engine_create")
+    nb, na = len(s.bonds), len(s.angles)
+    ba, bb = arr(s.bonds[:, 0], np.int32), arr(s.bonds[:, 1], np.int32)
+    aa, ab, ac = (arr(s.angles[:, k], np.int32) for k in range(3))
+    bk, br = np.full(nb, systems.BOND_K, np.float32), np.full(nb, systems.BOND_R0, np.float32)
+    ak, at = np.full(na, systems.ANGLE_K, np.float32), np.full(na, systems.ANGLE_T0, np.float32)
+    capi.check(lib.snb_engine_set_bonded(h, nb, ba.ctypes.data, bb.ctypes.data, bk.ctypes.data,
+                                         br.ctypes.data, na, aa.ctypes.data, ab.ctypes.data,
+                                         ac.ctypes.data, ak.ctypes.data, at.ctypes.data),
+               "set_bonded")
+    return h
+
+
+def _equilibrate(lib, h, s, crd, vel, invm, dt, steps, st, sp):
+    """Untimed NVE steps with the velocities rescaled to 300 K every 100."""
+    import torch
+    from sponge_b200 import capi, systems
+    P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    mass = torch.from_numpy(s.mass.astype(np.float64)).cuda()
+    for c0 in range(0, steps, 100):
+        with torch.cuda.stream(st):
+            capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm),
+                                                     ctypes.c_float(dt), c0,
+                                                     min(100, steps - c0), sp), "md_steps")
+            v = vel.view(s.n, 3).double()
+            t_now = float((mass[:, None] * v * v).sum()) / (3.0 * s.n * systems.KB)
+            vel.mul_(float(np.sqrt(300.0 / t_now)))
+    st.synchronize()
+
+
+def _timed_steps(lib, h, crd, vel, invm, dt, first, steps, st, sp):
+    """Device time (ms) of `steps` graph-replayed steps."""
+    import torch
+    from sponge_b200 import capi
+    P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st.synchronize()
+    e0.record(st)
+    with torch.cuda.stream(st):
+        capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                                 first, steps, sp), "md_steps")
+    e1.record(st)
+    st.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_small_box(lib):
+    """The 9,000-atom box (3,000 waters, cutoff 8 A, PME 48^3): 200 NVE steps
+    from the Maxwell-Boltzmann start after 20 untimed ones, and the total-energy
+    drift fitted over the next 200 steps."""
+    import torch
+    from sponge_b200 import systems
+    s = systems.config_small(seed=0)
+    h = make_engine(lib, s, 8.0)
+    crd = torch.from_numpy(s.crd.reshape(-1).copy()).cuda()
+    vel = torch.from_numpy(s.vel.reshape(-1).copy()).cuda()
+    invm = torch.from_numpy((1.0 / s.mass).astype(np.float32)).cuda()
+    dt = DT_FS * 1e-3 * systems.TIME_CONVERSION
+    st = torch.cuda.Stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+    ms = _timed_steps(lib, h, crd, vel, invm, dt, 0, 200, st, sp)
+    # the drift after 1,000 steps at 300 K (the lattice start releases
+    # potential energy into the first few hundred steps)
+    _equilibrate(lib, h, s, crd, vel, invm, dt, 1000, st, sp)
+    drift = nve_drift(lib, h, s, crd, vel, invm, 1200, 200, 21, dt,
+                      lib.snb_engine_md_steps_graph, st, sp)
+    lib.snb_engine_destroy(h)
+    return {"workload": f"{s.n}-atom water box, cutoff 8 A, skin 2 A, "
+                        f"PME {systems.fft_size(s.box)}^3, NVE 0.5 fs",
+            "steps": 200, "ms_per_step": ms / 200, "ns_per_day": ns_per_day(200 / (ms / 1e3)),
+            "timed_from": "Maxwell-Boltzmann 300 K lattice start (first 200 steps)",
+            "nve_drift": drift}
+
+
+def run_soft_core_box(args, lib):
+    """The large soft-core workload: a water + 0.15 M NaCl box with a 64-site
+    alchemical solute (soft-core LJ, alpha 0.5, p 1, sigma 3 A), cutoff 10 A,
+    PME by the reference's grid rule.  The windows are the LJ stage of a
+    decoupling: the solute's charges are off in every window (state B's
+    charges; with them on, water H atoms, which carry no LJ, fall onto the
+    charged sites once their LJ is softened, and the box blows up), and lambda
+    takes the solute's LJ from state A to state B through the soft core.
+    Each window runs its own engine with the soft-core tables at its lambda.
+    Untimed equilibration in the lambda 0 window with 300 K velocity
+    rescaling; each window then runs 10 untimed and 500 timed graph-replayed
+    NVE steps from the state the previous window left."""
+    import copy
+
+    import torch
+    from sponge_b200 import capi, systems
+    s, sc = systems.soft_core_box(args.soft_core_waters, n_solute=64, seed=0)
+    crd = torch.from_numpy(s.crd.reshape(-1).copy()).cuda()
+    vel = torch.from_numpy(s.vel.reshape(-1).copy()).cuda()
+    invm = torch.from_numpy((1.0 / s.mass).astype(np.float32)).cuda()
+    dt = DT_FS * 1e-3 * systems.TIME_CONVERSION
+    st = torch.cuda.Stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+    arr = np.ascontiguousarray
+    tA, tB = arr(sc.type_A, np.int32), arr(sc.type_B, np.int32)
+    AA, AB = arr(sc.AA, np.float32), arr(sc.AB, np.float32)
+    BA, BB = arr(sc.BA, np.float32), arr(sc.BB, np.float32)
+    mask = arr(sc.mask, np.int32)
+
+    def window(lam):
+        w = copy.copy(s)
+        w.charge = (s.charge.astype(np.float64) + sc.charge_B_A).astype(np.float32)
+        h = make_engine(lib, w, CUTOFF)
+        o = capi.options(cutoff=CUTOFF, skin=SKIN, lambda_lj=lam, soft_core_alpha=0.5,
+                         soft_core_powfer=1.0, soft_core_sigma=3.0, soft_core_sigma_min=0.0)
+        hs = ctypes.c_void_p()
+        capi.check(lib.snb_lj_soft_create(ctypes.byref(o), s.n, sc.n_types_A, sc.n_types_B,
+                                          tA.ctypes.data, tB.ctypes.data, AA.ctypes.data,
+                                          AB.ctypes.data, BA.ctypes.data, BB.ctypes.data,
+                                          mask.ctypes.data, CUTOFF, ctypes.byref(hs)),
+                   "lj_soft_create")
+        capi.check(lib.snb_engine_set_soft_core(h, hs), "set_soft_core")
+        return h, hs
+
+    def close(h, hs):
+        lib.snb_engine_destroy(h)
+        lib.snb_lj_soft_destroy(hs)
+
+    EQ = max(0, args.soft_core_equilibrate)
+    h, hs = window(0.0)
+    _equilibrate(lib, h, s, crd, vel, invm, dt, EQ, st, sp)
+    close(h, hs)
+    runs = []
+    step = EQ
+    for lam in (0.0, 0.25, 0.5, 0.75, 1.0):
+        h, hs = window(lam)
+        _timed_steps(lib, h, crd, vel, invm, dt, step, 10, st, sp)
+        r0, r1 = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        capi.check(lib.snb_engine_stats(h, ctypes.byref(r0), None, sp), "stats")
+        ms = _timed_steps(lib, h, crd, vel, invm, dt, step + 10, 500, st, sp)
+        capi.check(lib.snb_engine_stats(h, ctypes.byref(r1), None, sp), "stats")
+        close(h, hs)
+        step += 510
+        v = vel.view(-1, 3).double()
+        ke = 0.5 * (torch.from_numpy(s.mass).cuda().double()[:, None] * v * v).sum(1)
+        runs.append({"lambda": lam, "ms_per_step": ms / 500,
+                     "ns_per_day": ns_per_day(500 / (ms / 1e3)),
+                     "nl_rebuilds": int(r1.value - r0.value),
+                     "temperature_K": float(2.0 * ke.sum() / (3.0 * s.n * systems.KB)),
+                     "hottest_atom_kcal_per_mol": float(ke.max())})
+    ok = bool(torch.isfinite(crd).all().item())
+    return {"workload": f"{s.n}-atom water + NaCl box with a 64-site soft-core solute, "
+                        f"L = {s.box:.2f} A, cutoff 10 A, skin 2 A, "
+                        f"PME {systems.fft_size(s.box)}^3, NVE 0.5 fs, alpha 0.5, p 1, "
+                        "LJ decoupling windows (solute charges off)",
+            "atoms": s.n, "equilibration_steps": EQ, "steps_per_lambda": 500,
+            "lambdas": runs, "finite": ok}
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
@@ -646,6 +818,12 @@ def run_ours(args):
 
     lib.snb_engine_destroy(h)
     batch = run_batch(args, lib, world, rank, dist) if args.batch_systems > 0 else None
+    small = soft_box = None
+    if world == 1:  # single-GPU measurements of the other workloads
+        if not args.no_small_box:
+            small = run_small_box(lib)
+        if args.soft_core_waters > 0:
+            soft_box = run_soft_core_box(args, lib)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -678,6 +856,8 @@ def run_ours(args):
             ["pair_unroll", "pair_blocks_per_sm", "search_blocks_per_sm", "gather_threads"],
             [int(x) for x in tuned]))),
         "batch": batch,
+        "small_box": small,
+        "soft_core_box": soft_box,
         "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clk,
     }
     print(json.dumps(line))
