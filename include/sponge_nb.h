@@ -113,7 +113,10 @@ int snb_options_set(snb_options* opt, const char* key, const char* value);
 int snb_nl_create(const snb_options* opt, int atom_numbers, float cutoff,
                   float skin, snb_boundary boundary, snb_nl** out);
 /* NEIGHBOR_LIST::Update (neighbor_list.h:19-22, neighbor_list.cpp:974-1025).
- * crd: float[3*N].  ghost_numbers must be 0 (one domain). */
+ * crd: float[3*N].  ghost_numbers must be 0 (one domain).  A rectangular
+ * box that differs from the last one redraws the cell grid by the
+ * reference's rule and forces the rebuild (a barostat's box change; the
+ * reference re-initialises the list for a large change, main.cpp:2092). */
 int snb_nl_update(snb_nl* nl, const int* atom_local, int local_atom_numbers,
                   int ghost_numbers, const float* crd, snb_boundary boundary,
                   int step, int update, const int* excluded_list_start,
@@ -242,6 +245,13 @@ int snb_pme_excluded_force(snb_pme* pme, int atom_numbers,
  * of the last energy/virial evaluation, FP64 (host sync). */
 int snb_pme_energies(snb_pme* pme, double* h_reciprocal, double* h_self,
                      double* h_virial6, void* stream);
+/* Particle_Mesh::Update_Box (PM_force.h:180, PM_force.cpp:1171-1248): the
+ * reciprocal part follows the new rectangular box in `boundary` at the same
+ * grid size (the influence function and the neutralising term are formed
+ * from the new cell and volume).  g (LTMatrix3 box-change rate) and dt only
+ * move the reference's domain corners and are not used.  A box change large
+ * enough to move the grid (main.cpp:2092-2124) re-creates the handle. */
+int snb_pme_update_box(snb_pme* pme, snb_boundary boundary, const float* g, float dt);
 int snb_pme_destroy(snb_pme* pme);
 
 /* No counterpart in the reference.  The excluded-pair correction of
@@ -318,6 +328,12 @@ int snb_engine_set_bonded(snb_engine* e, int bond_numbers, const int* h_bond_a,
                           const int* h_angle_a, const int* h_angle_b,
                           const int* h_angle_c, const float* h_angle_k,
                           const float* h_angle_theta0);
+/* Box change of the engine's box (Main_Box_Change, main.cpp:2055-2090, for a
+ * barostat): the neighbor grid is redrawn for the new lengths by the
+ * reference's rule and the list is rebuilt at the next step; PME follows
+ * Update_Box at the same grid size; the tail terms follow the new volume.
+ * The caller scales the coordinates.  Single rectangular boxes. */
+int snb_engine_update_box(snb_engine* e, snb_boundary boundary);
 /* Soft-core LJ in the engine (main.cpp:1460-1465 runs LJ_SOFT_CORE in place
  * of the plain LJ module when it is initialised): the engine's pair step
  * takes the end-state tables, types, perturbation mask and lambda / alpha /

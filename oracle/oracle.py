@@ -247,6 +247,8 @@ class ReferenceCPU:
         L.ref_lj_long_range.restype = ctypes.c_int
         L.ref_lj_long_range.argtypes = [_f32p, _f32p, ctypes.c_float]
         L.ref_lj_long_range_factor.restype = ctypes.c_float
+        L.ref_box_change.restype = ctypes.c_int
+        L.ref_box_change.argtypes = [_f32p]
         L.ref_soft_init.restype = ctypes.c_int
         L.ref_soft_init.argtypes = [_i32p, _i32p, ctypes.c_int, ctypes.c_int, _f32p,
                                     _f32p, _f32p, _f32p, _i32p, ctypes.c_char_p]
@@ -368,6 +370,13 @@ class ReferenceCPU:
         if rc != 0:
             raise RuntimeError("reference excluded correction failed")
         return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6))
+
+    def box_change(self, box):
+        """Main_Box_Change for a small change to a cubic box of length `box`:
+        later calls use the new boundary; PME's Update_Box has run."""
+        cell = np.array([box, 0, box, 0, 0, box], np.float32)
+        if self.lib.ref_box_change(cell) != 0:
+            raise RuntimeError("reference box change failed")
 
     def lj_long_range(self, volume):
         vir = np.zeros(6, np.float32)

@@ -246,6 +246,25 @@ extern "C"
 
     float ref_lj_long_range_factor() { return g ? g->lj.long_range_factor : 0; }
 
+    /* A barostat's box change as main.cpp's Main_Box_Change makes it for a
+     * small change (main.cpp:2055-2090): the new rectangular cell becomes the
+     * boundary every later call uses, and Particle_Mesh::Update_Box
+     * recomputes the influence function at the same grid size.  The
+     * neighbor list keeps its Initial grid, as there. */
+    int ref_box_change(const float* cell6)
+    {
+        if (!g) return -1;
+        REF_TRY({
+            g->boundary.cell = LTMatrix3(cell6[0], cell6[1], cell6[2],
+                                         cell6[3], cell6[4], cell6[5]);
+            g->boundary.rcell = Invert_Lower_Triangular_Cell(g->boundary.cell);
+            g->box = VECTOR(cell6[0], cell6[2], cell6[5]);
+            LTMatrix3 rate = LTMatrix3(0, 0, 0, 0, 0, 0);
+            g->pm.Update_Box(g->boundary, rate, 0.0f);
+        });
+        return 0;
+    }
+
     /* LJ_SOFT_CORE::Initial on the current system (after ref_init): end
      * state types and tables, subsystem masks; lambda_lj and soft_core_*
      * come from `commands` ("key=value;..."). */

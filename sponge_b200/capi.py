@@ -57,10 +57,10 @@ EXPORTED = [
     "snb_lj_soft_create", "snb_lj_soft_pme_direct_force", "snb_lj_soft_dh_dlambda",
     "snb_lj_soft_long_range_correction", "snb_lj_soft_energy_sums", "snb_lj_soft_destroy",
     "snb_pme_create", "snb_pme_beta", "snb_pme_grid", "snb_pme_reciprocal_force",
-    "snb_pme_excluded_force", "snb_pme_energies", "snb_pme_destroy",
+    "snb_pme_excluded_force", "snb_pme_energies", "snb_pme_update_box", "snb_pme_destroy",
     "snb_pme_excluded_force_noalloc",
     "snb_engine_create", "snb_batch_create", "snb_engine_force", "snb_engine_set_bonded",
-    "snb_engine_set_soft_core",
+    "snb_engine_set_soft_core", "snb_engine_update_box",
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_profile_steps",
     "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
     "snb_engine_destroy",
@@ -111,6 +111,7 @@ _SIGS = {
                                       _P]),
     "snb_pme_excluded_force": (_I, [_P, _I, _P, _P, _P, snb_boundary, _P, _P, _P, _P, _P,
                                     _I, _P, _I, _P, _P]),
+    "snb_pme_update_box": (_I, [_P, snb_boundary, _P, _F]),
     "snb_pme_energies": (_I, [_P, _P, _P, _P, _P]),
     "snb_pme_destroy": (_I, [_P]),
     "snb_pme_excluded_force_noalloc": (_I, [_I, _P, snb_boundary, _P, _F, _P, _P, _P, _P,
@@ -122,6 +123,7 @@ _SIGS = {
     "snb_engine_force": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
     "snb_engine_set_bonded": (_I, [_P, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "snb_engine_set_soft_core": (_I, [_P, _P]),
+    "snb_engine_update_box": (_I, [_P, snb_boundary]),
     "snb_engine_md_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_md_steps_graph": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_profile_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P, _P]),

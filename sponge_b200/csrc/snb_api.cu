@@ -844,6 +844,14 @@ extern "C" int snb_pme_energies(snb_pme* h, double* rec, double* self, double* v
   return kOk;
 }
 
+extern "C" int snb_pme_update_box(snb_pme* h, snb_boundary boundary, const float* g,
+                                  float dt) {
+  (void)g;   // the box-change rate and time step only move the reference's
+  (void)dt;  // domain corners; the new cell is in `boundary`
+  if (!h) return fail(kBadInput, "pme_update_box: null handle");
+  return pme_update_box(h->p, boundary.cell);
+}
+
 extern "C" int snb_pme_destroy(snb_pme* h) {
   if (!h) return kOk;
   pme_free(h->p);
@@ -1268,6 +1276,43 @@ extern "C" int snb_engine_force(snb_engine* e, const float* crd, float* frc, int
   return launch_unpack(e->n, e->nl.d_inv_perm, e->acc, e->accum,
                        reinterpret_cast<float3*>(frc), nullptr, nullptr, nullptr, nullptr,
                        en, vi, st);
+}
+
+extern "C" int snb_engine_update_box(snb_engine* e, snb_boundary boundary) {
+  if (!e) return fail(kBadInput, "engine_update_box: null handle");
+  if (e->nsys > 0) return fail(kNotSupported, "engine_update_box: batch engines");
+  const float* c6 = boundary.cell;
+  if (c6[1] != 0.f || c6[3] != 0.f || c6[4] != 0.f)
+    return fail(kNotSupported, "engine_update_box: only rectangular boxes are supported");
+  if (!(c6[0] > 0.f && c6[2] > 0.f && c6[5] > 0.f))
+    return fail(kBadInput, "engine_update_box: box lengths must be > 0");
+  int rc = nl_regrid(e->nl, c6);
+  if (rc) return rc;
+  if ((rc = pme_update_box(e->pme, c6))) return rc;
+  e->cell = make_cell(c6);
+  Cell r{};
+  r.a11 = 1.0f / e->cell.a11;
+  r.a22 = 1.0f / e->cell.a22;
+  r.a33 = 1.0f / e->cell.a33;
+  e->rcell = r;
+  // tail terms at the new volume
+  const double vol = (double)e->cell.a11 * e->cell.a22 * e->cell.a33;
+  e->lrc_energy_lj = e->lj.long_range_factor / vol;
+  e->lrc_virial_lj = 2.0 * e->lj.long_range_factor / vol;
+  if (e->soft) {
+    e->lrc_energy = e->soft->lrc / vol;
+    e->lrc_virial = 2.0 * e->soft->lrc / vol;
+  } else {
+    e->lrc_energy = e->lrc_energy_lj;
+    e->lrc_virial = e->lrc_virial_lj;
+  }
+  if (e->graph_exec) {  // the captured step holds the old box and list arrays
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+  }
+  e->steps_done = 0;  // the next step rebuilds the list, as after Initial
+  return kOk;
 }
 
 extern "C" int snb_engine_set_soft_core(snb_engine* e, snb_lj_soft* soft) {

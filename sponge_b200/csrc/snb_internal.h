@@ -154,6 +154,8 @@ int nl_rebuild(NeighborList& nl, const float* crd, const int* atom_local,
                cudaStream_t st);
 int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st);
 int nl_force_next(NeighborList& nl, cudaStream_t st);
+// A new rectangular box (single-box list): re-grid and force the next build.
+int nl_regrid(NeighborList& nl, const float* cell6);
 // Reads the overflow flag and regrows the pair storage if needed (host sync).
 int nl_check_overflow(NeighborList& nl, bool* regrown, cudaStream_t st);
 int nl_total_pairs(NeighborList& nl, long long* total, cudaStream_t st);
@@ -307,6 +309,8 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
              bool excluded);
 // A batch of rectangular boxes (sys[s].cell, rcell, atom ranges set): one
 // grid per box by the reference's size rule; fills the PME fields of sys.
+// Particle_Mesh::Update_Box: a new rectangular box at the same grid size.
+int pme_update_box(PME& p, const float* cell6);
 int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
                    float tolerance, float grid_spacing, bool reciprocal, bool excluded);
 void pme_free(PME& p);

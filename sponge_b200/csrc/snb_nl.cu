@@ -716,16 +716,85 @@ void nl_free(NeighborList& nl) {
   nl = NeighborList();
 }
 
+// A new rectangular box for a single-box list (barostat box change): the
+// reference's grid rule for the new lengths, its neighbour runs when the
+// cell counts change, and a forced rebuild on the next update.  The pair
+// criterion is exact in any grid whose cells are at least r_l / 2 wide, so
+// the pair set is the exact one of the new box.
+int nl_regrid(NeighborList& nl, const float* cell6) {
+  if (nl.bv.nsys > 0) return fail(kNotSupported, "neighbor list: box change of a batch");
+  if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f)
+    return fail(kNotSupported,
+                "neighbor list: only rectangular boxes are supported "
+                "(triclinic cells are not built on this path)");
+  const Cell c = make_cell(cell6);
+  int N[3];
+  int rc = box_grid(nl.grid_length, c, N);
+  if (rc) return rc;
+  if (N[0] != nl.Nx || N[1] != nl.Ny || N[2] != nl.Nz) {
+    const int ncell = N[0] * N[1] * N[2];
+    std::vector<std::vector<int2>> per(ncell);
+    std::vector<std::vector<char4>> per_geom(ncell);
+    box_runs(N[0], N[1], N[2], 0, per, per_geom);
+    std::vector<int2> runs;
+    std::vector<char4> geom;
+    std::vector<int> counts;
+    int max_runs = 0;
+    pack_runs(per, per_geom, runs, geom, counts, max_runs);
+    int2* d_runs = nullptr;
+    char4* d_geom = nullptr;
+    int *d_run_count = nullptr, *d_cell_count = nullptr, *d_cell_start = nullptr;
+    SNB_CUDA_TRY(cudaMalloc(&d_runs, sizeof(int2) * runs.size()));
+    SNB_CUDA_TRY(cudaMalloc(&d_geom, sizeof(char4) * geom.size()));
+    SNB_CUDA_TRY(cudaMalloc(&d_run_count, sizeof(int) * ncell));
+    SNB_CUDA_TRY(cudaMalloc(&d_cell_count, sizeof(int) * ncell));
+    SNB_CUDA_TRY(cudaMalloc(&d_cell_start, sizeof(int) * (ncell + 1)));
+    SNB_CUDA_TRY(cudaMemcpy(d_runs, runs.data(), sizeof(int2) * runs.size(),
+                            cudaMemcpyHostToDevice));
+    SNB_CUDA_TRY(cudaMemcpy(d_geom, geom.data(), sizeof(char4) * geom.size(),
+                            cudaMemcpyHostToDevice));
+    SNB_CUDA_TRY(cudaMemcpy(d_run_count, counts.data(), sizeof(int) * ncell,
+                            cudaMemcpyHostToDevice));
+    rc = scan_reserve(nl.scan, std::max(ncell, nl.n));
+    if (rc) return rc;
+    // the old arrays may still be read by work queued before this call
+    SNB_CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(nl.d_run_ranges);
+    cudaFree(nl.d_run_geom);
+    cudaFree(nl.d_run_count);
+    cudaFree(nl.d_cell_count);
+    cudaFree(nl.d_cell_start);
+    nl.d_run_ranges = d_runs;
+    nl.d_run_geom = d_geom;
+    nl.d_run_count = d_run_count;
+    nl.d_cell_count = d_cell_count;
+    nl.d_cell_start = d_cell_start;
+    nl.max_runs = max_runs;
+    nl.Nx = N[0];
+    nl.Ny = N[1];
+    nl.Nz = N[2];
+    nl.ncell = ncell;
+    nl.trim = N[0] >= 5 && N[1] >= 5 && N[2] >= 5;
+  }
+  nl.cell = c;
+  nl.rcell = rect_rcell(c);
+  nl.wx = c.a11 / nl.Nx;
+  nl.wy = c.a22 / nl.Ny;
+  nl.iwz = nl.Nz / c.a33;
+  nl.generation = 0;  // the next update rebuilds
+  return kOk;
+}
+
 int nl_update(NeighborList& nl, const float* crd_f, const int* atom_local,
               const float* cell6, int step, int forced, const int* excl_start,
               const int* excl_list, const int* excl_numbers, cudaStream_t st) {
   if (cell6) {
     Cell c = make_cell(cell6);
     if (c.a11 != nl.cell.a11 || c.a22 != nl.cell.a22 || c.a33 != nl.cell.a33 ||
-        c.a21 != 0.f || c.a31 != 0.f || c.a32 != 0.f)
-      return fail(kNotSupported,
-                  "neighbor list: the box changed since Initial (NPT re-grid is "
-                  "not built on this path)");
+        c.a21 != 0.f || c.a31 != 0.f || c.a32 != 0.f) {
+      int rc = nl_regrid(nl, cell6);
+      if (rc) return rc;
+    }
   }
   int rc = nl_decide(nl, crd_f, step, forced, st);
   if (rc) return rc;

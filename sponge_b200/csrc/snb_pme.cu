@@ -707,6 +707,27 @@ static int source_bins(int K, int T, std::vector<int4>& src) {
   return 0;
 }
 
+// Particle_Mesh::Update_Box (PM_force.cpp:1171-1248): the influence
+// function and the neutralising term follow the new cell and volume at the
+// same grid size.  Both are formed from p.cell / p.rcell / p.volume at each
+// call, so the update replaces those.  (The reference also moves its domain
+// corners, which this one-domain path has none of.)
+int pme_update_box(PME& p, const float* cell6) {
+  if (p.bv.nsys > 0) return fail(kNotSupported, "PME: box change of a batch");
+  if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f)
+    return fail(kNotSupported, "PME: only rectangular boxes are supported");
+  if (!(cell6[0] > 0.f && cell6[2] > 0.f && cell6[5] > 0.f))
+    return fail(kBadInput, "PME: box lengths must be > 0");
+  p.cell = make_cell(cell6);
+  Cell rc{};
+  rc.a11 = 1.0f / p.cell.a11;
+  rc.a22 = 1.0f / p.cell.a22;
+  rc.a33 = 1.0f / p.cell.a33;
+  p.rcell = rc;
+  p.volume = (double)p.cell.a11 * p.cell.a22 * p.cell.a33;
+  return kOk;
+}
+
 int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
              float cutoff, float tolerance, int fftx, int ffty, int fftz,
              float grid_spacing, int update_interval, bool reciprocal,

@@ -15,8 +15,9 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _FIXTURES = sorted(f for f in os.listdir(os.path.join(HERE, "golden")) if f.endswith(".npz"))
-GOLDEN = [f for f in _FIXTURES if not f.startswith("soft_")]
+GOLDEN = [f for f in _FIXTURES if not f.startswith(("soft_", "boxchange_"))]
 SOFT = [f for f in _FIXTURES if f.startswith("soft_")]
+BOXCHANGE = [f for f in _FIXTURES if f.startswith("boxchange_")]
 
 
 def load_case(name):
@@ -165,3 +166,30 @@ def test_oracle_soft_core_matches_reference(oracle, name):
     V = float(np.float32(s.box) ** 3)
     # the reference sums dH/dlambda in float over the atoms
     assert d["dudl_lj"] + fti / V == pytest.approx(float(z["dhdl"]), rel=2e-5, abs=1e-3)
+
+
+@pytest.mark.parametrize("name", BOXCHANGE)
+def test_oracle_box_change_matches_reference(oracle, name):
+    """After a barostat's box change (the reference initialised on box0,
+    then the box and coordinates scaled; PME's Update_Box at the old grid
+    size, the list rebuilt in its Initial grid): the exact pair set of the new
+    box, and the PME forces and energies of the new box at the old grid size.
+    The reciprocal virial is pinned to the reference initialised at the new
+    box: Update_Box forms the virial factor with the opposite sign of the
+    pi^2 m^2 / beta^2 term (PM_force.cpp:1210-1236 against :557-604), so its
+    virial after a box change is not the target."""
+    s, z = load_case(name)
+    assert float(z["box"]) != float(z["box0"])
+    rs, cols = oracle.nl_pairs_system(s, float(z["cutoff"]), float(z["skin"]))
+    i = np.repeat(np.arange(s.n), np.diff(rs))
+    pairs = np.stack([i, cols.astype(np.int64)], 1)
+    digest = hashlib.sha256(np.ascontiguousarray(pairs, np.int32).tobytes()).hexdigest()
+    assert digest == str(z["nl_pair_sha256"])
+    p = oracle.pme_f64(s, tuple(z["grid"]), float(z["beta"]))
+    assert rel_rms(z["pme_frc"], p["frc"]) < 1e-5
+    assert float(z["pme_e_recip"]) == pytest.approx(p["e_recip"], rel=2e-6)
+    assert float(z["pme_e_self"]) == pytest.approx(p["e_self"], rel=1e-6)
+    assert rel_rms(z["pme_frc_fresh"], p["frc"]) < 1e-5
+    assert np.allclose(z["pme_virial_fresh"], p["virial"], rtol=1e-5,
+                       atol=1e-5 * np.abs(p["virial"]).max())
+    assert not np.allclose(z["pme_virial"], p["virial"], rtol=1e-2)
