@@ -81,20 +81,26 @@ constexpr int kHitCap = 512;   // per-warp hit list (entries)
 // candidates per lane per scan round: a template parameter (2, 4 or 8) that
 // the engine's autotuner picks; 4 elsewhere
 
-template <int ACCUM, bool ENERGY, bool VIRIAL>
+// COUL_ONLY: atom i's type has A' = B' = 0 with every type, so the LJ terms
+// are exact zeros and are not formed (the results are bitwise the same).
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool COUL_ONLY = false>
 __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
                                         const float* sA, const float* sB, int ti,
                                         float qi, int gi, float4 e, int j, int tj,
                                         float& fx, float& fy, float& fz, float& e_lj,
                                         float& e_c, float* vir) {
   const float r2 = e.x * e.x + e.y * e.y + e.z * e.z;
-  const int p = lj_pair_index(ti, tj);
-  const float A = sA[p], B = sB[p];
+  float A = 0.f, B = 0.f;
+  if (!COUL_ONLY) {
+    const int p = lj_pair_index(ti, tj);
+    A = sA[p];
+    B = sB[p];
+  }
   const float rinv = rsqrtf(r2);
   const float r = r2 * rinv;
   const float ir2 = rinv * rinv;
   const float ir6 = ir2 * ir2 * ir2;
-  const float flj = (B - A * ir6) * ir6 * ir2;
+  const float flj = COUL_ONLY ? 0.f : (B - A * ir6) * ir6 * ir2;
   const float qq = qi * e.w;
   const float br = a.beta * r;
   float ex;
@@ -109,7 +115,7 @@ __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
   if (ENERGY || VIRIAL) {
     const bool own_i = gi < a.global[j];
     if (ENERGY) {
-      const float elj = (0.083333333f * A * ir6 - 0.166666667f * B) * ir6;
+      const float elj = COUL_ONLY ? 0.f : (0.083333333f * A * ir6 - 0.166666667f * B) * ir6;
       const float ec = qq * erfc_br * rinv;
       if (own_i) {
         e_lj += elj;
@@ -173,6 +179,13 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   float e_lj = 0.f, e_c = 0.f;
   float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   const int k0 = a.row_start[i], k1 = k0 + a.row_count[i];
+  // a type without LJ against every type (water H): Coulomb-only row
+  bool coul_only = true;
+  for (int t = lane; t < a.n_types; t += 32) {
+    const int p = lj_pair_index(ti, t);
+    coul_only = coul_only && sA[p] == 0.f && sB[p] == 0.f;
+  }
+  coul_only = __all_sync(0xffffffffu, coul_only);
   {
     // the warp's next row: start pulling its indices from HBM into L2 now
     // (row starts are multiples of 8 entries, so 16-byte aligned)
@@ -212,15 +225,27 @@ k_lj_direct(PairArgs a, Accumulators acc) {
     }
     __syncwarp();
     // phase 2: pair terms over the hit list
-    for (int h = lane; h < count; h += 32) {
-      const int j = hits[h];
-      const float4 pj = a.pos[j];
-      const int tj = a.type[j];
-      const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri, cell,
-                                              rcell);
-      lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi,
-                                     make_float4(dr.x, dr.y, dr.z, pj.w), j, tj, fx, fy,
-                                     fz, e_lj, e_c, vir);
+    if (coul_only) {
+      for (int h = lane; h < count; h += 32) {
+        const int j = hits[h];
+        const float4 pj = a.pos[j];
+        const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri, cell,
+                                                rcell);
+        lj_pair<ACCUM, ENERGY, VIRIAL, true>(a, acc, sA, sB, ti, pi.w, gi,
+                                             make_float4(dr.x, dr.y, dr.z, pj.w), j, 0, fx,
+                                             fy, fz, e_lj, e_c, vir);
+      }
+    } else {
+      for (int h = lane; h < count; h += 32) {
+        const int j = hits[h];
+        const float4 pj = a.pos[j];
+        const int tj = a.type[j];
+        const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri, cell,
+                                                rcell);
+        lj_pair<ACCUM, ENERGY, VIRIAL>(a, acc, sA, sB, ti, pi.w, gi,
+                                       make_float4(dr.x, dr.y, dr.z, pj.w), j, tj, fx, fy,
+                                       fz, e_lj, e_c, vir);
+      }
     }
     __syncwarp();
   }
