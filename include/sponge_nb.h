@@ -379,6 +379,46 @@ int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
                      void* stream);
 int snb_engine_destroy(snb_engine* e);
 
+/* ------------------------------------------- native inputs and outputs */
+/* SPONGE's native text inputs of this path, read on the host.  Each reader
+ * reads the file's counts; called with NULL arrays it returns only those,
+ * so the caller can size its buffers and call again.  Conversions are the
+ * reference's (fscanf "%f" / "%d"; LJ tables stored as A' = 12 A,
+ * B' = 6 B).  A file that does not parse returns SNB_ERR_BAD_INPUT with
+ * the reference's "the format of ... is not right" message. */
+/* Xponge::Native_Load_LJ (xponge/load/native/lj.hpp:9-67): "N T", then
+ * T(T+1)/2 A, T(T+1)/2 B, N types.  A and B are [T(T+1)/2], type is [N]. */
+int snb_read_lj_in_file(const char* path, int* atom_numbers, int* atom_type_numbers,
+                        float* h_LJ_A, float* h_LJ_B, int* h_atom_LJ_type);
+/* Xponge::Native_Load_LJ_Soft_Core (xponge/load/native/lj_soft.hpp:8-89):
+ * "N TA TB", the AA, AB tables of state A, the BA, BB tables of state B,
+ * then N pairs "typeA typeB". */
+int snb_read_lj_soft_core_in_file(const char* path, int* atom_numbers,
+                                  int* atom_type_numbers_A, int* atom_type_numbers_B,
+                                  float* h_LJ_AA, float* h_LJ_AB, float* h_LJ_BA,
+                                  float* h_LJ_BB, int* h_LJ_type_A, int* h_LJ_type_B);
+/* subsys_division_in_file (xponge/load/native/lj_soft.hpp:91-124): "N", then
+ * N ints. */
+int snb_read_subsys_division_in_file(const char* path, int* atom_numbers,
+                                     int* h_subsys_division);
+/* Xponge::Native_Load_Charge / Native_Load_Mass
+ * (xponge/load/native/md_core.hpp:9-103): "N", then N floats (charges in
+ * the internal unit, already scaled by 18.2223). */
+int snb_read_charge_in_file(const char* path, int* atom_numbers, float* h_charge);
+int snb_read_mass_in_file(const char* path, int* atom_numbers, float* h_mass);
+/* Xponge::Native_Load_Exclusions (xponge/load/native/md_core.hpp:259-313):
+ * "N M", then per atom its count and excluded atoms; returned as the CSR
+ * that MD_INFORMATION::non_bond_information::Initial builds from it
+ * (MD_core/nb.hpp:32-76): start[N], numbers[N], list[M]. */
+int snb_read_exclude_in_file(const char* path, int* atom_numbers,
+                             int* excluded_atom_numbers, int* h_excluded_list_start,
+                             int* h_excluded_numbers, int* h_excluded_list);
+/* MD_INFORMATION::trajectory_output::Append_Frc_Traj_File
+ * (MD_core/output.hpp:1691-1700): appends one frame, the N float3 forces of
+ * device array d_frc, to the binary file at path (host sync). */
+int snb_append_frc_traj(const char* path, const float* d_frc, int atom_numbers,
+                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif

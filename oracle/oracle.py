@@ -260,6 +260,10 @@ class ReferenceCPU:
                                     ctypes.POINTER(ctypes.c_float)]
         L.ref_soft_long_range.restype = ctypes.c_int
         L.ref_soft_long_range.argtypes = [_f32p, _f32p, ctypes.c_float, _f32p]
+        L.ref_native_load.restype = ctypes.c_int
+        L.ref_native_load.argtypes = [ctypes.c_char_p]
+        L.ref_native_get.restype = ctypes.c_longlong
+        L.ref_native_get.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
         L.ref_set_threads.argtypes = [ctypes.c_int]
         L.ref_max_threads.restype = ctypes.c_int
         self.n = 0
@@ -370,6 +374,22 @@ class ReferenceCPU:
         if rc != 0:
             raise RuntimeError("reference excluded correction failed")
         return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6))
+
+    def native_load(self, files: dict):
+        """The reference's native-input loaders on {key: path} (mass_in_file,
+        charge_in_file, exclude_in_file, LJ_in_file, LJ_soft_core_in_file,
+        subsys_division_in_file)."""
+        cmd = ";".join(f"{k}={v}" for k, v in files.items())
+        if self.lib.ref_native_load(cmd.encode()) != 0:
+            raise RuntimeError("reference native load failed")
+
+    def native_get(self, name: str, dtype=np.float32):
+        n = int(self.lib.ref_native_get(name.encode(), None))
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(max(n, 1), dtype)
+        self.lib.ref_native_get(name.encode(), out.ctypes.data)
+        return out[:n]
 
     def box_change(self, box):
         """Main_Box_Change for a small change to a cubic box of length `box`:

@@ -20,6 +20,9 @@
 #include "PM_force/PM_force.h"
 #include "neighbor_list/neighbor_list.h"
 #include "ref_controller.h"
+#include "xponge/load/native/lj.hpp"
+#include "xponge/load/native/lj_soft.hpp"
+#include "xponge/load/native/md_core.hpp"
 
 /* --------------------------- the system --------------------------- */
 namespace
@@ -41,6 +44,7 @@ struct RefContext
     bool ready = false;
 };
 RefContext* g = NULL;
+Xponge::System g_native;
 std::string g_err;
 }  // namespace
 
@@ -361,5 +365,80 @@ extern "C"
             }
         });
         return 0;
+    }
+
+    /* The reference's native-input loaders (xponge/load/native/*.hpp) on
+     * the files named in `commands` ("key=path;..."): mass_in_file,
+     * charge_in_file, exclude_in_file, LJ_in_file, LJ_soft_core_in_file and
+     * subsys_division_in_file, each only when given.  The results stay in a
+     * System of their own; ref_native_get copies one field out. */
+    int ref_native_load(const char* commands)
+    {
+        REF_TRY({
+            controller.commands.clear();
+            std::string c = commands ? commands : "";
+            size_t pos = 0;
+            while (pos < c.size())
+            {
+                size_t end = c.find(';', pos);
+                if (end == std::string::npos) end = c.size();
+                std::string kv = c.substr(pos, end - pos);
+                size_t eq = kv.find('=');
+                if (eq != std::string::npos)
+                    controller.commands[kv.substr(0, eq)] = kv.substr(eq + 1);
+                pos = end + 1;
+            }
+            g_native = Xponge::System();
+            if (controller.Command_Exist("mass_in_file"))
+                Xponge::Native_Load_Mass(&g_native, &controller);
+            if (controller.Command_Exist("charge_in_file"))
+                Xponge::Native_Load_Charge(&g_native, &controller);
+            if (controller.Command_Exist("exclude_in_file"))
+                Xponge::Native_Load_Exclusions(&g_native, &controller);
+            Xponge::Native_Load_LJ(&g_native, &controller);
+            Xponge::Native_Load_LJ_Soft_Core(&g_native, &controller);
+        });
+        return 0;
+    }
+
+    /* Copies field `name` of the loaded System into out (when not NULL) and
+     * returns its length, or -1 for an unknown name. */
+    long long ref_native_get(const char* name, void* out)
+    {
+        const auto& ff = g_native.classical_force_field;
+        const auto& sc = ff.lj_soft_core;
+        std::string n = name ? name : "";
+        auto put_f = [&](const std::vector<float>& v) -> long long {
+            if (out) memcpy(out, v.data(), sizeof(float) * v.size());
+            return (long long)v.size();
+        };
+        auto put_i = [&](const std::vector<int>& v) -> long long {
+            if (out) memcpy(out, v.data(), sizeof(int) * v.size());
+            return (long long)v.size();
+        };
+        if (n == "mass") return put_f(g_native.atoms.mass);
+        if (n == "charge") return put_f(g_native.atoms.charge);
+        if (n == "lj_A") return put_f(ff.lj.pair_A);
+        if (n == "lj_B") return put_f(ff.lj.pair_B);
+        if (n == "lj_type") return put_i(ff.lj.atom_type);
+        if (n == "lj_type_numbers") return ff.lj.atom_type_numbers;
+        if (n == "AA") return put_f(sc.LJ_AA);
+        if (n == "AB") return put_f(sc.LJ_AB);
+        if (n == "BA") return put_f(sc.LJ_BA);
+        if (n == "BB") return put_f(sc.LJ_BB);
+        if (n == "type_A") return put_i(sc.atom_LJ_type_A);
+        if (n == "type_B") return put_i(sc.atom_LJ_type_B);
+        if (n == "subsys") return put_i(sc.subsystem_division);
+        if (n == "excl_numbers" || n == "excl_list")
+        {
+            std::vector<int> num, list;
+            for (const auto& e : g_native.exclusions.excluded_atoms)
+            {
+                num.push_back((int)e.size());
+                list.insert(list.end(), e.begin(), e.end());
+            }
+            return put_i(n == "excl_numbers" ? num : list);
+        }
+        return -1;
     }
 }

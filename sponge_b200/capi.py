@@ -64,7 +64,18 @@ EXPORTED = [
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_profile_steps",
     "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
     "snb_engine_destroy",
+    "snb_read_lj_in_file", "snb_read_lj_soft_core_in_file", "snb_read_subsys_division_in_file",
+    "snb_read_charge_in_file", "snb_read_mass_in_file", "snb_read_exclude_in_file",
+    "snb_append_frc_traj",
 ]
+
+# status codes of include/sponge_nb.h
+SNB_OK = 0
+SNB_ERR_BAD_INPUT = 1
+SNB_ERR_CUDA = 2
+SNB_ERR_OVERFLOW = 3
+SNB_ERR_TIMEOUT = 4
+SNB_ERR_NOT_SUPPORTED = 5
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -124,6 +135,14 @@ _SIGS = {
     "snb_engine_set_bonded": (_I, [_P, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "snb_engine_set_soft_core": (_I, [_P, _P]),
     "snb_engine_update_box": (_I, [_P, snb_boundary]),
+    "snb_read_lj_in_file": (_I, [ctypes.c_char_p, _P, _P, _P, _P, _P]),
+    "snb_read_lj_soft_core_in_file": (_I, [ctypes.c_char_p, _P, _P, _P, _P, _P, _P, _P,
+                                           _P, _P]),
+    "snb_read_subsys_division_in_file": (_I, [ctypes.c_char_p, _P, _P]),
+    "snb_read_charge_in_file": (_I, [ctypes.c_char_p, _P, _P]),
+    "snb_read_mass_in_file": (_I, [ctypes.c_char_p, _P, _P]),
+    "snb_read_exclude_in_file": (_I, [ctypes.c_char_p, _P, _P, _P, _P, _P]),
+    "snb_append_frc_traj": (_I, [ctypes.c_char_p, _P, _I, _P]),
     "snb_engine_md_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_md_steps_graph": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_profile_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P, _P]),

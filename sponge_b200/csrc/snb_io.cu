@@ -1,0 +1,191 @@
+// SPONGE's native text inputs of this path and its force trajectory output,
+// on the host: the LJ and soft-core LJ tables (Xponge::Native_Load_LJ,
+// xponge/load/native/lj.hpp:9-67; Native_Load_LJ_Soft_Core, lj_soft.hpp),
+// the subsystem division, the exclusion lists, charges and masses
+// (xponge/load/native/md_core.hpp), and the binary frc trajectory
+// (MD_core/output.hpp:1691-1700).
+//
+// Each reader reads the file's counts first.  Called with NULL arrays it
+// returns only the counts, so a caller can size its buffers and call again.
+// Values are read with the same conversions as the reference (fscanf "%f"
+// and "%d"; A' = 12 A and B' = 6 B as the tables are stored).
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "snb_internal.h"
+
+namespace snb {
+namespace {
+
+struct File {
+  FILE* fp = nullptr;
+  explicit File(const char* path) : fp(path ? fopen(path, "r") : nullptr) {}
+  ~File() {
+    if (fp) fclose(fp);
+  }
+};
+
+int bad_format(const char* what) {
+  return fail(kBadInput, std::string("the format of ") + what + " is not right");
+}
+
+int no_file(const char* what, const char* path) {
+  return fail(kBadInput, std::string("cannot open ") + what + " '" + (path ? path : "") + "'");
+}
+
+// n floats into out (or skipped when out is NULL), each times scale
+bool read_floats(FILE* fp, int n, float* out, float scale) {
+  for (int i = 0; i < n; ++i) {
+    float v;
+    if (fscanf(fp, "%f", &v) != 1) return false;
+    if (out) out[i] = v * scale;
+  }
+  return true;
+}
+
+bool read_ints(FILE* fp, int n, int* out) {
+  for (int i = 0; i < n; ++i) {
+    int v;
+    if (fscanf(fp, "%d", &v) != 1) return false;
+    if (out) out[i] = v;
+  }
+  return true;
+}
+
+}  // namespace
+}  // namespace snb
+
+using namespace snb;
+
+extern "C" int snb_read_lj_in_file(const char* path, int* atom_numbers,
+                                   int* atom_type_numbers, float* h_LJ_A, float* h_LJ_B,
+                                   int* h_atom_LJ_type) {
+  const char* what = "LJ_in_file";
+  if (!atom_numbers || !atom_type_numbers) return fail(kBadInput, "read_lj_in_file: null count");
+  File f(path);
+  if (!f.fp) return no_file(what, path);
+  int n = 0, t = 0;
+  if (fscanf(f.fp, "%d %d", &n, &t) != 2 || n < 0 || t <= 0) return bad_format(what);
+  *atom_numbers = n;
+  *atom_type_numbers = t;
+  if (!h_LJ_A && !h_LJ_B && !h_atom_LJ_type) return kOk;
+  if (!h_LJ_A || !h_LJ_B || !h_atom_LJ_type)
+    return fail(kBadInput, "read_lj_in_file: give all three arrays or none");
+  const int pairs = t * (t + 1) / 2;
+  if (!read_floats(f.fp, pairs, h_LJ_A, 12.0f) || !read_floats(f.fp, pairs, h_LJ_B, 6.0f) ||
+      !read_ints(f.fp, n, h_atom_LJ_type))
+    return bad_format(what);
+  return kOk;
+}
+
+extern "C" int snb_read_lj_soft_core_in_file(const char* path, int* atom_numbers,
+                                             int* atom_type_numbers_A,
+                                             int* atom_type_numbers_B, float* h_LJ_AA,
+                                             float* h_LJ_AB, float* h_LJ_BA, float* h_LJ_BB,
+                                             int* h_LJ_type_A, int* h_LJ_type_B) {
+  const char* what = "LJ_soft_core_in_file";
+  if (!atom_numbers || !atom_type_numbers_A || !atom_type_numbers_B)
+    return fail(kBadInput, "read_lj_soft_core_in_file: null count");
+  File f(path);
+  if (!f.fp) return no_file(what, path);
+  int n = 0, ta = 0, tb = 0;
+  if (fscanf(f.fp, "%d %d %d", &n, &ta, &tb) != 3 || n < 0 || ta <= 0 || tb <= 0)
+    return bad_format(what);
+  *atom_numbers = n;
+  *atom_type_numbers_A = ta;
+  *atom_type_numbers_B = tb;
+  const bool any = h_LJ_AA || h_LJ_AB || h_LJ_BA || h_LJ_BB || h_LJ_type_A || h_LJ_type_B;
+  if (!any) return kOk;
+  if (!h_LJ_AA || !h_LJ_AB || !h_LJ_BA || !h_LJ_BB || !h_LJ_type_A || !h_LJ_type_B)
+    return fail(kBadInput, "read_lj_soft_core_in_file: give all six arrays or none");
+  const int pa = ta * (ta + 1) / 2, pb = tb * (tb + 1) / 2;
+  if (!read_floats(f.fp, pa, h_LJ_AA, 12.0f) || !read_floats(f.fp, pa, h_LJ_AB, 6.0f) ||
+      !read_floats(f.fp, pb, h_LJ_BA, 12.0f) || !read_floats(f.fp, pb, h_LJ_BB, 6.0f))
+    return bad_format(what);
+  for (int i = 0; i < n; ++i)
+    if (fscanf(f.fp, "%d %d", h_LJ_type_A + i, h_LJ_type_B + i) != 2) return bad_format(what);
+  return kOk;
+}
+
+// One count then one value per atom: subsys_division_in_file (int),
+// charge_in_file and mass_in_file (float).
+static int read_per_atom(const char* path, const char* what, int* atom_numbers, float* fv,
+                         int* iv) {
+  if (!atom_numbers) return fail(kBadInput, std::string("read ") + what + ": null count");
+  File f(path);
+  if (!f.fp) return no_file(what, path);
+  int n = 0;
+  if (fscanf(f.fp, "%d", &n) != 1 || n < 0) return bad_format(what);
+  *atom_numbers = n;
+  if (fv && !read_floats(f.fp, n, fv, 1.0f)) return bad_format(what);
+  if (iv && !read_ints(f.fp, n, iv)) return bad_format(what);
+  return kOk;
+}
+
+extern "C" int snb_read_subsys_division_in_file(const char* path, int* atom_numbers,
+                                                int* h_subsys_division) {
+  return read_per_atom(path, "subsys_division_in_file", atom_numbers, nullptr,
+                       h_subsys_division);
+}
+
+extern "C" int snb_read_charge_in_file(const char* path, int* atom_numbers, float* h_charge) {
+  return read_per_atom(path, "charge_in_file", atom_numbers, h_charge, nullptr);
+}
+
+extern "C" int snb_read_mass_in_file(const char* path, int* atom_numbers, float* h_mass) {
+  return read_per_atom(path, "mass_in_file", atom_numbers, h_mass, nullptr);
+}
+
+extern "C" int snb_read_exclude_in_file(const char* path, int* atom_numbers,
+                                        int* excluded_atom_numbers, int* h_excluded_list_start,
+                                        int* h_excluded_numbers, int* h_excluded_list) {
+  const char* what = "exclude_in_file";
+  if (!atom_numbers || !excluded_atom_numbers)
+    return fail(kBadInput, "read_exclude_in_file: null count");
+  File f(path);
+  if (!f.fp) return no_file(what, path);
+  int n = 0, m = 0;
+  if (fscanf(f.fp, "%d %d", &n, &m) != 2 || n < 0 || m < 0) return bad_format(what);
+  *atom_numbers = n;
+  *excluded_atom_numbers = m;
+  const bool any = h_excluded_list_start || h_excluded_numbers || h_excluded_list;
+  if (!any) return kOk;
+  if (!h_excluded_list_start || !h_excluded_numbers || !h_excluded_list)
+    return fail(kBadInput, "read_exclude_in_file: give all three arrays or none");
+  int count = 0;
+  for (int i = 0; i < n; ++i) {
+    int k = 0;
+    if (fscanf(f.fp, "%d", &k) != 1 || k < 0) return bad_format(what);
+    h_excluded_list_start[i] = count;
+    h_excluded_numbers[i] = k;
+    for (int j = 0; j < k; ++j) {
+      int v;
+      if (fscanf(f.fp, "%d", &v) != 1) return bad_format(what);
+      if (count >= m)
+        return fail(kBadInput, "the format of exclude_in_file is not right "
+                               "(excluded_atom_numbers is not right)");
+      h_excluded_list[count++] = v;
+    }
+  }
+  if (count != m)
+    return fail(kBadInput, "the format of exclude_in_file is not right "
+                           "(excluded_atom_numbers is not right)");
+  return kOk;
+}
+
+extern "C" int snb_append_frc_traj(const char* path, const float* d_frc, int atom_numbers,
+                                   void* stream) {
+  if (!path || !d_frc || atom_numbers <= 0) return fail(kBadInput, "append_frc_traj: bad argument");
+  std::vector<float> h(3 * (size_t)atom_numbers);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  SNB_CUDA_TRY(cudaMemcpyAsync(h.data(), d_frc, sizeof(float) * h.size(),
+                               cudaMemcpyDeviceToHost, st));
+  SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  FILE* fp = fopen(path, "ab");
+  if (!fp) return no_file("frc trajectory", path);
+  const size_t w = fwrite(h.data(), sizeof(float) * 3, atom_numbers, fp);
+  fclose(fp);
+  if (w != (size_t)atom_numbers) return fail(kBadInput, "append_frc_traj: short write");
+  return kOk;
+}
