@@ -137,6 +137,9 @@ struct snb_engine {
   // into the same fixed-point accumulator (integer adds commute)
   cudaStream_t branch = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // third branch: the excluded correction and bonded terms, beside PME
+  cudaStream_t branch2 = nullptr;
+  cudaEvent_t ev_join2 = nullptr;
   int body_kernels = 0;         // kernel nodes inside the rebuild body
   // recovery snapshot for neighbor-list overflow
   float* d_snap_crd = nullptr;
@@ -948,9 +951,11 @@ static int engine_finish_create(snb_engine* e, int n, int n_types, const int* h_
     int lo = 0, hi = 0;
     SNB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     SNB_CUDA_TRY(cudaStreamCreateWithPriority(&e->branch, cudaStreamNonBlocking, hi));
+    SNB_CUDA_TRY(cudaStreamCreateWithPriority(&e->branch2, cudaStreamNonBlocking, hi));
   }
   SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
   SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
+  SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_join2, cudaEventDisableTiming));
   return kOk;
 }
 
@@ -1171,15 +1176,20 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   const bool fork = !e->prof_on;
   cudaStream_t sb = fork ? e->branch : st;
   if (fork) {
+    // PME on `branch`, the excluded correction and bonded terms on `branch2`,
+    // the pair kernel on the step's stream
+    cudaStream_t sb2 = e->branch2;
     SNB_CUDA_TRY(cudaEventRecord(e->ev_fork, st));
     SNB_CUDA_TRY(cudaStreamWaitEvent(sb, e->ev_fork, 0));
-    if (with_bonded && (rc = engine_bonded(e, crd, sb))) return rc;
+    SNB_CUDA_TRY(cudaStreamWaitEvent(sb2, e->ev_fork, 0));
+    if (with_bonded && (rc = engine_bonded(e, crd, sb2))) return rc;
     if (e->pme.excluded &&
         (rc = launch_excluded(e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
                               e->cell, e->rcell, e->pme.beta, e->d_excl_start,
                               e->d_excl_list, e->d_excl_numbers, e->nl.d_inv_perm, e->acc,
-                              e->accum, energy, virial, sb, e->bv)))
+                              e->accum, energy, virial, sb2, e->bv)))
       return rc;
+    SNB_CUDA_TRY(cudaEventRecord(e->ev_join2, sb2));
     if (do_pme && (rc = pme_after_bin(e->pme, e->n, e->acc, e->accum, energy, virial, sb)))
       return rc;
     SNB_CUDA_TRY(cudaEventRecord(e->ev_join, sb));
@@ -1236,6 +1246,7 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   if (rc) return rc;
   if (fork) {
     SNB_CUDA_TRY(cudaStreamWaitEvent(st, e->ev_join, 0));
+    SNB_CUDA_TRY(cudaStreamWaitEvent(st, e->ev_join2, 0));
     return kOk;
   }
   prof_mark(e, 3, st);
@@ -1718,6 +1729,8 @@ extern "C" int snb_engine_destroy(snb_engine* e) {
   if (e->branch) cudaStreamDestroy(e->branch);
   if (e->ev_fork) cudaEventDestroy(e->ev_fork);
   if (e->ev_join) cudaEventDestroy(e->ev_join);
+  if (e->branch2) cudaStreamDestroy(e->branch2);
+  if (e->ev_join2) cudaEventDestroy(e->ev_join2);
   nl_free(e->nl);
   pme_free(e->pme);
   acc_free(e->acc);

@@ -102,8 +102,8 @@ int launch_bonded(int nb, const int* ba, const int* bb, const float* bk,
   return kOk;
 }
 
-// Leap-frog from the fixed-point accumulator (sorted frame via map), zeroing
-// the accumulator for the next step.
+// Leap-frog from the fixed-point accumulator (sorted frame via map); the
+// launch then clears the accumulator for the next step.
 // When old_crd is given, also performs the refresh check of the next step
 // (Check_Refresh, neighbor_list.cpp:307-321) on the new coordinates and
 // raises flags[0] if any atom moved more than sqrt(permit2) since the build.
@@ -124,11 +124,8 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
   float3 r_old = make_float3(0.f, 0.f, 0.f);
   if (old_crd) r_old = old_crd[i];
   const int N = acc.n;
-  long long* __restrict__ f = acc.d_f;
+  const long long* __restrict__ f = acc.d_f;
   const long long fx_i = f[s], fy_i = f[N + s], fz_i = f[2 * N + s];
-  f[s] = 0;
-  f[N + s] = 0;
-  f[2 * N + s] = 0;
   const float fx = (float)((double)fx_i * kForceScaleInv);
   const float fy = (float)((double)fy_i * kForceScaleInv);
   const float fz = (float)((double)fz_i * kForceScaleInv);
@@ -165,6 +162,9 @@ int launch_leap_frog(int n, const int* map, Accumulators& acc, float3* crd,
                                                        dt, old_crd, cell, rcell, permit2,
                                                        flags, bv);
   SNB_CUDA_TRY(cudaGetLastError());
+  // the accumulator starts the next step at zero: one coalesced clear
+  // instead of scattered stores through the permutation
+  SNB_CUDA_TRY(cudaMemsetAsync(acc.d_f, 0, sizeof(long long) * 3 * (size_t)acc.n, st));
   return kOk;
 }
 
