@@ -796,9 +796,28 @@ int nl_update(NeighborList& nl, const float* crd_f, const int* atom_local,
       if (rc) return rc;
     }
   }
+  const bool first = nl.generation == 0;
   int rc = nl_decide(nl, crd_f, step, forced, st);
   if (rc) return rc;
-  return nl_rebuild(nl, crd_f, atom_local, excl_start, excl_list, excl_numbers, st);
+  rc = nl_rebuild(nl, crd_f, atom_local, excl_start, excl_list, excl_numbers, st);
+  if (rc || !first) return rc;
+  // The first build sizes the rows from the mean density of the box, which
+  // a box with empty regions (a slab, a droplet) underestimates: check it
+  // here, regrow and build again, so the first evaluation is complete.  (It
+  // is never inside a stream capture: later overflows are caught by
+  // nl_check_overflow at the caller's interval.)
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  SNB_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return kOk;
+  for (int tries = 0; tries < 4; ++tries) {
+    bool regrown = false;
+    if ((rc = nl_check_overflow(nl, &regrown, st))) return rc;
+    if (!regrown) return kOk;
+    if ((rc = nl_decide(nl, crd_f, step, 1, st))) return rc;
+    if ((rc = nl_rebuild(nl, crd_f, atom_local, excl_start, excl_list, excl_numbers, st)))
+      return rc;
+  }
+  return kOk;
 }
 
 // need_update decision of NEIGHBOR_LIST::Update (neighbor_list.cpp:983-999)

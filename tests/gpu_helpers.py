@@ -120,7 +120,7 @@ def pme_create(box: Box, cutoff, accumulation="fixed64", **opts):
     lib = capi.load()
     h = ctypes.c_void_p()
     o = capi.options(cutoff=cutoff, accumulation=accumulation, **opts)
-    L = np.array([box.s.box] * 3, np.float32)
+    L = np.array(getattr(box.s, "lengths", [box.s.box] * 3), np.float32)
     capi.check(lib.snb_pme_create(ctypes.byref(o), box.n, box.b, L.ctypes.data, cutoff,
                                   ctypes.byref(h)), "pme_create")
     beta = float(lib.snb_pme_beta(h))

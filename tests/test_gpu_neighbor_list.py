@@ -119,6 +119,7 @@ def test_list_overflow_regrows(g, oracle, small_box):
         import torch
         dense = (s.crd - s.crd.mean(0)) * np.float32(0.5) + np.float32(s.box / 2)
         crd = torch.from_numpy(dense.astype(np.float32).reshape(-1)).cuda()
+        g.nl_update(nl, box, forced=1)  # the first build, at the lattice density
         g.nl_update(nl, box, crd=crd, forced=1)
         regrown = ctypes.c_int(0)
         g.capi.check(lib.snb_nl_check_overflow(nl, ctypes.byref(regrown), g.stream()),
@@ -158,3 +159,24 @@ def test_list_is_deterministic(g, box_9k):
             lib.snb_nl_destroy(nl)
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_first_build_regrows_by_itself(g, oracle, small_box):
+    """A first build that outgrows the rows sized from the box's mean density
+    (here the atoms packed into an eighth of the box) regrows and builds
+    again before it returns: the list is exact without a Check_Overflow."""
+    import torch
+    s = small_box
+    box = g.Box(s)
+    nl = g.make_nl(box, 8.0, 2.0)
+    lib = g.capi.load()
+    dense = (s.crd - s.crd.mean(0)) * np.float32(0.5) + np.float32(s.box / 2)
+    try:
+        crd = torch.from_numpy(dense.astype(np.float32).reshape(-1)).cuda()
+        g.nl_update(nl, box, crd=crd, forced=1)
+        got = g.nl_pairs(nl)
+    finally:
+        lib.snb_nl_destroy(nl)
+    rs, cols = oracle.nl_pairs(dense.astype(np.float32), s.cell(), s.rcell(), 8.0, 2.0,
+                               s.excl_start, s.excl_numbers, s.excl_list)
+    assert np.array_equal(got, g.csr_to_pairs(rs, cols))
