@@ -8,7 +8,9 @@ below and stores what this project's path needs (coordinates, charges, LJ
 tables in SPONGE's A' = 12 A, B' = 6 B triangular form, the exclusion CSR)
 plus the bonded term lists and parameters the test evaluates in FP64, the
 residue ranges, and Amber's forces (iter0.npy) and potential energy
-(reference.json).  Needs the reference tree (this container):
+(reference.json), for the case's three frames: the minimised one and two
+made from it by the reference's own rigid-water perturbation (0.02 and
+0.05 A).  Needs the reference tree (this container):
 
     python tests/golden/make_amber_golden.py
 """
@@ -63,9 +65,37 @@ def read_rst7(path):
     return crd, box
 
 
+def frame(iteration, perturbation):
+    """Coordinates of one of the case's frames: the minimised one, perturbed
+    by the reference's own rigid-water perturbation (seed 20260217 +
+    2000 * iteration, as its comparison test calls it) for iterations > 0."""
+    import pathlib
+    import shutil
+    import sys
+    import tempfile
+    src = os.path.join(CASE, "statics", NAME, "system_minimized.rst7")
+    if perturbation == 0.0:
+        return read_rst7(src)
+    sys.path.insert(0, "/root/reference")
+    from benchmarks.comparison.tests.amber.tests.utils import (
+        perturb_rst7_with_rigid_water_inplace)
+    with tempfile.TemporaryDirectory() as d:
+        dst = os.path.join(d, "system.rst7")
+        shutil.copy(src, dst)
+        perturb_rst7_with_rigid_water_inplace(
+            pathlib.Path(dst), pathlib.Path(os.path.join(CASE, "statics", NAME, "system.parm7")),
+            perturbation=perturbation, seed=20260217 + 2000 * iteration)
+        return read_rst7(dst)
+
+
 def main():
+    for it, pert in ((0, 0.0), (1, 0.02), (2, 0.05)):
+        make(it, pert)
+
+
+def make(iteration, perturbation):
     p = read_parm7(os.path.join(CASE, "statics", NAME, "system.parm7"))
-    crd, box = read_rst7(os.path.join(CASE, "statics", NAME, "system_minimized.rst7"))
+    crd, box = frame(iteration, perturbation)
     n = p["POINTERS"][0]
     ntypes = p["POINTERS"][1]
     assert crd.shape == (n, 3)
@@ -102,7 +132,8 @@ def main():
     dihedrals = terms("DIHEDRALS_INC_HYDROGEN", "DIHEDRALS_WITHOUT_HYDROGEN", 5)
     ref = json.load(open(os.path.join(CASE, "reference.json")))
     entry = next(e for e in ref["entries"]
-                 if e["case_name"] == NAME and e["iteration"] == 0)
+                 if e["case_name"] == NAME and e["iteration"] == iteration)
+    assert abs(entry["perturbation"] - perturbation) < 1e-12
     forces = np.load(os.path.join(CASE, entry["forces_file"]))
     out = dict(
         crd=crd.astype(np.float32), crd64=crd, box=box,
@@ -122,7 +153,7 @@ def main():
         amber_forces=forces, amber_epot=np.float64(entry["energy_epot"]),
         cutoff=np.float32(8.0),
     )
-    path = os.path.join(HERE, "amber_alanine_dipeptide_tip4pew_iter0.npz")
+    path = os.path.join(HERE, f"amber_alanine_dipeptide_tip4pew_iter{iteration}.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes;", n, "sites,", len(flat), "exclusions")
 

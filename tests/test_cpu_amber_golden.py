@@ -1,7 +1,8 @@
 """Known answer from outside this project: the reference's Amber comparison
 case (alanine dipeptide in TIP4P-Ew water, 2,398 sites; sander's forces and
-potential energy of the minimised frame, cutoff 8 A, PME; the fixture
-tests/golden/amber_alanine_dipeptide_tip4pew_iter0.npz is made by
+potential energy of the minimised frame and of two frames the reference's
+test perturbs from it, cutoff 8 A, PME; the fixtures
+tests/golden/amber_alanine_dipeptide_tip4pew_iter*.npz are made by
 tests/golden/make_amber_golden.py).
 
 The nonbonded part comes from the FP64 oracle of this path (LJ + direct
@@ -23,13 +24,14 @@ import numpy as np
 import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-FIXTURE = os.path.join(HERE, "golden", "amber_alanine_dipeptide_tip4pew_iter0.npz")
+FRAMES = [0, 1, 2]  # the minimised frame and its 0.02 / 0.05 A perturbations
 
 
-def load_amber():
+def load_amber(iteration=0):
     from sponge_b200 import systems
 
-    z = np.load(FIXTURE)
+    z = np.load(os.path.join(HERE, "golden",
+                             f"amber_alanine_dipeptide_tip4pew_iter{iteration}.npz"))
 
     class RectSystem(systems.System):
         """A rectangular box of lengths `lengths`."""
@@ -171,19 +173,15 @@ def solute_atoms(z):
             for a in range(ptr[r], ptr[r + 1])]
 
 
-@pytest.fixture(scope="module")
-def amber_bonded():
-    s, z = load_amber()
-    x = np.asarray(z["crd64"], np.float64)
-    return bonded_forces(z, x, solute_atoms(z)), bonded_energy(z, x)
-
-
-def test_oracle_matches_amber_known_answer(oracle, amber_bonded):
-    s, z = load_amber()
+@pytest.mark.parametrize("iteration", FRAMES)
+def test_oracle_matches_amber_known_answer(oracle, iteration):
+    s, z = load_amber(iteration)
     f_nb, e_nb = nonbonded_f64(oracle, s)
-    f_b, e_b = amber_bonded
+    x = np.asarray(z["crd64"], np.float64)
+    f_b, e_b = bonded_forces(z, x, solute_atoms(z)), bonded_energy(z, x)
     st = compare(z, f_nb + f_b, e_nb + e_b)
-    print(f"\nAmber TIP4P-Ew alanine dipeptide, FP64 oracle: |dE| {st['de']:.4f}, "
+    print(f"\nAmber TIP4P-Ew alanine dipeptide frame {iteration}, FP64 oracle: "
+          f"|dE| {st['de']:.4f}, "
           f"max |dF| {st['max_abs']:.4f}, RMS dF {st['rms']:.4f}, cos {st['cos']:.6f}")
     assert st["de"] <= 0.5
     assert st["max_abs"] <= 0.10

@@ -19,10 +19,11 @@ def g():
     return gpu_helpers
 
 
-def test_engine_matches_fp64_and_amber(g, oracle):
+@pytest.mark.parametrize("iteration", [0, 1, 2])
+def test_engine_matches_fp64_and_amber(g, oracle, iteration):
     import torch
     from tests import test_cpu_amber_golden as am
-    s, z = am.load_amber()
+    s, z = am.load_amber(iteration)
     lib = g.capi.load()
     e = g.engine_create(s, 8.0)
     crd = g.dev(s.crd.reshape(-1), np.float32)
@@ -42,7 +43,8 @@ def test_engine_matches_fp64_and_amber(g, oracle):
     x = np.asarray(z["crd64"], np.float64)
     f_b = am.bonded_forces(z, x, am.solute_atoms(z))
     st = am.compare(z, got + f_b, e_gpu + am.bonded_energy(z, x))
-    print(f"\nAmber TIP4P-Ew alanine dipeptide, engine: |dE| {st['de']:.4f}, "
+    print(f"\nAmber TIP4P-Ew alanine dipeptide frame {iteration}, engine: "
+          f"|dE| {st['de']:.4f}, "
           f"max |dF| {st['max_abs']:.4f}, RMS dF {st['rms']:.4f}, cos {st['cos']:.6f}")
     assert st["de"] <= 0.5
     assert st["max_abs"] <= 0.10
