@@ -101,6 +101,7 @@ typedef struct snb_lj snb_lj;
 typedef struct snb_lj_soft snb_lj_soft;
 typedef struct snb_pme snb_pme;
 typedef struct snb_engine snb_engine;
+typedef struct snb_nb14 snb_nb14;
 
 /* ---------------------------------------------------------------- misc */
 int snb_version(void);
@@ -341,6 +342,12 @@ int snb_engine_update_box(snb_engine* e, snb_boundary boundary);
  * correction.  `soft` must outlive the engine's use of it; NULL turns the
  * plain LJ back on.  Single boxes, fixed-point accumulation. */
 int snb_engine_set_soft_core(snb_engine* e, snb_lj_soft* soft);
+/* 1-4 terms in the engine (main.cpp runs NON_BOND_14 in the same force
+ * pass): the pairs of `nb14` (created for the same atom count) are added to
+ * every step's forces and virial; their energy (LJ + Coulomb) fills slot 6
+ * of the totals.  `nb14` must outlive the engine's use of it; NULL removes
+ * them.  Single boxes, fixed-point accumulation. */
+int snb_engine_set_nb14(snb_engine* e, snb_nb14* nb14);
 int snb_engine_md_steps(snb_engine* e, float* crd, float* vel,
                         const float* inverse_mass, float dt, int first_step,
                         int steps, void* stream);
@@ -379,6 +386,29 @@ int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
                      void* stream);
 int snb_engine_destroy(snb_engine* e);
 
+/* ----------------------------------------------------------- 1-4 terms */
+/* NON_BOND_14 (nb14/nb14.h, nb14/nb14.cpp).  Pair t of atoms (a, b) at
+ * distance r (minimum image) adds E = A'/12 r^-12 - B'/6 r^-6
+ * + c q_a q_b / r with A', B' the pair's scaled LJ entries (A' = 12 A,
+ * B' = 6 B) and c its Coulomb scale factor; charges below 1e-10 in
+ * magnitude are taken as 1e-10.  Energy and virial go to atom a.
+ * Initial (nb14.cpp:102-176) / Parameter_Host_To_Device: host arrays of
+ * nb14_numbers entries. */
+int snb_nb14_create(int atom_numbers, int nb14_numbers, const int* h_atom_a,
+                    const int* h_atom_b, const float* h_A, const float* h_B,
+                    const float* h_cf_scale_factor, snb_nb14** out);
+/* Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial (nb14.cpp:292-305,
+ * kernel nb14.cpp:8-103): adds to frc[N*3], atom_energy[N] and
+ * atom_virial[N*6] (LTMatrix3 order) on `stream`. */
+int snb_nb14_force(snb_nb14* h, const float* crd, const float* charge,
+                   snb_boundary boundary, float* frc, int need_atom_energy,
+                   float* atom_energy, int need_virial, float* atom_virial,
+                   void* stream);
+/* Step_Print's sums (nb14.cpp:307-324) of the last call with energies:
+ * nb14_LJ and nb14_EE (host sync). */
+int snb_nb14_energy_sums(snb_nb14* h, float* h_lj, float* h_ee, void* stream);
+int snb_nb14_destroy(snb_nb14* h);
+
 /* ------------------------------------------- native inputs and outputs */
 /* SPONGE's native text inputs of this path, read on the host.  Each reader
  * reads the file's counts; called with NULL arrays it returns only those,
@@ -413,6 +443,17 @@ int snb_read_mass_in_file(const char* path, int* atom_numbers, float* h_mass);
 int snb_read_exclude_in_file(const char* path, int* atom_numbers,
                              int* excluded_atom_numbers, int* h_excluded_list_start,
                              int* h_excluded_numbers, int* h_excluded_list);
+/* Xponge::Native_Load_NB14 (xponge/load/native/nb14.hpp:8-101): the rows
+ * of extra_path ("M", then M rows "a b A B c", A and B stored times 12 and
+ * 6) first, then those of path ("K", then K rows "a b lj_scale c", A' and
+ * B' = lj_scale times the pair's h_LJ_A / h_LJ_B entry for the two atoms'
+ * types).  Either path may be NULL.  nb14_numbers = M + K.  An atom index
+ * outside [0, atom_numbers) returns SNB_ERR_BAD_INPUT. */
+int snb_read_nb14_in_file(const char* path, const char* extra_path, int atom_numbers,
+                          const int* h_atom_LJ_type, const float* h_LJ_A,
+                          const float* h_LJ_B, int* nb14_numbers, int* h_atom_a,
+                          int* h_atom_b, float* h_A, float* h_B,
+                          float* h_cf_scale_factor);
 /* MD_INFORMATION::trajectory_output::Append_Frc_Traj_File
  * (MD_core/output.hpp:1691-1700): appends one frame, the N float3 forces of
  * device array d_frc, to the binary file at path (host sync). */

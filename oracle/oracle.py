@@ -70,6 +70,10 @@ class Oracle:
         L.snbo_excluded_f64.argtypes = [
             ctypes.c_int, _f32p, _f32p, _f32p, _f32p, ctypes.c_float, _i32p,
             _i32p, _i32p, _f64p, _f64p, _f64p]
+        L.snbo_nb14_f64.restype = None
+        L.snbo_nb14_f64.argtypes = [
+            ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
+            _f64p, _f64p, _f64p, _f64p]
         L.snbo_pme_f64.restype = None
         L.snbo_pme_f64.argtypes = [
             ctypes.c_int, _f32p, _f32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int,
@@ -148,6 +152,21 @@ class Oracle:
             s.cell(), s.rcell(), beta, _c(s.excl_start, np.int32),
             _c(s.excl_numbers, np.int32), _c(el, np.int32), frc, ae, vir)
         return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6))
+
+    def nb14_f64(self, s, a, b, A, B, cf):
+        """1-4 terms of pairs (a[t], b[t]) with scaled LJ entries A, B and
+        Coulomb scale cf, in FP64 (nb14/nb14.cpp:8-103)."""
+        n, m = s.n, len(a)
+        frc, ae, vir, sums = np.zeros(3 * n), np.zeros(n), np.zeros(6 * n), np.zeros(2)
+        z32 = np.zeros(max(m, 1), np.float32)
+        zi = np.zeros(max(m, 1), np.int32)
+        self.lib.snbo_nb14_f64(
+            m, _c(a, np.int32) if m else zi, _c(b, np.int32) if m else zi,
+            _c(A, np.float32) if m else z32, _c(B, np.float32) if m else z32,
+            _c(cf, np.float32) if m else z32, _c(s.crd, np.float32).reshape(-1),
+            _c(s.charge, np.float32), s.cell(), s.rcell(), frc, ae, vir, sums)
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6),
+                    lj=sums[0], ee=sums[1])
 
     def pme_f64(self, s, grid, beta, want_phi=False):
         n = s.n
@@ -260,6 +279,9 @@ class ReferenceCPU:
                                     ctypes.POINTER(ctypes.c_float)]
         L.ref_soft_long_range.restype = ctypes.c_int
         L.ref_soft_long_range.argtypes = [_f32p, _f32p, ctypes.c_float, _f32p]
+        L.ref_nb14.restype = ctypes.c_int
+        L.ref_nb14.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p,
+                               _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f64p]
         L.ref_native_load.restype = ctypes.c_int
         L.ref_native_load.argtypes = [ctypes.c_char_p]
         L.ref_native_get.restype = ctypes.c_longlong
@@ -378,7 +400,7 @@ class ReferenceCPU:
     def native_load(self, files: dict):
         """The reference's native-input loaders on {key: path} (mass_in_file,
         charge_in_file, exclude_in_file, LJ_in_file, LJ_soft_core_in_file,
-        subsys_division_in_file)."""
+        subsys_division_in_file, nb14_in_file, nb14_extra_in_file)."""
         cmd = ";".join(f"{k}={v}" for k, v in files.items())
         if self.lib.ref_native_load(cmd.encode()) != 0:
             raise RuntimeError("reference native load failed")
@@ -390,6 +412,29 @@ class ReferenceCPU:
         out = np.zeros(max(n, 1), dtype)
         self.lib.ref_native_get(name.encode(), out.ctypes.data)
         return out[:n]
+
+    def nb14(self, s, a, b, A, B, cf):
+        """NON_BOND_14 of the reference on pairs (a[t], b[t]) with scaled LJ
+        entries A, B and Coulomb scale cf, in s's box (forces, per-atom
+        energies and virials, the LJ and Coulomb sums)."""
+        n, m = s.n, len(a)
+        frc, ae, vir = (np.zeros(3 * n, np.float32), np.zeros(n, np.float32),
+                        np.zeros(6 * n, np.float32))
+        sums = np.zeros(2)
+        pad = max(m, 1)
+
+        def arr(x, dt):
+            y = np.zeros(pad, dt)
+            y[:m] = x
+            return y
+        rc = self.lib.ref_nb14(n, m, arr(a, np.int32), arr(b, np.int32), arr(A, np.float32),
+                               arr(B, np.float32), arr(cf, np.float32),
+                               _c(s.crd, np.float32).reshape(-1), _c(s.charge, np.float32),
+                               _c(s.cell(), np.float32), frc, ae, vir, sums)
+        if rc != 0:
+            raise RuntimeError("reference nb14 failed")
+        return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6),
+                    lj=float(sums[0]), ee=float(sums[1]))
 
     def box_change(self, box):
         """Main_Box_Change for a small change to a cubic box of length `box`:

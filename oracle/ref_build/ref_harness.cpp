@@ -1,6 +1,7 @@
 /* TEST INFRASTRUCTURE ONLY -- builds the reference's own CPU implementation
  * of the nonbonded hot path (its unmodified neighbor_list.cpp,
- * Lennard_Jones_force.cpp, LJ_soft_core.cpp, PM_force.cpp and common.cpp,
+ * Lennard_Jones_force.cpp, LJ_soft_core.cpp, PM_force.cpp, nb14.cpp and
+ * common.cpp,
  * compiled from the reference tree by oracle/Makefile) into oracle/_ref/.
  *
  * The reference's MD_core, Domain_decomposition, Xponge loaders and CONTROLLER
@@ -18,11 +19,13 @@
 #include "Lennard_Jones_force/LJ_soft_core.h"
 #include "Lennard_Jones_force/Lennard_Jones_force.h"
 #include "PM_force/PM_force.h"
+#include "nb14/nb14.h"
 #include "neighbor_list/neighbor_list.h"
 #include "ref_controller.h"
 #include "xponge/load/native/lj.hpp"
 #include "xponge/load/native/lj_soft.hpp"
 #include "xponge/load/native/md_core.hpp"
+#include "xponge/load/native/nb14.hpp"
 
 /* --------------------------- the system --------------------------- */
 namespace
@@ -48,10 +51,10 @@ Xponge::System g_native;
 std::string g_err;
 }  // namespace
 
-#define REF_TRY(body)                      \
+#define REF_TRY(...)                       \
     try                                    \
     {                                      \
-        body;                              \
+        __VA_ARGS__;                       \
     }                                      \
     catch (const std::exception& e)        \
     {                                      \
@@ -367,10 +370,72 @@ extern "C"
         return 0;
     }
 
+    /* NON_BOND_14 on pairs given directly (the arrays Initial copies from
+     * its loader, nb14.cpp:155-163), one call of
+     * Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial after Get_Local
+     * over all n atoms of a periodic box cell6.  frc [n*3], atom_energy [n]
+     * and atom_virial [n*6] are added to; sums[0..1] = the per-pair LJ and
+     * Coulomb energies that Step_Print sums, here summed in double. */
+    int ref_nb14(int n, int m, const int* a, const int* b, const float* A,
+                 const float* B, const float* cf, const float* crd,
+                 const float* charge, const float* cell6, float* frc,
+                 float* atom_energy, float* atom_virial, double* sums)
+    {
+        REF_TRY({
+            NON_BOND_14 nb;
+            nb.nb14_numbers = m;
+            nb.Memory_Allocate();
+            for (int t = 0; t < m; ++t)
+            {
+                nb.h_atom_a[t] = a[t];
+                nb.h_atom_b[t] = b[t];
+                nb.h_A[t] = A[t];
+                nb.h_B[t] = B[t];
+                nb.h_cf_scale_factor[t] = cf[t];
+            }
+            nb.Parameter_Host_To_Device();
+            nb.is_initialized = 1;
+            std::vector<char> label(n, 1);
+            std::vector<int> id(n);
+            for (int i = 0; i < n; ++i) id[i] = i;
+            nb.Get_Local(id.data(), n, 0, label.data(), id.data());
+            Boundary bd;
+            bd.policy = BoundaryPolicy::Periodic;
+            bd.cell = LTMatrix3(cell6[0], cell6[1], cell6[2], cell6[3], cell6[4],
+                                cell6[5]);
+            bd.rcell = Invert_Lower_Triangular_Cell(bd.cell);
+            nb.Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial(
+                reinterpret_cast<const VECTOR*>(crd), charge, bd,
+                reinterpret_cast<VECTOR*>(frc), 1, atom_energy, 1,
+                reinterpret_cast<LTMatrix3*>(atom_virial));
+            double lj = 0.0, ee = 0.0;
+            for (int t = 0; t < m; ++t)
+            {
+                lj += nb.d_nb14_lj_energy[t];
+                ee += nb.d_nb14_cf_energy[t];
+            }
+            sums[0] = lj;
+            sums[1] = ee;
+            void* host[] = {nb.h_atom_a, nb.h_atom_b, nb.h_A, nb.h_B,
+                            nb.h_cf_scale_factor, nb.h_nb14_lj_energy_sum,
+                            nb.h_nb14_cf_energy_sum};
+            for (void* p : host) free(p);
+            void* dev[] = {nb.d_atom_a, nb.d_atom_b, nb.d_A, nb.d_B,
+                           nb.d_cf_scale_factor, nb.d_nb14_cf_energy,
+                           nb.d_nb14_lj_energy, nb.d_nb14_lj_energy_sum,
+                           nb.d_nb14_cf_energy_sum, nb.d_atom_a_local,
+                           nb.d_atom_b_local, nb.d_A_local, nb.d_B_local,
+                           nb.d_cf_scale_factor_local, nb.d_num_nb14_local};
+            for (void* p : dev) deviceFree(p);
+        });
+        return 0;
+    }
+
     /* The reference's native-input loaders (xponge/load/native/*.hpp) on
      * the files named in `commands` ("key=path;..."): mass_in_file,
-     * charge_in_file, exclude_in_file, LJ_in_file, LJ_soft_core_in_file and
-     * subsys_division_in_file, each only when given.  The results stay in a
+     * charge_in_file, exclude_in_file, LJ_in_file, LJ_soft_core_in_file,
+     * subsys_division_in_file, nb14_in_file and nb14_extra_in_file, each
+     * only when given.  The results stay in a
      * System of their own; ref_native_get copies one field out. */
     int ref_native_load(const char* commands)
     {
@@ -397,6 +462,7 @@ extern "C"
                 Xponge::Native_Load_Exclusions(&g_native, &controller);
             Xponge::Native_Load_LJ(&g_native, &controller);
             Xponge::Native_Load_LJ_Soft_Core(&g_native, &controller);
+            Xponge::Native_Load_NB14(&g_native, &controller);
         });
         return 0;
     }
@@ -429,6 +495,11 @@ extern "C"
         if (n == "type_A") return put_i(sc.atom_LJ_type_A);
         if (n == "type_B") return put_i(sc.atom_LJ_type_B);
         if (n == "subsys") return put_i(sc.subsystem_division);
+        if (n == "nb14_a") return put_i(ff.nb14.atom_a);
+        if (n == "nb14_b") return put_i(ff.nb14.atom_b);
+        if (n == "nb14_A") return put_f(ff.nb14.A);
+        if (n == "nb14_B") return put_f(ff.nb14.B);
+        if (n == "nb14_cf") return put_f(ff.nb14.cf_scale_factor);
         if (n == "excl_numbers" || n == "excl_list")
         {
             std::vector<int> num, list;

@@ -584,6 +584,54 @@ SNBO_API void snbo_excluded_f64(int n, const float* crd, const float* charge,
 }
 
 /* ------------------------------------------------------------------ */
+/* 1-4 terms, FP64 run of
+ * Dihedral_14_LJ_CF_Force_With_Atom_Energy_And_Virial_Device
+ * (nb14/nb14.cpp:8-103): for pair t, dr = r_b - r_a (minimum image),
+ * F/r = -A r^-14 + B r^-8 - c q_a q_b r^-3 applied +F to a and -F to b;
+ * energy (A/12 r^-12 - B/6 r^-6 + c q_a q_b / r, with the reference's
+ * constants 0.08333333 and 0.1666666) and virial -(F (x) dr) to atom a;
+ * a charge below 1e-10 in magnitude is taken as 1e-10 (nb14.cpp:4,55-58).
+ * sums[0] = LJ, sums[1] = Coulomb (Step_Print, nb14.cpp:307-324). */
+SNBO_API void snbo_nb14_f64(int m, const int* ia, const int* ib, const float* A,
+                            const float* B, const float* cf, const float* crd,
+                            const float* charge, const float* cell,
+                            const float* rcell, double* frc, double* atom_energy,
+                            double* virial, double* sums)
+{
+    for (int t = 0; t < m; ++t)
+    {
+        int a = ia[t], b = ib[t];
+        double dr[3];
+        min_image_f64(crd + 3 * b, crd + 3 * a, cell, rcell, dr);
+        double r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+        double r = sqrt(r2);
+        double ir2 = 1.0 / r2, ir = 1.0 / r;
+        double ir4 = ir2 * ir2, ir8 = ir4 * ir4, ir14 = ir8 * ir4 * ir2;
+        double qa = charge[a], qb = charge[b];
+        if (fabs(qa) < 1e-10) qa = (double)1e-10f;
+        if (fabs(qb) < 1e-10) qb = (double)1e-10f;
+        double f = -(double)A[t] * ir14 + (double)B[t] * ir8 -
+                   (double)cf[t] * ir2 * ir * qa * qb;
+        double g[3] = {f * dr[0], f * dr[1], f * dr[2]};
+        for (int c = 0; c < 3; ++c)
+        {
+            frc[3 * a + c] += g[c];
+            frc[3 * b + c] -= g[c];
+        }
+        double ec = (double)cf[t] * ir * qa * qb;
+        double el = (double)0.08333333f * A[t] * ir4 * ir8 -
+                    (double)0.1666666f * B[t] * ir4 * ir2;
+        if (atom_energy) atom_energy[a] += ec + el;
+        if (sums)
+        {
+            sums[0] += el;
+            sums[1] += ec;
+        }
+        if (virial) virial_add(virial + 6 * a, g, dr, -1.0);
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* PME reciprocal part in FP64 (PM_force.cpp:541-612 tables, 699-893 spread and
  * gather, 896-919 + 1142-1166 energies, 1024-1068 virial). */
 

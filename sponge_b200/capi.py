@@ -60,13 +60,14 @@ EXPORTED = [
     "snb_pme_excluded_force", "snb_pme_energies", "snb_pme_update_box", "snb_pme_destroy",
     "snb_pme_excluded_force_noalloc",
     "snb_engine_create", "snb_batch_create", "snb_engine_force", "snb_engine_set_bonded",
-    "snb_engine_set_soft_core", "snb_engine_update_box",
+    "snb_engine_set_soft_core", "snb_engine_update_box", "snb_engine_set_nb14",
+    "snb_nb14_create", "snb_nb14_force", "snb_nb14_energy_sums", "snb_nb14_destroy",
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_profile_steps",
     "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
     "snb_engine_destroy",
     "snb_read_lj_in_file", "snb_read_lj_soft_core_in_file", "snb_read_subsys_division_in_file",
     "snb_read_charge_in_file", "snb_read_mass_in_file", "snb_read_exclude_in_file",
-    "snb_append_frc_traj",
+    "snb_read_nb14_in_file", "snb_append_frc_traj",
 ]
 
 # status codes of include/sponge_nb.h
@@ -135,6 +136,13 @@ _SIGS = {
     "snb_engine_set_bonded": (_I, [_P, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "snb_engine_set_soft_core": (_I, [_P, _P]),
     "snb_engine_update_box": (_I, [_P, snb_boundary]),
+    "snb_engine_set_nb14": (_I, [_P, _P]),
+    "snb_nb14_create": (_I, [_I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    "snb_nb14_force": (_I, [_P, _P, _P, snb_boundary, _P, _I, _P, _I, _P, _P]),
+    "snb_nb14_energy_sums": (_I, [_P, _P, _P, _P]),
+    "snb_nb14_destroy": (_I, [_P]),
+    "snb_read_nb14_in_file": (_I, [ctypes.c_char_p, ctypes.c_char_p, _I, _P, _P, _P, _P,
+                                   _P, _P, _P, _P, _P]),
     "snb_read_lj_in_file": (_I, [ctypes.c_char_p, _P, _P, _P, _P, _P]),
     "snb_read_lj_soft_core_in_file": (_I, [ctypes.c_char_p, _P, _P, _P, _P, _P, _P, _P,
                                            _P, _P]),

@@ -88,6 +88,14 @@ struct snb_pme {
   float4* d_pos = nullptr;
 };
 
+struct snb_nb14 {
+  NB14 p;
+  int n = 0;
+  int accum = kAccumFixed;
+  Accumulators acc;
+  long long* d_sums = nullptr;  // [2] {LJ + Coulomb, Coulomb} of the last energy call
+};
+
 struct snb_engine {
   snb_options opt;
   int n = 0;
@@ -128,6 +136,8 @@ struct snb_engine {
   double lrc_virial = 0.0;   // tail virial (diagonal) summed over the boxes
   double lrc_energy_lj = 0.0, lrc_virial_lj = 0.0;  // the plain LJ module's
   snb_lj_soft* soft = nullptr;  // soft-core pair terms in place of plain LJ
+  snb_nb14* nb14 = nullptr;     // 1-4 terms beside the excluded correction
+  long long* d_nb14_sums = nullptr;  // [2]
   // launch shapes picked by snb_engine_autotune
   int pair_unroll = 4;
   int pair_blocks_per_sm = 0;
@@ -1189,6 +1199,11 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
                               e->d_excl_list, e->d_excl_numbers, e->nl.d_inv_perm, e->acc,
                               e->accum, energy, virial, sb2, e->bv)))
       return rc;
+    if (e->nb14 &&
+        (rc = launch_nb14(e->nb14->p, reinterpret_cast<const float3*>(crd), e->d_charge,
+                          e->cell, e->rcell, e->nl.d_inv_perm, e->acc, energy, virial, false,
+                          energy ? e->d_nb14_sums : nullptr, sb2)))
+      return rc;
     SNB_CUDA_TRY(cudaEventRecord(e->ev_join2, sb2));
     if (do_pme && (rc = pme_after_bin(e->pme, e->n, e->acc, e->accum, energy, virial, sb)))
       return rc;
@@ -1257,6 +1272,11 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
                          virial, st, e->bv);
     if (rc) return rc;
   }
+  if (e->nb14 &&
+      (rc = launch_nb14(e->nb14->p, reinterpret_cast<const float3*>(crd), e->d_charge, e->cell,
+                        e->rcell, e->nl.d_inv_perm, e->acc, energy, virial, false,
+                        energy ? e->d_nb14_sums : nullptr, st)))
+    return rc;
   prof_mark(e, 4, st);
   if (do_pme) {
     rc = pme_after_bin(e->pme, e->n, e->acc, e->accum, energy, virial, st);
@@ -1276,17 +1296,103 @@ extern "C" int snb_engine_force(snb_engine* e, const float* crd, float* frc, int
   bool en = need_energy != 0, vi = need_virial != 0;
   if ((en || vi) && !d_totals) return fail(kBadInput, "engine_force: d_totals required");
   if (en || vi) SNB_CUDA_TRY(cudaMemsetAsync(e->d_bonded_e, 0, sizeof(long long), st));
+  if (en && e->nb14)
+    SNB_CUDA_TRY(cudaMemsetAsync(e->d_nb14_sums, 0, sizeof(long long) * 2, st));
   int rc = engine_forces(e, crd, step, en, vi, e->steps_done == 0, st);
   if (rc) return rc;
   e->steps_done++;
   if (en || vi) {
-    rc = launch_totals(e->n, e->acc, e->d_isum, nullptr, e->pme.d_sums, e->lrc_energy,
+    rc = launch_totals(e->n, e->acc, e->d_isum, e->nb14 ? e->d_nb14_sums : nullptr,
+                       e->pme.d_sums, e->lrc_energy,
                        e->lrc_virial, d_totals, en, vi, e->pme.reciprocal, st);
     if (rc) return rc;
   }
   return launch_unpack(e->n, e->nl.d_inv_perm, e->acc, e->accum,
                        reinterpret_cast<float3*>(frc), nullptr, nullptr, nullptr, nullptr,
                        en, vi, st);
+}
+
+extern "C" int snb_nb14_create(int atom_numbers, int nb14_numbers, const int* h_atom_a,
+                               const int* h_atom_b, const float* h_A, const float* h_B,
+                               const float* h_cf_scale_factor, snb_nb14** out) {
+  if (!out) return fail(kBadInput, "nb14_create: null out");
+  *out = nullptr;
+  if (atom_numbers <= 0) return fail(kBadInput, "nb14_create: atom_numbers must be > 0");
+  snb_nb14* h = new snb_nb14();
+  h->n = atom_numbers;
+  int rc = nb14_init(h->p, nb14_numbers, h_atom_a, h_atom_b, h_A, h_B, h_cf_scale_factor,
+                     atom_numbers);
+  if (!rc) rc = acc_init(h->acc, atom_numbers);
+  if (!rc) {
+    cudaError_t ce = cudaMalloc(&h->d_sums, sizeof(long long) * 2);
+    if (ce == cudaSuccess) ce = cudaMemset(h->d_sums, 0, sizeof(long long) * 2);
+    if (ce != cudaSuccess) rc = fail(kCudaError, cudaGetErrorString(ce));
+  }
+  if (rc) {
+    nb14_free(h->p);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return kOk;
+}
+
+extern "C" int snb_nb14_force(snb_nb14* h, const float* crd, const float* charge,
+                              snb_boundary boundary, float* frc, int need_atom_energy,
+                              float* atom_energy, int need_virial, float* atom_virial,
+                              void* stream) {
+  if (!h || !crd || !charge || !frc) return fail(kBadInput, "nb14_force: bad argument");
+  cudaStream_t st = S(stream);
+  const bool en = need_atom_energy != 0, vi = need_virial != 0;
+  if (en) SNB_CUDA_TRY(cudaMemsetAsync(h->d_sums, 0, sizeof(long long) * 2, st));
+  int rc = launch_nb14(h->p, reinterpret_cast<const float3*>(crd), charge, cell_of(boundary),
+                       rcell_of(boundary), nullptr, h->acc, en, vi, true,
+                       en ? h->d_sums : nullptr, st);
+  if (rc) return rc;
+  return launch_unpack(h->n, nullptr, h->acc, h->accum, reinterpret_cast<float3*>(frc),
+                       en ? atom_energy : nullptr, nullptr, nullptr, vi ? atom_virial : nullptr,
+                       en, vi, st);
+}
+
+extern "C" int snb_nb14_energy_sums(snb_nb14* h, float* h_lj, float* h_ee, void* stream) {
+  if (!h || !h_lj || !h_ee) return fail(kBadInput, "nb14_energy_sums: null argument");
+  long long v[2];
+  cudaStream_t st = S(stream);
+  SNB_CUDA_TRY(cudaMemcpyAsync(v, h->d_sums, sizeof(v), cudaMemcpyDeviceToHost, st));
+  SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  *h_ee = (float)((double)v[1] * kEnergyScaleInv);
+  *h_lj = (float)((double)(v[0] - v[1]) * kEnergyScaleInv);
+  return kOk;
+}
+
+extern "C" int snb_nb14_destroy(snb_nb14* h) {
+  if (!h) return kOk;
+  nb14_free(h->p);
+  acc_free(h->acc);
+  cudaFree(h->d_sums);
+  delete h;
+  return kOk;
+}
+
+extern "C" int snb_engine_set_nb14(snb_engine* e, snb_nb14* nb14) {
+  if (!e) return fail(kBadInput, "engine_set_nb14: null handle");
+  if (nb14) {
+    if (e->nsys > 0) return fail(kNotSupported, "engine_set_nb14: batch engines");
+    if (e->accum != kAccumFixed)
+      return fail(kNotSupported, "engine_set_nb14: fixed-point accumulation required");
+    if (nb14->n != e->n) return fail(kBadInput, "engine_set_nb14: atom count differs");
+    if (!e->d_nb14_sums) {
+      SNB_CUDA_TRY(cudaMalloc(&e->d_nb14_sums, sizeof(long long) * 2));
+      SNB_CUDA_TRY(cudaMemset(e->d_nb14_sums, 0, sizeof(long long) * 2));
+    }
+  }
+  e->nb14 = nb14;
+  if (e->graph_exec) {  // the captured step holds the previous set of terms
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+  }
+  return kOk;
 }
 
 extern "C" int snb_engine_update_box(snb_engine* e, snb_boundary boundary) {
@@ -1745,6 +1851,7 @@ extern "C" int snb_engine_destroy(snb_engine* e) {
   cudaFree(e->d_excl_list);
   cudaFree(e->d_isum);
   cudaFree(e->d_bonded_e);
+  cudaFree(e->d_nb14_sums);
   cudaFree(e->d_totals_scratch);
   cudaFree(e->d_snap_crd);
   cudaFree(e->d_snap_vel);

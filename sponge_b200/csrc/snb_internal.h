@@ -223,6 +223,24 @@ struct PairArgs {
 int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool ortho, cudaStream_t st);
 
+// 1-4 terms (NON_BOND_14): pairs with their scaled A', B' and Coulomb scale.
+struct NB14 {
+  int m = 0;
+  int* d_a = nullptr;
+  int* d_b = nullptr;
+  float* d_A = nullptr;
+  float* d_B = nullptr;
+  float* d_cf = nullptr;
+};
+int nb14_init(NB14& p, int m, const int* a, const int* b, const float* A, const float* B,
+              const float* cf, int atom_numbers);
+void nb14_free(NB14& p);
+// map (may be null): caller index -> accumulator slot; per_atom: per-atom
+// energies into acc; sums (may be null): fixed-point {LJ + Coulomb, Coulomb}
+int launch_nb14(const NB14& p, const float3* crd, const float* charge, const Cell& cell,
+                const Cell& rcell, const int* map, Accumulators& acc, bool energy,
+                bool virial, bool per_atom, long long* sums, cudaStream_t st);
+
 // Soft-core LJ + direct Coulomb (LJ_SOFT_CORE).
 struct SoftArgs {
   int n;

@@ -2,7 +2,9 @@
 // on the host: the LJ and soft-core LJ tables (Xponge::Native_Load_LJ,
 // xponge/load/native/lj.hpp:9-67; Native_Load_LJ_Soft_Core, lj_soft.hpp),
 // the subsystem division, the exclusion lists, charges and masses
-// (xponge/load/native/md_core.hpp), and the binary frc trajectory
+// (xponge/load/native/md_core.hpp), the 1-4 pair list
+// (Xponge::Native_Load_NB14, xponge/load/native/nb14.hpp:8-101), and the
+// binary frc trajectory
 // (MD_core/output.hpp:1691-1700).
 //
 // Each reader reads the file's counts first.  Called with NULL arrays it
@@ -11,6 +13,7 @@
 // and "%d"; A' = 12 A and B' = 6 B as the tables are stored).
 #include <cstdio>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "snb_internal.h"
@@ -171,6 +174,54 @@ extern "C" int snb_read_exclude_in_file(const char* path, int* atom_numbers,
   if (count != m)
     return fail(kBadInput, "the format of exclude_in_file is not right "
                            "(excluded_atom_numbers is not right)");
+  return kOk;
+}
+
+extern "C" int snb_read_nb14_in_file(const char* path, const char* extra_path,
+                                     int atom_numbers, const int* h_atom_LJ_type,
+                                     const float* h_LJ_A, const float* h_LJ_B,
+                                     int* nb14_numbers, int* h_atom_a, int* h_atom_b,
+                                     float* h_A, float* h_B, float* h_cf_scale_factor) {
+  if (!nb14_numbers) return fail(kBadInput, "read_nb14_in_file: null count");
+  File f(path), fx(extra_path);
+  if (path && !f.fp) return no_file("nb14_in_file", path);
+  if (extra_path && !fx.fp) return no_file("nb14_extra_in_file", extra_path);
+  int n = 0, nx = 0;
+  if (f.fp && fscanf(f.fp, "%d", &n) != 1) return bad_format("nb14_in_file");
+  if (fx.fp && fscanf(fx.fp, "%d", &nx) != 1) return bad_format("nb14_extra_in_file");
+  if (n < 0) return bad_format("nb14_in_file");
+  if (nx < 0) return bad_format("nb14_extra_in_file");
+  *nb14_numbers = n + nx;
+  const bool any = h_atom_a || h_atom_b || h_A || h_B || h_cf_scale_factor;
+  if (!any) return kOk;
+  if (!h_atom_a || !h_atom_b || !h_A || !h_B || !h_cf_scale_factor)
+    return fail(kBadInput, "read_nb14_in_file: give all five arrays or none");
+  if (n > 0 && (!h_atom_LJ_type || !h_LJ_A || !h_LJ_B))
+    return fail(kBadInput, "'nb14_in_file' should be provided with initialized LJ parameters");
+  auto in_range = [&](int a) { return a >= 0 && a < atom_numbers; };
+  // the extra file's rows come first, with their own A, B (times 12 and 6)
+  for (int i = 0; i < nx; ++i) {
+    if (fscanf(fx.fp, "%d %d %f %f %f", &h_atom_a[i], &h_atom_b[i], &h_A[i], &h_B[i],
+               &h_cf_scale_factor[i]) != 5)
+      return bad_format("nb14_extra_in_file");
+    if (!in_range(h_atom_a[i]) || !in_range(h_atom_b[i]))
+      return fail(kBadInput, "nb14_extra_in_file: atom index out of range");
+    h_A[i] *= 12.0f;
+    h_B[i] *= 6.0f;
+  }
+  for (int i = nx; i < nx + n; ++i) {
+    float lj_scale = 0.0f;
+    if (fscanf(f.fp, "%d %d %f %f", &h_atom_a[i], &h_atom_b[i], &lj_scale,
+               &h_cf_scale_factor[i]) != 4)
+      return bad_format("nb14_in_file");
+    if (!in_range(h_atom_a[i]) || !in_range(h_atom_b[i]))
+      return fail(kBadInput, "nb14_in_file: atom index out of range");
+    int lo = h_atom_LJ_type[h_atom_a[i]], hi = h_atom_LJ_type[h_atom_b[i]];
+    if (lo > hi) std::swap(lo, hi);
+    const int pair = hi * (hi + 1) / 2 + lo;
+    h_A[i] = lj_scale * h_LJ_A[pair];
+    h_B[i] = lj_scale * h_LJ_B[pair];
+  }
   return kOk;
 }
 

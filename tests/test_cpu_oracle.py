@@ -15,7 +15,7 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _FIXTURES = sorted(f for f in os.listdir(os.path.join(HERE, "golden")) if f.endswith(".npz"))
-GOLDEN = [f for f in _FIXTURES if not f.startswith(("soft_", "boxchange_", "amber_"))]
+GOLDEN = [f for f in _FIXTURES if not f.startswith(("soft_", "boxchange_", "amber_", "nb14_"))]
 SOFT = [f for f in _FIXTURES if f.startswith("soft_")]
 BOXCHANGE = [f for f in _FIXTURES if f.startswith("boxchange_")]
 
