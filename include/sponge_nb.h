@@ -102,6 +102,7 @@ typedef struct snb_lj_soft snb_lj_soft;
 typedef struct snb_pme snb_pme;
 typedef struct snb_engine snb_engine;
 typedef struct snb_nb14 snb_nb14;
+typedef struct snb_settle snb_settle;
 
 /* ---------------------------------------------------------------- misc */
 int snb_version(void);
@@ -348,6 +349,14 @@ int snb_engine_set_soft_core(snb_engine* e, snb_lj_soft* soft);
  * of the totals.  `nb14` must outlive the engine's use of it; NULL removes
  * them.  Single boxes, fixed-point accumulation. */
 int snb_engine_set_nb14(snb_engine* e, snb_nb14* nb14);
+/* SETTLE in the engine's MD steps (main.cpp:1705,1772 around the NVE
+ * leap-frog, v_factor = x_factor = 1): the rigid triangles and pairs of
+ * `settle` (created for the same atom count) are remembered before each
+ * coordinate update and put back on their geometry after it; the neighbor
+ * refresh check runs on the constrained positions.  A rigid pair without a
+ * real update makes the MD call return SNB_ERR_BAD_INPUT.  NULL removes it.
+ * Single boxes. */
+int snb_engine_set_settle(snb_engine* e, snb_settle* settle);
 int snb_engine_md_steps(snb_engine* e, float* crd, float* vel,
                         const float* inverse_mass, float dt, int first_step,
                         int steps, void* stream);
@@ -408,6 +417,40 @@ int snb_nb14_force(snb_nb14* h, const float* crd, const float* charge,
  * nb14_LJ and nb14_EE (host sync). */
 int snb_nb14_energy_sums(snb_nb14* h, float* h_lj, float* h_ee, void* stream);
 int snb_nb14_destroy(snb_nb14* h);
+
+/* -------------------------------------------------------------- SETTLE */
+/* SETTLE (constrain/settle.h, constrain/settle.cpp).  Initial
+ * (settle.cpp:483-712): the constraint pairs (atom_i, atom_j, constant_r)
+ * are sorted, as the reference does, into rigid triangles (three atoms with
+ * two constraints each that close a triangle; A = the lowest index), rigid
+ * pairs (two atoms constrained only to each other) and the remaining pairs,
+ * which SETTLE leaves to SHAKE.  h_mass [atom_numbers] sets each group's
+ * masses and canonical frame. */
+int snb_settle_create(int atom_numbers, int constrain_pair_numbers, const int* h_atom_i,
+                      const int* h_atom_j, const float* h_constant_r, const float* h_mass,
+                      snb_settle** out);
+/* triangle_numbers, pair_numbers and the constraint pairs left over (their
+ * indices in the creation order into h_remaining_pairs when not NULL). */
+int snb_settle_counts(snb_settle* h, int* triangle_numbers, int* pair_numbers,
+                      int* remaining_pair_numbers, int* h_remaining_pairs);
+/* Remember_Last_Coordinates (settle.cpp:714-730): the displacements B - A,
+ * C - A and j - i at the start of the step. */
+int snb_settle_remember_last_coordinates(snb_settle* h, const float* crd,
+                                         snb_boundary boundary, void* stream);
+/* Do_SETTLE (settle.cpp:798-882) after the coordinate update: crd and vel
+ * [N*3] are corrected in place with the step dt and the integrator's
+ * v_factor / x_factor (1 and 1 for leap-frog NVE); with need_pressure the
+ * constraint virial / V is added to d_stress[6] (LTMatrix3 order).  A rigid
+ * pair without a real update is left unchanged and recorded: read it with
+ * snb_settle_status. */
+int snb_settle_do(snb_settle* h, float* crd, snb_boundary boundary, float* vel, float dt,
+                  float v_factor, float x_factor, int need_pressure, float* d_stress,
+                  void* stream);
+/* SNB_ERR_BAD_INPUT, with *invalid_pair the pair's index, when a call since
+ * the last status had a rigid pair without a real update; else SNB_OK and
+ * -1 (host sync; clears the record). */
+int snb_settle_status(snb_settle* h, int* invalid_pair, void* stream);
+int snb_settle_destroy(snb_settle* h);
 
 /* ------------------------------------------- native inputs and outputs */
 /* SPONGE's native text inputs of this path, read on the host.  Each reader

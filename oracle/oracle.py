@@ -74,6 +74,11 @@ class Oracle:
         L.snbo_nb14_f64.argtypes = [
             ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
             _f64p, _f64p, _f64p, _f64p]
+        L.snbo_shake_f64.restype = ctypes.c_int
+        L.snbo_shake_f64.argtypes = [
+            ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f64p, _f64p, _f32p, _f32p, _f64p,
+            _f64p, _f64p, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+            _f64p]
         L.snbo_pme_f64.restype = None
         L.snbo_pme_f64.argtypes = [
             ctypes.c_int, _f32p, _f32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int,
@@ -167,6 +172,23 @@ class Oracle:
             _c(s.charge, np.float32), s.cell(), s.rcell(), frc, ae, vir, sums)
         return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6),
                     lj=sums[0], ee=sums[1])
+
+    def shake_f64(self, cell, rcell, ai, aj, r0, mass, crd_old, crd, vel, dt,
+                  v_factor=1.0, x_factor=1.0, tol=1e-13):
+        """Constraints (ai, aj, r0) solved by iterated SHAKE in FP64 from the
+        unconstrained crd with the bond vectors of crd_old; returns the new
+        crd, vel, the constraint virial [6] and the sweeps used."""
+        n, m = len(mass), len(ai)
+        x = np.array(crd, np.float64).reshape(-1).copy()
+        v = np.array(vel, np.float64).reshape(-1).copy()
+        vir = np.zeros(6)
+        z = np.zeros(1, np.int32)
+        sweeps = self.lib.snbo_shake_f64(
+            n, m, _c(ai, np.int32) if m else z, _c(aj, np.int32) if m else z,
+            _c(r0, np.float64) if m else np.zeros(1), _c(mass, np.float64),
+            _c(cell, np.float32), _c(rcell, np.float32),
+            _c(crd_old, np.float64).reshape(-1), x, v, dt, v_factor, x_factor, tol, vir)
+        return dict(crd=x.reshape(n, 3), vel=v.reshape(n, 3), virial=vir, sweeps=sweeps)
 
     def pme_f64(self, s, grid, beta, want_phi=False):
         n = s.n
@@ -282,6 +304,9 @@ class ReferenceCPU:
         L.ref_nb14.restype = ctypes.c_int
         L.ref_nb14.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p,
                                _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f64p]
+        L.ref_settle.restype = ctypes.c_int
+        L.ref_settle.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p,
+                                 _f32p, _f32p, _f32p, ctypes.c_float, _f32p, _i32p, _i32p]
         L.ref_native_load.restype = ctypes.c_int
         L.ref_native_load.argtypes = [ctypes.c_char_p]
         L.ref_native_get.restype = ctypes.c_longlong
@@ -435,6 +460,26 @@ class ReferenceCPU:
             raise RuntimeError("reference nb14 failed")
         return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6),
                     lj=float(sums[0]), ee=float(sums[1]))
+
+    def settle(self, cell, ai, aj, r0, mass, crd_old, crd, vel, dt):
+        """SETTLE of the reference on one step (see ref_settle): the new crd
+        and vel, stress[6] (virial / V), {triangles, pairs, left over} and the
+        atom pairs of the constraints left over."""
+        n, m = len(mass), len(ai)
+        x = np.array(crd, np.float32).reshape(-1).copy()
+        v = np.array(vel, np.float32).reshape(-1).copy()
+        stress = np.zeros(6, np.float32)
+        counts = np.zeros(3, np.int32)
+        left = np.zeros(2 * max(m, 1), np.int32)
+        pad = lambda a, dt_: np.ascontiguousarray(a, dt_) if m else np.zeros(1, dt_)
+        rc = self.lib.ref_settle(n, m, pad(ai, np.int32), pad(aj, np.int32),
+                                 pad(r0, np.float32), _c(mass, np.float32),
+                                 _c(cell, np.float32), _c(crd_old, np.float32).reshape(-1),
+                                 x, v, dt, stress, counts, left)
+        if rc != 0:
+            raise RuntimeError("reference SETTLE failed")
+        return dict(crd=x.reshape(n, 3), vel=v.reshape(n, 3), stress=stress,
+                    counts=counts, left=left[:2 * counts[2]].reshape(-1, 2))
 
     def box_change(self, box):
         """Main_Box_Change for a small change to a cubic box of length `box`:

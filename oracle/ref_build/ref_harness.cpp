@@ -1,7 +1,7 @@
 /* TEST INFRASTRUCTURE ONLY -- builds the reference's own CPU implementation
  * of the nonbonded hot path (its unmodified neighbor_list.cpp,
- * Lennard_Jones_force.cpp, LJ_soft_core.cpp, PM_force.cpp, nb14.cpp and
- * common.cpp,
+ * Lennard_Jones_force.cpp, LJ_soft_core.cpp, PM_force.cpp, nb14.cpp,
+ * settle.cpp and common.cpp,
  * compiled from the reference tree by oracle/Makefile) into oracle/_ref/.
  *
  * The reference's MD_core, Domain_decomposition, Xponge loaders and CONTROLLER
@@ -19,6 +19,7 @@
 #include "Lennard_Jones_force/LJ_soft_core.h"
 #include "Lennard_Jones_force/Lennard_Jones_force.h"
 #include "PM_force/PM_force.h"
+#include "constrain/settle.h"
 #include "nb14/nb14.h"
 #include "neighbor_list/neighbor_list.h"
 #include "ref_controller.h"
@@ -427,6 +428,72 @@ extern "C"
                            nb.d_atom_b_local, nb.d_A_local, nb.d_B_local,
                            nb.d_cf_scale_factor_local, nb.d_num_nb14_local};
             for (void* p : dev) deviceFree(p);
+        });
+        return 0;
+    }
+
+    /* SETTLE on one step: Initial from the constraint pairs (atom_i,
+     * atom_j, constant_r) and masses, Get_Local over all n atoms,
+     * Remember_Last_Coordinates on crd_old, then Do_SETTLE with the step
+     * dt (v_factor = x_factor = 1) on crd / vel, which are updated in place;
+     * stress[6] receives the constraint virial / V.  counts = {triangles,
+     * rigid pairs, constraint pairs left over}; left [2 m] receives the
+     * atoms (i, j) of the pairs left over. */
+    int ref_settle(int n, int m, const int* ai, const int* aj, const float* r0,
+                   const float* mass, const float* cell6, const float* crd_old,
+                   float* crd, float* vel, float dt, float* stress, int* counts,
+                   int* left)
+    {
+        REF_TRY({
+            CONSTRAIN c;
+            c.atom_numbers = n;
+            c.dt = dt;
+            c.constrain_pair_numbers = m;
+            c.h_constrain_pair = (CONSTRAIN_PAIR*)malloc(sizeof(CONSTRAIN_PAIR) * (m > 0 ? m : 1));
+            c.d_constrain_pair = (CONSTRAIN_PAIR*)malloc(sizeof(CONSTRAIN_PAIR) * (m > 0 ? m : 1));
+            for (int p = 0; p < m; ++p)
+            {
+                c.h_constrain_pair[p].atom_i_serial = ai[p];
+                c.h_constrain_pair[p].atom_j_serial = aj[p];
+                c.h_constrain_pair[p].constant_r = r0[p];
+                c.h_constrain_pair[p].constrain_k =
+                    mass[ai[p]] * mass[aj[p]] / (mass[ai[p]] + mass[aj[p]]);
+            }
+            std::vector<float> h_mass(mass, mass + n);
+            SETTLE s;
+            s.Initial(&controller, &c, h_mass.data());
+            counts[0] = s.triangle_numbers;
+            counts[1] = s.pair_numbers;
+            counts[2] = c.constrain_pair_numbers;
+            for (int p = 0; p < c.constrain_pair_numbers; ++p)
+            {
+                left[2 * p] = c.h_constrain_pair[p].atom_i_serial;
+                left[2 * p + 1] = c.h_constrain_pair[p].atom_j_serial;
+            }
+            if (s.is_initialized)
+            {
+                std::vector<char> label(n, 1);
+                std::vector<int> id(n);
+                for (int i = 0; i < n; ++i) id[i] = i;
+                s.Get_Local(id.data(), label.data(), n);
+                Boundary bd;
+                bd.policy = BoundaryPolicy::Periodic;
+                bd.cell = LTMatrix3(cell6[0], cell6[1], cell6[2], cell6[3],
+                                    cell6[4], cell6[5]);
+                bd.rcell = Invert_Lower_Triangular_Cell(bd.cell);
+                s.Remember_Last_Coordinates(
+                    reinterpret_cast<const VECTOR*>(crd_old), bd);
+                LTMatrix3 st = {0, 0, 0, 0, 0, 0};
+                s.Do_SETTLE(&controller, id.data(), h_mass.data(),
+                            reinterpret_cast<VECTOR*>(crd), bd,
+                            reinterpret_cast<VECTOR*>(vel), 1, &st);
+                stress[0] = st.a11;
+                stress[1] = st.a21;
+                stress[2] = st.a22;
+                stress[3] = st.a31;
+                stress[4] = st.a32;
+                stress[5] = st.a33;
+            }
         });
         return 0;
     }

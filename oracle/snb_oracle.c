@@ -632,6 +632,82 @@ SNBO_API void snbo_nb14_f64(int m, const int* ia, const int* ib, const float* A,
 }
 
 /* ------------------------------------------------------------------ */
+/* Rigid-geometry constraints in FP64 by iterated SHAKE (Ryckaert,
+ * Ciccotti and Berendsen, J. Comput. Phys. 23, 327 (1977)): every listed
+ * constraint (ai, aj, r0) moves its atoms along the bond vector at the
+ * start of the step (from crd_old) until each length is r0 to `tol`
+ * relative.  SETTLE (constrain/settle.cpp) solves the same equations
+ * analytically, so for its rigid triangles and pairs the two agree.
+ * crd / vel are updated in place: vel += v_factor / (dt x_factor) times
+ * the position change.  virial[6] (LTMatrix3 order, off-diagonal pairs
+ * summed) = sum over constraints of F (x) s_old with F = the total
+ * multiplier times s_old / (dt^2 x_factor).  Returns the sweeps used, or
+ * -1 without convergence in 10000 sweeps. */
+static void min_image_d(const double* a, const double* b, const float* cell,
+                        const float* rcell, double* out)
+{
+    double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    double sx = dx * rcell[0] + dy * rcell[1] + dz * rcell[3];
+    double sy = dy * rcell[2] + dz * rcell[4];
+    double sz = dz * rcell[5];
+    double fx = floor(sx + 0.5), fy = floor(sy + 0.5), fz = floor(sz + 0.5);
+    out[0] = dx - (fx * cell[0] + fy * cell[1] + fz * cell[3]);
+    out[1] = dy - (fy * cell[2] + fz * cell[4]);
+    out[2] = dz - fz * cell[5];
+}
+
+SNBO_API int snbo_shake_f64(int n, int m, const int* ai, const int* aj,
+                            const double* r0, const double* mass,
+                            const float* cell, const float* rcell,
+                            const double* crd_old, double* crd, double* vel,
+                            double dt, double v_factor, double x_factor,
+                            double tol, double* virial)
+{
+    double* s = (double*)malloc(sizeof(double) * 3 * (m > 0 ? m : 1));
+    double* g = (double*)calloc(m > 0 ? m : 1, sizeof(double));
+    double* x0 = (double*)malloc(sizeof(double) * 3 * (n > 0 ? n : 1));
+    memcpy(x0, crd, sizeof(double) * 3 * n);
+    for (int k = 0; k < m; ++k)
+        min_image_d(crd_old + 3 * aj[k], crd_old + 3 * ai[k], cell, rcell, s + 3 * k);
+    int sweep = 0, done = 0;
+    for (; sweep < 10000 && !done; ++sweep)
+    {
+        done = 1;
+        for (int k = 0; k < m; ++k)
+        {
+            int i = ai[k], j = aj[k];
+            double d[3];
+            min_image_d(crd + 3 * j, crd + 3 * i, cell, rcell, d);
+            double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            double t2 = r0[k] * r0[k];
+            if (fabs(d2 - t2) > tol * t2) done = 0;
+            double ds = d[0] * s[3 * k] + d[1] * s[3 * k + 1] + d[2] * s[3 * k + 2];
+            double wi = 1.0 / mass[i], wj = 1.0 / mass[j];
+            double gk = (t2 - d2) / (2.0 * ds * (wi + wj));
+            for (int c = 0; c < 3; ++c)
+            {
+                crd[3 * i + c] -= gk * wi * s[3 * k + c];
+                crd[3 * j + c] += gk * wj * s[3 * k + c];
+            }
+            g[k] += gk;
+        }
+    }
+    for (int i = 0; i < 3 * n; ++i)
+        vel[i] += v_factor / (dt * x_factor) * (crd[i] - x0[i]);
+    for (int c = 0; c < 6; ++c) virial[c] = 0.0;
+    for (int k = 0; k < m; ++k)
+    {
+        double f[3], c = g[k] / (dt * dt * x_factor);
+        for (int q = 0; q < 3; ++q) f[q] = c * s[3 * k + q];
+        virial_add(virial, f, s + 3 * k, 1.0);
+    }
+    free(s);
+    free(g);
+    free(x0);
+    return done ? sweep : -1;
+}
+
+/* ------------------------------------------------------------------ */
 /* PME reciprocal part in FP64 (PM_force.cpp:541-612 tables, 699-893 spread and
  * gather, 896-919 + 1142-1166 energies, 1024-1068 virial). */
 

@@ -62,6 +62,9 @@ EXPORTED = [
     "snb_engine_create", "snb_batch_create", "snb_engine_force", "snb_engine_set_bonded",
     "snb_engine_set_soft_core", "snb_engine_update_box", "snb_engine_set_nb14",
     "snb_nb14_create", "snb_nb14_force", "snb_nb14_energy_sums", "snb_nb14_destroy",
+    "snb_engine_set_settle", "snb_settle_create", "snb_settle_counts",
+    "snb_settle_remember_last_coordinates", "snb_settle_do", "snb_settle_status",
+    "snb_settle_destroy",
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_profile_steps",
     "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
     "snb_engine_destroy",
@@ -141,6 +144,13 @@ _SIGS = {
     "snb_nb14_force": (_I, [_P, _P, _P, snb_boundary, _P, _I, _P, _I, _P, _P]),
     "snb_nb14_energy_sums": (_I, [_P, _P, _P, _P]),
     "snb_nb14_destroy": (_I, [_P]),
+    "snb_engine_set_settle": (_I, [_P, _P]),
+    "snb_settle_create": (_I, [_I, _I, _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    "snb_settle_counts": (_I, [_P, _P, _P, _P, _P]),
+    "snb_settle_remember_last_coordinates": (_I, [_P, _P, snb_boundary, _P]),
+    "snb_settle_do": (_I, [_P, _P, snb_boundary, _P, _F, _F, _F, _I, _P, _P]),
+    "snb_settle_status": (_I, [_P, _P, _P]),
+    "snb_settle_destroy": (_I, [_P]),
     "snb_read_nb14_in_file": (_I, [ctypes.c_char_p, ctypes.c_char_p, _I, _P, _P, _P, _P,
                                    _P, _P, _P, _P, _P]),
     "snb_read_lj_in_file": (_I, [ctypes.c_char_p, _P, _P, _P, _P, _P]),

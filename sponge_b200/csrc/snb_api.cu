@@ -96,6 +96,10 @@ struct snb_nb14 {
   long long* d_sums = nullptr;  // [2] {LJ + Coulomb, Coulomb} of the last energy call
 };
 
+struct snb_settle {
+  Settle s;
+};
+
 struct snb_engine {
   snb_options opt;
   int n = 0;
@@ -137,6 +141,7 @@ struct snb_engine {
   double lrc_energy_lj = 0.0, lrc_virial_lj = 0.0;  // the plain LJ module's
   snb_lj_soft* soft = nullptr;  // soft-core pair terms in place of plain LJ
   snb_nb14* nb14 = nullptr;     // 1-4 terms beside the excluded correction
+  snb_settle* settle = nullptr;  // rigid triangles / pairs after the coordinate update
   long long* d_nb14_sums = nullptr;  // [2]
   // launch shapes picked by snb_engine_autotune
   int pair_unroll = 4;
@@ -1395,6 +1400,87 @@ extern "C" int snb_engine_set_nb14(snb_engine* e, snb_nb14* nb14) {
   return kOk;
 }
 
+extern "C" int snb_settle_create(int atom_numbers, int constrain_pair_numbers,
+                                 const int* h_atom_i, const int* h_atom_j,
+                                 const float* h_constant_r, const float* h_mass,
+                                 snb_settle** out) {
+  if (!out) return fail(kBadInput, "settle_create: null out");
+  *out = nullptr;
+  snb_settle* h = new snb_settle();
+  int rc = settle_init(h->s, atom_numbers, constrain_pair_numbers, h_atom_i, h_atom_j,
+                       h_constant_r, h_mass);
+  if (rc) {
+    settle_free(h->s);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return kOk;
+}
+
+extern "C" int snb_settle_counts(snb_settle* h, int* triangle_numbers, int* pair_numbers,
+                                 int* remaining_pair_numbers, int* h_remaining_pairs) {
+  if (!h) return fail(kBadInput, "settle_counts: null handle");
+  if (triangle_numbers) *triangle_numbers = h->s.nt;
+  if (pair_numbers) *pair_numbers = h->s.np;
+  if (remaining_pair_numbers) *remaining_pair_numbers = (int)h->s.remaining.size();
+  if (h_remaining_pairs)
+    for (size_t k = 0; k < h->s.remaining.size(); ++k) h_remaining_pairs[k] = h->s.remaining[k];
+  return kOk;
+}
+
+extern "C" int snb_settle_remember_last_coordinates(snb_settle* h, const float* crd,
+                                                    snb_boundary boundary, void* stream) {
+  if (!h || !crd) return fail(kBadInput, "settle_remember: bad argument");
+  return launch_settle_remember(h->s, reinterpret_cast<const float3*>(crd), cell_of(boundary),
+                                rcell_of(boundary), S(stream));
+}
+
+extern "C" int snb_settle_do(snb_settle* h, float* crd, snb_boundary boundary, float* vel,
+                             float dt, float v_factor, float x_factor, int need_pressure,
+                             float* d_stress, void* stream) {
+  if (!h || !crd || !vel || !(dt > 0.f) || (need_pressure && !d_stress))
+    return fail(kBadInput, "settle_do: bad argument");
+  return launch_settle(h->s, reinterpret_cast<float3*>(crd), reinterpret_cast<float3*>(vel),
+                       cell_of(boundary), rcell_of(boundary), dt, v_factor, x_factor,
+                       need_pressure ? d_stress : nullptr, S(stream));
+}
+
+extern "C" int snb_settle_status(snb_settle* h, int* invalid_pair, void* stream) {
+  if (!h || !invalid_pair) return fail(kBadInput, "settle_status: bad argument");
+  int v = 0;
+  cudaStream_t st = S(stream);
+  SNB_CUDA_TRY(cudaMemcpyAsync(&v, h->s.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SNB_CUDA_TRY(cudaMemsetAsync(h->s.d_err, 0, sizeof(int), st));
+  SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  *invalid_pair = v - 1;
+  return v ? fail(kBadInput, "SETTLE: rigid pair " + std::to_string(v - 1) +
+                                 " has no real position update")
+           : kOk;
+}
+
+extern "C" int snb_settle_destroy(snb_settle* h) {
+  if (!h) return kOk;
+  settle_free(h->s);
+  delete h;
+  return kOk;
+}
+
+extern "C" int snb_engine_set_settle(snb_engine* e, snb_settle* settle) {
+  if (!e) return fail(kBadInput, "engine_set_settle: null handle");
+  if (settle) {
+    if (e->nsys > 0) return fail(kNotSupported, "engine_set_settle: batch engines");
+    if (settle->s.n != e->n) return fail(kBadInput, "engine_set_settle: atom count differs");
+  }
+  e->settle = settle;
+  if (e->graph_exec) {  // the captured step holds the previous integration
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+  }
+  return kOk;
+}
+
 extern "C" int snb_engine_update_box(snb_engine* e, snb_boundary boundary) {
   if (!e) return fail(kBadInput, "engine_update_box: null handle");
   if (e->nsys > 0) return fail(kNotSupported, "engine_update_box: batch engines");
@@ -1510,10 +1596,24 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
   // the next step's refresh check rides on the coordinate update
   const bool check = e->opt.nl_refresh_interval <= 0;
   const float permit = e->opt.skin * e->opt.nl_skin_permit;
+  if (e->settle && (rc = launch_settle_remember(e->settle->s,
+                                                reinterpret_cast<const float3*>(crd), e->cell,
+                                                e->rcell, st)))
+    return rc;
+  // with SETTLE the check waits for the constrained positions
+  const bool fused = check && !e->settle;
   rc = launch_leap_frog(e->n, e->nl.d_inv_perm, e->acc, reinterpret_cast<float3*>(crd),
                         reinterpret_cast<float3*>(vel), invm, dt,
-                        check ? e->nl.d_old_crd : nullptr, e->cell, e->rcell,
+                        fused ? e->nl.d_old_crd : nullptr, e->cell, e->rcell,
                         permit * permit, e->nl.d_flags, st, e->bv);
+  if (rc) return rc;
+  if (e->settle) {
+    rc = launch_settle(e->settle->s, reinterpret_cast<float3*>(crd),
+                       reinterpret_cast<float3*>(vel), e->cell, e->rcell, dt, 1.0f, 1.0f,
+                       nullptr, st);
+    if (!rc && check) rc = nl_check_moved(e->nl, crd, st);
+    if (rc) return rc;
+  }
   prof_mark(e, 7, st);
   return rc;
 }
@@ -1572,6 +1672,16 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
     bool regrown = false;
     int rc = nl_check_overflow(e->nl, &regrown, st);
     if (rc) return rc;
+    if (e->settle) {
+      int bad = 0;
+      SNB_CUDA_TRY(cudaMemcpyAsync(&bad, e->settle->s.d_err, sizeof(int),
+                                   cudaMemcpyDeviceToHost, st));
+      SNB_CUDA_TRY(cudaStreamSynchronize(st));
+      if (bad)
+        return fail(kBadInput, "SETTLE: rigid pair " + std::to_string(bad - 1) +
+                                   " has no real position update; reduce the time step or "
+                                   "minimise the input");
+    }
     if (regrown) {
       if (e->opt.nl_throw_error_when_overflow)
         return fail(kOverflow, "neighbor list overflow");

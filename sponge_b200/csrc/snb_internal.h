@@ -153,6 +153,9 @@ int nl_rebuild(NeighborList& nl, const float* crd, const int* atom_local,
                const int* excl_start, const int* excl_list, const int* excl_numbers,
                cudaStream_t st);
 int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st);
+// Raises the need flag when an atom of crd is more than skin * skin_permit
+// from where it was at the last build (single boxes).
+int nl_check_moved(NeighborList& nl, const float* crd, cudaStream_t st);
 int nl_force_next(NeighborList& nl, cudaStream_t st);
 // A new rectangular box (single-box list): re-grid and force the next build.
 int nl_regrid(NeighborList& nl, const float* cell6);
@@ -224,6 +227,39 @@ int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool ortho, cudaStream_t st);
 
 // 1-4 terms (NON_BOND_14): pairs with their scaled A', B' and Coulomb scale.
+// Rigid triangle: atoms A, B, C, canonical frame (A at (0, ra), B at (rc, rb),
+// C at (rd, re) about the centre of mass) and masses.
+struct SettleTri {
+  int a, b, c;
+  float ra, rb, rc, rd, re;
+  float ma, mb, mc;
+};
+// Rigid pair i-j of length r0; k = 1 / (m_i + m_j).
+struct SettlePair {
+  int i, j;
+  float r0, k, mi, mj;
+};
+struct Settle {
+  int n = 0, nt = 0, np = 0;
+  std::vector<int> remaining;  // constraint pairs SETTLE leaves to SHAKE
+  SettleTri* d_tri = nullptr;
+  SettlePair* d_pair = nullptr;
+  float3* d_last_ba = nullptr;
+  float3* d_last_ca = nullptr;
+  float3* d_last_ab = nullptr;
+  long long* d_vir = nullptr;  // [6] constraint virial of the last call, fixed point
+  int* d_err = nullptr;        // 1 + index of a pair without a real solution, else 0
+};
+int settle_init(Settle& s, int n, int m, const int* ai, const int* aj, const float* r0,
+                const float* mass);
+void settle_free(Settle& s);
+int launch_settle_remember(const Settle& s, const float3* crd, const Cell& cell,
+                           const Cell& rcell, cudaStream_t st);
+// stress (may be null): += constraint virial / V.
+int launch_settle(const Settle& s, float3* crd, float3* vel, const Cell& cell,
+                  const Cell& rcell, float dt, float v_factor, float x_factor, float* stress,
+                  cudaStream_t st);
+
 struct NB14 {
   int m = 0;
   int* d_a = nullptr;

@@ -427,6 +427,15 @@ int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_
   return kOk;
 }
 
+int nl_check_moved(NeighborList& nl, const float* crd_f, cudaStream_t st) {
+  const float permit = nl.skin * nl.skin_permit;
+  k_check_refresh<false><<<ceil_div(nl.n, 256), 256, 0, st>>>(
+      nl.n, reinterpret_cast<const float3*>(crd_f), nl.d_old_crd, nl.cell, nl.rcell,
+      permit * permit, nl.d_flags, nl.bv);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
 int nl_force_next(NeighborList& nl, cudaStream_t st) {
   k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 1);
   SNB_CUDA_TRY(cudaGetLastError());
