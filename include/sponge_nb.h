@@ -357,6 +357,15 @@ int snb_engine_set_nb14(snb_engine* e, snb_nb14* nb14);
  * real update makes the MD call return SNB_ERR_BAD_INPUT.  NULL removes it.
  * Single boxes. */
 int snb_engine_set_settle(snb_engine* e, snb_settle* settle);
+/* Stress and pressure (MD_INFORMATION::Get_pressure, MD_core.cpp:1080-1107;
+ * MD_core/sys.hpp:14-85): d_out[0..5] = (W + sum_i m_i v_i (x) v_i) / V in
+ * LTMatrix3 order (kcal/mol/A^3, off-diagonal pairs summed), d_out[6] =
+ * their trace / 3 in bar (CONSTANT_PRES_CONVERTION).  W = the potential
+ * virial in slots 8..13 of d_totals (from snb_engine_force with
+ * need_virial; NULL leaves it out) plus, with SETTLE set, the constraint
+ * virial of the last MD step.  vel and mass [N] on the device. */
+int snb_engine_pressure(snb_engine* e, const float* vel, const float* mass,
+                        const double* d_totals, double* d_out, void* stream);
 int snb_engine_md_steps(snb_engine* e, float* crd, float* vel,
                         const float* inverse_mass, float dt, int first_step,
                         int steps, void* stream);

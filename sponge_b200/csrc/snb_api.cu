@@ -143,6 +143,7 @@ struct snb_engine {
   snb_nb14* nb14 = nullptr;     // 1-4 terms beside the excluded correction
   snb_settle* settle = nullptr;  // rigid triangles / pairs after the coordinate update
   long long* d_nb14_sums = nullptr;  // [2]
+  double* d_kin = nullptr;           // [6] scratch of the pressure call
   // launch shapes picked by snb_engine_autotune
   int pair_unroll = 4;
   int pair_blocks_per_sm = 0;
@@ -1466,6 +1467,19 @@ extern "C" int snb_settle_destroy(snb_settle* h) {
   return kOk;
 }
 
+extern "C" int snb_engine_pressure(snb_engine* e, const float* vel, const float* mass,
+                                   const double* d_totals, double* d_out, void* stream) {
+  if (!e || !vel || !mass || !d_out) return fail(kBadInput, "engine_pressure: bad argument");
+  if (e->nsys > 0) return fail(kNotSupported, "engine_pressure: batch engines");
+  if (!e->d_kin) SNB_CUDA_TRY(cudaMalloc(&e->d_kin, sizeof(double) * 6));
+  // 1 / V of the cell, as Get_Volume gives it (MD_core/sys.hpp:493-525)
+  const double inv_v = 1.0 / ((double)e->cell.a11 * e->cell.a22 * e->cell.a33);
+  return launch_pressure(e->n, reinterpret_cast<const float3*>(vel), mass,
+                         d_totals ? d_totals + 8 : nullptr,
+                         e->settle ? e->settle->s.d_vir : nullptr, inv_v, e->d_kin, d_out,
+                         S(stream));
+}
+
 extern "C" int snb_engine_set_settle(snb_engine* e, snb_settle* settle) {
   if (!e) return fail(kBadInput, "engine_set_settle: null handle");
   if (settle) {
@@ -1962,6 +1976,7 @@ extern "C" int snb_engine_destroy(snb_engine* e) {
   cudaFree(e->d_isum);
   cudaFree(e->d_bonded_e);
   cudaFree(e->d_nb14_sums);
+  cudaFree(e->d_kin);
   cudaFree(e->d_totals_scratch);
   cudaFree(e->d_snap_crd);
   cudaFree(e->d_snap_vel);

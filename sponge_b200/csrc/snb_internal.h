@@ -153,6 +153,11 @@ int nl_rebuild(NeighborList& nl, const float* crd, const int* atom_local,
                const int* excl_start, const int* excl_list, const int* excl_numbers,
                cudaStream_t st);
 int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st);
+// stress = (virial [6] (may be null) + constraint virial (fixed point, may be
+// null) + sum m v (x) v) * inv_v into out[0..5], pressure in bar into out[6].
+int launch_pressure(int n, const float3* vel, const float* mass, const double* virial,
+                    const long long* constraint_virial, double inv_v, double* scratch6,
+                    double* out, cudaStream_t st);
 // Raises the need flag when an atom of crd is more than skin * skin_permit
 // from where it was at the last build (single boxes).
 int nl_check_moved(NeighborList& nl, const float* crd, cudaStream_t st);
@@ -247,7 +252,7 @@ struct Settle {
   float3* d_last_ba = nullptr;
   float3* d_last_ca = nullptr;
   float3* d_last_ab = nullptr;
-  long long* d_vir = nullptr;  // [6] constraint virial of the last call, fixed point
+  long long* d_vir = nullptr;  // [6] constraint virial since the last remember, fixed point
   int* d_err = nullptr;        // 1 + index of a pair without a real solution, else 0
 };
 int settle_init(Settle& s, int n, int m, const int* ai, const int* aj, const float* r0,

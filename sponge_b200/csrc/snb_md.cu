@@ -235,6 +235,63 @@ int launch_totals(int n, Accumulators& acc, long long* isum, const long long* bo
   return kOk;
 }
 
+// Stress and pressure (MD_INFORMATION::Get_pressure, MD_core.cpp:1080-1107,
+// with Get_Stress_Potential_Contribution / Get_Stress_Kinetic_Contribution,
+// MD_core/sys.hpp:14-85): stress = (virial + sum_i m_i v_i (x) v_i) / V,
+// LTMatrix3 order with the off-diagonal pairs summed; pressure = trace / 3.
+// out[0..5] = stress (kcal/mol/A^3), out[6] = pressure in bar.
+__global__ void k_kinetic_stress(int n, const float3* __restrict__ vel,
+                                 const float* __restrict__ mass, double* __restrict__ acc) {
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float3 v = vel[i];
+    const double m = mass[i];
+    s[0] += m * v.x * v.x;
+    s[1] += m * 2.0 * v.x * v.y;
+    s[2] += m * v.y * v.y;
+    s[3] += m * 2.0 * v.x * v.z;
+    s[4] += m * 2.0 * v.y * v.z;
+    s[5] += m * v.z * v.z;
+  }
+  __shared__ double sh[6][32];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double x = warp_sum(s[c]);
+    if ((threadIdx.x & 31) == 0) sh[c][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double x = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
+    atomicAdd(acc + threadIdx.x, x);
+  }
+}
+
+__global__ void k_pressure(const double* __restrict__ kin, const double* __restrict__ virial,
+                           const long long* __restrict__ constraint_virial, double inv_v,
+                           double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double tr = 0.0;
+  for (int c = 0; c < 6; ++c) {
+    double w = virial ? virial[c] : 0.0;
+    if (constraint_virial) w += (double)constraint_virial[c] * kEnergyScaleInv;
+    out[c] = (w + kin[c]) * inv_v;
+  }
+  tr = out[0] + out[2] + out[5];
+  out[6] = tr / 3.0 * 6.946827162543585e4;  // kcal/mol/A^3 -> bar
+}
+
+int launch_pressure(int n, const float3* vel, const float* mass, const double* virial,
+                    const long long* constraint_virial, double inv_v, double* scratch6,
+                    double* out, cudaStream_t st) {
+  SNB_CUDA_TRY(cudaMemsetAsync(scratch6, 0, sizeof(double) * 6, st));
+  k_kinetic_stress<<<std::max(1, std::min(ceil_div(n, 256), 148 * 4)), 256, 0, st>>>(
+      n, vel, mass, scratch6);
+  k_pressure<<<1, 32, 0, st>>>(scratch6, virial, constraint_virial, inv_v, out);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
 // d_potential[0] += e; d_virial[0..5] += v (reference folds global terms into
 // slot 0 of the per-atom arrays, main.cpp:1473-1483,1541-1544).
 __global__ void k_add_scalars(float* d_potential, float* d_virial,

@@ -22,8 +22,10 @@
 //    reference stops the run there).
 // The constraint virial, sum of F (x) r_old over the constrained atoms with
 // F = m (r_new - r_unconstrained) / (dt^2 x_factor), is accumulated in fixed
-// point and added as virial / V to the caller's stress
+// point (reset by the remember kernel, so it holds the last step's) and, on
+// request, added as virial / V to the caller's stress
 // (Sum_Virial_Tensor_To_Stress, settle.cpp:450-481).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <vector>
@@ -65,8 +67,9 @@ __global__ void k_settle_remember(int nt, const SettleTri* __restrict__ tri, int
                                   const SettlePair* __restrict__ pair,
                                   const float3* __restrict__ crd, Cell cell, Cell rcell,
                                   float3* __restrict__ last_ba, float3* __restrict__ last_ca,
-                                  float3* __restrict__ last_ab) {
+                                  float3* __restrict__ last_ab, long long* __restrict__ vir_sum) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < 6) vir_sum[t] = 0;  // the step's constraint virial starts here
   if (t < nt) {
     const SettleTri g = tri[t];
     const float3 a = crd[g.a];
@@ -349,9 +352,9 @@ int launch_settle_remember(const Settle& s, const float3* crd, const Cell& cell,
                            const Cell& rcell, cudaStream_t st) {
   const int w = s.nt + s.np;
   if (w == 0) return kOk;
-  k_settle_remember<<<ceil_div(w, 256), 256, 0, st>>>(s.nt, s.d_tri, s.np, s.d_pair, crd, cell,
-                                                      rcell, s.d_last_ba, s.d_last_ca,
-                                                      s.d_last_ab);
+  k_settle_remember<<<ceil_div(std::max(w, 6), 256), 256, 0, st>>>(
+      s.nt, s.d_tri, s.np, s.d_pair, crd, cell, rcell, s.d_last_ba, s.d_last_ca, s.d_last_ab,
+      s.d_vir);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -361,11 +364,9 @@ int launch_settle(const Settle& s, float3* crd, float3* vel, const Cell& cell,
                   cudaStream_t st) {
   const int w = s.nt + s.np;
   if (w == 0) return kOk;
-  if (stress) SNB_CUDA_TRY(cudaMemsetAsync(s.d_vir, 0, sizeof(long long) * 6, st));
   k_settle<<<ceil_div(w, 128), 128, 0, st>>>(s.nt, s.d_tri, s.np, s.d_pair, crd, vel, cell,
                                              rcell, s.d_last_ba, s.d_last_ca, s.d_last_ab, dt,
-                                             v_factor, x_factor, stress ? s.d_vir : nullptr,
-                                             s.d_err);
+                                             v_factor, x_factor, s.d_vir, s.d_err);
   SNB_CUDA_TRY(cudaGetLastError());
   if (stress) {
     k_settle_stress<<<1, 32, 0, st>>>(s.d_vir, rcell, stress);
