@@ -231,7 +231,6 @@ struct PairArgs {
 int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool ortho, cudaStream_t st);
 
-// 1-4 terms (NON_BOND_14): pairs with their scaled A', B' and Coulomb scale.
 // Rigid triangle: atoms A, B, C, canonical frame (A at (0, ra), B at (rc, rb),
 // C at (rd, re) about the centre of mass) and masses.
 struct SettleTri {
@@ -265,6 +264,7 @@ int launch_settle(const Settle& s, float3* crd, float3* vel, const Cell& cell,
                   const Cell& rcell, float dt, float v_factor, float x_factor, float* stress,
                   cudaStream_t st);
 
+// 1-4 terms (NON_BOND_14): pairs with their scaled A', B' and Coulomb scale.
 struct NB14 {
   int m = 0;
   int* d_a = nullptr;
