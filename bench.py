@@ -760,15 +760,22 @@ def run_ours(args):
     rebuilds, pairs = ctypes.c_longlong(0), ctypes.c_longlong(0)
     capi.check(lib.snb_engine_stats(h, ctypes.byref(rebuilds), ctypes.byref(pairs), sp), "stats")
 
-    # end-to-end through the public API with host buffers: every step copies
-    # crd + vel from pinned host memory, runs one step, reads crd + vel back
+    # end-to-end through the public API with host buffers: every call copies
+    # crd + vel from pinned host memory, runs one step and copies crd + vel
+    # back (snb_engine_md_steps_host, one synchronisation per call)
     h_crd = torch.from_numpy(crd.cpu().numpy().copy()).pin_memory()
     h_vel = torch.from_numpy(vel.cpu().numpy().copy()).pin_memory()
     E = max(10, min(K, 200))
+    host_steps = lib.snb_engine_md_steps_host if not args.no_graph else None
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with torch.cuda.stream(st):
         for k in range(E):
+            if host_steps is not None:
+                capi.check(host_steps(h, P(h_crd), P(h_vel), P(crd), P(vel), P(invm),
+                                      ctypes.c_float(dt), EQ + W + K + 1000 + k, 1, sp),
+                           "e2e step")
+                continue
             crd.copy_(h_crd, non_blocking=True)
             vel.copy_(h_vel, non_blocking=True)
             capi.check(run_steps(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),

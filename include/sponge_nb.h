@@ -374,6 +374,15 @@ int snb_engine_md_steps(snb_engine* e, float* crd, float* vel,
 int snb_engine_md_steps_graph(snb_engine* e, float* crd, float* vel,
                               const float* inverse_mass, float dt,
                               int first_step, int steps, void* stream);
+/* snb_engine_md_steps_graph for a caller that keeps the state in host
+ * memory (no counterpart in the reference, whose state stays on the
+ * device): h_crd and h_vel [N*3] (pinned for full speed) are copied into the
+ * device work buffers crd and vel, the steps run, and the results are
+ * copied back into h_crd and h_vel; the list-overflow check and the copy
+ * back share one synchronisation, after which the call returns. */
+int snb_engine_md_steps_host(snb_engine* e, float* h_crd, float* h_vel, float* crd,
+                             float* vel, const float* inverse_mass, float dt,
+                             int first_step, int steps, void* stream);
 /* Tracing (the CUDA-event counterpart of the reference's TIME_RECORDER,
  * utils/control/time_recorder.hpp:9-43): runs `steps` stream-launched steps
  * with events between phases and writes the mean milliseconds per step of

@@ -65,7 +65,8 @@ EXPORTED = [
     "snb_engine_set_settle", "snb_engine_pressure", "snb_settle_create", "snb_settle_counts",
     "snb_settle_remember_last_coordinates", "snb_settle_do", "snb_settle_status",
     "snb_settle_destroy",
-    "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_profile_steps",
+    "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_md_steps_host",
+    "snb_engine_profile_steps",
     "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
     "snb_engine_destroy",
     "snb_read_lj_in_file", "snb_read_lj_soft_core_in_file", "snb_read_subsys_division_in_file",
@@ -164,6 +165,7 @@ _SIGS = {
     "snb_append_frc_traj": (_I, [ctypes.c_char_p, _P, _I, _P]),
     "snb_engine_md_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_md_steps_graph": (_I, [_P, _P, _P, _P, _F, _I, _I, _P]),
+    "snb_engine_md_steps_host": (_I, [_P, _P, _P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_profile_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P, _P]),
     "snb_engine_autotune": (_I, [_P, _P, _P, _P, _F, _I, _P, _P]),
     "snb_engine_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I),

@@ -1636,8 +1636,12 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
 // overflow flag and, on overflow, regrows the list, restores the snapshot
 // and repeats the steps since it (the recovery loop Check_Overflow was meant
 // to provide, neighbor_list.cpp:1027-1103).
+// h_crd_out / h_vel_out (host, may be null): the final crd / vel are copied
+// there before the last overflow check, so that one synchronisation serves
+// both (a repeat after an overflow copies them again).
 static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, float dt,
-                      int first, int steps, cudaStream_t st, bool use_graph) {
+                      int first, int steps, cudaStream_t st, bool use_graph,
+                      float* h_crd_out = nullptr, float* h_vel_out = nullptr) {
   const int chk = std::max(1, e->opt.nl_check_overflow_interval);
   int s = 0;
   int retries = 0;
@@ -1682,6 +1686,14 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
         if (rc) return rc;
       }
       e->steps_done++;
+    }
+    if (s + chunk == steps) {
+      if (h_crd_out)
+        SNB_CUDA_TRY(cudaMemcpyAsync(h_crd_out, crd, sizeof(float) * 3 * e->n,
+                                     cudaMemcpyDeviceToHost, st));
+      if (h_vel_out)
+        SNB_CUDA_TRY(cudaMemcpyAsync(h_vel_out, vel, sizeof(float) * 3 * e->n,
+                                     cudaMemcpyDeviceToHost, st));
     }
     bool regrown = false;
     int rc = nl_check_overflow(e->nl, &regrown, st);
@@ -1732,6 +1744,24 @@ extern "C" int snb_engine_md_steps_graph(snb_engine* e, float* crd, float* vel,
     return fail(kBadInput, "graph replay needs a non-default stream");
   bool graphable = e->opt.nl_refresh_interval <= 0 && e->pme.update_interval == 1;
   return engine_run(e, crd, vel, invm, dt, first, steps, S(stream), graphable);
+}
+
+extern "C" int snb_engine_md_steps_host(snb_engine* e, float* h_crd, float* h_vel,
+                                        float* crd, float* vel, const float* invm, float dt,
+                                        int first, int steps, void* stream) {
+  if (!e || !h_crd || !h_vel || !crd || !vel || !invm || steps < 0)
+    return fail(kBadInput, "engine_md_steps_host: bad argument");
+  cudaStream_t st = S(stream);
+  if (st == nullptr) return fail(kBadInput, "engine_md_steps_host: needs a non-default stream");
+  const size_t bytes = sizeof(float) * 3 * (size_t)e->n;
+  SNB_CUDA_TRY(cudaMemcpyAsync(crd, h_crd, bytes, cudaMemcpyHostToDevice, st));
+  SNB_CUDA_TRY(cudaMemcpyAsync(vel, h_vel, bytes, cudaMemcpyHostToDevice, st));
+  if (steps == 0) return kOk;
+  bool graphable = e->opt.nl_refresh_interval <= 0 && e->pme.update_interval == 1;
+  int rc = engine_run(e, crd, vel, invm, dt, first, steps, st, graphable, h_crd, h_vel);
+  if (rc) return rc;
+  SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  return kOk;
 }
 
 // Stream-launched steps with CUDA events between phases; h_phase_ms gets the
