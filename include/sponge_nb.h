@@ -156,7 +156,11 @@ int snb_lj_get_local(snb_lj* lj, const int* atom_local, int local_atom_numbers,
                      int ghost_numbers, void* stream);
 /* LENNARD_JONES_INFORMATION::LJ_PME_Direct_Force_With_Atom_Energy_And_Virial
  * (Lennard_Jones_force.h:139-145, Lennard_Jones_force.cpp:326-384).  `nl` is
- * the neighbor list handle whose d_nl the reference would pass. */
+ * the neighbor list handle whose d_nl the reference would pass.  With
+ * solvent_numbers > 0 the pairs of two atoms of the trailing water block
+ * (the last solvent_numbers atoms) are left to
+ * snb_solvent_lj_pme_direct_force, as the reference leaves the rows of those
+ * atoms to SOLVENT_LENNARD_JONES.  ghost_numbers must be 0. */
 int snb_lj_pme_direct_force(snb_lj* lj, int atom_numbers,
                             int local_atom_numbers, int solvent_numbers,
                             int ghost_numbers, const float* crd,
@@ -165,6 +169,19 @@ int snb_lj_pme_direct_force(snb_lj* lj, int atom_numbers,
                             int need_atom_energy, float* atom_energy,
                             int need_virial, float* atom_virial,
                             float* atom_direct_pme_energy, void* stream);
+/* SOLVENT_LENNARD_JONES::LJ_PME_Direct_Force_With_Atom_Energy_And_Virial
+ * (solvent_LJ.h:23-42, solvent_LJ.cpp:256-432): the pairs between atoms of
+ * the trailing water block (the last solvent_numbers atoms), which
+ * snb_lj_pme_direct_force leaves out when given the same solvent_numbers
+ * (main.cpp runs the two one after the other, 1453-1467).  It uses the LJ
+ * handle's tables and the same list, and adds to frc, atom_energy,
+ * atom_virial and atom_direct_pme_energy without clearing them. */
+int snb_solvent_lj_pme_direct_force(snb_lj* lj, snb_nl* nl, int atom_numbers,
+                                    int solvent_numbers, const float* crd,
+                                    const float* charge, float* frc, snb_boundary boundary,
+                                    float pme_beta, int need_atom_energy,
+                                    float* atom_energy, int need_virial, float* atom_virial,
+                                    float* atom_direct_pme_energy, void* stream);
 /* LENNARD_JONES_INFORMATION::Long_Range_Correction (:168-170, .cpp:287-308) */
 int snb_lj_long_range_correction(snb_lj* lj, int need_pressure, float* d_virial,
                                  int need_potential, float* d_potential,

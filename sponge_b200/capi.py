@@ -51,7 +51,7 @@ EXPORTED = [
     "snb_version", "snb_last_error", "snb_options_default", "snb_options_set",
     "snb_nl_create", "snb_nl_update", "snb_nl_check_overflow", "snb_nl_pair_count",
     "snb_nl_export_pairs", "snb_nl_export_atom_groups", "snb_nl_destroy",
-    "snb_lj_create", "snb_lj_get_local", "snb_lj_pme_direct_force",
+    "snb_lj_create", "snb_lj_get_local", "snb_lj_pme_direct_force", "snb_solvent_lj_pme_direct_force",
     "snb_lj_long_range_correction", "snb_lj_energy_sum", "snb_lj_long_range_factor",
     "snb_lj_destroy",
     "snb_lj_soft_create", "snb_lj_soft_pme_direct_force", "snb_lj_soft_dh_dlambda",
@@ -106,6 +106,8 @@ _SIGS = {
     "snb_lj_get_local": (_I, [_P, _P, _I, _I, _P]),
     "snb_lj_pme_direct_force": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, snb_boundary, _P,
                                      _F, _I, _P, _I, _P, _P, _P]),
+    "snb_solvent_lj_pme_direct_force": (_I, [_P, _P, _I, _I, _P, _P, _P, snb_boundary, _F,
+                                             _I, _P, _I, _P, _P, _P]),
     "snb_lj_long_range_correction": (_I, [_P, _I, _P, _I, _P, _F, _P]),
     "snb_lj_energy_sum": (_I, [_P, ctypes.POINTER(_F), _P]),
     "snb_lj_long_range_factor": (_F, [_P]),

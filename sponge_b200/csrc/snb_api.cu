@@ -390,26 +390,12 @@ extern "C" int snb_lj_get_local(snb_lj* h, const int* atom_local, int local_n,
                             S(stream));
 }
 
-extern "C" int snb_lj_pme_direct_force(snb_lj* h, int atom_numbers, int local_n,
-                                       int solvent_n, int ghost_n, const float* crd,
-                                       const float* charge, float* frc,
-                                       snb_boundary boundary, snb_nl* nl,
-                                       float pme_beta, int need_atom_energy,
-                                       float* atom_energy, int need_virial,
-                                       float* atom_virial,
-                                       float* atom_direct_pme_energy, void* stream) {
-  if (!h || !nl) return fail(kBadInput, "lj_pme_direct_force: null handle");
-  cudaStream_t st = S(stream);
-  if (need_atom_energy) {
-    if (atom_direct_pme_energy)
-      SNB_CUDA_TRY(cudaMemsetAsync(atom_direct_pme_energy, 0, sizeof(float) * h->n, st));
-    SNB_CUDA_TRY(cudaMemsetAsync(h->d_lj_energy, 0, sizeof(float) * h->n, st));
-  }
-  if (atom_numbers == 0 || local_n == 0) return kOk;
-  if (ghost_n != 0 || solvent_n != 0)
-    return fail(kNotSupported, "lj_pme_direct_force: ghost/solvent atoms");
-  if (local_n != h->n || nl->nl.n != h->n)
-    return fail(kBadInput, "lj_pme_direct_force: atom count mismatch");
+// Direct-space pairs of the LJ module over the list: solvent_mode 0 every
+// pair, 1 all but the solvent-solvent ones, 2 only those (see PairArgs).
+static int lj_direct(snb_lj* h, snb_nl* nl, const float* crd, const float* charge,
+                     float* frc, snb_boundary boundary, float pme_beta, bool en, bool vi,
+                     float* atom_energy, float* atom_virial, float* atom_direct_pme_energy,
+                     int solvent_mode, int solvent_begin, cudaStream_t st) {
   int rc = launch_pack(h->n, reinterpret_cast<const float3*>(crd), charge,
                        h->p.d_type_local, nl->nl.d_perm, h->d_pos, h->d_type_sorted, st);
   if (rc) return rc;
@@ -429,8 +415,9 @@ extern "C" int snb_lj_pme_direct_force(snb_lj* h, int atom_numbers, int local_n,
   a.rcell = rcell_of(boundary);
   a.cutoff2 = h->p.cutoff * h->p.cutoff;
   a.beta = pme_beta;
+  a.solvent_mode = solvent_mode;
+  a.solvent_begin = solvent_begin;
   bool ortho = a.cell.a21 == 0.f && a.cell.a31 == 0.f && a.cell.a32 == 0.f;
-  bool en = need_atom_energy != 0, vi = need_virial != 0;
   rc = launch_pair(a, h->acc, h->accum, en, vi, ortho, st);
   if (rc) return rc;
   return launch_unpack(h->n, nl->nl.d_inv_perm, h->acc, h->accum,
@@ -438,6 +425,55 @@ extern "C" int snb_lj_pme_direct_force(snb_lj* h, int atom_numbers, int local_n,
                        en ? h->d_lj_energy : nullptr,
                        en ? atom_direct_pme_energy : nullptr,
                        vi ? atom_virial : nullptr, en, vi, st);
+}
+
+extern "C" int snb_lj_pme_direct_force(snb_lj* h, int atom_numbers, int local_n,
+                                       int solvent_n, int ghost_n, const float* crd,
+                                       const float* charge, float* frc,
+                                       snb_boundary boundary, snb_nl* nl,
+                                       float pme_beta, int need_atom_energy,
+                                       float* atom_energy, int need_virial,
+                                       float* atom_virial,
+                                       float* atom_direct_pme_energy, void* stream) {
+  if (!h || !nl) return fail(kBadInput, "lj_pme_direct_force: null handle");
+  cudaStream_t st = S(stream);
+  if (need_atom_energy) {
+    if (atom_direct_pme_energy)
+      SNB_CUDA_TRY(cudaMemsetAsync(atom_direct_pme_energy, 0, sizeof(float) * h->n, st));
+    SNB_CUDA_TRY(cudaMemsetAsync(h->d_lj_energy, 0, sizeof(float) * h->n, st));
+  }
+  if (atom_numbers == 0 || local_n == 0) return kOk;
+  if (ghost_n != 0) return fail(kNotSupported, "lj_pme_direct_force: ghost atoms");
+  if (local_n != h->n || nl->nl.n != h->n)
+    return fail(kBadInput, "lj_pme_direct_force: atom count mismatch");
+  if (solvent_n < 0 || solvent_n > local_n)
+    return fail(kBadInput, "lj_pme_direct_force: solvent_numbers out of range");
+  if (solvent_n > 0 && nl->nl.bv.nsys > 0)
+    return fail(kNotSupported, "lj_pme_direct_force: solvent split of a batch");
+  return lj_direct(h, nl, crd, charge, frc, boundary, pme_beta, need_atom_energy != 0,
+                   need_virial != 0, atom_energy, atom_virial, atom_direct_pme_energy,
+                   solvent_n > 0 ? 1 : 0, local_n - solvent_n, st);
+}
+
+extern "C" int snb_solvent_lj_pme_direct_force(snb_lj* h, snb_nl* nl, int atom_numbers,
+                                               int solvent_numbers, const float* crd,
+                                               const float* charge, float* frc,
+                                               snb_boundary boundary, float pme_beta,
+                                               int need_atom_energy, float* atom_energy,
+                                               int need_virial, float* atom_virial,
+                                               float* atom_direct_pme_energy,
+                                               void* stream) {
+  if (!h || !nl) return fail(kBadInput, "solvent_lj_pme_direct_force: null handle");
+  if (atom_numbers != h->n || nl->nl.n != h->n)
+    return fail(kBadInput, "solvent_lj_pme_direct_force: atom count mismatch");
+  if (solvent_numbers < 0 || solvent_numbers > atom_numbers)
+    return fail(kBadInput, "solvent_lj_pme_direct_force: solvent_numbers out of range");
+  if (nl->nl.bv.nsys > 0)
+    return fail(kNotSupported, "solvent_lj_pme_direct_force: batch lists");
+  if (solvent_numbers == 0) return kOk;
+  return lj_direct(h, nl, crd, charge, frc, boundary, pme_beta, need_atom_energy != 0,
+                   need_virial != 0, atom_energy, atom_virial, atom_direct_pme_energy, 2,
+                   atom_numbers - solvent_numbers, S(stream));
 }
 
 extern "C" int snb_lj_long_range_correction(snb_lj* h, int need_pressure,

@@ -227,6 +227,12 @@ struct PairArgs {
   BatchView bv;                 // nsys > 0: per-system boxes (rectangular)
   int unroll = 4;               // scan candidates per lane per round (2, 4, 8)
   int blocks_per_sm = 0;        // persistent blocks per SM, 0: occupancy maximum
+  // solvent split (single box): the atoms with global id >= solvent_begin
+  // are the trailing water block.  solvent_mode 1: every pair but the
+  // solvent-solvent ones (LENNARD_JONES_INFORMATION with solvent_numbers);
+  // 2: only those (SOLVENT_LENNARD_JONES); 0: every pair
+  int solvent_mode = 0;
+  int solvent_begin = 0;
 };
 int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool ortho, cudaStream_t st);

@@ -142,7 +142,10 @@ __device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
   }
 }
 
-template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO, bool BATCH, int kScanU>
+// SOLV 1 / 2: the solvent split of PairArgs::solvent_mode (pairs with both
+// global ids >= solvent_begin left out / taken alone); 0: every pair.
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO, bool BATCH, int kScanU,
+          int SOLV = 0>
 __global__ void __launch_bounds__(256, 4)
 k_lj_direct(PairArgs a, Accumulators acc) {
   static_assert(kScanU >= 1 && 32 * kScanU < kHitCap, "scan round exceeds the hit list");
@@ -170,7 +173,8 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   const float4 pi = a.pos[i];
   const float3 ri = make_float3(pi.x, pi.y, pi.z);
   const int ti = a.type[i];
-  const int gi = ENERGY || VIRIAL ? a.global[i] : 0;
+  const int gi = ENERGY || VIRIAL || SOLV ? a.global[i] : 0;
+  const bool i_solvent = SOLV && gi >= a.solvent_begin;
   // box of atom i (and of all its pairs)
   const SysGeom* gs = BATCH ? a.bv.sys + a.bv.sys_of[i] : nullptr;
   const Cell& cell = BATCH ? gs->cell : a.cell;
@@ -217,6 +221,10 @@ k_lj_direct(PairArgs a, Accumulators acc) {
           const float3 dr = min_image_fast<ORTHO>(make_float3(pp[u].x, pp[u].y, pp[u].z),
                                                   ri, cell, rcell);
           in = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z < a.cutoff2;
+          if (SOLV && in) {
+            const bool both = i_solvent && a.global[jj[u]] >= a.solvent_begin;
+            in = SOLV == 1 ? !both : both;
+          }
         }
         const unsigned m = __ballot_sync(0xffffffffu, in);
         if (in) hits[count + __popc(m & lt)] = jj[u];
@@ -277,7 +285,12 @@ static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream
   // only, rectangular); the others take 4
   const bool tunable = ACCUM == kAccumFixed && !ENERGY && !VIRIAL && ortho;
   const int u = tunable ? a.unroll : 4;
-  if (a.bv.nsys > 0)
+  if (a.solvent_mode != 0 && a.bv.nsys == 0)
+    kern = ortho ? (a.solvent_mode == 1 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4, 1>
+                                        : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4, 2>)
+                 : (a.solvent_mode == 1 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, false, false, 4, 1>
+                                        : k_lj_direct<ACCUM, ENERGY, VIRIAL, false, false, 4, 2>);
+  else if (a.bv.nsys > 0)
     kern = u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 2>
          : u == 8 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 8>
                   : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 4>;
