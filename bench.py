@@ -763,16 +763,28 @@ def run_ours(args):
     # end-to-end through the public API with host buffers: every call copies
     # crd + vel from pinned host memory, runs one step and copies crd + vel
     # back (snb_engine_md_steps_host, one synchronisation per call)
-    h_crd = torch.from_numpy(crd.cpu().numpy().copy()).pin_memory()
-    h_vel = torch.from_numpy(vel.cpu().numpy().copy()).pin_memory()
+    # (the state sits in one [crd | vel] array on each side, so each
+    # direction is one copy; one untimed call captures the step graph for
+    # these buffers)
     E = max(10, min(K, 200))
     host_steps = lib.snb_engine_md_steps_host if not args.no_graph else None
+    if host_steps is not None:
+        d_state = torch.cat([crd, vel])
+        h_state = d_state.cpu().pin_memory()
+        d_crd, d_vel = d_state[:3 * n], d_state[3 * n:]
+        h_crd, h_vel = h_state[:3 * n], h_state[3 * n:]
+        with torch.cuda.stream(st):
+            capi.check(host_steps(h, P(h_crd), P(h_vel), P(d_crd), P(d_vel), P(invm),
+                                  ctypes.c_float(dt), EQ + W + K + 999, 1, sp), "e2e warm-up")
+    else:
+        h_crd = torch.from_numpy(crd.cpu().numpy().copy()).pin_memory()
+        h_vel = torch.from_numpy(vel.cpu().numpy().copy()).pin_memory()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with torch.cuda.stream(st):
         for k in range(E):
             if host_steps is not None:
-                capi.check(host_steps(h, P(h_crd), P(h_vel), P(crd), P(vel), P(invm),
+                capi.check(host_steps(h, P(h_crd), P(h_vel), P(d_crd), P(d_vel), P(invm),
                                       ctypes.c_float(dt), EQ + W + K + 1000 + k, 1, sp),
                            "e2e step")
                 continue
@@ -784,6 +796,10 @@ def run_ours(args):
             h_vel.copy_(vel, non_blocking=True)
             st.synchronize()
     t_e2e = time.perf_counter() - t0
+    if host_steps is not None:  # the run continues from the e2e leg's state
+        crd.copy_(d_crd)
+        vel.copy_(d_vel)
+        torch.cuda.synchronize()
     e2e_t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)

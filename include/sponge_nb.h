@@ -396,7 +396,9 @@ int snb_engine_md_steps_graph(snb_engine* e, float* crd, float* vel,
  * device): h_crd and h_vel [N*3] (pinned for full speed) are copied into the
  * device work buffers crd and vel, the steps run, and the results are
  * copied back into h_crd and h_vel; the list-overflow check and the copy
- * back share one synchronisation, after which the call returns. */
+ * back share one synchronisation, after which the call returns.  When vel
+ * follows crd directly on both sides (one [2][N*3] state array each), each
+ * direction is one copy. */
 int snb_engine_md_steps_host(snb_engine* e, float* h_crd, float* h_vel, float* crd,
                              float* vel, const float* inverse_mass, float dt,
                              int first_step, int steps, void* stream);

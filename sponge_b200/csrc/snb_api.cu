@@ -1724,12 +1724,15 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
       e->steps_done++;
     }
     if (s + chunk == steps) {
-      if (h_crd_out)
-        SNB_CUDA_TRY(cudaMemcpyAsync(h_crd_out, crd, sizeof(float) * 3 * e->n,
-                                     cudaMemcpyDeviceToHost, st));
-      if (h_vel_out)
-        SNB_CUDA_TRY(cudaMemcpyAsync(h_vel_out, vel, sizeof(float) * 3 * e->n,
-                                     cudaMemcpyDeviceToHost, st));
+      const size_t b3 = sizeof(float) * 3 * e->n;
+      if (h_crd_out && h_vel_out == h_crd_out + 3 * (size_t)e->n && vel == crd + 3 * (size_t)e->n) {
+        SNB_CUDA_TRY(cudaMemcpyAsync(h_crd_out, crd, 2 * b3, cudaMemcpyDeviceToHost, st));
+      } else {
+        if (h_crd_out)
+          SNB_CUDA_TRY(cudaMemcpyAsync(h_crd_out, crd, b3, cudaMemcpyDeviceToHost, st));
+        if (h_vel_out)
+          SNB_CUDA_TRY(cudaMemcpyAsync(h_vel_out, vel, b3, cudaMemcpyDeviceToHost, st));
+      }
     }
     bool regrown = false;
     int rc = nl_check_overflow(e->nl, &regrown, st);
@@ -1790,8 +1793,13 @@ extern "C" int snb_engine_md_steps_host(snb_engine* e, float* h_crd, float* h_ve
   cudaStream_t st = S(stream);
   if (st == nullptr) return fail(kBadInput, "engine_md_steps_host: needs a non-default stream");
   const size_t bytes = sizeof(float) * 3 * (size_t)e->n;
-  SNB_CUDA_TRY(cudaMemcpyAsync(crd, h_crd, bytes, cudaMemcpyHostToDevice, st));
-  SNB_CUDA_TRY(cudaMemcpyAsync(vel, h_vel, bytes, cudaMemcpyHostToDevice, st));
+  if (h_vel == h_crd + 3 * (size_t)e->n && vel == crd + 3 * (size_t)e->n) {
+    // crd and vel side by side on both ends: one copy each way
+    SNB_CUDA_TRY(cudaMemcpyAsync(crd, h_crd, 2 * bytes, cudaMemcpyHostToDevice, st));
+  } else {
+    SNB_CUDA_TRY(cudaMemcpyAsync(crd, h_crd, bytes, cudaMemcpyHostToDevice, st));
+    SNB_CUDA_TRY(cudaMemcpyAsync(vel, h_vel, bytes, cudaMemcpyHostToDevice, st));
+  }
   if (steps == 0) return kOk;
   bool graphable = e->opt.nl_refresh_interval <= 0 && e->pme.update_interval == 1;
   int rc = engine_run(e, crd, vel, invm, dt, first, steps, st, graphable, h_crd, h_vel);

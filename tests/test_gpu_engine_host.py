@@ -2,7 +2,8 @@
 memory.  Thirty one-step calls that copy crd / vel in from pinned host
 buffers and back out give, bit for bit, the trajectory of thirty
 device-resident graph steps; the host buffers hold the result when the call
-returns."""
+returns.  Both layouts: crd and vel apart, and side by side in one state
+array on each end (one copy each way)."""
 
 import ctypes
 
@@ -20,7 +21,8 @@ def g():
     return gpu_helpers
 
 
-def test_host_steps_equal_device_steps(g):
+@pytest.mark.parametrize("layout", ["apart", "state"])
+def test_host_steps_equal_device_steps(g, layout):
     import torch
     from sponge_b200 import systems
     s = systems.water_box(500, seed=9)
@@ -35,6 +37,10 @@ def test_host_steps_equal_device_steps(g):
         invm = g.dev((1.0 / s.mass).astype(np.float32))
         h_crd = torch.from_numpy(s.crd.reshape(-1).astype(np.float32).copy()).pin_memory()
         h_vel = torch.from_numpy(s.vel.reshape(-1).astype(np.float32).copy()).pin_memory()
+        if host and layout == "state":
+            d_state, h_state = torch.cat([crd, vel]), torch.cat([h_crd, h_vel]).pin_memory()
+            crd, vel = d_state[:3 * s.n], d_state[3 * s.n:]
+            h_crd, h_vel = h_state[:3 * s.n], h_state[3 * s.n:]
         st = torch.cuda.Stream()
         sp = ctypes.c_void_p(st.cuda_stream)
         try:
