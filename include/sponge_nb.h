@@ -466,6 +466,12 @@ int snb_nb14_destroy(snb_nb14* h);
 int snb_settle_create(int atom_numbers, int constrain_pair_numbers, const int* h_atom_i,
                       const int* h_atom_j, const float* h_constant_r, const float* h_mass,
                       snb_settle** out);
+/* The grouping of snb_settle_create alone, on the host (no device memory):
+ * counts[3] = {rigid triangles, rigid pairs, pairs left over} and, when
+ * h_remaining_pairs is not NULL, the indices of the left-over pairs. */
+int snb_settle_group(int atom_numbers, int constrain_pair_numbers, const int* h_atom_i,
+                     const int* h_atom_j, const float* h_constant_r, const float* h_mass,
+                     int* counts, int* h_remaining_pairs);
 /* triangle_numbers, pair_numbers and the constraint pairs left over (their
  * indices in the creation order into h_remaining_pairs when not NULL). */
 int snb_settle_counts(snb_settle* h, int* triangle_numbers, int* pair_numbers,

@@ -62,7 +62,7 @@ EXPORTED = [
     "snb_engine_create", "snb_batch_create", "snb_engine_force", "snb_engine_set_bonded",
     "snb_engine_set_soft_core", "snb_engine_update_box", "snb_engine_set_nb14",
     "snb_nb14_create", "snb_nb14_force", "snb_nb14_energy_sums", "snb_nb14_destroy",
-    "snb_engine_set_settle", "snb_engine_pressure", "snb_settle_create", "snb_settle_counts",
+    "snb_engine_set_settle", "snb_engine_pressure", "snb_settle_create", "snb_settle_group", "snb_settle_counts",
     "snb_settle_remember_last_coordinates", "snb_settle_do", "snb_settle_status",
     "snb_settle_destroy",
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_md_steps_host",
@@ -150,6 +150,7 @@ _SIGS = {
     "snb_engine_set_settle": (_I, [_P, _P]),
     "snb_engine_pressure": (_I, [_P, _P, _P, _P, _P, _P]),
     "snb_settle_create": (_I, [_I, _I, _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    "snb_settle_group": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     "snb_settle_counts": (_I, [_P, _P, _P, _P, _P]),
     "snb_settle_remember_last_coordinates": (_I, [_P, _P, snb_boundary, _P]),
     "snb_settle_do": (_I, [_P, _P, snb_boundary, _P, _F, _F, _F, _I, _P, _P]),

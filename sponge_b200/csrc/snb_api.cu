@@ -1455,6 +1455,25 @@ extern "C" int snb_settle_create(int atom_numbers, int constrain_pair_numbers,
   return kOk;
 }
 
+extern "C" int snb_settle_group(int atom_numbers, int constrain_pair_numbers,
+                                const int* h_atom_i, const int* h_atom_j,
+                                const float* h_constant_r, const float* h_mass,
+                                int* counts, int* h_remaining_pairs) {
+  if (!counts) return fail(kBadInput, "settle_group: null counts");
+  std::vector<SettleTri> tri;
+  std::vector<SettlePair> pair;
+  std::vector<int> rem;
+  int rc = settle_group(atom_numbers, constrain_pair_numbers, h_atom_i, h_atom_j,
+                        h_constant_r, h_mass, tri, pair, rem);
+  if (rc) return rc;
+  counts[0] = (int)tri.size();
+  counts[1] = (int)pair.size();
+  counts[2] = (int)rem.size();
+  if (h_remaining_pairs)
+    for (size_t k = 0; k < rem.size(); ++k) h_remaining_pairs[k] = rem[k];
+  return kOk;
+}
+
 extern "C" int snb_settle_counts(snb_settle* h, int* triangle_numbers, int* pair_numbers,
                                  int* remaining_pair_numbers, int* h_remaining_pairs) {
   if (!h) return fail(kBadInput, "settle_counts: null handle");

@@ -260,6 +260,9 @@ struct Settle {
   long long* d_vir = nullptr;  // [6] constraint virial since the last remember, fixed point
   int* d_err = nullptr;        // 1 + index of a pair without a real solution, else 0
 };
+int settle_group(int n, int m, const int* ai, const int* aj, const float* r0,
+                 const float* mass, std::vector<SettleTri>& tri,
+                 std::vector<SettlePair>& pair, std::vector<int>& remaining);
 int settle_init(Settle& s, int n, int m, const int* ai, const int* aj, const float* r0,
                 const float* mass);
 void settle_free(Settle& s);

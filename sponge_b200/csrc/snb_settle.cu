@@ -235,8 +235,10 @@ static void triangle_frame(double rAB, double rAC, double rBC, double mA, double
   t.re = (float)y[2];
 }
 
-int settle_init(Settle& s, int n, int m, const int* ai, const int* aj, const float* r0,
-                const float* mass) {
+// The host side of SETTLE::Initial: groups and the left-over pair indices.
+int settle_group(int n, int m, const int* ai, const int* aj, const float* r0,
+                 const float* mass, std::vector<SettleTri>& tri,
+                 std::vector<SettlePair>& pair, std::vector<int>& remaining) {
   if (n <= 0 || m < 0 || (m > 0 && (!ai || !aj || !r0)) || !mass)
     return fail(kBadInput, "SETTLE::Initial: bad argument");
   for (int p = 0; p < m; ++p)
@@ -286,8 +288,8 @@ int settle_init(Settle& s, int n, int m, const int* ai, const int* aj, const flo
       }
     }
   }
-  std::vector<SettleTri> tri;
-  std::vector<SettlePair> pair;
+  tri.clear();
+  pair.clear();
   for (int i = 0; i < n; ++i) {
     if (role[i] == 2) {
       SettleTri g;
@@ -310,12 +312,21 @@ int settle_init(Settle& s, int n, int m, const int* ai, const int* aj, const flo
       pair.push_back(p);
     }
   }
+  remaining.clear();
+  for (int p = 0; p < m; ++p)
+    if (role[ai[p]] == 3) remaining.push_back(p);
+  return kOk;
+}
+
+int settle_init(Settle& s, int n, int m, const int* ai, const int* aj, const float* r0,
+                const float* mass) {
+  std::vector<SettleTri> tri;
+  std::vector<SettlePair> pair;
+  int rc = settle_group(n, m, ai, aj, r0, mass, tri, pair, s.remaining);
+  if (rc) return rc;
   s.n = n;
   s.nt = (int)tri.size();
   s.np = (int)pair.size();
-  s.remaining.clear();
-  for (int p = 0; p < m; ++p)
-    if (role[ai[p]] == 3) s.remaining.push_back(p);
   const size_t kt = std::max(s.nt, 1), kp = std::max(s.np, 1);
   SNB_CUDA_TRY(cudaMalloc(&s.d_tri, sizeof(SettleTri) * kt));
   SNB_CUDA_TRY(cudaMalloc(&s.d_pair, sizeof(SettlePair) * kp));

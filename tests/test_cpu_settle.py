@@ -75,3 +75,30 @@ def test_oracle_keeps_rigid_bodies_rigid(oracle):
     k = settled_mask(z)
     d = o["crd"][z["atom_j"][k]] - o["crd"][z["atom_i"][k]]
     assert np.abs(np.linalg.norm(d, axis=1) - z["constant_r"][k]).max() <= 1e-12
+
+
+def test_grouping_matches_reference():
+    """snb_settle_group (host code, no GPU) sorts the case's constraint pairs
+    into the reference's 284 triangles, 10 rigid pairs and 7 left-over pairs,
+    the same left-over pairs as the reference's SETTLE::Initial keeps."""
+    import ctypes
+    from sponge_b200 import capi
+    z = load()
+    lib = capi.load()
+    ai = np.ascontiguousarray(z["atom_i"], np.int32)
+    aj = np.ascontiguousarray(z["atom_j"], np.int32)
+    r0 = np.ascontiguousarray(z["constant_r"], np.float32)
+    mass = np.ascontiguousarray(z["mass"], np.float32)
+    counts = np.zeros(3, np.int32)
+    left = np.zeros(len(ai), np.int32)
+    capi.check(lib.snb_settle_group(len(mass), len(ai), ai.ctypes.data, aj.ctypes.data,
+                                    r0.ctypes.data, mass.ctypes.data, counts.ctypes.data,
+                                    left.ctypes.data), "settle_group")
+    assert list(counts) == list(z["ref_counts"])
+    k = left[:counts[2]]
+    assert np.array_equal(np.stack([ai[k], aj[k]], 1), z["ref_left"])
+    bad = ai.copy()
+    bad[0] = len(mass)
+    assert lib.snb_settle_group(len(mass), len(ai), bad.ctypes.data, aj.ctypes.data,
+                                r0.ctypes.data, mass.ctypes.data, counts.ctypes.data,
+                                None) == capi.SNB_ERR_BAD_INPUT
