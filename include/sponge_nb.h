@@ -285,9 +285,11 @@ int snb_pme_destroy(snb_pme* pme);
  * on a device, so calls that may overlap in time (unordered streams,
  * concurrent threads) race and give wrong results: order them.  The array
  * must start at zero; the first call on each device clears it and each
- * completed call leaves it zero.  That first call looks up the array's
- * address and enqueues the clear, so make it before any stream capture
- * begins. */
+ * completed call leaves it zero.  Every call looks up the array's address
+ * in the current context; the first call on a device (which may load the
+ * module) also enqueues the clear, so make it before any stream capture
+ * begins.  After cudaDeviceReset, or in another context on the same device,
+ * the array is a fresh one and a changed address is cleared again. */
 #define SNB_NOALLOC_MAX_ATOMS 65536
 int snb_pme_excluded_force_noalloc(int atom_numbers, const float* crd,
                                    snb_boundary boundary, const float* charge,
@@ -468,7 +470,9 @@ int snb_settle_create(int atom_numbers, int constrain_pair_numbers, const int* h
                       snb_settle** out);
 /* The grouping of snb_settle_create alone, on the host (no device memory):
  * counts[3] = {rigid triangles, rigid pairs, pairs left over} and, when
- * h_remaining_pairs is not NULL, the indices of the left-over pairs. */
+ * h_remaining_pairs is not NULL, the indices of the left-over pairs.
+ * h_remaining_pairs must hold counts[2] ints; constrain_pair_numbers ints
+ * always suffice, or call once with NULL to read counts[2] first. */
 int snb_settle_group(int atom_numbers, int constrain_pair_numbers, const int* h_atom_i,
                      const int* h_atom_j, const float* h_constant_r, const float* h_mass,
                      int* counts, int* h_remaining_pairs);

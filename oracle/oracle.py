@@ -36,14 +36,21 @@ def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
 
 
+def reference_sources() -> str | None:
+    """The reference's SPONGE/ source folder, from the environment variable
+    SPONGE_REFERENCE (the reference checkout's root), or None when unset."""
+    root = os.environ.get("SPONGE_REFERENCE")
+    return os.path.join(root, "SPONGE") if root else None
+
+
 def build_oracle(ref_root: str | None = None, with_reference: bool = True,
                  with_gpu: bool = True) -> None:
     """Build the checkers (``make -C oracle [ref]``).  The reference part only
     builds where its sources exist."""
     import subprocess
     subprocess.check_call(["make", "-s", "-C", HERE, "libsnb_oracle.so"])
-    ref_root = ref_root or "/root/reference/SPONGE"
-    if with_reference and os.path.isdir(ref_root):
+    ref_root = ref_root or reference_sources()
+    if with_reference and ref_root and os.path.isdir(ref_root):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"])
         if with_gpu:
             subprocess.check_call(["make", "-s", "-C", HERE, "refgpu", f"REF={ref_root}"])

@@ -153,7 +153,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // erfc(x) and exp(-x^2) together for x >= 0.  erfcx(x) = erfc(x) e^{x^2} is
 // a degree-8 polynomial in t = 1/(1 + x/2) on [0, 4] (weighted least-squares
-// fit, csrc/fit_erfcx.py; max relative error 3.3e-7 in float32), so
+// fit against double-precision erfcx; max relative error 3.3e-7 in float32), so
 // erfc(x) = P(t) * exp(-x^2).  exp uses the hardware exp2 (__expf: error
 // 2 + 1.16|x^2| ulp, below 1e-6 relative for x <= 4); t uses the fast
 // hardware division (2 ulp; |t P'(t) / P(t)| <= 2.26 on the range, so P

@@ -20,9 +20,13 @@
 //    at zero again (the unpack kernel resets what it reads).  A call that
 //    returns an error after launching work marks the device's scratch for a
 //    fresh clear on its next call.
-//  * The first call on each device resolves the scratch address with
-//    cudaGetSymbolAddress (which may load the module) and enqueues the clear;
-//    make that first call before any stream capture begins.
+//  * Every call looks the scratch address up with cudaGetSymbolAddress in
+//    the context current on the calling thread; the first call on a device
+//    (which may load the module) also enqueues the clear, so make that first
+//    call before any stream capture begins.  The address is not kept between
+//    calls as the truth: after cudaDeviceReset, or under another context on
+//    the same device, the module is loaded again, possibly elsewhere, and a
+//    changed address is cleared again before use.
 #include <mutex>
 #include <string>
 
@@ -39,7 +43,10 @@ constexpr int kWordsPerAtom = 12;
 constexpr int kMaxDevices = 64;
 
 std::mutex g_mutex;
-long long* g_scratch[kMaxDevices] = {};  // device address, per device ordinal
+// address seen by the last call on each device ordinal; a call that finds
+// another address (a reset or another context loaded the module again)
+// clears the array before using it
+long long* g_scratch[kMaxDevices] = {};
 bool g_needs_clear[kMaxDevices] = {};
 
 }  // namespace
@@ -75,14 +82,15 @@ extern "C" int snb_pme_excluded_force_noalloc(
                                    std::to_string(dev) + " out of range");
   long long* scratch = nullptr;
   {
+    // the address in the current context; cheap once the module is loaded
+    void* p = nullptr;
+    cudaError_t err = cudaGetSymbolAddress(&p, g_excluded_scratch);
+    if (err != cudaSuccess)
+      return fail(kCudaError,
+                  std::string("pme_excluded_force_noalloc: cudaGetSymbolAddress: ") +
+                      cudaGetErrorString(err));
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch[dev]) {
-      void* p = nullptr;
-      cudaError_t err = cudaGetSymbolAddress(&p, g_excluded_scratch);
-      if (err != cudaSuccess)
-        return fail(kCudaError,
-                    std::string("pme_excluded_force_noalloc: cudaGetSymbolAddress: ") +
-                        cudaGetErrorString(err));
+    if (g_scratch[dev] != static_cast<long long*>(p)) {
       g_scratch[dev] = static_cast<long long*>(p);
       g_needs_clear[dev] = true;
     }

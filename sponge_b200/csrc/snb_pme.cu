@@ -49,28 +49,26 @@ int fft_size(float length) {  // Get_Fft_Patameter (common.cpp:639-659)
   }
 }
 
-// Ewald beta by bisection on erfc(beta*rc)/rc = tolerance with the
-// reference's float iteration (Get_Beta, PM_force.cpp:246-274).
+// Ewald beta with erfc(beta rc) / rc = tolerance, found the way the
+// reference finds it (Get_Beta, PM_force.cpp:246-274), since beta must come
+// out bit-identical: the smallest power of two h with a screened value at or
+// below the tolerance, then (doublings + 50) halvings of [0, h] in float, each
+// keeping the half whose lower end still screens at or above the tolerance;
+// the result is the last midpoint (lo + hi) / 2.
 float get_beta(float cutoff, float tolerance) {
-  float beta = 0.f, low, high = 1.0f, tempf;
-  int ilow, ihigh = 1;
-  for (;;) {
-    tempf = erfcf(high * cutoff) / cutoff;
-    if (tempf <= tolerance) break;
-    high *= 2;
-    ihigh++;
+  const auto screened = [cutoff](float b) { return erfcf(b * cutoff) / cutoff; };
+  float hi = 1.0f;
+  int doublings = 0;
+  while (screened(hi) > tolerance) {
+    hi *= 2;
+    ++doublings;
   }
-  ihigh += 50;
-  low = 0.0f;
-  for (ilow = 1; ilow < ihigh; ilow++) {
-    beta = (low + high) / 2;
-    tempf = erfcf(beta * cutoff) / cutoff;
-    if (tempf >= tolerance)
-      low = beta;
-    else
-      high = beta;
+  float lo = 0.0f, mid = 0.0f;
+  for (int halving = 0; halving < doublings + 50; ++halving) {
+    mid = (lo + hi) / 2;
+    (screened(mid) >= tolerance ? lo : hi) = mid;
   }
-  return beta;
+  return mid;
 }
 
 // |b(k)|^2 of the order-4 Euler exponential spline (getb, PM_force.cpp:40-64),

@@ -10,9 +10,9 @@ plus the bonded term lists and parameters the test evaluates in FP64, the
 residue ranges, and Amber's forces (iter0.npy) and potential energy
 (reference.json), for the case's three frames: the minimised one and two
 made from it by the reference's own rigid-water perturbation (0.02 and
-0.05 A).  Needs the reference tree (this container):
+0.05 A).  Needs the reference checkout, named by SPONGE_REFERENCE:
 
-    python tests/golden/make_amber_golden.py
+    SPONGE_REFERENCE=<reference checkout> python tests/golden/make_amber_golden.py
 """
 
 import json
@@ -22,7 +22,9 @@ import re
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASE = "/root/reference/benchmarks/comparison/reference/amber"
+# the reference checkout's root, from the environment (required to regenerate)
+REF_ROOT = os.environ.get("SPONGE_REFERENCE", "")
+CASE = os.path.join(REF_ROOT, "benchmarks", "comparison", "reference", "amber")
 NAME = "alanine_dipeptide_tip4pew"
 
 
@@ -76,7 +78,7 @@ def frame(iteration, perturbation):
     src = os.path.join(CASE, "statics", NAME, "system_minimized.rst7")
     if perturbation == 0.0:
         return read_rst7(src)
-    sys.path.insert(0, "/root/reference")
+    sys.path.insert(0, REF_ROOT)
     from benchmarks.comparison.tests.amber.tests.utils import (
         perturb_rst7_with_rigid_water_inplace)
     with tempfile.TemporaryDirectory() as d:
@@ -159,4 +161,6 @@ def make(iteration, perturbation):
 
 
 if __name__ == "__main__":
+    if not os.path.isdir(CASE):
+        raise SystemExit("set SPONGE_REFERENCE to the reference checkout's root")
     main()

@@ -87,3 +87,33 @@ def test_noalloc_rejects_more_atoms_than_its_scratch(g):
         None, None, None, None, 0, None, 0, None, None)
     assert rc == 1
     assert b"65536" in lib.snb_last_error()
+
+
+def test_noalloc_later_calls_leave_free_device_memory_unchanged(g, box_9k):
+    """After the first call (which may load the module and with it the static
+    array), further calls take no device memory: the free bytes the driver
+    reports stay the same and torch's allocator sees no new reservation."""
+    import torch
+    box = g.Box(box_9k)
+    beta, want = _with_handle(g, box)
+    _same(_noalloc(g, box, beta), want)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    reserved0 = torch.cuda.memory_reserved()
+    lib = g.capi.load()
+    n = box.n
+    frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+    ae = torch.zeros(n, dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6 * n, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    reserved1 = torch.cuda.memory_reserved()
+    for _ in range(3):
+        g.capi.check(lib.snb_pme_excluded_force_noalloc(
+            n, g.ptr(box.crd), box.b, g.ptr(box.charge), ctypes.c_float(beta), g.ptr(box.es),
+            g.ptr(box.el), g.ptr(box.en), g.ptr(frc), 1, g.ptr(ae), 1, g.ptr(vir),
+            g.stream()), "pme_excluded_force_noalloc")
+    torch.cuda.synchronize()
+    free2, _ = torch.cuda.mem_get_info()
+    assert torch.cuda.memory_reserved() == reserved1
+    assert free2 == free1, (free0, free1, free2, reserved0, reserved1)
