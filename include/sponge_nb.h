@@ -106,6 +106,13 @@ typedef struct snb_settle snb_settle;
 
 /* ---------------------------------------------------------------- misc */
 int snb_version(void);
+/* No counterpart in the reference: a self-check of the pair kernels'
+ * screened-Coulomb factors.  For each x = d_x[i] >= 0 writes d_out[4i..4i+3]
+ * = {erfc(x), exp(-x^2)} as the pair kernels form them (erfc from a
+ * polynomial in 1/(1 + x/2) times exp(-x^2) for x <= 4) and CUDA's
+ * {erfcf(x), expf(-x^2)}, so tests can hold the two against each other and
+ * against double precision. */
+int snb_check_erfc_exp(int n, const float* d_x, float* d_out, void* stream);
 const char* snb_last_error(void);
 void snb_options_default(snb_options* opt);
 int snb_options_set(snb_options* opt, const char* key, const char* value);
@@ -264,6 +271,15 @@ int snb_pme_excluded_force(snb_pme* pme, int atom_numbers,
  * of the last energy/virial evaluation, FP64 (host sync). */
 int snb_pme_energies(snb_pme* pme, double* h_reciprocal, double* h_self,
                      double* h_virial6, void* stream);
+/* The spread step of PME_Q_Spread (PM_force.cpp:765-814) sums each grid
+ * point's charge in int32 fixed point (2^22 per 18.2223-scaled charge unit,
+ * so |Q| < 512 at a point) inside its 8x8x8 tile.  A bound on every point's
+ * sum is kept per 4x4x4 octant of the tile (the atoms' |q| times the largest
+ * B-spline weight product); a tile where it could reach the int32 range (far
+ * above any dense liquid) is taken again with int64 sums, so the grid stays
+ * exact.  *count = how many tiles were taken again since the handle was made
+ * (host sync). */
+int snb_pme_spread_wide_tiles(snb_pme* pme, int* count, void* stream);
 /* Particle_Mesh::Update_Box (PM_force.h:180, PM_force.cpp:1171-1248): the
  * reciprocal part follows the new rectangular box in `boundary` at the same
  * grid size (the influence function and the neutralising term are formed
@@ -432,6 +448,8 @@ int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
 /* Number of neighbor-list rebuilds so far and current pair count (host sync). */
 int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
                      void* stream);
+/* snb_pme_spread_wide_tiles of the engine's PME (host sync). */
+int snb_engine_spread_wide_tiles(snb_engine* e, int* count, void* stream);
 int snb_engine_destroy(snb_engine* e);
 
 /* ----------------------------------------------------------- 1-4 terms */

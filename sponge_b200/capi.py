@@ -49,6 +49,7 @@ class snb_options(ctypes.Structure):
 
 EXPORTED = [
     "snb_version", "snb_last_error", "snb_options_default", "snb_options_set",
+    "snb_check_erfc_exp",
     "snb_nl_create", "snb_nl_update", "snb_nl_check_overflow", "snb_nl_pair_count",
     "snb_nl_export_pairs", "snb_nl_export_atom_groups", "snb_nl_destroy",
     "snb_lj_create", "snb_lj_get_local", "snb_lj_pme_direct_force", "snb_solvent_lj_pme_direct_force",
@@ -57,7 +58,7 @@ EXPORTED = [
     "snb_lj_soft_create", "snb_lj_soft_pme_direct_force", "snb_lj_soft_dh_dlambda",
     "snb_lj_soft_long_range_correction", "snb_lj_soft_energy_sums", "snb_lj_soft_destroy",
     "snb_pme_create", "snb_pme_beta", "snb_pme_grid", "snb_pme_reciprocal_force",
-    "snb_pme_excluded_force", "snb_pme_energies", "snb_pme_update_box", "snb_pme_destroy",
+    "snb_pme_excluded_force", "snb_pme_energies", "snb_pme_spread_wide_tiles", "snb_pme_update_box", "snb_pme_destroy",
     "snb_pme_excluded_force_noalloc",
     "snb_engine_create", "snb_batch_create", "snb_engine_force", "snb_engine_set_bonded",
     "snb_engine_set_soft_core", "snb_engine_update_box", "snb_engine_set_nb14",
@@ -68,6 +69,7 @@ EXPORTED = [
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_md_steps_host",
     "snb_engine_profile_steps",
     "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
+    "snb_engine_spread_wide_tiles",
     "snb_engine_destroy",
     "snb_read_lj_in_file", "snb_read_lj_soft_core_in_file", "snb_read_subsys_division_in_file",
     "snb_read_charge_in_file", "snb_read_mass_in_file", "snb_read_exclude_in_file",
@@ -131,6 +133,8 @@ _SIGS = {
                                     _I, _P, _I, _P, _P]),
     "snb_pme_update_box": (_I, [_P, snb_boundary, _P, _F]),
     "snb_pme_energies": (_I, [_P, _P, _P, _P, _P]),
+    "snb_pme_spread_wide_tiles": (_I, [_P, ctypes.POINTER(ctypes.c_int), _P]),
+    "snb_check_erfc_exp": (_I, [_I, _P, _P, _P]),
     "snb_pme_destroy": (_I, [_P]),
     "snb_pme_excluded_force_noalloc": (_I, [_I, _P, snb_boundary, _P, _F, _P, _P, _P, _P,
                                             _I, _P, _I, _P, _P]),
@@ -174,6 +178,7 @@ _SIGS = {
     "snb_engine_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I),
                                    ctypes.POINTER(_I), _P]),
     "snb_engine_stats": (_I, [_P, ctypes.POINTER(_LL), ctypes.POINTER(_LL), _P]),
+    "snb_engine_spread_wide_tiles": (_I, [_P, ctypes.POINTER(ctypes.c_int), _P]),
     "snb_engine_destroy": (_I, [_P]),
 }
 

@@ -885,6 +885,11 @@ extern "C" int snb_pme_excluded_force(snb_pme* h, int atom_numbers,
                        need_energy != 0, need_virial != 0, st);
 }
 
+extern "C" int snb_pme_spread_wide_tiles(snb_pme* h, int* count, void* stream) {
+  if (!h || !count) return fail(kBadInput, "pme_spread_wide_tiles: null argument");
+  return pme_wide_tiles(h->p, count, S(stream));
+}
+
 extern "C" int snb_pme_energies(snb_pme* h, double* rec, double* self, double* vir,
                                 void* stream) {
   if (!h) return fail(kBadInput, "pme_energies: null handle");
@@ -2029,6 +2034,11 @@ extern "C" int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
   rc = count(g, library_kernel_nodes);
   cudaGraphDestroy(g);
   return rc;
+}
+
+extern "C" int snb_engine_spread_wide_tiles(snb_engine* e, int* count, void* stream) {
+  if (!e || !count) return fail(kBadInput, "engine_spread_wide_tiles: null argument");
+  return pme_wide_tiles(e->pme, count, S(stream));
 }
 
 extern "C" int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,

@@ -155,10 +155,12 @@ __device__ __forceinline__ double warp_sum(double v) {
 // a degree-8 polynomial in t = 1/(1 + x/2) on [0, 4] (weighted least-squares
 // fit against double-precision erfcx; max relative error 3.3e-7 in float32), so
 // erfc(x) = P(t) * exp(-x^2).  exp uses the hardware exp2 (__expf: error
-// 2 + 1.16|x^2| ulp, below 1e-6 relative for x <= 4); t uses the fast
-// hardware division (2 ulp; |t P'(t) / P(t)| <= 2.26 on the range, so P
-// moves by at most 5.4e-7 relative through it).  Beyond x = 4 CUDA's erfcf
-// and expf are used.
+// 2 + 1.16|x^2| ulp; measured 8.9e-7 relative at most on [0, 3], the range
+// beta r takes below the cutoff); t uses the fast hardware division (2 ulp;
+// |t P'(t) / P(t)| <= 2.26 on the range, so P moves by at most 5.4e-7
+// relative through it).  Together erfc is within 1.01e-6 of double
+// precision on [0, 3] (measured on B200), CUDA's erfcf within 2.9e-7.
+// Beyond x = 4 CUDA's erfcf and expf are used.
 __device__ __forceinline__ float erfc_and_exp(float x, float* e_out) {
   if (x > 4.0f) {
     *e_out = expf(-x * x);

@@ -370,6 +370,10 @@ struct PME {
   double* d_sys_sums = nullptr;    // [nsys][8]
   int* d_tile_sys = nullptr;       // [ntiles]
   int gather_threads = 256;        // threads per block of the force gather
+  // running count of spread tiles whose int32 fixed-point sums could have
+  // left the int32 range (an octant bound of 512 charge units or more at a
+  // point) and were taken again in int64
+  int* d_wide_tiles = nullptr;
 };
 int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
              float cutoff, float tolerance, int fftx, int ffty, int fftz,
@@ -394,6 +398,8 @@ int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const in
                  const int* perm, float4* pos, int* type_sorted, cudaStream_t st);
 int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
                   bool need_virial, cudaStream_t st);
+// Reads the count of spread tiles redone with int64 sums (host sync).
+int pme_wide_tiles(PME& p, int* count, cudaStream_t st);
 
 // Excluded-pair correction (PM_force.cpp:1745-1817).  Caller-frame inputs;
 // forces land in acc at map[i] (map = inv_perm, or nullptr for identity).

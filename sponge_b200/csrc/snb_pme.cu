@@ -277,9 +277,36 @@ __device__ __forceinline__ void stencil_local(int u, int K, int lo, int hi, int*
   }
 }
 
-__device__ __forceinline__ void spread_atom(int* sq, float4 f, int up, const TileGeom& g,
+// Bound on the int32 tile sums.  A point's sum is at most the sum, over the
+// atoms whose stencils reach it, of |q| 2^22 (2/3)^3 (each B-spline weight is
+// at most 2/3) plus 1/2 for the rounding; every such atom's stencil meets the
+// 4x4x4 octant of the tile that holds the point.  So each lane keeps, per
+// octant, the bound of the atoms it spreads that meet the octant; when the
+// block's sum of some octant could reach the int32 range the tile is taken
+// again with int64 sums.  A liquid's octants stay below a tenth of the range.
+constexpr float kPointWeightBound = 0.2963f * 1.0001f;  // (2/3)^3 and float slack
+constexpr float kTileSumLimit = 0.99f * 2147483648.0f;
+
+__device__ __forceinline__ void tile_add(int* p, int c) { atomicAdd(p, c); }
+__device__ __forceinline__ void tile_add(long long* p, int c) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(p),
+            static_cast<unsigned long long>((long long)c));
+}
+
+// Bits of the 4-point halves (local index >> 2) a stencil axis touches.
+__device__ __forceinline__ int halves_of(const int* l) {
+  int m = 0;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) m |= l[o] >= 0 ? 1 << (l[o] >> 2) : 0;
+  return m;
+}
+
+// Spreads one atom into the tile's store sq (local x runs from lo0); with
+// BOUND the atom's per-point bound is added to each octant its stencil meets.
+template <typename Acc, bool BOUND>
+__device__ __forceinline__ void spread_atom(Acc* sq, float4 f, int up, const TileGeom& g,
                                             int lo0, int hi0, int lo1, int hi1, int lo2,
-                                            int hi2) {
+                                            int hi2, float* oct) {
   const int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
   int lx[4], ly[4], lz[4];
   stencil_local(ux, g.K0, lo0, hi0, lx);
@@ -290,6 +317,14 @@ __device__ __forceinline__ void spread_atom(int* sq, float4 f, int up, const Til
   bspline4(f.y, wy);
   bspline4(f.z, wz);
   const float qs = f.w * kGridScale;
+  if (BOUND) {
+    const float b = fabsf(qs) * kPointWeightBound + 0.5f;
+    const int mx = halves_of(lx), my = halves_of(ly), mz = halves_of(lz);
+#pragma unroll
+    for (int o = 0; o < 8; ++o)
+      if ((mx >> (o >> 2) & 1) && (my >> ((o >> 1) & 1) & 1) && (mz >> (o & 1) & 1))
+        oct[o] += b;
+  }
 #pragma unroll
   for (int ox = 0; ox < 4; ++ox) {
     if (lx[ox] < 0) continue;
@@ -298,64 +333,21 @@ __device__ __forceinline__ void spread_atom(int* sq, float4 f, int up, const Til
     for (int oy = 0; oy < 4; ++oy) {
       if (ly[oy] < 0) continue;
       const float wxy = wq * wy[oy];
-      int* row = sq + (lx[ox] * kTile + ly[oy]) * kTile;
+      Acc* row = sq + (lx[ox] * kTile + ly[oy]) * kTile;
 #pragma unroll
       for (int oz = 0; oz < 4; ++oz)
-        if (lz[oz] >= 0) atomicAdd(row + lz[oz], __float2int_rn(wxy * wz[oz]));
+        if (lz[oz] >= 0) tile_add(row + lz[oz], __float2int_rn(wxy * wz[oz]));
     }
   }
 }
 
-template <bool BATCH>
-__global__ void __launch_bounds__(32 * kSpreadWarps)
-k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
-             const float4* __restrict__ binned, const int* __restrict__ binned_u,
-             const int4* __restrict__ src0, const int4* __restrict__ src1,
-             const int4* __restrict__ src2, float* __restrict__ Q, int ntiles,
-             BatchView bv) {
-  __shared__ int sq[kTile3];
-  __shared__ int list_all[kSpreadWarps][kSpreadList];
+// The contributors of one tile (pass 1 of k_pme_spread) spread into sq.
+template <typename Acc, bool BOUND>
+__device__ __forceinline__ void spread_contributors(
+    Acc* sq, int* list, const TileGeom& g, const float4* __restrict__ binned,
+    const int* __restrict__ binned_u, int lo0, int hi0, int lo1, int hi1, int lo2,
+    int hi2, int nb, int beg, int cnt, int excl, int total, float* oct) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int t = blockIdx.x;
-  int* list = list_all[w];
-  if (BATCH) {  // tile of one system: its geometry, tables and grid
-    const SysGeom& sg = bv.sys[bv.tile_sys[t]];
-    g = sys_tiles(sg);
-    t -= sg.tile_begin;
-    tile_start += sg.tile_begin;
-    src0 += sg.src_begin0;
-    src1 += sg.src_begin1;
-    src2 += sg.src_begin2;
-    Q += sg.grid_begin;
-  }
-  const int t2 = t % g.nt2, t1 = (t / g.nt2) % g.nt1, t0 = t / (g.nt1 * g.nt2);
-  const int lo0 = t0 * g.T, hi0 = min(lo0 + g.T, g.K0);
-  const int lo1 = t1 * g.T, hi1 = min(lo1 + g.T, g.K1);
-  const int lo2 = t2 * g.T, hi2 = min(lo2 + g.T, g.K2);
-  for (int k = threadIdx.x; k < kTile3; k += blockDim.x) sq[k] = 0;
-  __syncthreads();
-  // the (up to 27) source bins: lane b holds bin b's first atom and count
-  const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
-  const int nb = s0.x * s1.x * s2.x;
-  int beg = 0, cnt = 0;
-  if (lane < nb) {
-    const int a = lane / (s1.x * s2.x), b = (lane / s2.x) % s1.x, c = lane % s2.x;
-    const int b0 = a == 0 ? s0.y : (a == 1 ? s0.z : s0.w);
-    const int b1 = b == 0 ? s1.y : (b == 1 ? s1.z : s1.w);
-    const int b2 = c == 0 ? s2.y : (c == 1 ? s2.z : s2.w);
-    const int bin = (b0 * g.nt1 + b1) * g.nt2 + b2;
-    beg = tile_start[bin];
-    cnt = tile_start[bin + 1] - beg;
-  }
-  int incl = cnt;  // inclusive prefix of the counts over the bins
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
-  const int excl = incl - cnt;
-  __syncwarp();
   const unsigned lt = (1u << lane) - 1u;
   int n_list = 0, bin_cursor = 0;
   for (int base = 32 * w; base < total; base += 32 * kSpreadWarps) {
@@ -384,14 +376,113 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
       __syncwarp();
       for (int e = lane; e < n_list; e += 32) {
         const int ka = list[e];
-        spread_atom(sq, binned[ka], binned_u[ka], g, lo0, hi0, lo1, hi1, lo2, hi2);
+        spread_atom<Acc, BOUND>(sq, binned[ka], binned_u[ka], g, lo0, hi0, lo1, hi1, lo2,
+                                hi2, oct);
       }
       __syncwarp();
       n_list = 0;
     }
   }
+}
+
+// wide_tiles (may be null): running count of tiles taken again with int64
+// sums because an octant's bound could reach the int32 range.  Sixteen
+// blocks of 64 threads at 64 registers fill an SM's register file.
+template <bool BATCH>
+__global__ void __launch_bounds__(32 * kSpreadWarps, 16)
+k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
+             const float4* __restrict__ binned, const int* __restrict__ binned_u,
+             const int4* __restrict__ src0, const int4* __restrict__ src1,
+             const int4* __restrict__ src2, float* __restrict__ Q, int ntiles,
+             BatchView bv, int* __restrict__ wide_tiles) {
+  // the tile's int32 sums; the same 2 KB hold half a tile of int64 sums
+  __shared__ __align__(8) int sq[kTile3];
+  __shared__ int list_all[kSpreadWarps][kSpreadList];
+  __shared__ float oct_sum[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int t = blockIdx.x;
+  int* list = list_all[w];
+  if (BATCH) {  // tile of one system: its geometry, tables and grid
+    const SysGeom& sg = bv.sys[bv.tile_sys[t]];
+    g = sys_tiles(sg);
+    t -= sg.tile_begin;
+    tile_start += sg.tile_begin;
+    src0 += sg.src_begin0;
+    src1 += sg.src_begin1;
+    src2 += sg.src_begin2;
+    Q += sg.grid_begin;
+  }
+  const int t2 = t % g.nt2, t1 = (t / g.nt2) % g.nt1, t0 = t / (g.nt1 * g.nt2);
+  const int lo0 = t0 * g.T, hi0 = min(lo0 + g.T, g.K0);
+  const int lo1 = t1 * g.T, hi1 = min(lo1 + g.T, g.K1);
+  const int lo2 = t2 * g.T, hi2 = min(lo2 + g.T, g.K2);
+  for (int k = threadIdx.x; k < kTile3; k += blockDim.x) sq[k] = 0;
+  if (threadIdx.x < 8) oct_sum[threadIdx.x] = 0.f;
   __syncthreads();
+  // the (up to 27) source bins: lane b holds bin b's first atom and count
+  const int4 s0 = src0[t0], s1 = src1[t1], s2 = src2[t2];
+  const int nb = s0.x * s1.x * s2.x;
+  int beg = 0, cnt = 0;
+  if (lane < nb) {
+    const int a = lane / (s1.x * s2.x), b = (lane / s2.x) % s1.x, c = lane % s2.x;
+    const int b0 = a == 0 ? s0.y : (a == 1 ? s0.z : s0.w);
+    const int b1 = b == 0 ? s1.y : (b == 1 ? s1.z : s1.w);
+    const int b2 = c == 0 ? s2.y : (c == 1 ? s2.z : s2.w);
+    const int bin = (b0 * g.nt1 + b1) * g.nt2 + b2;
+    beg = tile_start[bin];
+    cnt = tile_start[bin + 1] - beg;
+  }
+  int incl = cnt;  // inclusive prefix of the counts over the bins
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  const int excl = incl - cnt;
+  __syncwarp();
+  float oct[8];
+#pragma unroll
+  for (int o = 0; o < 8; ++o) oct[o] = 0.f;
+  spread_contributors<int, true>(sq, list, g, binned, binned_u, lo0, hi0, lo1, hi1, lo2,
+                                 hi2, nb, beg, cnt, excl, total, oct);
+#pragma unroll
+  for (int o = 0; o < 8; ++o) {
+    const float v = warp_sum(oct[o]);
+    if (lane == 0 && v != 0.f) atomicAdd(&oct_sum[o], v);
+  }
+  __syncthreads();
+  bool wide = false;
+#pragma unroll
+  for (int o = 0; o < 8; ++o) wide |= !(oct_sum[o] < kTileSumLimit);
   const int w0 = hi0 - lo0, w1 = hi1 - lo1, w2 = hi2 - lo2;
+  if (wide) {
+    // some point's int32 sum could have wrapped: take the tile again in two
+    // halves along x, each with int64 sums (exact and order-independent like
+    // the int32 ones) in the same 2 KB; values that fit int32 convert to the
+    // same floats
+    long long* sq64 = reinterpret_cast<long long*>(sq);
+    constexpr int kHalf = kTile3 / 2;
+    for (int h = 0; h < 2; ++h) {
+      const int hlo = lo0 + 4 * h, hhi = min(hlo + 4, hi0);
+      __syncthreads();
+      for (int k = threadIdx.x; k < kHalf; k += blockDim.x) sq64[k] = 0;
+      __syncthreads();
+      if (hlo < hhi)
+        spread_contributors<long long, false>(sq64, list, g, binned, binned_u, hlo, hhi,
+                                              lo1, hi1, lo2, hi2, nb, beg, cnt, excl,
+                                              total, oct);
+      __syncthreads();
+      for (int k = threadIdx.x; k < kHalf; k += blockDim.x) {
+        int x = k / (kTile * kTile), y = (k / kTile) % kTile, z = k % kTile;
+        if (x < hhi - hlo && y < w1 && z < w2)
+          Q[((size_t)(hlo + x) * g.K1 + (lo1 + y)) * g.K2 + (lo2 + z)] =
+              (float)((double)sq64[k] * (double)kGridScaleInv);
+      }
+    }
+    if (threadIdx.x == 0 && wide_tiles) atomicAdd(wide_tiles, 1);
+    return;
+  }
   for (int k = threadIdx.x; k < kTile3; k += blockDim.x) {
     int x = k / (kTile * kTile), y = (k / kTile) % kTile, z = k % kTile;
     if (x < w0 && y < w1 && z < w2)
@@ -788,6 +879,8 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
   SNB_CUDA_TRY(cudaMalloc(&p.d_partial, sizeof(double) * 8 * p.partial_blocks));
   SNB_CUDA_TRY(cudaMalloc(&p.d_sums, sizeof(double) * 8));
   SNB_CUDA_TRY(cudaMemset(p.d_sums, 0, sizeof(double) * 8));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_wide_tiles, sizeof(int)));
+  SNB_CUDA_TRY(cudaMemset(p.d_wide_tiles, 0, sizeof(int)));
   if (scan_reserve(p.scan, p.ntiles)) return kCudaError;
   if (cufftPlan3d(&p.plan_r2c, p.K[0], p.K[1], p.K[2], CUFFT_R2C) != CUFFT_SUCCESS ||
       cufftPlan3d(&p.plan_c2r, p.K[0], p.K[1], p.K[2], CUFFT_C2R) != CUFFT_SUCCESS)
@@ -923,6 +1016,8 @@ int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
   SNB_CUDA_TRY(cudaMalloc(&p.d_partial, sizeof(double) * 8 * p.partial_blocks));
   SNB_CUDA_TRY(cudaMalloc(&p.d_sums, sizeof(double) * 8));
   SNB_CUDA_TRY(cudaMemset(p.d_sums, 0, sizeof(double) * 8));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_wide_tiles, sizeof(int)));
+  SNB_CUDA_TRY(cudaMemset(p.d_wide_tiles, 0, sizeof(int)));
   if (scan_reserve(p.scan, p.ntiles)) return kCudaError;
   for (auto& fg : p.groups) {
     int dims[3] = {fg.K[0], fg.K[1], fg.K[2]};
@@ -935,7 +1030,18 @@ int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
   return kOk;
 }
 
+int pme_wide_tiles(PME& p, int* count, cudaStream_t st) {
+  int v = 0;
+  if (p.d_wide_tiles) {
+    SNB_CUDA_TRY(cudaMemcpyAsync(&v, p.d_wide_tiles, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SNB_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  *count = v;
+  return kOk;
+}
+
 void pme_free(PME& p) {
+  cudaFree(p.d_wide_tiles);
   for (auto& fg : p.groups) {
     if (fg.r2c) cufftDestroy(fg.r2c);
     if (fg.c2r) cufftDestroy(fg.c2r);
@@ -1009,11 +1115,11 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
     if (batch)
       k_pme_spread<true><<<sblocks, 32 * kSpreadWarps, 0, st>>>(
           g, p.d_tile_start, p.d_binned, p.d_binned_u, p.d_src[0], p.d_src[1], p.d_src[2],
-          p.d_Q, p.ntiles, p.bv);
+          p.d_Q, p.ntiles, p.bv, p.d_wide_tiles);
     else
       k_pme_spread<false><<<sblocks, 32 * kSpreadWarps, 0, st>>>(
           g, p.d_tile_start, p.d_binned, p.d_binned_u, p.d_src[0], p.d_src[1], p.d_src[2],
-          p.d_Q, p.ntiles, p.bv);
+          p.d_Q, p.ntiles, p.bv, p.d_wide_tiles);
   } else {
     if (batch) return fail(kNotSupported, "PME batch: fixed-point accumulation only");
     SNB_CUDA_TRY(cudaMemsetAsync(p.d_Q, 0, sizeof(float) * p.nall, st));

@@ -307,3 +307,29 @@ int launch_unpack(int n, const int* map, Accumulators& acc, int accum,
 }
 
 }  // namespace snb
+
+// ---------------------------------------------------------------------------
+// Self-check of the pair kernels' screened-Coulomb factors: erfc(x) and
+// exp(-x^2) as erfc_and_exp forms them, beside CUDA's erfcf and expf.
+__global__ void k_check_erfc(int n, const float* __restrict__ x, float* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float v = x[i];
+  float e;
+  const float c = snb::erfc_and_exp(v, &e);
+  out[4 * i + 0] = c;
+  out[4 * i + 1] = e;
+  out[4 * i + 2] = erfcf(v);
+  out[4 * i + 3] = expf(-v * v);
+}
+
+extern "C" int snb_check_erfc_exp(int n, const float* d_x, float* d_out, void* stream) {
+  using namespace snb;
+  if (n < 0 || (n > 0 && (!d_x || !d_out)))
+    return fail(kBadInput, "check_erfc_exp: bad arguments");
+  if (n == 0) return kOk;
+  k_check_erfc<<<ceil_div(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      n, d_x, d_out);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
