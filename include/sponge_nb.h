@@ -450,6 +450,22 @@ int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
                      void* stream);
 /* snb_pme_spread_wide_tiles of the engine's PME (host sync). */
 int snb_engine_spread_wide_tiles(snb_engine* e, int* count, void* stream);
+/* The engine's neighbor list holds the pair set of NEIGHBOR_LIST::Update
+ * (neighbor_list.cpp:974-1025) in one of two forms.  Rows (the default):
+ * one row of partners per atom, as snb_nl keeps them.  Clusters (on request,
+ * for one rectangular box of at least five cells per axis, not with the
+ * soft-core kernel): runs of up to four atoms of a cell, and per cluster
+ * the clusters with a pair within cutoff + skin, each with its 4x4 pair
+ * mask; the pair kernel loads a neighbour cluster once for four atoms.
+ * Both hold the same pairs.  clusters = 0 / 1 picks the form (1 is refused
+ * where the box or the soft-core kernel does not allow it); the next step
+ * rebuilds the list. */
+int snb_engine_set_list_form(snb_engine* e, int clusters);
+int snb_engine_list_form(snb_engine* e, int* clusters);
+/* The engine's current pair set in global ids, lo < hi, in no particular
+ * order (as snb_nl_export_pairs; host sync). */
+int snb_engine_export_pairs(snb_engine* e, int* d_pi, int* d_pj, long long cap,
+                            long long* count, void* stream);
 int snb_engine_destroy(snb_engine* e);
 
 /* ----------------------------------------------------------- 1-4 terms */

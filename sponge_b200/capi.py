@@ -69,7 +69,8 @@ EXPORTED = [
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_md_steps_host",
     "snb_engine_profile_steps",
     "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
-    "snb_engine_spread_wide_tiles",
+    "snb_engine_spread_wide_tiles", "snb_engine_set_list_form", "snb_engine_list_form",
+    "snb_engine_export_pairs",
     "snb_engine_destroy",
     "snb_read_lj_in_file", "snb_read_lj_soft_core_in_file", "snb_read_subsys_division_in_file",
     "snb_read_charge_in_file", "snb_read_mass_in_file", "snb_read_exclude_in_file",
@@ -179,6 +180,9 @@ _SIGS = {
                                    ctypes.POINTER(_I), _P]),
     "snb_engine_stats": (_I, [_P, ctypes.POINTER(_LL), ctypes.POINTER(_LL), _P]),
     "snb_engine_spread_wide_tiles": (_I, [_P, ctypes.POINTER(ctypes.c_int), _P]),
+    "snb_engine_set_list_form": (_I, [_P, _I]),
+    "snb_engine_list_form": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
+    "snb_engine_export_pairs": (_I, [_P, _P, _P, _LL, ctypes.POINTER(_LL), _P]),
     "snb_engine_destroy": (_I, [_P]),
 }
 

@@ -1219,12 +1219,15 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   if (rc) return rc;
   prof_mark(e, 1, st);
   const bool do_pme = e->pme.reciprocal && step % e->pme.update_interval == 0;
+  // cluster form: the pair frame holds each atom in its cell's image
+  const bool clus = e->nl.clusters && !e->soft;
+  const float3* img = clus ? e->nl.d_img_off : nullptr;
   if (do_pme)
     rc = pme_pack_bin(e->pme, e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
-                      e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st);
+                      e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st, img);
   else
     rc = launch_pack(e->n, reinterpret_cast<const float3*>(crd), e->d_charge,
-                     e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st);
+                     e->lj.d_type, e->nl.d_perm, e->d_pos, e->d_type_sorted, st, img);
   if (rc) return rc;
   if (e->soft)
     k_pack_soft<<<ceil_div(e->n, 256), 256, 0, st>>>(e->n, e->nl.d_perm, e->soft->d_par_local,
@@ -1302,6 +1305,25 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
     sa.sigma6 = e->soft->sigma6;
     sa.sigma6_min = e->soft->sigma6_min;
     rc = launch_soft_rows(sa, e->acc, energy, virial, st);
+  } else if (clus) {
+    ClusterPairArgs ca;
+    ca.clus = e->nl.d_clus;
+    ca.nclus = e->nl.d_nclus;
+    ca.crow_count = e->nl.d_crow_count;
+    ca.centry = e->nl.d_centry;
+    ca.ccap = e->nl.ccap;
+    ca.pos = e->d_pos;
+    ca.type = e->d_type_sorted;
+    ca.global = e->nl.d_global;
+    ca.nl_flags = e->nl.d_flags;
+    ca.A = e->lj.d_A;
+    ca.B = e->lj.d_B;
+    ca.n_types = e->lj.n_types;
+    ca.box = make_float3(e->cell.a11, e->cell.a22, e->cell.a33);
+    ca.cutoff2 = a.cutoff2;
+    ca.beta = a.beta;
+    ca.blocks_per_sm = e->pair_blocks_per_sm;
+    rc = launch_pair_clusters(ca, e->acc, e->accum, energy, virial, st);
   } else {
     rc = launch_pair(a, e->acc, e->accum, energy, virial, true, st);
   }
@@ -1601,6 +1623,12 @@ extern "C" int snb_engine_set_soft_core(snb_engine* e, snb_lj_soft* soft) {
     if (soft->n != e->n) return fail(kBadInput, "engine_set_soft_core: atom count differs");
   }
   e->soft = soft;
+  // the soft-core pair kernel reads the rows
+  if (soft && e->nl.clusters) {
+    int rc = nl_set_clusters(e->nl, false);
+    if (rc) return rc;
+    e->steps_done = 0;  // the next step rebuilds the list in its new form
+  }
   if (soft) {
     const double vol = (double)e->cell.a11 * e->cell.a22 * e->cell.a33;
     e->lrc_energy = soft->lrc / vol;
@@ -1921,8 +1949,10 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
   int rc = kOk;
   double best = 1e30, ms = 0.0;
   int bu = e->pair_unroll, bb = e->pair_blocks_per_sm;
+  const bool rows = !(e->nl.clusters && !e->soft);
   for (int u : {2, 4, 8})
     for (int b : {0, 2, 3}) {
+      if (!rows && u != bu) continue;  // the cluster kernel has no unroll choice
       e->pair_unroll = u;
       e->pair_blocks_per_sm = b;
       if ((rc = measure(-1, false, &ms))) break;  // the step, PME branch alongside
@@ -2034,6 +2064,34 @@ extern "C" int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
   rc = count(g, library_kernel_nodes);
   cudaGraphDestroy(g);
   return rc;
+}
+
+extern "C" int snb_engine_set_list_form(snb_engine* e, int clusters) {
+  if (!e) return fail(kBadInput, "engine_set_list_form: null handle");
+  if (clusters && e->soft)
+    return fail(kNotSupported, "engine_set_list_form: the soft-core kernel reads rows");
+  int rc = nl_set_clusters(e->nl, clusters != 0);
+  if (rc) return rc;
+  if (e->graph_exec) {  // the captured step holds the previous list form
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+    e->graph = nullptr;
+  }
+  e->steps_done = 0;
+  return kOk;
+}
+
+extern "C" int snb_engine_list_form(snb_engine* e, int* clusters) {
+  if (!e || !clusters) return fail(kBadInput, "engine_list_form: null argument");
+  *clusters = e->nl.clusters && !e->soft ? 1 : 0;
+  return kOk;
+}
+
+extern "C" int snb_engine_export_pairs(snb_engine* e, int* d_pi, int* d_pj, long long cap,
+                                       long long* count, void* stream) {
+  if (!e || !count) return fail(kBadInput, "engine_export_pairs: null argument");
+  return nl_export_pairs(e->nl, d_pi, d_pj, cap, count, S(stream));
 }
 
 extern "C" int snb_engine_spread_wide_tiles(snb_engine* e, int* count, void* stream) {

@@ -130,7 +130,32 @@ struct NeighborList {
   ScanScratch scan;
   long long last_total = 0;
   int generation = 0;
+  // Cluster form of the list (the engine's single-box step; needs at least
+  // five cells per axis).  Inside a cell the atoms follow a path up and down
+  // its four xy quarter columns, and every run of up to kClusterSize of them
+  // is one cluster.  Row c lists the j-clusters with a pair within r_l of
+  // i-cluster c: {first sorted atom of j, 4x4 pair mask | shift code << 16}.
+  // Pair-frame coordinates are crd - img_off (each atom in its build-time
+  // cell image); the shift code gives the periodic image of j's cell.
+  bool clusters = false;
+  int maxclus = 0;
+  int* d_atom_key = nullptr;     // [n] caller frame: order key inside the cell
+  int* d_clus_count = nullptr;   // [ncell] clusters of each cell
+  int* d_cell_clus = nullptr;    // [ncell + 1] first cluster of each cell
+  int2* d_clus = nullptr;        // [maxclus] {first sorted atom, atom count}
+  float4* d_clus_lo = nullptr;   // [maxclus] bounding box in the wrapped frame
+  float4* d_clus_hi = nullptr;
+  int* d_nclus = nullptr;        // [1] clusters of the last build
+  float3* d_img_off = nullptr;   // [n] sorted frame: box offset of the cell image
+  int* d_crow_count = nullptr;   // [maxclus]
+  int2* d_centry = nullptr;      // [maxclus * ccap]
+  int ccap = 0;
 };
+constexpr int kClusterSize = 4;
+// Turns the cluster form on or off (single box, rectangular, at least five
+// cells per axis); the next update rebuilds.  Returns kNotSupported when the
+// box does not allow it.
+int nl_set_clusters(NeighborList& nl, bool on);
 
 int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell6,
             int refresh_interval, float skin_permit, int max_neighbor_numbers,
@@ -236,6 +261,28 @@ struct PairArgs {
 };
 int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool ortho, cudaStream_t st);
+
+// The pair kernel over the cluster form of the list.
+struct ClusterPairArgs {
+  const int2* clus;             // {first sorted atom, atom count}
+  const int* nclus;             // device count of clusters
+  const int* crow_count;
+  const int2* centry;           // {first atom of j, mask | shift code << 16}
+  int ccap;
+  const float4* pos;            // pair frame (x,y,z,q), sorted
+  const int* type;              // sorted LJ type
+  const int* global;            // sorted -> global id (owner rule)
+  const int* nl_flags;          // skip when the list overflowed
+  const float* A;
+  const float* B;
+  int n_types;
+  float3 box;                   // rectangular box lengths (image shifts)
+  float cutoff2;
+  float beta;
+  int blocks_per_sm = 0;        // persistent blocks per SM, 0: occupancy maximum
+};
+int launch_pair_clusters(const ClusterPairArgs& a, Accumulators& acc, int accum,
+                         bool energy, bool virial, cudaStream_t st);
 
 // Rigid triangle: atoms A, B, C, canonical frame (A at (0, ra), B at (rc, rb),
 // C at (rd, re) about the centre of mass) and masses.
@@ -394,8 +441,11 @@ int fft_size(float length);
 int pme_reciprocal(PME& p, const float4* pos, int n, Accumulators& acc,
                    int accum, bool need_energy, bool need_virial,
                    cudaStream_t st);
+// img_off (may be null): sorted-frame offsets subtracted from the pair
+// frame's coordinates (pos) only; the PME binning takes crd as given.
 int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const int* type,
-                 const int* perm, float4* pos, int* type_sorted, cudaStream_t st);
+                 const int* perm, float4* pos, int* type_sorted, cudaStream_t st,
+                 const float3* img_off = nullptr);
 int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
                   bool need_virial, cudaStream_t st);
 // Reads the count of spread tiles redone with int64 sums (host sync).
@@ -412,8 +462,10 @@ int launch_excluded(int n, const float3* crd, const float* charge,
 
 // ----------------------------------------------------------------------------
 // Frame conversion kernels.
+// pos[s] = (crd[perm[s]] - img_off[s] (when given), charge[perm[s]]).
 int launch_pack(int n, const float3* crd, const float* charge, const int* type,
-                const int* perm, float4* pos, int* type_sorted, cudaStream_t st);
+                const int* perm, float4* pos, int* type_sorted, cudaStream_t st,
+                const float3* img_off = nullptr);
 // frc[caller i] += acc[map[i]] (converted), optional energies/virials, then
 // zero the accumulators.
 int launch_unpack(int n, const int* map, Accumulators& acc, int accum,

@@ -18,6 +18,7 @@
 // within rl of atom i.  Hits go in one pass into rows of fixed capacity;
 // a row that would overflow raises a flag and the host regrows the rows.
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <map>
 #include <vector>
@@ -71,12 +72,31 @@ __device__ __forceinline__ int wrapped_cell(float3 r, const Cell& cell, int Nx,
   return (nx * Ny + ny) * Nz + nz;
 }
 
+// Order key of an atom inside its cell for the cluster form: the cell's four
+// xy quarter columns in the order (0,0) (0,1) (1,1) (1,0), z rising in the
+// first and third and falling in the second and fourth, so that consecutive
+// atoms stay close across the turns; z in 2^-22 steps of the cell height.
+__device__ __forceinline__ int cell_order_key(float3 r, const Cell& cell, int Nx, int Ny,
+                                              int Nz, int c) {
+  const float x = r.x - floorf(r.x / cell.a11) * cell.a11;
+  const float y = r.y - floorf(r.y / cell.a22) * cell.a22;
+  const float z = r.z - floorf(r.z / cell.a33) * cell.a33;
+  const int cz = c % Nz, cy = (c / Nz) % Ny, cx = c / (Nz * Ny);
+  const bool hx = x / cell.a11 * Nx - (float)cx >= 0.5f;
+  const bool hy = y / cell.a22 * Ny - (float)cy >= 0.5f;
+  const int q = hx ? (hy ? 2 : 3) : (hy ? 1 : 0);
+  int zq = (int)((z / cell.a33 * Nz - (float)cz) * 4194304.0f);
+  zq = zq < 0 ? 0 : (zq > 4194303 ? 4194303 : zq);
+  if (q & 1) zq = 4194303 - zq;
+  return (q << 22) | zq;
+}
+
 template <bool BATCH>
 __global__ void k_bin_count(int n, const float3* __restrict__ crd, Cell cell,
                             int Nx, int Ny, int Nz, int* __restrict__ atom_cell,
                             int* __restrict__ atom_slot, int* __restrict__ cell_count,
                             int* __restrict__ excl_count, const int* flags,
-                            BatchView bv) {
+                            BatchView bv, int* __restrict__ atom_key) {
   if (flags[kFlagNeed] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -86,6 +106,7 @@ __global__ void k_bin_count(int n, const float3* __restrict__ crd, Cell cell,
     c = g.cell_begin + wrapped_cell(crd[i], g.cell, g.Nx, g.Ny, g.Nz);
   } else {
     c = wrapped_cell(crd[i], cell, Nx, Ny, Nz);
+    if (atom_key) atom_key[i] = cell_order_key(crd[i], cell, Nx, Ny, Nz, c);
   }
   atom_cell[i] = c;
   atom_slot[i] = atomicAdd(&cell_count[c], 1);
@@ -124,10 +145,12 @@ __global__ void k_bin_scatter(int n, const int* __restrict__ atom_cell,
   }
 }
 
-// One warp per cell: stable order inside the cell by caller index (rank sort).
+// One warp per cell: order inside the cell by caller index (rank sort), or
+// by (key, caller index) when keys are given.
 __global__ void k_cell_order(int ncell, const int* __restrict__ cell_start,
                              const int* __restrict__ unsorted,
-                             int* __restrict__ perm, const int* flags) {
+                             int* __restrict__ perm, const int* flags,
+                             const int* __restrict__ key) {
   if (flags[kFlagNeed] == 0) return;
   int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   int lane = threadIdx.x & 31;
@@ -136,17 +159,29 @@ __global__ void k_cell_order(int ncell, const int* __restrict__ cell_start,
   for (int k = a + lane; k < b; k += 32) {
     int v = unsorted[k];
     int rank = 0;
-    for (int m = a; m < b; ++m) rank += unsorted[m] < v;
+    if (key) {
+      const int kv = key[v];
+      for (int m = a; m < b; ++m) {
+        const int u = unsorted[m];
+        const int ku = key[u];
+        rank += ku < kv || (ku == kv && u < v);
+      }
+    } else {
+      for (int m = a; m < b; ++m) rank += unsorted[m] < v;
+    }
     perm[a + rank] = v;
   }
 }
 
+// img_off (may be null, single rectangular box): the offset that wraps the
+// atom into the box at this build, floor(r / L) L per axis, which the pair
+// frame subtracts until the next build.
 __global__ void k_fill_sorted(int n, const int* __restrict__ perm,
                               const float3* __restrict__ crd,
                               const int* __restrict__ atom_local,
                               int* __restrict__ inv_perm, int* __restrict__ global,
                               float4* __restrict__ pos, float3* __restrict__ old_crd,
-                              const int* flags) {
+                              const int* flags, float3* __restrict__ img_off, Cell cell) {
   if (flags[kFlagNeed] == 0) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
@@ -157,6 +192,10 @@ __global__ void k_fill_sorted(int n, const int* __restrict__ perm,
   float3 r = crd[i];
   pos[s] = make_float4(r.x, r.y, r.z, __int_as_float(g));  // w: global id bits
   old_crd[i] = r;
+  if (img_off)
+    img_off[s] = make_float3(floorf(r.x / cell.a11) * cell.a11,
+                             floorf(r.y / cell.a22) * cell.a22,
+                             floorf(r.z / cell.a33) * cell.a33);
 }
 
 // ---------------------------------------------------------------------------
@@ -388,6 +427,294 @@ k_pair_search(SearchArgs a) {
       atomicMax(&a.flags[kFlagMaxRow], count);
     }
   }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cluster form.  Clusters of a cell: ceil(count / kClusterSize).
+__global__ void k_clus_count(int ncell, const int* __restrict__ cell_start,
+                             int* __restrict__ clus_count, const int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ncell) return;
+  clus_count[k] = (cell_start[k + 1] - cell_start[k] + kClusterSize - 1) / kClusterSize;
+}
+
+// One thread per cell: its clusters' atom ranges and bounding boxes (in the
+// wrapped frame the binning used).
+__global__ void k_clus_fill(int ncell, const int* __restrict__ cell_start,
+                            const int* __restrict__ cell_clus,
+                            const float4* __restrict__ pos, Cell cell,
+                            int2* __restrict__ clus, float4* __restrict__ lo,
+                            float4* __restrict__ hi, const int* flags) {
+  if (flags[kFlagNeed] == 0) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ncell) return;
+  const int a = cell_start[k], b = cell_start[k + 1];
+  int cc = cell_clus[k];
+  for (int s = a; s < b; s += kClusterSize, ++cc) {
+    const int m = min(kClusterSize, b - s);
+    float3 l = make_float3(FLT_MAX, FLT_MAX, FLT_MAX);
+    float3 h = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    for (int t = 0; t < m; ++t) {
+      const float4 p = pos[s + t];
+      const float x = p.x - floorf(p.x / cell.a11) * cell.a11;
+      const float y = p.y - floorf(p.y / cell.a22) * cell.a22;
+      const float z = p.z - floorf(p.z / cell.a33) * cell.a33;
+      l = make_float3(fminf(l.x, x), fminf(l.y, y), fminf(l.z, z));
+      h = make_float3(fmaxf(h.x, x), fmaxf(h.y, y), fmaxf(h.z, z));
+    }
+    clus[cc] = make_int2(s, m);
+    lo[cc] = make_float4(l.x, l.y, l.z, 0.f);
+    hi[cc] = make_float4(h.x, h.y, h.z, 0.f);
+  }
+}
+
+struct ClusterSearchArgs {
+  const float4* pos;          // sorted build-time coordinates (x,y,z, global id bits)
+  const int* sorted_cell;
+  const int* cell_clus;
+  const int2* clus;
+  const float4* clus_lo;
+  const float4* clus_hi;
+  const int* nclus;
+  const int2* runs;
+  const char4* geom;
+  const int* run_count;
+  int max_runs;
+  int Nx, Ny, Nz;
+  Cell cell, rcell;
+  float rl2, rl2_lo, rl2_hi;
+  float reach2;               // (rl + margin)^2 for the box and run tests
+  float wx, wy, wz;           // cell widths
+  const int* excl_start;
+  const int* excl_list;
+  const int* excl_numbers;
+  const int* excl_count;      // E(x) sizes, or null
+  const int* excl_partner;
+  int* crow_count;
+  int ccap;
+  int2* centry;
+  int* flags;
+};
+
+// Distance, in cell widths, from the span [lo, hi] (fractions of the own
+// cell) to the cell at integer offset o along one axis.
+__device__ __forceinline__ float span_gap(int o, float lo, float hi) {
+  const float g = o > 0 ? (float)o - hi : (o < 0 ? lo - (float)(o + 1) : 0.f);
+  return fmaxf(g, 0.f);
+}
+
+// Gap between two boxes along an axis (centre distance minus half widths).
+__device__ __forceinline__ float box_gap(float lo_a, float hi_a, float lo_b, float hi_b,
+                                         float shift) {
+  const float d = fabsf(0.5f * (lo_b + hi_b) + shift - 0.5f * (lo_a + hi_a));
+  return fmaxf(d - 0.5f * (hi_a - lo_a) - 0.5f * (hi_b - lo_b), 0.f);
+}
+
+// One warp per i-cluster.  The candidates are the clusters of the own cell
+// from this one on and those of the owned runs, each run cut to the cells
+// within reach of the cluster's box; a candidate whose box (in the run's
+// periodic image) is within reach has its pairs tested with the reference's
+// exact criterion, eight candidates at a time (lane = 4 k + j: candidate k,
+// its atom j against the four i atoms every lane holds), and is listed when
+// any pair passes.  Exclusions and, inside one cluster, the order j > i are
+// applied in the mask.  The box tests only drop clusters that hold no pair
+// within r_l: box gaps bound the distances of the atoms inside from below,
+// with a 0.01 A margin over the rounding.
+__global__ void __launch_bounds__(256, 2) k_cluster_search(ClusterSearchArgs a) {
+  if (a.flags[kFlagNeed] == 0) return;
+  __shared__ int4 pass_all[8][32];  // {cluster, shift code, first atom, atoms}
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int nclus = *a.nclus;
+  const int per_block = (nclus + gridDim.x - 1) / gridDim.x;
+  const int c_end = min(nclus, (int)blockIdx.x * per_block + per_block);
+  const float Lx = a.cell.a11, Ly = a.cell.a22, Lz = a.cell.a33;
+  for (int c = blockIdx.x * per_block + w; c < c_end; c += nw) {
+    const int2 ci = a.clus[c];
+    const int cell = a.sorted_cell[ci.x];
+    const int cz = cell % a.Nz, cy = (cell / a.Nz) % a.Ny, cx = cell / (a.Nz * a.Ny);
+    const float4 blo = a.clus_lo[c], bhi = a.clus_hi[c];
+    const float flx = blo.x / a.wx - (float)cx, fhx = bhi.x / a.wx - (float)cx;
+    const float fly = blo.y / a.wy - (float)cy, fhy = bhi.y / a.wy - (float)cy;
+    const float flz = blo.z / a.wz - (float)cz, fhz = bhi.z / a.wz - (float)cz;
+    // the i atoms and their first two excluded partners, in every lane
+    float4 p_i[kClusterSize];
+    int g_i[kClusterSize], nex_i[kClusterSize], ex0_i[kClusterSize], ex1_i[kClusterSize];
+    bool lists_i[kClusterSize];
+    {
+      const bool own = lane < ci.y;
+      const float4 pl = a.pos[ci.x + (own ? lane : 0)];
+      const int gl = __float_as_int(pl.w);
+      int nl_ = 0, e0 = -1, e1 = -1;
+      bool li = a.excl_numbers != nullptr;
+      if (own && a.excl_count) {
+        nl_ = a.excl_count[gl];
+        if (nl_ <= kExclCap) {
+          li = false;
+          if (nl_ > 0) e0 = a.excl_partner[gl * kExclCap];
+          if (nl_ > 1) e1 = a.excl_partner[gl * kExclCap + 1];
+        } else {
+          nl_ = 0;
+        }
+      }
+#pragma unroll
+      for (int ii = 0; ii < kClusterSize; ++ii) {
+        p_i[ii] = make_float4(__shfl_sync(0xffffffffu, pl.x, ii),
+                              __shfl_sync(0xffffffffu, pl.y, ii),
+                              __shfl_sync(0xffffffffu, pl.z, ii), 0.f);
+        g_i[ii] = __shfl_sync(0xffffffffu, gl, ii);
+        nex_i[ii] = __shfl_sync(0xffffffffu, nl_, ii);
+        ex0_i[ii] = __shfl_sync(0xffffffffu, e0, ii);
+        ex1_i[ii] = __shfl_sync(0xffffffffu, e1, ii);
+        lists_i[ii] = __shfl_sync(0xffffffffu, (int)li, ii) != 0;
+      }
+    }
+    int count = 0, pairs = 0;
+    int2* out = a.centry + (size_t)c * a.ccap;
+    const int nr = a.run_count[cell];
+    for (int r0 = -1; r0 < nr; r0 += 32) {
+      const int r = r0 + lane;
+      int lo = 0, len = 0, code = 13;
+      if (r < 0) {
+        lo = c;
+        len = a.cell_clus[cell + 1] - c;
+      } else if (r < nr) {
+        const int2 rr = a.runs[(size_t)cell * a.max_runs + r];
+        const char4 g = a.geom[(size_t)cell * a.max_runs + r];
+        const float gx = span_gap(g.x, flx, fhx) * a.wx;
+        const float gy = span_gap(g.y, fly, fhy) * a.wy;
+        const float s2 = a.reach2 - gx * gx - gy * gy;
+        if (s2 >= 0.f) {
+          const float sz = sqrtf(s2) / a.wz;
+          const int zmax = (int)floorf(fhz + sz), zmin = (int)ceilf(flz - 1.f - sz);
+          const int z0 = max((int)g.z, zmin), z1 = min((int)g.w, zmax);
+          if (z0 <= z1) {
+            const int f = rr.x + (z0 - g.z), l = rr.y - (g.w - z1);
+            lo = a.cell_clus[f];
+            len = a.cell_clus[l + 1] - lo;
+            // periodic image of the run's cells relative to the own cell
+            const int ux = cx + g.x, uy = cy + g.y, uz = cz + g.z;
+            const int sx = ux < 0 ? -1 : (ux >= a.Nx ? 1 : 0);
+            const int sy = uy < 0 ? -1 : (uy >= a.Ny ? 1 : 0);
+            const int szz = uz < 0 ? -1 : (uz >= a.Nz ? 1 : 0);
+            code = (sx + 1) * 9 + (sy + 1) * 3 + (szz + 1);
+          }
+        }
+      }
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      const int excl = incl - len;
+      const int nq = min(32, nr - r0);
+      int cursor = 0;
+      for (int base = 0; base < total; base += 32) {
+        const int fi = base + lane;
+        int jc = -1, jcode = 13;
+        for (int q = cursor; q < nq; ++q) {  // warp-uniform
+          const int eq = __shfl_sync(0xffffffffu, excl, q);
+          const int lq = __shfl_sync(0xffffffffu, len, q);
+          const int oq = __shfl_sync(0xffffffffu, lo, q);
+          const int cq = __shfl_sync(0xffffffffu, code, q);
+          if (eq >= base + 32) break;
+          if (fi >= eq && fi < eq + lq) {
+            jc = oq + (fi - eq);
+            jcode = cq;
+          }
+          if (eq + lq > base + 32) break;
+          cursor = q + 1;
+        }
+        bool pass = false;
+        int2 cj = make_int2(0, 0);
+        if (jc >= 0) {
+          const float4 jl = a.clus_lo[jc], jh = a.clus_hi[jc];
+          cj = a.clus[jc];
+          const float shx = (float)(jcode / 9 - 1) * Lx;
+          const float shy = (float)((jcode / 3) % 3 - 1) * Ly;
+          const float shz = (float)(jcode % 3 - 1) * Lz;
+          const float gx = box_gap(blo.x, bhi.x, jl.x, jh.x, shx);
+          const float gy = box_gap(blo.y, bhi.y, jl.y, jh.y, shy);
+          const float gz = box_gap(blo.z, bhi.z, jl.z, jh.z, shz);
+          pass = gx * gx + gy * gy + gz * gz < a.reach2;
+        }
+        const unsigned pm = __ballot_sync(0xffffffffu, pass);
+        if (pass) pass_all[w][__popc(pm & lt)] = make_int4(jc, jcode, cj.x, cj.y);
+        __syncwarp();
+        const int np = __popc(pm);
+        const int kk = lane >> 2, jj = lane & 3;
+        for (int k0 = 0; k0 < np; k0 += 8) {
+          const bool have = k0 + kk < np;
+          const int4 pj = pass_all[w][have ? k0 + kk : k0];
+          const bool j_ok = have && jj < pj.w;
+          const float4 pj4 = j_ok ? a.pos[pj.z + jj] : make_float4(0.f, 0.f, 0.f, 0.f);
+          const int gj = __float_as_int(pj4.w);
+          unsigned mask = 0;  // bits 4 ii + jj of this lane's candidate
+#pragma unroll
+          for (int ii = 0; ii < kClusterSize; ++ii) {
+            bool hit = false, unsure = false;
+            if (j_ok && ii < ci.y && (pj.x != c || jj > ii)) {
+              const float ex_ = min_image_axis(pj4.x - p_i[ii].x, a.cell.a11, a.rcell.a11);
+              const float ey_ = min_image_axis(pj4.y - p_i[ii].y, a.cell.a22, a.rcell.a22);
+              const float ez_ = min_image_axis(pj4.z - p_i[ii].z, a.cell.a33, a.rcell.a33);
+              const float r2f = ex_ * ex_ + ey_ * ey_ + ez_ * ez_;
+              hit = r2f < a.rl2_lo;
+              unsure = !hit && r2f <= a.rl2_hi;
+            }
+            if (__any_sync(0xffffffffu, unsure) && unsure) {
+              // the band: the exact criterion, dr = crd[lower id] - crd[higher id]
+              float dx = __fsub_rn(p_i[ii].x, pj4.x);
+              float dy = __fsub_rn(p_i[ii].y, pj4.y);
+              float dz = __fsub_rn(p_i[ii].z, pj4.z);
+              if (gj < g_i[ii]) {
+                dx = -dx;
+                dy = -dy;
+                dz = -dz;
+              }
+              const float3 d = min_image_exact_rect(dx, dy, dz, a.cell, a.rcell);
+              hit = norm2_exact(d) < a.rl2;
+            }
+            if (hit && nex_i[ii] > 0) {
+              if (gj == ex0_i[ii] || gj == ex1_i[ii]) hit = false;
+              for (int q = 2; q < nex_i[ii] && hit; ++q)
+                if (a.excl_partner[g_i[ii] * kExclCap + q] == gj) hit = false;
+            }
+            if (hit && lists_i[ii])
+              hit = !excluded_pair(min(g_i[ii], gj), max(g_i[ii], gj), a.excl_start,
+                                   a.excl_list, a.excl_numbers);
+            mask |= hit ? 1u << (4 * ii + jj) : 0u;
+          }
+          // the candidate's mask: OR over its four lanes
+          mask |= __shfl_xor_sync(0xffffffffu, mask, 1);
+          mask |= __shfl_xor_sync(0xffffffffu, mask, 2);
+          const bool lead = jj == 0 && mask != 0u;
+          const unsigned lm = __ballot_sync(0xffffffffu, lead);
+          if (lead) {
+            const int slot = count + __popc(lm & lt);
+            if (slot < a.ccap)
+              out[slot] = make_int2(pj.z, (int)(mask | ((unsigned)pj.y << 16)));
+          }
+          count += __popc(lm);
+          pairs += __popc(mask) * (jj == 0);
+        }
+        __syncwarp();
+      }
+    }
+    pairs = __reduce_add_sync(0xffffffffu, pairs);
+    if (lane == 0) {
+      a.crow_count[c] = count < a.ccap ? count : a.ccap;
+      atomicAdd(&a.flags[kFlagTotal], pairs);
+      if (count > a.ccap) {
+        a.flags[kFlagListOverflow] = 1;
+        atomicMax(&a.flags[kFlagMaxRow], count);
+      }
+    }
   }
 }
 
@@ -699,7 +1026,83 @@ static int nl_alloc(NeighborList& nl, int n, long long initial_capacity,
   return scan_reserve(nl.scan, std::max(nl.ncell, n));
 }
 
+static void clusters_free(NeighborList& nl) {
+  cudaFree(nl.d_atom_key);
+  cudaFree(nl.d_clus_count);
+  cudaFree(nl.d_cell_clus);
+  cudaFree(nl.d_clus);
+  cudaFree(nl.d_clus_lo);
+  cudaFree(nl.d_clus_hi);
+  cudaFree(nl.d_nclus);
+  cudaFree(nl.d_img_off);
+  cudaFree(nl.d_crow_count);
+  cudaFree(nl.d_centry);
+  nl.d_atom_key = nl.d_clus_count = nl.d_cell_clus = nl.d_nclus = nl.d_crow_count = nullptr;
+  nl.d_clus = nl.d_centry = nullptr;
+  nl.d_clus_lo = nl.d_clus_hi = nullptr;
+  nl.d_img_off = nullptr;
+  nl.maxclus = 0;
+}
+
+// Storage of the cluster form for the current grid.  Row capacity: 1.5x the
+// mean number of clusters in half a sphere of radius r_l + 3 A (a cluster's
+// reach) plus a margin; regrown on overflow by nl_check_overflow.
+static int clusters_alloc(NeighborList& nl) {
+  clusters_free(nl);
+  const int n = nl.n;
+  nl.maxclus = (n + 3 * nl.ncell) / kClusterSize + 1;
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_atom_key, sizeof(int) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_clus_count, sizeof(int) * nl.ncell));
+  SNB_CUDA_TRY(cudaMemset(nl.d_clus_count, 0, sizeof(int) * nl.ncell));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_cell_clus, sizeof(int) * (nl.ncell + 1)));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_clus, sizeof(int2) * nl.maxclus));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_clus_lo, sizeof(float4) * nl.maxclus));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_clus_hi, sizeof(float4) * nl.maxclus));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_nclus, sizeof(int)));
+  SNB_CUDA_TRY(cudaMemset(nl.d_nclus, 0, sizeof(int)));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_img_off, sizeof(float3) * n));
+  SNB_CUDA_TRY(cudaMemset(nl.d_img_off, 0, sizeof(float3) * n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_crow_count, sizeof(int) * nl.maxclus));
+  SNB_CUDA_TRY(cudaMemset(nl.d_crow_count, 0, sizeof(int) * nl.maxclus));
+  if (nl.ccap <= 0) {
+    const double vol = (double)nl.cell.a11 * nl.cell.a22 * nl.cell.a33;
+    const double rho_c = (double)nl.maxclus / vol;
+    const double R = sqrt((double)nl.rl2) + 3.0;
+    const double mean = 0.5 * rho_c * 4.18879020478639 * R * R * R;
+    nl.ccap = (int)std::min<double>(1.5 * mean + 32.0, (double)nl.maxclus);
+    nl.ccap = std::max(nl.ccap, 32);
+    nl.ccap = (nl.ccap + 3) & ~3;
+  }
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_centry, sizeof(int2) * (size_t)nl.maxclus * nl.ccap));
+  return kOk;
+}
+
+int nl_set_clusters(NeighborList& nl, bool on) {
+  if (!on) {
+    if (nl.clusters) {
+      clusters_free(nl);
+      nl.clusters = false;
+      nl.generation = 0;
+    }
+    return kOk;
+  }
+  if (nl.bv.nsys > 0 || !nl.ortho || !nl.trim)
+    return fail(kNotSupported,
+                "neighbor list: the cluster form needs one rectangular box of at least "
+                "five cells per axis");
+  if (nl.n >= (1 << 27))  // the pair kernel packs a sorted index into 27 bits
+    return fail(kNotSupported, "neighbor list: the cluster form holds up to 2^27 atoms");
+  if (!nl.clusters || nl.maxclus == 0) {
+    int rc = clusters_alloc(nl);
+    if (rc) return rc;
+  }
+  nl.clusters = true;
+  nl.generation = 0;
+  return kOk;
+}
+
 void nl_free(NeighborList& nl) {
+  clusters_free(nl);
   cudaFree(nl.d_unsorted);
   cudaFree(nl.d_sorted_cell);
   cudaFree(nl.d_run_ranges);
@@ -785,12 +1188,25 @@ int nl_regrid(NeighborList& nl, const float* cell6) {
     nl.ncell = ncell;
     nl.trim = N[0] >= 5 && N[1] >= 5 && N[2] >= 5;
   }
+  // cluster storage is sized by the cell count
+  const bool regridded =
+      nl.clusters && nl.maxclus != (nl.n + 3 * nl.ncell) / kClusterSize + 1;
   nl.cell = c;
   nl.rcell = rect_rcell(c);
   nl.wx = c.a11 / nl.Nx;
   nl.wy = c.a22 / nl.Ny;
   nl.iwz = nl.Nz / c.a33;
   nl.generation = 0;  // the next update rebuilds
+  if (nl.clusters) {
+    // the cluster form needs five cells per axis; below that the rows serve
+    if (!nl.trim) {
+      clusters_free(nl);
+      nl.clusters = false;
+    } else if (regridded) {
+      SNB_CUDA_TRY(cudaDeviceSynchronize());
+      return clusters_alloc(nl);
+    }
+  }
   return kOk;
 }
 
@@ -865,14 +1281,15 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   int* excl_count = (excl_numbers && !atom_local) ? nl.d_excl_count : nullptr;
   SNB_CUDA_TRY(cudaMemsetAsync(nl.d_cell_count, 0, sizeof(int) * nl.ncell, st));
   k_rebuild_begin<<<1, 1, 0, st>>>(nl.d_flags);
+  const bool clus = nl.clusters;
   if (nl.bv.nsys > 0)
     k_bin_count<true><<<ceil_div(n, 256), 256, 0, st>>>(
         n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz, nl.d_atom_cell, nl.d_atom_slot,
-        nl.d_cell_count, excl_count, nl.d_flags, nl.bv);
+        nl.d_cell_count, excl_count, nl.d_flags, nl.bv, nullptr);
   else
     k_bin_count<false><<<ceil_div(n, 256), 256, 0, st>>>(
         n, crd, nl.cell, nl.Nx, nl.Ny, nl.Nz, nl.d_atom_cell, nl.d_atom_slot,
-        nl.d_cell_count, excl_count, nl.d_flags, nl.bv);
+        nl.d_cell_count, excl_count, nl.d_flags, nl.bv, clus ? nl.d_atom_key : nullptr);
   int rc = scan_exclusive(nl.d_cell_count, nl.d_cell_start, nl.ncell, nullptr,
                           nl.scan, st);
   if (rc) return rc;
@@ -881,14 +1298,65 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
       excl_list, excl_numbers, excl_count, nl.d_excl_partner, nl.d_flags);
   k_cell_order<<<ceil_div(nl.ncell, 8), 256, 0, st>>>(nl.ncell, nl.d_cell_start,
                                                       nl.d_unsorted, nl.d_perm,
-                                                      nl.d_flags);
+                                                      nl.d_flags,
+                                                      clus ? nl.d_atom_key : nullptr);
   k_fill_sorted<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_perm, crd, atom_local,
                                                   nl.d_inv_perm, nl.d_global,
-                                                  nl.d_pos, nl.d_old_crd, nl.d_flags);
+                                                  nl.d_pos, nl.d_old_crd, nl.d_flags,
+                                                  clus ? nl.d_img_off : nullptr, nl.cell);
   k_sorted_cell<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_perm, nl.d_atom_cell,
                                                   nl.d_sorted_cell, nl.d_flags);
   static int sms = 0;
   if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  if (clus) {
+    k_clus_count<<<ceil_div(nl.ncell, 256), 256, 0, st>>>(nl.ncell, nl.d_cell_start,
+                                                          nl.d_clus_count, nl.d_flags);
+    rc = scan_exclusive(nl.d_clus_count, nl.d_cell_clus, nl.ncell, nl.d_nclus, nl.scan,
+                        st);
+    if (rc) return rc;
+    k_clus_fill<<<ceil_div(nl.ncell, 128), 128, 0, st>>>(
+        nl.ncell, nl.d_cell_start, nl.d_cell_clus, nl.d_pos, nl.cell, nl.d_clus,
+        nl.d_clus_lo, nl.d_clus_hi, nl.d_flags);
+    ClusterSearchArgs ca;
+    ca.pos = nl.d_pos;
+    ca.sorted_cell = nl.d_sorted_cell;
+    ca.cell_clus = nl.d_cell_clus;
+    ca.clus = nl.d_clus;
+    ca.clus_lo = nl.d_clus_lo;
+    ca.clus_hi = nl.d_clus_hi;
+    ca.nclus = nl.d_nclus;
+    ca.runs = nl.d_run_ranges;
+    ca.geom = nl.d_run_geom;
+    ca.run_count = nl.d_run_count;
+    ca.max_runs = nl.max_runs;
+    ca.Nx = nl.Nx;
+    ca.Ny = nl.Ny;
+    ca.Nz = nl.Nz;
+    ca.cell = nl.cell;
+    ca.rcell = nl.rcell;
+    ca.rl2 = nl.rl2;
+    ca.rl2_lo = nl.rl2 * (1.0f - 2e-5f);
+    ca.rl2_hi = nl.rl2 * (1.0f + 2e-5f);
+    ca.reach2 = nl.reach2;
+    ca.wx = nl.cell.a11 / nl.Nx;
+    ca.wy = nl.cell.a22 / nl.Ny;
+    ca.wz = nl.cell.a33 / nl.Nz;
+    ca.excl_start = excl_start;
+    ca.excl_list = excl_list;
+    ca.excl_numbers = excl_numbers;
+    ca.excl_count = excl_count;
+    ca.excl_partner = nl.d_excl_partner;
+    ca.crow_count = nl.d_crow_count;
+    ca.ccap = nl.ccap;
+    ca.centry = nl.d_centry;
+    ca.flags = nl.d_flags;
+    const int cblocks = std::min(ceil_div(nl.maxclus, 8),
+                                 sms * std::max(1, nl.search_blocks_per_sm));
+    k_cluster_search<<<cblocks, 256, 0, st>>>(ca);
+    k_finish_build<<<1, 1, 0, st>>>(nl.d_flags);
+    SNB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+  }
   SearchArgs sa;
   sa.n = n;
   sa.pos = nl.d_pos;
@@ -937,6 +1405,22 @@ int nl_check_overflow(NeighborList& nl, bool* regrown, cudaStream_t st) {
                                cudaMemcpyDeviceToHost, st));
   SNB_CUDA_TRY(cudaStreamSynchronize(st));
   nl.last_total = nl.h_flags[kFlagTotal];
+  if (nl.h_flags[kFlagListOverflow] && nl.clusters) {
+    const long long need = nl.h_flags[kFlagMaxRow];
+    int cap = (int)std::min<long long>(need + need / 5 + 16, nl.maxclus);
+    cap = (std::max(cap, nl.ccap + 16) + 3) & ~3;
+    SNB_CUDA_TRY(cudaStreamSynchronize(st));
+    SNB_CUDA_TRY(cudaFree(nl.d_centry));
+    nl.d_centry = nullptr;
+    nl.ccap = cap;
+    SNB_CUDA_TRY(cudaMalloc(&nl.d_centry, sizeof(int2) * (size_t)nl.maxclus * nl.ccap));
+    int zero = 0;
+    SNB_CUDA_TRY(cudaMemcpyAsync(nl.d_flags + kFlagListOverflow, &zero, sizeof(int),
+                                 cudaMemcpyHostToDevice, st));
+    SNB_CUDA_TRY(cudaStreamSynchronize(st));
+    *regrown = true;
+    return kOk;
+  }
   if (nl.h_flags[kFlagListOverflow]) {
     long long need = nl.h_flags[kFlagMaxRow];
     int cap = (int)std::min<long long>(need + need / 5 + 32, nl.n);
@@ -1038,6 +1522,8 @@ __global__ void k_export_groups_counts(int n, AtomGroupABI* groups, const int* c
 
 int nl_export_atom_groups(NeighborList& nl, void* d_groups, int* d_slab,
                           int max_neighbor_numbers, cudaStream_t st) {
+  if (nl.clusters)
+    return fail(kNotSupported, "neighbor list export: ATOM_GROUP rows of the cluster form");
   const int n = nl.n;
   int* counts = nullptr;
   SNB_CUDA_TRY(cudaMallocAsync(&counts, sizeof(int) * n, st));
@@ -1064,6 +1550,31 @@ int nl_export_atom_groups(NeighborList& nl, void* d_groups, int* d_slab,
   return kOk;
 }
 
+// Pairs of the cluster form in global ids (lo, hi), in no particular order.
+__global__ void k_export_cluster_pairs(const int* __restrict__ nclus,
+                                       const int2* __restrict__ clus,
+                                       const int* __restrict__ crow_count,
+                                       const int2* __restrict__ centry, int ccap,
+                                       const int* __restrict__ global, int* pi, int* pj,
+                                       long long cap, unsigned long long* next) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= *nclus) return;
+  const int si = clus[c].x;
+  for (int e = lane; e < crow_count[c]; e += 32) {
+    const int2 en = centry[(size_t)c * ccap + e];
+    for (int b = 0; b < 16; ++b) {
+      if (!((en.y >> b) & 1)) continue;
+      const int gi = global[si + (b >> 2)], gj = global[en.x + (b & 3)];
+      const unsigned long long o = atomicAdd(next, 1ull);
+      if ((long long)o < cap) {
+        pi[o] = gi < gj ? gi : gj;
+        pj[o] = gi < gj ? gj : gi;
+      }
+    }
+  }
+}
+
 int nl_export_pairs(NeighborList& nl, int* d_pi, int* d_pj, long long cap,
                     long long* count, cudaStream_t st) {
   long long total = 0;
@@ -1071,6 +1582,19 @@ int nl_export_pairs(NeighborList& nl, int* d_pi, int* d_pj, long long cap,
   if (rc) return rc;
   *count = total;
   if (total > cap) return fail(kOverflow, "export_pairs: capacity too small");
+  if (nl.clusters) {
+    unsigned long long* next = nullptr;
+    SNB_CUDA_TRY(cudaMalloc(&next, sizeof(unsigned long long)));
+    SNB_CUDA_TRY(cudaMemsetAsync(next, 0, sizeof(unsigned long long), st));
+    k_export_cluster_pairs<<<ceil_div(nl.maxclus, 8), 256, 0, st>>>(
+        nl.d_nclus, nl.d_clus, nl.d_crow_count, nl.d_centry, nl.ccap, nl.d_global, d_pi,
+        d_pj, cap, next);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(next);
+    if (e != cudaSuccess) return fail(kCudaError, cudaGetErrorString(e));
+    SNB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+  }
   // output offsets of the rows (host prefix sum of the row counts)
   std::vector<int> counts(nl.n);
   SNB_CUDA_TRY(cudaMemcpy(counts.data(), nl.d_row_count, sizeof(int) * nl.n,

@@ -83,8 +83,8 @@ constexpr int kHitCap = 512;   // per-warp hit list (entries)
 
 // COUL_ONLY: atom i's type has A' = B' = 0 with every type, so the LJ terms
 // are exact zeros and are not formed (the results are bitwise the same).
-template <int ACCUM, bool ENERGY, bool VIRIAL, bool COUL_ONLY = false>
-__device__ __forceinline__ void lj_pair(const PairArgs& a, Accumulators& acc,
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool COUL_ONLY = false, typename Args>
+__device__ __forceinline__ void lj_pair(const Args& a, Accumulators& acc,
                                         const float* sA, const float* sB, int ti,
                                         float qi, int gi, float4 e, int j, int tj,
                                         float& fx, float& fy, float& fz, float& e_lj,
@@ -333,6 +333,221 @@ int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
     launch2<kAccumFloat>(a, acc, energy, virial, ortho, st);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// The same pair terms over the cluster form of the list.  One warp per
+// i-cluster (up to four sorted atoms, held in every lane's registers) at a
+// time.  Phase 1 scans the row eight entries per round: lane l takes entry
+// l/4 and its j atom l%4 (one 16-byte load, the entry's periodic image
+// added), tests it against the four i atoms under the entry's mask and the
+// cutoff, and appends each hit to the list of its i atom (ballot + popc):
+// no index load per candidate, and the j atoms of an entry are contiguous.
+// Phase 2 runs the pair terms of each i atom's list 32 at a time as the row
+// kernel does, i force in registers, j forces to the accumulators.
+// Coordinates are in the pair frame (each atom in its cell's image), so the
+// displacement is (x_j + shift) - x_i with no rounding to an image.
+constexpr int kCWarps = 8;
+constexpr int kSubCap = 256;  // per i atom list of hits
+constexpr int kCScanU = 2;    // rounds of eight entries in flight in phase 1
+
+template <int ACCUM, bool ENERGY, bool VIRIAL>
+__global__ void __launch_bounds__(32 * kCWarps, 3)
+k_lj_clusters(ClusterPairArgs a, Accumulators acc) {
+  extern __shared__ float sh_tab[];
+  __shared__ int hits_all[kCWarps][kClusterSize][kSubCap];
+  __shared__ float4 shift_tab[27];
+  float* sA = sh_tab;
+  float* sB = sh_tab + a.n_types * (a.n_types + 1) / 2;
+  const int npair = a.n_types * (a.n_types + 1) / 2;
+  for (int k = threadIdx.x; k < npair; k += blockDim.x) {
+    sA[k] = a.A[k];
+    sB[k] = a.B[k];
+  }
+  if (threadIdx.x < 27) {
+    const int k = threadIdx.x;
+    shift_tab[k] = make_float4((float)(k / 9 - 1) * a.box.x, (float)((k / 3) % 3 - 1) * a.box.y,
+                               (float)(k % 3 - 1) * a.box.z, 0.f);
+  }
+  __syncthreads();
+  if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int nclus = *a.nclus;
+  const int per_block = (nclus + gridDim.x - 1) / gridDim.x;
+  const int c_end = min(nclus, (int)blockIdx.x * per_block + per_block);
+  for (int c = blockIdx.x * per_block + w; c < c_end; c += kCWarps) {
+    const int2 ci = a.clus[c];
+    // the i atoms, broadcast from lanes 0..3
+    const bool own = lane < ci.y;
+    const float4 pl = own ? a.pos[ci.x + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int tl = own ? a.type[ci.x + lane] : 0;
+    const int gl = (ENERGY || VIRIAL) && own ? a.global[ci.x + lane] : 0;
+    float4 p_i[kClusterSize];
+    int t_i[kClusterSize], g_i[kClusterSize];
+    bool coul_only[kClusterSize];
+#pragma unroll
+    for (int ii = 0; ii < kClusterSize; ++ii) {
+      p_i[ii] = make_float4(__shfl_sync(0xffffffffu, pl.x, ii), __shfl_sync(0xffffffffu, pl.y, ii),
+                            __shfl_sync(0xffffffffu, pl.z, ii), __shfl_sync(0xffffffffu, pl.w, ii));
+      t_i[ii] = __shfl_sync(0xffffffffu, tl, ii);
+      g_i[ii] = __shfl_sync(0xffffffffu, gl, ii);
+      // a type without LJ against every type (water H): Coulomb-only terms
+      bool co = true;
+      for (int t = lane; t < a.n_types; t += 32) {
+        const int p = lj_pair_index(t_i[ii], t);
+        co = co && sA[p] == 0.f && sB[p] == 0.f;
+      }
+      coul_only[ii] = __all_sync(0xffffffffu, co);
+    }
+    float f_i[kClusterSize][3];
+    float elj_i[kClusterSize], ec_i[kClusterSize], vir_i[kClusterSize][6];
+#pragma unroll
+    for (int ii = 0; ii < kClusterSize; ++ii) {
+      f_i[ii][0] = f_i[ii][1] = f_i[ii][2] = 0.f;
+      elj_i[ii] = ec_i[ii] = 0.f;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) vir_i[ii][q] = 0.f;
+    }
+    const int n_ent = min(a.crow_count[c], a.ccap);
+    const int2* row = a.centry + (size_t)c * a.ccap;
+    {
+      // the warp's next row: start pulling its entries into L2 now (rows
+      // start on 32-byte boundaries)
+      const int cn = c + kCWarps;
+      if (lane == 0 && cn < c_end) {
+        const int m = min(a.crow_count[cn], a.ccap);
+        if (m > 0)
+          prefetch_l2(a.centry + (size_t)cn * a.ccap, (unsigned)(m * 8 + 15) & ~15u);
+      }
+    }
+    const int jl = lane & 3, eo = lane >> 2;
+    for (int base = 0; base < n_ent;) {
+      // phase 1: candidates -> per-i hit lists, kCScanU rounds of eight
+      // entries in flight per pass
+      int cnt[kClusterSize] = {0, 0, 0, 0};
+      for (; base < n_ent &&
+             max(max(cnt[0], cnt[1]), max(cnt[2], cnt[3])) <= kSubCap - 32 * kCScanU;
+           base += 8 * kCScanU) {
+        int2 en[kCScanU];
+#pragma unroll
+        for (int u = 0; u < kCScanU; ++u) {
+          const int e = base + 8 * u + eo;
+          en[u] = e < n_ent ? row[e] : make_int2(0, 0);
+        }
+        float4 pp[kCScanU];
+#pragma unroll
+        for (int u = 0; u < kCScanU; ++u)
+          if (((unsigned)en[u].y >> jl) & 0x1111u) pp[u] = a.pos[en[u].x + jl];
+#pragma unroll
+        for (int u = 0; u < kCScanU; ++u) {
+          const unsigned col = ((unsigned)en[u].y >> jl) & 0x1111u;
+          const unsigned code = ((unsigned)en[u].y >> 16) & 31u;
+          float3 pj = make_float3(0.f, 0.f, 0.f);
+          if (col) {
+            const float4 sh = shift_tab[code];
+            pj = make_float3(pp[u].x + sh.x, pp[u].y + sh.y, pp[u].z + sh.z);
+          }
+          const int hcode = (en[u].x + jl) | (int)(code << 27);
+#pragma unroll
+          for (int ii = 0; ii < kClusterSize; ++ii) {
+            bool hit = false;
+            if ((col >> (4 * ii)) & 1u) {
+              const float dx = pj.x - p_i[ii].x, dy = pj.y - p_i[ii].y, dz = pj.z - p_i[ii].z;
+              hit = dx * dx + dy * dy + dz * dz < a.cutoff2;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) hits_all[w][ii][cnt[ii] + __popc(m & lt)] = hcode;
+            cnt[ii] += __popc(m);
+          }
+        }
+      }
+      __syncwarp();
+      // phase 2: pair terms of each i atom's hits
+#pragma unroll
+      for (int ii = 0; ii < kClusterSize; ++ii) {
+        const int* hits = hits_all[w][ii];
+        if (coul_only[ii]) {
+          for (int h = lane; h < cnt[ii]; h += 32) {
+            const int hc = hits[h];
+            const int jj = hc & 0x7FFFFFF;
+            const float4 pj = a.pos[jj];
+            const float4 sh = shift_tab[(unsigned)hc >> 27];
+            lj_pair<ACCUM, ENERGY, VIRIAL, true>(
+                a, acc, sA, sB, t_i[ii], p_i[ii].w, g_i[ii],
+                make_float4(pj.x + sh.x - p_i[ii].x, pj.y + sh.y - p_i[ii].y,
+                            pj.z + sh.z - p_i[ii].z, pj.w),
+                jj, 0, f_i[ii][0], f_i[ii][1], f_i[ii][2], elj_i[ii], ec_i[ii], vir_i[ii]);
+          }
+        } else {
+          for (int h = lane; h < cnt[ii]; h += 32) {
+            const int hc = hits[h];
+            const int jj = hc & 0x7FFFFFF;
+            const float4 pj = a.pos[jj];
+            const int tj = a.type[jj];
+            const float4 sh = shift_tab[(unsigned)hc >> 27];
+            lj_pair<ACCUM, ENERGY, VIRIAL>(
+                a, acc, sA, sB, t_i[ii], p_i[ii].w, g_i[ii],
+                make_float4(pj.x + sh.x - p_i[ii].x, pj.y + sh.y - p_i[ii].y,
+                            pj.z + sh.z - p_i[ii].z, pj.w),
+                jj, tj, f_i[ii][0], f_i[ii][1], f_i[ii][2], elj_i[ii], ec_i[ii], vir_i[ii]);
+          }
+        }
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int ii = 0; ii < kClusterSize; ++ii) {
+      if (ii >= ci.y) break;  // warp-uniform
+      const float fx = warp_sum(f_i[ii][0]), fy = warp_sum(f_i[ii][1]),
+                  fz = warp_sum(f_i[ii][2]);
+      float el = 0.f, ec = 0.f;
+      if (ENERGY) {
+        el = warp_sum(elj_i[ii]);
+        ec = warp_sum(ec_i[ii]);
+      }
+      if (VIRIAL) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) vir_i[ii][q] = warp_sum(vir_i[ii][q]);
+      }
+      if (lane == 0) {
+        add_force<ACCUM>(acc, ci.x + ii, fx, fy, fz);
+        if (ENERGY) add_energy<ACCUM>(acc, ci.x + ii, el + ec, el, ec);
+        if (VIRIAL) add_virial<ACCUM>(acc, ci.x + ii, vir_i[ii]);
+      }
+    }
+  }
+}
+
+template <int ACCUM, bool ENERGY, bool VIRIAL>
+static int launch_clusters3(const ClusterPairArgs& a, Accumulators& acc, cudaStream_t st) {
+  const size_t smem = sizeof(float) * a.n_types * (a.n_types + 1);
+  auto kern = k_lj_clusters<ACCUM, ENERGY, VIRIAL>;
+  static int sms = 0;
+  if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kCWarps, smem);
+  per_sm = std::max(per_sm, 1);
+  if (a.blocks_per_sm > 0) per_sm = std::min(per_sm, a.blocks_per_sm);
+  kern<<<sms * per_sm, 32 * kCWarps, smem, st>>>(a, acc);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+template <int ACCUM>
+static int launch_clusters2(const ClusterPairArgs& a, Accumulators& acc, bool energy,
+                            bool virial, cudaStream_t st) {
+  if (energy && virial) return launch_clusters3<ACCUM, true, true>(a, acc, st);
+  if (energy) return launch_clusters3<ACCUM, true, false>(a, acc, st);
+  if (virial) return launch_clusters3<ACCUM, false, true>(a, acc, st);
+  return launch_clusters3<ACCUM, false, false>(a, acc, st);
+}
+
+int launch_pair_clusters(const ClusterPairArgs& a, Accumulators& acc, int accum,
+                         bool energy, bool virial, cudaStream_t st) {
+  return accum == kAccumFixed ? launch_clusters2<kAccumFixed>(a, acc, energy, virial, st)
+                              : launch_clusters2<kAccumFloat>(a, acc, energy, virial, st);
 }
 
 // ---------------------------------------------------------------------------

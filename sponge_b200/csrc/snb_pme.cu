@@ -170,7 +170,7 @@ __global__ void k_pack_pme_bin(int n, const float3* __restrict__ crd,
                                TileGeom g, int* __restrict__ atom_tile,
                                int* __restrict__ atom_slot, int* __restrict__ tile_count,
                                float4* __restrict__ frq, int* __restrict__ upk,
-                               BatchView bv) {
+                               BatchView bv, const float3* __restrict__ img_off) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = s < n;
   int t = 0;
@@ -180,7 +180,12 @@ __global__ void k_pack_pme_bin(int n, const float3* __restrict__ crd,
     int i = perm ? perm[s] : s;
     float3 r = crd[i];
     float q = charge[i];
-    pos[s] = make_float4(r.x, r.y, r.z, q);
+    if (img_off) {
+      const float3 o = img_off[s];
+      pos[s] = make_float4(r.x - o.x, r.y - o.y, r.z - o.z, q);
+    } else {
+      pos[s] = make_float4(r.x, r.y, r.z, q);
+    }
     if (type_sorted) type_sorted[s] = type[i];
     int tile_begin = 0;
     if (BATCH) {
@@ -1074,17 +1079,18 @@ void pme_free(PME& p) {
 // Binning from caller-frame coordinates through a permutation, fused with
 // the pack of the pair kernel's input (pos, type_sorted may be null).
 int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const int* type,
-                 const int* perm, float4* pos, int* type_sorted, cudaStream_t st) {
+                 const int* perm, float4* pos, int* type_sorted, cudaStream_t st,
+                 const float3* img_off) {
   if (n != p.n) return fail(kBadInput, "PME: atom count differs from Initial");
   TileGeom g{p.K[0], p.K[1], p.K[2], p.T, p.nt[0], p.nt[1], p.nt[2], p.rcell};
   if (p.bv.nsys > 0)
     k_pack_pme_bin<true><<<ceil_div(n, 256), 256, 0, st>>>(
         n, crd, charge, type, perm, pos, type_sorted, g, p.d_atom_tile, p.d_atom_slot,
-        p.d_tile_count, p.d_frq, p.d_upk, p.bv);
+        p.d_tile_count, p.d_frq, p.d_upk, p.bv, img_off);
   else
     k_pack_pme_bin<false><<<ceil_div(n, 256), 256, 0, st>>>(
         n, crd, charge, type, perm, pos, type_sorted, g, p.d_atom_tile, p.d_atom_slot,
-        p.d_tile_count, p.d_frq, p.d_upk, p.bv);
+        p.d_tile_count, p.d_frq, p.d_upk, p.bv, img_off);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }

@@ -201,20 +201,26 @@ int launch_zero_acc(Accumulators& a, int accum, bool energy, bool virial,
 __global__ void k_pack(int n, const float3* __restrict__ crd,
                        const float* __restrict__ charge,
                        const int* __restrict__ type, const int* __restrict__ perm,
-                       float4* __restrict__ pos, int* __restrict__ type_sorted) {
+                       float4* __restrict__ pos, int* __restrict__ type_sorted,
+                       const float3* __restrict__ img_off) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   int i = perm ? perm[s] : s;
   float3 r = crd[i];
+  if (img_off) {
+    const float3 o = img_off[s];
+    r = make_float3(r.x - o.x, r.y - o.y, r.z - o.z);
+  }
   pos[s] = make_float4(r.x, r.y, r.z, charge[i]);
   if (type_sorted) type_sorted[s] = type[i];
 }
 
 int launch_pack(int n, const float3* crd, const float* charge, const int* type,
-                const int* perm, float4* pos, int* type_sorted, cudaStream_t st) {
+                const int* perm, float4* pos, int* type_sorted, cudaStream_t st,
+                const float3* img_off) {
   if (n <= 0) return kOk;
   k_pack<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, charge, type, perm, pos,
-                                          type_sorted);
+                                          type_sorted, img_off);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
