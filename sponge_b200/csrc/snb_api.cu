@@ -1026,6 +1026,10 @@ extern "C" int snb_engine_create(const snb_options* opt, int n, snb_boundary bou
   if (n <= 0 || n_types <= 0 || !h_type || !h_A || !h_B || !h_charge)
     return fail(kBadInput, "engine_create: bad argument");
   if (boundary.policy != 1) return fail(kNotSupported, "engine: periodic box required");
+  if (boundary.cell[1] != 0.f || boundary.cell[3] != 0.f || boundary.cell[4] != 0.f)
+    return fail(kNotSupported,
+                "engine: rectangular boxes (skewed cells run through the modules: "
+                "snb_nl, snb_lj, snb_pme)");
   snb_engine* e = new snb_engine();
   e->opt = opts_or_default(opt);
   e->n = n;

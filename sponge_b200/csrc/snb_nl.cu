@@ -56,13 +56,21 @@ __global__ void k_check_refresh(int n, const float3* __restrict__ crd,
 __global__ void k_set_need(int* flags, int v) { flags[kFlagNeed] = v; }
 
 // ---------------------------------------------------------------------------
-// Binning.  Cell of the wrapped coordinate with uniform cells of side L/N.
+// Binning.  Cell of the wrapped coordinate with uniform cells of side a_ii/N.
+// The coordinate is wrapped into the brick [0, a11) x [0, a22) x [0, a33),
+// which tiles space under the lattice of the lower-triangular cell (the
+// reduction of Put_Atom_In_Grids, neighbor_list.cpp:365-373; for a
+// rectangular box it is x - floor(x / L) L per axis).
 __device__ __forceinline__ int wrapped_cell(float3 r, const Cell& cell, int Nx,
                                             int Ny, int Nz) {
-  // Wrap_Coordinate-style reduction into [0, L) for a rectangular box.
-  float x = r.x - floorf(r.x / cell.a11) * cell.a11;
-  float y = r.y - floorf(r.y / cell.a22) * cell.a22;
-  float z = r.z - floorf(r.z / cell.a33) * cell.a33;
+  float z = r.z, y = r.y, x = r.x;
+  const float k3 = floorf(z / cell.a33);
+  z -= k3 * cell.a33;
+  y -= k3 * cell.a32;
+  const float k2 = floorf(y / cell.a22);
+  y -= k2 * cell.a22;
+  x -= k3 * cell.a31 + k2 * cell.a21;
+  x -= floorf(x / cell.a11) * cell.a11;
   int nx = (int)(x / cell.a11 * Nx);
   int ny = (int)(y / cell.a22 * Ny);
   int nz = (int)(z / cell.a33 * Nz);
@@ -228,6 +236,8 @@ struct SearchArgs {
   Cell cell, rcell;
   float rl2;
   float rl2_lo, rl2_hi;     // rl2 (1 -+ 2e-5): outside, the fast |dr|^2 decides
+  bool ortho;               // rectangular; otherwise every candidate is decided
+                            // by the exact criterion on the full cell
   bool trim;                // cell offsets are unique (>= 5 cells per axis)
   float reach2;             // (rl + margin)^2 for trimming runs
   float wx, wy, iwz;        // cell widths x, y and 1/width z
@@ -381,29 +391,43 @@ k_pair_search(SearchArgs a) {
       if (j >= 0) {
         pj4 = a.pos[j];
         gj = __float_as_int(pj4.w);
-        // fast |dr|^2 (contracted, FMA-pipe min image) first: it differs from
-        // the exact one by far less than the band, so outside the band it
-        // decides the criterion alone
-        const float ex_ = min_image_axis(pj4.x - pi4.x, cell.a11, rcell.a11);
-        const float ey_ = min_image_axis(pj4.y - pi4.y, cell.a22, rcell.a22);
-        const float ez_ = min_image_axis(pj4.z - pi4.z, cell.a33, rcell.a33);
-        const float r2f = ex_ * ex_ + ey_ * ey_ + ez_ * ez_;
-        hit = r2f < a.rl2_lo;
-        unsure = !hit && r2f <= a.rl2_hi;
+        if (a.ortho) {
+          // fast |dr|^2 (contracted, FMA-pipe min image) first: it differs
+          // from the exact one by far less than the band, so outside the
+          // band it decides the criterion alone
+          const float ex_ = min_image_axis(pj4.x - pi4.x, cell.a11, rcell.a11);
+          const float ey_ = min_image_axis(pj4.y - pi4.y, cell.a22, rcell.a22);
+          const float ez_ = min_image_axis(pj4.z - pi4.z, cell.a33, rcell.a33);
+          const float r2f = ex_ * ex_ + ey_ * ey_ + ez_ * ez_;
+          hit = r2f < a.rl2_lo;
+          unsure = !hit && r2f <= a.rl2_hi;
+        } else {
+          // a skewed cell: the image choice of a rounded fractional
+          // displacement can differ between two roundings, so no fast path
+          unsure = true;
+        }
       }
       if (__any_sync(0xffffffffu, unsure) && unsure) {
-        // the band: the exact criterion, dr = crd[lower id] - crd[higher id]
-        // as the reference forms it, no contraction
-        float dx = __fsub_rn(pi4.x, pj4.x);
-        float dy = __fsub_rn(pi4.y, pj4.y);
-        float dz = __fsub_rn(pi4.z, pj4.z);
-        if (gj < gi) {
-          dx = -dx;
-          dy = -dy;
-          dz = -dz;
+        // the exact criterion, dr = crd[lower id] - crd[higher id] as the
+        // reference forms it, no contraction
+        if (a.ortho) {
+          float dx = __fsub_rn(pi4.x, pj4.x);
+          float dy = __fsub_rn(pi4.y, pj4.y);
+          float dz = __fsub_rn(pi4.z, pj4.z);
+          if (gj < gi) {
+            dx = -dx;
+            dy = -dy;
+            dz = -dz;
+          }
+          const float3 d = min_image_exact_rect(dx, dy, dz, cell, rcell);
+          hit = norm2_exact(d) < a.rl2;
+        } else {
+          const float3 ri = make_float3(pi4.x, pi4.y, pi4.z);
+          const float3 rj = make_float3(pj4.x, pj4.y, pj4.z);
+          const float3 d = gi < gj ? min_image_exact(ri, rj, cell, rcell)
+                                   : min_image_exact(rj, ri, cell, rcell);
+          hit = norm2_exact(d) < a.rl2;
         }
-        const float3 d = min_image_exact_rect(dx, dy, dz, cell, rcell);
-        hit = norm2_exact(d) < a.rl2;
       }
       if (n_ex > 0 && (gj == ex0 || gj == ex1)) hit = false;
       for (int k = 2; k < n_ex; ++k)  // warp-uniform
@@ -821,6 +845,82 @@ static void box_runs(int Nx, int Ny, int Nz, int offset,
       }
 }
 
+// Neighbour cells of every cell of a box with a general lower-triangular
+// cell (a = (a11,0,0), b = (a21,a22,0), c = (a31,a32,a33)), cells of the
+// brick [0,a11) x [0,a22) x [0,a33) of side a_ii / N.  A pair within r_l
+// has j's wrapped position at i's plus a displacement of length below r_l
+// less a lattice vector; for every lattice vector that can occur the cells
+// that i's cell plus the displacement box reach are taken (with 0.01 A over
+// r_l for the rounding of the wrap), the same cell once.  Ownership as for
+// small rectangular boxes: the cell with the smaller index scans the pair,
+// the own cell holds its later atoms.  Runs are cut along z as in box_runs;
+// the offsets are not used (no trimming for skewed cells).
+static void skewed_runs(int Nx, int Ny, int Nz, const Cell& cl, float rl,
+                        std::vector<std::vector<int2>>& per,
+                        std::vector<std::vector<char4>>& per_geom) {
+  const double a11 = cl.a11, a21 = cl.a21, a22 = cl.a22, a31 = cl.a31, a32 = cl.a32,
+               a33 = cl.a33;
+  const double wx = a11 / Nx, wy = a22 / Ny, wz = a33 / Nz;
+  const double reach = (double)rl + 0.01;
+  // lattice-vector counts that keep both wrapped points inside the brick
+  const int nc_max = (int)std::ceil(1.0 + reach / a33);
+  const int nb_max = (int)std::ceil(1.0 + (reach + std::fabs(a32) * nc_max) / a22);
+  const int na_max = (int)std::ceil(
+      1.0 + (reach + std::fabs(a21) * nb_max + std::fabs(a31) * nc_max) / a11);
+  auto range = [](double lo, double hi, double w, int N, int* k0, int* k1) {
+    *k0 = std::max(0, (int)std::floor(lo / w));
+    *k1 = std::min(N - 1, (int)std::floor(hi / w));
+    return *k0 <= *k1;
+  };
+  for (int cx = 0; cx < Nx; ++cx)
+    for (int cy = 0; cy < Ny; ++cy)
+      for (int cz = 0; cz < Nz; ++cz) {
+        const int c = (cx * Ny + cy) * Nz + cz;
+        std::map<int, char4> nb;
+        for (int nc = -nc_max; nc <= nc_max; ++nc)
+          for (int nbv = -nb_max; nbv <= nb_max; ++nbv)
+            for (int na = -na_max; na <= na_max; ++na) {
+              const double tx = na * a11 + nbv * a21 + nc * a31;
+              const double ty = nbv * a22 + nc * a32;
+              const double tz = nc * a33;
+              int x0, x1, y0, y1, z0, z1;
+              if (!range(cx * wx - reach - tx, (cx + 1) * wx + reach - tx, wx, Nx, &x0, &x1) ||
+                  !range(cy * wy - reach - ty, (cy + 1) * wy + reach - ty, wy, Ny, &y0, &y1) ||
+                  !range(cz * wz - reach - tz, (cz + 1) * wz + reach - tz, wz, Nz, &z0, &z1))
+                continue;
+              for (int x = x0; x <= x1; ++x)
+                for (int y = y0; y <= y1; ++y)
+                  for (int z = z0; z <= z1; ++z) {
+                    const int o = (x * Ny + y) * Nz + z;
+                    if (o > c) nb[o] = make_char4(0, 0, 0, 0);
+                  }
+            }
+        std::vector<int2> rr;
+        for (const auto& kv : nb) {
+          const int o = kv.first;
+          if (!rr.empty() && rr.back().y == o - 1 && (o - 1) / Nz == o / Nz)
+            rr.back().y = o;
+          else
+            rr.push_back(make_int2(o, o));
+        }
+        per[c] = rr;
+        per_geom[c].assign(rr.size(), make_char4(0, 0, 0, 0));
+      }
+}
+
+// Inverse of a lower-triangular cell in Invert_Lower_Triangular_Cell's
+// operation order (utils/boundary.h:61-72): the pair criterion reads it.
+static Cell lower_rcell(const Cell& c) {
+  Cell r{};
+  r.a11 = 1.0f / c.a11;
+  r.a22 = 1.0f / c.a22;
+  r.a33 = 1.0f / c.a33;
+  r.a21 = -c.a21 / (c.a11 * c.a22);
+  r.a31 = (c.a21 * c.a32 - c.a22 * c.a31) / (c.a11 * c.a22 * c.a33);
+  r.a32 = -c.a32 / (c.a22 * c.a33);
+  return r;
+}
+
 // Per-cell run lists as fixed-width tables [ncell][max_runs].
 static void pack_runs(const std::vector<std::vector<int2>>& per,
                       const std::vector<std::vector<char4>>& per_geom,
@@ -893,12 +993,10 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
   if (n <= 0) return fail(kBadInput, "neighbor list: atom_numbers must be > 0");
   nl_common(nl, n, cutoff, skin, refresh_interval, skin_permit, max_neighbor_numbers);
   nl.cell = make_cell(cell6);
-  if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f)
-    return fail(kNotSupported,
-                "neighbor list: only rectangular boxes are supported "
-                "(triclinic cells are not built on this path)");
-  nl.rcell = rect_rcell(nl.cell);
-  nl.ortho = true;
+  nl.ortho = cell6[1] == 0.f && cell6[3] == 0.f && cell6[4] == 0.f;
+  nl.rcell = nl.ortho ? rect_rcell(nl.cell) : lower_rcell(nl.cell);
+  if (!(nl.cell.a11 > 0.f && nl.cell.a22 > 0.f && nl.cell.a33 > 0.f))
+    return fail(kBadInput, "neighbor list: the cell's diagonal must be positive");
   int N[3];
   int rc = box_grid(nl.grid_length, nl.cell, N);
   if (rc) return rc;
@@ -906,13 +1004,16 @@ int nl_init(NeighborList& nl, int n, float cutoff, float skin, const float* cell
   nl.Ny = N[1];
   nl.Nz = N[2];
   nl.ncell = nl.Nx * nl.Ny * nl.Nz;
-  nl.trim = nl.Nx >= 5 && nl.Ny >= 5 && nl.Nz >= 5;
+  nl.trim = nl.ortho && nl.Nx >= 5 && nl.Ny >= 5 && nl.Nz >= 5;
   nl.wx = nl.cell.a11 / nl.Nx;
   nl.wy = nl.cell.a22 / nl.Ny;
   nl.iwz = nl.Nz / nl.cell.a33;
   std::vector<std::vector<int2>> per(nl.ncell);
   std::vector<std::vector<char4>> per_geom(nl.ncell);
-  box_runs(nl.Nx, nl.Ny, nl.Nz, 0, per, per_geom);
+  if (nl.ortho)
+    box_runs(nl.Nx, nl.Ny, nl.Nz, 0, per, per_geom);
+  else
+    skewed_runs(nl.Nx, nl.Ny, nl.Nz, nl.cell, sqrtf(nl.rl2), per, per_geom);
   std::vector<int2> runs;
   std::vector<char4> geom;
   std::vector<int> counts;
@@ -1135,10 +1236,9 @@ void nl_free(NeighborList& nl) {
 // the pair set is the exact one of the new box.
 int nl_regrid(NeighborList& nl, const float* cell6) {
   if (nl.bv.nsys > 0) return fail(kNotSupported, "neighbor list: box change of a batch");
-  if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f)
+  if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f || !nl.ortho)
     return fail(kNotSupported,
-                "neighbor list: only rectangular boxes are supported "
-                "(triclinic cells are not built on this path)");
+                "neighbor list: a box change is supported for rectangular boxes");
   const Cell c = make_cell(cell6);
   int N[3];
   int rc = box_grid(nl.grid_length, c, N);
@@ -1216,7 +1316,7 @@ int nl_update(NeighborList& nl, const float* crd_f, const int* atom_local,
   if (cell6) {
     Cell c = make_cell(cell6);
     if (c.a11 != nl.cell.a11 || c.a22 != nl.cell.a22 || c.a33 != nl.cell.a33 ||
-        c.a21 != 0.f || c.a31 != 0.f || c.a32 != 0.f) {
+        c.a21 != nl.cell.a21 || c.a31 != nl.cell.a31 || c.a32 != nl.cell.a32) {
       int rc = nl_regrid(nl, cell6);
       if (rc) return rc;
     }
@@ -1374,6 +1474,7 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   sa.rl2 = nl.rl2;
   sa.rl2_lo = nl.rl2 * (1.0f - 2e-5f);
   sa.rl2_hi = nl.rl2 * (1.0f + 2e-5f);
+  sa.ortho = nl.ortho;
   sa.trim = nl.trim;
   sa.reach2 = nl.reach2;
   sa.wx = nl.wx;

@@ -834,12 +834,20 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
   p.reciprocal = reciprocal;
   p.excluded = excluded;
   p.cell = make_cell(cell6);
-  if (cell6[1] != 0.f || cell6[3] != 0.f || cell6[4] != 0.f)
-    return fail(kNotSupported, "PME: only rectangular boxes are supported");
+  if (!(p.cell.a11 > 0.f && p.cell.a22 > 0.f && p.cell.a33 > 0.f))
+    return fail(kBadInput, "PME: the cell's diagonal must be positive");
+  // fractional coordinates through the inverse of the lower-triangular cell
+  // (Invert_Lower_Triangular_Cell, utils/boundary.h:61-72); the reciprocal
+  // vectors m = rcell k of the influence function and the force chain rule
+  // use all six entries
   Cell rc{};
   rc.a11 = 1.0f / p.cell.a11;
   rc.a22 = 1.0f / p.cell.a22;
   rc.a33 = 1.0f / p.cell.a33;
+  rc.a21 = -p.cell.a21 / (p.cell.a11 * p.cell.a22);
+  rc.a31 = (p.cell.a21 * p.cell.a32 - p.cell.a22 * p.cell.a31) /
+           (p.cell.a11 * p.cell.a22 * p.cell.a33);
+  rc.a32 = -p.cell.a32 / (p.cell.a22 * p.cell.a33);
   p.rcell = rc;
   p.volume = (double)p.cell.a11 * p.cell.a22 * p.cell.a33;
   if (grid_spacing <= 0.f) grid_spacing = 1.0f;
