@@ -103,6 +103,8 @@ typedef struct snb_pme snb_pme;
 typedef struct snb_engine snb_engine;
 typedef struct snb_nb14 snb_nb14;
 typedef struct snb_settle snb_settle;
+typedef struct snb_bond snb_bond;
+typedef struct snb_angle snb_angle;
 
 /* ---------------------------------------------------------------- misc */
 int snb_version(void);
@@ -468,6 +470,41 @@ int snb_engine_export_pairs(snb_engine* e, int* d_pi, int* d_pj, long long cap,
                             long long* count, void* stream);
 int snb_engine_destroy(snb_engine* e);
 
+/* ------------------------------------------------------ bonds, angles */
+/* BOND (bond/bond.h, bond/bond.cpp).  Bond t of atoms (a, b), dr = r_a - r_b
+ * (minimum image): E = k (|dr| - r0)^2, f_a = -2 k (|dr| - r0) / |dr| dr,
+ * f_b = -f_a; its energy and virial f_a (x) dr go to atom a.
+ * Initial (bond.cpp:65-156): host arrays of bond_numbers entries. */
+int snb_bond_create(int atom_numbers, int bond_numbers, const int* h_atom_a,
+                    const int* h_atom_b, const float* h_k, const float* h_r0,
+                    snb_bond** out);
+/* Bond_Force_With_Atom_Energy_And_Virial (bond.cpp:242-258, kernel
+ * bond.cpp:15-60): adds to frc[N*3], atom_energy[N] and atom_virial[N*6]
+ * (LTMatrix3 order) on `stream`. */
+int snb_bond_force(snb_bond* h, const float* crd, snb_boundary boundary, float* frc,
+                   int need_atom_energy, float* atom_energy, int need_virial,
+                   float* atom_virial, void* stream);
+/* Step_Print's sum of the bond energies (bond.cpp:260-274) of the last call
+ * with energies (host sync). */
+int snb_bond_energy(snb_bond* h, float* h_energy, void* stream);
+int snb_bond_destroy(snb_bond* h);
+/* ANGLE (angle/angle.h, angle/angle.cpp).  Angle t of atoms (a, b, c), b the
+ * vertex: E = k (theta - theta0)^2 with cos(theta) clamped to +-0.999999;
+ * its energy and the virial f_a (x) (r_a - r_b) + f_c (x) (r_c - r_b) go to
+ * atom a.  Initial (angle.cpp:83-150): host arrays of angle_numbers
+ * entries, theta0 in radians. */
+int snb_angle_create(int atom_numbers, int angle_numbers, const int* h_atom_a,
+                     const int* h_atom_b, const int* h_atom_c, const float* h_k,
+                     const float* h_theta0, snb_angle** out);
+/* Angle_Force_With_Atom_Energy_And_Virial (angle.cpp:253-269, kernel
+ * angle.cpp:6-80): adds to frc[N*3], atom_energy[N] and atom_virial[N*6]. */
+int snb_angle_force(snb_angle* h, const float* crd, snb_boundary boundary, float* frc,
+                    int need_atom_energy, float* atom_energy, int need_virial,
+                    float* atom_virial, void* stream);
+/* Step_Print's sum of the angle energies (angle.cpp:271-289) (host sync). */
+int snb_angle_energy(snb_angle* h, float* h_energy, void* stream);
+int snb_angle_destroy(snb_angle* h);
+
 /* ----------------------------------------------------------- 1-4 terms */
 /* NON_BOND_14 (nb14/nb14.h, nb14/nb14.cpp).  Pair t of atoms (a, b) at
  * distance r (minimum image) adds E = A'/12 r^-12 - B'/6 r^-6
@@ -573,6 +610,14 @@ int snb_read_exclude_in_file(const char* path, int* atom_numbers,
  * B' = lj_scale times the pair's h_LJ_A / h_LJ_B entry for the two atoms'
  * types).  Either path may be NULL.  nb14_numbers = M + K.  An atom index
  * outside [0, atom_numbers) returns SNB_ERR_BAD_INPUT. */
+/* Xponge::Native_Load_Bonds (xponge/load/native/bond.hpp:9-42): "M", then
+ * M rows "a b k r0". */
+int snb_read_bond_in_file(const char* path, int* bond_numbers, int* h_atom_a,
+                          int* h_atom_b, float* h_k, float* h_r0);
+/* Xponge::Native_Load_Angles (xponge/load/native/angle.hpp:8-44): "M", then
+ * M rows "a b c k theta0". */
+int snb_read_angle_in_file(const char* path, int* angle_numbers, int* h_atom_a,
+                           int* h_atom_b, int* h_atom_c, float* h_k, float* h_theta0);
 int snb_read_nb14_in_file(const char* path, const char* extra_path, int atom_numbers,
                           const int* h_atom_LJ_type, const float* h_LJ_A,
                           const float* h_LJ_B, int* nb14_numbers, int* h_atom_a,

@@ -36,6 +36,21 @@ def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
 
 
+def _terms(arrays, k):
+    """Contiguous arrays of a term list of k columns: the atom indices (two
+    for a bond, k = 4; three for an angle, k = 5) as int32, the parameters as
+    float32; padded to length 1 when empty."""
+    m = len(arrays[0])
+    out = []
+    for t, a in enumerate(arrays):
+        is_index = t < (2 if k == 4 else 3)
+        dt = np.int32 if is_index else np.float32
+        x = np.zeros(max(m, 1), dt)
+        x[:m] = np.asarray(a, dt)
+        out.append(x)
+    return out
+
+
 def reference_sources() -> str | None:
     """The reference's SPONGE/ source folder, from the environment variable
     SPONGE_REFERENCE (the reference checkout's root), or None when unset."""
@@ -81,6 +96,11 @@ class Oracle:
         L.snbo_nb14_f64.argtypes = [
             ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
             _f64p, _f64p, _f64p, _f64p]
+        L.snbo_bonded_f64.restype = None
+        L.snbo_bonded_f64.argtypes = [
+            ctypes.c_int, _i32p, _i32p, _f32p, _f32p, ctypes.c_int, _i32p, _i32p, _i32p,
+            _f32p, _f32p, _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
+            _f64p]
         L.snbo_shake_f64.restype = ctypes.c_int
         L.snbo_shake_f64.argtypes = [
             ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f64p, _f64p, _f32p, _f32p, _f64p,
@@ -179,6 +199,25 @@ class Oracle:
             _c(s.charge, np.float32), s.cell(), s.rcell(), frc, ae, vir, sums)
         return dict(frc=frc.reshape(n, 3), atom_energy=ae, virial=vir.reshape(n, 6),
                     lj=sums[0], ee=sums[1])
+
+    def bonded_f64(self, crd, cell, rcell, bonds, angles):
+        """Harmonic bonds and angles in FP64 (bond/bond.cpp:15-60,
+        angle/angle.cpp:6-80).  bonds = (a, b, k, r0), angles = (a, b, c, k,
+        theta0); returns per family the forces, per-atom energies, per-atom
+        virials and the energy sum."""
+        crd = _c(crd, np.float32).reshape(-1)
+        n = crd.size // 3
+        ba, bb, bk, br = _terms(bonds, 4)
+        aa, ab, ac, ak, at = _terms(angles, 5)
+        out = [np.zeros(3 * n), np.zeros(n), np.zeros(6 * n),
+               np.zeros(3 * n), np.zeros(n), np.zeros(6 * n), np.zeros(2)]
+        self.lib.snbo_bonded_f64(len(bonds[0]), ba, bb, bk, br, len(angles[0]), aa, ab, ac,
+                                 ak, at, crd, _c(cell, np.float32), _c(rcell, np.float32),
+                                 *out)
+        return (dict(frc=out[0].reshape(n, 3), atom_energy=out[1],
+                     virial=out[2].reshape(n, 6), energy=out[6][0]),
+                dict(frc=out[3].reshape(n, 3), atom_energy=out[4],
+                     virial=out[5].reshape(n, 6), energy=out[6][1]))
 
     def shake_f64(self, cell, rcell, ai, aj, r0, mass, crd_old, crd, vel, dt,
                   v_factor=1.0, x_factor=1.0, tol=1e-13):
@@ -311,6 +350,10 @@ class ReferenceCPU:
         L.ref_nb14.restype = ctypes.c_int
         L.ref_nb14.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p,
                                _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f64p]
+        L.ref_bonded.restype = ctypes.c_int
+        L.ref_bonded.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p,
+                                 ctypes.c_int, _i32p, _i32p, _i32p, _f32p, _f32p, _f32p,
+                                 _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f64p]
         L.ref_settle.restype = ctypes.c_int
         L.ref_settle.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p,
                                  _f32p, _f32p, _f32p, ctypes.c_float, _f32p, _i32p, _i32p]
@@ -444,6 +487,27 @@ class ReferenceCPU:
         out = np.zeros(max(n, 1), dtype)
         self.lib.ref_native_get(name.encode(), out.ctypes.data)
         return out[:n]
+
+    def bonded(self, crd, cell, bonds, angles):
+        """BOND and ANGLE of the reference on the given terms in the box
+        cell (one force call each): per family forces, per-atom energies,
+        per-atom virials and the energy sum Step_Print forms."""
+        crd = _c(crd, np.float32).reshape(-1)
+        n = crd.size // 3
+        ba, bb, bk, br = _terms(bonds, 4)
+        aa, ab, ac, ak, at = _terms(angles, 5)
+        out = [np.zeros(3 * n, np.float32), np.zeros(n, np.float32),
+               np.zeros(6 * n, np.float32), np.zeros(3 * n, np.float32),
+               np.zeros(n, np.float32), np.zeros(6 * n, np.float32)]
+        sums = np.zeros(2)
+        rc = self.lib.ref_bonded(n, len(bonds[0]), ba, bb, bk, br, len(angles[0]), aa, ab,
+                                 ac, ak, at, crd, _c(cell, np.float32), *out, sums)
+        if rc != 0:
+            raise RuntimeError("reference bonded terms failed")
+        return (dict(frc=out[0].reshape(n, 3), atom_energy=out[1],
+                     virial=out[2].reshape(n, 6), energy=sums[0]),
+                dict(frc=out[3].reshape(n, 3), atom_energy=out[4],
+                     virial=out[5].reshape(n, 6), energy=sums[1]))
 
     def nb14(self, s, a, b, A, B, cf):
         """NON_BOND_14 of the reference on pairs (a[t], b[t]) with scaled LJ

@@ -17,12 +17,16 @@
 #include <string>
 
 #include "Lennard_Jones_force/LJ_soft_core.h"
+#include "angle/angle.h"
+#include "bond/bond.h"
 #include "Lennard_Jones_force/Lennard_Jones_force.h"
 #include "PM_force/PM_force.h"
 #include "constrain/settle.h"
 #include "nb14/nb14.h"
 #include "neighbor_list/neighbor_list.h"
 #include "ref_controller.h"
+#include "xponge/load/native/angle.hpp"
+#include "xponge/load/native/bond.hpp"
 #include "xponge/load/native/lj.hpp"
 #include "xponge/load/native/lj_soft.hpp"
 #include "xponge/load/native/md_core.hpp"
@@ -432,6 +436,69 @@ extern "C"
         return 0;
     }
 
+    /* BOND and ANGLE over terms given directly (Xponge::system's bond and
+     * angle tables, which their Initial copies), Get_Local over all n atoms,
+     * then one call each of Bond_Force_With_Atom_Energy_And_Virial and
+     * Angle_Force_With_Atom_Energy_And_Virial in a periodic box cell6, each
+     * into its own frc [n*3], atom_energy [n] and atom_virial [n*6] (added
+     * to).  sums[0..1] = the per-term bond and angle energies that Step_Print
+     * sums, here summed in double. */
+    int ref_bonded(int n, int nb, const int* ba, const int* bb, const float* bk,
+                   const float* br0, int na, const int* aa, const int* ab,
+                   const int* ac, const float* ak, const float* at0, const float* crd,
+                   const float* cell6, float* bond_frc, float* bond_energy,
+                   float* bond_virial, float* angle_frc, float* angle_energy,
+                   float* angle_virial, double* sums)
+    {
+        REF_TRY({
+            auto& B = Xponge::system.classical_force_field.bonds;
+            B.atom_a.assign(ba, ba + nb);
+            B.atom_b.assign(bb, bb + nb);
+            B.k.assign(bk, bk + nb);
+            B.r0.assign(br0, br0 + nb);
+            auto& A = Xponge::system.classical_force_field.angles;
+            A.atom_a.assign(aa, aa + na);
+            A.atom_b.assign(ab, ab + na);
+            A.atom_c.assign(ac, ac + na);
+            A.k.assign(ak, ak + na);
+            A.theta0.assign(at0, at0 + na);
+            std::vector<char> label(n, 1);
+            std::vector<int> id(n);
+            for (int i = 0; i < n; ++i) id[i] = i;
+            Boundary bd;
+            bd.policy = BoundaryPolicy::Periodic;
+            bd.cell = LTMatrix3(cell6[0], cell6[1], cell6[2], cell6[3], cell6[4],
+                                cell6[5]);
+            bd.rcell = Invert_Lower_Triangular_Cell(bd.cell);
+            sums[0] = sums[1] = 0.0;
+            if (nb > 0)
+            {
+                BOND bond;
+                bond.Initial(&controller, NULL, NULL);
+                bond.Get_Local(id.data(), n, 0, label.data(), id.data());
+                bond.Bond_Force_With_Atom_Energy_And_Virial(
+                    reinterpret_cast<const VECTOR*>(crd), bd,
+                    reinterpret_cast<VECTOR*>(bond_frc), 1, bond_energy, 1,
+                    reinterpret_cast<LTMatrix3*>(bond_virial));
+                for (int t = 0; t < nb; ++t) sums[0] += bond.d_bond_ene[t];
+            }
+            if (na > 0)
+            {
+                ANGLE angle;
+                angle.Initial(&controller);
+                angle.Get_Local(id.data(), n, 0, label.data(), id.data());
+                angle.Angle_Force_With_Atom_Energy_And_Virial(
+                    reinterpret_cast<const VECTOR*>(crd), bd,
+                    reinterpret_cast<VECTOR*>(angle_frc), 1, angle_energy, 1,
+                    reinterpret_cast<LTMatrix3*>(angle_virial));
+                for (int t = 0; t < na; ++t) sums[1] += angle.d_angle_ene[t];
+            }
+            B = Xponge::Bonds();
+            A = Xponge::Angles();
+        });
+        return 0;
+    }
+
     /* SETTLE on one step: Initial from the constraint pairs (atom_i,
      * atom_j, constant_r) and masses, Get_Local over all n atoms,
      * Remember_Last_Coordinates on crd_old, then Do_SETTLE with the step
@@ -530,6 +597,12 @@ extern "C"
             Xponge::Native_Load_LJ(&g_native, &controller);
             Xponge::Native_Load_LJ_Soft_Core(&g_native, &controller);
             Xponge::Native_Load_NB14(&g_native, &controller);
+            if (controller.Command_Exist("bond_in_file"))
+                Xponge::Native_Load_Bonds(&g_native.classical_force_field.bonds,
+                                          &controller, "bond");
+            if (controller.Command_Exist("angle_in_file"))
+                Xponge::Native_Load_Angles(&g_native.classical_force_field.angles,
+                                           &controller, "angle");
         });
         return 0;
     }
@@ -567,6 +640,15 @@ extern "C"
         if (n == "nb14_A") return put_f(ff.nb14.A);
         if (n == "nb14_B") return put_f(ff.nb14.B);
         if (n == "nb14_cf") return put_f(ff.nb14.cf_scale_factor);
+        if (n == "bond_a") return put_i(ff.bonds.atom_a);
+        if (n == "bond_b") return put_i(ff.bonds.atom_b);
+        if (n == "bond_k") return put_f(ff.bonds.k);
+        if (n == "bond_r0") return put_f(ff.bonds.r0);
+        if (n == "angle_a") return put_i(ff.angles.atom_a);
+        if (n == "angle_b") return put_i(ff.angles.atom_b);
+        if (n == "angle_c") return put_i(ff.angles.atom_c);
+        if (n == "angle_k") return put_f(ff.angles.k);
+        if (n == "angle_theta0") return put_f(ff.angles.theta0);
         if (n == "excl_numbers" || n == "excl_list")
         {
             std::vector<int> num, list;

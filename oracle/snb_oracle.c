@@ -632,6 +632,81 @@ SNBO_API void snbo_nb14_f64(int m, const int* ia, const int* ib, const float* A,
 }
 
 /* ------------------------------------------------------------------ */
+/* Harmonic bonds (BOND, bond/bond.cpp:15-60) and angles (ANGLE,
+ * angle/angle.cpp:6-80) in FP64.
+ * Bond t of atoms (i, j): dr = r_i - r_j (minimum image), r = |dr|,
+ *   E = k (r - r0)^2, f_i = -2 k (r - r0) / r dr, f_j = -f_i;
+ *   energy and virial f_i (x) dr (off-diagonal pairs summed) on atom i.
+ * Angle t of atoms (i, j, k), j the vertex: a = r_i - r_j, b = r_k - r_j,
+ *   cos = a.b / (|a| |b|) clamped to [-0.999999, 0.999999], theta = acos,
+ *   E = K (theta - theta0)^2, c = -2 K (theta - theta0) / sin(theta),
+ *   f_i = c (cos a / |a|^2 - b / (|a||b|)), f_k = c (cos b / |b|^2 - a /
+ *   (|a||b|)), f_j = -f_i - f_k; energy and virial f_i (x) a + f_k (x) b
+ *   on atom i.
+ * Each family's forces, per-atom energies and virials [n*6] are added to
+ * its own arrays; sums[0..1] += the bond and the angle energy. */
+SNBO_API void snbo_bonded_f64(int nb, const int* ba, const int* bb, const float* bk,
+                              const float* br0, int na, const int* aa,
+                              const int* ab, const int* ac, const float* ak,
+                              const float* at0, const float* crd,
+                              const float* cell, const float* rcell,
+                              double* bond_frc, double* bond_energy,
+                              double* bond_virial, double* angle_frc,
+                              double* angle_energy, double* angle_virial,
+                              double* sums)
+{
+    for (int t = 0; t < nb; ++t)
+    {
+        int i = ba[t], j = bb[t];
+        double dr[3];
+        min_image_f64(crd + 3 * i, crd + 3 * j, cell, rcell, dr);
+        double r = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+        double dev = r - (double)br0[t];
+        double s = -2.0 * (double)bk[t] * dev / r;
+        double f[3] = {s * dr[0], s * dr[1], s * dr[2]};
+        for (int c = 0; c < 3; ++c)
+        {
+            bond_frc[3 * i + c] += f[c];
+            bond_frc[3 * j + c] -= f[c];
+        }
+        double e = (double)bk[t] * dev * dev;
+        bond_energy[i] += e;
+        sums[0] += e;
+        virial_add(bond_virial + 6 * i, f, dr, 1.0);
+    }
+    for (int t = 0; t < na; ++t)
+    {
+        int i = aa[t], j = ab[t], k = ac[t];
+        double a[3], b[3];
+        min_image_f64(crd + 3 * i, crd + 3 * j, cell, rcell, a);
+        min_image_f64(crd + 3 * k, crd + 3 * j, cell, rcell, b);
+        double ia2 = 1.0 / (a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        double ib2 = 1.0 / (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+        double iab = sqrt(ia2 * ib2);
+        double cs = (a[0] * b[0] + a[1] * b[1] + a[2] * b[2]) * iab;
+        if (cs > 0.999999) cs = 0.999999;
+        if (cs < -0.999999) cs = -0.999999;
+        double th = acos(cs);
+        double dth = th - (double)at0[t];
+        double c = -2.0 * (double)ak[t] * dth / sin(th);
+        double fi[3], fk[3];
+        for (int d = 0; d < 3; ++d)
+        {
+            fi[d] = c * cs * ia2 * a[d] - c * iab * b[d];
+            fk[d] = c * cs * ib2 * b[d] - c * iab * a[d];
+            angle_frc[3 * i + d] += fi[d];
+            angle_frc[3 * k + d] += fk[d];
+            angle_frc[3 * j + d] -= fi[d] + fk[d];
+        }
+        double e = (double)ak[t] * dth * dth;
+        angle_energy[i] += e;
+        sums[1] += e;
+        virial_add(angle_virial + 6 * i, fi, a, 1.0);
+        virial_add(angle_virial + 6 * i, fk, b, 1.0);
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* Rigid-geometry constraints in FP64 by iterated SHAKE (Ryckaert,
  * Ciccotti and Berendsen, J. Comput. Phys. 23, 327 (1977)): every listed
  * constraint (ai, aj, r0) moves its atoms along the bond vector at the

@@ -72,6 +72,9 @@ EXPORTED = [
     "snb_engine_spread_wide_tiles", "snb_engine_set_list_form", "snb_engine_list_form",
     "snb_engine_export_pairs",
     "snb_engine_destroy",
+    "snb_bond_create", "snb_bond_force", "snb_bond_energy", "snb_bond_destroy",
+    "snb_angle_create", "snb_angle_force", "snb_angle_energy", "snb_angle_destroy",
+    "snb_read_bond_in_file", "snb_read_angle_in_file",
     "snb_read_lj_in_file", "snb_read_lj_soft_core_in_file", "snb_read_subsys_division_in_file",
     "snb_read_charge_in_file", "snb_read_mass_in_file", "snb_read_exclude_in_file",
     "snb_read_nb14_in_file", "snb_append_frc_traj",
@@ -181,6 +184,17 @@ _SIGS = {
     "snb_engine_stats": (_I, [_P, ctypes.POINTER(_LL), ctypes.POINTER(_LL), _P]),
     "snb_engine_spread_wide_tiles": (_I, [_P, ctypes.POINTER(ctypes.c_int), _P]),
     "snb_engine_set_list_form": (_I, [_P, _I]),
+    "snb_bond_create": (_I, [_I, _I, _P, _P, _P, _P, _P]),
+    "snb_bond_force": (_I, [_P, _P, snb_boundary, _P, _I, _P, _I, _P, _P]),
+    "snb_bond_energy": (_I, [_P, ctypes.POINTER(ctypes.c_float), _P]),
+    "snb_bond_destroy": (_I, [_P]),
+    "snb_angle_create": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
+    "snb_angle_force": (_I, [_P, _P, snb_boundary, _P, _I, _P, _I, _P, _P]),
+    "snb_angle_energy": (_I, [_P, ctypes.POINTER(ctypes.c_float), _P]),
+    "snb_angle_destroy": (_I, [_P]),
+    "snb_read_bond_in_file": (_I, [ctypes.c_char_p, ctypes.POINTER(_I), _P, _P, _P, _P]),
+    "snb_read_angle_in_file": (_I, [ctypes.c_char_p, ctypes.POINTER(_I), _P, _P, _P, _P,
+                                    _P]),
     "snb_engine_list_form": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
     "snb_engine_export_pairs": (_I, [_P, _P, _P, _LL, ctypes.POINTER(_LL), _P]),
     "snb_engine_destroy": (_I, [_P]),

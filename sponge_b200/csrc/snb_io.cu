@@ -240,3 +240,49 @@ extern "C" int snb_append_frc_traj(const char* path, const float* d_frc, int ato
   if (w != (size_t)atom_numbers) return fail(kBadInput, "append_frc_traj: short write");
   return kOk;
 }
+
+// Xponge::Native_Load_Bonds (xponge/load/native/bond.hpp:9-42): "M", then M
+// rows "a b k r0" (fscanf "%d %d %f %f").
+extern "C" int snb_read_bond_in_file(const char* path, int* bond_numbers, int* h_atom_a,
+                                     int* h_atom_b, float* h_k, float* h_r0) {
+  using namespace snb;
+  const char* what = "bond_in_file";
+  if (!bond_numbers) return fail(kBadInput, "read_bond_in_file: null count");
+  File f(path);
+  if (!f.fp) return no_file(what, path);
+  int m = 0;
+  if (fscanf(f.fp, "%d", &m) != 1 || m < 0) return bad_format(what);
+  *bond_numbers = m;
+  const bool any = h_atom_a || h_atom_b || h_k || h_r0;
+  if (!any) return kOk;
+  if (!h_atom_a || !h_atom_b || !h_k || !h_r0)
+    return fail(kBadInput, "read_bond_in_file: give all four arrays or none");
+  for (int i = 0; i < m; ++i)
+    if (fscanf(f.fp, "%d %d %f %f", &h_atom_a[i], &h_atom_b[i], &h_k[i], &h_r0[i]) != 4)
+      return bad_format(what);
+  return kOk;
+}
+
+// Xponge::Native_Load_Angles (xponge/load/native/angle.hpp:8-44): "M", then
+// M rows "a b c k theta0" (fscanf "%d %d %d %f %f", theta0 in radians).
+extern "C" int snb_read_angle_in_file(const char* path, int* angle_numbers, int* h_atom_a,
+                                      int* h_atom_b, int* h_atom_c, float* h_k,
+                                      float* h_theta0) {
+  using namespace snb;
+  const char* what = "angle_in_file";
+  if (!angle_numbers) return fail(kBadInput, "read_angle_in_file: null count");
+  File f(path);
+  if (!f.fp) return no_file(what, path);
+  int m = 0;
+  if (fscanf(f.fp, "%d", &m) != 1 || m < 0) return bad_format(what);
+  *angle_numbers = m;
+  const bool any = h_atom_a || h_atom_b || h_atom_c || h_k || h_theta0;
+  if (!any) return kOk;
+  if (!h_atom_a || !h_atom_b || !h_atom_c || !h_k || !h_theta0)
+    return fail(kBadInput, "read_angle_in_file: give all five arrays or none");
+  for (int i = 0; i < m; ++i)
+    if (fscanf(f.fp, "%d %d %d %f %f", &h_atom_a[i], &h_atom_b[i], &h_atom_c[i], &h_k[i],
+               &h_theta0[i]) != 5)
+      return bad_format(what);
+  return kOk;
+}
