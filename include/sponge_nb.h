@@ -105,6 +105,7 @@ typedef struct snb_nb14 snb_nb14;
 typedef struct snb_settle snb_settle;
 typedef struct snb_bond snb_bond;
 typedef struct snb_angle snb_angle;
+typedef struct snb_vatom snb_vatom;
 
 /* ---------------------------------------------------------------- misc */
 int snb_version(void);
@@ -463,6 +464,11 @@ int snb_engine_spread_wide_tiles(snb_engine* e, int* count, void* stream);
  * where the box or the soft-core kernel does not allow it); the next step
  * rebuilds the list. */
 int snb_engine_set_list_form(snb_engine* e, int clusters);
+/* Virtual atoms in the engine (NULL to remove): every force evaluation moves
+ * the sites' forces onto their atoms before the forces are returned or the
+ * coordinates updated, and every MD step places the sites after the update
+ * (and before the first step).  The sites' inverse masses must be 0. */
+int snb_engine_set_virtual_atoms(snb_engine* e, snb_vatom* vatom);
 int snb_engine_list_form(snb_engine* e, int* clusters);
 /* The engine's current pair set in global ids, lo < hi, in no particular
  * order (as snb_nl_export_pairs; host sync). */
@@ -504,6 +510,32 @@ int snb_angle_force(snb_angle* h, const float* crd, snb_boundary boundary, float
 /* Step_Print's sum of the angle energies (angle.cpp:271-289) (host sync). */
 int snb_angle_energy(snb_angle* h, float* h_energy, void* stream);
 int snb_angle_destroy(snb_angle* h);
+
+/* ------------------------------------------------------- virtual atoms */
+/* VIRTUAL_INFORMATION (virtual_atoms/virtual_atoms.h, virtual_atoms.cpp) for
+ * the types 0-3 of virtual_atoms.h:8-105: massless sites placed from one to
+ * three atoms (0: mirror z -> 2h - z; 1: r_1 + a r_21; 2: r_1 + a r_21 +
+ * b r_31; 3: r_1 + d (r_21 + k r_32) / |r_21 + k r_32|), whose forces are
+ * moved onto those atoms.  A site may be built from sites; they are
+ * processed in dependency levels.  Initial (virtual_atoms.cpp:338-866) from
+ * record_numbers records: h_type, h_virtual_atom, h_from [3 per record,
+ * unused -1] and h_parameter [2 per record: h | a | a, b | d, k].  Refused:
+ * other types, a site defined twice, a site that depends on itself. */
+int snb_vatom_create(int atom_numbers, int record_numbers, const int* h_type,
+                     const int* h_virtual_atom, const int* h_from, const float* h_parameter,
+                     snb_vatom** out);
+int snb_vatom_levels(snb_vatom* v, int* levels);
+/* Coordinate_Refresh (virtual_atoms.cpp:867-932): crd [N*3] updated in place. */
+int snb_vatom_coordinate_refresh(snb_vatom* v, float* crd, snb_boundary boundary,
+                                 void* stream);
+/* Force_Redistribute (virtual_atoms.cpp:934-1001): each site's force in
+ * frc [N*3] added onto its atoms, then set to zero. */
+int snb_vatom_force_redistribute(snb_vatom* v, const float* crd, snb_boundary boundary,
+                                 float* frc, void* stream);
+/* The first record whose type-3 direction had zero length since creation,
+ * or -1 (the reference stops with a runtime error there; host sync). */
+int snb_vatom_status(snb_vatom* v, int* bad_record, void* stream);
+int snb_vatom_destroy(snb_vatom* v);
 
 /* ----------------------------------------------------------- 1-4 terms */
 /* NON_BOND_14 (nb14/nb14.h, nb14/nb14.cpp).  Pair t of atoms (a, b) at
@@ -618,6 +650,11 @@ int snb_read_bond_in_file(const char* path, int* bond_numbers, int* h_atom_a,
  * M rows "a b c k theta0". */
 int snb_read_angle_in_file(const char* path, int* angle_numbers, int* h_atom_a,
                            int* h_atom_b, int* h_atom_c, float* h_k, float* h_theta0);
+/* Xponge::Native_Load_Virtual_Atoms (xponge/load/native/virtual_atoms.hpp:
+ * 10-120): one record per line, "type virtual_atom" then the type's fields;
+ * records in file order, from [3m] (unused -1) and parameter [2m]. */
+int snb_read_virtual_atom_in_file(const char* path, int* record_numbers, int* h_type,
+                                  int* h_virtual_atom, int* h_from, float* h_parameter);
 int snb_read_nb14_in_file(const char* path, const char* extra_path, int atom_numbers,
                           const int* h_atom_LJ_type, const float* h_LJ_A,
                           const float* h_LJ_B, int* nb14_numbers, int* h_atom_a,

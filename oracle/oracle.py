@@ -101,6 +101,9 @@ class Oracle:
             ctypes.c_int, _i32p, _i32p, _f32p, _f32p, ctypes.c_int, _i32p, _i32p, _i32p,
             _f32p, _f32p, _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
             _f64p]
+        L.snbo_vatom_f64.restype = ctypes.c_int
+        L.snbo_vatom_f64.argtypes = [ctypes.c_int, _i32p, _i32p, _i32p, _f32p, _f32p,
+                                     _f32p, _f64p, _f64p]
         L.snbo_shake_f64.restype = ctypes.c_int
         L.snbo_shake_f64.argtypes = [
             ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f64p, _f64p, _f32p, _f32p, _f64p,
@@ -218,6 +221,22 @@ class Oracle:
                      virial=out[2].reshape(n, 6), energy=out[6][0]),
                 dict(frc=out[3].reshape(n, 3), atom_energy=out[4],
                      virial=out[5].reshape(n, 6), energy=out[6][1]))
+
+    def vatom_f64(self, records, cell, rcell, crd, frc):
+        """Virtual atoms (types 0-3) in FP64: positions in record order from
+        crd, then frc's virtual-atom forces moved onto their sources in
+        reverse order.  records = (type [m], virtual [m], from [m, 3],
+        param [m, 2]).  Returns (crd, frc, 1 + first bad record or 0)."""
+        ty, vi, fr, pa = records
+        m = len(ty)
+        x = np.array(crd, np.float64).reshape(-1).copy()
+        f = np.array(frc, np.float64).reshape(-1).copy()
+        bad = self.lib.snbo_vatom_f64(
+            m, _c(ty if m else [0], np.int32), _c(vi if m else [0], np.int32),
+            _c(fr if m else [[0, 0, 0]], np.int32).reshape(-1),
+            _c(pa if m else [[0, 0]], np.float32).reshape(-1), _c(cell, np.float32),
+            _c(rcell, np.float32), x, f)
+        return x.reshape(-1, 3), f.reshape(-1, 3), int(bad)
 
     def shake_f64(self, cell, rcell, ai, aj, r0, mass, crd_old, crd, vel, dt,
                   v_factor=1.0, x_factor=1.0, tol=1e-13):
@@ -350,6 +369,9 @@ class ReferenceCPU:
         L.ref_nb14.restype = ctypes.c_int
         L.ref_nb14.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p, _f32p,
                                _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f64p]
+        L.ref_vatom.restype = ctypes.c_int
+        L.ref_vatom.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _i32p, _f32p,
+                                _f32p, _f32p, _f32p]
         L.ref_bonded.restype = ctypes.c_int
         L.ref_bonded.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p,
                                  ctypes.c_int, _i32p, _i32p, _i32p, _f32p, _f32p, _f32p,
@@ -508,6 +530,19 @@ class ReferenceCPU:
                      virial=out[2].reshape(n, 6), energy=sums[0]),
                 dict(frc=out[3].reshape(n, 3), atom_energy=out[4],
                      virial=out[5].reshape(n, 6), energy=sums[1]))
+
+    def vatom(self, records, cell, crd, frc):
+        """The reference's own virtual-atom formulas record by record
+        (positions in order, forces in reverse order), in FP32."""
+        ty, vi, fr, pa = records
+        m = len(ty)
+        x = np.array(crd, np.float32).reshape(-1).copy()
+        f = np.array(frc, np.float32).reshape(-1).copy()
+        bad = self.lib.ref_vatom(
+            len(x) // 3, m, _c(ty, np.int32), _c(vi, np.int32),
+            _c(fr, np.int32).reshape(-1), _c(pa, np.float32).reshape(-1),
+            _c(cell, np.float32), x, f)
+        return x.reshape(-1, 3), f.reshape(-1, 3), int(bad)
 
     def nb14(self, s, a, b, A, B, cf):
         """NON_BOND_14 of the reference on pairs (a[t], b[t]) with scaled LJ

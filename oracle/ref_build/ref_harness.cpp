@@ -19,6 +19,7 @@
 #include "Lennard_Jones_force/LJ_soft_core.h"
 #include "angle/angle.h"
 #include "bond/bond.h"
+#include "virtual_atoms/virtual_atom_math.h"
 #include "Lennard_Jones_force/Lennard_Jones_force.h"
 #include "PM_force/PM_force.h"
 #include "constrain/settle.h"
@@ -31,6 +32,7 @@
 #include "xponge/load/native/lj_soft.hpp"
 #include "xponge/load/native/md_core.hpp"
 #include "xponge/load/native/nb14.hpp"
+#include "xponge/load/native/virtual_atoms.hpp"
 
 /* --------------------------- the system --------------------------- */
 namespace
@@ -499,6 +501,76 @@ extern "C"
         return 0;
     }
 
+    /* Virtual atoms of types 0-3 through the reference's own position and
+     * force formulas (virtual_atoms/virtual_atom_math.h), record by record:
+     * positions in the given order (each record after the ones it depends
+     * on), then the force of each virtual atom moved onto its sources in
+     * the reverse order and set to zero (Force_Redistribute).  from [3m]
+     * (unused slots ignored), param [2m]; crd [n*3] and frc [n*3] are
+     * updated in place.  Returns 1 + the record of a type 3 geometry the
+     * reference rejects, else 0. */
+    int ref_vatom(int n, int m, const int* type, const int* virt, const int* from,
+                  const float* param, const float* cell6, float* crd, float* frc)
+    {
+        Boundary bd;
+        bd.policy = BoundaryPolicy::Periodic;
+        bd.cell = LTMatrix3(cell6[0], cell6[1], cell6[2], cell6[3], cell6[4], cell6[5]);
+        bd.rcell = Invert_Lower_Triangular_Cell(bd.cell);
+        VECTOR* x = reinterpret_cast<VECTOR*>(crd);
+        VECTOR* f = reinterpret_cast<VECTOR*>(frc);
+        int bad = 0;
+        for (int t = 0; t < m; ++t)
+        {
+            const int v = virt[t], a = from[3 * t], b = from[3 * t + 1],
+                      c = from[3 * t + 2];
+            const float p = param[2 * t], q = param[2 * t + 1];
+            if (type[t] == 0) x[v] = Virtual_Atom_Type_0_Position(x[a], p);
+            else if (type[t] == 1) x[v] = Virtual_Atom_Type_1_Position(x[a], x[b], p, bd);
+            else if (type[t] == 2)
+                x[v] = Virtual_Atom_Type_2_Position(x[a], x[b], x[c], p, q, bd);
+            else if (!Virtual_Atom_Type_3_Position(x[a], x[b], x[c], p, q, bd, &x[v]) &&
+                     !bad)
+                bad = 1 + t;
+        }
+        for (int t = m - 1; t >= 0; --t)
+        {
+            const int v = virt[t], a = from[3 * t], b = from[3 * t + 1],
+                      c = from[3 * t + 2];
+            const float p = param[2 * t], q = param[2 * t + 1];
+            const VECTOR fv = f[v];
+            VECTOR f1, f2, f3;
+            if (type[t] == 0)
+            {
+                f[a] = f[a] + Virtual_Atom_Type_0_Source_Force(fv);
+            }
+            else if (type[t] == 1)
+            {
+                Virtual_Atom_Type_1_Source_Forces(fv, p, &f1, &f2);
+                f[a] = f[a] + f1;
+                f[b] = f[b] + f2;
+            }
+            else if (type[t] == 2)
+            {
+                Virtual_Atom_Type_2_Source_Forces(fv, p, q, &f1, &f2, &f3);
+                f[a] = f[a] + f1;
+                f[b] = f[b] + f2;
+                f[c] = f[c] + f3;
+            }
+            else
+            {
+                if (!Virtual_Atom_Type_3_Source_Forces(x[a], x[b], x[c], fv, p, q, bd, &f1,
+                                                       &f2, &f3) &&
+                    !bad)
+                    bad = 1 + t;
+                f[a] = f[a] + f1;
+                f[b] = f[b] + f2;
+                f[c] = f[c] + f3;
+            }
+            f[v] = VECTOR(0.0f);
+        }
+        return bad;
+    }
+
     /* SETTLE on one step: Initial from the constraint pairs (atom_i,
      * atom_j, constant_r) and masses, Get_Local over all n atoms,
      * Remember_Last_Coordinates on crd_old, then Do_SETTLE with the step
@@ -597,6 +669,8 @@ extern "C"
             Xponge::Native_Load_LJ(&g_native, &controller);
             Xponge::Native_Load_LJ_Soft_Core(&g_native, &controller);
             Xponge::Native_Load_NB14(&g_native, &controller);
+            if (controller.Command_Exist("virtual_atom_in_file"))
+                Xponge::Native_Load_Virtual_Atoms(&g_native.virtual_atoms, &controller);
             if (controller.Command_Exist("bond_in_file"))
                 Xponge::Native_Load_Bonds(&g_native.classical_force_field.bonds,
                                           &controller, "bond");
@@ -640,6 +714,24 @@ extern "C"
         if (n == "nb14_A") return put_f(ff.nb14.A);
         if (n == "nb14_B") return put_f(ff.nb14.B);
         if (n == "nb14_cf") return put_f(ff.nb14.cf_scale_factor);
+        if (n == "vatom_type" || n == "vatom_virtual" || n == "vatom_from" ||
+            n == "vatom_param")
+        {
+            // one entry per record; three sources and two parameters per
+            // record, unused slots -1 / 0
+            std::vector<int> vi;
+            std::vector<float> vf;
+            for (const auto& r : g_native.virtual_atoms.records)
+            {
+                if (n == "vatom_type") vi.push_back(r.type);
+                if (n == "vatom_virtual") vi.push_back(r.virtual_atom);
+                for (int k = 0; k < 3 && n == "vatom_from"; ++k)
+                    vi.push_back(k < (int)r.from.size() ? r.from[k] : -1);
+                for (int k = 0; k < 2 && n == "vatom_param"; ++k)
+                    vf.push_back(k < (int)r.parameter.size() ? r.parameter[k] : 0.0f);
+            }
+            return n == "vatom_param" ? put_f(vf) : put_i(vi);
+        }
         if (n == "bond_a") return put_i(ff.bonds.atom_a);
         if (n == "bond_b") return put_i(ff.bonds.atom_b);
         if (n == "bond_k") return put_f(ff.bonds.k);

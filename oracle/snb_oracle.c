@@ -707,6 +707,127 @@ SNBO_API void snbo_bonded_f64(int nb, const int* ba, const int* bb, const float*
 }
 
 /* ------------------------------------------------------------------ */
+/* Virtual atoms of types 0-3 in FP64 (virtual_atoms/virtual_atom_math.h,
+ * virtual_atoms.h:8-105), record by record: positions in the given order,
+ * then each virtual atom's force moved onto its sources in reverse order
+ * and zeroed.  r_ij is the minimum-image r_i - r_j.
+ *   0: x_v = x_1, y_v = y_1, z_v = 2h - z_1;   F_1 += (Fx, Fy, -Fz).
+ *   1: r_v = r_1 + a r_21;                     F_1 += (1-a) F, F_2 += a F.
+ *   2: r_v = r_1 + a r_21 + b r_31;            F_1 += (1-a-b) F, F_2 += a F,
+ *                                              F_3 += b F.
+ *   3: q = r_21 + k r_32, u = q/|q|, r_v = r_1 + d u; g = d/|q| (F - (F.u) u),
+ *      F_1 += F - g, F_2 += (1-k) g, F_3 += k g; |d| <= 1e-6 puts the site
+ *      on atom 1 with all its force; |q|^2 <= 1e-12 is an invalid geometry
+ *      (site on atom 1, no force, and 1 + the record is returned).
+ * crd [n*3] and frc [n*3] in double, updated in place. */
+static void min_image_d(const double* a, const double* b, const float* cell,
+                        const float* rcell, double* out);
+
+SNBO_API int snbo_vatom_f64(int m, const int* type, const int* virt, const int* from,
+                            const float* param, const float* cell,
+                            const float* rcell, double* crd, double* frc)
+{
+    int bad = 0;
+    for (int t = 0; t < m; ++t)
+    {
+        const int v = virt[t], a = from[3 * t], b = from[3 * t + 1], c = from[3 * t + 2];
+        const double p = param[2 * t], q = param[2 * t + 1];
+        double* xv = crd + 3 * v;
+        const double* x1 = crd + 3 * a;
+        if (type[t] == 0)
+        {
+            xv[0] = x1[0];
+            xv[1] = x1[1];
+            xv[2] = 2.0 * p - x1[2];
+        }
+        else if (type[t] == 1 || type[t] == 2)
+        {
+            double r21[3], r31[3] = {0.0, 0.0, 0.0};
+            min_image_d(crd + 3 * b, x1, cell, rcell, r21);
+            if (type[t] == 2) min_image_d(crd + 3 * c, x1, cell, rcell, r31);
+            double o[3];
+            for (int d = 0; d < 3; ++d) o[d] = x1[d] + p * r21[d] + q * r31[d];
+            for (int d = 0; d < 3; ++d) xv[d] = o[d];
+        }
+        else
+        {
+            double r21[3], r32[3], w[3];
+            min_image_d(crd + 3 * b, x1, cell, rcell, r21);
+            min_image_d(crd + 3 * c, crd + 3 * b, cell, rcell, r32);
+            for (int d = 0; d < 3; ++d) w[d] = r21[d] + q * r32[d];
+            const double n2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+            double o[3] = {x1[0], x1[1], x1[2]};
+            if (fabs(p) > 1e-6)
+            {
+                if (n2 <= 1e-12)
+                {
+                    if (!bad) bad = 1 + t;
+                }
+                else
+                {
+                    const double s = p / sqrt(n2);
+                    for (int d = 0; d < 3; ++d) o[d] += s * w[d];
+                }
+            }
+            for (int d = 0; d < 3; ++d) xv[d] = o[d];
+        }
+    }
+    for (int t = m - 1; t >= 0; --t)
+    {
+        const int v = virt[t], a = from[3 * t], b = from[3 * t + 1], c = from[3 * t + 2];
+        const double p = param[2 * t], q = param[2 * t + 1];
+        double F[3] = {frc[3 * v], frc[3 * v + 1], frc[3 * v + 2]};
+        if (type[t] == 0)
+        {
+            frc[3 * a] += F[0];
+            frc[3 * a + 1] += F[1];
+            frc[3 * a + 2] -= F[2];
+        }
+        else if (type[t] == 1 || type[t] == 2)
+        {
+            const double q2 = type[t] == 2 ? q : 0.0;
+            for (int d = 0; d < 3; ++d)
+            {
+                frc[3 * a + d] += (1.0 - p - q2) * F[d];
+                frc[3 * b + d] += p * F[d];
+                if (type[t] == 2) frc[3 * c + d] += q2 * F[d];
+            }
+        }
+        else if (fabs(p) <= 1e-6)
+        {
+            for (int d = 0; d < 3; ++d) frc[3 * a + d] += F[d];
+        }
+        else
+        {
+            double r21[3], r32[3], w[3];
+            min_image_d(crd + 3 * b, crd + 3 * a, cell, rcell, r21);
+            min_image_d(crd + 3 * c, crd + 3 * b, cell, rcell, r32);
+            for (int d = 0; d < 3; ++d) w[d] = r21[d] + q * r32[d];
+            const double n2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+            if (n2 <= 1e-12)
+            {
+                if (!bad) bad = 1 + t;
+            }
+            else
+            {
+                const double in = 1.0 / sqrt(n2);
+                const double u[3] = {w[0] * in, w[1] * in, w[2] * in};
+                const double fu = F[0] * u[0] + F[1] * u[1] + F[2] * u[2];
+                for (int d = 0; d < 3; ++d)
+                {
+                    const double g = p * in * (F[d] - fu * u[d]);
+                    frc[3 * a + d] += F[d] - g;
+                    frc[3 * b + d] += (1.0 - q) * g;
+                    frc[3 * c + d] += q * g;
+                }
+            }
+        }
+        frc[3 * v] = frc[3 * v + 1] = frc[3 * v + 2] = 0.0;
+    }
+    return bad;
+}
+
+/* ------------------------------------------------------------------ */
 /* Rigid-geometry constraints in FP64 by iterated SHAKE (Ryckaert,
  * Ciccotti and Berendsen, J. Comput. Phys. 23, 327 (1977)): every listed
  * constraint (ai, aj, r0) moves its atoms along the bond vector at the

@@ -74,7 +74,10 @@ EXPORTED = [
     "snb_engine_destroy",
     "snb_bond_create", "snb_bond_force", "snb_bond_energy", "snb_bond_destroy",
     "snb_angle_create", "snb_angle_force", "snb_angle_energy", "snb_angle_destroy",
-    "snb_read_bond_in_file", "snb_read_angle_in_file",
+    "snb_read_bond_in_file", "snb_read_angle_in_file", "snb_read_virtual_atom_in_file",
+    "snb_vatom_create", "snb_vatom_levels", "snb_vatom_coordinate_refresh",
+    "snb_vatom_force_redistribute", "snb_vatom_status", "snb_vatom_destroy",
+    "snb_engine_set_virtual_atoms",
     "snb_read_lj_in_file", "snb_read_lj_soft_core_in_file", "snb_read_subsys_division_in_file",
     "snb_read_charge_in_file", "snb_read_mass_in_file", "snb_read_exclude_in_file",
     "snb_read_nb14_in_file", "snb_append_frc_traj",
@@ -193,6 +196,15 @@ _SIGS = {
     "snb_angle_energy": (_I, [_P, ctypes.POINTER(ctypes.c_float), _P]),
     "snb_angle_destroy": (_I, [_P]),
     "snb_read_bond_in_file": (_I, [ctypes.c_char_p, ctypes.POINTER(_I), _P, _P, _P, _P]),
+    "snb_read_virtual_atom_in_file": (_I, [ctypes.c_char_p, ctypes.POINTER(_I), _P, _P, _P,
+                                           _P]),
+    "snb_vatom_create": (_I, [_I, _I, _P, _P, _P, _P, _P]),
+    "snb_vatom_levels": (_I, [_P, ctypes.POINTER(_I)]),
+    "snb_vatom_coordinate_refresh": (_I, [_P, _P, snb_boundary, _P]),
+    "snb_vatom_force_redistribute": (_I, [_P, _P, snb_boundary, _P, _P]),
+    "snb_vatom_status": (_I, [_P, ctypes.POINTER(_I), _P]),
+    "snb_vatom_destroy": (_I, [_P]),
+    "snb_engine_set_virtual_atoms": (_I, [_P, _P]),
     "snb_read_angle_in_file": (_I, [ctypes.c_char_p, ctypes.POINTER(_I), _P, _P, _P, _P,
                                     _P]),
     "snb_engine_list_form": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),

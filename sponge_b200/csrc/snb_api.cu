@@ -142,6 +142,7 @@ struct snb_engine {
   snb_lj_soft* soft = nullptr;  // soft-core pair terms in place of plain LJ
   snb_nb14* nb14 = nullptr;     // 1-4 terms beside the excluded correction
   snb_settle* settle = nullptr;  // rigid triangles / pairs after the coordinate update
+  snb_vatom* vatom = nullptr;    // massless sites: forces moved, positions refreshed
   long long* d_nb14_sums = nullptr;  // [2]
   double* d_kin = nullptr;           // [6] scratch of the pressure call
   // launch shapes picked by snb_engine_autotune
@@ -1380,6 +1381,9 @@ extern "C" int snb_engine_force(snb_engine* e, const float* crd, float* frc, int
                        e->lrc_virial, d_totals, en, vi, e->pme.reciprocal, st);
     if (rc) return rc;
   }
+  if (e->vatom && (rc = vatom_spread_fixed(e->vatom, crd, e->cell, e->rcell,
+                                           e->nl.d_inv_perm, e->acc, st)))
+    return rc;
   return launch_unpack(e->n, e->nl.d_inv_perm, e->acc, e->accum,
                        reinterpret_cast<float3*>(frc), nullptr, nullptr, nullptr, nullptr,
                        en, vi, st);
@@ -1618,6 +1622,25 @@ extern "C" int snb_engine_update_box(snb_engine* e, snb_boundary boundary) {
   return kOk;
 }
 
+extern "C" int snb_engine_set_virtual_atoms(snb_engine* e, snb_vatom* vatom) {
+  if (!e) return fail(kBadInput, "engine_set_virtual_atoms: null handle");
+  if (vatom) {
+    if (e->nsys > 0) return fail(kNotSupported, "engine_set_virtual_atoms: batch engines");
+    if (e->accum != kAccumFixed)
+      return fail(kNotSupported, "engine_set_virtual_atoms: fixed-point accumulation only");
+    if (vatom_atoms(vatom) != e->n)
+      return fail(kBadInput, "engine_set_virtual_atoms: atom count differs");
+  }
+  e->vatom = vatom;
+  if (e->graph_exec) {  // the captured step holds the previous step shape
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+    e->graph = nullptr;
+  }
+  return kOk;
+}
+
 extern "C" int snb_engine_set_soft_core(snb_engine* e, snb_lj_soft* soft) {
   if (!e) return fail(kBadInput, "engine_set_soft_core: null handle");
   if (soft) {
@@ -1699,6 +1722,10 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
     return fail(kNotSupported, "md steps need the fixed-point accumulation");
   int rc = engine_forces(e, crd, step, false, false, forced_nl, st, in_graph, true);
   if (rc) return rc;
+  // the sites' forces onto their atoms before the update (Force_Redistribute)
+  if (e->vatom && (rc = vatom_spread_fixed(e->vatom, crd, e->cell, e->rcell,
+                                           e->nl.d_inv_perm, e->acc, st)))
+    return rc;
   // the next step's refresh check rides on the coordinate update
   const bool check = e->opt.nl_refresh_interval <= 0;
   const float permit = e->opt.skin * e->opt.nl_skin_permit;
@@ -1706,8 +1733,8 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
                                                 reinterpret_cast<const float3*>(crd), e->cell,
                                                 e->rcell, st)))
     return rc;
-  // with SETTLE the check waits for the constrained positions
-  const bool fused = check && !e->settle;
+  // with SETTLE or virtual sites the check waits for the final positions
+  const bool fused = check && !e->settle && !e->vatom;
   rc = launch_leap_frog(e->n, e->nl.d_inv_perm, e->acc, reinterpret_cast<float3*>(crd),
                         reinterpret_cast<float3*>(vel), invm, dt,
                         fused ? e->nl.d_old_crd : nullptr, e->cell, e->rcell,
@@ -1717,6 +1744,11 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
     rc = launch_settle(e->settle->s, reinterpret_cast<float3*>(crd),
                        reinterpret_cast<float3*>(vel), e->cell, e->rcell, dt, 1.0f, 1.0f,
                        nullptr, st);
+    if (!rc && check && !e->vatom) rc = nl_check_moved(e->nl, crd, st);
+    if (rc) return rc;
+  }
+  if (e->vatom) {  // the sites follow their atoms (Coordinate_Refresh)
+    rc = vatom_refresh(e->vatom, crd, e->cell, e->rcell, st);
     if (!rc && check) rc = nl_check_moved(e->nl, crd, st);
     if (rc) return rc;
   }
@@ -1737,6 +1769,11 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
   const int chk = std::max(1, e->opt.nl_check_overflow_interval);
   int s = 0;
   int retries = 0;
+  // sites placed from the given atoms before the first force
+  if (e->vatom && e->steps_done == 0) {
+    int rc = vatom_refresh(e->vatom, crd, e->cell, e->rcell, st);
+    if (rc) return rc;
+  }
   while (s < steps) {
     int chunk = std::min(chk, steps - s);
     SNB_CUDA_TRY(cudaMemcpyAsync(e->d_snap_crd, crd, sizeof(float) * 3 * e->n,
@@ -1793,6 +1830,13 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
     bool regrown = false;
     int rc = nl_check_overflow(e->nl, &regrown, st);
     if (rc) return rc;
+    if (e->vatom) {
+      int bad = 0;
+      if ((rc = vatom_status(e->vatom, &bad, st))) return rc;
+      if (bad)
+        return fail(kBadInput, "virtual atom record " + std::to_string(bad - 1) +
+                                   ": the direction of a type-3 site has zero length");
+    }
     if (e->settle) {
       int bad = 0;
       SNB_CUDA_TRY(cudaMemcpyAsync(&bad, e->settle->s.d_err, sizeof(int),

@@ -10,6 +10,8 @@
 
 #include "snb_common.cuh"
 
+struct snb_vatom;  // virtual atoms (snb_vatom.cu)
+
 namespace snb {
 
 // ----------------------------------------------------------------------------
@@ -448,6 +450,17 @@ int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const in
                  const float3* img_off = nullptr);
 int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
                   bool need_virial, cudaStream_t st);
+// Virtual atoms for the engine: positions refreshed in crd (caller frame),
+// site forces moved onto their sources inside the fixed-point accumulator
+// (at map[atom]); status = 1 + the first record of an invalid type-3
+// geometry since creation, else 0 (host sync).
+int vatom_refresh(snb_vatom* h, float* crd, const Cell& cell, const Cell& rcell,
+                  cudaStream_t st);
+int vatom_spread_fixed(snb_vatom* h, const float* crd, const Cell& cell, const Cell& rcell,
+                       const int* map, Accumulators& acc, cudaStream_t st);
+int vatom_status(snb_vatom* h, int* bad, cudaStream_t st);
+int vatom_atoms(snb_vatom* h);
+
 // Reads the count of spread tiles redone with int64 sums (host sync).
 int pme_wide_tiles(PME& p, int* count, cudaStream_t st);
 

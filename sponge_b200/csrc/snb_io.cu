@@ -12,6 +12,7 @@
 // Values are read with the same conversions as the reference (fscanf "%f"
 // and "%d"; A' = 12 A and B' = 6 B as the tables are stored).
 #include <cstdio>
+#include <sstream>
 #include <string>
 #include <utility>
 #include <vector>
@@ -284,5 +285,59 @@ extern "C" int snb_read_angle_in_file(const char* path, int* angle_numbers, int*
     if (fscanf(f.fp, "%d %d %d %f %f", &h_atom_a[i], &h_atom_b[i], &h_atom_c[i], &h_k[i],
                &h_theta0[i]) != 5)
       return bad_format(what);
+  return kOk;
+}
+
+// Xponge::Native_Load_Virtual_Atoms (xponge/load/native/virtual_atoms.hpp:
+// 10-120): one record per line, "type virtual_atom" then the type's fields
+// (0: from h; 1: from1 from2 a; 2 and 3: from1 from2 from3 a b); lines
+// without the two leading integers are skipped, an unknown type or missing
+// fields are format errors, and trailing fields must start with '#'.
+// Records come back in file order: from [3m] (unused slots -1) and
+// parameter [2m] (unused 0).
+extern "C" int snb_read_virtual_atom_in_file(const char* path, int* record_numbers,
+                                             int* h_type, int* h_virtual_atom, int* h_from,
+                                             float* h_parameter) {
+  using namespace snb;
+  const char* what = "virtual_atom_in_file";
+  if (!record_numbers) return fail(kBadInput, "read_virtual_atom_in_file: null count");
+  const bool any = h_type || h_virtual_atom || h_from || h_parameter;
+  if (any && (!h_type || !h_virtual_atom || !h_from || !h_parameter))
+    return fail(kBadInput, "read_virtual_atom_in_file: give all four arrays or none");
+  File f(path);
+  if (!f.fp) return no_file(what, path);
+  char line[4096];
+  int m = 0, line_no = 0;
+  while (fgets(line, sizeof(line), f.fp)) {
+    ++line_no;
+    std::istringstream in(line);
+    int type = -1, v = -1;
+    if (!(in >> type >> v)) continue;
+    int src[3] = {-1, -1, -1};
+    float par[2] = {0.f, 0.f};
+    bool ok = false;
+    if (type == 0) {
+      ok = static_cast<bool>(in >> src[0] >> par[0]);
+    } else if (type == 1) {
+      ok = static_cast<bool>(in >> src[0] >> src[1] >> par[0]);
+    } else if (type == 2 || type == 3) {
+      ok = static_cast<bool>(in >> src[0] >> src[1] >> src[2] >> par[0] >> par[1]);
+    } else {
+      return fail(kBadInput, "virtual_atom_in_file contains an unsupported virtual atom type");
+    }
+    if (!ok) return bad_format(what);
+    std::string trailing;
+    if (in >> trailing && (trailing.empty() || trailing[0] != '#'))
+      return fail(kBadInput, "virtual_atom_in_file line " + std::to_string(line_no) +
+                                 " contains unexpected trailing fields");
+    if (any) {
+      h_type[m] = type;
+      h_virtual_atom[m] = v;
+      for (int k = 0; k < 3; ++k) h_from[3 * m + k] = src[k];
+      for (int k = 0; k < 2; ++k) h_parameter[2 * m + k] = par[k];
+    }
+    ++m;
+  }
+  *record_numbers = m;
   return kOk;
 }
