@@ -34,12 +34,15 @@ def g():
 
 
 def _create(g, n, records):
-    ty, vi, fr, pa = (np.ascontiguousarray(a) for a in records)
+    # the arrays stay referenced until the call returns
+    ty, vi, fr, pa = (np.ascontiguousarray(records[0], np.int32),
+                      np.ascontiguousarray(records[1], np.int32),
+                      np.ascontiguousarray(records[2], np.int32),
+                      np.ascontiguousarray(records[3], np.float32))
     h = ctypes.c_void_p()
     g.capi.check(g.capi.load().snb_vatom_create(
-        n, len(ty), ty.astype(np.int32).ctypes.data, vi.astype(np.int32).ctypes.data,
-        np.ascontiguousarray(fr, np.int32).ctypes.data,
-        np.ascontiguousarray(pa, np.float32).ctypes.data, ctypes.byref(h)), "vatom_create")
+        n, len(ty), ty.ctypes.data, vi.ctypes.data, fr.ctypes.data, pa.ctypes.data,
+        ctypes.byref(h)), "vatom_create")
     return h
 
 
