@@ -8,6 +8,10 @@
 * ``ReferenceGPU``: the reference's own GPU modules (FP32, float atomics)
   compiled from its sources as CUDA (``oracle/_ref/libsponge_ref_gpu.so``,
   ``make -C oracle refgpu``); one box per process.
+* The reference-side adapter (``ref_build/sponge_nb_adapter.*``: SPONGE's
+  module structs over this library's C ABI) and its driver, built by
+  ``make -C oracle adapter`` into ``oracle/_ref/libsponge_nb_adapter.so``;
+  tests/test_gpu_adapter.py loads it.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
 this module.  The product never does.
@@ -67,8 +71,25 @@ def build_oracle(ref_root: str | None = None, with_reference: bool = True,
     ref_root = ref_root or reference_sources()
     if with_reference and ref_root and os.path.isdir(ref_root):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"])
+        with open(os.path.join(HERE, "_ref", "REFERENCE_SOURCES"), "w") as f:
+            f.write(os.path.abspath(ref_root) + "\n")
         if with_gpu:
             subprocess.check_call(["make", "-s", "-C", HERE, "refgpu", f"REF={ref_root}"])
+            subprocess.check_call(["make", "-s", "-C", HERE, "adapter", f"REF={ref_root}"])
+
+
+def built_reference_sources() -> str | None:
+    """The reference source folder the last build_oracle() compiled from, when
+    it is still present on this machine (absent where only the prebuilt
+    checkers travelled)."""
+    root = reference_sources()
+    if not root:
+        try:
+            with open(os.path.join(HERE, "_ref", "REFERENCE_SOURCES")) as f:
+                root = f.read().strip()
+        except OSError:
+            return None
+    return root if root and os.path.isdir(root) else None
 
 
 class Oracle:
