@@ -35,6 +35,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "ns/day at 100k-atom LJ+PME water; batched steps/s; force rel-err vs FP64"
 DT_FS = 0.5
+# the launch shapes snb_engine_autotune reports, in its h_choice order
+TUNED_KEYS = ["pair_unroll", "pair_blocks_per_sm", "search_blocks_per_sm", "gather_threads",
+              "pair_warps", "spread_tile_edge", "spread_warps", "pair_hit_stash"]
 CUTOFF = 10.0
 SKIN = 2.0
 
@@ -480,7 +483,7 @@ def run_batch(args, lib, world, rank, dist):
     with torch.cuda.stream(st):
         capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
                                                  0, 100, sp), "batch warm-up")
-    tuned = np.zeros(4, np.int32)
+    tuned = np.zeros(8, np.int32)
     if not args.no_tune:
         with torch.cuda.stream(st):
             capi.check(lib.snb_engine_autotune(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
@@ -569,9 +572,7 @@ def run_batch(args, lib, world, rank, dist):
             "accuracy": batch_acc,
             "kernels_per_step": kn.value - libk.value, "library_kernels_per_step": libk.value,
             "pme_grids": f"{min(K)}^3..{max(K)}^3",
-            "tuned": (None if args.no_tune else dict(zip(
-                ["pair_unroll", "pair_blocks_per_sm", "search_blocks_per_sm",
-                 "gather_threads"], [int(x) for x in tuned]))),
+            "tuned": (None if args.no_tune else dict(zip(TUNED_KEYS, [int(x) for x in tuned]))),
             "workload": "256 water+NaCl boxes (seeds 0-255, 200-2000 waters each, 1 g/cm^3), "
                         "cutoff 8 A, skin 2 A, PME order 4 at 1 A spacing, NVE 0.5 fs, "
                         "fixed-point accumulation"}
@@ -922,7 +923,7 @@ def run_ours(args):
             ke = 0.5 * (mass[:, None] * v * v).sum()
             t_now = 2.0 * ke / (3.0 * n * systems.KB)
             vel.mul_(float(torch.sqrt(300.0 / t_now)))
-    tuned = np.zeros(4, np.int32)
+    tuned = np.zeros(8, np.int32)
     if not args.no_tune:
         with torch.cuda.stream(st):
             capi.check(lib.snb_engine_autotune(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
@@ -1146,9 +1147,7 @@ def run_ours(args):
                               "integrate"], [round(float(x), 5) for x in phases])),
         "nl_rebuilds": int(rebuilds.value), "pairs": listed,
         "nve_drift": drift,
-        "tuned": (None if args.no_tune else dict(zip(
-            ["pair_unroll", "pair_blocks_per_sm", "search_blocks_per_sm", "gather_threads"],
-            [int(x) for x in tuned]))),
+        "tuned": (None if args.no_tune else dict(zip(TUNED_KEYS, [int(x) for x in tuned]))),
         "batch": batch,
         "small_box": small,
         "soft_core_box": soft_box,

@@ -417,9 +417,11 @@ int snb_engine_md_steps_graph(snb_engine* e, float* crd, float* vel,
  * device): h_crd and h_vel [N*3] (pinned for full speed) are copied into the
  * device work buffers crd and vel, the steps run, and the results are
  * copied back into h_crd and h_vel; the list-overflow check and the copy
- * back share one synchronisation, after which the call returns.  When vel
- * follows crd directly on both sides (one [2][N*3] state array each), each
- * direction is one copy. */
+ * back share one synchronisation, after which the call returns.  The
+ * coordinates are copied in first; the velocities follow on a second stream
+ * while the forces are computed, and the first coordinate update waits for
+ * them.  When vel follows crd directly on both sides (one [2][N*3] state
+ * array each), the copy back is one copy. */
 int snb_engine_md_steps_host(snb_engine* e, float* h_crd, float* h_vel, float* crd,
                              float* vel, const float* inverse_mass, float dt,
                              int first_step, int steps, void* stream);
@@ -434,14 +436,28 @@ int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
 /* Autotuner (no counterpart in the reference).  Times `steps` stream-launched
  * steps from the same coordinates for each candidate launch shape and keeps
  * the fastest: the pair kernel's candidates per lane per scan round
- * (2, 4, 8) and persistent blocks per SM (occupancy maximum, 2, 3), the
- * pair search's blocks per SM (4, 8, 16), the PME gather's threads per block
- * (128, 256, 512).  crd / vel are restored; the next step rebuilds the list
- * and recaptures the step graph.  h_choice[0..3] receives the choices in
- * that order (0 blocks per SM = occupancy maximum).  Allocates scratch. */
+ * (2, 4, 8) and persistent blocks per SM (occupancy maximum, 2, 3), its rows
+ * in flight per block (4, 8, 16 warps; plain single box), whether its hit
+ * list keeps each hit's displacement, charge and LJ pair index in shared
+ * memory (so that the pair terms gather nothing; plain single box, at most 4
+ * candidates per lane), the pair search's
+ * blocks per SM (4, 8, 16), the PME gather's threads per block (128, 256,
+ * 512) and the PME spread's shape (tiles of edge 8 with 1, 2, 4 warps per
+ * tile or edge 16 with 4, 8; or edge 0: int64 global atomics, no tiles;
+ * single box).  Each step of a measurement starts from the given frame.
+ * Results are bitwise the same for every shape.  crd / vel are restored; the next step rebuilds the list and
+ * recaptures the step graph.  h_choice[0..7] receives {unroll, blocks per
+ * SM (0 = occupancy maximum), search blocks per SM, gather threads, pair
+ * warps per block, spread tile edge, spread warps per tile, hit stash (0 /
+ * 1)}.  Allocates scratch. */
 int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
                         const float* inverse_mass, float dt, int steps,
                         int* h_choice, void* stream);
+/* No counterpart in the reference: sets the launch shapes directly, in the
+ * h_choice order of snb_engine_autotune (for instance to reuse a tuned
+ * choice); values outside the tuned sets are refused.  Results are bitwise
+ * the same for every shape. */
+int snb_engine_set_launch_shapes(snb_engine* e, const int* h_choice);
 /* Kernel nodes of the captured one-step graph: top level (a step without a
  * neighbor rebuild), cuFFT's share of them, and the kernels inside the
  * conditional rebuild node. */

@@ -68,7 +68,8 @@ EXPORTED = [
     "snb_settle_destroy",
     "snb_engine_md_steps", "snb_engine_md_steps_graph", "snb_engine_md_steps_host",
     "snb_engine_profile_steps",
-    "snb_engine_autotune", "snb_engine_graph_info", "snb_engine_stats",
+    "snb_engine_autotune", "snb_engine_set_launch_shapes", "snb_engine_graph_info",
+    "snb_engine_stats",
     "snb_engine_spread_wide_tiles", "snb_engine_set_list_form", "snb_engine_list_form",
     "snb_engine_export_pairs",
     "snb_engine_destroy",
@@ -182,6 +183,7 @@ _SIGS = {
     "snb_engine_md_steps_host": (_I, [_P, _P, _P, _P, _P, _P, _F, _I, _I, _P]),
     "snb_engine_profile_steps": (_I, [_P, _P, _P, _P, _F, _I, _I, _P, _P]),
     "snb_engine_autotune": (_I, [_P, _P, _P, _P, _F, _I, _P, _P]),
+    "snb_engine_set_launch_shapes": (_I, [_P, _P]),
     "snb_engine_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I),
                                    ctypes.POINTER(_I), _P]),
     "snb_engine_stats": (_I, [_P, ctypes.POINTER(_LL), ctypes.POINTER(_LL), _P]),

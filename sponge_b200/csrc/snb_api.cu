@@ -130,6 +130,14 @@ struct snb_engine {
   const float* g_invm = nullptr;
   float g_dt = 0.f;
   cudaStream_t g_stream = nullptr;
+  bool g_vel_wait = false;  // the graph waits on ev_vel_in before the update
+  // host-buffer steps: the velocities cross the link on `io` while the
+  // forces are computed; the update waits on ev_vel_in (recorded after that
+  // copy and the velocity snapshot)
+  cudaStream_t io = nullptr;
+  cudaEvent_t ev_crd_in = nullptr, ev_vel_in = nullptr;
+  bool vel_wait = false;      // steps of this call wait on ev_vel_in
+  bool vel_snapped = false;   // the first chunk's velocity snapshot is taken
   // a batch of independent boxes (nsys > 0)
   int nsys = 0;
   std::vector<SysGeom> h_sys;
@@ -148,6 +156,8 @@ struct snb_engine {
   // launch shapes picked by snb_engine_autotune
   int pair_unroll = 4;
   int pair_blocks_per_sm = 0;
+  int pair_warps = 16;  // measured on the 100k box: 4 candidates x 16 rows is the fastest
+  bool pair_stash = false;
   cudaStream_t side = nullptr;  // captures the conditional rebuild body
   // second branch of a step: excluded correction, bonded terms and PME run
   // on `branch` while the pair kernel runs on the step's stream; both add
@@ -1014,6 +1024,10 @@ static int engine_finish_create(snb_engine* e, int n, int n_types, const int* h_
   SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
   SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
   SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_join2, cudaEventDisableTiming));
+  SNB_CUDA_TRY(cudaStreamCreateWithFlags(&e->io, cudaStreamNonBlocking));
+  SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_crd_in, cudaEventDisableTiming));
+  SNB_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_vel_in, cudaEventDisableTiming));
+  SNB_CUDA_TRY(cudaEventRecord(e->ev_vel_in, e->io));  // a completed record
   return kOk;
 }
 
@@ -1283,6 +1297,8 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   a.bv = e->bv;
   a.unroll = e->pair_unroll;
   a.blocks_per_sm = e->pair_blocks_per_sm;
+  a.warps = e->pair_warps;
+  a.stash = e->pair_stash;
   if (e->soft) {
     SoftArgs sa;
     sa.n = e->n;
@@ -1735,6 +1751,10 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
     return rc;
   // with SETTLE or virtual sites the check waits for the final positions
   const bool fused = check && !e->settle && !e->vatom;
+  // host-buffer steps: the velocities copied in beside the force phase
+  if (e->vel_wait)
+    SNB_CUDA_TRY(cudaStreamWaitEvent(st, e->ev_vel_in,
+                                     in_graph ? cudaEventWaitExternal : cudaEventWaitDefault));
   rc = launch_leap_frog(e->n, e->nl.d_inv_perm, e->acc, reinterpret_cast<float3*>(crd),
                         reinterpret_cast<float3*>(vel), invm, dt,
                         fused ? e->nl.d_old_crd : nullptr, e->cell, e->rcell,
@@ -1778,8 +1798,10 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
     int chunk = std::min(chk, steps - s);
     SNB_CUDA_TRY(cudaMemcpyAsync(e->d_snap_crd, crd, sizeof(float) * 3 * e->n,
                                  cudaMemcpyDeviceToDevice, st));
-    SNB_CUDA_TRY(cudaMemcpyAsync(e->d_snap_vel, vel, sizeof(float) * 3 * e->n,
-                                 cudaMemcpyDeviceToDevice, st));
+    if (!e->vel_snapped)
+      SNB_CUDA_TRY(cudaMemcpyAsync(e->d_snap_vel, vel, sizeof(float) * 3 * e->n,
+                                   cudaMemcpyDeviceToDevice, st));
+    e->vel_snapped = false;  // later chunks start from velocities on the device
     for (int k = 0; k < chunk; ++k) {
       int step = first + s + k;
       // forced rebuild on the first step and every DOM_DEC_update_interval
@@ -1788,7 +1810,7 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
       bool forced = e->steps_done == 0 || (ui > 0 && step > 0 && step % ui == 0);
       if (use_graph && !forced) {
         if (!e->graph_exec || e->g_crd != crd || e->g_vel != vel || e->g_invm != invm ||
-            e->g_dt != dt || e->g_stream != st) {
+            e->g_dt != dt || e->g_stream != st || e->g_vel_wait != e->vel_wait) {
           if (e->graph_exec) {
             cudaGraphExecDestroy(e->graph_exec);
             cudaGraphDestroy(e->graph);
@@ -1808,6 +1830,7 @@ static int engine_run(snb_engine* e, float* crd, float* vel, const float* invm, 
           e->g_invm = invm;
           e->g_dt = dt;
           e->g_stream = st;
+          e->g_vel_wait = e->vel_wait;
         }
         SNB_CUDA_TRY(cudaGraphLaunch(e->graph_exec, st));
       } else {
@@ -1893,17 +1916,31 @@ extern "C" int snb_engine_md_steps_host(snb_engine* e, float* h_crd, float* h_ve
   cudaStream_t st = S(stream);
   if (st == nullptr) return fail(kBadInput, "engine_md_steps_host: needs a non-default stream");
   const size_t bytes = sizeof(float) * 3 * (size_t)e->n;
-  if (h_vel == h_crd + 3 * (size_t)e->n && vel == crd + 3 * (size_t)e->n) {
-    // crd and vel side by side on both ends: one copy each way
-    SNB_CUDA_TRY(cudaMemcpyAsync(crd, h_crd, 2 * bytes, cudaMemcpyHostToDevice, st));
-  } else {
+  if (steps == 0) {
     SNB_CUDA_TRY(cudaMemcpyAsync(crd, h_crd, bytes, cudaMemcpyHostToDevice, st));
     SNB_CUDA_TRY(cudaMemcpyAsync(vel, h_vel, bytes, cudaMemcpyHostToDevice, st));
+    return kOk;
   }
-  if (steps == 0) return kOk;
+  // the coordinates first: the forces need them.  The velocities follow on
+  // the link while the forces are computed (the copies are issued one after
+  // the other, so the coordinates get the link's full bandwidth), and the
+  // first update waits for them.
+  SNB_CUDA_TRY(cudaMemcpyAsync(crd, h_crd, bytes, cudaMemcpyHostToDevice, st));
+  SNB_CUDA_TRY(cudaEventRecord(e->ev_crd_in, st));
+  SNB_CUDA_TRY(cudaStreamWaitEvent(e->io, e->ev_crd_in, 0));
+  SNB_CUDA_TRY(cudaMemcpyAsync(vel, h_vel, bytes, cudaMemcpyHostToDevice, e->io));
+  SNB_CUDA_TRY(cudaMemcpyAsync(e->d_snap_vel, vel, bytes, cudaMemcpyDeviceToDevice, e->io));
+  SNB_CUDA_TRY(cudaEventRecord(e->ev_vel_in, e->io));
   bool graphable = e->opt.nl_refresh_interval <= 0 && e->pme.update_interval == 1;
+  e->vel_wait = true;
+  e->vel_snapped = true;
   int rc = engine_run(e, crd, vel, invm, dt, first, steps, st, graphable, h_crd, h_vel);
-  if (rc) return rc;
+  e->vel_wait = false;
+  e->vel_snapped = false;
+  if (rc) {
+    cudaStreamSynchronize(e->io);
+    return rc;
+  }
   SNB_CUDA_TRY(cudaStreamSynchronize(st));
   return kOk;
 }
@@ -1969,12 +2006,15 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   SNB_CUDA_TRY(cudaEventCreate(&t0));
   SNB_CUDA_TRY(cudaEventCreate(&t1));
+  // Every step starts from the saved frame, so that each measures the same
+  // work and no list rebuild falls into a window by chance (one costs about
+  // two steps).
   auto measure = [&](int ph, bool force_nl, double* ms) -> int {
-    SNB_CUDA_TRY(cudaMemcpyAsync(crd, c0, bytes, cudaMemcpyDeviceToDevice, st));
-    SNB_CUDA_TRY(cudaMemcpyAsync(vel, v0, bytes, cudaMemcpyDeviceToDevice, st));
     double acc = 0.0;
     e->prof_on = ph >= 0;
     for (int s = -1; s < steps; ++s) {  // s = -1: untimed warm-up step
+      SNB_CUDA_TRY(cudaMemcpyAsync(crd, c0, bytes, cudaMemcpyDeviceToDevice, st));
+      SNB_CUDA_TRY(cudaMemcpyAsync(vel, v0, bytes, cudaMemcpyDeviceToDevice, st));
       SNB_CUDA_TRY(cudaEventRecord(t0, st));
       int rc = engine_md_step(e, crd, vel, invm, dt, 1 + s, force_nl || s < 0, st);
       if (rc) {
@@ -1998,20 +2038,52 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
   double best = 1e30, ms = 0.0;
   int bu = e->pair_unroll, bb = e->pair_blocks_per_sm;
   const bool rows = !(e->nl.clusters && !e->soft);
+  // candidates per lane per round and rows in flight per block (the row
+  // kernel of the plain single box) together, then blocks per SM
+  int bw = e->pair_warps;
+  const bool warps_knob = rows && !e->soft && e->nsys == 0;
   for (int u : {2, 4, 8})
-    for (int b : {0, 2, 3}) {
+    for (int w : {4, 8, 16}) {
+      if (rc) break;
       if (!rows && u != bu) continue;  // the cluster kernel has no unroll choice
+      if (!warps_knob && w != bw) continue;
       e->pair_unroll = u;
-      e->pair_blocks_per_sm = b;
+      e->pair_warps = w;
+      e->pair_blocks_per_sm = 0;
       if ((rc = measure(-1, false, &ms))) break;  // the step, PME branch alongside
       if (ms < best) {
         best = ms;
         bu = u;
-        bb = b;
+        bw = w;
       }
     }
   e->pair_unroll = bu;
+  e->pair_warps = bw;
+  bb = 0;  // the joint search above ran at the occupancy maximum
+  for (int b : {2, 3}) {
+    if (rc) break;
+    e->pair_blocks_per_sm = b;
+    if ((rc = measure(-1, false, &ms))) break;
+    if (ms < best) {
+      best = ms;
+      bb = b;
+    }
+  }
   e->pair_blocks_per_sm = bb;
+  // the hit stash (phase 2 without gathers), same kernel otherwise
+  bool bst = e->pair_stash;
+  if (!rc && rows && !e->soft && e->nsys == 0) {
+    best = 1e30;
+    for (bool sx : {false, true}) {
+      e->pair_stash = sx;
+      if ((rc = measure(-1, false, &ms))) break;
+      if (ms < best) {
+        best = ms;
+        bst = sx;
+      }
+    }
+  }
+  e->pair_stash = bst;
   int bs = e->nl.search_blocks_per_sm;
   best = 1e30;
   for (int b : {4, 8, 16}) {
@@ -2036,6 +2108,24 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
     }
   }
   e->pme.gather_threads = bg;
+  // spread tile shape: edge and warps per tile (one box), timed as the whole
+  // step with the PME chain beside the pair kernel
+  int bt = e->pme.spread_atomic ? 0 : e->pme.T;
+  int bsw = e->pme.spread_atomic ? 0 : e->pme.spread_warps;
+  if (!rc && e->nsys == 0 && e->pme.reciprocal) {
+    best = 1e30;
+    const int shapes[6][2] = {{8, 1}, {8, 2}, {8, 4}, {16, 4}, {16, 8}, {0, 0}};
+    for (const auto& sh : shapes) {
+      if ((rc = pme_set_spread_shape(e->pme, sh[0], sh[1]))) break;
+      if ((rc = measure(-1, false, &ms))) break;
+      if (ms < best) {
+        best = ms;
+        bt = sh[0];
+        bsw = sh[1];
+      }
+    }
+    if (!rc) rc = pme_set_spread_shape(e->pme, bt, bsw);
+  }
   cudaMemcpyAsync(crd, c0, bytes, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(vel, v0, bytes, cudaMemcpyDeviceToDevice, st);
   cudaStreamSynchronize(st);
@@ -2056,6 +2146,39 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
     h_choice[1] = e->pair_blocks_per_sm;
     h_choice[2] = e->nl.search_blocks_per_sm;
     h_choice[3] = e->pme.gather_threads;
+    h_choice[4] = e->pair_warps;
+    h_choice[5] = e->pme.spread_atomic ? 0 : e->pme.T;
+    h_choice[6] = e->pme.spread_atomic ? 0 : e->pme.spread_warps;
+    h_choice[7] = e->pair_stash ? 1 : 0;
+  }
+  return kOk;
+}
+
+extern "C" int snb_engine_set_launch_shapes(snb_engine* e, const int* h_choice) {
+  if (!e || !h_choice) return fail(kBadInput, "engine_set_launch_shapes: bad argument");
+  const int u = h_choice[0], b = h_choice[1], sb = h_choice[2], gt = h_choice[3];
+  const int w = h_choice[4], T = h_choice[5], sw = h_choice[6], sx = h_choice[7];
+  if ((u != 2 && u != 4 && u != 8) || b < 0 || b > 32 || (sb != 4 && sb != 8 && sb != 16) ||
+      (gt != 128 && gt != 256 && gt != 512) || (w != 4 && w != 8 && w != 16) ||
+      (sx != 0 && sx != 1))
+    return fail(kBadInput, "engine_set_launch_shapes: a shape outside the tuned set");
+  if (e->nsys == 0) {
+    int rc = pme_set_spread_shape(e->pme, T, sw);
+    if (rc) return rc;
+  } else if (T != e->pme.T || sw != e->pme.spread_warps || e->pme.spread_atomic) {
+    return fail(kNotSupported, "engine_set_launch_shapes: the spread shape of a batch is fixed");
+  }
+  e->pair_unroll = u;
+  e->pair_blocks_per_sm = b;
+  e->nl.search_blocks_per_sm = sb;
+  e->pme.gather_threads = gt;
+  e->pair_warps = w;
+  e->pair_stash = sx != 0;
+  if (e->graph_exec) {  // recapture with these shapes
+    cudaGraphExecDestroy(e->graph_exec);
+    cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+    e->graph = nullptr;
   }
   return kOk;
 }
@@ -2170,6 +2293,9 @@ extern "C" int snb_engine_destroy(snb_engine* e) {
   if (e->ev_join) cudaEventDestroy(e->ev_join);
   if (e->branch2) cudaStreamDestroy(e->branch2);
   if (e->ev_join2) cudaEventDestroy(e->ev_join2);
+  if (e->io) cudaStreamDestroy(e->io);
+  if (e->ev_crd_in) cudaEventDestroy(e->ev_crd_in);
+  if (e->ev_vel_in) cudaEventDestroy(e->ev_vel_in);
   nl_free(e->nl);
   pme_free(e->pme);
   acc_free(e->acc);

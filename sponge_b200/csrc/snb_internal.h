@@ -254,6 +254,8 @@ struct PairArgs {
   BatchView bv;                 // nsys > 0: per-system boxes (rectangular)
   int unroll = 4;               // scan candidates per lane per round (2, 4, 8)
   int blocks_per_sm = 0;        // persistent blocks per SM, 0: occupancy maximum
+  int warps = 8;                // rows in flight per block (4, 8, 16)
+  bool stash = false;           // hits keep displacement / pair index (row kernel)
   // solvent split (single box): the atoms with global id >= solvent_begin
   // are the trailing water block.  solvent_mode 1: every pair but the
   // solvent-solvent ones (LENNARD_JONES_INFORMATION with solvent_numbers);
@@ -381,8 +383,13 @@ struct PME {
   bool reciprocal = true, excluded = true;
   Cell cell{}, rcell{};
   double volume = 0.0;
-  // tiles of the charge grid owned by spread CTAs
+  // tiles of the charge grid owned by spread CTAs: edge T, warps per tile
   int T = 8;
+  int spread_warps = 2;
+  // spread by int64 fixed-point atomics into d_Q64 instead of the tiles
+  // (one box; the same grid bit for bit)
+  bool spread_atomic = false;
+  long long* d_Q64 = nullptr;   // [nall], zero between steps
   int nt[3] = {0, 0, 0};
   int ntiles = 0;
   float* d_B[3] = {nullptr, nullptr, nullptr};  // |b(k)|^2 per axis
@@ -432,6 +439,7 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
 // grid per box by the reference's size rule; fills the PME fields of sys.
 // Particle_Mesh::Update_Box: a new rectangular box at the same grid size.
 int pme_update_box(PME& p, const float* cell6);
+int pme_set_spread_shape(PME& p, int T, int W);
 int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
                    float tolerance, float grid_spacing, bool reciprocal, bool excluded);
 void pme_free(PME& p);

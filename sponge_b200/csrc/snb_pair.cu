@@ -21,6 +21,10 @@
 #include <algorithm>
 #include <cfloat>
 
+#include <mutex>
+#include <utility>
+#include <vector>
+
 #include "snb_internal.h"
 
 namespace snb {
@@ -76,26 +80,27 @@ __device__ __forceinline__ void add_virial(Accumulators& acc, int s, const float
 // 32 pairs at a time, so every lane of the expensive part does useful work
 // and the scan carries no force state.  A row with more hits than the list
 // holds is taken in several rounds.
-constexpr int kWarps = 8;
+constexpr int kWarps = 8;      // rows in flight per block (warps per block)
 constexpr int kHitCap = 512;   // per-warp hit list (entries)
-// candidates per lane per scan round: a template parameter (2, 4 or 8) that
-// the engine's autotuner picks; 4 elsewhere
+// STASH: phase 1 keeps, per hit, the displacement and charge (float4) and
+// the atom and LJ type-pair index (int2) in dynamic shared memory, so that
+// phase 2 gathers nothing from global memory; the displacement is the one
+// the cutoff test used, so the results are bitwise those of the plain list.
+constexpr int kStashCap = 256;
+// candidates per lane per scan round: a template parameter (2, 4 or 8), and
+// rows in flight per block (4, 8 or 16 warps), that the engine's autotuner
+// picks; 4 and 8 elsewhere
 
-// COUL_ONLY: atom i's type has A' = B' = 0 with every type, so the LJ terms
-// are exact zeros and are not formed (the results are bitwise the same).
+// The pair terms of i and j with the LJ coefficients A' = 12 A, B' = 6 B of
+// their type pair.  COUL_ONLY: atom i's type has A' = B' = 0 with every
+// type, so the LJ terms are exact zeros and are not formed (the results are
+// bitwise the same).
 template <int ACCUM, bool ENERGY, bool VIRIAL, bool COUL_ONLY = false, typename Args>
-__device__ __forceinline__ void lj_pair(const Args& a, Accumulators& acc,
-                                        const float* sA, const float* sB, int ti,
-                                        float qi, int gi, float4 e, int j, int tj,
-                                        float& fx, float& fy, float& fz, float& e_lj,
-                                        float& e_c, float* vir) {
+__device__ __forceinline__ void lj_pair_ab(const Args& a, Accumulators& acc, float A,
+                                           float B, float qi, int gi, float4 e, int j,
+                                           float& fx, float& fy, float& fz, float& e_lj,
+                                           float& e_c, float* vir) {
   const float r2 = e.x * e.x + e.y * e.y + e.z * e.z;
-  float A = 0.f, B = 0.f;
-  if (!COUL_ONLY) {
-    const int p = lj_pair_index(ti, tj);
-    A = sA[p];
-    B = sB[p];
-  }
   const float rinv = rsqrtf(r2);
   const float r = r2 * rinv;
   const float ir2 = rinv * rinv;
@@ -142,18 +147,40 @@ __device__ __forceinline__ void lj_pair(const Args& a, Accumulators& acc,
   }
 }
 
+// The same with the coefficients looked up from the types' pair index.
+template <int ACCUM, bool ENERGY, bool VIRIAL, bool COUL_ONLY = false, typename Args>
+__device__ __forceinline__ void lj_pair(const Args& a, Accumulators& acc,
+                                        const float* sA, const float* sB, int ti,
+                                        float qi, int gi, float4 e, int j, int tj,
+                                        float& fx, float& fy, float& fz, float& e_lj,
+                                        float& e_c, float* vir) {
+  float A = 0.f, B = 0.f;
+  if (!COUL_ONLY) {
+    const int p = lj_pair_index(ti, tj);
+    A = sA[p];
+    B = sB[p];
+  }
+  lj_pair_ab<ACCUM, ENERGY, VIRIAL, COUL_ONLY>(a, acc, A, B, qi, gi, e, j, fx, fy, fz, e_lj,
+                                               e_c, vir);
+}
+
 // SOLV 1 / 2: the solvent split of PairArgs::solvent_mode (pairs with both
 // global ids >= solvent_begin left out / taken alone); 0: every pair.
 template <int ACCUM, bool ENERGY, bool VIRIAL, bool ORTHO, bool BATCH, int kScanU,
-          int SOLV = 0>
-__global__ void __launch_bounds__(256, 4)
+          int SOLV = 0, int WARPS = kWarps, bool STASH = false>
+__global__ void __launch_bounds__(32 * WARPS, 32 / WARPS)
 k_lj_direct(PairArgs a, Accumulators acc) {
-  static_assert(kScanU >= 1 && 32 * kScanU < kHitCap, "scan round exceeds the hit list");
-  extern __shared__ float sh_tab[];
-  __shared__ int hits_all[kWarps][kHitCap];
-  float* sA = sh_tab;
-  float* sB = sh_tab + a.n_types * (a.n_types + 1) / 2;
+  constexpr int kCap = STASH ? kStashCap : kHitCap;
+  static_assert(kScanU >= 1 && 32 * kScanU < kCap, "scan round exceeds the hit list");
+  extern __shared__ float4 sh_dyn[];
+  __shared__ int hits_all[STASH ? 1 : WARPS][STASH ? 1 : kHitCap];
   const int npair = a.n_types * (a.n_types + 1) / 2;
+  // dynamic shared memory: [stash e: WARPS][kCap] float4, [stash jt] int2,
+  // then the LJ tables
+  float4* stash_e = sh_dyn;
+  int2* stash_jt = reinterpret_cast<int2*>(sh_dyn + (STASH ? WARPS * kCap : 0));
+  float* sA = reinterpret_cast<float*>(stash_jt + (STASH ? WARPS * kCap : 0));
+  float* sB = sA + npair;
   for (int k = threadIdx.x; k < npair; k += blockDim.x) {
     sA[k] = a.A[k];
     sB[k] = a.B[k];
@@ -161,7 +188,9 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
-  int* hits = hits_all[w];
+  int* hits = hits_all[STASH ? 0 : w];
+  float4* se = stash_e + (STASH ? w * kCap : 0);
+  int2* sjt = stash_jt + (STASH ? w * kCap : 0);
   if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
   // Each block owns a contiguous range of sorted atoms, so the neighbours its
   // warps gather overlap and stay in this SM's L1.
@@ -169,7 +198,7 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   const int i_begin = blockIdx.x * per_block;
   const int i_end = min(a.n, i_begin + per_block);
   const unsigned lt = (1u << lane) - 1u;
-  for (int i = i_begin + w; i < i_end; i += kWarps) {
+  for (int i = i_begin + w; i < i_end; i += WARPS) {
   const float4 pi = a.pos[i];
   const float3 ri = make_float3(pi.x, pi.y, pi.z);
   const int ti = a.type[i];
@@ -193,17 +222,21 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   {
     // the warp's next row: start pulling its indices from HBM into L2 now
     // (row starts are multiples of 8 entries, so 16-byte aligned)
-    const int inext = i + kWarps;
+    const int inext = i + WARPS;
     if (lane == 0 && inext < i_end) {
       const int cn = a.row_count[inext];
       if (cn > 0)
         prefetch_l2(a.cols + a.row_start[inext], (unsigned)(cn * 4 + 15) & ~15u);
     }
   }
+  // hits of the row taken in earlier rounds: lane l takes the row's hits
+  // l, l + 32, ... in order whatever the rounds, so the float sums of i's
+  // force are the same for every hit-list capacity and scan width
+  int done = 0;
   for (int base = k0; base < k1;) {
     // phase 1: candidates -> hit list
     int count = 0;
-    for (; base < k1 && count <= kHitCap - 32 * kScanU; base += 32 * kScanU) {
+    for (; base < k1 && count <= kCap - 32 * kScanU; base += 32 * kScanU) {
       int jj[kScanU];
 #pragma unroll
       for (int u = 0; u < kScanU; ++u) {
@@ -211,9 +244,12 @@ k_lj_direct(PairArgs a, Accumulators acc) {
         jj[u] = k < k1 ? a.cols[k] : -1;
       }
       float4 pp[kScanU];
+      int tt[kScanU];
 #pragma unroll
-      for (int u = 0; u < kScanU; ++u)
+      for (int u = 0; u < kScanU; ++u) {
         if (jj[u] >= 0) pp[u] = a.pos[jj[u]];
+        tt[u] = STASH && !coul_only && jj[u] >= 0 ? a.type[jj[u]] : 0;
+      }
 #pragma unroll
       for (int u = 0; u < kScanU; ++u) {
         bool in = false;
@@ -227,14 +263,37 @@ k_lj_direct(PairArgs a, Accumulators acc) {
           }
         }
         const unsigned m = __ballot_sync(0xffffffffu, in);
-        if (in) hits[count + __popc(m & lt)] = jj[u];
+        if (in) {
+          const int slot = count + __popc(m & lt);
+          if (STASH) {
+            const float3 dr = min_image_fast<ORTHO>(make_float3(pp[u].x, pp[u].y, pp[u].z),
+                                                    ri, cell, rcell);
+            se[slot] = make_float4(dr.x, dr.y, dr.z, pp[u].w);
+            sjt[slot] = make_int2(jj[u], coul_only ? 0 : lj_pair_index(ti, tt[u]));
+          } else {
+            hits[slot] = jj[u];
+          }
+        }
         count += __popc(m);
       }
     }
     __syncwarp();
     // phase 2: pair terms over the hit list
-    if (coul_only) {
-      for (int h = lane; h < count; h += 32) {
+    const int h0 = (lane - done) & 31;
+    if (STASH && coul_only) {
+      for (int h = h0; h < count; h += 32) {
+        const int2 jt = sjt[h];
+        lj_pair_ab<ACCUM, ENERGY, VIRIAL, true>(a, acc, 0.f, 0.f, pi.w, gi, se[h], jt.x, fx,
+                                                fy, fz, e_lj, e_c, vir);
+      }
+    } else if (STASH) {
+      for (int h = h0; h < count; h += 32) {
+        const int2 jt = sjt[h];
+        lj_pair_ab<ACCUM, ENERGY, VIRIAL>(a, acc, sA[jt.y], sB[jt.y], pi.w, gi, se[h], jt.x,
+                                          fx, fy, fz, e_lj, e_c, vir);
+      }
+    } else if (coul_only) {
+      for (int h = h0; h < count; h += 32) {
         const int j = hits[h];
         const float4 pj = a.pos[j];
         const float3 dr = min_image_fast<ORTHO>(make_float3(pj.x, pj.y, pj.z), ri, cell,
@@ -244,7 +303,7 @@ k_lj_direct(PairArgs a, Accumulators acc) {
                                              fy, fz, e_lj, e_c, vir);
       }
     } else {
-      for (int h = lane; h < count; h += 32) {
+      for (int h = h0; h < count; h += 32) {
         const int j = hits[h];
         const float4 pj = a.pos[j];
         const int tj = a.type[j];
@@ -255,6 +314,7 @@ k_lj_direct(PairArgs a, Accumulators acc) {
                                        fz, e_lj, e_c, vir);
       }
     }
+    done += count;
     __syncwarp();
   }
   fx = warp_sum(fx);
@@ -276,15 +336,47 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   }
 }
 
+using RowKern = void (*)(PairArgs, Accumulators);
+
+// The plain single-box row kernel of W warps per block with or without the
+// hit stash (which needs at most 4 candidates per lane per round).
+template <int ACCUM, bool ENERGY, bool VIRIAL, int W, bool S>
+static RowKern row_kernel(int u) {
+  if constexpr (S)
+    return u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 2, 0, W, true>
+                  : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4, 0, W, true>;
+  else
+    return u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 2, 0, W>
+         : u == 8 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 8, 0, W>
+                  : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4, 0, W>;
+}
+
+// Raises a kernel's dynamic shared memory limit once, when it needs more
+// than the default 48 KB.
+static void allow_smem(RowKern k, size_t smem) {
+  static std::mutex mu;
+  static std::vector<std::pair<RowKern, size_t>> done;
+  if (smem <= 48 * 1024) return;
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& d : done)
+    if (d.first == k && d.second >= smem) return;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  done.push_back({k, smem});
+}
+
 template <int ACCUM, bool ENERGY, bool VIRIAL>
 static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream_t st) {
   size_t smem = sizeof(float) * a.n_types * (a.n_types + 1);
-  using Kern = void (*)(PairArgs, Accumulators);
-  Kern kern;
-  // the unroll choice applies to the MD step's variant (fixed point, force
-  // only, rectangular); the others take 4
-  const bool tunable = ACCUM == kAccumFixed && !ENERGY && !VIRIAL && ortho;
+  RowKern kern;
+  // the launch-shape choices apply to the MD step's variant (fixed point,
+  // force only, rectangular, one box, no solvent split); the others take 4
+  // candidates per lane and 8 warps without the stash
+  constexpr bool kTunable = ACCUM == kAccumFixed && !ENERGY && !VIRIAL;
+  const bool tunable = kTunable && ortho;
+  const bool single = a.bv.nsys == 0 && a.solvent_mode == 0;
   const int u = tunable ? a.unroll : 4;
+  const int wb = tunable && single ? a.warps : kWarps;
+  const bool stash = tunable && single && a.stash;
   if (a.solvent_mode != 0 && a.bv.nsys == 0)
     kern = ortho ? (a.solvent_mode == 1 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4, 1>
                                         : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4, 2>)
@@ -294,21 +386,35 @@ static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream
     kern = u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 2>
          : u == 8 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 8>
                   : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 4>;
-  else if (ortho)
-    kern = u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 2>
-         : u == 8 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 8>
-                  : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4>;
-  else
+  else if (ortho) {
+    if constexpr (kTunable) {
+      if (wb == 4)
+        kern = stash ? row_kernel<ACCUM, ENERGY, VIRIAL, 4, true>(u)
+                     : row_kernel<ACCUM, ENERGY, VIRIAL, 4, false>(u);
+      else if (wb == 16)
+        kern = stash ? row_kernel<ACCUM, ENERGY, VIRIAL, 16, true>(u)
+                     : row_kernel<ACCUM, ENERGY, VIRIAL, 16, false>(u);
+      else
+        kern = stash ? row_kernel<ACCUM, ENERGY, VIRIAL, kWarps, true>(u)
+                     : row_kernel<ACCUM, ENERGY, VIRIAL, kWarps, false>(u);
+    } else {
+      kern = row_kernel<ACCUM, ENERGY, VIRIAL, kWarps, false>(u);
+    }
+  } else {
     kern = k_lj_direct<ACCUM, ENERGY, VIRIAL, false, false, 4>;
+  }
+  if (stash) smem += (sizeof(float4) + sizeof(int2)) * (size_t)wb * kStashCap;
+  allow_smem(kern, smem);
   // persistent grid: as many blocks as fit at once, or the tuned count
   static int sms = 0;
   if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const int threads = 32 * wb;
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   per_sm = std::max(per_sm, 1);
   if (a.blocks_per_sm > 0) per_sm = std::min(per_sm, a.blocks_per_sm);
-  int blocks = std::max(1, std::min(sms * per_sm, ceil_div(a.n, kWarps)));
-  kern<<<blocks, 32 * kWarps, smem, st>>>(a, acc);
+  int blocks = std::max(1, std::min(sms * per_sm, ceil_div(a.n, threads / 32)));
+  kern<<<blocks, threads, smem, st>>>(a, acc);
 }
 
 template <int ACCUM>

@@ -200,8 +200,9 @@ __global__ void k_pack_pme_bin(int n, const float3* __restrict__ crd,
     fr4 = make_float4(fx, fy, fz, q);
     up = pack_u(ux, uy, uz);
   }
-  // sorted neighbours share tiles: one atomic per tile per warp
-  const int slot = warp_aggregated_inc(tile_count, t, active);
+  // sorted neighbours share tiles: one atomic per tile per warp (no tile
+  // counts for the atomic spread: tile_count null, uniform over the warp)
+  const int slot = tile_count ? warp_aggregated_inc(tile_count, t, active) : 0;
   if (!active) return;
   atom_tile[s] = t;
   atom_slot[s] = slot;
@@ -255,9 +256,9 @@ __device__ __forceinline__ int stencil_mask(int u, int K, int lo, int hi) {
 }
 
 constexpr int kTile = kTileEdge;
-constexpr int kTile3 = kTile * kTile * kTile;
 
-// One block of kSpreadWarps warps per 8x8x8 tile of the charge grid,
+// One block of W warps per T x T x T tile of the charge grid (T = 8, W = 2
+// unless the engine's autotuner picks another shape: T in {8, 16}),
 // accumulating in a shared-memory tile.  src{0,1,2}[t] = {count, b0, b1, b2}
 // lists the bins along each axis whose atoms can reach tile t.  The warps
 // take interleaved rounds of 32 atoms from those bins (one flat range of up
@@ -268,7 +269,7 @@ constexpr int kTile3 = kTile * kTile * kTile;
 // per charge unit).  Block barriers only after zeroing and before the single
 // store of the tile: no global atomics, and the grid is the same bit pattern
 // for any atom order.  A list that fills up is drained and refilled.
-constexpr int kSpreadWarps = 2;
+constexpr int kSpreadWarps = 2;   // W of the default shape
 constexpr int kSpreadList = 256;  // per-warp list of contributing atoms
 
 // Local index (p - lo) of the stencil point u - o on an axis of K points,
@@ -285,7 +286,7 @@ __device__ __forceinline__ void stencil_local(int u, int K, int lo, int hi, int*
 // Bound on the int32 tile sums.  A point's sum is at most the sum, over the
 // atoms whose stencils reach it, of |q| 2^22 (2/3)^3 (each B-spline weight is
 // at most 2/3) plus 1/2 for the rounding; every such atom's stencil meets the
-// 4x4x4 octant of the tile that holds the point.  So each lane keeps, per
+// (T/2)^3 octant of the tile that holds the point.  So each lane keeps, per
 // octant, the bound of the atoms it spreads that meet the octant; when the
 // block's sum of some octant could reach the int32 range the tile is taken
 // again with int64 sums.  A liquid's octants stay below a tenth of the range.
@@ -298,17 +299,18 @@ __device__ __forceinline__ void tile_add(long long* p, int c) {
             static_cast<unsigned long long>((long long)c));
 }
 
-// Bits of the 4-point halves (local index >> 2) a stencil axis touches.
+// Bits of the T/2-point halves (local index / (T/2)) a stencil axis touches.
+template <int T>
 __device__ __forceinline__ int halves_of(const int* l) {
   int m = 0;
 #pragma unroll
-  for (int o = 0; o < 4; ++o) m |= l[o] >= 0 ? 1 << (l[o] >> 2) : 0;
+  for (int o = 0; o < 4; ++o) m |= l[o] >= 0 ? 1 << (l[o] / (T / 2)) : 0;
   return m;
 }
 
 // Spreads one atom into the tile's store sq (local x runs from lo0); with
 // BOUND the atom's per-point bound is added to each octant its stencil meets.
-template <typename Acc, bool BOUND>
+template <int T, typename Acc, bool BOUND>
 __device__ __forceinline__ void spread_atom(Acc* sq, float4 f, int up, const TileGeom& g,
                                             int lo0, int hi0, int lo1, int hi1, int lo2,
                                             int hi2, float* oct) {
@@ -324,7 +326,7 @@ __device__ __forceinline__ void spread_atom(Acc* sq, float4 f, int up, const Til
   const float qs = f.w * kGridScale;
   if (BOUND) {
     const float b = fabsf(qs) * kPointWeightBound + 0.5f;
-    const int mx = halves_of(lx), my = halves_of(ly), mz = halves_of(lz);
+    const int mx = halves_of<T>(lx), my = halves_of<T>(ly), mz = halves_of<T>(lz);
 #pragma unroll
     for (int o = 0; o < 8; ++o)
       if ((mx >> (o >> 2) & 1) && (my >> ((o >> 1) & 1) & 1) && (mz >> (o & 1) & 1))
@@ -338,7 +340,7 @@ __device__ __forceinline__ void spread_atom(Acc* sq, float4 f, int up, const Til
     for (int oy = 0; oy < 4; ++oy) {
       if (ly[oy] < 0) continue;
       const float wxy = wq * wy[oy];
-      Acc* row = sq + (lx[ox] * kTile + ly[oy]) * kTile;
+      Acc* row = sq + (lx[ox] * T + ly[oy]) * T;
 #pragma unroll
       for (int oz = 0; oz < 4; ++oz)
         if (lz[oz] >= 0) tile_add(row + lz[oz], __float2int_rn(wxy * wz[oz]));
@@ -347,7 +349,7 @@ __device__ __forceinline__ void spread_atom(Acc* sq, float4 f, int up, const Til
 }
 
 // The contributors of one tile (pass 1 of k_pme_spread) spread into sq.
-template <typename Acc, bool BOUND>
+template <int T, int W, typename Acc, bool BOUND>
 __device__ __forceinline__ void spread_contributors(
     Acc* sq, int* list, const TileGeom& g, const float4* __restrict__ binned,
     const int* __restrict__ binned_u, int lo0, int hi0, int lo1, int hi1, int lo2,
@@ -355,7 +357,7 @@ __device__ __forceinline__ void spread_contributors(
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   int n_list = 0, bin_cursor = 0;
-  for (int base = 32 * w; base < total; base += 32 * kSpreadWarps) {
+  for (int base = 32 * w; base < total; base += 32 * W) {
     // atom of flat index base + lane: the bin whose range holds it
     const int fi = base + lane;
     int k = -1;
@@ -377,12 +379,12 @@ __device__ __forceinline__ void spread_contributors(
     const unsigned m = __ballot_sync(0xffffffffu, in);
     if (in) list[n_list + __popc(m & lt)] = k;
     n_list += __popc(m);
-    if (n_list > kSpreadList - 32 || base + 32 * kSpreadWarps >= total) {
+    if (n_list > kSpreadList - 32 || base + 32 * W >= total) {
       __syncwarp();
       for (int e = lane; e < n_list; e += 32) {
         const int ka = list[e];
-        spread_atom<Acc, BOUND>(sq, binned[ka], binned_u[ka], g, lo0, hi0, lo1, hi1, lo2,
-                                hi2, oct);
+        spread_atom<T, Acc, BOUND>(sq, binned[ka], binned_u[ka], g, lo0, hi0, lo1, hi1, lo2,
+                                   hi2, oct);
       }
       __syncwarp();
       n_list = 0;
@@ -391,18 +393,20 @@ __device__ __forceinline__ void spread_contributors(
 }
 
 // wide_tiles (may be null): running count of tiles taken again with int64
-// sums because an octant's bound could reach the int32 range.  Sixteen
-// blocks of 64 threads at 64 registers fill an SM's register file.
-template <bool BATCH>
-__global__ void __launch_bounds__(32 * kSpreadWarps, 16)
+// sums because an octant's bound could reach the int32 range.  At the
+// default shape sixteen blocks of 64 threads at 64 registers fill an SM's
+// register file.
+template <bool BATCH, int T = kTile, int W = kSpreadWarps>
+__global__ void __launch_bounds__(32 * W, 32 / W)
 k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
              const float4* __restrict__ binned, const int* __restrict__ binned_u,
              const int4* __restrict__ src0, const int4* __restrict__ src1,
              const int4* __restrict__ src2, float* __restrict__ Q, int ntiles,
              BatchView bv, int* __restrict__ wide_tiles) {
-  // the tile's int32 sums; the same 2 KB hold half a tile of int64 sums
+  // the tile's int32 sums; the same bytes hold half a tile of int64 sums
+  constexpr int kTile3 = T * T * T;
   __shared__ __align__(8) int sq[kTile3];
-  __shared__ int list_all[kSpreadWarps][kSpreadList];
+  __shared__ int list_all[W][kSpreadList];
   __shared__ float oct_sum[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int t = blockIdx.x;
@@ -449,8 +453,8 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
   float oct[8];
 #pragma unroll
   for (int o = 0; o < 8; ++o) oct[o] = 0.f;
-  spread_contributors<int, true>(sq, list, g, binned, binned_u, lo0, hi0, lo1, hi1, lo2,
-                                 hi2, nb, beg, cnt, excl, total, oct);
+  spread_contributors<T, W, int, true>(sq, list, g, binned, binned_u, lo0, hi0, lo1, hi1,
+                                       lo2, hi2, nb, beg, cnt, excl, total, oct);
 #pragma unroll
   for (int o = 0; o < 8; ++o) {
     const float v = warp_sum(oct[o]);
@@ -464,22 +468,22 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
   if (wide) {
     // some point's int32 sum could have wrapped: take the tile again in two
     // halves along x, each with int64 sums (exact and order-independent like
-    // the int32 ones) in the same 2 KB; values that fit int32 convert to the
-    // same floats
+    // the int32 ones) in the same shared bytes; values that fit int32
+    // convert to the same floats
     long long* sq64 = reinterpret_cast<long long*>(sq);
     constexpr int kHalf = kTile3 / 2;
     for (int h = 0; h < 2; ++h) {
-      const int hlo = lo0 + 4 * h, hhi = min(hlo + 4, hi0);
+      const int hlo = lo0 + (T / 2) * h, hhi = min(hlo + T / 2, hi0);
       __syncthreads();
       for (int k = threadIdx.x; k < kHalf; k += blockDim.x) sq64[k] = 0;
       __syncthreads();
       if (hlo < hhi)
-        spread_contributors<long long, false>(sq64, list, g, binned, binned_u, hlo, hhi,
-                                              lo1, hi1, lo2, hi2, nb, beg, cnt, excl,
-                                              total, oct);
+        spread_contributors<T, W, long long, false>(sq64, list, g, binned, binned_u, hlo,
+                                                    hhi, lo1, hi1, lo2, hi2, nb, beg, cnt,
+                                                    excl, total, oct);
       __syncthreads();
       for (int k = threadIdx.x; k < kHalf; k += blockDim.x) {
-        int x = k / (kTile * kTile), y = (k / kTile) % kTile, z = k % kTile;
+        int x = k / (T * T), y = (k / T) % T, z = k % T;
         if (x < hhi - hlo && y < w1 && z < w2)
           Q[((size_t)(hlo + x) * g.K1 + (lo1 + y)) * g.K2 + (lo2 + z)] =
               (float)((double)sq64[k] * (double)kGridScaleInv);
@@ -489,10 +493,58 @@ k_pme_spread(TileGeom g, const int* __restrict__ tile_start,
     return;
   }
   for (int k = threadIdx.x; k < kTile3; k += blockDim.x) {
-    int x = k / (kTile * kTile), y = (k / kTile) % kTile, z = k % kTile;
+    int x = k / (T * T), y = (k / T) % T, z = k % T;
     if (x < w0 && y < w1 && z < w2)
       Q[((size_t)(lo0 + x) * g.K1 + (lo1 + y)) * g.K2 + (lo2 + z)] =
           (float)sq[k] * kGridScaleInv;
+  }
+}
+
+// The same grid by global atomics: 16 lanes per atom, lane (ox, oy) adds
+// the four points of its z line in int64 fixed point (the products formed
+// in the tile path's order, so every point gets the same integers; integer
+// sums do not depend on their order).  Atoms in the pair kernel's sorted
+// order, so a warp's two atoms are neighbours.
+__global__ void __launch_bounds__(256)
+k_pme_spread_red(int n, const float4* __restrict__ frq, const int* __restrict__ upk,
+                 TileGeom g, long long* __restrict__ Q64) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t >> 4, l = t & 15;
+  if (i >= n) return;
+  const float4 f = frq[i];
+  const int up = upk[i];
+  const int ux = up >> 20, uy = (up >> 10) & 1023, uz = up & 1023;
+  const int ox = l >> 2, oy = l & 3;
+  float wx[4], wy[4], wz[4];
+  bspline4(f.x, wx);
+  bspline4(f.y, wy);
+  bspline4(f.z, wz);
+  const float qs = f.w * kGridScale;
+  const float wxy = qs * wx[ox] * wy[oy];
+  int px = ux - ox;
+  px += px < 0 ? g.K0 : 0;
+  int py = uy - oy;
+  py += py < 0 ? g.K1 : 0;
+  unsigned long long* row =
+      reinterpret_cast<unsigned long long*>(Q64) + ((size_t)px * g.K1 + py) * g.K2;
+#pragma unroll
+  for (int oz = 0; oz < 4; ++oz) {
+    int pz = uz - oz;
+    pz += pz < 0 ? g.K2 : 0;
+    const long long c = __float2int_rn(wxy * wz[oz]);
+    atomicAdd(row + pz, static_cast<unsigned long long>(c));
+  }
+}
+
+// int64 fixed-point grid -> float grid for the transform; the sums are
+// cleared for the next spread.  (float)v * 2^-22 equals the tile path's
+// conversion of the same integer (an int32 one, or an int64 one scaled in
+// double: the scale is a power of two).
+__global__ void k_pme_grid_float(int nall, long long* __restrict__ Q64,
+                                 float* __restrict__ Q) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nall; k += gridDim.x * blockDim.x) {
+    Q[k] = (float)Q64[k] * kGridScaleInv;
+    Q64[k] = 0;
   }
 }
 
@@ -901,6 +953,58 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
   return kOk;
 }
 
+// Spread shape of a one-box PME: edge T (8 or 16 grid points) and W warps
+// per tile (1, 2, 4 at T = 8; 4, 8 at T = 16), or T = 0 (W = 0): int64
+// global atomics instead of tiles.  Redraws the tiles and their source bins;
+// the grid, and so every result, is the same bit pattern for every shape.
+int pme_set_spread_shape(PME& p, int T, int W) {
+  if (p.bv.nsys > 0) return fail(kNotSupported, "PME: spread shape of a batch");
+  const bool ok = (T == 8 && (W == 1 || W == 2 || W == 4)) ||
+                  (T == 16 && (W == 4 || W == 8)) || (T == 0 && W == 0);
+  if (!ok) return fail(kBadInput, "PME: spread shape must be T 8 with 1, 2, 4 warps, T 16 "
+                                  "with 4, 8 warps, or T 0 (atomics)");
+  if (T == 0) {
+    if (!p.d_Q64) {
+      SNB_CUDA_TRY(cudaMalloc(&p.d_Q64, sizeof(long long) * (size_t)p.nall));
+      SNB_CUDA_TRY(cudaMemset(p.d_Q64, 0, sizeof(long long) * (size_t)p.nall));
+    }
+    if (!p.spread_atomic) {
+      // the tile counts restart from zero when the tiles come back
+      SNB_CUDA_TRY(cudaDeviceSynchronize());
+      SNB_CUDA_TRY(cudaMemset(p.d_tile_count, 0, sizeof(int) * p.ntiles));
+    }
+    p.spread_atomic = true;
+    return kOk;
+  }
+  p.spread_atomic = false;
+  p.spread_warps = W;
+  if (T == p.T) return kOk;
+  int nt[3];
+  std::vector<int4> src[3];
+  for (int d = 0; d < 3; ++d) {
+    nt[d] = ceil_div(p.K[d], T);
+    if (source_bins(p.K[d], T, src[d])) return fail(kBadInput, "PME: tile geometry");
+  }
+  const int ntiles = nt[0] * nt[1] * nt[2];
+  SNB_CUDA_TRY(cudaDeviceSynchronize());  // nothing in flight reads the old tiles
+  for (int d = 0; d < 3; ++d) {
+    cudaFree(p.d_src[d]);
+    SNB_CUDA_TRY(cudaMalloc(&p.d_src[d], sizeof(int4) * nt[d]));
+    SNB_CUDA_TRY(cudaMemcpy(p.d_src[d], src[d].data(), sizeof(int4) * nt[d],
+                            cudaMemcpyHostToDevice));
+    p.nt[d] = nt[d];
+  }
+  cudaFree(p.d_tile_count);
+  cudaFree(p.d_tile_start);
+  SNB_CUDA_TRY(cudaMalloc(&p.d_tile_count, sizeof(int) * ntiles));
+  SNB_CUDA_TRY(cudaMemset(p.d_tile_count, 0, sizeof(int) * ntiles));
+  SNB_CUDA_TRY(cudaMalloc(&p.d_tile_start, sizeof(int) * (ntiles + 1)));
+  p.T = T;
+  p.ntiles = ntiles;
+  if (scan_reserve(p.scan, p.ntiles)) return kCudaError;
+  return kOk;
+}
+
 int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
                    float tolerance, float grid_spacing, bool reciprocal, bool excluded) {
   if (n <= 0 || sys.empty()) return fail(kBadInput, "PME: empty batch");
@@ -1055,6 +1159,7 @@ int pme_wide_tiles(PME& p, int* count, cudaStream_t st) {
 
 void pme_free(PME& p) {
   cudaFree(p.d_wide_tiles);
+  cudaFree(p.d_Q64);
   for (auto& fg : p.groups) {
     if (fg.r2c) cufftDestroy(fg.r2c);
     if (fg.c2r) cufftDestroy(fg.c2r);
@@ -1098,7 +1203,7 @@ int pme_pack_bin(PME& p, int n, const float3* crd, const float* charge, const in
   else
     k_pack_pme_bin<false><<<ceil_div(n, 256), 256, 0, st>>>(
         n, crd, charge, type, perm, pos, type_sorted, g, p.d_atom_tile, p.d_atom_slot,
-        p.d_tile_count, p.d_frq, p.d_upk, p.bv, img_off);
+        p.spread_atomic ? nullptr : p.d_tile_count, p.d_frq, p.d_upk, p.bv, img_off);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -1118,7 +1223,10 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
              cufftSetStream(p.plan_c2r, st) != CUFFT_SUCCESS) {
     return fail(kCudaError, "PME: cufftSetStream failed");
   }
-  if (accum == kAccumFixed) {
+  if (accum == kAccumFixed && !batch && p.spread_atomic) {
+    k_pme_spread_red<<<ceil_div(n, 16), 256, 0, st>>>(n, p.d_frq, p.d_upk, g, p.d_Q64);
+    k_pme_grid_float<<<ceil_div(p.nall, 256 * 4), 256, 0, st>>>(p.nall, p.d_Q64, p.d_Q);
+  } else if (accum == kAccumFixed) {
     int rc = scan_exclusive(p.d_tile_count, p.d_tile_start, p.ntiles, nullptr, p.scan,
                             st);
     if (rc) return rc;
@@ -1126,14 +1234,23 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
         n, p.d_atom_tile, p.d_atom_slot, p.d_tile_start, p.d_frq, p.d_upk, p.d_binned,
         p.d_binned_u, p.d_tile_count, p.ntiles);
     const int sblocks = p.ntiles;  // one block per tile
+#define SNB_SPREAD(B, T, W)                                                              \
+  k_pme_spread<B, T, W><<<sblocks, 32 * (W), 0, st>>>(                                    \
+      g, p.d_tile_start, p.d_binned, p.d_binned_u, p.d_src[0], p.d_src[1], p.d_src[2],   \
+      p.d_Q, p.ntiles, p.bv, p.d_wide_tiles)
     if (batch)
-      k_pme_spread<true><<<sblocks, 32 * kSpreadWarps, 0, st>>>(
-          g, p.d_tile_start, p.d_binned, p.d_binned_u, p.d_src[0], p.d_src[1], p.d_src[2],
-          p.d_Q, p.ntiles, p.bv, p.d_wide_tiles);
+      SNB_SPREAD(true, kTile, kSpreadWarps);
+    else if (p.T == 16 && p.spread_warps == 8)
+      SNB_SPREAD(false, 16, 8);
+    else if (p.T == 16)
+      SNB_SPREAD(false, 16, 4);
+    else if (p.spread_warps == 4)
+      SNB_SPREAD(false, kTile, 4);
+    else if (p.spread_warps == 1)
+      SNB_SPREAD(false, kTile, 1);
     else
-      k_pme_spread<false><<<sblocks, 32 * kSpreadWarps, 0, st>>>(
-          g, p.d_tile_start, p.d_binned, p.d_binned_u, p.d_src[0], p.d_src[1], p.d_src[2],
-          p.d_Q, p.ntiles, p.bv, p.d_wide_tiles);
+      SNB_SPREAD(false, kTile, kSpreadWarps);
+#undef SNB_SPREAD
   } else {
     if (batch) return fail(kNotSupported, "PME batch: fixed-point accumulation only");
     SNB_CUDA_TRY(cudaMemsetAsync(p.d_Q, 0, sizeof(float) * p.nall, st));

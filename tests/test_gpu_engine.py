@@ -161,7 +161,7 @@ def test_autotune_keeps_results_bitwise(g, box_9k):
     try:
         f0 = force()
         c0, v0 = crd.cpu().numpy(), vel.cpu().numpy()
-        choice = np.zeros(4, np.int32)
+        choice = np.zeros(8, np.int32)
         with torch.cuda.stream(st):
             g.capi.check(lib.snb_engine_autotune(e, g.ptr(crd), g.ptr(vel), g.ptr(invm),
                                                  ctypes.c_float(dt), 3, choice.ctypes.data,
@@ -171,6 +171,9 @@ def test_autotune_keeps_results_bitwise(g, box_9k):
         assert np.array_equal(vel.cpu().numpy(), v0)
         assert choice[0] in (2, 4, 8) and choice[1] in (0, 2, 3)
         assert choice[2] in (4, 8, 16) and choice[3] in (128, 256, 512)
+        assert choice[4] in (4, 8, 16)
+        assert (choice[5], choice[6]) in ((8, 1), (8, 2), (8, 4), (16, 4), (16, 8), (0, 0))
+        assert choice[7] in (0, 1)
         f1 = force()
         assert np.array_equal(f0, f1)
         with torch.cuda.stream(st):  # graph steps with the tuned shapes
@@ -178,5 +181,58 @@ def test_autotune_keeps_results_bitwise(g, box_9k):
                                                        ctypes.c_float(dt), 0, 20, sp), "md")
         st.synchronize()
         assert np.isfinite(crd.cpu().numpy()).all()
+    finally:
+        lib.snb_engine_destroy(e)
+
+
+@pytest.mark.parametrize("shape", [(8, 1), (8, 4), (16, 4), (16, 8), (0, 0)])
+def test_launch_shapes_keep_forces_bitwise(g, box_9k, shape):
+    """Every spread shape (tiles, or int64 global atomics), every
+    rows-in-flight choice of the pair kernel and its hit stash give the same
+    fixed-point forces, bit for bit, as the tile spread of edge 8 with 2
+    warps, 8 rows per block and no stash, through graph steps too."""
+    import torch
+    from sponge_b200 import systems
+    s = box_9k
+    lib = g.capi.load()
+    st = torch.cuda.Stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+    dt = ctypes.c_float(0.5e-3 * systems.TIME_CONVERSION)
+    out = []
+    for choice in ([4, 0, 8, 256, 8, 8, 2, 0], [8, 0, 16, 128, 16, *shape, 0],
+                   [2, 2, 4, 512, 4, *shape, 1], [4, 0, 8, 256, 8, *shape, 1],
+                   [8, 3, 8, 256, 16, *shape, 1]):
+        e = g.engine_create(s, 8.0)
+        g.engine_set_water_bonded(e, s)
+        crd = g.dev(s.crd.reshape(-1), np.float32)
+        vel = g.dev(s.vel.reshape(-1), np.float32)
+        invm = g.dev((1.0 / s.mass).astype(np.float32))
+        f = torch.zeros(3 * s.n, dtype=torch.float32, device="cuda")
+        c = np.array(choice, np.int32)
+        try:
+            g.capi.check(lib.snb_engine_set_launch_shapes(e, c.ctypes.data), "shapes")
+            with torch.cuda.stream(st):
+                g.capi.check(lib.snb_engine_force(e, g.ptr(crd), g.ptr(f), 0, 0, 0, None, sp),
+                             "engine_force")
+                g.capi.check(lib.snb_engine_md_steps_graph(e, g.ptr(crd), g.ptr(vel),
+                                                           g.ptr(invm), dt, 1, 10, sp), "md")
+            st.synchronize()
+            out.append((f.cpu().numpy(), crd.cpu().numpy(), vel.cpu().numpy()))
+        finally:
+            lib.snb_engine_destroy(e)
+    for o in out[1:]:
+        for a, b in zip(out[0], o):
+            assert np.array_equal(a, b)
+
+
+def test_launch_shapes_refuse_values_outside_the_tuned_set(g, box_9k):
+    lib = g.capi.load()
+    e = g.engine_create(box_9k, 8.0)
+    try:
+        for bad in ([3, 0, 8, 256, 8, 8, 2, 0], [4, 0, 8, 256, 6, 8, 2, 0],
+                    [4, 0, 8, 256, 8, 16, 2, 0], [4, 0, 8, 256, 8, 12, 4, 0],
+                    [4, 0, 8, 256, 8, 8, 2, 2]):
+            c = np.array(bad, np.int32)
+            assert lib.snb_engine_set_launch_shapes(e, c.ctypes.data) != 0
     finally:
         lib.snb_engine_destroy(e)

@@ -1,9 +1,10 @@
 """snb_engine_md_steps_host: MD steps for a caller whose state lives in host
-memory.  Thirty one-step calls that copy crd / vel in from pinned host
-buffers and back out give, bit for bit, the trajectory of thirty
-device-resident graph steps; the host buffers hold the result when the call
-returns.  Both layouts: crd and vel apart, and side by side in one state
-array on each end (one copy each way)."""
+memory.  Thirty steps in calls that copy crd / vel in from pinned host
+buffers and back out (one step per call, or ten) give, bit for bit, the
+trajectory of thirty device-resident graph steps; the host buffers hold the
+result when the call returns.  The velocities cross the link beside the
+force phase and the first update waits for them.  Both layouts: crd and vel
+apart, and side by side in one state array on each end."""
 
 import ctypes
 
@@ -21,8 +22,9 @@ def g():
     return gpu_helpers
 
 
+@pytest.mark.parametrize("per_call", [1, 10])
 @pytest.mark.parametrize("layout", ["apart", "state"])
-def test_host_steps_equal_device_steps(g, layout):
+def test_host_steps_equal_device_steps(g, layout, per_call):
     import torch
     from sponge_b200 import systems
     s = systems.water_box(500, seed=9)
@@ -46,10 +48,10 @@ def test_host_steps_equal_device_steps(g, layout):
         try:
             with torch.cuda.stream(st):
                 if host:
-                    for k in range(30):
+                    for k in range(0, 30, per_call):
                         g.capi.check(lib.snb_engine_md_steps_host(
                             e, g.ptr(h_crd), g.ptr(h_vel), g.ptr(crd), g.ptr(vel), g.ptr(invm),
-                            dt, k, 1, sp), "host steps")
+                            dt, k, per_call, sp), "host steps")
                     out.append((h_crd.numpy().copy(), h_vel.numpy().copy()))
                 else:
                     for k in range(30):
