@@ -37,7 +37,7 @@ METRIC = "ns/day at 100k-atom LJ+PME water; batched steps/s; force rel-err vs FP
 DT_FS = 0.5
 # the launch shapes snb_engine_autotune reports, in its h_choice order
 TUNED_KEYS = ["pair_unroll", "pair_blocks_per_sm", "search_blocks_per_sm", "gather_threads",
-              "pair_warps", "spread_tile_edge", "spread_warps", "pair_hit_stash"]
+              "pair_warps", "spread_tile_edge", "spread_warps", "pair_hit_stash", "own_fft"]
 CUTOFF = 10.0
 SKIN = 2.0
 
@@ -483,7 +483,7 @@ def run_batch(args, lib, world, rank, dist):
     with torch.cuda.stream(st):
         capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
                                                  0, 100, sp), "batch warm-up")
-    tuned = np.zeros(8, np.int32)
+    tuned = np.zeros(9, np.int32)
     if not args.no_tune:
         with torch.cuda.stream(st):
             capi.check(lib.snb_engine_autotune(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
@@ -923,7 +923,7 @@ def run_ours(args):
             ke = 0.5 * (mass[:, None] * v * v).sum()
             t_now = 2.0 * ke / (3.0 * n * systems.KB)
             vel.mul_(float(torch.sqrt(300.0 / t_now)))
-    tuned = np.zeros(8, np.int32)
+    tuned = np.zeros(9, np.int32)
     if not args.no_tune:
         with torch.cuda.stream(st):
             capi.check(lib.snb_engine_autotune(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),

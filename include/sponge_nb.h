@@ -442,21 +442,26 @@ int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
  * memory (so that the pair terms gather nothing; plain single box, at most 4
  * candidates per lane), the pair search's
  * blocks per SM (4, 8, 16), the PME gather's threads per block (128, 256,
- * 512) and the PME spread's shape (tiles of edge 8 with 1, 2, 4 warps per
+ * 512), the PME spread's shape (tiles of edge 8 with 1, 2, 4 warps per
  * tile or edge 16 with 4, 8; or edge 0: int64 global atomics, no tiles;
- * single box).  Each step of a measurement starts from the given frame.
- * Results are bitwise the same for every shape.  crd / vel are restored; the next step rebuilds the list and
- * recaptures the step graph.  h_choice[0..7] receives {unroll, blocks per
+ * single box) and the PME convolution's FFT (cuFFT, or this library's own
+ * mixed-radix passes with the influence function fused between the forward
+ * and inverse x transforms; single box, axes of at most 256 points).  Each
+ * step of a measurement starts from the given frame.  Results are bitwise
+ * the same for every shape but the FFT, whose two choices differ by float
+ * rounding in the reciprocal part.  crd / vel are restored; the next step rebuilds the list and
+ * recaptures the step graph.  h_choice[0..8] receives {unroll, blocks per
  * SM (0 = occupancy maximum), search blocks per SM, gather threads, pair
  * warps per block, spread tile edge, spread warps per tile, hit stash (0 /
- * 1)}.  Allocates scratch. */
+ * 1), own FFT (0 / 1)}.  Allocates scratch. */
 int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
                         const float* inverse_mass, float dt, int steps,
                         int* h_choice, void* stream);
 /* No counterpart in the reference: sets the launch shapes directly, in the
  * h_choice order of snb_engine_autotune (for instance to reuse a tuned
- * choice); values outside the tuned sets are refused.  Results are bitwise
- * the same for every shape. */
+ * choice); values outside the tuned sets are refused, and so is the own FFT
+ * where the grid does not allow it.  Results are bitwise the same for every
+ * shape but the FFT choice. */
 int snb_engine_set_launch_shapes(snb_engine* e, const int* h_choice);
 /* Kernel nodes of the captured one-step graph: top level (a step without a
  * neighbor rebuild), cuFFT's share of them, and the kernels inside the
@@ -467,7 +472,10 @@ int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
 /* Number of neighbor-list rebuilds so far and current pair count (host sync). */
 int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
                      void* stream);
-/* snb_pme_spread_wide_tiles of the engine's PME (host sync). */
+/* snb_pme_spread_wide_tiles of the engine's PME (host sync).  A single-box
+ * engine spreads by int64 global atomics unless snb_engine_set_launch_shapes
+ * or snb_engine_autotune picks a tile shape; with the atomics no tile is
+ * taken again and the count stays 0. */
 int snb_engine_spread_wide_tiles(snb_engine* e, int* count, void* stream);
 /* The engine's neighbor list holds the pair set of NEIGHBOR_LIST::Update
  * (neighbor_list.cpp:974-1025) in one of two forms.  Rows (the default):

@@ -371,6 +371,16 @@ int launch_soft_rows(const SoftArgs& a, Accumulators& acc, bool energy, bool vir
                      cudaStream_t st);
 
 // ----------------------------------------------------------------------------
+// One axis of the convolution's own FFT passes (snb_fft.cuh): length and
+// radices in stage order.
+constexpr int kFftMaxN = 256;   // longest axis the passes take
+constexpr int kFftMaxStages = 8;
+struct FftAxis {
+  int N = 0;
+  int nst = 0;
+  int R[kFftMaxStages] = {};
+};
+
 // Particle mesh Ewald (reciprocal part).
 struct PME {
   int n = 0;
@@ -390,6 +400,12 @@ struct PME {
   // (one box; the same grid bit for bit)
   bool spread_atomic = false;
   long long* d_Q64 = nullptr;   // [nall], zero between steps
+  // the convolution by the own FFT passes instead of cuFFT (one box)
+  bool own_fft = false;
+  FftAxis fax[3];
+  float2* d_tw[3] = {nullptr, nullptr, nullptr};  // exp(-2 pi i k / K) per axis
+  double* d_xpartial = nullptr;  // [xblocks][8] sums of the x pass
+  int xblocks = 0;
   int nt[3] = {0, 0, 0};
   int ntiles = 0;
   float* d_B[3] = {nullptr, nullptr, nullptr};  // |b(k)|^2 per axis
@@ -440,6 +456,7 @@ int pme_init(PME& p, int n, const float* cell6, const float* box_length3,
 // Particle_Mesh::Update_Box: a new rectangular box at the same grid size.
 int pme_update_box(PME& p, const float* cell6);
 int pme_set_spread_shape(PME& p, int T, int W);
+int pme_set_own_fft(PME& p, bool own);
 int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
                    float tolerance, float grid_spacing, bool reciprocal, bool excluded);
 void pme_free(PME& p);

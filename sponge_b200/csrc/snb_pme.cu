@@ -22,6 +22,7 @@
 #include <tuple>
 #include <vector>
 
+#include "snb_fft.cuh"
 #include "snb_internal.h"
 
 namespace snb {
@@ -587,6 +588,65 @@ struct SpecGeom {
 
 constexpr int kSpecBlock = 256;
 
+// One point (kx, ky, kz) of the half spectrum: its influence BC(m) (0 at the
+// origin) scales c, and |c|^2 BC feeds the energy and virial sums.
+template <bool VIRIAL>
+__device__ __forceinline__ float2 influence_point(int kx, int ky, int kz, const SpecGeom& g,
+                                                  const float* __restrict__ B0,
+                                                  const float* __restrict__ B1,
+                                                  const float* __restrict__ B2, float2 c,
+                                                  bool energy, double& e, double* v) {
+  const bool origin = (kx | ky | kz) == 0;
+  float kxr = kx > g.K0 / 2 ? kx - g.K0 : kx;
+  float kyr = ky > g.K1 / 2 ? ky - g.K1 : ky;
+  float kzr = kz;
+  float mx = kxr * g.rcell.a11;
+  float my = kxr * g.rcell.a21 + kyr * g.rcell.a22;
+  float mz = kxr * g.rcell.a31 + kyr * g.rcell.a32 + kzr * g.rcell.a33;
+  float msq = mx * mx + my * my + mz * mz;
+  float bc = 0.f;
+  if (!origin) bc = g.inv_pi_v / msq * expf(-g.mpre * msq) * B0[kx] * B1[ky] * B2[kz];
+  float f2 = c.x * c.x + c.y * c.y;
+  if (energy) {
+    float we = (kz == 0 || (2 * kz == g.K2)) ? 0.5f : 1.0f;
+    e += (double)(we * bc * f2);
+  }
+  if (VIRIAL && !origin) {
+    float factor = (kz == 0 || kz == g.nc - 1) ? 0.5f : 1.0f;
+    float s = factor * f2 * 0.5f * bc;
+    float cc = 2.0f / msq * (1.0f + g.mpre * msq);
+    v[0] -= (double)(s * (1.0f - cc * mx * mx));
+    v[1] -= (double)(s * (0.0f - cc * my * mx));
+    v[2] -= (double)(s * (1.0f - cc * my * my));
+    v[3] -= (double)(s * (0.0f - cc * mz * mx));
+    v[4] -= (double)(s * (0.0f - cc * mz * my));
+    v[5] -= (double)(s * (1.0f - cc * mz * mz));
+  }
+  c.x *= bc;
+  c.y *= bc;
+  return c;
+}
+
+// Block sums of the energy and virial in FP64, fixed order, to
+// partial[block][0..6].
+__device__ __forceinline__ void influence_partials(double e, const double* v,
+                                                   double* __restrict__ partial) {
+  __shared__ double sh[kSpecBlock / 32][7];
+  double vals[7] = {e, v[0], v[1], v[2], v[3], v[4], v[5]};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    double x = warp_sum(vals[c]);
+    if (lane == 0) sh[warp][c] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w][threadIdx.x];
+    partial[(size_t)blockIdx.x * 8 + threadIdx.x] = s;
+  }
+}
+
 template <bool VIRIAL, bool BATCH>
 __global__ void __launch_bounds__(kSpecBlock)
 k_pme_influence(int nfft, SpecGeom g, const float* __restrict__ B0,
@@ -617,51 +677,51 @@ k_pme_influence(int nfft, SpecGeom g, const float* __restrict__ B0,
     int kz = idx % g.nc;
     int ky = (idx / g.nc) % g.K1;
     int kx = idx / (g.nc * g.K1);
-    float kxr = kx > g.K0 / 2 ? kx - g.K0 : kx;
-    float kyr = ky > g.K1 / 2 ? ky - g.K1 : ky;
-    float kzr = kz;
-    float mx = kxr * g.rcell.a11;
-    float my = kxr * g.rcell.a21 + kyr * g.rcell.a22;
-    float mz = kxr * g.rcell.a31 + kyr * g.rcell.a32 + kzr * g.rcell.a33;
-    float msq = mx * mx + my * my + mz * mz;
-    float bc = 0.f;
-    if (idx != 0) bc = g.inv_pi_v / msq * expf(-g.mpre * msq) * B0[kx] * B1[ky] * B2[kz];
-    cufftComplex c = FQ[idx];
-    float f2 = c.x * c.x + c.y * c.y;
-    if (energy) {
-      float we = (kz == 0 || (2 * kz == g.K2)) ? 0.5f : 1.0f;
-      e += (double)(we * bc * f2);
-    }
-    if (VIRIAL && idx != 0) {
-      float factor = (kz == 0 || kz == g.nc - 1) ? 0.5f : 1.0f;
-      float s = factor * f2 * 0.5f * bc;
-      float cc = 2.0f / msq * (1.0f + g.mpre * msq);
-      v[0] -= (double)(s * (1.0f - cc * mx * mx));
-      v[1] -= (double)(s * (0.0f - cc * my * mx));
-      v[2] -= (double)(s * (1.0f - cc * my * my));
-      v[3] -= (double)(s * (0.0f - cc * mz * mx));
-      v[4] -= (double)(s * (0.0f - cc * mz * my));
-      v[5] -= (double)(s * (1.0f - cc * mz * mz));
-    }
-    c.x *= bc;
-    c.y *= bc;
-    FQ[idx] = c;
+    const cufftComplex c = FQ[idx];
+    const float2 r = influence_point<VIRIAL>(kx, ky, kz, g, B0, B1, B2,
+                                             make_float2(c.x, c.y), energy, e, v);
+    FQ[idx] = make_cuComplex(r.x, r.y);
   }
-  // block reduction in FP64, fixed order
-  __shared__ double sh[kSpecBlock / 32][7];
-  double vals[7] = {e, v[0], v[1], v[2], v[3], v[4], v[5]};
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int c = 0; c < 7; ++c) {
-    double x = warp_sum(vals[c]);
-    if (lane == 0) sh[warp][c] = x;
+  influence_partials(e, v, partial);
+}
+
+// x pass of the convolution: the forward x transform of L columns (ky, kz)
+// of the half spectrum, the influence function with the energy / virial
+// sums, and the inverse x transform, in one pass over the columns.
+template <bool VIRIAL>
+__global__ void __launch_bounds__(kFftThreads)
+k_fft_x_influence(float2* __restrict__ FQ, int K1, int nc, FftAxis ax,
+                  const float2* __restrict__ tw_g, SpecGeom g, const float* __restrict__ B0,
+                  const float* __restrict__ B1, const float* __restrict__ B2,
+                  double* __restrict__ partial, bool energy) {
+  extern __shared__ float2 fsm[];
+  const int N = ax.N;  // == K0
+  const int L = fft_lines_per_block(N), S = L + 1;
+  float2* tw = fsm;
+  float2* A = fsm + N;
+  float2* B = A + N * S;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = tw_g[k];
+  const int ncol = K1 * nc, c0 = blockIdx.x * L;
+  for (int t = threadIdx.x; t < N * L; t += blockDim.x) {
+    const int line = t % L, n = t / L, c = c0 + line;
+    A[n * S + line] = c < ncol ? FQ[(size_t)n * ncol + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  if (threadIdx.x < 7) {
-    double s = 0.0;
-    for (int w = 0; w < kSpecBlock / 32; ++w) s += sh[w][threadIdx.x];
-    partial[(size_t)blockIdx.x * 8 + threadIdx.x] = s;
+  float2* Z = fft_lines<-1>(A, B, tw, ax, L);
+  double e = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
+  for (int t = threadIdx.x; t < N * L; t += blockDim.x) {
+    const int line = t % L, kx = t / L, c = c0 + line;
+    if (c < ncol)
+      Z[kx * S + line] = influence_point<VIRIAL>(kx, c / nc, c % nc, g, B0, B1, B2,
+                                                 Z[kx * S + line], energy, e, v);
   }
+  __syncthreads();
+  const float2* Y = fft_lines<1>(Z, Z == A ? B : A, tw, ax, L);
+  for (int t = threadIdx.x; t < N * L; t += blockDim.x) {
+    const int line = t % L, n = t / L, c = c0 + line;
+    if (c < ncol) FQ[(size_t)n * ncol + c] = Y[n * S + line];
+  }
+  influence_partials(e, v, partial);
 }
 
 // Final FP64 sums of the block partials plus the self / neutralising energy:
@@ -1005,6 +1065,42 @@ int pme_set_spread_shape(PME& p, int T, int W) {
   return kOk;
 }
 
+// The convolution by the own FFT passes (one box): radices and twiddles of
+// the three axes.  Refused when an axis is longer than kFftMaxN, the z axis
+// is odd, or a length has a prime factor above 7.
+int pme_set_own_fft(PME& p, bool own) {
+  if (p.bv.nsys > 0) return fail(kNotSupported, "PME: own FFT of a batch");
+  if (!own) {
+    p.own_fft = false;
+    return kOk;
+  }
+  if (!p.d_tw[0]) {
+    FftAxis ax[3];
+    for (int d = 0; d < 3; ++d)
+      if (!fft_axis(p.K[d], ax[d]))
+        return fail(kNotSupported, "PME: own FFT needs axes of at most 256 points with "
+                                   "factors 2, 3, 5, 7");
+    if (p.K[2] % 2) return fail(kNotSupported, "PME: own FFT needs an even z axis");
+    for (int d = 0; d < 3; ++d) {
+      const int N = p.K[d];
+      std::vector<float2> tw(N);
+      for (int k = 0; k < N; ++k) {
+        const double a = 2.0 * M_PI * (double)k / (double)N;
+        tw[k] = make_float2((float)std::cos(a), (float)-std::sin(a));
+      }
+      SNB_CUDA_TRY(cudaMalloc(&p.d_tw[d], sizeof(float2) * N));
+      SNB_CUDA_TRY(cudaMemcpy(p.d_tw[d], tw.data(), sizeof(float2) * N,
+                              cudaMemcpyHostToDevice));
+      p.fax[d] = ax[d];
+    }
+    const int nc = p.K[2] / 2 + 1;
+    p.xblocks = ceil_div(p.K[1] * nc, fft_lines_per_block(p.K[0]));
+    SNB_CUDA_TRY(cudaMalloc(&p.d_xpartial, sizeof(double) * 8 * (size_t)p.xblocks));
+  }
+  p.own_fft = true;
+  return kOk;
+}
+
 int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
                    float tolerance, float grid_spacing, bool reciprocal, bool excluded) {
   if (n <= 0 || sys.empty()) return fail(kBadInput, "PME: empty batch");
@@ -1160,6 +1256,8 @@ int pme_wide_tiles(PME& p, int* count, cudaStream_t st) {
 void pme_free(PME& p) {
   cudaFree(p.d_wide_tiles);
   cudaFree(p.d_Q64);
+  for (int d = 0; d < 3; ++d) cudaFree(p.d_tw[d]);
+  cudaFree(p.d_xpartial);
   for (auto& fg : p.groups) {
     if (fg.r2c) cufftDestroy(fg.r2c);
     if (fg.c2r) cufftDestroy(fg.c2r);
@@ -1257,14 +1355,6 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
     SNB_CUDA_TRY(cudaMemsetAsync(p.d_tile_count, 0, sizeof(int) * p.ntiles, st));
     k_pme_spread_atomic<<<ceil_div(n, 16), 256, 0, st>>>(n, p.d_frq, p.d_upk, g, p.d_Q);
   }
-  if (batch) {
-    for (auto& fg : p.groups)
-      if (cufftExecR2C(fg.r2c, p.d_Q + fg.grid_begin, p.d_FQ + fg.spec_begin) !=
-          CUFFT_SUCCESS)
-        return fail(kCudaError, "PME: cufftExecR2C failed");
-  } else if (cufftExecR2C(p.plan_r2c, p.d_Q, p.d_FQ) != CUFFT_SUCCESS) {
-    return fail(kCudaError, "PME: cufftExecR2C failed");
-  }
   SpecGeom sg;
   sg.K0 = p.K[0];
   sg.K1 = p.K[1];
@@ -1273,6 +1363,48 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
   sg.rcell = p.rcell;
   sg.mpre = (float)(M_PI * M_PI / ((double)p.beta * p.beta));
   sg.inv_pi_v = (float)(1.0 / (M_PI * p.volume));
+  if (!batch && p.own_fft) {
+    // z, y, then x with the influence function and back, then y and z
+    float2* FQ = reinterpret_cast<float2*>(p.d_FQ);
+    const int nrows = p.K[0] * p.K[1], nc = sg.nc;
+    const int zp = fft_row_pairs(p.K[2]);
+    const int zblocks = ceil_div(ceil_div(nrows, 2), zp);
+    const int yblocks = p.K[0] * ceil_div(nc, fft_lines_per_block(p.K[1]));
+    const size_t zs = fft_smem_rows(p.K[2]), ys = fft_smem_lines(p.K[1]);
+    const size_t xs = fft_smem_lines(p.K[0]);
+    if (zp == 16)
+      k_fft_r2c_z<16><<<zblocks, kFftThreads, zs, st>>>(p.d_Q, FQ, nrows, p.fax[2], nc,
+                                                        p.d_tw[2]);
+    else
+      k_fft_r2c_z<8><<<zblocks, kFftThreads, zs, st>>>(p.d_Q, FQ, nrows, p.fax[2], nc,
+                                                       p.d_tw[2]);
+    k_fft_y<-1><<<yblocks, kFftThreads, ys, st>>>(FQ, p.K[1], nc, p.fax[1], p.d_tw[1]);
+    if (need_virial)
+      k_fft_x_influence<true><<<p.xblocks, kFftThreads, xs, st>>>(
+          FQ, p.K[1], nc, p.fax[0], p.d_tw[0], sg, p.d_B[0], p.d_B[1], p.d_B[2],
+          p.d_xpartial, need_energy);
+    else
+      k_fft_x_influence<false><<<p.xblocks, kFftThreads, xs, st>>>(
+          FQ, p.K[1], nc, p.fax[0], p.d_tw[0], sg, p.d_B[0], p.d_B[1], p.d_B[2],
+          p.d_xpartial, need_energy);
+    if (need_energy || need_virial)
+      k_pme_finish<<<1, 1024, 0, st>>>(p.xblocks, p.d_xpartial, p.d_frq, n, (double)p.beta,
+                                       p.volume, p.d_sums, need_energy);
+    k_fft_y<1><<<yblocks, kFftThreads, ys, st>>>(FQ, p.K[1], nc, p.fax[1], p.d_tw[1]);
+    if (zp == 16)
+      k_fft_c2r_z<16><<<zblocks, kFftThreads, zs, st>>>(FQ, p.d_phi, nrows, p.fax[2], nc,
+                                                        p.d_tw[2]);
+    else
+      k_fft_c2r_z<8><<<zblocks, kFftThreads, zs, st>>>(FQ, p.d_phi, nrows, p.fax[2], nc,
+                                                       p.d_tw[2]);
+  } else if (batch) {
+    for (auto& fg : p.groups)
+      if (cufftExecR2C(fg.r2c, p.d_Q + fg.grid_begin, p.d_FQ + fg.spec_begin) !=
+          CUFFT_SUCCESS)
+        return fail(kCudaError, "PME: cufftExecR2C failed");
+  } else if (cufftExecR2C(p.plan_r2c, p.d_Q, p.d_FQ) != CUFFT_SUCCESS) {
+    return fail(kCudaError, "PME: cufftExecR2C failed");
+  }
   if (batch) {
     if (need_virial)
       k_pme_influence<true, true><<<p.spec_blocks, kSpecBlock, 0, st>>>(
@@ -1298,19 +1430,21 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
     SNB_CUDA_TRY(cudaGetLastError());
     return kOk;
   }
-  if (need_virial)
-    k_pme_influence<true, false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
-        p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy, p.bv,
-        nullptr);
-  else
-    k_pme_influence<false, false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
-        p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy, p.bv,
-        nullptr);
-  if (need_energy || need_virial)
-    k_pme_finish<<<1, 1024, 0, st>>>(p.partial_blocks, p.d_partial, p.d_frq, n,
-                                     (double)p.beta, p.volume, p.d_sums, need_energy);
-  if (cufftExecC2R(p.plan_c2r, p.d_FQ, p.d_phi) != CUFFT_SUCCESS)
-    return fail(kCudaError, "PME: cufftExecC2R failed");
+  if (!p.own_fft) {
+    if (need_virial)
+      k_pme_influence<true, false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
+          p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy, p.bv,
+          nullptr);
+    else
+      k_pme_influence<false, false><<<p.partial_blocks, kSpecBlock, 0, st>>>(
+          p.nfft, sg, p.d_B[0], p.d_B[1], p.d_B[2], p.d_FQ, p.d_partial, need_energy, p.bv,
+          nullptr);
+    if (need_energy || need_virial)
+      k_pme_finish<<<1, 1024, 0, st>>>(p.partial_blocks, p.d_partial, p.d_frq, n,
+                                       (double)p.beta, p.volume, p.d_sums, need_energy);
+    if (cufftExecC2R(p.plan_c2r, p.d_FQ, p.d_phi) != CUFFT_SUCCESS)
+      return fail(kCudaError, "PME: cufftExecC2R failed");
+  }
   const float scale = (float)p.update_interval;
   const int gt = p.gather_threads;  // 4 lanes per atom
   if (accum == kAccumFixed)

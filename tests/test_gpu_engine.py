@@ -35,11 +35,16 @@ def oracle_total(oracle, s, cutoff, skin=2.0):
     return frc, energies, vir
 
 
-def test_engine_force_and_energy(g, oracle, box_9k):
+@pytest.mark.parametrize("own_fft", [0, 1])
+def test_engine_force_and_energy(g, oracle, box_9k, own_fft):
+    """Forces, energies and the virial against FP64, with the PME
+    convolution through cuFFT and through the library's own FFT passes."""
     import torch
     s = box_9k
     lib = g.capi.load()
     e = g.engine_create(s, 8.0)
+    c = np.array([4, 0, 8, 256, 16, 0, 0, 0, own_fft], np.int32)
+    g.capi.check(lib.snb_engine_set_launch_shapes(e, c.ctypes.data), "shapes")
     crd = g.dev(s.crd.reshape(-1), np.float32)
     frc = torch.zeros(3 * s.n, dtype=torch.float32, device="cuda")
     tot = torch.zeros(16, dtype=torch.float64, device="cuda")
@@ -161,7 +166,7 @@ def test_autotune_keeps_results_bitwise(g, box_9k):
     try:
         f0 = force()
         c0, v0 = crd.cpu().numpy(), vel.cpu().numpy()
-        choice = np.zeros(8, np.int32)
+        choice = np.zeros(9, np.int32)
         with torch.cuda.stream(st):
             g.capi.check(lib.snb_engine_autotune(e, g.ptr(crd), g.ptr(vel), g.ptr(invm),
                                                  ctypes.c_float(dt), 3, choice.ctypes.data,
@@ -173,7 +178,7 @@ def test_autotune_keeps_results_bitwise(g, box_9k):
         assert choice[2] in (4, 8, 16) and choice[3] in (128, 256, 512)
         assert choice[4] in (4, 8, 16)
         assert (choice[5], choice[6]) in ((8, 1), (8, 2), (8, 4), (16, 4), (16, 8), (0, 0))
-        assert choice[7] in (0, 1)
+        assert choice[7] in (0, 1) and choice[8] in (0, 1)
         f1 = force()
         assert np.array_equal(f0, f1)
         with torch.cuda.stream(st):  # graph steps with the tuned shapes
@@ -199,9 +204,9 @@ def test_launch_shapes_keep_forces_bitwise(g, box_9k, shape):
     sp = ctypes.c_void_p(st.cuda_stream)
     dt = ctypes.c_float(0.5e-3 * systems.TIME_CONVERSION)
     out = []
-    for choice in ([4, 0, 8, 256, 8, 8, 2, 0], [8, 0, 16, 128, 16, *shape, 0],
-                   [2, 2, 4, 512, 4, *shape, 1], [4, 0, 8, 256, 8, *shape, 1],
-                   [8, 3, 8, 256, 16, *shape, 1]):
+    for choice in ([4, 0, 8, 256, 8, 8, 2, 0, 0], [8, 0, 16, 128, 16, *shape, 0, 0],
+                   [2, 2, 4, 512, 4, *shape, 1, 0], [4, 0, 8, 256, 8, *shape, 1, 0],
+                   [8, 3, 8, 256, 16, *shape, 1, 0]):
         e = g.engine_create(s, 8.0)
         g.engine_set_water_bonded(e, s)
         crd = g.dev(s.crd.reshape(-1), np.float32)
@@ -229,10 +234,40 @@ def test_launch_shapes_refuse_values_outside_the_tuned_set(g, box_9k):
     lib = g.capi.load()
     e = g.engine_create(box_9k, 8.0)
     try:
-        for bad in ([3, 0, 8, 256, 8, 8, 2, 0], [4, 0, 8, 256, 6, 8, 2, 0],
-                    [4, 0, 8, 256, 8, 16, 2, 0], [4, 0, 8, 256, 8, 12, 4, 0],
-                    [4, 0, 8, 256, 8, 8, 2, 2]):
+        for bad in ([3, 0, 8, 256, 8, 8, 2, 0, 0], [4, 0, 8, 256, 6, 8, 2, 0, 0],
+                    [4, 0, 8, 256, 8, 16, 2, 0, 0], [4, 0, 8, 256, 8, 12, 4, 0, 0],
+                    [4, 0, 8, 256, 8, 8, 2, 2, 0], [4, 0, 8, 256, 8, 8, 2, 0, 2]):
             c = np.array(bad, np.int32)
             assert lib.snb_engine_set_launch_shapes(e, c.ctypes.data) != 0
     finally:
         lib.snb_engine_destroy(e)
+
+
+@pytest.mark.parametrize("waters", [216, 520, 1400])
+def test_own_fft_matches_cufft(g, waters):
+    """The library's own FFT passes (grids 20^3 = 4 5, 28^3 = 4 7, 36^3 =
+    4 3 3) against cuFFT through the whole engine force: forces, reciprocal
+    energy and virial agree to float rounding."""
+    import torch
+    from sponge_b200 import systems
+    s = systems.water_box(waters, seed=3)
+    lib = g.capi.load()
+    out = []
+    for own in (0, 1):
+        e = g.engine_create(s, 8.0)
+        c = np.array([4, 0, 8, 256, 16, 0, 0, 0, own], np.int32)
+        crd = g.dev(s.crd.reshape(-1), np.float32)
+        frc = torch.zeros(3 * s.n, dtype=torch.float32, device="cuda")
+        tot = torch.zeros(16, dtype=torch.float64, device="cuda")
+        try:
+            g.capi.check(lib.snb_engine_set_launch_shapes(e, c.ctypes.data), "shapes")
+            g.capi.check(lib.snb_engine_force(e, g.ptr(crd), g.ptr(frc), 0, 1, 1, g.ptr(tot),
+                                              g.stream()), "engine_force")
+            torch.cuda.synchronize()
+        finally:
+            lib.snb_engine_destroy(e)
+        out.append((frc.cpu().numpy(), tot.cpu().numpy()))
+    (f0, t0), (f1, t1) = out
+    assert g.rel_rms(f1, f0) <= 1e-6
+    assert abs(t1[4] - t0[4]) <= 1e-6 * abs(t0[4])
+    assert np.all(np.abs(t1[8:14] - t0[8:14]) <= 1e-6 * np.abs(t0[8:14]).max())
