@@ -927,7 +927,7 @@ def run_ours(args):
     if not args.no_tune:
         with torch.cuda.stream(st):
             capi.check(lib.snb_engine_autotune(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
-                                               10, tuned.ctypes.data, sp), "autotune")
+                                               30, tuned.ctypes.data, sp), "autotune")
     with torch.cuda.stream(st):
         steps(EQ, W)
     st.synchronize()

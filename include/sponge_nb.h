@@ -433,9 +433,10 @@ int snb_engine_md_steps_host(snb_engine* e, float* h_crd, float* h_vel, float* c
 int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
                              const float* inverse_mass, float dt, int first_step,
                              int steps, double* h_phase_ms, void* stream);
-/* Autotuner (no counterpart in the reference).  Times `steps` stream-launched
- * steps from the same coordinates for each candidate launch shape and keeps
- * the fastest: the pair kernel's candidates per lane per scan round
+/* Autotuner (no counterpart in the reference).  For each candidate launch
+ * shape, times `steps` replays of the captured step graph (stream-launched
+ * steps for the pair search's shape, or where the stream is the legacy
+ * default one), each from the given coordinates, and keeps the fastest: the pair kernel's candidates per lane per scan round
  * (2, 4, 8) and persistent blocks per SM (occupancy maximum, 2, 3), its rows
  * in flight per block (4, 8, 16 warps; plain single box), whether its hit
  * list keeps each hit's displacement, charge and LJ pair index in shared
@@ -443,11 +444,12 @@ int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
  * candidates per lane), the pair search's
  * blocks per SM (4, 8, 16), the PME gather's threads per block (128, 256,
  * 512), the PME spread's shape (tiles of edge 8 with 1, 2, 4 warps per
- * tile or edge 16 with 4, 8; or edge 0: int64 global atomics, no tiles;
- * single box) and the PME convolution's FFT (cuFFT, or this library's own
+ * tile, or edge 0: int64 global atomics, no tiles; single box; edge 16 with
+ * 4, 8 warps is only set by snb_engine_set_launch_shapes) and the PME
+ * convolution's FFT (cuFFT, or this library's own
  * mixed-radix passes with the influence function fused between the forward
- * and inverse x transforms; single box, axes of at most 256 points).  Each
- * step of a measurement starts from the given frame.  Results are bitwise
+ * and inverse x transforms; single box, axes of at most 256 points).
+ * Results are bitwise
  * the same for every shape but the FFT, whose two choices differ by float
  * rounding in the reciprocal part.  crd / vel are restored; the next step rebuilds the list and
  * recaptures the step graph.  h_choice[0..8] receives {unroll, blocks per

@@ -177,7 +177,7 @@ def test_autotune_keeps_results_bitwise(g, box_9k):
         assert choice[0] in (2, 4, 8) and choice[1] in (0, 2, 3)
         assert choice[2] in (4, 8, 16) and choice[3] in (128, 256, 512)
         assert choice[4] in (4, 8, 16)
-        assert (choice[5], choice[6]) in ((8, 1), (8, 2), (8, 4), (16, 4), (16, 8), (0, 0))
+        assert (choice[5], choice[6]) in ((8, 1), (8, 2), (8, 4), (0, 0))
         assert choice[7] in (0, 1) and choice[8] in (0, 1)
         f1 = force()
         assert np.array_equal(f0, f1)
