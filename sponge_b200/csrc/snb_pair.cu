@@ -233,6 +233,17 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   // l, l + 32, ... in order whatever the rounds, so the float sums of i's
   // force are the same for every hit-list capacity and scan width
   int done = 0;
+  // with up to 4 candidates per lane, each round's indices are loaded one
+  // round ahead, so the gathers of a round wait only on their own load (at 8
+  // the extra registers spill).  The index stream is read once: loaded
+  // evict-first (__ldcs) so that L1 keeps the positions the rows share.
+  constexpr bool kAhead = kScanU <= 4;
+  int jn[kScanU];
+#pragma unroll
+  for (int u = 0; u < kScanU; ++u) {
+    const int k = k0 + 32 * u + lane;
+    jn[u] = kAhead && k < k1 ? __ldcs(a.cols + k) : -1;
+  }
   for (int base = k0; base < k1;) {
     // phase 1: candidates -> hit list
     int count = 0;
@@ -240,8 +251,14 @@ k_lj_direct(PairArgs a, Accumulators acc) {
       int jj[kScanU];
 #pragma unroll
       for (int u = 0; u < kScanU; ++u) {
-        const int k = base + 32 * u + lane;
-        jj[u] = k < k1 ? a.cols[k] : -1;
+        if (kAhead) {
+          jj[u] = jn[u];
+          const int k = base + 32 * (kScanU + u) + lane;
+          jn[u] = k < k1 ? __ldcs(a.cols + k) : -1;
+        } else {
+          const int k = base + 32 * u + lane;
+          jj[u] = k < k1 ? __ldcs(a.cols + k) : -1;
+        }
       }
       float4 pp[kScanU];
       int tt[kScanU];
