@@ -824,11 +824,20 @@ def run_soft_core_box(args, lib):
     EQ = max(0, args.soft_core_equilibrate)
     h, hs = window(0.0)
     _equilibrate(lib, h, s, crd, vel, invm, dt, EQ, st, sp)
+    # launch shapes tuned once, in the first window, and set in every window
+    P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    tuned = np.zeros(9, np.int32)
+    if not args.no_tune:
+        with torch.cuda.stream(st):
+            capi.check(lib.snb_engine_autotune(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
+                                               5, tuned.ctypes.data, sp), "soft-core autotune")
     close(h, hs)
     runs = []
     step = EQ
     for lam in (0.0, 0.25, 0.5, 0.75, 1.0):
         h, hs = window(lam)
+        if not args.no_tune:
+            capi.check(lib.snb_engine_set_launch_shapes(h, tuned.ctypes.data), "shapes")
         _timed_steps(lib, h, crd, vel, invm, dt, step, 10, st, sp)
         r0, r1 = ctypes.c_longlong(0), ctypes.c_longlong(0)
         capi.check(lib.snb_engine_stats(h, ctypes.byref(r0), None, sp), "stats")
@@ -852,6 +861,7 @@ def run_soft_core_box(args, lib):
                         f"PME {systems.fft_size(s.box)}^3, NVE 0.5 fs, alpha 0.5, p 1, "
                         "LJ decoupling windows (solute charges off)",
             "atoms": s.n, "equilibration_steps": EQ, "steps_per_lambda": 500,
+            "tuned": (None if args.no_tune else dict(zip(TUNED_KEYS, [int(x) for x in tuned]))),
             "lambdas": runs, "finite": ok}
 
 

@@ -475,9 +475,9 @@ int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
 int snb_engine_stats(snb_engine* e, long long* rebuilds, long long* pairs,
                      void* stream);
 /* snb_pme_spread_wide_tiles of the engine's PME (host sync).  A single-box
- * engine spreads by int64 global atomics unless snb_engine_set_launch_shapes
- * or snb_engine_autotune picks a tile shape; with the atomics no tile is
- * taken again and the count stays 0. */
+ * engine of up to 500,000 atoms spreads by int64 global atomics unless
+ * snb_engine_set_launch_shapes or snb_engine_autotune picks a tile shape;
+ * with the atomics no tile is taken again and the count stays 0. */
 int snb_engine_spread_wide_tiles(snb_engine* e, int* count, void* stream);
 /* The engine's neighbor list holds the pair set of NEIGHBOR_LIST::Update
  * (neighbor_list.cpp:974-1025) in one of two forms.  Rows (the default):

@@ -1060,10 +1060,11 @@ extern "C" int snb_engine_create(const snb_options* opt, int n, snb_boundary bou
                   e->opt.pm_fftx, e->opt.pm_ffty, e->opt.pm_fftz, e->opt.pm_grid_spacing,
                   e->opt.pme_update_interval, e->opt.pme_calculate_reciprocal_part != 0,
                   e->opt.pme_calculate_excluded_part != 0);
-  // the engine spreads by int64 atomics unless a launch shape says
-  // otherwise: measured on the 100k box, the step is 14 us shorter than with
-  // the tiles (the same grid)
-  if (!rc) rc = pme_set_spread_shape(e->pme, 0, 0);
+  // the engine spreads by int64 atomics up to half a million atoms unless a
+  // launch shape says otherwise (the same grid as the tiles): on the 100k box
+  // the step is 14 us shorter than with the tiles; on the 1M box the 64 M
+  // reductions of the atomic spread made it 0.16 ms longer
+  if (!rc && n <= 500000) rc = pme_set_spread_shape(e->pme, 0, 0);
   if (!rc)
     rc = engine_finish_create(e, n, n_types, h_type, h_A, h_B, h_charge, h_es, h_en, h_el,
                               n_excl);
