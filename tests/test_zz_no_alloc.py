@@ -117,3 +117,36 @@ def test_noalloc_later_calls_leave_free_device_memory_unchanged(g, box_9k):
     free2, _ = torch.cuda.mem_get_info()
     assert torch.cuda.memory_reserved() == reserved1
     assert free2 == free1, (free0, free1, free2, reserved0, reserved1)
+
+
+def test_noalloc_call_captured_in_a_graph(g, box_9k):
+    """After a first call outside any capture, a call captured in a CUDA
+    graph and replayed gives the handle path's results, replay after
+    replay (the scratch is cleared by each call)."""
+    import torch
+    lib = g.capi.load()
+    box = g.Box(box_9k)
+    beta, want = _with_handle(g, box)
+    _noalloc(g, box, beta)  # the first call resolves the scratch
+    n = box.n
+    frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+    ae = torch.zeros(n, dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6 * n, dtype=torch.float32, device="cuda")
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side, capture_error_mode="thread_local"):
+            g.capi.check(lib.snb_pme_excluded_force_noalloc(
+                n, g.ptr(box.crd), box.b, g.ptr(box.charge), ctypes.c_float(beta),
+                g.ptr(box.es), g.ptr(box.el), g.ptr(box.en), g.ptr(frc), 1, g.ptr(ae), 1,
+                g.ptr(vir), ctypes.c_void_p(side.cuda_stream)), "captured call")
+    torch.cuda.synchronize()
+    for _ in range(2):
+        for t in (frc, ae, vir):
+            t.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        _same(dict(frc=frc.cpu().numpy().reshape(n, 3), atom_energy=ae.cpu().numpy(),
+                   virial=vir.cpu().numpy().reshape(n, 6)), want)
+    del graph
