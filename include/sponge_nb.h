@@ -436,12 +436,13 @@ int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
 /* Autotuner (no counterpart in the reference).  For each candidate launch
  * shape, times `steps` replays of the captured step graph (stream-launched
  * steps for the pair search's shape, or where the stream is the legacy
- * default one), each from the given coordinates, and keeps the fastest: the pair kernel's candidates per lane per scan round
- * (2, 4, 8) and persistent blocks per SM (occupancy maximum, 2, 3), its rows
- * in flight per block (4, 8, 16 warps; plain single box), whether its hit
- * list keeps each hit's displacement, charge and LJ pair index in shared
- * memory (so that the pair terms gather nothing; plain single box, at most 4
- * candidates per lane), the pair search's
+ * default one), each from the given coordinates, and keeps the fastest:
+ * the pair kernel's candidates per lane per scan round (2, 4, 8) and
+ * persistent blocks per SM (occupancy maximum, 2, 3), its rows in flight
+ * per block (4, 8, 16 warps for one box, 8 or 16 for a batch; plain LJ),
+ * whether its hit list keeps each hit's displacement, charge and LJ pair
+ * index in shared memory (so that the pair terms gather nothing; plain
+ * single box, at most 4 candidates per lane), the pair search's
  * blocks per SM (4, 8, 16), the PME gather's threads per block (128, 256,
  * 512), the PME spread's shape (tiles of edge 8 with 1, 2, 4 warps per
  * tile, or edge 0: int64 global atomics, no tiles; single box; edge 16 with

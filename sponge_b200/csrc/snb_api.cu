@@ -2084,12 +2084,12 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
   // candidates per lane per round and rows in flight per block (the row
   // kernel of the plain single box) together, then blocks per SM
   int bw = e->pair_warps;
-  const bool warps_knob = rows && !e->soft && e->nsys == 0;
+  const bool warps_knob = rows && !e->soft;
   for (int u : {2, 4, 8})
     for (int w : {4, 8, 16}) {
       if (rc) break;
       if (!rows && u != bu) continue;  // the cluster kernel has no unroll choice
-      if (!warps_knob && w != bw) continue;
+      if ((!warps_knob && w != bw) || (e->nsys > 0 && w == 4)) continue;
       e->pair_unroll = u;
       e->pair_warps = w;
       e->pair_blocks_per_sm = 0;

@@ -392,13 +392,21 @@ static void launch3(const PairArgs& a, Accumulators& acc, bool ortho, cudaStream
   const bool tunable = kTunable && ortho;
   const bool single = a.bv.nsys == 0 && a.solvent_mode == 0;
   const int u = tunable ? a.unroll : 4;
-  const int wb = tunable && single ? a.warps : kWarps;
+  // rows in flight per block: 4, 8 or 16 warps for one box, 8 or 16 for a
+  // batch; 8 for the other variants
+  int wb = kWarps;
+  if (tunable && a.solvent_mode == 0)
+    wb = a.bv.nsys == 0 ? a.warps : (a.warps == 16 ? 16 : kWarps);
   const bool stash = tunable && single && a.stash;
   if (a.solvent_mode != 0 && a.bv.nsys == 0)
     kern = ortho ? (a.solvent_mode == 1 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4, 1>
                                         : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, false, 4, 2>)
                  : (a.solvent_mode == 1 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, false, false, 4, 1>
                                         : k_lj_direct<ACCUM, ENERGY, VIRIAL, false, false, 4, 2>);
+  else if (a.bv.nsys > 0 && kTunable && wb == 16)
+    kern = u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 2, 0, 16>
+         : u == 8 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 8, 0, 16>
+                  : k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 4, 0, 16>;
   else if (a.bv.nsys > 0)
     kern = u == 2 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 2>
          : u == 8 ? k_lj_direct<ACCUM, ENERGY, VIRIAL, true, true, 8>
