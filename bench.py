@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--soft-core-waters", type=int, default=333333,
                    help="waters of the soft-core box (about 1M atoms; 0: skip)")
     p.add_argument("--soft-core-equilibrate", type=int, default=1000)
+    p.add_argument("--soft-core-grid150", type=int, default=1,
+                   help="also run the soft-core box's lambda 0.5 window with PME 150^3 (0: skip)")
     p.add_argument("--no-accuracy", action="store_true",
                    help="skip the FP64 accuracy checks (outside the timed regions)")
     p.add_argument("--plain-gpu-steps", type=int, default=1000,
@@ -656,7 +658,7 @@ def plain_gpu_run(s, crd0, vel0, steps, warmup):
                     "float atomics, driven in main.cpp's order; NVE leap-frog"}
 
 
-def soft_accuracy(lib, h, s, sc, crd, lam, step, st, sp):
+def soft_accuracy(lib, h, s, sc, crd, lam, step, st, sp, grid=None):
     """Force rel-RMS of the soft-core engine at the current frame against the
     FP64 oracle (soft-core direct terms, PME, excluded correction) over all
     atoms; the windows' charges are state B's (solute charges off)."""
@@ -678,16 +680,17 @@ def soft_accuracy(lib, h, s, sc, crd, lam, step, st, sp):
     scb = copy.copy(sc)
     scb.charge_B_A = np.zeros_like(sc.charge_B_A)
     want = accuracy.soft_reference_forces(Oracle(), f, scb, CUTOFF, lam, 0.5, 1.0, 3.0, 0.0,
-                                          SKIN)
+                                          SKIN, grid=None if grid is None else (grid,) * 3)
     return {"lambda": lam, "force_rel_rms": accuracy.force_rel_rms(
         frc.cpu().numpy().reshape(-1, 3), want),
         "reference": "FP64 oracle over all atoms at the frame after the window"}
 
 
-def make_engine(lib, s, cutoff):
-    """Single-box engine over System `s` with its water bonds and angles."""
+def make_engine(lib, s, cutoff, **keys):
+    """Single-box engine over System `s` with its water bonds and angles
+    (`keys`: more input keys, e.g. PM_fftx)."""
     from sponge_b200 import capi, systems
-    opts = capi.options(cutoff=cutoff, skin=SKIN)
+    opts = capi.options(cutoff=cutoff, skin=SKIN, **keys)
     h = ctypes.c_void_p()
     arr = np.ascontiguousarray
     t, A, B = arr(s.lj_type, np.int32), arr(s.lj_A, np.float32), arr(s.lj_B, np.float32)
@@ -801,10 +804,11 @@ def run_soft_core_box(args, lib):
     BA, BB = arr(sc.BA, np.float32), arr(sc.BB, np.float32)
     mask = arr(sc.mask, np.int32)
 
-    def window(lam):
+    def window(lam, grid=None):
         w = copy.copy(s)
         w.charge = (s.charge.astype(np.float64) + sc.charge_B_A).astype(np.float32)
-        h = make_engine(lib, w, CUTOFF)
+        keys = {} if grid is None else {"PM_fftx": grid, "PM_ffty": grid, "PM_fftz": grid}
+        h = make_engine(lib, w, CUTOFF, **keys)
         o = capi.options(cutoff=CUTOFF, skin=SKIN, lambda_lj=lam, soft_core_alpha=0.5,
                          soft_core_powfer=1.0, soft_core_sigma=3.0, soft_core_sigma_min=0.0)
         hs = ctypes.c_void_p()
@@ -854,8 +858,24 @@ def run_soft_core_box(args, lib):
                      "nl_rebuilds": int(r1.value - r0.value),
                      "temperature_K": float(2.0 * ke.sum() / (3.0 * s.n * systems.KB)),
                      "hottest_atom_kcal_per_mol": float(ke.max())})
+    # the stated grid variant: PME 150^3 set explicitly (the reference's
+    # PM_fftx/y/z keys) in the lambda 0.5 window, from the state the windows
+    # left
+    g150 = None
+    if args.soft_core_grid150:
+        h, hs = window(0.5, grid=150)
+        if not args.no_tune:
+            capi.check(lib.snb_engine_set_launch_shapes(h, tuned.ctypes.data), "shapes")
+        _timed_steps(lib, h, crd, vel, invm, dt, step, 10, st, sp)
+        ms = _timed_steps(lib, h, crd, vel, invm, dt, step + 10, 500, st, sp)
+        g150 = {"lambda": 0.5, "pme_grid": [150, 150, 150], "steps": 500,
+                "ms_per_step": ms / 500, "ns_per_day": ns_per_day(500 / (ms / 1e3))}
+        if not args.no_accuracy:
+            a150 = soft_accuracy(lib, h, s, sc, crd, 0.5, step + 510, st, sp, grid=150)
+            g150["force_rel_rms"] = a150["force_rel_rms"]
+        close(h, hs)
     ok = bool(torch.isfinite(crd).all().item())
-    return {"accuracy": acc,
+    return {"accuracy": acc, "grid_150": g150,
             "workload": f"{s.n}-atom water + NaCl box with a 64-site soft-core solute, "
                         f"L = {s.box:.2f} A, cutoff 10 A, skin 2 A, "
                         f"PME {systems.fft_size(s.box)}^3, NVE 0.5 fs, alpha 0.5, p 1, "
