@@ -494,6 +494,8 @@ def run_batch(args, lib, world, rank, dist):
         capi.check(lib.snb_engine_md_steps_graph(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
                                                  100, WB, sp), "batch warm-up")
     st.synchronize()
+    rb0, rb1 = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    capi.check(lib.snb_engine_stats(h, ctypes.byref(rb0), None, sp), "stats")
     if dist:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -504,6 +506,7 @@ def run_batch(args, lib, world, rank, dist):
     e1.record(st)
     st.synchronize()
     ms_b = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    capi.check(lib.snb_engine_stats(h, ctypes.byref(rb1), None, sp), "stats")
     kn, libk, bodyk = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
     capi.check(lib.snb_engine_graph_info(h, ctypes.byref(kn), ctypes.byref(libk),
                                          ctypes.byref(bodyk), sp), "graph_info")
@@ -568,6 +571,8 @@ def run_batch(args, lib, world, rank, dist):
     return {"systems": args.batch_systems, "systems_per_rank": len(boxes),
             "atoms_per_rank": int(offs[-1]), "steps": KB,
             "steps_per_s": sps_b, "ms_per_step": float(ms_b.item()) / KB,
+            # steps of the timed window on which at least one box rebuilt its list
+            "steps_with_rebuild": int(rb1.value - rb0.value),
             "one_system_per_launch_steps_per_s": sps_s,
             "one_system_per_launch_steps": KS,
             "speedup_vs_one_system_per_launch": sps_b / sps_s,

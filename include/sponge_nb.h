@@ -343,8 +343,11 @@ int snb_engine_create(const snb_options* opt, int atom_numbers,
  * one PME spread / gather with a grid per box, one batched cuFFT plan per
  * grid size).  Each box gets the single-box defaults: its own cell grid and
  * PME grid (by PM_grid_spacing); PME every step, displacement-triggered list
- * updates and fixed-point accumulation are required.  Energies and virials
- * from snb_engine_force are sums over the systems. */
+ * updates and fixed-point accumulation are required.  A list update starts
+ * when an atom of some box moved more than half the skin since that box's
+ * last build; it rebuilds that box's list and those of the boxes with an
+ * atom past three quarters of that allowance, and keeps the others.
+ * Energies and virials from snb_engine_force are sums over the systems. */
 int snb_batch_create(const snb_options* opt, int n_systems,
                      const int* atoms_per_system, const float* box_lengths,
                      int atom_type_numbers, const int* h_atom_LJ_type,

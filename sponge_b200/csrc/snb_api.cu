@@ -143,6 +143,8 @@ struct snb_engine {
   std::vector<SysGeom> h_sys;
   SysGeom* d_sys = nullptr;
   int* d_sys_of = nullptr;
+  int* d_cell_sys = nullptr;          // [ncell] system of each neighbor cell
+  unsigned char* d_box_need = nullptr;  // [nsys] systems whose list is rebuilt
   BatchView bv;
   double lrc_energy = 0.0;   // tail energy summed over the boxes
   double lrc_virial = 0.0;   // tail virial (diagonal) summed over the boxes
@@ -1148,10 +1150,27 @@ extern "C" int snb_batch_create(const snb_options* opt, int n_systems,
       rc = fail(kCudaError, "batch_create: system table upload failed");
   }
   if (!rc) {
+    // each system rebuilds its list when its own atoms moved past the skin
+    // allowance: cell -> system map and the per-system flags
+    std::vector<int> cell_sys(e->nl.ncell, 0);
+    for (int s = 0; s < n_systems; ++s) {
+      const SysGeom& g = e->h_sys[s];
+      for (int c = g.cell_begin; c < g.cell_begin + g.Nx * g.Ny * g.Nz; ++c) cell_sys[c] = s;
+    }
+    if (cudaMalloc(&e->d_cell_sys, sizeof(int) * cell_sys.size()) != cudaSuccess ||
+        cudaMemcpy(e->d_cell_sys, cell_sys.data(), sizeof(int) * cell_sys.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc(&e->d_box_need, n_systems) != cudaSuccess ||
+        cudaMemset(e->d_box_need, 0, n_systems) != cudaSuccess)
+      rc = fail(kCudaError, "batch_create: per-system rebuild tables failed");
+  }
+  if (!rc) {
     e->bv.sys = e->d_sys;
     e->bv.sys_of = e->d_sys_of;
     e->bv.tile_sys = e->pme.d_tile_sys;
     e->bv.nsys = n_systems;
+    e->bv.box_need = e->d_box_need;
+    e->bv.cell_sys = e->d_cell_sys;
     e->nl.bv = e->bv;
     e->pme.bv = e->bv;
     rc = engine_finish_create(e, n, n_types, h_type, h_A, h_B, h_charge, h_es, h_en, h_el,
@@ -2384,6 +2403,8 @@ extern "C" int snb_engine_destroy(snb_engine* e) {
   cudaFree(e->d_snap_vel);
   cudaFree(e->d_sys);
   cudaFree(e->d_sys_of);
+  cudaFree(e->d_cell_sys);
+  cudaFree(e->d_box_need);
   for (void* p : {(void*)e->d_ba, (void*)e->d_bb, (void*)e->d_bk, (void*)e->d_br0,
                   (void*)e->d_aa, (void*)e->d_ab, (void*)e->d_ac, (void*)e->d_ak,
                   (void*)e->d_at0})

@@ -76,7 +76,30 @@ struct BatchView {
   const int* sys_of = nullptr;   // [n] system of each atom
   const int* tile_sys = nullptr;  // [ntiles] system of each PME tile
   int nsys = 0;
+  // per-system list rebuild: box_need[s] set when an atom of system s moved
+  // past the skin allowance (cleared after each rebuild); cell_sys maps a
+  // neighbor cell to its system
+  unsigned char* box_need = nullptr;  // [nsys]
+  const int* cell_sys = nullptr;      // [ncell]
 };
+
+// A batch rebuilds the lists of the systems that need it.  A system joins a
+// rebuild once one of its atoms has moved more than kBatchEarly x the skin
+// allowance; only a move past the full allowance starts one.  Systems near
+// their own limit thus rebuild together, so fewer steps rebuild at all.
+constexpr float kBatchEarly = 0.75f;
+
+// Marks system s of a batch for the next rebuild after an atom of it moved
+// by sqrt(d2) (permit2: the squared allowance).
+__device__ __forceinline__ void box_mark(unsigned char* need, int s, float d2, float permit2) {
+  if (d2 > permit2 * (kBatchEarly * kBatchEarly) && need[s] == 0) need[s] = 1;
+}
+
+// True unless i (an atom, or a sorted slot: a system's sorted slots are its
+// own atom range) belongs to a system that keeps its list this rebuild.
+__device__ __forceinline__ bool box_rebuilds(const unsigned char* need, const int* sys, int i) {
+  return need == nullptr || need[sys[i]] != 0;
+}
 
 // ----------------------------------------------------------------------------
 // Neighbor list: cell grid of side >= (cutoff+skin)/2 (neighbor_list.cpp:943),

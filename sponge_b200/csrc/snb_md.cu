@@ -144,7 +144,9 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
       rcell = sg.rcell;
     }
     float3 d = min_image_fast<false>(r, r_old, cell, rcell);
-    bool moved = d.x * d.x + d.y * d.y + d.z * d.z > permit2;
+    const float d2 = d.x * d.x + d.y * d.y + d.z * d.z;
+    bool moved = d2 > permit2;
+    if (BATCH && bv.box_need) box_mark(bv.box_need, bv.sys_of[i], d2, permit2);
     if (__any_sync(__activemask(), moved) && moved) atomicExch(&flags[0], 1);
   }
 }

@@ -28,8 +28,10 @@
 namespace snb {
 
 // flags layout
+// kFlagFull: the pending rebuild covers every system of a batch (so the
+// pair total restarts from zero instead of being corrected row by row)
 enum { kFlagNeed = 0, kFlagListOverflow = 1, kFlagTotal = 2, kFlagGeneration = 3,
-       kFlagExportOverflow = 4, kFlagMaxRow = 5, kNumFlags = 8 };
+       kFlagExportOverflow = 4, kFlagMaxRow = 5, kFlagFull = 6, kNumFlags = 8 };
 
 // ---------------------------------------------------------------------------
 // Refresh decision (Check_Refresh, neighbor_list.cpp:307-321): any atom moved
@@ -47,13 +49,26 @@ __global__ void k_check_refresh(int n, const float3* __restrict__ crd,
       rcell = g.rcell;
     }
     float3 d = min_image_fast<false>(crd[i], old_crd[i], cell, rcell);
-    moved = d.x * d.x + d.y * d.y + d.z * d.z > permit2;
+    const float d2 = d.x * d.x + d.y * d.y + d.z * d.z;
+    moved = d2 > permit2;
+    if (BATCH && bv.box_need) box_mark(bv.box_need, bv.sys_of[i], d2, permit2);
   }
   if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0)
     atomicExch(&flags[kFlagNeed], 1);
 }
 
 __global__ void k_set_need(int* flags, int v) { flags[kFlagNeed] = v; }
+
+// A rebuild of every system: the need flag, the full flag and each system's
+// flag of a batch (nsys 0: one box).
+__global__ void k_set_need_all(int* flags, unsigned char* box_need, int nsys) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    flags[kFlagNeed] = 1;
+    flags[kFlagFull] = 1;
+  }
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x)
+    box_need[s] = 1;
+}
 
 // ---------------------------------------------------------------------------
 // Binning.  Cell of the wrapped coordinate with uniform cells of side a_ii/N.
@@ -108,6 +123,7 @@ __global__ void k_bin_count(int n, const float3* __restrict__ crd, Cell cell,
   if (flags[kFlagNeed] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (BATCH && !box_rebuilds(bv.box_need, bv.sys_of, i)) return;
   int c;
   if (BATCH) {
     const SysGeom& g = bv.sys[bv.sys_of[i]];
@@ -135,10 +151,12 @@ __global__ void k_bin_scatter(int n, const int* __restrict__ atom_cell,
                               const int* __restrict__ excl_list,
                               const int* __restrict__ excl_numbers,
                               int* __restrict__ excl_count, int* __restrict__ excl_partner,
-                              const int* flags) {
+                              const int* flags, const unsigned char* __restrict__ box_need,
+                              const int* __restrict__ sys_of) {
   if (flags[kFlagNeed] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (!box_rebuilds(box_need, sys_of, i)) return;
   unsorted[cell_start[atom_cell[i]] + atom_slot[i]] = i;
   if (!excl_count) return;
   const int cnt = excl_numbers[i];
@@ -158,11 +176,14 @@ __global__ void k_bin_scatter(int n, const int* __restrict__ atom_cell,
 __global__ void k_cell_order(int ncell, const int* __restrict__ cell_start,
                              const int* __restrict__ unsorted,
                              int* __restrict__ perm, const int* flags,
-                             const int* __restrict__ key) {
+                             const int* __restrict__ key,
+                             const unsigned char* __restrict__ box_need,
+                             const int* __restrict__ cell_sys) {
   if (flags[kFlagNeed] == 0) return;
   int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   int lane = threadIdx.x & 31;
   if (c >= ncell) return;
+  if (!box_rebuilds(box_need, cell_sys, c)) return;
   int a = cell_start[c], b = cell_start[c + 1];
   for (int k = a + lane; k < b; k += 32) {
     int v = unsorted[k];
@@ -189,10 +210,13 @@ __global__ void k_fill_sorted(int n, const int* __restrict__ perm,
                               const int* __restrict__ atom_local,
                               int* __restrict__ inv_perm, int* __restrict__ global,
                               float4* __restrict__ pos, float3* __restrict__ old_crd,
-                              const int* flags, float3* __restrict__ img_off, Cell cell) {
+                              const int* flags, float3* __restrict__ img_off, Cell cell,
+                              const unsigned char* __restrict__ box_need,
+                              const int* __restrict__ sys_of) {
   if (flags[kFlagNeed] == 0) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
+  if (!box_rebuilds(box_need, sys_of, s)) return;
   int i = perm[s];
   inv_perm[i] = s;
   const int g = atom_local ? atom_local[i] : i;
@@ -268,16 +292,26 @@ __device__ __forceinline__ float cell_gap(int o, float f) {
 // Each run is cut down to the cells whose box is within rl (plus a margin)
 // of atom i.  With at least 5 cells per axis a pair within rl sits at the
 // run's cell offset in its minimum image, so a cut cell holds no hit.
+constexpr int kSearchChunk = 32;
+
 template <bool BATCH>
 __global__ void __launch_bounds__(256)
 k_pair_search(SearchArgs a) {
   if (a.flags[kFlagNeed] == 0) return;
   const int lane = threadIdx.x & 31;
   const int nw = blockDim.x >> 5;
-  // contiguous range of sorted atoms per block: shared neighbour cells in L1
-  const int per_block = (a.n + gridDim.x - 1) / gridDim.x;
-  const int i_end = min(a.n, (int)blockIdx.x * per_block + per_block);
-  for (int i = blockIdx.x * per_block + (threadIdx.x >> 5); i < i_end; i += nw) {
+  // One box: a contiguous range of sorted atoms per block (shared neighbour
+  // cells in L1).  Batch: chunks of kSearchChunk sorted atoms dealt to the
+  // blocks in turn, so that the few boxes of a partial rebuild spread over
+  // every SM.  i grows with t, so the first i past the end ends the loop.
+  const int per_block = BATCH ? kSearchChunk : (a.n + gridDim.x - 1) / gridDim.x;
+  const int stride = BATCH ? (int)gridDim.x * kSearchChunk : 0;
+  for (int t = threadIdx.x >> 5;; t += nw) {
+  const int q = t / per_block, r = t - q * per_block;
+  if (!BATCH && q > 0) break;
+  const int i = (int)blockIdx.x * per_block + q * stride + r;
+  if (i >= a.n) break;
+  if (BATCH && !box_rebuilds(a.bv.box_need, a.bv.sys_of, i)) continue;  // warp-uniform
   const float4 pi4 = a.pos[i];
   const int gi = __float_as_int(pi4.w);
   const int c = a.sorted_cell[i];
@@ -444,8 +478,10 @@ k_pair_search(SearchArgs a) {
     }
   }
   if (lane == 0) {
+    // a partial batch rebuild replaces this row's share of the kept total
+    const int prev = (BATCH && a.flags[kFlagFull] == 0) ? a.row_count[i] : 0;
     a.row_count[i] = count < a.row_cap ? count : a.row_cap;
-    atomicAdd(&a.flags[kFlagTotal], count);
+    atomicAdd(&a.flags[kFlagTotal], count - prev);
     if (count > a.row_cap) {
       a.flags[kFlagListOverflow] = 1;
       atomicMax(&a.flags[kFlagMaxRow], count);
@@ -742,9 +778,10 @@ __global__ void __launch_bounds__(256, 2) k_cluster_search(ClusterSearchArgs a) 
   }
 }
 
-__global__ void k_rebuild_begin(int* flags) {
+// batch: a rebuild of only some systems keeps the total of the others
+__global__ void k_rebuild_begin(int* flags, bool batch) {
   if (flags[kFlagNeed] == 0) return;
-  flags[kFlagTotal] = 0;
+  if (!batch || flags[kFlagFull] != 0) flags[kFlagTotal] = 0;
   flags[kFlagMaxRow] = 0;
 }
 
@@ -755,15 +792,28 @@ __global__ void k_row_starts(int n, int row_cap, int* row_start) {
 
 __global__ void k_sorted_cell(int n, const int* __restrict__ perm,
                               const int* __restrict__ atom_cell, int* __restrict__ sc,
-                              const int* flags) {
+                              const int* flags, const unsigned char* __restrict__ box_need,
+                              const int* __restrict__ sys_of) {
   if (flags[kFlagNeed] == 0) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < n) sc[s] = atom_cell[perm[s]];
+  if (s < n && box_rebuilds(box_need, sys_of, s)) sc[s] = atom_cell[perm[s]];
+}
+
+// Zeroes the cell counts of the systems that rebuild (all cells for one
+// box): the others keep the counts of their last build, so the scan gives
+// their cells the same starts again.
+__global__ void k_zero_cells(int ncell, int* __restrict__ cell_count, const int* flags,
+                             const unsigned char* __restrict__ box_need,
+                             const int* __restrict__ cell_sys) {
+  if (flags[kFlagNeed] == 0) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncell && box_rebuilds(box_need, cell_sys, c)) cell_count[c] = 0;
 }
 
 __global__ void k_finish_build(int* flags) {
   if (flags[kFlagNeed] != 0) flags[kFlagGeneration] += 1;
   flags[kFlagNeed] = 0;
+  flags[kFlagFull] = 0;
 }
 
 // Reads the rebuild flag into the graph's conditional handle (the IF node
@@ -780,15 +830,27 @@ int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_
 
 int nl_check_moved(NeighborList& nl, const float* crd_f, cudaStream_t st) {
   const float permit = nl.skin * nl.skin_permit;
-  k_check_refresh<false><<<ceil_div(nl.n, 256), 256, 0, st>>>(
-      nl.n, reinterpret_cast<const float3*>(crd_f), nl.d_old_crd, nl.cell, nl.rcell,
-      permit * permit, nl.d_flags, nl.bv);
+  if (nl.bv.nsys > 0)
+    k_check_refresh<true><<<ceil_div(nl.n, 256), 256, 0, st>>>(
+        nl.n, reinterpret_cast<const float3*>(crd_f), nl.d_old_crd, nl.cell, nl.rcell,
+        permit * permit, nl.d_flags, nl.bv);
+  else
+    k_check_refresh<false><<<ceil_div(nl.n, 256), 256, 0, st>>>(
+        nl.n, reinterpret_cast<const float3*>(crd_f), nl.d_old_crd, nl.cell, nl.rcell,
+        permit * permit, nl.d_flags, nl.bv);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
 
+// The next rebuild covers every system.
+static void nl_need_all(NeighborList& nl, cudaStream_t st) {
+  const int nsys = (nl.bv.nsys > 0 && nl.bv.box_need) ? nl.bv.nsys : 0;
+  k_set_need_all<<<std::max(1, std::min(ceil_div(nsys, 256), 64)), 256, 0, st>>>(
+      nl.d_flags, nl.bv.box_need, nsys);
+}
+
 int nl_force_next(NeighborList& nl, cudaStream_t st) {
-  k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 1);
+  nl_need_all(nl, st);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -1353,7 +1415,7 @@ int nl_decide(NeighborList& nl, const float* crd_f, int step, int forced,
   if (nl.generation == 0) forced = 1;  // nothing built yet
   nl.generation += 1;
   if (forced) {
-    k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 1);
+    nl_need_all(nl, st);
   } else if (nl.refresh_interval <= 0) {
     k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 0);
     float permit = nl.skin * nl.skin_permit;
@@ -1364,7 +1426,10 @@ int nl_decide(NeighborList& nl, const float* crd_f, int step, int forced,
       k_check_refresh<false><<<ceil_div(n, 256), 256, 0, st>>>(
           n, crd, nl.d_old_crd, nl.cell, nl.rcell, permit * permit, nl.d_flags, nl.bv);
   } else {
-    k_set_need<<<1, 1, 0, st>>>(nl.d_flags, (step + 1) % nl.refresh_interval == 0);
+    if ((step + 1) % nl.refresh_interval == 0)
+      nl_need_all(nl, st);
+    else
+      k_set_need<<<1, 1, 0, st>>>(nl.d_flags, 0);
   }
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
@@ -1379,8 +1444,15 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   const int n = nl.n;
   // Excluded-partner sets need global ids equal to the caller's indices.
   int* excl_count = (excl_numbers && !atom_local) ? nl.d_excl_count : nullptr;
-  SNB_CUDA_TRY(cudaMemsetAsync(nl.d_cell_count, 0, sizeof(int) * nl.ncell, st));
-  k_rebuild_begin<<<1, 1, 0, st>>>(nl.d_flags);
+  const unsigned char* need = nl.bv.nsys > 0 ? nl.bv.box_need : nullptr;
+  const int* sys_of = nl.bv.nsys > 0 ? nl.bv.sys_of : nullptr;
+  const int* cell_sys = nl.bv.nsys > 0 ? nl.bv.cell_sys : nullptr;
+  if (need)
+    k_zero_cells<<<ceil_div(nl.ncell, 256), 256, 0, st>>>(nl.ncell, nl.d_cell_count,
+                                                          nl.d_flags, need, cell_sys);
+  else
+    SNB_CUDA_TRY(cudaMemsetAsync(nl.d_cell_count, 0, sizeof(int) * nl.ncell, st));
+  k_rebuild_begin<<<1, 1, 0, st>>>(nl.d_flags, need != nullptr);
   const bool clus = nl.clusters;
   if (nl.bv.nsys > 0)
     k_bin_count<true><<<ceil_div(n, 256), 256, 0, st>>>(
@@ -1395,17 +1467,19 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   if (rc) return rc;
   k_bin_scatter<<<ceil_div(n, 256), 256, 0, st>>>(
       n, nl.d_atom_cell, nl.d_atom_slot, nl.d_cell_start, nl.d_unsorted, excl_start,
-      excl_list, excl_numbers, excl_count, nl.d_excl_partner, nl.d_flags);
+      excl_list, excl_numbers, excl_count, nl.d_excl_partner, nl.d_flags, need, sys_of);
   k_cell_order<<<ceil_div(nl.ncell, 8), 256, 0, st>>>(nl.ncell, nl.d_cell_start,
                                                       nl.d_unsorted, nl.d_perm,
                                                       nl.d_flags,
-                                                      clus ? nl.d_atom_key : nullptr);
+                                                      clus ? nl.d_atom_key : nullptr, need,
+                                                      cell_sys);
   k_fill_sorted<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_perm, crd, atom_local,
                                                   nl.d_inv_perm, nl.d_global,
                                                   nl.d_pos, nl.d_old_crd, nl.d_flags,
-                                                  clus ? nl.d_img_off : nullptr, nl.cell);
+                                                  clus ? nl.d_img_off : nullptr, nl.cell,
+                                                  need, sys_of);
   k_sorted_cell<<<ceil_div(n, 256), 256, 0, st>>>(n, nl.d_perm, nl.d_atom_cell,
-                                                  nl.d_sorted_cell, nl.d_flags);
+                                                  nl.d_sorted_cell, nl.d_flags, need, sys_of);
   static int sms = 0;
   if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
   if (clus) {
@@ -1496,6 +1570,8 @@ int nl_rebuild(NeighborList& nl, const float* crd_f, const int* atom_local,
   else
     k_pair_search<false><<<blocks, 256, 0, st>>>(sa);
   k_finish_build<<<1, 1, 0, st>>>(nl.d_flags);
+  if (need)  // the systems' flags for the next decision
+    SNB_CUDA_TRY(cudaMemsetAsync(nl.bv.box_need, 0, nl.bv.nsys, st));
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }

@@ -176,9 +176,10 @@ def test_native_inputs_reject_malformed_files(files, tmp_path):
     bad2.write_text("\n".join([f"{hdr[0]} {int(hdr[1]) + 1}"] + rows[1:]))
     m = ctypes.c_int(0)
     st = np.zeros(int(hdr[0]), np.int32)
+    num = np.zeros(int(hdr[0]), np.int32)  # held by name: the reader writes into it
     lst = np.zeros(int(hdr[1]) + 1, np.int32)
     rc = lib.snb_read_exclude_in_file(str(bad2).encode(), ctypes.byref(n), ctypes.byref(m),
-                                      st.ctypes.data, st.copy().ctypes.data, lst.ctypes.data)
+                                      st.ctypes.data, num.ctypes.data, lst.ctypes.data)
     assert rc == capi.SNB_ERR_BAD_INPUT
     assert b"excluded_atom_numbers is not right" in lib.snb_last_error()
     rc = lib.snb_read_charge_in_file(str(tmp_path / "missing.txt").encode(),

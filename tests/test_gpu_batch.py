@@ -79,9 +79,39 @@ def test_batch_forces_match_fp64_and_single_box(g, oracle, boxes):
     assert abs(tb[7] - sum(en_sum.values())) <= 1e-6 * sum(abs(v) for v in en_sum.values())
 
 
+def _export_pairs(g, h):
+    """The engine's pair set as sorted (lo, hi) rows, and its kept total."""
+    import torch
+    lib = g.capi.load()
+    cnt = ctypes.c_longlong(0)
+    g.capi.check(lib.snb_engine_stats(h, None, ctypes.byref(cnt), g.stream()), "stats")
+    n = cnt.value
+    pi = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    pj = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    got = ctypes.c_longlong(0)
+    g.capi.check(lib.snb_engine_export_pairs(h, g.ptr(pi), g.ptr(pj), n, ctypes.byref(got),
+                                             g.stream()), "engine_export_pairs")
+    p = np.stack([pi[:got.value].cpu().numpy(), pj[:got.value].cpu().numpy()], 1)
+    return p.astype(np.int64), n, got.value
+
+
+def _pairs_within(crd, box, cutoff, base, excluded):
+    """(lo, hi) global ids of one box's pairs closer than cutoff (minimum
+    image), excluded pairs left out."""
+    d = crd[:, None, :] - crd[None, :, :]
+    d -= box * np.round(d / box)
+    r2 = (d * d).sum(-1)
+    i, j = np.nonzero(np.triu(r2 < cutoff * cutoff, 1))
+    keep = [(a, b) not in excluded for a, b in zip(i + base, j + base)]
+    return np.stack([i + base, j + base], 1)[np.array(keep, bool)]
+
+
 def test_batch_md_matches_single_boxes(g, boxes):
     """100 graph-replayed NVE steps of the batch stay with single-box runs of
-    the same boxes (both fixed-point; coordinates agree to 1e-3 A)."""
+    the same boxes (both fixed-point; coordinates agree to 1e-3 A).  Each box
+    rebuilds its own list when its own atoms moved past the skin allowance;
+    after the steps every box's list still holds every pair within the
+    cutoff, and the kept pair total equals the exported list's size."""
     import torch
     from sponge_b200 import systems
     lib = g.capi.load()
@@ -106,8 +136,23 @@ def test_batch_md_matches_single_boxes(g, boxes):
                          "batch md")
         st.synchronize()
         cb = crd.cpu().numpy().reshape(-1, 3)
+        listed, total, exported = _export_pairs(g, h)
     finally:
         lib.snb_engine_destroy(h)
+    assert total == exported
+    excluded = set()
+    for a in range(len(c["excl_numbers"])):
+        for k in range(c["excl_numbers"][a]):
+            b = int(c["excl_list"][c["excl_start"][a] + k])
+            excluded.add((min(a, b), max(a, b)))
+    listed = set(map(tuple, listed.tolist()))
+    base = 0
+    for s in boxes:
+        need = _pairs_within(cb[base:base + s.n].astype(np.float64), float(s.box), CUTOFF,
+                             base, excluded)
+        missing = [p for p in map(tuple, need.tolist()) if p not in listed]
+        assert not missing, f"box at atom {base}: {len(missing)} pairs within the cutoff unlisted"
+        base += s.n
     base = 0
     for s in boxes:
         hs = g.engine_create(s, CUTOFF)
