@@ -968,6 +968,8 @@ def run_ours(args):
     st.synchronize()
     r0 = ctypes.c_longlong(0)
     capi.check(lib.snb_engine_stats(h, ctypes.byref(r0), None, sp), "stats")
+    pp0, pp1 = ctypes.c_int(0), ctypes.c_int(0)
+    capi.check(lib.snb_engine_prune_passes(h, ctypes.byref(pp0), None, sp), "prune passes")
     # state at the start of the timed region: the reference's GPU path
     # starts from it too (plain_gpu below)
     start_state = (crd.clone(), vel.clone())
@@ -998,7 +1000,9 @@ def run_ours(args):
 
     r1 = ctypes.c_longlong(0)
     capi.check(lib.snb_engine_stats(h, ctypes.byref(r1), None, sp), "stats")
+    capi.check(lib.snb_engine_prune_passes(h, ctypes.byref(pp1), None, sp), "prune passes")
     timed_rebuilds = int(r1.value - r0.value)
+    timed_prunes = int(pp1.value - pp0.value)
     # graph composition: our kernels per step
     kn, libk, bodyk = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
     if not args.no_graph:  # with --no-graph no step graph exists to count
@@ -1009,10 +1013,14 @@ def run_ours(args):
 
     # per-phase timing (stream launches, events between phases)
     phases = np.zeros(7)
+    pq0, pq1, kept = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_longlong(0)
+    capi.check(lib.snb_engine_prune_passes(h, ctypes.byref(pq0), None, sp), "prune passes")
     with torch.cuda.stream(st):
         capi.check(lib.snb_engine_profile_steps(h, P(crd), P(vel), P(invm), ctypes.c_float(dt),
                                                 EQ + W + K, args.profile_steps,
                                                 phases.ctypes.data, sp), "profile")
+    capi.check(lib.snb_engine_prune_passes(h, ctypes.byref(pq1), ctypes.byref(kept), sp),
+               "prune passes")
     rebuilds, pairs = ctypes.c_longlong(0), ctypes.c_longlong(0)
     capi.check(lib.snb_engine_stats(h, ctypes.byref(rebuilds), ctypes.byref(pairs), sp), "stats")
 
@@ -1109,10 +1117,19 @@ def run_ours(args):
         if "ns_per_day" in plain:
             plain["speedup_vs_plain"] = plain["this_engine_ns_per_day"] / plain["ns_per_day"]
 
-    # roofline of the dominant kernel (the pair kernel), HBM view
+    # roofline of the dominant kernel (the pair kernel), HBM view.  Per
+    # launch, averaged over the profiled steps: the list entries scanned
+    # (the full rows on a prune pass, the kept entries otherwise), the
+    # positions, forces and row counts, and on a prune pass the kept entries
+    # written with the rows' counts and positions
     pair_ms = float(phases[2])
     listed = int(pairs.value)
-    alg_bytes = 4 * listed + 16 * n + 24 * n + 4 * (n + 1) + 4 * n
+    prof_prunes = int(pq1.value - pq0.value)
+    f_prune = prof_prunes / max(1, args.profile_steps) if kept.value > 0 else 1.0
+    kept_n = int(kept.value) if kept.value > 0 else listed
+    scanned = f_prune * listed + (1.0 - f_prune) * kept_n
+    alg_bytes = (4 * scanned + 16 * n + 24 * n + 4 * (n + 1) + 4 * n
+                 + (f_prune * (4 * kept_n + 20 * n) if kept.value > 0 else 0.0))
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (pair_ms * 1e-3) / 1e9
     traffic = committed_traffic()
@@ -1120,11 +1137,13 @@ def run_ours(args):
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": achieved / peak,
                 "traffic": (traffic["dram_bytes_per_launch"] if traffic else None),
-                "algorithmic_bytes": alg_bytes, "kernel_ms": pair_ms}
+                "algorithmic_bytes": alg_bytes, "kernel_ms": pair_ms,
+                "entries_scanned_per_launch": scanned, "prune_passes_profiled": prof_prunes,
+                "profiled_steps": args.profile_steps}
     # FP32-pipe view: 47 flops per in-cutoff pair (force only) + 10 per other
-    # listed pair; in-cutoff count from the oracle-free density estimate
+    # scanned entry; in-cutoff count from the oracle-free density estimate
     in_cut = listed * (CUTOFF / (CUTOFF + SKIN)) ** 3
-    flops = 47 * in_cut + 10 * (listed - in_cut)
+    flops = 47 * in_cut + 10 * (scanned - in_cut)
     roofline["fp32_tflops"] = flops / (pair_ms * 1e-3) / 1e12
 
     cpu_base = None
@@ -1165,6 +1184,10 @@ def run_ours(args):
         "accumulation": "64-bit fixed point (forces 2^40, energies and virials 2^32)",
         "equilibration_steps": EQ,
         "nl_rebuilds_timed": timed_rebuilds,
+        # pair-kernel passes over the full rows (every rebuild, and whenever
+        # an atom moved half the 0.8 A prune margin); the other steps scan
+        # only the entries kept within cutoff + margin
+        "prune_passes_timed": timed_prunes,
         "forced_rebuild_steps_in_timed_region": forced_steps,
         "value_rebuild_amortised": world * ns_per_day(1e3 / ms_amort),
         "rebuild_amortisation": {"rebuild_cost_ms": rebuild_cost_ms,

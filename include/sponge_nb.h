@@ -500,6 +500,22 @@ int snb_engine_set_list_form(snb_engine* e, int clusters);
  * (and before the first step).  The sites' inverse masses must be 0. */
 int snb_engine_set_virtual_atoms(snb_engine* e, snb_vatom* vatom);
 int snb_engine_list_form(snb_engine* e, int* clusters);
+/* No counterpart in the reference.  Pruned rows for the plain LJ rows of a
+ * single box: a prune pass of the pair kernel scans the full rows (the
+ * entries within cutoff + skin) and keeps those within cutoff + margin; the
+ * steps after it scan only the kept entries, until an atom has moved more
+ * than half the margin since the pass or the list is rebuilt.  A pair
+ * outside cutoff + margin at the pass stays outside the cutoff until then,
+ * so every step sees the same pairs within the cutoff as without pruning
+ * and the forces are the same bit for bit.  snb_engine_create sets a margin
+ * of 0.8 A; margin 0 turns it off.  Force calls outside the MD steps always
+ * scan the full rows.  Not used with the cluster form, the soft-core kernel
+ * or a batch. */
+int snb_engine_set_prune_margin(snb_engine* e, float margin);
+/* Prune passes run so far, and (kept_entries may be null) the entries the
+ * last pass kept in all rows (host sync; 0 while pruning was never on). */
+int snb_engine_prune_passes(snb_engine* e, int* passes, long long* kept_entries,
+                            void* stream);
 /* The engine's current pair set in global ids, lo < hi, in no particular
  * order (as snb_nl_export_pairs; host sync). */
 int snb_engine_export_pairs(snb_engine* e, int* d_pi, int* d_pj, long long cap,

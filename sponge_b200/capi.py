@@ -71,6 +71,7 @@ EXPORTED = [
     "snb_engine_autotune", "snb_engine_set_launch_shapes", "snb_engine_graph_info",
     "snb_engine_stats",
     "snb_engine_spread_wide_tiles", "snb_engine_set_list_form", "snb_engine_list_form",
+    "snb_engine_set_prune_margin", "snb_engine_prune_passes",
     "snb_engine_export_pairs",
     "snb_engine_destroy",
     "snb_bond_create", "snb_bond_force", "snb_bond_energy", "snb_bond_destroy",
@@ -189,6 +190,9 @@ _SIGS = {
     "snb_engine_stats": (_I, [_P, ctypes.POINTER(_LL), ctypes.POINTER(_LL), _P]),
     "snb_engine_spread_wide_tiles": (_I, [_P, ctypes.POINTER(ctypes.c_int), _P]),
     "snb_engine_set_list_form": (_I, [_P, _I]),
+    "snb_engine_set_prune_margin": (_I, [_P, _F]),
+    "snb_engine_prune_passes": (_I, [_P, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_longlong), _P]),
     "snb_bond_create": (_I, [_I, _I, _P, _P, _P, _P, _P]),
     "snb_bond_force": (_I, [_P, _P, snb_boundary, _P, _I, _P, _I, _P, _P]),
     "snb_bond_energy": (_I, [_P, ctypes.POINTER(ctypes.c_float), _P]),

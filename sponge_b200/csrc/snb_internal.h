@@ -101,6 +101,12 @@ __device__ __forceinline__ bool box_rebuilds(const unsigned char* need, const in
   return need == nullptr || need[sys[i]] != 0;
 }
 
+// Device flags of a neighbor list (NeighborList::d_flags).  kFlagFull: the
+// pending rebuild covers every system of a batch (so the pair total restarts
+// from zero instead of being corrected row by row).
+enum { kFlagNeed = 0, kFlagListOverflow = 1, kFlagTotal = 2, kFlagGeneration = 3,
+       kFlagExportOverflow = 4, kFlagMaxRow = 5, kFlagFull = 6, kNumFlags = 8 };
+
 // ----------------------------------------------------------------------------
 // Neighbor list: cell grid of side >= (cutoff+skin)/2 (neighbor_list.cpp:943),
 // atoms counting-sorted by cell (stable: ties by caller index), half list in
@@ -146,6 +152,12 @@ struct NeighborList {
   int* d_row_start = nullptr;   // [n + 1] = i * row_cap
   int* d_cols = nullptr;        // [n * row_cap] sorted-frame j of each pair
   int row_cap = 0;
+  // pruned rows (engine, single box): the entries of each row within
+  // cutoff + prune margin at the last prune pass, in the rows' layout, and
+  // the sorted positions that pass saw (null until nl_enable_prune)
+  int* d_cols_in = nullptr;     // [n * row_cap]
+  int* d_row_in_count = nullptr;  // [n]
+  float4* d_prune_ref = nullptr;  // [n]
   long long cap = 0;
   int* d_unsorted = nullptr;    // [n] cell-binned caller indices before ordering
   int* d_sorted_cell = nullptr;  // [n] cell of each sorted atom
@@ -192,6 +204,8 @@ int nl_init_batch(NeighborList& nl, int n, float cutoff, float skin,
                   std::vector<SysGeom>& sys, int refresh_interval, float skin_permit,
                   int max_neighbor_numbers);
 void nl_free(NeighborList& nl);
+// Allocates the pruned rows (NeighborList::d_cols_in and the rest).
+int nl_enable_prune(NeighborList& nl);
 // Update as NEIGHBOR_LIST::Update (neighbor_list.cpp:974-1025): forced, or
 // conditional on the displacement check / refresh interval.  Device-side
 // decision; no host sync.
@@ -285,9 +299,30 @@ struct PairArgs {
   // 2: only those (SOLVENT_LENNARD_JONES); 0: every pair
   int solvent_mode = 0;
   int solvent_begin = 0;
+  // pruned rows (single box, solvent_mode 0; prune == null: full rows only).
+  // prune[0] != 0: a prune pass scans the full rows and keeps the entries
+  // within sqrt(prune2) in cols_in / row_in_count, with row i's position in
+  // prune_ref[i]; otherwise the scan reads cols_in / row_in_count.
+  const int* prune = nullptr;
+  int* cols_in = nullptr;
+  int* row_in_count = nullptr;
+  float4* prune_ref = nullptr;
+  float prune2 = 0.f;
 };
 int launch_pair(const PairArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool ortho, cudaStream_t st);
+
+// The pruned rows' displacement check of the next step: flag[0] is raised
+// when an atom lies more than sqrt(permit2) from ref[its sorted slot] (the
+// position the last prune pass saw).  ref == null: no check.
+struct PruneCheck {
+  const float4* ref = nullptr;
+  float permit2 = 0.f;
+  int* flag = nullptr;
+};
+// The same check alone, on final coordinates (after constraints or sites).
+int launch_prune_check(int n, const float3* crd, const int* map, const PruneCheck& pc,
+                       const Cell& cell, const Cell& rcell, cudaStream_t st);
 
 // The pair kernel over the cluster form of the list.
 struct ClusterPairArgs {

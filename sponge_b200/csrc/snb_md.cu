@@ -106,13 +106,15 @@ int launch_bonded(int nb, const int* ba, const int* bb, const float* bk,
 // launch then clears the accumulator for the next step.
 // When old_crd is given, also performs the refresh check of the next step
 // (Check_Refresh, neighbor_list.cpp:307-321) on the new coordinates and
-// raises flags[0] if any atom moved more than sqrt(permit2) since the build.
+// raises flags[0] if any atom moved more than sqrt(permit2) since the build;
+// with pc.ref, the pruned rows' check likewise.
 template <bool BATCH>
 __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc,
                             float3* __restrict__ crd, float3* __restrict__ vel,
                             const float* __restrict__ inv_mass, float dt,
                             const float3* __restrict__ old_crd, Cell cell, Cell rcell,
-                            float permit2, int* __restrict__ flags, BatchView bv) {
+                            float permit2, int* __restrict__ flags, BatchView bv,
+                            PruneCheck pc) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   // every load is issued before the first store: the force reads wait on the
@@ -149,20 +151,46 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
     if (BATCH && bv.box_need) box_mark(bv.box_need, bv.sys_of[i], d2, permit2);
     if (__any_sync(__activemask(), moved) && moved) atomicExch(&flags[0], 1);
   }
+  if (!BATCH && pc.ref) {
+    const float4 q = pc.ref[s];
+    const float3 d = min_image_fast<false>(r, make_float3(q.x, q.y, q.z), cell, rcell);
+    const bool far = d.x * d.x + d.y * d.y + d.z * d.z > pc.permit2;
+    if (__any_sync(__activemask(), far) && far) atomicExch(pc.flag, 1);
+  }
+}
+
+__global__ void k_prune_check(int n, const float3* __restrict__ crd,
+                              const int* __restrict__ map, PruneCheck pc, Cell cell,
+                              Cell rcell) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 q = pc.ref[map[i]];
+  const float3 d = min_image_fast<false>(crd[i], make_float3(q.x, q.y, q.z), cell, rcell);
+  const bool far = d.x * d.x + d.y * d.y + d.z * d.z > pc.permit2;
+  if (__any_sync(__activemask(), far) && far) atomicExch(pc.flag, 1);
+}
+
+int launch_prune_check(int n, const float3* crd, const int* map, const PruneCheck& pc,
+                       const Cell& cell, const Cell& rcell, cudaStream_t st) {
+  if (!pc.ref) return kOk;
+  k_prune_check<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, map, pc, cell, rcell);
+  SNB_CUDA_TRY(cudaGetLastError());
+  return kOk;
 }
 
 int launch_leap_frog(int n, const int* map, Accumulators& acc, float3* crd,
                      float3* vel, const float* inv_mass, float dt,
                      const float3* old_crd, const Cell& cell, const Cell& rcell,
-                     float permit2, int* flags, cudaStream_t st, const BatchView& bv) {
+                     float permit2, int* flags, cudaStream_t st, const BatchView& bv,
+                     const PruneCheck& pc) {
   if (bv.nsys > 0)
     k_leap_frog<true><<<ceil_div(n, 256), 256, 0, st>>>(n, map, acc, crd, vel, inv_mass, dt,
                                                       old_crd, cell, rcell, permit2, flags,
-                                                      bv);
+                                                      bv, PruneCheck());
   else
     k_leap_frog<false><<<ceil_div(n, 256), 256, 0, st>>>(n, map, acc, crd, vel, inv_mass,
                                                        dt, old_crd, cell, rcell, permit2,
-                                                       flags, bv);
+                                                       flags, bv, pc);
   SNB_CUDA_TRY(cudaGetLastError());
   // the accumulator starts the next step at zero: one coalesced clear
   // instead of scattered stores through the permutation

@@ -27,12 +27,6 @@
 
 namespace snb {
 
-// flags layout
-// kFlagFull: the pending rebuild covers every system of a batch (so the
-// pair total restarts from zero instead of being corrected row by row)
-enum { kFlagNeed = 0, kFlagListOverflow = 1, kFlagTotal = 2, kFlagGeneration = 3,
-       kFlagExportOverflow = 4, kFlagMaxRow = 5, kFlagFull = 6, kNumFlags = 8 };
-
 // ---------------------------------------------------------------------------
 // Refresh decision (Check_Refresh, neighbor_list.cpp:307-321): any atom moved
 // more than skin*skin_permit since the last build.
@@ -1264,8 +1258,22 @@ int nl_set_clusters(NeighborList& nl, bool on) {
   return kOk;
 }
 
+// The pruned rows' storage (rows' layout; contents written by the pair
+// kernel's prune passes).
+int nl_enable_prune(NeighborList& nl) {
+  if (nl.d_cols_in) return kOk;
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_cols_in, sizeof(int) * nl.cap));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_row_in_count, sizeof(int) * nl.n));
+  SNB_CUDA_TRY(cudaMalloc(&nl.d_prune_ref, sizeof(float4) * nl.n));
+  SNB_CUDA_TRY(cudaMemset(nl.d_row_in_count, 0, sizeof(int) * nl.n));
+  return kOk;
+}
+
 void nl_free(NeighborList& nl) {
   clusters_free(nl);
+  cudaFree(nl.d_cols_in);
+  cudaFree(nl.d_row_in_count);
+  cudaFree(nl.d_prune_ref);
   cudaFree(nl.d_unsorted);
   cudaFree(nl.d_sorted_cell);
   cudaFree(nl.d_run_ranges);
@@ -1607,6 +1615,11 @@ int nl_check_overflow(NeighborList& nl, bool* regrown, cudaStream_t st) {
     if (nl.cap + nl.row_cap > 2147483647LL)
       return fail(kOverflow, "neighbor list: rows exceed 32-bit offsets");
     SNB_CUDA_TRY(cudaMalloc(&nl.d_cols, sizeof(int) * nl.cap));
+    if (nl.d_cols_in) {  // the pruned rows follow the rows' capacity
+      SNB_CUDA_TRY(cudaFree(nl.d_cols_in));
+      nl.d_cols_in = nullptr;
+      SNB_CUDA_TRY(cudaMalloc(&nl.d_cols_in, sizeof(int) * nl.cap));
+    }
     k_row_starts<<<ceil_div(nl.n + 1, 256), 256, 0, st>>>(nl.n, nl.row_cap, nl.d_row_start);
     int zero = 0;
     SNB_CUDA_TRY(cudaMemcpyAsync(nl.d_flags + kFlagListOverflow, &zero, sizeof(int),

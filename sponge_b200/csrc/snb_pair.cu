@@ -192,6 +192,13 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   float4* se = stash_e + (STASH ? w * kCap : 0);
   int2* sjt = stash_jt + (STASH ? w * kCap : 0);
   if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
+  // Pruned rows: a prune pass scans the full rows and keeps the candidates
+  // within cutoff + margin; the steps between scan only those.
+  constexpr bool kPrunable = !BATCH && SOLV == 0;
+  const bool prune_pass = kPrunable && a.prune != nullptr && a.prune[0] != 0;
+  const bool use_inner = kPrunable && a.prune != nullptr && !prune_pass;
+  const int* __restrict__ cols = use_inner ? a.cols_in : a.cols;
+  const int* __restrict__ rcount = use_inner ? a.row_in_count : a.row_count;
   // Each block owns a contiguous range of sorted atoms, so the neighbours its
   // warps gather overlap and stay in this SM's L1.
   const int per_block = (a.n + gridDim.x - 1) / gridDim.x;
@@ -211,7 +218,8 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   float fx = 0.f, fy = 0.f, fz = 0.f;
   float e_lj = 0.f, e_c = 0.f;
   float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  const int k0 = a.row_start[i], k1 = k0 + a.row_count[i];
+  const int k0 = a.row_start[i], k1 = k0 + rcount[i];
+  int kept = 0;  // prune pass: entries kept so far
   // a type without LJ against every type (water H): Coulomb-only row
   bool coul_only = true;
   for (int t = lane; t < a.n_types; t += 32) {
@@ -224,9 +232,9 @@ k_lj_direct(PairArgs a, Accumulators acc) {
     // (row starts are multiples of 8 entries, so 16-byte aligned)
     const int inext = i + WARPS;
     if (lane == 0 && inext < i_end) {
-      const int cn = a.row_count[inext];
+      const int cn = rcount[inext];
       if (cn > 0)
-        prefetch_l2(a.cols + a.row_start[inext], (unsigned)(cn * 4 + 15) & ~15u);
+        prefetch_l2(cols + a.row_start[inext], (unsigned)(cn * 4 + 15) & ~15u);
     }
   }
   // hits of the row taken in earlier rounds: lane l takes the row's hits
@@ -242,7 +250,7 @@ k_lj_direct(PairArgs a, Accumulators acc) {
 #pragma unroll
   for (int u = 0; u < kScanU; ++u) {
     const int k = k0 + 32 * u + lane;
-    jn[u] = kAhead && k < k1 ? __ldcs(a.cols + k) : -1;
+    jn[u] = kAhead && k < k1 ? __ldcs(cols + k) : -1;
   }
   for (int base = k0; base < k1;) {
     // phase 1: candidates -> hit list
@@ -254,10 +262,10 @@ k_lj_direct(PairArgs a, Accumulators acc) {
         if (kAhead) {
           jj[u] = jn[u];
           const int k = base + 32 * (kScanU + u) + lane;
-          jn[u] = k < k1 ? __ldcs(a.cols + k) : -1;
+          jn[u] = k < k1 ? __ldcs(cols + k) : -1;
         } else {
           const int k = base + 32 * u + lane;
-          jj[u] = k < k1 ? __ldcs(a.cols + k) : -1;
+          jj[u] = k < k1 ? __ldcs(cols + k) : -1;
         }
       }
       float4 pp[kScanU];
@@ -269,15 +277,22 @@ k_lj_direct(PairArgs a, Accumulators acc) {
       }
 #pragma unroll
       for (int u = 0; u < kScanU; ++u) {
-        bool in = false;
+        bool in = false, keep = false;
         if (jj[u] >= 0) {
           const float3 dr = min_image_fast<ORTHO>(make_float3(pp[u].x, pp[u].y, pp[u].z),
                                                   ri, cell, rcell);
-          in = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z < a.cutoff2;
+          const float d2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+          in = d2 < a.cutoff2;
+          keep = kPrunable && d2 < a.prune2;
           if (SOLV && in) {
             const bool both = i_solvent && a.global[jj[u]] >= a.solvent_begin;
             in = SOLV == 1 ? !both : both;
           }
+        }
+        if (kPrunable && prune_pass) {  // warp-uniform
+          const unsigned mk = __ballot_sync(0xffffffffu, keep);
+          if (keep) a.cols_in[k0 + kept + __popc(mk & lt)] = jj[u];
+          kept += __popc(mk);
         }
         const unsigned m = __ballot_sync(0xffffffffu, in);
         if (in) {
@@ -333,6 +348,10 @@ k_lj_direct(PairArgs a, Accumulators acc) {
     }
     done += count;
     __syncwarp();
+  }
+  if (kPrunable && prune_pass && lane == 0) {
+    a.row_in_count[i] = kept;
+    a.prune_ref[i] = pi;
   }
   fx = warp_sum(fx);
   fy = warp_sum(fy);
