@@ -206,8 +206,7 @@ __global__ void k_prune_decide(int* prune, const int* nl_flags) {
 constexpr float kDefaultPruneMargin = 0.8f;  // A
 
 static bool engine_prunes(const snb_engine* e) {
-  return e->prune_margin > 0.f && e->d_prune && e->bv.nsys == 0 && !e->soft &&
-         !e->nl.clusters;
+  return e->prune_margin > 0.f && e->d_prune && !e->soft && !e->nl.clusters;
 }
 
 // The check that follows an update: displacements above half the margin
@@ -1226,6 +1225,7 @@ extern "C" int snb_batch_create(const snb_options* opt, int n_systems,
     rc = engine_finish_create(e, n, n_types, h_type, h_A, h_B, h_charge, h_es, h_en, h_el,
                               n_excl);
   }
+  if (!rc) rc = snb_engine_set_prune_margin(e, kDefaultPruneMargin);
   if (rc) {
     snb_engine_destroy(e);
     return rc;
@@ -1865,7 +1865,7 @@ static int engine_md_step(snb_engine* e, float* crd, float* vel, const float* in
     if (rc) return rc;
   }
   if (late && (rc = launch_prune_check(e->n, reinterpret_cast<const float3*>(crd),
-                                       e->nl.d_inv_perm, pc, e->cell, e->rcell, st)))
+                                       e->nl.d_inv_perm, pc, e->cell, e->rcell, st, e->bv)))
     return rc;
   prof_mark(e, 7, st);
   return rc;

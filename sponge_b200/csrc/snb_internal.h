@@ -299,7 +299,7 @@ struct PairArgs {
   // 2: only those (SOLVENT_LENNARD_JONES); 0: every pair
   int solvent_mode = 0;
   int solvent_begin = 0;
-  // pruned rows (single box, solvent_mode 0; prune == null: full rows only).
+  // pruned rows (solvent_mode 0; prune == null: full rows only).
   // prune[0] != 0: a prune pass scans the full rows and keeps the entries
   // within sqrt(prune2) in cols_in / row_in_count, with row i's position in
   // prune_ref[i]; otherwise the scan reads cols_in / row_in_count.
@@ -322,7 +322,8 @@ struct PruneCheck {
 };
 // The same check alone, on final coordinates (after constraints or sites).
 int launch_prune_check(int n, const float3* crd, const int* map, const PruneCheck& pc,
-                       const Cell& cell, const Cell& rcell, cudaStream_t st);
+                       const Cell& cell, const Cell& rcell, cudaStream_t st,
+                       const BatchView& bv);
 
 // The pair kernel over the cluster form of the list.
 struct ClusterPairArgs {

@@ -139,19 +139,19 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
   r.y += dt * v.y;
   r.z += dt * v.z;
   crd[i] = r;
+  if (BATCH && (old_crd || pc.ref)) {  // the atom's own box
+    const SysGeom& sg = bv.sys[bv.sys_of[i]];
+    cell = sg.cell;
+    rcell = sg.rcell;
+  }
   if (old_crd) {
-    if (BATCH) {
-      const SysGeom& sg = bv.sys[bv.sys_of[i]];
-      cell = sg.cell;
-      rcell = sg.rcell;
-    }
     float3 d = min_image_fast<false>(r, r_old, cell, rcell);
     const float d2 = d.x * d.x + d.y * d.y + d.z * d.z;
     bool moved = d2 > permit2;
     if (BATCH && bv.box_need) box_mark(bv.box_need, bv.sys_of[i], d2, permit2);
     if (__any_sync(__activemask(), moved) && moved) atomicExch(&flags[0], 1);
   }
-  if (!BATCH && pc.ref) {
+  if (pc.ref) {
     const float4 q = pc.ref[s];
     const float3 d = min_image_fast<false>(r, make_float3(q.x, q.y, q.z), cell, rcell);
     const bool far = d.x * d.x + d.y * d.y + d.z * d.z > pc.permit2;
@@ -159,11 +159,17 @@ __global__ void k_leap_frog(int n, const int* __restrict__ map, Accumulators acc
   }
 }
 
+template <bool BATCH>
 __global__ void k_prune_check(int n, const float3* __restrict__ crd,
                               const int* __restrict__ map, PruneCheck pc, Cell cell,
-                              Cell rcell) {
+                              Cell rcell, BatchView bv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (BATCH) {
+    const SysGeom& sg = bv.sys[bv.sys_of[i]];
+    cell = sg.cell;
+    rcell = sg.rcell;
+  }
   const float4 q = pc.ref[map[i]];
   const float3 d = min_image_fast<false>(crd[i], make_float3(q.x, q.y, q.z), cell, rcell);
   const bool far = d.x * d.x + d.y * d.y + d.z * d.z > pc.permit2;
@@ -171,9 +177,13 @@ __global__ void k_prune_check(int n, const float3* __restrict__ crd,
 }
 
 int launch_prune_check(int n, const float3* crd, const int* map, const PruneCheck& pc,
-                       const Cell& cell, const Cell& rcell, cudaStream_t st) {
+                       const Cell& cell, const Cell& rcell, cudaStream_t st,
+                       const BatchView& bv) {
   if (!pc.ref) return kOk;
-  k_prune_check<<<ceil_div(n, 256), 256, 0, st>>>(n, crd, map, pc, cell, rcell);
+  if (bv.nsys > 0)
+    k_prune_check<true><<<ceil_div(n, 256), 256, 0, st>>>(n, crd, map, pc, cell, rcell, bv);
+  else
+    k_prune_check<false><<<ceil_div(n, 256), 256, 0, st>>>(n, crd, map, pc, cell, rcell, bv);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -186,7 +196,7 @@ int launch_leap_frog(int n, const int* map, Accumulators& acc, float3* crd,
   if (bv.nsys > 0)
     k_leap_frog<true><<<ceil_div(n, 256), 256, 0, st>>>(n, map, acc, crd, vel, inv_mass, dt,
                                                       old_crd, cell, rcell, permit2, flags,
-                                                      bv, PruneCheck());
+                                                      bv, pc);
   else
     k_leap_frog<false><<<ceil_div(n, 256), 256, 0, st>>>(n, map, acc, crd, vel, inv_mass,
                                                        dt, old_crd, cell, rcell, permit2,

@@ -194,7 +194,7 @@ k_lj_direct(PairArgs a, Accumulators acc) {
   if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
   // Pruned rows: a prune pass scans the full rows and keeps the candidates
   // within cutoff + margin; the steps between scan only those.
-  constexpr bool kPrunable = !BATCH && SOLV == 0;
+  constexpr bool kPrunable = SOLV == 0;
   const bool prune_pass = kPrunable && a.prune != nullptr && a.prune[0] != 0;
   const bool use_inner = kPrunable && a.prune != nullptr && !prune_pass;
   const int* __restrict__ cols = use_inner ? a.cols_in : a.cols;

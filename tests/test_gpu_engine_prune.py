@@ -141,3 +141,40 @@ def test_prune_margin_refuses_bad_values(g, box_9k):
         assert lib.snb_engine_set_prune_margin(e, ctypes.c_float(0.0)) == g.capi.SNB_OK
     finally:
         lib.snb_engine_destroy(e)
+
+
+def test_pruned_batch_md_is_bitwise_unchanged(g):
+    """A batch of five boxes, 120 graph-replayed steps: pruned rows (per-box
+    minimum images in the check) against full rows."""
+    import torch
+    from sponge_b200 import systems
+    boxes = [systems.water_box(nw, seed=s, ion_pairs=None)
+             for s, nw in enumerate([200, 450, 700, 260, 520])]
+    offs = np.cumsum([0] + [b.n for b in boxes])[:-1]
+    lib = g.capi.load()
+    dt = 0.5e-3 * systems.TIME_CONVERSION
+    out = []
+    for margin in (0.0, 0.8):
+        h, c = g.batch_create(boxes, 8.0)
+        try:
+            bonded = type("B", (), {})()
+            bonded.bonds = np.concatenate([b.bonds + o for b, o in zip(boxes, offs)]).astype(np.int32)
+            bonded.angles = np.concatenate([b.angles + o for b, o in zip(boxes, offs)]).astype(np.int32)
+            g.engine_set_water_bonded(h, bonded)
+            g.capi.check(lib.snb_engine_set_prune_margin(h, ctypes.c_float(margin)), "margin")
+            crd, vel = g.dev(c["crd"]), g.dev(c["vel"])
+            invm = g.dev((1.0 / c["mass"]).astype(np.float32))
+            st = torch.cuda.Stream()
+            sp = ctypes.c_void_p(st.cuda_stream)
+            with torch.cuda.stream(st):
+                g.capi.check(lib.snb_engine_md_steps_graph(h, g.ptr(crd), g.ptr(vel), g.ptr(invm),
+                                                           ctypes.c_float(dt), 0, 120, sp), "md")
+            st.synchronize()
+            passes = ctypes.c_int(0)
+            g.capi.check(lib.snb_engine_prune_passes(h, ctypes.byref(passes), None, sp), "passes")
+        finally:
+            lib.snb_engine_destroy(h)
+        out.append((crd.cpu().numpy(), vel.cpu().numpy(), passes.value))
+    assert out[0][2] == 0 and out[1][2] >= 2
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
