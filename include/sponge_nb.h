@@ -510,7 +510,7 @@ int snb_engine_list_form(snb_engine* e, int* clusters);
  * and the forces are the same bit for bit.  snb_engine_create and
  * snb_batch_create set a margin of 0.8 A; margin 0 turns it off.  Force
  * calls outside the MD steps always scan the full rows.  Not used with the
- * cluster form or the soft-core kernel. */
+ * cluster form. */
 int snb_engine_set_prune_margin(snb_engine* e, float margin);
 /* Prune passes run so far, and (kept_entries may be null) the entries the
  * last pass kept in all rows (host sync; 0 while pruning was never on). */

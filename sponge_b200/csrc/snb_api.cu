@@ -206,7 +206,7 @@ __global__ void k_prune_decide(int* prune, const int* nl_flags) {
 constexpr float kDefaultPruneMargin = 0.8f;  // A
 
 static bool engine_prunes(const snb_engine* e) {
-  return e->prune_margin > 0.f && e->d_prune && !e->soft && !e->nl.clusters;
+  return e->prune_margin > 0.f && e->d_prune && !(e->nl.clusters && !e->soft);
 }
 
 // The check that follows an update: displacements above half the margin
@@ -1411,6 +1411,11 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
     sa.p = e->soft->p;
     sa.sigma6 = e->soft->sigma6;
     sa.sigma6_min = e->soft->sigma6_min;
+    sa.prune = a.prune;
+    sa.cols_in = a.cols_in;
+    sa.row_in_count = a.row_in_count;
+    sa.prune_ref = a.prune_ref;
+    sa.prune2 = a.prune2;
     rc = launch_soft_rows(sa, e->acc, energy, virial, st);
   } else if (clus) {
     ClusterPairArgs ca;

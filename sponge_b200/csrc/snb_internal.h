@@ -422,6 +422,12 @@ struct SoftArgs {
   float beta;
   float lambda, alpha, p;
   float sigma6, sigma6_min;
+  // pruned rows of the engine's row kernel, as PairArgs::prune
+  const int* prune = nullptr;
+  int* cols_in = nullptr;
+  int* row_in_count = nullptr;
+  float4* prune_ref = nullptr;
+  float prune2 = 0.f;
 };
 int launch_soft(const SoftArgs& a, Accumulators& acc, int accum, bool energy,
                 bool virial, bool dudl, long long* dudl_total, cudaStream_t st);

@@ -959,6 +959,11 @@ k_lj_soft_rows(SoftArgs a, Accumulators acc) {
   const int w = threadIdx.x >> 5;
   int* hits = hits_all[w];
   if (a.nl_flags && a.nl_flags[1]) return;  // list overflowed: rows not written
+  // pruned rows, as in k_lj_direct
+  const bool prune_pass = a.prune != nullptr && a.prune[0] != 0;
+  const bool use_inner = a.prune != nullptr && !prune_pass;
+  const int* __restrict__ cols = use_inner ? a.cols_in : a.cols;
+  const int* __restrict__ rcount = use_inner ? a.row_in_count : a.row_count;
   const float alp_A = a.alpha * powf(a.lambda, a.p);
   const float alp_B = a.alpha * powf(1.0f - a.lambda, a.p);
   const int per_block = (a.n + gridDim.x - 1) / gridDim.x;
@@ -978,7 +983,8 @@ k_lj_soft_rows(SoftArgs a, Accumulators acc) {
     float fx = 0.f, fy = 0.f, fz = 0.f;
     float e_lj = 0.f, e_c = 0.f;
     float vir[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    const int k0 = a.row_start[i], k1 = k0 + a.row_count[i];
+    const int k0 = a.row_start[i], k1 = k0 + rcount[i];
+    int kept = 0;  // prune pass: entries kept so far
     for (int base = k0; base < k1;) {
       int count = 0;
       for (; base < k1 && count <= kHitCap - 32 * kScanU; base += 32 * kScanU) {
@@ -986,7 +992,7 @@ k_lj_soft_rows(SoftArgs a, Accumulators acc) {
 #pragma unroll
         for (int u = 0; u < kScanU; ++u) {
           const int k = base + 32 * u + lane;
-          jj[u] = k < k1 ? a.cols[k] : -1;
+          jj[u] = k < k1 ? cols[k] : -1;
         }
         float4 pp[kScanU];
 #pragma unroll
@@ -994,11 +1000,18 @@ k_lj_soft_rows(SoftArgs a, Accumulators acc) {
           if (jj[u] >= 0) pp[u] = a.pos[jj[u]];
 #pragma unroll
         for (int u = 0; u < kScanU; ++u) {
-          bool in = false;
+          bool in = false, keep = false;
           if (jj[u] >= 0) {
             const float3 dr = min_image_fast<true>(make_float3(pp[u].x, pp[u].y, pp[u].z),
                                                    ri, a.cell, a.rcell);
-            in = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z < a.cutoff2;
+            const float d2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+            in = d2 < a.cutoff2;
+            keep = d2 < a.prune2;
+          }
+          if (prune_pass) {  // warp-uniform
+            const unsigned mk = __ballot_sync(0xffffffffu, keep);
+            if (keep) a.cols_in[k0 + kept + __popc(mk & lt)] = jj[u];
+            kept += __popc(mk);
           }
           const unsigned m = __ballot_sync(0xffffffffu, in);
           if (in) hits[count + __popc(m & lt)] = jj[u];
@@ -1058,6 +1071,10 @@ k_lj_soft_rows(SoftArgs a, Accumulators acc) {
         }
       }
       __syncwarp();
+    }
+    if (prune_pass && lane == 0) {
+      a.row_in_count[i] = kept;
+      a.prune_ref[i] = pi;
     }
     fx = warp_sum(fx);
     fy = warp_sum(fy);

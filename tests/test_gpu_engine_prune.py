@@ -178,3 +178,42 @@ def test_pruned_batch_md_is_bitwise_unchanged(g):
     assert out[0][2] == 0 and out[1][2] >= 2
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_pruned_soft_core_md_is_bitwise_unchanged(g):
+    """The engine's soft-core rows at lambda 0.5: 80 graph-replayed steps
+    with pruned rows against full rows."""
+    import torch
+    from sponge_b200 import systems
+    s, sc = systems.soft_core_box(1000, n_solute=32, seed=3)
+    lib = g.capi.load()
+    box = g.Box(s)
+    dt = 0.5e-3 * systems.TIME_CONVERSION
+    params = {"lambda_lj": 0.5, "soft_core_alpha": 0.5, "soft_core_powfer": 1.0,
+              "soft_core_sigma": 3.0, "soft_core_sigma_min": 0.0}
+    out = []
+    for margin in (0.0, 0.3):
+        e = g.engine_create(s, 10.0)
+        g.engine_set_water_bonded(e, s)
+        h = g.soft_create(box, sc, 10.0, params)
+        crd = g.dev(s.crd.reshape(-1), np.float32)
+        vel = g.dev(s.vel.reshape(-1), np.float32)
+        invm = g.dev((1.0 / s.mass).astype(np.float32))
+        st = torch.cuda.Stream()
+        sp = ctypes.c_void_p(st.cuda_stream)
+        passes = ctypes.c_int(0)
+        try:
+            g.capi.check(lib.snb_engine_set_soft_core(e, h), "set_soft_core")
+            g.capi.check(lib.snb_engine_set_prune_margin(e, ctypes.c_float(margin)), "margin")
+            with torch.cuda.stream(st):
+                g.capi.check(lib.snb_engine_md_steps_graph(e, g.ptr(crd), g.ptr(vel), g.ptr(invm),
+                                                           ctypes.c_float(dt), 0, 80, sp), "md")
+            st.synchronize()
+            g.capi.check(lib.snb_engine_prune_passes(e, ctypes.byref(passes), None, sp), "passes")
+        finally:
+            lib.snb_engine_destroy(e)
+            lib.snb_lj_soft_destroy(h)
+        out.append((crd.cpu().numpy(), vel.cpu().numpy(), passes.value))
+    assert out[1][2] >= 2
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
