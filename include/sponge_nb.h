@@ -507,8 +507,9 @@ int snb_engine_list_form(snb_engine* e, int* clusters);
  * than half the margin since the pass or the list is rebuilt.  A pair
  * outside cutoff + margin at the pass stays outside the cutoff until then,
  * so every step sees the same pairs within the cutoff as without pruning
- * and the forces are the same bit for bit.  snb_engine_create and
- * snb_batch_create set a margin of 0.8 A; margin 0 turns it off.  Force
+ * and the forces are the same bit for bit.  snb_engine_create (for boxes of
+ * at least 20,000 atoms) and snb_batch_create set a margin of 0.8 A;
+ * margin 0 turns it off.  Force
  * calls outside the MD steps always scan the full rows.  Not used with the
  * cluster form. */
 int snb_engine_set_prune_margin(snb_engine* e, float margin);

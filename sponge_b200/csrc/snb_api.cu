@@ -204,6 +204,7 @@ __global__ void k_prune_decide(int* prune, const int* nl_flags) {
 }
 
 constexpr float kDefaultPruneMargin = 0.8f;  // A
+constexpr int kPruneMinAtoms = 20000;        // single boxes below: full rows
 
 static bool engine_prunes(const snb_engine* e) {
   return e->prune_margin > 0.f && e->d_prune && !(e->nl.clusters && !e->soft);
@@ -1117,8 +1118,10 @@ extern "C" int snb_engine_create(const snb_options* opt, int n, snb_boundary bou
   // pruned rows at 0.8 A: on the 100k box (cutoff 10 A, skin 2 A) a prune
   // pass every 7-8 steps and the MD step 4 % shorter than with full rows
   // (0.3 A: 269-275 us, 0.5: 271-272, 0.8: 268-271, 1.2: 273-275; off:
-  // 276-285)
-  if (!rc) rc = snb_engine_set_prune_margin(e, kDefaultPruneMargin);
+  // 276-285).  On the 9,000-atom box the extra launch and the passes cost
+  // more than they save (631 against 680 ns/day), so small boxes keep the
+  // full rows.
+  if (!rc && n >= kPruneMinAtoms) rc = snb_engine_set_prune_margin(e, kDefaultPruneMargin);
   if (rc) {
     snb_engine_destroy(e);
     return rc;
