@@ -1250,7 +1250,7 @@ static int capture_conditional_rebuild(snb_engine* e, const float* crd, cudaStre
   if (cs != cudaStreamCaptureStatusActive) return fail(kCudaError, "capture not active");
   cudaGraphConditionalHandle hc;
   SNB_CUDA_TRY(cudaGraphConditionalHandleCreate(&hc, cg, 0, cudaGraphCondAssignDefault));
-  int rc = nl_set_condition(e->nl, hc, st);
+  int rc = nl_set_condition(e->nl, hc, st, engine_prunes(e) ? e->d_prune : nullptr);
   if (rc) return rc;
   SNB_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd));
   cudaGraphNodeParams cp{};
@@ -1377,8 +1377,10 @@ static int engine_forces(snb_engine* e, const float* crd, int step, bool energy,
   a.warps = e->pair_warps;
   a.stash = e->pair_stash;
   if (engine_prunes(e)) {
-    k_prune_decide<<<1, 1, 0, st>>>(e->d_prune, e->nl.d_flags);
-    SNB_CUDA_TRY(cudaGetLastError());
+    if (!in_graph) {  // (in the graph the rebuild condition's kernel decides)
+      k_prune_decide<<<1, 1, 0, st>>>(e->d_prune, e->nl.d_flags);
+      SNB_CUDA_TRY(cudaGetLastError());
+    }
     const float rp = e->opt.cutoff + e->prune_margin;
     a.prune = e->d_prune;
     a.cols_in = e->nl.d_cols_in;

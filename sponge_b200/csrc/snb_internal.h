@@ -216,7 +216,10 @@ int nl_decide(NeighborList& nl, const float* crd, int step, int forced, cudaStre
 int nl_rebuild(NeighborList& nl, const float* crd, const int* atom_local,
                const int* excl_start, const int* excl_list, const int* excl_numbers,
                cudaStream_t st);
-int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st);
+// Sets the graph's rebuild condition from the need flag; with prune (an
+// engine's pruned-row flags) also decides the step's prune pass.
+int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st,
+                     int* prune = nullptr);
 // stress = (virial [6] (may be null) + constraint virial (fixed point, may be
 // null) + sum m v (x) v) * inv_v into out[0..5], pressure in bar into out[6].
 int launch_pressure(int n, const float3* vel, const float* mass, const double* virial,

@@ -812,12 +812,26 @@ __global__ void k_finish_build(int* flags) {
 
 // Reads the rebuild flag into the graph's conditional handle (the IF node
 // that holds the rebuild kernels).
-__global__ void k_set_rebuild_condition(cudaGraphConditionalHandle h, const int* flags) {
-  cudaGraphSetConditional(h, flags[kFlagNeed] != 0 ? 1u : 0u);
+// prune (may be null): the pruned rows' flags of an engine, decided here in
+// the same launch: the step prunes when it rebuilds or when an atom moved
+// past half the prune margin ({pass, moved, generation after this step,
+// passes}).
+__global__ void k_set_rebuild_condition(cudaGraphConditionalHandle h, const int* flags,
+                                        int* prune) {
+  const int need = flags[kFlagNeed] != 0 ? 1 : 0;
+  cudaGraphSetConditional(h, need ? 1u : 0u);
+  if (prune) {
+    const int pass = (prune[1] != 0 || need) ? 1 : 0;
+    prune[0] = pass;
+    prune[1] = 0;
+    prune[2] = flags[kFlagGeneration] + need;  // the rebuild adds one
+    prune[3] += pass;
+  }
 }
 
-int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st) {
-  k_set_rebuild_condition<<<1, 1, 0, st>>>(h, nl.d_flags);
+int nl_set_condition(NeighborList& nl, cudaGraphConditionalHandle h, cudaStream_t st,
+                     int* prune) {
+  k_set_rebuild_condition<<<1, 1, 0, st>>>(h, nl.d_flags, prune);
   SNB_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
