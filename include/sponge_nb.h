@@ -340,8 +340,10 @@ int snb_engine_create(const snb_options* opt, int atom_numbers,
  * exclusion indices are global atom indices that stay inside their system.
  * Every engine call below then acts on all systems at once, each step being
  * one launch per phase over all boxes (one neighbor list, one pair kernel,
- * one PME spread / gather with a grid per box, one batched cuFFT plan per
- * grid size).  Each box gets the single-box defaults: its own cell grid and
+ * one PME spread / gather with a grid per box, and for the convolution the
+ * library's own passes, one launch per pass over all grids, where every
+ * grid axis has 4-64 points (multiples of 4), else one batched cuFFT plan
+ * per grid size).  Each box gets the single-box defaults: its own cell grid and
  * PME grid (by PM_grid_spacing); PME every step, displacement-triggered list
  * updates and fixed-point accumulation are required.  A list update starts
  * when an atom of some box moved more than half the skin since that box's
@@ -452,7 +454,9 @@ int snb_engine_profile_steps(snb_engine* e, float* crd, float* vel,
  * 4, 8 warps is only set by snb_engine_set_launch_shapes) and the PME
  * convolution's FFT (cuFFT, or this library's own
  * mixed-radix passes with the influence function fused between the forward
- * and inverse x transforms; single box, axes of at most 256 points).
+ * and inverse x transforms: for one box, axes of at most 256 points; for a
+ * batch, axes of 4-64 points, multiples of 4, each line transformed in
+ * registers, one launch per pass over all boxes).
  * Results are bitwise
  * the same for every shape but the FFT, whose two choices differ by float
  * rounding in the reciprocal part.  crd / vel are restored; the next step rebuilds the list and

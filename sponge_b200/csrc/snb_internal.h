@@ -474,6 +474,17 @@ struct PME {
   float2* d_tw[3] = {nullptr, nullptr, nullptr};  // exp(-2 pi i k / K) per axis
   double* d_xpartial = nullptr;  // [xblocks][8] sums of the x pass
   int xblocks = 0;
+  // a batch's own passes (snb_fft_reg.cuh): jobs {box, first, count} of the
+  // z passes (row pairs), y passes and x pass (lines), and the x jobs'
+  // first block per box
+  int4* d_zjobs = nullptr;
+  int4* d_yjobs = nullptr;
+  int4* d_xjobs = nullptr;
+  int* d_xjob_begin = nullptr;    // [nsys + 1]
+  int nzjobs = 0, nyjobs = 0, nxjobs = 0;
+  size_t zsmem = 0;
+  int reg_kmax = 0;               // longest axis of the batch's grids
+  std::vector<SysGeom> h_sys;     // a batch's boxes (host copy)
   int nt[3] = {0, 0, 0};
   int ntiles = 0;
   float* d_B[3] = {nullptr, nullptr, nullptr};  // |b(k)|^2 per axis

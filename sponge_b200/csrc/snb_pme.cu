@@ -20,9 +20,11 @@
 #include <cmath>
 #include <set>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "snb_fft.cuh"
+#include "snb_fft_reg.cuh"
 #include "snb_internal.h"
 
 namespace snb {
@@ -724,6 +726,260 @@ k_fft_x_influence(float2* __restrict__ FQ, int K1, int nc, FftAxis ax,
   influence_partials(e, v, partial);
 }
 
+// ---------------------------------------------------------------------------
+// The batch's convolution by the library's own passes: one launch per pass
+// over all boxes, each block on one box's lines (job {box, first, count}),
+// each thread on one line held in registers (snb_fft_reg.cuh).
+constexpr int kRegZPairs = 64;   // row pairs (threads) per block of the z passes
+constexpr int kRegLines = 128;   // lines (threads) per block of the y and x passes
+
+// z, forward: `pairs` pairs of real rows of N points from src (contiguous)
+// to their half spectra (NC = N / 2 + 1 complex per row) in dst, through
+// shared memory both ways so that global accesses are coalesced.  A pair
+// a + i b is one complex transform, separated as
+// A[k] = (Z[k] + conj Z[N-k]) / 2, B[k] = (Z[k] - conj Z[N-k]) / 2i.
+template <int N>
+__device__ __forceinline__ void regz_r2c(const float* __restrict__ src,
+                                         float2* __restrict__ dst, int pairs, float* sm) {
+  constexpr int NC = N / 2 + 1, S = N + 1, SC = NC + 1;
+  const int rows = 2 * pairs, p = threadIdx.x;
+  // rows of N (a multiple of 4) floats from a 16-byte aligned start: float4
+  // loads, eight in flight per thread
+  {
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    const int n4 = rows * N / 4;
+    for (int t0 = threadIdx.x; t0 < n4; t0 += 8 * blockDim.x) {
+      float4 q[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int t = t0 + u * blockDim.x;
+        if (t < n4) q[u] = s4[t];
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int t = t0 + u * blockDim.x;
+        if (t < n4) {
+          float* d = sm + (4 * t / N) * S + (4 * t) % N;
+          d[0] = q[u].x;
+          d[1] = q[u].y;
+          d[2] = q[u].z;
+          d[3] = q[u].w;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  float2 v[N];
+  if (p < pairs) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) v[n] = make_float2(sm[2 * p * S + n], sm[(2 * p + 1) * S + n]);
+  }
+  __syncthreads();
+  float2* out = reinterpret_cast<float2*>(sm);
+  if (p < pairs) {
+    fft_reg<N, -1>(v);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+      const float2 zk = v[k], zm = v[(N - k) % N];
+      out[2 * p * SC + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      out[(2 * p + 1) * SC + k] = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < rows * NC; t += blockDim.x) dst[t] = out[(t / NC) * SC + t % NC];
+}
+
+// Eight float2 loads in flight per thread: src[0, count) into the padded
+// rows of `in` (NC per row, stride SC).
+template <int NC, int SC>
+__device__ __forceinline__ void regz_load_spec(const float2* __restrict__ src, float2* in,
+                                               int count) {
+  for (int t0 = threadIdx.x; t0 < count; t0 += 8 * blockDim.x) {
+    float2 q[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < count) q[u] = src[t];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < count) in[(t / NC) * SC + t % NC] = q[u];
+    }
+  }
+}
+
+// z, inverse: half spectra back to pairs of real rows.  Z = A + i B over the
+// full spectrum (A[N-k] = conj A[k]); the imaginary parts of the points 0
+// and N / 2 of a half spectrum are dropped (a real row's spectrum has none).
+template <int N>
+__device__ __forceinline__ void regz_c2r(const float2* __restrict__ src,
+                                         float* __restrict__ dst, int pairs, float* sm) {
+  constexpr int NC = N / 2 + 1, S = N + 1, SC = NC + 1;
+  const int rows = 2 * pairs, p = threadIdx.x;
+  float2* in = reinterpret_cast<float2*>(sm);
+  regz_load_spec<NC, SC>(src, in, rows * NC);
+  __syncthreads();
+  float2 v[N];
+  if (p < pairs) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      float2 a, b;
+      if (k < NC) {
+        a = in[2 * p * SC + k];
+        b = in[(2 * p + 1) * SC + k];
+        if (k == 0 || 2 * k == N) {
+          a.y = 0.f;
+          b.y = 0.f;
+        }
+      } else {
+        a = in[2 * p * SC + N - k];
+        b = in[(2 * p + 1) * SC + N - k];
+        a.y = -a.y;
+        b.y = -b.y;
+      }
+      v[k] = make_float2(a.x - b.y, a.y + b.x);
+    }
+  }
+  __syncthreads();
+  if (p < pairs) {
+    fft_reg<N, 1>(v);
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      sm[2 * p * S + n] = v[n].x;
+      sm[(2 * p + 1) * S + n] = v[n].y;
+    }
+  }
+  __syncthreads();
+  float4* d4 = reinterpret_cast<float4*>(dst);  // 16-byte aligned rows of N floats
+  for (int t = threadIdx.x; t < rows * N / 4; t += blockDim.x) {
+    const float* q = sm + (4 * t / N) * S + (4 * t) % N;
+    d4[t] = make_float4(q[0], q[1], q[2], q[3]);
+  }
+}
+
+// Shared bytes of a z block for axes up to kmax.
+inline size_t regz_smem(int kmax) {
+  return sizeof(float) * 2 * kRegZPairs * (size_t)(kmax + 4);
+}
+
+// KMAX: the longest axis compiled in (the register count follows it).
+template <bool R2C, int KMAX>
+__global__ void __launch_bounds__(kRegZPairs)
+k_fftb_z(float* __restrict__ Q, float2* __restrict__ FQ, const int4* __restrict__ jobs,
+         BatchView bv) {
+  extern __shared__ float regz_sm[];
+  const int4 jb = jobs[blockIdx.x];  // {box, first row pair, pairs}
+  const SysGeom& g = bv.sys[jb.x];
+  const int N = g.K2, nc = N / 2 + 1;
+  float* rows = Q + g.grid_begin + (size_t)(2 * jb.y) * N;
+  float2* spec = FQ + g.spec_begin + (size_t)(2 * jb.y) * nc;
+  switch (N) {
+#define SNB_CASE(n)                                              \
+  case n:                                                        \
+    if constexpr (n <= KMAX) {                                   \
+      if (R2C)                                                   \
+        regz_r2c<n>(rows, spec, jb.z, regz_sm);                  \
+      else                                                       \
+        regz_c2r<n>(spec, rows, jb.z, regz_sm);                  \
+    }                                                            \
+    break;
+    SNB_REG_FFT_SIZES(SNB_CASE)
+#undef SNB_CASE
+    default:
+      break;
+  }
+}
+
+// y pass: the line (x, kz) of a box's half spectrum [K0][K1][nc], K1 = N.
+template <int N, int DIR>
+__device__ __forceinline__ void regy(float2* __restrict__ box, int nc, int line) {
+  const int x = line / nc, kz = line - x * nc;
+  float2* base = box + (size_t)x * N * nc + kz;
+  float2 v[N];
+#pragma unroll
+  for (int y = 0; y < N; ++y) v[y] = base[(size_t)y * nc];
+  fft_reg<N, DIR>(v);
+#pragma unroll
+  for (int y = 0; y < N; ++y) base[(size_t)y * nc] = v[y];
+}
+
+template <int DIR, int KMAX>
+__global__ void __launch_bounds__(kRegLines, KMAX <= 40 ? 4 : 1)
+k_fftb_y(float2* __restrict__ FQ, const int4* __restrict__ jobs, BatchView bv) {
+  const int4 jb = jobs[blockIdx.x];  // {box, first line, lines}
+  if ((int)threadIdx.x >= jb.z) return;
+  const SysGeom& g = bv.sys[jb.x];
+  const int nc = g.K2 / 2 + 1, line = jb.y + threadIdx.x;
+  switch (g.K1) {
+#define SNB_CASE(n)                                              \
+  case n:                                                        \
+    if constexpr (n <= KMAX) regy<n, DIR>(FQ + g.spec_begin, nc, line); \
+    break;
+    SNB_REG_FFT_SIZES(SNB_CASE)
+#undef SNB_CASE
+    default:
+      break;
+  }
+}
+
+// x pass: the column (ky, kz) of a box's half spectrum, K0 = N: forward
+// transform, influence function (with the energy / virial sums), inverse.
+template <int N, bool VIRIAL>
+__device__ __forceinline__ void regx(float2* __restrict__ box, int K1, int nc, int line,
+                                     const SpecGeom& g, const float* __restrict__ B0,
+                                     const float* __restrict__ B1,
+                                     const float* __restrict__ B2, bool energy, double& e,
+                                     double* vir) {
+  const int ky = line / nc, kz = line - ky * nc;
+  const size_t stride = (size_t)K1 * nc;
+  float2* base = box + line;
+  float2 v[N];
+#pragma unroll
+  for (int x = 0; x < N; ++x) v[x] = base[x * stride];
+  fft_reg<N, -1>(v);
+#pragma unroll
+  for (int kx = 0; kx < N; ++kx)
+    v[kx] = influence_point<VIRIAL>(kx, ky, kz, g, B0, B1, B2, v[kx], energy, e, vir);
+  fft_reg<N, 1>(v);
+#pragma unroll
+  for (int x = 0; x < N; ++x) base[x * stride] = v[x];
+}
+
+template <bool VIRIAL, int KMAX>
+__global__ void __launch_bounds__(kRegLines, KMAX <= 40 ? 3 : 1)
+k_fftb_x_influence(float2* __restrict__ FQ, const int4* __restrict__ jobs, BatchView bv,
+                   const float* __restrict__ B0, const float* __restrict__ B1,
+                   const float* __restrict__ B2, double* __restrict__ partial, bool energy) {
+  const int4 jb = jobs[blockIdx.x];  // {box, first column, columns}
+  const SysGeom& sg = bv.sys[jb.x];
+  SpecGeom g;
+  g.K0 = sg.K0;
+  g.K1 = sg.K1;
+  g.K2 = sg.K2;
+  g.nc = sg.K2 / 2 + 1;
+  g.rcell = sg.rcell;
+  g.mpre = sg.mpre;
+  g.inv_pi_v = sg.inv_pi_v;
+  double e = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};
+  if ((int)threadIdx.x < jb.z) {
+    const int line = jb.y + threadIdx.x;
+    switch (sg.K0) {
+#define SNB_CASE(n)                                                                     \
+  case n:                                                                               \
+    if constexpr (n <= KMAX)                                                            \
+      regx<n, VIRIAL>(FQ + sg.spec_begin, sg.K1, g.nc, line, g, B0 + sg.b_begin0,       \
+                      B1 + sg.b_begin1, B2 + sg.b_begin2, energy, e, vir);              \
+    break;
+      SNB_REG_FFT_SIZES(SNB_CASE)
+#undef SNB_CASE
+      default:
+        break;
+    }
+  }
+  influence_partials(e, vir, partial);  // every thread of the block
+}
+
 // Final FP64 sums of the block partials plus the self / neutralising energy:
 // E_self = -beta/sqrt(pi) sum q^2 - pi/(2 beta^2 V) (sum q)^2
 // (PM_force.cpp:1149-1162).
@@ -1068,12 +1324,65 @@ int pme_set_spread_shape(PME& p, int T, int W) {
 // The convolution by the own FFT passes (one box): radices and twiddles of
 // the three axes.  Refused when an axis is longer than kFftMaxN, the z axis
 // is odd, or a length has a prime factor above 7.
+// A batch: every axis of every box at most kRegFftMax points (factors 2, 3,
+// 5, 7, a multiple of 4); job tables of the five passes.
+static int pme_set_own_fft_batch(PME& p) {
+  for (const SysGeom& g : p.h_sys)
+    if (!reg_fft_size(g.K0) || !reg_fft_size(g.K1) || !reg_fft_size(g.K2))
+      return fail(kNotSupported, "PME: the own FFT of a batch needs axes of 4-64 points, "
+                                 "multiples of 4 with factors 2, 3, 5, 7");
+  if (!p.d_zjobs) {
+    std::vector<int4> zj, yj, xj;
+    std::vector<int> xb;
+    int kmax = 4;
+    for (int s = 0; s < (int)p.h_sys.size(); ++s) {
+      const SysGeom& g = p.h_sys[s];
+      const int nc = g.K2 / 2 + 1;
+      kmax = std::max({kmax, g.K0, g.K1, g.K2});
+      const int pairs = g.K0 * g.K1 / 2;  // K0 K1 is even (multiples of 4)
+      for (int a = 0; a < pairs; a += kRegZPairs)
+        zj.push_back(make_int4(s, a, std::min(kRegZPairs, pairs - a), 0));
+      const int ylines = g.K0 * nc;
+      for (int a = 0; a < ylines; a += kRegLines)
+        yj.push_back(make_int4(s, a, std::min(kRegLines, ylines - a), 0));
+      xb.push_back((int)xj.size());
+      const int xlines = g.K1 * nc;
+      for (int a = 0; a < xlines; a += kRegLines)
+        xj.push_back(make_int4(s, a, std::min(kRegLines, xlines - a), 0));
+    }
+    xb.push_back((int)xj.size());
+    auto up = [](auto** d, const auto& h) -> int {
+      SNB_CUDA_TRY(cudaMalloc(d, sizeof(h[0]) * h.size()));
+      SNB_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(h[0]) * h.size(), cudaMemcpyHostToDevice));
+      return kOk;
+    };
+    int rc = up(&p.d_zjobs, zj);
+    if (!rc) rc = up(&p.d_yjobs, yj);
+    if (!rc) rc = up(&p.d_xjobs, xj);
+    if (!rc) rc = up(&p.d_xjob_begin, xb);
+    if (rc) return rc;
+    p.nzjobs = (int)zj.size();
+    p.nyjobs = (int)yj.size();
+    p.nxjobs = (int)xj.size();
+    p.zsmem = regz_smem(kmax);
+    p.reg_kmax = kmax;
+    cudaFree(p.d_xpartial);
+    p.d_xpartial = nullptr;
+    SNB_CUDA_TRY(cudaMalloc(&p.d_xpartial, sizeof(double) * 8 * (size_t)p.nxjobs));
+  }
+  std::vector<float2> tw(kRegTwTotal);
+  reg_fft_twiddles(tw.data());
+  SNB_CUDA_TRY(cudaMemcpyToSymbol(c_reg_tw, tw.data(), sizeof(float2) * kRegTwTotal));
+  p.own_fft = true;
+  return kOk;
+}
+
 int pme_set_own_fft(PME& p, bool own) {
-  if (p.bv.nsys > 0) return fail(kNotSupported, "PME: own FFT of a batch");
   if (!own) {
     p.own_fft = false;
     return kOk;
   }
+  if (p.bv.nsys > 0) return pme_set_own_fft_batch(p);
   if (!p.d_tw[0]) {
     FftAxis ax[3];
     for (int d = 0; d < 3; ++d)
@@ -1232,6 +1541,7 @@ int pme_init_batch(PME& p, int n, std::vector<SysGeom>& sys, float cutoff,
   SNB_CUDA_TRY(cudaMalloc(&p.d_wide_tiles, sizeof(int)));
   SNB_CUDA_TRY(cudaMemset(p.d_wide_tiles, 0, sizeof(int)));
   if (scan_reserve(p.scan, p.ntiles)) return kCudaError;
+  p.h_sys = sys;
   for (auto& fg : p.groups) {
     int dims[3] = {fg.K[0], fg.K[1], fg.K[2]};
     if (cufftPlanMany(&fg.r2c, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C,
@@ -1258,6 +1568,10 @@ void pme_free(PME& p) {
   cudaFree(p.d_Q64);
   for (int d = 0; d < 3; ++d) cudaFree(p.d_tw[d]);
   cudaFree(p.d_xpartial);
+  cudaFree(p.d_zjobs);
+  cudaFree(p.d_yjobs);
+  cudaFree(p.d_xjobs);
+  cudaFree(p.d_xjob_begin);
   for (auto& fg : p.groups) {
     if (fg.r2c) cufftDestroy(fg.r2c);
     if (fg.c2r) cufftDestroy(fg.c2r);
@@ -1363,6 +1677,42 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
   sg.rcell = p.rcell;
   sg.mpre = (float)(M_PI * M_PI / ((double)p.beta * p.beta));
   sg.inv_pi_v = (float)(1.0 / (M_PI * p.volume));
+  if (batch && p.own_fft) {
+    // z, y, then x with the influence function and back, then y and z, one
+    // launch per pass over all boxes
+    float2* FQ = reinterpret_cast<float2*>(p.d_FQ);
+    auto passes = [&](auto kmax) {
+      constexpr int KM = decltype(kmax)::value;
+      k_fftb_z<true, KM><<<p.nzjobs, kRegZPairs, p.zsmem, st>>>(p.d_Q, FQ, p.d_zjobs, p.bv);
+      k_fftb_y<-1, KM><<<p.nyjobs, kRegLines, 0, st>>>(FQ, p.d_yjobs, p.bv);
+      if (need_virial)
+        k_fftb_x_influence<true, KM><<<p.nxjobs, kRegLines, 0, st>>>(
+            FQ, p.d_xjobs, p.bv, p.d_B[0], p.d_B[1], p.d_B[2], p.d_xpartial, need_energy);
+      else
+        k_fftb_x_influence<false, KM><<<p.nxjobs, kRegLines, 0, st>>>(
+            FQ, p.d_xjobs, p.bv, p.d_B[0], p.d_B[1], p.d_B[2], p.d_xpartial, need_energy);
+      if (need_energy || need_virial) {
+        k_pme_finish_batch<<<p.bv.nsys, 256, 0, st>>>(p.bv, p.d_xjob_begin, p.d_xpartial,
+                                                      p.d_frq, (double)p.beta, p.d_sys_sums,
+                                                      need_energy);
+        k_pme_sum_systems<<<1, 32, 0, st>>>(p.bv.nsys, p.d_sys_sums, p.d_sums);
+      }
+      k_fftb_y<1, KM><<<p.nyjobs, kRegLines, 0, st>>>(FQ, p.d_yjobs, p.bv);
+      k_fftb_z<false, KM><<<p.nzjobs, kRegZPairs, p.zsmem, st>>>(p.d_phi, FQ, p.d_zjobs,
+                                                                 p.bv);
+    };
+    if (p.reg_kmax <= 32)
+      passes(std::integral_constant<int, 32>());
+    else if (p.reg_kmax <= 40)
+      passes(std::integral_constant<int, 40>());
+    else
+      passes(std::integral_constant<int, kRegFftMax>());
+    const int gt = p.gather_threads;  // 4 lanes per atom
+    k_pme_gather<kAccumFixed, true><<<ceil_div(n, gt / 4), gt, 0, st>>>(
+        n, p.d_frq, p.d_upk, g, p.d_phi, 1.0f, acc, p.bv);
+    SNB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+  }
   if (!batch && p.own_fft) {
     // z, y, then x with the influence function and back, then y and z
     float2* FQ = reinterpret_cast<float2*>(p.d_FQ);

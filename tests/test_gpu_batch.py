@@ -191,3 +191,49 @@ def test_batch_rejects_cross_system_exclusion(g, boxes):
                               el.ctypes.data, c["n_excl"], ct.byref(h))
     assert rc == 1
     assert b"between two systems" in lib.snb_last_error()
+
+
+def test_batch_own_fft_matches_cufft(g, boxes):
+    """The batch's own FFT passes (one launch per pass over the five boxes'
+    grids 20^3-28^3, lines in registers) against the batched cuFFT plans
+    through the whole batch force: forces, reciprocal energy and virial agree
+    to float rounding, and no cuFFT kernel is left in the step graph."""
+    import torch
+    from sponge_b200 import systems
+    lib = g.capi.load()
+    out = []
+    for own in (0, 1):
+        h, c = g.batch_create(boxes, CUTOFF)
+        n = len(c["charge"])
+        try:
+            shapes = np.zeros(9, np.int32)
+            crd = g.dev(c["crd"])
+            vel = g.dev(np.zeros_like(c["crd"]))
+            invm = g.dev((1.0 / c["mass"]).astype(np.float32))
+            st = torch.cuda.Stream()
+            sp = ctypes.c_void_p(st.cuda_stream)
+            # the engine's own shapes first, then the FFT switched
+            with torch.cuda.stream(st):
+                g.capi.check(lib.snb_engine_autotune(h, g.ptr(crd), g.ptr(vel), g.ptr(invm),
+                                                     ctypes.c_float(0.0), 1,
+                                                     shapes.ctypes.data, sp), "autotune")
+            st.synchronize()
+            shapes[8] = own
+            g.capi.check(lib.snb_engine_set_launch_shapes(h, shapes.ctypes.data), "shapes")
+            frc, tot = _force(g, h, crd, n)
+            with torch.cuda.stream(st):
+                g.capi.check(lib.snb_engine_md_steps_graph(
+                    h, g.ptr(crd), g.ptr(vel), g.ptr(invm),
+                    ctypes.c_float(0.5e-3 * systems.TIME_CONVERSION), 0, 2, sp), "md")
+            st.synchronize()
+            kn, libk, bodyk = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+            g.capi.check(lib.snb_engine_graph_info(h, ctypes.byref(kn), ctypes.byref(libk),
+                                                   ctypes.byref(bodyk), sp), "graph_info")
+        finally:
+            lib.snb_engine_destroy(h)
+        out.append((frc, tot, libk.value))
+    (f0, t0, l0), (f1, t1, l1) = out
+    assert l0 > 0 and l1 == 0
+    assert g.rel_rms(f1, f0) <= 1e-6
+    assert abs(t1[4] - t0[4]) <= 1e-6 * abs(t0[4])
+    assert np.all(np.abs(t1[8:14] - t0[8:14]) <= 1e-6 * np.abs(t0[8:14]).max())
