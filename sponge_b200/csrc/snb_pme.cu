@@ -590,24 +590,41 @@ struct SpecGeom {
 
 constexpr int kSpecBlock = 256;
 
+// The influence BC(m) of the point (kx, ky, kz) of the half spectrum (0 at
+// the origin), with m and |m|^2.
+__device__ __forceinline__ float influence_bc(int kx, int ky, int kz, const SpecGeom& g,
+                                              const float* __restrict__ B0,
+                                              const float* __restrict__ B1,
+                                              const float* __restrict__ B2, float& mx,
+                                              float& my, float& mz, float& msq) {
+  const bool origin = (kx | ky | kz) == 0;
+  float kxr = kx > g.K0 / 2 ? kx - g.K0 : kx;
+  float kyr = ky > g.K1 / 2 ? ky - g.K1 : ky;
+  float kzr = kz;
+  mx = kxr * g.rcell.a11;
+  my = kxr * g.rcell.a21 + kyr * g.rcell.a22;
+  mz = kxr * g.rcell.a31 + kyr * g.rcell.a32 + kzr * g.rcell.a33;
+  msq = mx * mx + my * my + mz * mz;
+  float bc = 0.f;
+  if (!origin) bc = g.inv_pi_v / msq * expf(-g.mpre * msq) * B0[kx] * B1[ky] * B2[kz];
+  return bc;
+}
+
 // One point (kx, ky, kz) of the half spectrum: its influence BC(m) (0 at the
 // origin) scales c, and |c|^2 BC feeds the energy and virial sums.
+// bc_given >= 0: BC taken from a table instead of computed (m is still
+// computed for the virial).
 template <bool VIRIAL>
 __device__ __forceinline__ float2 influence_point(int kx, int ky, int kz, const SpecGeom& g,
                                                   const float* __restrict__ B0,
                                                   const float* __restrict__ B1,
                                                   const float* __restrict__ B2, float2 c,
-                                                  bool energy, double& e, double* v) {
+                                                  bool energy, double& e, double* v,
+                                                  float bc_given = -1.0f) {
   const bool origin = (kx | ky | kz) == 0;
-  float kxr = kx > g.K0 / 2 ? kx - g.K0 : kx;
-  float kyr = ky > g.K1 / 2 ? ky - g.K1 : ky;
-  float kzr = kz;
-  float mx = kxr * g.rcell.a11;
-  float my = kxr * g.rcell.a21 + kyr * g.rcell.a22;
-  float mz = kxr * g.rcell.a31 + kyr * g.rcell.a32 + kzr * g.rcell.a33;
-  float msq = mx * mx + my * my + mz * mz;
-  float bc = 0.f;
-  if (!origin) bc = g.inv_pi_v / msq * expf(-g.mpre * msq) * B0[kx] * B1[ky] * B2[kz];
+  float mx, my, mz, msq;
+  float bc = influence_bc(kx, ky, kz, g, B0, B1, B2, mx, my, mz, msq);
+  if (bc_given >= 0.0f) bc = bc_given;
   float f2 = c.x * c.x + c.y * c.y;
   if (energy) {
     float we = (kz == 0 || (2 * kz == g.K2)) ? 0.5f : 1.0f;
@@ -924,13 +941,17 @@ k_fftb_y(float2* __restrict__ FQ, const int4* __restrict__ jobs, BatchView bv) {
 }
 
 // x pass: the column (ky, kz) of a box's half spectrum, K0 = N: forward
-// transform, influence function (with the energy / virial sums), inverse.
-template <int N, bool VIRIAL>
+// transform, influence function read from the box's table (in the
+// spectrum's layout; with SUMS also the energy / virial sums), inverse.
+// Every call takes BC from the table, so the forces do not depend on
+// whether the sums are asked for.
+template <int N, bool VIRIAL, bool SUMS>
 __device__ __forceinline__ void regx(float2* __restrict__ box, int K1, int nc, int line,
                                      const SpecGeom& g, const float* __restrict__ B0,
                                      const float* __restrict__ B1,
-                                     const float* __restrict__ B2, bool energy, double& e,
-                                     double* vir) {
+                                     const float* __restrict__ B2,
+                                     const float* __restrict__ bc_box, bool energy,
+                                     double& e, double* vir) {
   const int ky = line / nc, kz = line - ky * nc;
   const size_t stride = (size_t)K1 * nc;
   float2* base = box + line;
@@ -939,18 +960,27 @@ __device__ __forceinline__ void regx(float2* __restrict__ box, int K1, int nc, i
   for (int x = 0; x < N; ++x) v[x] = base[x * stride];
   fft_reg<N, -1>(v);
 #pragma unroll
-  for (int kx = 0; kx < N; ++kx)
-    v[kx] = influence_point<VIRIAL>(kx, ky, kz, g, B0, B1, B2, v[kx], energy, e, vir);
+  for (int kx = 0; kx < N; ++kx) {
+    const float bc = bc_box[line + kx * stride];
+    if (SUMS) {
+      v[kx] = influence_point<VIRIAL>(kx, ky, kz, g, B0, B1, B2, v[kx], energy, e, vir, bc);
+    } else {
+      v[kx].x *= bc;
+      v[kx].y *= bc;
+    }
+  }
   fft_reg<N, 1>(v);
 #pragma unroll
   for (int x = 0; x < N; ++x) base[x * stride] = v[x];
 }
 
-template <bool VIRIAL, int KMAX>
+// SUMS: the energy / virial sums too (into partial).
+template <bool VIRIAL, int KMAX, bool SUMS>
 __global__ void __launch_bounds__(kRegLines, KMAX <= 40 ? 3 : 1)
 k_fftb_x_influence(float2* __restrict__ FQ, const int4* __restrict__ jobs, BatchView bv,
                    const float* __restrict__ B0, const float* __restrict__ B1,
-                   const float* __restrict__ B2, double* __restrict__ partial, bool energy) {
+                   const float* __restrict__ B2, const float* __restrict__ bc,
+                   double* __restrict__ partial, bool energy) {
   const int4 jb = jobs[blockIdx.x];  // {box, first column, columns}
   const SysGeom& sg = bv.sys[jb.x];
   SpecGeom g;
@@ -968,8 +998,9 @@ k_fftb_x_influence(float2* __restrict__ FQ, const int4* __restrict__ jobs, Batch
 #define SNB_CASE(n)                                                                     \
   case n:                                                                               \
     if constexpr (n <= KMAX)                                                            \
-      regx<n, VIRIAL>(FQ + sg.spec_begin, sg.K1, g.nc, line, g, B0 + sg.b_begin0,       \
-                      B1 + sg.b_begin1, B2 + sg.b_begin2, energy, e, vir);              \
+      regx<n, VIRIAL, SUMS>(FQ + sg.spec_begin, sg.K1, g.nc, line, g, B0 + sg.b_begin0,  \
+                            B1 + sg.b_begin1, B2 + sg.b_begin2, bc + sg.spec_begin,     \
+                            energy, e, vir);                                            \
     break;
       SNB_REG_FFT_SIZES(SNB_CASE)
 #undef SNB_CASE
@@ -977,7 +1008,31 @@ k_fftb_x_influence(float2* __restrict__ FQ, const int4* __restrict__ jobs, Batch
         break;
     }
   }
-  influence_partials(e, vir, partial);  // every thread of the block
+  if (SUMS) influence_partials(e, vir, partial);  // every thread of the block
+}
+
+// A batch's influence table: BC at every point of every box's half
+// spectrum (the boxes of a batch do not change).
+__global__ void __launch_bounds__(kSpecBlock)
+k_pme_bc_table(BatchView bv, const int4* __restrict__ blocks, const float* __restrict__ B0,
+               const float* __restrict__ B1, const float* __restrict__ B2,
+               float* __restrict__ bc) {
+  const int4 bk = blocks[blockIdx.x];  // {system, first, end} of one box's spectrum
+  const SysGeom& sg = bv.sys[bk.x];
+  SpecGeom g;
+  g.K0 = sg.K0;
+  g.K1 = sg.K1;
+  g.K2 = sg.K2;
+  g.nc = sg.K2 / 2 + 1;
+  g.rcell = sg.rcell;
+  g.mpre = sg.mpre;
+  g.inv_pi_v = sg.inv_pi_v;
+  for (int idx = bk.y + threadIdx.x; idx < bk.z; idx += blockDim.x) {
+    const int kz = idx % g.nc, ky = (idx / g.nc) % g.K1, kx = idx / (g.nc * g.K1);
+    float mx, my, mz, msq;
+    bc[sg.spec_begin + idx] = influence_bc(kx, ky, kz, g, B0 + sg.b_begin0, B1 + sg.b_begin1,
+                                           B2 + sg.b_begin2, mx, my, mz, msq);
+  }
 }
 
 // Final FP64 sums of the block partials plus the self / neutralising energy:
@@ -1366,6 +1421,11 @@ static int pme_set_own_fft_batch(PME& p) {
     p.nxjobs = (int)xj.size();
     p.zsmem = regz_smem(kmax);
     p.reg_kmax = kmax;
+    SNB_CUDA_TRY(cudaMalloc(&p.d_bc, sizeof(float) * (size_t)p.nfft));
+    k_pme_bc_table<<<p.spec_blocks, kSpecBlock>>>(p.bv, p.d_spec_blocks, p.d_B[0], p.d_B[1],
+                                                  p.d_B[2], p.d_bc);
+    SNB_CUDA_TRY(cudaGetLastError());
+    SNB_CUDA_TRY(cudaDeviceSynchronize());
     cudaFree(p.d_xpartial);
     p.d_xpartial = nullptr;
     SNB_CUDA_TRY(cudaMalloc(&p.d_xpartial, sizeof(double) * 8 * (size_t)p.nxjobs));
@@ -1569,6 +1629,7 @@ void pme_free(PME& p) {
   for (int d = 0; d < 3; ++d) cudaFree(p.d_tw[d]);
   cudaFree(p.d_xpartial);
   cudaFree(p.d_zjobs);
+  cudaFree(p.d_bc);
   cudaFree(p.d_yjobs);
   cudaFree(p.d_xjobs);
   cudaFree(p.d_xjob_begin);
@@ -1686,11 +1747,16 @@ int pme_after_bin(PME& p, int n, Accumulators& acc, int accum, bool need_energy,
       k_fftb_z<true, KM><<<p.nzjobs, kRegZPairs, p.zsmem, st>>>(p.d_Q, FQ, p.d_zjobs, p.bv);
       k_fftb_y<-1, KM><<<p.nyjobs, kRegLines, 0, st>>>(FQ, p.d_yjobs, p.bv);
       if (need_virial)
-        k_fftb_x_influence<true, KM><<<p.nxjobs, kRegLines, 0, st>>>(
-            FQ, p.d_xjobs, p.bv, p.d_B[0], p.d_B[1], p.d_B[2], p.d_xpartial, need_energy);
-      else
-        k_fftb_x_influence<false, KM><<<p.nxjobs, kRegLines, 0, st>>>(
-            FQ, p.d_xjobs, p.bv, p.d_B[0], p.d_B[1], p.d_B[2], p.d_xpartial, need_energy);
+        k_fftb_x_influence<true, KM, true><<<p.nxjobs, kRegLines, 0, st>>>(
+            FQ, p.d_xjobs, p.bv, p.d_B[0], p.d_B[1], p.d_B[2], p.d_bc, p.d_xpartial,
+            need_energy);
+      else if (need_energy)
+        k_fftb_x_influence<false, KM, true><<<p.nxjobs, kRegLines, 0, st>>>(
+            FQ, p.d_xjobs, p.bv, p.d_B[0], p.d_B[1], p.d_B[2], p.d_bc, p.d_xpartial,
+            need_energy);
+      else  // forces only: no sums
+        k_fftb_x_influence<false, KM, false><<<p.nxjobs, kRegLines, 0, st>>>(
+            FQ, p.d_xjobs, p.bv, p.d_B[0], p.d_B[1], p.d_B[2], p.d_bc, nullptr, false);
       if (need_energy || need_virial) {
         k_pme_finish_batch<<<p.bv.nsys, 256, 0, st>>>(p.bv, p.d_xjob_begin, p.d_xpartial,
                                                       p.d_frq, (double)p.beta, p.d_sys_sums,

@@ -237,3 +237,53 @@ def test_batch_own_fft_matches_cufft(g, boxes):
     assert g.rel_rms(f1, f0) <= 1e-6
     assert abs(t1[4] - t0[4]) <= 1e-6 * abs(t0[4])
     assert np.all(np.abs(t1[8:14] - t0[8:14]) <= 1e-6 * np.abs(t0[8:14]).max())
+
+
+def test_batch_own_fft_every_class_of_length(g):
+    """Grids of 24, 32, 36, 48, 56 and 64 points per axis in one batch (the
+    register passes compiled for the longest axis, 64): the whole batch
+    force with the own passes against the batched cuFFT plans."""
+    import torch
+    from sponge_b200 import systems
+    boxes = [systems.water_box(nw, seed=k, ion_pairs=None)
+             for k, nw in enumerate([381, 948, 1373, 3361, 5411, 8161])]
+    assert sorted({systems.fft_size(b.box) for b in boxes}) == [24, 32, 36, 48, 56, 64]
+    lib = g.capi.load()
+    out = []
+    for own in (0, 1):
+        h, c = g.batch_create(boxes, CUTOFF)
+        try:
+            shapes = np.array([2, 0, 16, 128, 16, 8, 2, 0, own], np.int32)
+            g.capi.check(lib.snb_engine_set_launch_shapes(h, shapes.ctypes.data), "shapes")
+            out.append(_force(g, h, g.dev(c["crd"]), len(c["charge"])))
+        finally:
+            lib.snb_engine_destroy(h)
+    (f0, t0), (f1, t1) = out
+    assert g.rel_rms(f1, f0) <= 1e-6
+    assert abs(t1[4] - t0[4]) <= 1e-6 * abs(t0[4])
+    assert np.all(np.abs(t1[8:14] - t0[8:14]) <= 1e-6 * np.abs(t0[8:14]).max())
+
+
+def test_batch_force_only_own_fft_matches_cufft(g, boxes):
+    """Force-only calls of a batch (the own passes multiply by the table of
+    the influence function and form no sums) against the batched cuFFT
+    plans."""
+    import torch
+    lib = g.capi.load()
+    out = []
+    for own in (0, 1):
+        h, c = g.batch_create(boxes, CUTOFF)
+        n = len(c["charge"])
+        try:
+            shapes = np.array([2, 0, 16, 128, 16, 8, 2, 0, own], np.int32)
+            g.capi.check(lib.snb_engine_set_launch_shapes(h, shapes.ctypes.data), "shapes")
+            crd = g.dev(c["crd"])
+            frc = torch.zeros(3 * n, dtype=torch.float32, device="cuda")
+            tot = torch.zeros(16, dtype=torch.float64, device="cuda")
+            g.capi.check(lib.snb_engine_force(h, g.ptr(crd), g.ptr(frc), 0, 0, 0,
+                                              g.ptr(tot), g.stream()), "engine_force")
+            torch.cuda.synchronize()
+            out.append(frc.cpu().numpy())
+        finally:
+            lib.snb_engine_destroy(h)
+    assert g.rel_rms(out[1], out[0]) <= 1e-6
